@@ -1,0 +1,323 @@
+/*
+ * splat_cuda.h — C ABI of libsplatcuda.so, the sm_100a implementation of
+ * nano-optimize's differentiable Gaussian-splat rasteriser and optimiser
+ * step (ssoj13/nanotracer, crates/nano-optimize).
+ *
+ * Every entry point below names the reference interface it replaces
+ * (file:line inside the reference project).  Conventions:
+ *
+ *   - Plain C types only: device memory is passed as `void*`/typed device
+ *     pointers obtained from sc_buffer_alloc (or any cudaMalloc'd memory on
+ *     the context's device), sizes are element counts, compound objects are
+ *     opaque handles owned by the library.
+ *   - Every call returns sc_status.  The reference panics or asserts where
+ *     this ABI returns SC_ERR_INVALID_ARG / SC_ERR_CAPACITY; the one call that
+ *     returned Result in the reference (WgpuCtx::new) maps to sc_ctx_create.
+ *   - All calls are asynchronous on the context's stream except
+ *     *_readback, sc_*_info, sc_ctx_synchronize and the PLY functions, which
+ *     block — matching WgpuCtx::readback (gpu.rs:119-152).
+ *   - A context is thread-compatible (one thread at a time), like one
+ *     WgpuCtx per thread in the reference (docs/src/decisions.md:161-165).
+ *   - Bounded device-side waits: kernels that spin on a flag (decoupled
+ *     look-back) give up after a fixed iteration count and raise
+ *     SC_ERR_TIMEOUT on the next status check instead of hanging.
+ */
+#ifndef SPLAT_CUDA_H
+#define SPLAT_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SC_ABI_VERSION 1
+
+typedef enum sc_status {
+  SC_OK = 0,
+  SC_ERR_INVALID_ARG = 1,  /* a size, pointer or handle is invalid              */
+  SC_ERR_OOM = 2,          /* device allocation failed                           */
+  SC_ERR_CAPACITY = 3,     /* a device-side capacity overflowed (retry larger)   */
+  SC_ERR_CUDA = 4,         /* a CUDA runtime error; sc_last_error() says which   */
+  SC_ERR_TIMEOUT = 5,      /* a bounded device wait gave up                      */
+  SC_ERR_NONFINITE = 6,    /* non-finite values where finite ones are required   */
+  SC_ERR_IO = 7,           /* file could not be opened / read / written          */
+  SC_ERR_FORMAT = 8        /* PLY header or record not understood                */
+} sc_status;
+
+typedef struct sc_ctx sc_ctx;          /* device + stream + scratch arena    */
+typedef struct sc_splats sc_splats;    /* GpuSplatBuffer                     */
+typedef struct sc_grads sc_grads;      /* GradSplatBuffers                   */
+typedef struct sc_moments sc_moments;  /* AdamMomentBuffers                  */
+typedef struct sc_bins sc_bins;        /* TileBinningResult                  */
+typedef struct sc_trainer sc_trainer;  /* batched whole-iteration trainer    */
+
+/* Host splat arrays, the flat layout of SplatBuffer (splat_store.rs:20-36):
+ * positions n*3, rotations n*4 (w,x,y,z), scales n*3 (log sigma),
+ * opacities n (logit), sh_dc n*3, sh_rest n*45 planar R[15] G[15] B[15].
+ * The same struct carries gradients and Adam moments (AdamState slabs,
+ * adam.rs:48-56, train.rs:84-89) in identical layout. */
+typedef struct sc_host_splats {
+  uint32_t n;
+  float* positions;
+  float* rotations;
+  float* scales;
+  float* opacities;
+  float* sh_dc;
+  float* sh_rest;
+} sc_host_splats;
+
+/* CameraUniform (raster.rs:60-77): 96 bytes, view is column-major. */
+typedef struct sc_camera {
+  float view[16];
+  float cam_pos[3];
+  float near_plane;
+  float focal;
+  float width;
+  float height;
+  uint32_t n_splats;
+} sc_camera;
+
+/* TilingParams (tile_binner.rs:21-42).  The reference's square tile_size is
+ * tile_w == tile_h; non-square tiles (32x8) are an extension. */
+typedef struct sc_tiling {
+  uint32_t width;
+  uint32_t height;
+  uint32_t tile_w;
+  uint32_t tile_h;
+  float depth_max;
+} sc_tiling;
+
+/* ProjectedSplat (raster.rs:27-37), 48 bytes. */
+typedef struct sc_projected_splat {
+  float mean_xy[2];
+  float depth;
+  float radius;
+  float conic[3];
+  float visible;
+  float color[3];
+  float opacity;
+} sc_projected_splat;
+
+/* ProjectedGrad (raster.rs:46-55), 48 bytes. */
+typedef struct sc_projected_grad {
+  float dmean_opacity[4]; /* dmean.xy, dopacity, pad */
+  float dconic[4];        /* a, b, c, pad            */
+  float dcolor[4];        /* r, g, b, pad            */
+} sc_projected_grad;
+
+/* AdamConfig (adam.rs:22-39). */
+typedef struct sc_adam_config {
+  float lr;
+  float beta1;
+  float beta2;
+  float eps;
+} sc_adam_config;
+
+/* Six learning-rate groups (pos, rot, scale, opacity, sh_dc, sh_rest).  The
+ * reference's two groups (adam_gpu.rs:334-427: pos vs the rest) are
+ * lr = {pos, attr, attr, attr, attr, attr}. */
+typedef struct sc_adam_groups {
+  float lr[6];
+  float beta1;
+  float beta2;
+  float eps;
+} sc_adam_groups;
+
+/* Backward transmittance semantics.
+ * SC_BWD_REF:   rasterize_backward.wgsl:73-210 — reverse walk over every
+ *               entry of the tile from T = 1 - out.w, stopping at T > 1.0001.
+ * SC_BWD_EXACT: reverse walk from each pixel's last contributor with the
+ *               final transmittance recorded by the forward (aux buffer). */
+typedef enum sc_bwd_mode { SC_BWD_REF = 0, SC_BWD_EXACT = 1 } sc_bwd_mode;
+
+/* Key layouts for sc_bin.
+ * SC_KEYS_REF32: (tile_id << 16) | u16(depth/depth_max * 65535), 32-bit keys,
+ *                tile_emit.wgsl:54-61; at most 65536 tiles.
+ * SC_KEYS_NATIVE64: (tile_id << 32) | float_bits(depth), 64-bit keys. */
+typedef enum sc_key_mode { SC_KEYS_REF32 = 0, SC_KEYS_NATIVE64 = 1 } sc_key_mode;
+
+#define SC_SPLATS_BF16_REST 1u   /* sh_rest stored as bf16 on the device    */
+#define SC_MOMENTS_BF16 1u       /* Adam m and v stored as bf16             */
+
+/* ------------------------------------------------------------------ runtime
+ * replaces WgpuCtx (crates/nano-optimize/src/gpu.rs:21-153) */
+const char* sc_status_string(sc_status s);
+int sc_abi_version(void);
+sc_status sc_ctx_create(int device, sc_ctx** out);                 /* WgpuCtx::new, gpu.rs:31-77 */
+void sc_ctx_destroy(sc_ctx* ctx);
+const char* sc_last_error(const sc_ctx* ctx);
+sc_status sc_ctx_synchronize(sc_ctx* ctx);                         /* queue.poll(Wait), gpu.rs:140-146 */
+void* sc_ctx_stream(sc_ctx* ctx);                                  /* the cudaStream_t calls run on */
+sc_status sc_ctx_set_stream(sc_ctx* ctx, void* stream);
+sc_status sc_ctx_device_info(sc_ctx* ctx, int* sm_count, size_t* free_bytes, size_t* total_bytes);
+/* Number of kernels this context has launched so far (diagnostics / bench). */
+uint64_t sc_ctx_launch_count(const sc_ctx* ctx);
+sc_status sc_buffer_alloc(sc_ctx* ctx, size_t bytes, void** dptr);  /* storage_buffer_zeroed, gpu.rs:98-107 */
+sc_status sc_buffer_free(sc_ctx* ctx, void* dptr);
+sc_status sc_buffer_upload(sc_ctx* ctx, void* dst, const void* src, size_t bytes);   /* queue.write_buffer */
+sc_status sc_buffer_readback(sc_ctx* ctx, void* dst, const void* src, size_t bytes); /* readback, gpu.rs:119-152 */
+sc_status sc_buffer_zero(sc_ctx* ctx, void* dptr, size_t bytes);
+
+/* ------------------------------------------------------------- parameters
+ * replaces GpuSplatBuffer / GradSplatBuffers / AdamMomentBuffers
+ * (crates/nano-optimize/src/splat_gpu.rs:29-423) */
+sc_status sc_splats_upload(sc_ctx* ctx, const sc_host_splats* src, uint32_t capacity, uint32_t flags,
+                           sc_splats** out);                        /* GpuSplatBuffer::upload, splat_gpu.rs:94-120 */
+sc_status sc_splats_sync_from(sc_ctx* ctx, sc_splats* dst, const sc_host_splats* src); /* sync_from, :126-152 */
+sc_status sc_splats_readback(sc_ctx* ctx, const sc_splats* src, sc_host_splats* dst);  /* readback, :156-187 */
+uint32_t sc_splats_count(const sc_splats* s);
+uint32_t sc_splats_capacity(const sc_splats* s);
+void sc_splats_free(sc_ctx* ctx, sc_splats* s);
+
+sc_status sc_grads_create(sc_ctx* ctx, uint32_t capacity, sc_grads** out);  /* GradSplatBuffers::new, :36-57 */
+sc_status sc_grads_zero(sc_ctx* ctx, sc_grads* g, uint32_t n);               /* GradSplatBuffers::zero, :62-75 */
+sc_status sc_grads_upload(sc_ctx* ctx, sc_grads* g, const sc_host_splats* src);
+sc_status sc_grads_readback(sc_ctx* ctx, const sc_grads* g, uint32_t n, sc_host_splats* dst);
+void sc_grads_free(sc_ctx* ctx, sc_grads* g);
+
+sc_status sc_moments_create(sc_ctx* ctx, uint32_t capacity, uint32_t flags, sc_moments** out); /* :202-240 */
+sc_status sc_moments_upload(sc_ctx* ctx, sc_moments* mo, const sc_host_splats* m, const sc_host_splats* v); /* :246-300 */
+sc_status sc_moments_readback(sc_ctx* ctx, const sc_moments* mo, uint32_t n, sc_host_splats* m,
+                              sc_host_splats* v);                             /* download_to_cpu */
+void sc_moments_free(sc_ctx* ctx, sc_moments* mo);
+
+/* ------------------------------------------------------------- rasteriser
+ * replaces Rasterizer (crates/nano-optimize/src/raster.rs:103-804) */
+void sc_camera_from_pose(const float eye[3], const float target[3], const float up[3], float fov_y,
+                         uint32_t width, uint32_t height, uint32_t n_splats,
+                         sc_camera* out);                            /* CameraUniform::from_pose, raster.rs:79-99 */
+
+/* project_gaussians.wgsl:156-259 for n_views cameras: projected holds
+ * n_views * sc_splats_capacity() records, view-major. */
+sc_status sc_project(sc_ctx* ctx, const sc_splats* s, const sc_camera* cams, uint32_t n_views,
+                     sc_projected_splat* projected);                 /* Rasterizer::project, raster.rs:731-794 */
+
+/* ----------------------------------------------------------- tile binner
+ * replaces TileBinner / RadixSort / PrefixScan
+ * (tile_binner.rs:21-416, radix_sort.rs:32-303, prefix_scan.rs:18-258) */
+sc_status sc_bins_create(sc_ctx* ctx, sc_bins** out);
+void sc_bins_free(sc_ctx* ctx, sc_bins* b);
+/* Bins n_views * n_splats projected records (view-major, stride = stride_splats
+ * records per view).  Tiles of view v are numbered v*num_tiles + tile.
+ * Blocks once to read the pair count (tile_binner.rs:243-245 does the same). */
+sc_status sc_bin(sc_ctx* ctx, const sc_projected_splat* projected, uint32_t n_splats, uint32_t stride_splats,
+                 uint32_t n_views, const sc_tiling* tiling, sc_key_mode mode, sc_bins* bins); /* TileBinner::bin */
+/* total pairs, number of tiles (all views) and the device arrays of the last sc_bin:
+ * sorted keys (uint32 for REF32, uint64 for NATIVE64), payloads (uint32 splat
+ * index), tile ranges (2 x uint32 per tile, [begin, end), empty = (0,0)). */
+sc_status sc_bins_info(const sc_bins* b, uint64_t* total_pairs, uint32_t* num_tiles, const void** sorted_keys,
+                       const uint32_t** sorted_payloads, const uint32_t** tile_ranges);
+
+/* Stable LSD radix sort (onesweep, decoupled look-back) of n (key, value)
+ * pairs in place; keys_tmp / vals_tmp are ping-pong buffers of the same size.
+ * key_bits: number of low key bits that can be non-zero.  RadixSort::sort,
+ * radix_sort.rs:144-303 (32 one-bit passes there; 8-bit digits here). */
+sc_status sc_radix_sort_u32(sc_ctx* ctx, uint32_t* keys, uint32_t* vals, uint32_t* keys_tmp, uint32_t* vals_tmp,
+                            uint64_t n, uint32_t key_bits);
+sc_status sc_radix_sort_u64(sc_ctx* ctx, uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* vals_tmp,
+                            uint64_t n, uint32_t key_bits);
+/* Exclusive prefix sum of n uint32 in place (single pass, decoupled look-back);
+ * total (device pointer, may be NULL) receives the sum.  PrefixScan::scan,
+ * prefix_scan.rs:127-186 (limited to 2^24 elements there). */
+sc_status sc_exclusive_scan_u32(sc_ctx* ctx, uint32_t* data, uint64_t n, uint64_t* total);
+
+/* rasterize.wgsl:48-118 over n_views views; image is n_views*W*H float4
+ * (rgb, 1-T).  aux (nullable) receives per pixel {T_final bits, last
+ * contributor count} for SC_BWD_EXACT. */
+sc_status sc_composite(sc_ctx* ctx, const sc_projected_splat* projected, uint32_t stride_splats, uint32_t n_views,
+                       const sc_bins* bins, const sc_tiling* tiling, float* image,
+                       uint32_t* aux);                               /* Rasterizer::composite, raster.rs:468-529 */
+
+/* loss.rs:163-179 on the device: dl_dc = scale * 2 (p - t) / (3 W H) as float4,
+ * loss_out (device double, nullable) receives sum (p-t)^2 / (3 W H) per view.
+ * target is n_views*W*H float3. */
+sc_status sc_mse_loss_grad(sc_ctx* ctx, const float* pred, const float* target, uint32_t n_views,
+                           const sc_tiling* tiling, float scale, float* dl_dc, double* loss_out);
+
+/* rasterize_backward.wgsl:73-210: accumulates into projected_grad, which the
+ * caller zeroes first (raster.rs:647-651). */
+sc_status sc_composite_backward(sc_ctx* ctx, const sc_projected_splat* projected, uint32_t stride_splats,
+                                uint32_t n_views, const sc_bins* bins, const sc_tiling* tiling,
+                                const float* forward_out, const float* dl_dc, sc_bwd_mode mode,
+                                const uint32_t* aux, sc_projected_grad* projected_grad); /* raster.rs:653-724 */
+
+/* project_backward.wgsl:79-304 for one view; overwrites grads (accumulate = 0)
+ * or adds into them (accumulate = 1, multi-view sums). */
+sc_status sc_project_backward(sc_ctx* ctx, const sc_splats* s, const sc_projected_grad* projected_grad,
+                              const sc_camera* cam, sc_grads* grads,
+                              int accumulate);                       /* Rasterizer::project_backward, raster.rs:559-645 */
+
+/* tonemap.wgsl:27-41 into a headless RGBA8 buffer (viewer path). */
+sc_status sc_tonemap(sc_ctx* ctx, const float* image, uint32_t width, uint32_t height, uint8_t* rgba8);
+
+/* ------------------------------------------------------------- optimiser
+ * replaces AdamGpu (crates/nano-optimize/src/adam_gpu.rs:31-547) */
+sc_status sc_adam_step(sc_ctx* ctx, float* params, const float* grads, float* m, float* v, uint64_t n,
+                       float lr, uint64_t t, const sc_adam_config* cfg);   /* AdamGpu::step, :224-323 */
+sc_status sc_adam_step_all(sc_ctx* ctx, sc_splats* s, const sc_grads* g, sc_moments* mo, uint64_t t,
+                           const sc_adam_groups* groups);                  /* AdamGpu::step_all, :334-427 */
+sc_status sc_apply_constraints(sc_ctx* ctx, sc_splats* s, float log_scale_min, float log_scale_max,
+                               float opacity_logit_max);                   /* :431-489 */
+sc_status sc_accumulate_grad(sc_ctx* ctx, const sc_grads* g, float* grad_acc, uint32_t n); /* :492-541 */
+
+/* ------------------------------------------------------- densify / prune
+ * replaces train.rs:414-602 (CPU round trip there; stream compaction here).
+ * The result order equals the reference's swap_remove order exactly. */
+sc_status sc_prune_low_opacity(sc_ctx* ctx, sc_splats* s, sc_moments* mo, float* grad_acc, float threshold,
+                               uint32_t* removed);                          /* prune_low_opacity, :572-602 */
+sc_status sc_densify(sc_ctx* ctx, sc_splats* s, sc_moments* mo, float* grad_acc, uint32_t grad_count,
+                     float grad_threshold, float split_log_scale_threshold, uint32_t max_splats, uint32_t iter,
+                     uint32_t counts[3]);                                   /* densify, :414-549 */
+
+/* ------------------------------------------------------------------ PLY
+ * replaces nano-splat read_ply / write_ply (crates/nano-splat/src/ply.rs:17-256)
+ * together with SplatBuffer::{from,to}_gaussians (splat_store.rs:60-94). */
+sc_status sc_write_ply(const char* path, const sc_host_splats* s);
+/* Reads the header; *n_out receives the vertex count.  When dst is non-NULL
+ * and dst->n >= count, the records are decoded into dst and dst->n = count. */
+sc_status sc_read_ply(const char* path, sc_host_splats* dst, uint32_t* n_out);
+
+/* --------------------------------------------------------------- trainer
+ * The batched whole iteration of train() (train.rs:155-250) for n_views
+ * views per step: project -> bin -> composite + fused MSE -> backward ->
+ * project backward summed over views -> accumulate -> Adam -> constraints,
+ * replayed as one CUDA graph.  Loss is the mean of the per-view MSE. */
+typedef struct sc_train_config {
+  uint32_t n_views;            /* views per step                                 */
+  sc_tiling tiling;            /* image size and tile shape                      */
+  sc_adam_groups adam;         /* per-group learning rates                        */
+  uint32_t bwd_mode;           /* sc_bwd_mode                                    */
+  uint32_t use_graph;          /* capture the iteration as a CUDA graph          */
+  uint32_t blend_batch;        /* splats staged per shared-memory batch (0=auto) */
+  uint32_t sort_mode;          /* 0 = auto, 1 = depth presort + tile pass, 2 = 64-bit key sort */
+  float log_scale_min, log_scale_max, opacity_logit_max; /* train.rs:37-39 */
+} sc_train_config;
+
+sc_status sc_trainer_create(sc_ctx* ctx, const sc_train_config* cfg, sc_trainer** out);
+void sc_trainer_free(sc_ctx* ctx, sc_trainer* tr);
+/* targets: device array n_views*W*H float3 (rgb). */
+sc_status sc_trainer_set_targets(sc_trainer* tr, const float* targets);
+/* One training step with cameras cams[n_views] (host array); t is the new Adam
+ * step count.  Blocks until the step has finished; loss_out (host, nullable)
+ * receives the mean loss.  A step whose pair lists overflowed the device
+ * capacity changes no parameter and is re-run with larger buffers. */
+sc_status sc_trainer_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, float* grad_acc, const sc_camera* cams,
+                          uint64_t t, double* loss_out);
+/* device array of the last step: images n_views*W*H float4 (rgb, 1-T) */
+sc_status sc_trainer_images(const sc_trainer* tr, const float** images);
+/* pairs: (tile, splat) pairs of the last step (all views); n_kernels: kernel
+ * launches per step; names / avg_ms (arrays of SC_TRAINER_STAGES, nullable):
+ * stage names and average device time per stage in ms over the steps since
+ * profiling was enabled. */
+#define SC_TRAINER_STAGES 9
+sc_status sc_trainer_stats(const sc_trainer* tr, uint64_t* pairs, uint32_t* n_kernels, const char** names,
+                           float* avg_ms);
+/* Record CUDA events between the stages of each step (also inside the graph). */
+sc_status sc_trainer_set_profiling(sc_trainer* tr, int enabled);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPLAT_CUDA_H */

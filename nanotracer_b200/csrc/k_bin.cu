@@ -1,0 +1,239 @@
+// k_bin.cu — tile binning: per-splat tile counts, pair emission, per-tile ranges.
+//
+// Reference-shaped path (sc_bin):  tile_count.wgsl:28-55 -> scan ->
+// tile_emit.wgsl:36-67 -> radix sort -> tile_ranges.wgsl:22-41, extended to
+// n_views views (tile ids view*num_tiles + tile) and two key layouts:
+//   REF32   (tile << 16) | u16(clamp(depth / depth_max, 0, 1) * 65535)
+//   NATIVE  ((view*num_tiles + tile) << 32) | float_bits(depth)   (u64)
+// Emission order is (view, splat, ty, tx), so a stable key sort reproduces
+// the reference's order exactly (ties resolve to ascending splat index).
+//
+// Native pipeline path (trainer): splats are first sorted by depth within
+// each view (u64 key (view << 32) | depth bits), then pairs are emitted in
+// that order with a u32 key view*num_tiles + tile, so a stable sort on the
+// tile key alone (2 passes of 8 bits instead of 6) gives the same per-tile
+// front-to-back order as the 64-bit key.
+#include "sc_internal.cuh"
+
+namespace sck {
+
+struct BinArgs {
+  uint32_t tw, th, tiles_x, tiles_y, num_tiles;
+  float depth_max;
+};
+
+static BinArgs bin_args(const sc_tiling* tl) {
+  BinArgs a;
+  a.tw = tl->tile_w; a.th = tl->tile_h;
+  a.tiles_x = (tl->width + tl->tile_w - 1) / tl->tile_w;
+  a.tiles_y = (tl->height + tl->tile_h - 1) / tl->tile_h;
+  a.num_tiles = a.tiles_x * a.tiles_y;
+  a.depth_max = tl->depth_max;
+  return a;
+}
+
+__device__ __forceinline__ bool rect_of(const float4 ra, const float4 rb, const BinArgs& a, int& x0, int& y0, int& x1,
+                                        int& y1) {
+  if (rb.w == 0.0f) return false;
+  const float tsw = (float)a.tw, tsh = (float)a.th;
+  x0 = max((int)floorf(__fdiv_rn(ra.x - ra.w, tsw)), 0);
+  y0 = max((int)floorf(__fdiv_rn(ra.y - ra.w, tsh)), 0);
+  x1 = min((int)floorf(__fdiv_rn(ra.x + ra.w, tsw)), (int)a.tiles_x - 1);
+  y1 = min((int)floorf(__fdiv_rn(ra.y + ra.w, tsh)), (int)a.tiles_y - 1);
+  return !(x1 < x0 || y1 < y0);
+}
+
+__global__ void k_tile_count(const float4* __restrict__ rec, uint32_t n, uint32_t stride, uint32_t n_views, BinArgs a,
+                             uint32_t* __restrict__ counts) {
+  const uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (uint64_t)n_views * n) return;
+  const uint32_t v = (uint32_t)(q / n), i = (uint32_t)(q % n);
+  const size_t o = (size_t)v * stride + i;
+  int x0, y0, x1, y1;
+  uint32_t c = 0;
+  if (rect_of(rec[3 * o], rec[3 * o + 1], a, x0, y0, x1, y1)) c = (uint32_t)(x1 - x0 + 1) * (uint32_t)(y1 - y0 + 1);
+  counts[q] = c;
+}
+
+sc_status launch_tile_count(sc_ctx* ctx, const float4* rec, uint32_t n, uint32_t stride, uint32_t n_views,
+                            const sc_tiling* tl, uint32_t* counts) {
+  const uint64_t total = (uint64_t)n * n_views;
+  if (total == 0) return SC_OK;
+  k_tile_count<<<(unsigned)sc_div_up(total, 256), 256, 0, ctx->stream>>>(rec, n, stride, n_views, bin_args(tl), counts);
+  return sc_check_launch(ctx, "k_tile_count");
+}
+
+template <int MODE>
+__global__ void k_tile_emit(const float4* __restrict__ rec, uint32_t n, uint32_t stride, uint32_t n_views, BinArgs a,
+                            const uint32_t* __restrict__ offsets, void* __restrict__ keys_v,
+                            uint32_t* __restrict__ payloads, uint64_t cap) {
+  const uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (uint64_t)n_views * n) return;
+  const uint32_t v = (uint32_t)(q / n), i = (uint32_t)(q % n);
+  const size_t o = (size_t)v * stride + i;
+  const float4 ra = rec[3 * o], rb = rec[3 * o + 1];
+  int x0, y0, x1, y1;
+  if (!rect_of(ra, rb, a, x0, y0, x1, y1)) return;
+  uint64_t w = offsets[q];
+  if (MODE == 0) {
+    // tile_emit.wgsl:54-55
+    const float dn = fminf(fmaxf(__fdiv_rn(ra.z, a.depth_max), 0.0f), 1.0f);
+    const uint32_t d16 = (uint32_t)(dn * 65535.0f);
+    uint32_t* keys = reinterpret_cast<uint32_t*>(keys_v);
+    const uint32_t vbase = v * a.num_tiles;
+    for (int ty = y0; ty <= y1; ++ty)
+      for (int tx = x0; tx <= x1; ++tx) {
+        if (w >= cap) return;
+        keys[w] = ((vbase + (uint32_t)ty * a.tiles_x + (uint32_t)tx) << 16) | d16;
+        payloads[w] = i;
+        ++w;
+      }
+  } else {
+    const uint64_t db = __float_as_uint(ra.z);
+    uint64_t* keys = reinterpret_cast<uint64_t*>(keys_v);
+    const uint64_t vbase = (uint64_t)v * a.num_tiles;
+    for (int ty = y0; ty <= y1; ++ty)
+      for (int tx = x0; tx <= x1; ++tx) {
+        if (w >= cap) return;
+        keys[w] = ((vbase + (uint64_t)ty * a.tiles_x + (uint64_t)tx) << 32) | db;
+        payloads[w] = i;
+        ++w;
+      }
+  }
+}
+
+sc_status launch_tile_emit(sc_ctx* ctx, const float4* rec, uint32_t n, uint32_t stride, uint32_t n_views,
+                           const sc_tiling* tl, const uint32_t* offsets, int key_mode, void* keys, uint32_t* payloads,
+                           uint64_t cap) {
+  const uint64_t total = (uint64_t)n * n_views;
+  if (total == 0) return SC_OK;
+  const unsigned g = (unsigned)sc_div_up(total, 256);
+  if (key_mode == SC_KEYS_REF32)
+    k_tile_emit<0><<<g, 256, 0, ctx->stream>>>(rec, n, stride, n_views, bin_args(tl), offsets, keys, payloads, cap);
+  else
+    k_tile_emit<1><<<g, 256, 0, ctx->stream>>>(rec, n, stride, n_views, bin_args(tl), offsets, keys, payloads, cap);
+  return sc_check_launch(ctx, "k_tile_emit");
+}
+
+// tile_ranges.wgsl:22-41.  tile of a key: REF32 key >> 16, NATIVE key >> 32,
+// presorted u32 key itself (mode 2).
+template <int MODE>
+__global__ void k_tile_ranges(const void* __restrict__ keys_v, const uint64_t* __restrict__ d_total, uint64_t cap,
+                              uint32_t num_tiles, uint32_t* __restrict__ ranges) {
+  const uint64_t K = min(*d_total, cap);
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < K; j += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t t, tp = ~0ull, tn = ~0ull;
+    if (MODE == 0) {
+      const uint32_t* k = reinterpret_cast<const uint32_t*>(keys_v);
+      t = k[j] >> 16;
+      if (j > 0) tp = k[j - 1] >> 16;
+      if (j + 1 < K) tn = k[j + 1] >> 16;
+    } else if (MODE == 1) {
+      const uint64_t* k = reinterpret_cast<const uint64_t*>(keys_v);
+      t = k[j] >> 32;
+      if (j > 0) tp = k[j - 1] >> 32;
+      if (j + 1 < K) tn = k[j + 1] >> 32;
+    } else {
+      const uint32_t* k = reinterpret_cast<const uint32_t*>(keys_v);
+      t = k[j];
+      if (j > 0) tp = k[j - 1];
+      if (j + 1 < K) tn = k[j + 1];
+    }
+    if (t >= num_tiles) continue;
+    if (tp != t) ranges[2 * t] = (uint32_t)j;
+    if (tn != t) ranges[2 * t + 1] = (uint32_t)(j + 1);
+  }
+}
+
+sc_status launch_tile_ranges(sc_ctx* ctx, const void* keys, int key_mode, const uint64_t* d_total, uint64_t cap,
+                             uint32_t num_tiles, uint32_t* ranges) {
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(ranges, 0, (size_t)num_tiles * 8, ctx->stream), "memset ranges");
+  if (cap == 0) return SC_OK;
+  const unsigned g = (unsigned)std::min<uint64_t>(sc_div_up(cap, 256), (uint64_t)ctx->sm_count * 16);
+  if (key_mode == 0)
+    k_tile_ranges<0><<<g, 256, 0, ctx->stream>>>(keys, d_total, cap, num_tiles, ranges);
+  else if (key_mode == 1)
+    k_tile_ranges<1><<<g, 256, 0, ctx->stream>>>(keys, d_total, cap, num_tiles, ranges);
+  else
+    k_tile_ranges<2><<<g, 256, 0, ctx->stream>>>(keys, d_total, cap, num_tiles, ranges);
+  return sc_check_launch(ctx, "k_tile_ranges");
+}
+
+// ---------------------------------------------------------------- depth-presorted path
+// sorted_ids[v*stride + r] is the splat of depth rank r in view v.
+__global__ void k_presorted_counts(const uint32_t* __restrict__ counts_by_id, uint32_t stride, uint32_t n_views,
+                                   const uint32_t* __restrict__ sorted_ids, uint32_t* __restrict__ counts) {
+  const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= (uint64_t)n_views * stride) return;
+  const uint32_t v = (uint32_t)(j / stride);
+  counts[j] = counts_by_id[(size_t)v * stride + sorted_ids[j]];
+}
+
+sc_status launch_presorted_counts(sc_ctx* ctx, const uint32_t* counts_by_id, uint32_t stride, uint32_t n_views,
+                                   const uint32_t* sorted_ids, uint32_t* counts) {
+  const uint64_t total = (uint64_t)n_views * stride;
+  if (total == 0) return SC_OK;
+  k_presorted_counts<<<(unsigned)sc_div_up(total, 256), 256, 0, ctx->stream>>>(counts_by_id, stride, n_views,
+                                                                               sorted_ids, counts);
+  return sc_check_launch(ctx, "k_presorted_counts");
+}
+
+// One warp emits the pairs of 32 consecutive depth-ranked splats: the lanes
+// walk the concatenation of the 32 tile rectangles, so long rectangles do not
+// serialise a single thread.
+__global__ void __launch_bounds__(256) k_presorted_emit(const float4* __restrict__ rec, uint32_t stride,
+                                                         uint32_t n_views, const uint32_t* __restrict__ sorted_ids,
+                                                         const uint32_t* __restrict__ offsets, BinArgs a,
+                                                         uint32_t* __restrict__ keys, uint32_t* __restrict__ payloads,
+                                                         uint64_t cap, uint32_t* __restrict__ err) {
+  const uint64_t total = (uint64_t)n_views * stride;
+  const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  int x0 = 0, y0 = 0, x1 = -1, y1 = -1;
+  uint32_t id = 0, v = 0, cnt = 0;
+  uint64_t off = 0;
+  if (j < total) {
+    v = (uint32_t)(j / stride);
+    id = sorted_ids[j];
+    const size_t o = (size_t)v * stride + id;
+    if (rect_of(rec[3 * o], rec[3 * o + 1], a, x0, y0, x1, y1)) {
+      cnt = (uint32_t)(x1 - x0 + 1) * (uint32_t)(y1 - y0 + 1);
+      off = offsets[j];
+    }
+  }
+  if (cnt && off + cnt > cap) {
+    atomicOr(err, SC_DEVERR_CAPACITY);
+    cnt = 0;
+  }
+  // warp-cooperative emission: process the lanes' rectangles one lane at a time,
+  // all 32 lanes writing consecutive pairs of that rectangle
+  unsigned pending = __ballot_sync(0xffffffffu, cnt > 0);
+  while (pending) {
+    const int src = __ffs(pending) - 1;
+    pending &= pending - 1;
+    const uint32_t c = __shfl_sync(0xffffffffu, cnt, src);
+    const uint64_t base = __shfl_sync(0xffffffffu, off, src);
+    const int rx0 = __shfl_sync(0xffffffffu, x0, src), ry0 = __shfl_sync(0xffffffffu, y0, src);
+    const int rx1 = __shfl_sync(0xffffffffu, x1, src);
+    const uint32_t sid = __shfl_sync(0xffffffffu, id, src), sv = __shfl_sync(0xffffffffu, v, src);
+    const uint32_t wdt = (uint32_t)(rx1 - rx0 + 1);
+    const uint32_t vbase = sv * a.num_tiles;
+    for (uint32_t k = lane; k < c; k += 32) {
+      const uint32_t ry = k / wdt, rx = k - ry * wdt;
+      keys[base + k] = vbase + (uint32_t)(ry0 + (int)ry) * a.tiles_x + (uint32_t)(rx0 + (int)rx);
+      payloads[base + k] = sid;
+    }
+  }
+}
+
+sc_status launch_presorted_emit(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
+                                const uint32_t* sorted_ids, const uint32_t* offsets, const sc_tiling* tl,
+                                uint32_t* keys, uint32_t* payloads, uint64_t cap, uint32_t* d_error) {
+  const uint64_t total = (uint64_t)n_views * stride;
+  if (total == 0) return SC_OK;
+  k_presorted_emit<<<(unsigned)sc_div_up(total, 256), 256, 0, ctx->stream>>>(rec, stride, n_views, sorted_ids, offsets,
+                                                                             bin_args(tl), keys, payloads, cap, d_error);
+  return sc_check_launch(ctx, "k_presorted_emit");
+}
+
+}  // namespace sck

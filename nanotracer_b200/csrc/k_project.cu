@@ -1,0 +1,458 @@
+// k_project.cu — per-splat projection (forward) and its adjoint.
+//
+// Forward: the arithmetic of project_gaussians.wgsl:156-259 (pinhole, RH view,
+// Sigma2D + 0.3 I low-pass, 3-sigma radius, frustum cull, order-3 SH,
+// sigmoid opacity).  The 2D covariance is formed as B B^T with
+// B = J W R diag(sigma) (2x3), which is algebraically the reference's
+// J (W R S^2 R^T W^T) J^T with fewer operations.  One thread per splat loops
+// over all views, so the 236 bytes of parameters are read once per step.
+//
+// Backward: project_backward.wgsl:79-304, with the same omissions as the
+// reference (no dJ/dt in the position gradient, no SH view-direction
+// gradient, no colour-clamp gate).  The fused variant sums the per-view
+// gradients in registers and applies grad accumulation (accumulate_grad_pos.wgsl),
+// Adam (adam_step.wgsl / adam.rs:70-90) and the constraints
+// (apply_constraints.wgsl) in the same thread, so the 59 gradient rows never
+// touch HBM.
+#include "sc_internal.cuh"
+
+namespace sck {
+
+// SH constants, project_gaussians.wgsl:47-61
+#define SH_C0 0.2820948f
+#define SH_C1 0.488602f
+#define SH_C2_0 1.0925485f
+#define SH_C2_1 -1.0925485f
+#define SH_C2_2 0.31539157f
+#define SH_C2_3 -1.0925485f
+#define SH_C2_4 0.54627424f
+#define SH_C3_0 -0.5900436f
+#define SH_C3_1 2.8906114f
+#define SH_C3_2 -0.4570458f
+#define SH_C3_3 0.37317634f
+#define SH_C3_4 -0.4570458f
+#define SH_C3_5 1.4453057f
+#define SH_C3_6 -0.5900436f
+
+struct Cam {
+  float v[16];
+  float cp[3];
+  float near_plane, focal, width, height;
+};
+
+__device__ __forceinline__ Cam load_cam(const sc_camera* c) {
+  Cam k;
+  const float4* p = reinterpret_cast<const float4*>(c);
+  float4 a = __ldg(p + 0), b = __ldg(p + 1), cc = __ldg(p + 2), d = __ldg(p + 3), e = __ldg(p + 4), f = __ldg(p + 5);
+  k.v[0] = a.x; k.v[1] = a.y; k.v[2] = a.z; k.v[3] = a.w;
+  k.v[4] = b.x; k.v[5] = b.y; k.v[6] = b.z; k.v[7] = b.w;
+  k.v[8] = cc.x; k.v[9] = cc.y; k.v[10] = cc.z; k.v[11] = cc.w;
+  k.v[12] = d.x; k.v[13] = d.y; k.v[14] = d.z; k.v[15] = d.w;
+  k.cp[0] = e.x; k.cp[1] = e.y; k.cp[2] = e.z; k.near_plane = e.w;
+  k.focal = f.x; k.width = f.y; k.height = f.z;
+  return k;
+}
+
+__device__ __forceinline__ void sh_basis15(float x, float y, float z, float b[15]) {
+  const float xx = x * x, yy = y * y, zz = z * z;
+  b[0] = -SH_C1 * y; b[1] = SH_C1 * z; b[2] = -SH_C1 * x;
+  b[3] = SH_C2_0 * x * y;
+  b[4] = SH_C2_1 * y * z;
+  b[5] = SH_C2_2 * (2.0f * zz - xx - yy);
+  b[6] = SH_C2_3 * x * z;
+  b[7] = SH_C2_4 * (xx - yy);
+  b[8] = SH_C3_0 * y * (3.0f * xx - yy);
+  b[9] = SH_C3_1 * x * y * z;
+  b[10] = SH_C3_2 * y * (4.0f * zz - xx - yy);
+  b[11] = SH_C3_3 * z * (2.0f * zz - 3.0f * xx - 3.0f * yy);
+  b[12] = SH_C3_4 * x * (4.0f * zz - xx - yy);
+  b[13] = SH_C3_5 * z * (xx - yy);
+  b[14] = SH_C3_6 * x * (xx - 3.0f * yy);
+}
+
+// rotation matrix (row r, column c) of quaternion (w, x, y, z), project_gaussians.wgsl:68-80
+__device__ __forceinline__ void quat_rot(float w, float x, float y, float z, float R[3][3]) {
+  R[0][0] = 1.0f - 2.0f * (y * y + z * z); R[1][0] = 2.0f * (x * y + w * z); R[2][0] = 2.0f * (x * z - w * y);
+  R[0][1] = 2.0f * (x * y - w * z); R[1][1] = 1.0f - 2.0f * (x * x + z * z); R[2][1] = 2.0f * (y * z + w * x);
+  R[0][2] = 2.0f * (x * z + w * y); R[1][2] = 2.0f * (y * z - w * x); R[2][2] = 1.0f - 2.0f * (x * x + y * y);
+}
+
+// Geometry shared by forward and backward for one (splat, view).
+struct Geo {
+  float tx, ty, tz;         // camera-space x, y and positive depth
+  float R[3][3];            // rotation, R[row][col]
+  float W[3][3];            // view rotation, W[row][col]
+  float sig[3];             // exp(log-sigma)
+  float j0[3], j1[3];       // projection Jacobian rows
+  float s00, s01, s11, det; // dilated 2D covariance
+  float ca, cb, cc;         // conic
+};
+
+// returns false when culled by the near plane or a non-positive determinant
+__device__ __forceinline__ bool geometry(const Cam& c, float px, float py, float pz, float qw, float qx, float qy,
+                                         float qz, float l0, float l1, float l2, int precise, Geo& g) {
+  const float vx = c.v[0] * px + c.v[4] * py + c.v[8] * pz + c.v[12];
+  const float vy = c.v[1] * px + c.v[5] * py + c.v[9] * pz + c.v[13];
+  const float vz = c.v[2] * px + c.v[6] * py + c.v[10] * pz + c.v[14];
+  const float vw = c.v[3] * px + c.v[7] * py + c.v[11] * pz + c.v[15];
+  const float depth = -(vz / vw);
+  if (!(depth >= c.near_plane)) return false;
+  g.tx = vx / vw; g.ty = vy / vw; g.tz = depth;
+  quat_rot(qw, qx, qy, qz, g.R);
+  for (int r = 0; r < 3; ++r)
+    for (int k = 0; k < 3; ++k) g.W[r][k] = c.v[4 * k + r];
+  g.sig[0] = expf(l0); g.sig[1] = expf(l1); g.sig[2] = expf(l2);
+  const float f = c.focal;
+  const float iz = 1.0f / g.tz, iz2 = iz * iz;
+  g.j0[0] = f * iz; g.j0[1] = 0.0f; g.j0[2] = -f * g.tx * iz2;
+  g.j1[0] = 0.0f; g.j1[1] = -f * iz; g.j1[2] = f * g.ty * iz2;
+  // B = J W R S (2x3)
+  float JW0[3], JW1[3];
+  for (int k = 0; k < 3; ++k) {
+    JW0[k] = g.j0[0] * g.W[0][k] + g.j0[2] * g.W[2][k];
+    JW1[k] = g.j1[1] * g.W[1][k] + g.j1[2] * g.W[2][k];
+  }
+  float B0[3], B1[3];
+  for (int k = 0; k < 3; ++k) {
+    B0[k] = (JW0[0] * g.R[0][k] + JW0[1] * g.R[1][k] + JW0[2] * g.R[2][k]) * g.sig[k];
+    B1[k] = (JW1[0] * g.R[0][k] + JW1[1] * g.R[1][k] + JW1[2] * g.R[2][k]) * g.sig[k];
+  }
+  const float a = B0[0] * B0[0] + B0[1] * B0[1] + B0[2] * B0[2];
+  const float b = B0[0] * B1[0] + B0[1] * B1[1] + B0[2] * B1[2];
+  const float d = B1[0] * B1[0] + B1[1] * B1[1] + B1[2] * B1[2];
+  g.s00 = a + 0.3f; g.s01 = b; g.s11 = d + 0.3f;
+  g.det = g.s00 * g.s11 - g.s01 * g.s01;
+  if (precise && g.det < 9.765625e-4f * g.s00 * g.s11) {
+    // near-degenerate (needle-like) splat: the f32 determinant has lost more
+    // than 10 bits to cancellation.  Re-form it in FP64 through Lagrange's
+    // identity |B0|^2 |B1|^2 - (B0.B1)^2 = |B0 x B1|^2, which has no
+    // cancellation, and invert in FP64.
+    const double c0 = (double)B0[1] * B1[2] - (double)B0[2] * B1[1];
+    const double c1 = (double)B0[2] * B1[0] - (double)B0[0] * B1[2];
+    const double c2 = (double)B0[0] * B1[1] - (double)B0[1] * B1[0];
+    const double ad = (double)B0[0] * B0[0] + (double)B0[1] * B0[1] + (double)B0[2] * B0[2];
+    const double dd = (double)B1[0] * B1[0] + (double)B1[1] * B1[1] + (double)B1[2] * B1[2];
+    const double bd = (double)B0[0] * B1[0] + (double)B0[1] * B1[1] + (double)B0[2] * B1[2];
+    const double detd = (c0 * c0 + c1 * c1 + c2 * c2) + 0.3 * (ad + dd) + 0.09;
+    const double inv = 1.0 / detd;
+    g.det = (float)detd;
+    g.ca = (float)((dd + 0.3) * inv); g.cb = (float)(-bd * inv); g.cc = (float)((ad + 0.3) * inv);
+    return true;
+  }
+  if (!(g.det > 0.0f)) return false;
+  const float inv = 1.0f / g.det;
+  g.ca = g.s11 * inv; g.cb = -g.s01 * inv; g.cc = g.s00 * inv;
+  return true;
+}
+
+// tile rectangle of a projected record, tile_count.wgsl:40-50 (same float ops)
+__device__ __forceinline__ bool tile_rect(float mx, float my, float r, float vis, uint32_t tw, uint32_t th,
+                                          uint32_t tiles_x, uint32_t tiles_y, int& x0, int& y0, int& x1, int& y1) {
+  if (vis == 0.0f) return false;
+  const float tsw = (float)tw, tsh = (float)th;
+  x0 = max((int)floorf(__fdiv_rn(mx - r, tsw)), 0);
+  y0 = max((int)floorf(__fdiv_rn(my - r, tsh)), 0);
+  x1 = min((int)floorf(__fdiv_rn(mx + r, tsw)), (int)tiles_x - 1);
+  y1 = min((int)floorf(__fdiv_rn(my + r, tsh)), (int)tiles_y - 1);
+  return !(x1 < x0 || y1 < y0);
+}
+
+struct TileArgs { uint32_t tw, th, tiles_x, tiles_y; };
+
+__global__ void __launch_bounds__(128) k_project(DSplats s, const sc_camera* __restrict__ cams, uint32_t n_views,
+                                                 uint32_t stride, float4* __restrict__ rec, TileArgs ta,
+                                                 uint64_t* __restrict__ depth_keys, uint32_t* __restrict__ ids,
+                                                 uint32_t* __restrict__ counts, int precise) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= stride) return;
+  const bool live = i < s.n;
+  float px = 0, py = 0, pz = 0, qw = 1, qx = 0, qy = 0, qz = 0, l0 = 0, l1 = 0, l2 = 0, op = 0, d0 = 0, d1 = 0, d2 = 0;
+  if (live) {
+    px = sp_row(s, 0, i); py = sp_row(s, 1, i); pz = sp_row(s, 2, i);
+    qw = sp_row(s, 3, i); qx = sp_row(s, 4, i); qy = sp_row(s, 5, i); qz = sp_row(s, 6, i);
+    l0 = sp_row(s, 7, i); l1 = sp_row(s, 8, i); l2 = sp_row(s, 9, i);
+    op = sp_row(s, 10, i);
+    d0 = sp_row(s, 11, i); d1 = sp_row(s, 12, i); d2 = sp_row(s, 13, i);
+  }
+  const float opacity = 1.0f / (1.0f + expf(-op));
+  for (uint32_t v = 0; v < n_views; ++v) {
+    float4 ra = make_float4(0, 0, 0, 0), rb = ra, rc = ra;
+    uint32_t key = 0xFFFFFFFFu, cnt = 0;  // splats that emit no pair sort after every emitting one
+    if (live) {
+      const Cam c = load_cam(cams + v);
+      Geo g;
+      if (geometry(c, px, py, pz, qw, qx, qy, qz, l0, l1, l2, precise, g)) {
+        const float f = c.focal;
+        const float mx = c.width * 0.5f + (f * g.tx) / g.tz;
+        const float my = c.height * 0.5f - (f * g.ty) / g.tz;
+        const float mid = 0.5f * (g.s00 + g.s11);
+        const float lambda = mid + sqrtf(fmaxf(mid * mid - g.det, 0.0f));
+        const float radius = ceilf(3.0f * sqrtf(lambda));
+        const float maxp = fmaxf(c.width, c.height) + radius;
+        if (!(mx < -radius || mx >= c.width + radius || my < -radius || my >= c.height + radius || radius >= maxp)) {
+          float dx = c.cp[0] - px, dy = c.cp[1] - py, dz = c.cp[2] - pz;
+          const float len = sqrtf(dx * dx + dy * dy + dz * dz);
+          dx /= len; dy /= len; dz /= len;
+          float b[15];
+          sh_basis15(dx, dy, dz, b);
+          float ar = 0.f, ag = 0.f, ab = 0.f;
+#pragma unroll
+          for (int k = 0; k < 15; ++k) {
+            ar += sp_row(s, SC_ROW_REST + k, i) * b[k];
+            ag += sp_row(s, SC_ROW_REST + 15 + k, i) * b[k];
+            ab += sp_row(s, SC_ROW_REST + 30 + k, i) * b[k];
+          }
+          const float cr = fmaxf(SH_C0 * d0 + ar + 0.5f, 0.0f);
+          const float cg = fmaxf(SH_C0 * d1 + ag + 0.5f, 0.0f);
+          const float cb = fmaxf(SH_C0 * d2 + ab + 0.5f, 0.0f);
+          ra = make_float4(mx, my, g.tz, radius);
+          rb = make_float4(g.ca, g.cb, g.cc, 1.0f);
+          rc = make_float4(cr, cg, cb, opacity);
+          if (depth_keys) {
+            int x0, y0, x1, y1;
+            if (tile_rect(mx, my, radius, 1.0f, ta.tw, ta.th, ta.tiles_x, ta.tiles_y, x0, y0, x1, y1)) {
+              cnt = (uint32_t)(x1 - x0 + 1) * (uint32_t)(y1 - y0 + 1);
+              key = __float_as_uint(g.tz);
+            }
+          }
+        }
+      }
+    }
+    const size_t o = (size_t)v * stride + i;
+    rec[3 * o + 0] = ra; rec[3 * o + 1] = rb; rec[3 * o + 2] = rc;
+    if (depth_keys) {
+      depth_keys[o] = ((uint64_t)v << 32) | key;
+      ids[o] = i;
+      counts[o] = cnt;
+    }
+  }
+}
+
+sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams, uint32_t n_views, uint32_t stride,
+                         float4* rec, const sc_tiling* tl, uint64_t* depth_keys, uint32_t* ids, uint32_t* counts,
+                         int precise) {
+  if (stride == 0 || n_views == 0) return SC_OK;
+  TileArgs ta{1, 1, 1, 1};
+  if (tl) ta = TileArgs{tl->tile_w, tl->tile_h, (tl->width + tl->tile_w - 1) / tl->tile_w,
+                        (tl->height + tl->tile_h - 1) / tl->tile_h};
+  const uint32_t bs = 128;
+  k_project<<<(unsigned)sc_div_up(stride, bs), bs, 0, ctx->stream>>>(s, d_cams, n_views, stride, rec, ta, depth_keys,
+                                                                     ids, counts, precise);
+  return sc_check_launch(ctx, "k_project");
+}
+
+// ---------------------------------------------------------------- backward
+// Per-view gradient of one splat (project_backward.wgsl:79-304).  Writes the
+// 11 geometric gradients into gpos/grot/gsc/gop and returns the colour
+// gradient and SH basis for the caller to form the 48 SH gradients.
+__device__ __forceinline__ bool splat_backward_view(const Cam& c, float px, float py, float pz, float qw, float qx,
+                                                    float qy, float qz, float l0, float l1, float l2, float opacity,
+                                                    const float4 pg0, const float4 pg1, const float4 pg2,
+                                                    float gpos[3], float grot[4], float gsc[3], float& gop,
+                                                    float basis[15]) {
+  Geo g;
+  if (!geometry(c, px, py, pz, qw, qx, qy, qz, l0, l1, l2, 0, g)) return false;
+  const float f = c.focal;
+  const float iz = 1.0f / g.tz, iz2 = iz * iz;
+  // opacity logit
+  gop += pg0.z * opacity * (1.0f - opacity);
+  // SH basis at the view direction
+  float dx = c.cp[0] - px, dy = c.cp[1] - py, dz = c.cp[2] - pz;
+  const float len = sqrtf(dx * dx + dy * dy + dz * dz);
+  sh_basis15(dx / len, dy / len, dz / len, basis);
+  // dSigma2D = -C dConic C with the off-diagonal conic gradient halved
+  const float C00 = g.ca, C01 = g.cb, C11 = g.cc;
+  const float D00 = pg1.x, D01 = 0.5f * pg1.y, D11 = pg1.z;
+  const float P00 = C00 * D00 + C01 * D01, P10 = C01 * D00 + C11 * D01;
+  const float P01 = C00 * D01 + C01 * D11, P11 = C01 * D01 + C11 * D11;
+  const float ds00 = -(P00 * C00 + P01 * C01);
+  const float ds11 = -(P10 * C01 + P11 * C11);
+  const float ds01 = -(P00 * C01 + P01 * C11) - (P10 * C00 + P11 * C01);
+  const float h = 0.5f * ds01;
+  // dSigma_cam = J^T dS J (3x3 symmetric); J rows j0 = (j0x, 0, j0z), j1 = (0, j1y, j1z)
+  float dC[3][3];
+  {
+    const float a0[3] = {g.j0[0], g.j0[1], g.j0[2]}, a1[3] = {g.j1[0], g.j1[1], g.j1[2]};
+    for (int r = 0; r < 3; ++r)
+      for (int k = 0; k < 3; ++k)
+        dC[r][k] = a0[r] * ds00 * a0[k] + a0[r] * h * a1[k] + a1[r] * h * a0[k] + a1[r] * ds11 * a1[k];
+  }
+  // dSigma_world = W^T dC W
+  float T1[3][3], dW[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int k = 0; k < 3; ++k) T1[r][k] = dC[r][0] * g.W[0][k] + dC[r][1] * g.W[1][k] + dC[r][2] * g.W[2][k];
+  for (int r = 0; r < 3; ++r)
+    for (int k = 0; k < 3; ++k) dW[r][k] = g.W[0][r] * T1[0][k] + g.W[1][r] * T1[1][k] + g.W[2][r] * T1[2][k];
+  // dR = (dW + dW^T) R S^2 ; G[row][col]
+  const float s2[3] = {g.sig[0] * g.sig[0], g.sig[1] * g.sig[1], g.sig[2] * g.sig[2]};
+  float G[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int k = 0; k < 3; ++k) {
+      float acc = 0.f;
+      for (int m = 0; m < 3; ++m) acc += (dW[r][m] + dW[m][r]) * g.R[m][k];
+      G[r][k] = acc * s2[k];
+    }
+  // log-sigma: dL/d(s_k^2) = R_k^T dW R_k, times 2 s_k^2
+  for (int k = 0; k < 3; ++k) {
+    float acc = 0.f;
+    for (int r = 0; r < 3; ++r) {
+      float row = dW[r][0] * g.R[0][k] + dW[r][1] * g.R[1][k] + dW[r][2] * g.R[2][k];
+      acc += g.R[r][k] * row;
+    }
+    gsc[k] += acc * 2.0f * s2[k];
+  }
+  // quaternion, project_backward.wgsl:280-286
+  grot[0] += 2.0f * (qz * (G[1][0] - G[0][1]) + qy * (G[0][2] - G[2][0]) + qx * (G[2][1] - G[1][2]));
+  grot[1] += 2.0f * (qy * (G[0][1] + G[1][0]) + qz * (G[0][2] + G[2][0]) + qw * (G[2][1] - G[1][2])) -
+             4.0f * qx * (G[1][1] + G[2][2]);
+  grot[2] += -4.0f * qy * (G[0][0] + G[2][2]) +
+             2.0f * (qx * (G[0][1] + G[1][0]) + qw * (G[0][2] - G[2][0]) + qz * (G[1][2] + G[2][1]));
+  grot[3] += -4.0f * qz * (G[0][0] + G[1][1]) +
+             2.0f * (qw * (G[1][0] - G[0][1]) + qx * (G[0][2] + G[2][0]) + qy * (G[1][2] + G[2][1]));
+  // position, project_backward.wgsl:288-303
+  const float dtx = f * iz * pg0.x;
+  const float dty = -f * iz * pg0.y;
+  const float dtz = -f * g.tx * iz2 * pg0.x + f * g.ty * iz2 * pg0.y;
+  const float cx = dtx, cy = dty, cz = -dtz;
+  for (int k = 0; k < 3; ++k) gpos[k] += g.W[0][k] * cx + g.W[1][k] * cy + g.W[2][k] * cz;
+  return true;
+}
+
+__global__ void __launch_bounds__(128) k_project_backward(DSplats s, const float4* __restrict__ pg,
+                                                          const sc_camera* __restrict__ cam, float* __restrict__ out,
+                                                          uint32_t gcap, int accumulate) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n) return;
+  const Cam c = load_cam(cam);
+  float gpos[3] = {0, 0, 0}, grot[4] = {0, 0, 0, 0}, gsc[3] = {0, 0, 0}, gop = 0, basis[15];
+  const float4 p0 = pg[3 * (size_t)i], p1 = pg[3 * (size_t)i + 1], p2 = pg[3 * (size_t)i + 2];
+  const float op = 1.0f / (1.0f + expf(-sp_row(s, 10, i)));
+  const bool ok = splat_backward_view(c, sp_row(s, 0, i), sp_row(s, 1, i), sp_row(s, 2, i), sp_row(s, 3, i),
+                                      sp_row(s, 4, i), sp_row(s, 5, i), sp_row(s, 6, i), sp_row(s, 7, i),
+                                      sp_row(s, 8, i), sp_row(s, 9, i), op, p0, p1, p2, gpos, grot, gsc, gop, basis);
+  float row[SC_NROWS];
+#pragma unroll
+  for (int r = 0; r < SC_NROWS; ++r) row[r] = 0.f;
+  if (ok) {
+    row[0] = gpos[0]; row[1] = gpos[1]; row[2] = gpos[2];
+    row[3] = grot[0]; row[4] = grot[1]; row[5] = grot[2]; row[6] = grot[3];
+    row[7] = gsc[0]; row[8] = gsc[1]; row[9] = gsc[2];
+    row[10] = gop;
+    row[11] = p2.x * SH_C0; row[12] = p2.y * SH_C0; row[13] = p2.z * SH_C0;
+#pragma unroll
+    for (int k = 0; k < 15; ++k) {
+      row[14 + k] = p2.x * basis[k]; row[29 + k] = p2.y * basis[k]; row[44 + k] = p2.z * basis[k];
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < SC_NROWS; ++r) {
+    float* dst = out + (size_t)r * gcap + i;
+    *dst = accumulate ? *dst + row[r] : row[r];
+  }
+}
+
+sc_status launch_project_backward(sc_ctx* ctx, const DSplats& s, const float4* pg, const sc_camera* d_cam,
+                                  float* grads, uint32_t gcap, int accumulate) {
+  if (s.n == 0) return SC_OK;
+  k_project_backward<<<(unsigned)sc_div_up(s.n, 128), 128, 0, ctx->stream>>>(s, pg, d_cam, grads, gcap, accumulate);
+  return sc_check_launch(ctx, "k_project_backward");
+}
+
+// ---------------------------------------------------------------- fused backward + Adam
+__device__ __forceinline__ float ld_m(const DMoments& mo, const float* f, const __nv_bfloat16* h, size_t k) {
+  return mo.bf16 ? __bfloat162float(h[k]) : f[k];
+}
+__device__ __forceinline__ void st_m(const DMoments& mo, float* f, __nv_bfloat16* h, size_t k, float x) {
+  if (mo.bf16) h[k] = __float2bfloat16_rn(x); else f[k] = x;
+}
+
+__device__ __forceinline__ int lr_group(int r) {
+  return r < 3 ? 0 : (r < 7 ? 1 : (r < 10 ? 2 : (r < 11 ? 3 : (r < 14 ? 4 : 5))));
+}
+
+// Adam for one scalar (adam_step.wgsl:24-36)
+__device__ __forceinline__ float adam_one(const DMoments& mo, size_t k, float p, float gr, float lr, const AdamParams& ap) {
+  const float m = ap.beta1 * ld_m(mo, mo.m, mo.m16, k) + (1.0f - ap.beta1) * gr;
+  const float v = ap.beta2 * ld_m(mo, mo.v, mo.v16, k) + (1.0f - ap.beta2) * gr * gr;
+  st_m(mo, mo.m, mo.m16, k, m);
+  st_m(mo, mo.v, mo.v16, k, v);
+  const float mh = m / ap.bc1, vh = v / ap.bc2;
+  return p - lr * mh / (sqrtf(vh) + ap.eps);
+}
+
+__global__ void __launch_bounds__(128) k_fused_backward_adam(DSplats s, DMoments mo, const float4* __restrict__ pg,
+                                                             uint32_t stride, const sc_camera* __restrict__ cams,
+                                                             uint32_t n_views, float* __restrict__ grad_acc,
+                                                             AdamParams ap, const uint32_t* __restrict__ skip,
+                                                             const float* __restrict__ d_bc) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n) return;
+  if (skip && (*skip & SC_DEVERR_CAPACITY)) return;  // a capacity overflow earlier in the step: leave parameters untouched
+  if (d_bc) { ap.bc1 = d_bc[0]; ap.bc2 = d_bc[1]; }
+  const float px = sp_row(s, 0, i), py = sp_row(s, 1, i), pz = sp_row(s, 2, i);
+  const float qw = sp_row(s, 3, i), qx = sp_row(s, 4, i), qy = sp_row(s, 5, i), qz = sp_row(s, 6, i);
+  const float l0 = sp_row(s, 7, i), l1 = sp_row(s, 8, i), l2 = sp_row(s, 9, i);
+  const float olog = sp_row(s, 10, i);
+  const float opacity = 1.0f / (1.0f + expf(-olog));
+  float gpos[3] = {0, 0, 0}, grot[4] = {0, 0, 0, 0}, gsc[3] = {0, 0, 0}, gop = 0;
+  float gdc[3] = {0, 0, 0};
+  float grest[45];
+#pragma unroll
+  for (int k = 0; k < 45; ++k) grest[k] = 0.f;
+  for (uint32_t v = 0; v < n_views; ++v) {
+    const size_t o = (size_t)v * stride + i;
+    const float4 p2 = pg[3 * o + 2];
+    const float4 p0 = pg[3 * o], p1 = pg[3 * o + 1];
+    if (p0.x == 0.f && p0.y == 0.f && p0.z == 0.f && p1.x == 0.f && p1.y == 0.f && p1.z == 0.f && p2.x == 0.f &&
+        p2.y == 0.f && p2.z == 0.f)
+      continue;  // splat untouched in this view: every gradient term is zero
+    const Cam c = load_cam(cams + v);
+    float basis[15];
+    if (!splat_backward_view(c, px, py, pz, qw, qx, qy, qz, l0, l1, l2, opacity, p0, p1, p2, gpos, grot, gsc, gop,
+                             basis))
+      continue;
+    gdc[0] += p2.x * SH_C0; gdc[1] += p2.y * SH_C0; gdc[2] += p2.z * SH_C0;
+#pragma unroll
+    for (int k = 0; k < 15; ++k) {
+      grest[k] += p2.x * basis[k]; grest[15 + k] += p2.y * basis[k]; grest[30 + k] += p2.z * basis[k];
+    }
+  }
+  // densify statistic, accumulate_grad_pos.wgsl:17-23 (before the step, train.rs:228)
+  if (grad_acc) grad_acc[i] = grad_acc[i] + fabsf(gpos[0]) + fabsf(gpos[1]) + fabsf(gpos[2]);
+  const size_t cap = s.cap;
+  // geometric rows
+  const float gg[14] = {gpos[0], gpos[1], gpos[2], grot[0], grot[1], grot[2], grot[3],
+                        gsc[0], gsc[1], gsc[2], gop, gdc[0], gdc[1], gdc[2]};
+  const float pp[14] = {px, py, pz, qw, qx, qy, qz, l0, l1, l2, olog, sp_row(s, 11, i), sp_row(s, 12, i),
+                        sp_row(s, 13, i)};
+  float np[14];
+#pragma unroll
+  for (int r = 0; r < 14; ++r) np[r] = adam_one(mo, (size_t)r * mo.cap + i, pp[r], gg[r], ap.lr[lr_group(r)], ap);
+  // constraints, apply_constraints.wgsl:24-41
+  {
+    const float n2 = np[3] * np[3] + np[4] * np[4] + np[5] * np[5] + np[6] * np[6];
+    const float nrm = fmaxf(sqrtf(n2), 1e-8f);
+    np[3] /= nrm; np[4] /= nrm; np[5] /= nrm; np[6] /= nrm;
+    for (int k = 7; k < 10; ++k) np[k] = fminf(fmaxf(np[k], ap.log_scale_min), ap.log_scale_max);
+    np[10] = fminf(fmaxf(np[10], -ap.opacity_logit_max), ap.opacity_logit_max);
+  }
+#pragma unroll
+  for (int r = 0; r < 14; ++r) s.slab[(size_t)r * cap + i] = np[r];
+#pragma unroll
+  for (int k = 0; k < 45; ++k) {
+    const int r = SC_ROW_REST + k;
+    const float p = sp_row(s, r, i);
+    sp_set(s, r, i, adam_one(mo, (size_t)r * mo.cap + i, p, grest[k], ap.lr[5], ap));
+  }
+}
+
+sc_status launch_fused_backward_adam(sc_ctx* ctx, const DSplats& s, const DMoments& mo, const float4* pg,
+                                     uint32_t stride, const sc_camera* d_cams, uint32_t n_views, float* grad_acc,
+                                     const AdamParams& ap, const uint32_t* d_skip, const float* d_bc) {
+  if (s.n == 0) return SC_OK;
+  k_fused_backward_adam<<<(unsigned)sc_div_up(s.n, 128), 128, 0, ctx->stream>>>(s, mo, pg, stride, d_cams, n_views,
+                                                                                 grad_acc, ap, d_skip, d_bc);
+  return sc_check_launch(ctx, "k_fused_backward_adam");
+}
+
+}  // namespace sck

@@ -1,0 +1,392 @@
+// k_sort.cu — single-pass exclusive scan and onesweep LSD radix sort, both
+// with decoupled look-back (Merrill & Garland 2016; Adinets & Merrill 2022).
+//
+// Replaces the reference's 3-level Hillis-Steele scan (prefix_scan.rs:127-186,
+// n <= 2^24) and its 32 one-bit split passes (radix_sort.rs:144-303, ~160
+// dispatches per sort).  Here one sort is one histogram kernel plus one kernel
+// per 8-bit digit.  Both are stable and deterministic: tiles take their
+// position from an atomic ticket, rank their items warp-by-warp in input
+// order (match.any), and obtain the running digit offsets from their
+// predecessors' published aggregates.
+//
+// Every look-back wait is bounded: after SC_SPIN_LIMIT polls the block sets
+// SC_DEVERR_TIMEOUT in the context's error word and proceeds with what it has
+// (the output is then garbage, the host reports SC_ERR_TIMEOUT) instead of
+// hanging the GPU.
+#include "sc_internal.cuh"
+
+namespace sck {
+
+// ---------------------------------------------------------------- memory-order helpers
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// ---------------------------------------------------------------- exclusive scan
+#define SCAN_THREADS 256
+#define SCAN_IPT 16
+#define SCAN_TILE (SCAN_THREADS * SCAN_IPT)
+#define SCAN_FLAG_AGG (1ull << 62)
+#define SCAN_FLAG_PRE (2ull << 62)
+#define SCAN_VAL_MASK ((1ull << 62) - 1)
+
+__device__ __forceinline__ unsigned long long warp_incl_scan_u64(unsigned long long x) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  return x;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan(uint32_t* __restrict__ data, uint64_t n,
+                                                       unsigned long long* __restrict__ status,
+                                                       unsigned* __restrict__ ticket, uint64_t* __restrict__ total,
+                                                       uint32_t* __restrict__ err) {
+  __shared__ unsigned s_tile;
+  __shared__ unsigned long long s_warp[SCAN_THREADS / 32];
+  __shared__ unsigned long long s_excl;
+  if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+  __syncthreads();
+  const unsigned tile = s_tile;
+  const uint64_t base = (uint64_t)tile * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_IPT;
+  uint32_t x[SCAN_IPT];
+  unsigned long long tsum = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_IPT; ++k) {
+    x[k] = (base + k < n) ? data[base + k] : 0u;
+    tsum += x[k];
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned long long incl = warp_incl_scan_u64(tsum);
+  if (lane == 31) s_warp[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    unsigned long long w = lane < SCAN_THREADS / 32 ? s_warp[lane] : 0ull;
+    w = warp_incl_scan_u64(w);
+    if (lane < SCAN_THREADS / 32) s_warp[lane] = w;  // inclusive per warp
+    // look-back by warp 0
+    const unsigned long long agg = __shfl_sync(0xffffffffu, w, SCAN_THREADS / 32 - 1);
+    if (lane == 0) st_release_u64(&status[tile], (tile == 0 ? SCAN_FLAG_PRE : SCAN_FLAG_AGG) | agg);
+    unsigned long long excl = 0;
+    if (tile > 0) {
+      // warp-wide look-back: lane l inspects predecessor pred - l; indices below
+      // zero read as an inclusive prefix of 0, so the walk always terminates.
+      long long pred = (long long)tile - 1;
+      unsigned spins = 0;
+      bool gave_up = false;
+      for (;;) {
+        const long long idx = pred - lane;
+        unsigned long long st = 0;
+        for (;;) {
+          st = idx >= 0 ? ld_acquire_u64(&status[idx]) : SCAN_FLAG_PRE;
+          if (__all_sync(0xffffffffu, (st >> 62) != 0ull)) break;
+          if (++spins > SC_SPIN_LIMIT) { gave_up = true; break; }
+          __nanosleep(32);
+        }
+        if (gave_up) break;
+        const unsigned pre = __ballot_sync(0xffffffffu, (st >> 62) == 2ull);
+        const int first = pre ? __ffs(pre) - 1 : 32;  // nearest predecessor holding an inclusive prefix
+        unsigned long long val = (lane <= first) ? (st & SCAN_VAL_MASK) : 0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
+        excl += val;
+        if (pre) break;
+        pred -= 32;
+      }
+      if (gave_up && lane == 0) atomicOr(err, SC_DEVERR_TIMEOUT);
+      if (lane == 0) st_release_u64(&status[tile], SCAN_FLAG_PRE | ((excl + agg) & SCAN_VAL_MASK));
+    }
+    if (lane == 0) s_excl = excl;
+  }
+  __syncthreads();
+  unsigned long long run = s_excl + (warp > 0 ? s_warp[warp - 1] : 0ull) + (incl - tsum);
+#pragma unroll
+  for (int k = 0; k < SCAN_IPT; ++k) {
+    if (base + k < n) data[base + k] = (uint32_t)run;
+    run += x[k];
+  }
+  // the thread holding the last element publishes the total
+  if (total && n > 0 && base <= n - 1 && n - 1 < base + SCAN_IPT) *total = run;
+}
+
+size_t scan_scratch_bytes(uint64_t n) {
+  const uint64_t tiles = sc_div_up(n, SCAN_TILE);
+  return 256 + tiles * 8;
+}
+
+sc_status scan_u32(sc_ctx* ctx, uint32_t* data, uint64_t n, uint64_t* d_total, void* scratch, size_t bytes) {
+  if (n == 0) {
+    if (d_total) SC_CUDA_TRY(ctx, cudaMemsetAsync(d_total, 0, 8, ctx->stream), "memset total");
+    return SC_OK;
+  }
+  const uint64_t tiles = sc_div_up(n, SCAN_TILE);
+  if (bytes < scan_scratch_bytes(n)) return sc_fail(ctx, SC_ERR_INVALID_ARG, "scan scratch too small");
+  unsigned* ticket = reinterpret_cast<unsigned*>(scratch);
+  unsigned long long* status = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(scratch) + 256);
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(scratch, 0, scan_scratch_bytes(n), ctx->stream), "memset scan status");
+  k_scan<<<(unsigned)tiles, SCAN_THREADS, 0, ctx->stream>>>(data, n, status, ticket, d_total, ctx->d_error);
+  return sc_check_launch(ctx, "k_scan");
+}
+
+// ---------------------------------------------------------------- onesweep radix sort
+#define RS_THREADS 256
+#define RS_WARPS (RS_THREADS / 32)
+#define RS_RADIX 256
+#define RS_FLAG_AGG (1u << 30)
+#define RS_FLAG_PRE (2u << 30)
+#define RS_VAL_MASK ((1u << 30) - 1)
+#define RS_HIST_BLOCKS_PER_SM 4
+
+template <typename K> struct RsCfg;
+template <> struct RsCfg<uint32_t> { static constexpr int IPT = 16; };
+template <> struct RsCfg<uint64_t> { static constexpr int IPT = 12; };
+
+// Global digit histograms of all passes in one read of the keys.
+template <typename K>
+__global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const K* __restrict__ keys, uint64_t n_cap,
+                                                        const uint64_t* __restrict__ d_n, int passes,
+                                                        uint32_t* __restrict__ hist /* passes x 256 */) {
+  __shared__ uint32_t sh[8][RS_RADIX];
+  for (int t = threadIdx.x; t < passes * RS_RADIX; t += RS_THREADS) (&sh[0][0])[t] = 0;
+  __syncthreads();
+  const uint64_t n = d_n ? min(*d_n, n_cap) : n_cap;
+  for (uint64_t i = (uint64_t)blockIdx.x * RS_THREADS + threadIdx.x; i < n; i += (uint64_t)gridDim.x * RS_THREADS) {
+    const K k = keys[i];
+    for (int p = 0; p < passes; ++p) atomicAdd(&sh[p][(uint32_t)(k >> (8 * p)) & 0xFFu], 1u);
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < passes * RS_RADIX; t += RS_THREADS) {
+    const uint32_t c = (&sh[0][0])[t];
+    if (c) atomicAdd(&hist[t], c);
+  }
+}
+
+// exclusive scan of each pass's 256 bins (one block per pass)
+__global__ void __launch_bounds__(RS_RADIX) k_rs_hist_scan(uint32_t* __restrict__ hist) {
+  __shared__ uint32_t s[RS_RADIX];
+  uint32_t* h = hist + blockIdx.x * RS_RADIX;
+  const uint32_t v = h[threadIdx.x];
+  s[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = 1; o < RS_RADIX; o <<= 1) {
+    uint32_t y = threadIdx.x >= (unsigned)o ? s[threadIdx.x - o] : 0u;
+    __syncthreads();
+    s[threadIdx.x] += y;
+    __syncthreads();
+  }
+  h[threadIdx.x] = s[threadIdx.x] - v;
+}
+
+template <typename K>
+struct RsSmem {
+  static constexpr int IPT = RsCfg<K>::IPT;
+  static constexpr int TILE = RS_THREADS * IPT;
+  K keys[TILE];
+  uint32_t vals[TILE];
+  uint32_t warp_hist[RS_WARPS][RS_RADIX];
+  uint32_t tile_excl[RS_RADIX];
+  long long out_base[RS_RADIX];
+  uint32_t tile_id;
+};
+
+template <typename K>
+__global__ void __launch_bounds__(RS_THREADS) k_rs_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
+                                                        K* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                        uint64_t n_cap, const uint64_t* __restrict__ d_n, int shift,
+                                                        const uint32_t* __restrict__ digit_base,
+                                                        unsigned* __restrict__ lookback, unsigned* __restrict__ ticket,
+                                                        uint32_t* __restrict__ err) {
+  constexpr int IPT = RsCfg<K>::IPT;
+  constexpr int TILE = RS_THREADS * IPT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  RsSmem<K>& sm = *reinterpret_cast<RsSmem<K>*>(smem_raw);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) sm.tile_id = atomicAdd(ticket, 1u);
+  for (int t = threadIdx.x; t < RS_WARPS * RS_RADIX; t += RS_THREADS) (&sm.warp_hist[0][0])[t] = 0;
+  __syncthreads();
+  const uint32_t tile = sm.tile_id;
+  const uint64_t n = d_n ? min(*d_n, n_cap) : n_cap;
+  const uint64_t tbase = (uint64_t)tile * TILE;
+  if (tbase >= n) return;  // every later ticket is beyond n as well: nobody waits on this tile
+  // warp-striped load: item k of lane l in warp w is tbase + w*32*IPT + k*32 + l
+  const uint64_t wbase = tbase + (uint64_t)warp * 32 * IPT;
+  K key[IPT];
+  uint32_t rank[IPT];
+  uint32_t dig[IPT];
+#pragma unroll
+  for (int k = 0; k < IPT; ++k) {
+    const uint64_t i = wbase + (uint64_t)k * 32 + lane;
+    const bool valid = i < n;
+    key[k] = valid ? kin[i] : (K)0;
+    dig[k] = valid ? (uint32_t)(key[k] >> shift) & 0xFFu : 256u;
+  }
+  const unsigned lt = lanemask_lt();
+#pragma unroll
+  for (int k = 0; k < IPT; ++k) {
+    const unsigned peers = __match_any_sync(0xffffffffu, dig[k]);
+    const int leader = 31 - __clz(peers);
+    uint32_t old = 0;
+    if (lane == leader && dig[k] < 256u) {
+      old = sm.warp_hist[warp][dig[k]];
+      sm.warp_hist[warp][dig[k]] = old + __popc(peers);
+    }
+    old = __shfl_sync(0xffffffffu, old, leader);
+    rank[k] = old + __popc(peers & lt);
+    __syncwarp();
+  }
+  __syncthreads();
+  // per digit: exclusive prefix over warps, tile count
+  const int d = threadIdx.x;  // RS_THREADS == RS_RADIX
+  uint32_t cnt = 0;
+#pragma unroll
+  for (int w = 0; w < RS_WARPS; ++w) {
+    const uint32_t c = sm.warp_hist[w][d];
+    sm.warp_hist[w][d] = cnt;
+    cnt += c;
+  }
+  // publish this tile's count, then look back for the running prefix
+  unsigned* lb = lookback + (size_t)tile * RS_RADIX;
+  st_release_u32(&lb[d], (tile == 0 ? RS_FLAG_PRE : RS_FLAG_AGG) | cnt);
+  uint32_t excl = 0;
+  if (tile > 0) {
+    long long pred = (long long)tile - 1;
+    unsigned spins = 0;
+    while (pred >= 0) {
+      const unsigned st = ld_acquire_u32(&lookback[(size_t)pred * RS_RADIX + d]);
+      const unsigned flag = st & ~RS_VAL_MASK;
+      if (flag == 0u) {
+        if (++spins > SC_SPIN_LIMIT) { atomicOr(err, SC_DEVERR_TIMEOUT); break; }
+        __nanosleep(20);
+        continue;
+      }
+      excl += st & RS_VAL_MASK;
+      if (flag == RS_FLAG_PRE) break;
+      --pred;
+    }
+    st_release_u32(&lb[d], RS_FLAG_PRE | ((excl + cnt) & RS_VAL_MASK));
+  }
+  // tile-local exclusive scan of the digit counts (256 values, one per thread)
+  {
+    uint32_t x = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    __shared__ uint32_t s_w[RS_WARPS];
+    if (lane == 31) s_w[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t w = lane < RS_WARPS ? s_w[lane] : 0u;
+#pragma unroll
+      for (int o = 1; o < RS_WARPS; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      if (lane < RS_WARPS) s_w[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t te = x - cnt + (warp > 0 ? s_w[warp - 1] : 0u);
+    sm.tile_excl[d] = te;
+    sm.out_base[d] = (long long)digit_base[d] + (long long)excl - (long long)te;
+  }
+  __syncthreads();
+  // scatter into shared memory in digit order
+#pragma unroll
+  for (int k = 0; k < IPT; ++k) {
+    if (dig[k] < 256u) {
+      const uint32_t pos = sm.tile_excl[dig[k]] + sm.warp_hist[warp][dig[k]] + rank[k];
+      sm.keys[pos] = key[k];
+      const uint64_t i = wbase + (uint64_t)k * 32 + lane;
+      sm.vals[pos] = vin[i];
+    }
+  }
+  __syncthreads();
+  const uint32_t valid = (uint32_t)min((uint64_t)TILE, n - tbase);
+  for (uint32_t idx = threadIdx.x; idx < valid; idx += RS_THREADS) {
+    const K kk = sm.keys[idx];
+    const uint32_t dd = (uint32_t)(kk >> shift) & 0xFFu;
+    const long long g = sm.out_base[dd] + (long long)idx;
+    kout[g] = kk;
+    vout[g] = sm.vals[idx];
+  }
+}
+
+size_t radix_scratch_bytes(uint64_t n, uint32_t key_bytes) {
+  const int tile = RS_THREADS * (key_bytes == 4 ? RsCfg<uint32_t>::IPT : RsCfg<uint64_t>::IPT);
+  const uint64_t tiles = sc_div_up(n > 0 ? n : 1, tile);
+  const int max_passes = key_bytes * 8 / 8;
+  // [hist passes x 256 u32][tickets 16 u32][lookback passes x tiles x 256 u32]
+  return 4096 * 2 + 64 + (size_t)max_passes * tiles * RS_RADIX * 4;
+}
+
+template <typename K>
+sc_status radix_sort(sc_ctx* ctx, K* keys, uint32_t* vals, K* keys_tmp, uint32_t* vals_tmp, uint64_t n_cap,
+                     uint32_t key_bits, const uint64_t* d_n, void* scratch, size_t bytes, bool* result_in_tmp) {
+  *result_in_tmp = false;
+  if (n_cap == 0) return SC_OK;
+  if (n_cap > RS_VAL_MASK) return sc_fail(ctx, SC_ERR_CAPACITY, "radix sort limited to 2^30 - 1 elements");
+  if (key_bits > sizeof(K) * 8) return sc_fail(ctx, SC_ERR_INVALID_ARG, "key_bits larger than the key type");
+  const int passes = (int)((key_bits + 7) / 8);
+  if (passes == 0) return SC_OK;
+  constexpr int TILE = RS_THREADS * RsCfg<K>::IPT;
+  const uint64_t tiles = sc_div_up(n_cap, TILE);
+  const size_t need = 4096 * 2 + 64 + (size_t)passes * tiles * RS_RADIX * 4;
+  if (bytes < need) return sc_fail(ctx, SC_ERR_INVALID_ARG, "radix scratch too small");
+  uint32_t* hist = reinterpret_cast<uint32_t*>(scratch);
+  unsigned* tickets = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(scratch) + 8192);
+  unsigned* lookback = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(scratch) + 8192 + 64);
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(scratch, 0, need, ctx->stream), "memset radix scratch");
+  const unsigned hist_blocks = (unsigned)std::min<uint64_t>(sc_div_up(n_cap, RS_THREADS),
+                                                            (uint64_t)ctx->sm_count * RS_HIST_BLOCKS_PER_SM);
+  k_rs_hist<K><<<hist_blocks, RS_THREADS, 0, ctx->stream>>>(keys, n_cap, d_n, passes, hist);
+  SC_TRY(sc_check_launch(ctx, "k_rs_hist"));
+  k_rs_hist_scan<<<passes, RS_RADIX, 0, ctx->stream>>>(hist);
+  SC_TRY(sc_check_launch(ctx, "k_rs_hist_scan"));
+  const size_t smem = sizeof(RsSmem<K>);
+  static bool attr_set = false;
+  if (!attr_set) {
+    SC_CUDA_TRY(ctx, cudaFuncSetAttribute(k_rs_pass<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                "smem attr");
+    attr_set = true;
+  }
+  K* kin = keys; uint32_t* vin = vals; K* kout = keys_tmp; uint32_t* vout = vals_tmp;
+  for (int p = 0; p < passes; ++p) {
+    k_rs_pass<K><<<(unsigned)tiles, RS_THREADS, smem, ctx->stream>>>(kin, vin, kout, vout, n_cap, d_n, 8 * p,
+                                                                     hist + p * RS_RADIX,
+                                                                     lookback + (size_t)p * tiles * RS_RADIX,
+                                                                     tickets + p, ctx->d_error);
+    SC_TRY(sc_check_launch(ctx, "k_rs_pass"));
+    std::swap(kin, kout);
+    std::swap(vin, vout);
+  }
+  *result_in_tmp = (passes & 1) != 0;
+  return SC_OK;
+}
+
+template sc_status radix_sort<uint32_t>(sc_ctx*, uint32_t*, uint32_t*, uint32_t*, uint32_t*, uint64_t, uint32_t,
+                                        const uint64_t*, void*, size_t, bool*);
+template sc_status radix_sort<uint64_t>(sc_ctx*, uint64_t*, uint32_t*, uint64_t*, uint32_t*, uint64_t, uint32_t,
+                                        const uint64_t*, void*, size_t, bool*);
+
+}  // namespace sck

@@ -1,0 +1,210 @@
+// sc_internal.cuh — shared definitions of libsplatcuda (sm_100a).
+//
+// Device layout of the splat parameters ("slab", coefficient-major SoA):
+//   row r of the 59 parameter rows lives at slab[r * cap + i] for splat i,
+//   rows 0-2 position, 3-6 rotation (w,x,y,z), 7-9 log-sigma, 10 opacity
+//   logit, 11-13 SH DC, 14-58 SH rest (planar R[15] G[15] B[15]).
+// Every per-splat read or write of a row is a coalesced 4-byte access across
+// a warp, the gather/scatter of densify is row-wise, and Adam is one
+// elementwise pass over the slab.  With SC_SPLATS_BF16_REST the 45 rest rows
+// live in a separate bf16 slab (rest16[k * cap + i]).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/splat_cuda.h"
+
+#define SC_NROWS 59
+#define SC_ROW_POS 0
+#define SC_ROW_ROT 3
+#define SC_ROW_SCALE 7
+#define SC_ROW_OP 10
+#define SC_ROW_DC 11
+#define SC_ROW_REST 14
+#define SC_MAX_VIEWS 64
+
+// device error word bits
+#define SC_DEVERR_TIMEOUT 1u
+#define SC_DEVERR_CAPACITY 2u
+
+// bounded spin limit for decoupled look-back waits (iterations of a poll loop
+// with a nanosleep back-off; ~1 s worst case before giving up)
+#define SC_SPIN_LIMIT (1u << 22)
+
+struct sc_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int sm_count = 0;
+  std::string last_error;
+  uint32_t* d_error = nullptr;    // device error word
+  uint64_t* d_counters = nullptr; // scratch counters (tile ids, totals)
+  uint32_t* h_error = nullptr;    // pinned mirror
+  uint64_t launches = 0;
+  // grow-only scratch arena for temporaries of the reference-shaped calls
+  void* scratch = nullptr;
+  size_t scratch_bytes = 0;
+};
+
+struct sc_splats {
+  uint32_t n = 0, cap = 0, flags = 0;
+  float* slab = nullptr;            // 14 or 59 rows x cap
+  __nv_bfloat16* rest16 = nullptr;  // 45 rows x cap when bf16
+};
+
+struct sc_grads {
+  uint32_t cap = 0;
+  float* slab = nullptr;  // 59 rows x cap
+};
+
+struct sc_moments {
+  uint32_t cap = 0, flags = 0;
+  float* m = nullptr; float* v = nullptr;                  // fp32: 59 rows x cap
+  __nv_bfloat16* m16 = nullptr; __nv_bfloat16* v16 = nullptr;  // bf16 form
+};
+
+// ---------------------------------------------------------------- views
+struct DSplats {
+  float* slab;
+  __nv_bfloat16* rest16;
+  uint32_t n, cap, bf16;
+};
+
+struct DMoments {
+  float* m; float* v;
+  __nv_bfloat16* m16; __nv_bfloat16* v16;
+  uint32_t cap, bf16;
+};
+
+static inline DSplats dview(const sc_splats* s) {
+  return DSplats{s->slab, s->rest16, s->n, s->cap, (s->flags & SC_SPLATS_BF16_REST) ? 1u : 0u};
+}
+static inline DMoments dview(const sc_moments* m) {
+  return DMoments{m->m, m->v, m->m16, m->v16, m->cap, (m->flags & SC_MOMENTS_BF16) ? 1u : 0u};
+}
+
+__device__ __forceinline__ float sp_row(const DSplats& s, int r, uint32_t i) {
+  if (r >= SC_ROW_REST && s.bf16) return __bfloat162float(s.rest16[(size_t)(r - SC_ROW_REST) * s.cap + i]);
+  return s.slab[(size_t)r * s.cap + i];
+}
+__device__ __forceinline__ void sp_set(const DSplats& s, int r, uint32_t i, float v) {
+  if (r >= SC_ROW_REST && s.bf16) { s.rest16[(size_t)(r - SC_ROW_REST) * s.cap + i] = __float2bfloat16_rn(v); return; }
+  s.slab[(size_t)r * s.cap + i] = v;
+}
+
+// ---------------------------------------------------------------- host helpers
+sc_status sc_fail(sc_ctx* ctx, sc_status st, const std::string& msg);
+sc_status sc_cuda_fail(sc_ctx* ctx, cudaError_t e, const char* what);
+sc_status sc_check_launch(sc_ctx* ctx, const char* what);
+// scratch arena: returns a device pointer to at least `bytes` (reused across calls
+// on the same stream; contents undefined)
+sc_status sc_scratch(sc_ctx* ctx, size_t bytes, void** out);
+// read-and-clear the device error word (blocks)
+sc_status sc_check_device_error(sc_ctx* ctx);
+
+#define SC_TRY(expr)                      \
+  do {                                    \
+    sc_status _st = (expr);               \
+    if (_st != SC_OK) return _st;         \
+  } while (0)
+
+#define SC_CUDA_TRY(ctx, expr, what)                      \
+  do {                                                    \
+    cudaError_t _e = (expr);                              \
+    if (_e != cudaSuccess) return sc_cuda_fail(ctx, _e, what); \
+  } while (0)
+
+static inline uint64_t sc_div_up(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
+
+// ---------------------------------------------------------------- kernel entry points
+// (defined in the k_*.cu files, launched by the API layer)
+namespace sck {
+
+// projection: writes n_views*stride records; when depth_keys != nullptr also
+// writes per (view, splat) a depth sort key (float bits, 0xFFFFFFFF when the
+// splat emits no pairs) and the tile count (for the native pipeline).
+sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams, uint32_t n_views,
+                         uint32_t stride, float4* rec, const sc_tiling* tiling, uint64_t* depth_keys,
+                         uint32_t* splat_ids, uint32_t* counts, int precise_det);
+
+sc_status launch_project_backward(sc_ctx* ctx, const DSplats& s, const float4* proj_grad, const sc_camera* d_cam,
+                                  float* grads, uint32_t gcap, int accumulate);
+
+// fused multi-view project backward + grad accumulation + Adam + constraints
+struct AdamParams {
+  float lr[6];
+  float beta1, beta2, eps, bc1, bc2;
+  float log_scale_min, log_scale_max, opacity_logit_max;
+};
+sc_status launch_fused_backward_adam(sc_ctx* ctx, const DSplats& s, const DMoments& mo, const float4* proj_grad,
+                                     uint32_t stride, const sc_camera* d_cams, uint32_t n_views, float* grad_acc,
+                                     const AdamParams& ap, const uint32_t* d_skip_flag, const float* d_bc);
+
+// scan / sort
+sc_status scan_u32(sc_ctx* ctx, uint32_t* data, uint64_t n, uint64_t* d_total, void* scratch, size_t scratch_bytes);
+size_t scan_scratch_bytes(uint64_t n);
+template <typename K>
+sc_status radix_sort(sc_ctx* ctx, K* keys, uint32_t* vals, K* keys_tmp, uint32_t* vals_tmp, uint64_t n,
+                     uint32_t key_bits, const uint64_t* d_n, void* scratch, size_t scratch_bytes, bool* result_in_tmp);
+size_t radix_scratch_bytes(uint64_t n, uint32_t key_bytes);
+
+// binning
+sc_status launch_tile_count(sc_ctx* ctx, const float4* rec, uint32_t n, uint32_t stride, uint32_t n_views,
+                            const sc_tiling* tl, uint32_t* counts);
+sc_status launch_tile_emit(sc_ctx* ctx, const float4* rec, uint32_t n, uint32_t stride, uint32_t n_views,
+                           const sc_tiling* tl, const uint32_t* offsets, int key_mode, void* keys,
+                           uint32_t* payloads, uint64_t cap);
+sc_status launch_tile_ranges(sc_ctx* ctx, const void* keys, int key_mode, const uint64_t* d_total, uint64_t cap,
+                             uint32_t num_tiles, uint32_t* ranges);
+// depth-presorted emission for the native pipeline
+sc_status launch_presorted_counts(sc_ctx* ctx, const uint32_t* counts_by_id, uint32_t stride, uint32_t n_views,
+                                  const uint32_t* sorted_ids, uint32_t* counts);
+sc_status launch_presorted_emit(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
+                                const uint32_t* sorted_ids, const uint32_t* offsets, const sc_tiling* tl,
+                                uint32_t* keys, uint32_t* payloads, uint64_t cap, uint32_t* d_error);
+
+// blending
+sc_status launch_composite(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
+                           const uint32_t* payloads, const uint32_t* ranges, const sc_tiling* tl, float4* image,
+                           uint2* aux, const float* target, float mse_scale, float4* dl_dc, double* loss,
+                           const uint32_t* d_skip);
+sc_status launch_mse(sc_ctx* ctx, const float4* pred, const float* target, uint64_t pixels_per_view,
+                     uint32_t n_views, float scale, float4* dl_dc, double* loss);
+sc_status launch_composite_backward(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
+                                    const uint32_t* payloads, const uint32_t* ranges, const sc_tiling* tl,
+                                    const float4* fwd, const float4* dl_dc, int mode, const uint2* aux,
+                                    float4* proj_grad, const uint32_t* d_skip);
+sc_status launch_tonemap(sc_ctx* ctx, const float4* img, uint32_t w, uint32_t h, uint8_t* out);
+
+// optimiser
+sc_status launch_adam_lanes(sc_ctx* ctx, float* p, const float* g, float* m, float* v, uint64_t n, float lr,
+                            float b1, float b2, float eps, float bc1, float bc2);
+sc_status launch_adam_all(sc_ctx* ctx, const DSplats& s, const float* g, uint32_t gcap, const DMoments& mo,
+                          const AdamParams& ap);
+sc_status launch_constraints(sc_ctx* ctx, const DSplats& s, float lsmin, float lsmax, float opmax);
+sc_status launch_accumulate(sc_ctx* ctx, const float* g, uint32_t gcap, float* acc, uint32_t n);
+
+// densify / prune (compaction through a source map)
+sc_status prune(sc_ctx* ctx, sc_splats* s, sc_moments* mo, float* acc, float thr, uint32_t* removed);
+sc_status densify(sc_ctx* ctx, sc_splats* s, sc_moments* mo, float* acc, uint32_t grad_count, float gthr,
+                  float sthr, uint32_t max_splats, uint32_t iter, uint32_t counts[3]);
+
+}  // namespace sck
+
+// host-side f32 x^t by square-and-multiply (the algorithm behind f32::powi,
+// used for Adam's bias corrections, adam_gpu.rs:275-276)
+static inline float sc_powi_f32(float a, int b) {
+  const bool recip = b < 0;
+  float r = 1.0f;
+  for (;;) {
+    if (b & 1) r *= a;
+    b /= 2;
+    if (b == 0) break;
+    a *= a;
+  }
+  return recip ? 1.0f / r : r;
+}

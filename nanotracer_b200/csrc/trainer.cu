@@ -1,0 +1,410 @@
+// trainer.cu — the batched training iteration (train.rs:155-250 for n_views
+// views per step) as one stream of kernels, replayed as a CUDA graph.
+//
+//   H2D step params (cameras, Adam bias corrections)       memcpy node
+//   project + SH for all views, per-view depth keys, counts  k_project
+//   per-view depth sort of the splats                        onesweep u64 (view<<32 | depth bits)
+//   tile counts in depth order -> offsets                    gather + decoupled-look-back scan
+//   pair emission (view*T + tile, splat)                     warp-cooperative emit
+//   stable tile sort of the pairs                            onesweep u32 (ceil(log2(V*T)) bits)
+//   per-tile ranges                                          k_tile_ranges
+//   alpha-blend forward + fused MSE dL/dC                    k_composite
+//   alpha-blend backward (exact or reference transmittance) k_composite_backward
+//   project backward over all views + grad acc + Adam + constraints   k_fused_backward_adam
+//   loss / pair count / error word -> pinned host           finalize + memcpy node
+//
+// The pair buffers have a device-side capacity.  When a step emits more pairs
+// than fit, the emit kernel raises SC_DEVERR_CAPACITY, the blend and Adam
+// kernels of that step skip their work (parameters are untouched), and the host
+// grows the buffers and runs the step again.
+#include "sc_internal.cuh"
+
+#include <algorithm>
+#include <cstddef>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace {
+
+struct StepParams {
+  sc_camera cams[SC_MAX_VIEWS];
+  float bc[4];  // bc1, bc2
+};
+
+struct StepOut {
+  double loss;
+  unsigned long long pairs;
+  uint32_t err;
+  uint32_t pad;
+};
+
+__global__ void k_finalize(const double* __restrict__ loss_sums, uint32_t n_views, double inv_count,
+                           const uint64_t* __restrict__ d_total, const uint32_t* __restrict__ err,
+                           StepOut* __restrict__ out) {
+  double acc = 0.0;
+  for (uint32_t v = 0; v < n_views; ++v) acc += loss_sums[v] * inv_count;
+  out->loss = acc / (double)n_views;
+  out->pairs = *d_total;
+  out->err = *err;
+}
+
+const char* kStageNames[] = {"project", "depth_sort", "count_scan", "emit", "tile_sort", "ranges",
+                             "blend_fwd", "blend_bwd", "bwd_adam"};
+constexpr int kStages = 9;
+
+uint32_t bits_for(uint64_t max_value) {
+  uint32_t b = 0;
+  while (b < 64 && (max_value >> b) != 0) ++b;
+  return b;
+}
+
+}  // namespace
+
+struct sc_trainer {
+  sc_ctx* ctx = nullptr;
+  sc_train_config cfg{};
+  uint32_t V = 0, tiles_x = 0, tiles_y = 0, T = 0;
+  uint64_t P = 0;
+  uint32_t stride = 0;
+  StepParams* h_params = nullptr;
+  StepParams* d_params = nullptr;
+  StepOut* h_out = nullptr;
+  StepOut* d_out = nullptr;
+  // per (view, splat)
+  float4* rec = nullptr; float4* pgrad = nullptr;
+  uint64_t* dkeys = nullptr; uint64_t* dkeys_tmp = nullptr;
+  uint32_t* ids = nullptr; uint32_t* ids_tmp = nullptr;
+  uint32_t* counts_by_id = nullptr; uint32_t* counts = nullptr;
+  // pairs
+  uint64_t kcap = 0;
+  uint32_t* keys = nullptr; uint32_t* keys_tmp = nullptr; uint32_t* vals = nullptr; uint32_t* vals_tmp = nullptr;
+  // per (view, tile) / pixel
+  uint32_t* ranges = nullptr;
+  float4* image = nullptr; uint2* aux = nullptr; float4* dl_dc = nullptr;
+  const float* targets = nullptr;
+  double* d_loss = nullptr;
+  uint64_t* d_total = nullptr;
+  void* scratch = nullptr; size_t scratch_bytes = 0;
+  // graph
+  cudaGraphExec_t exec = nullptr;
+  const void* g_key[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  uint64_t g_key_n = 0, g_key_kcap = 0;
+  // results of the last step
+  uint64_t last_pairs = 0;
+  uint32_t kernels_per_step = 0;
+  // profiling
+  bool profiling = false;
+  cudaEvent_t ev[kStages + 1] = {};
+  double acc_ms[kStages] = {};
+  uint64_t prof_steps = 0;
+  float avg_ms_out[kStages] = {};
+};
+
+static void trainer_free_splat_arrays(sc_trainer* tr) {
+  cudaFree(tr->rec); cudaFree(tr->pgrad); cudaFree(tr->dkeys); cudaFree(tr->dkeys_tmp);
+  cudaFree(tr->ids); cudaFree(tr->ids_tmp); cudaFree(tr->counts_by_id); cudaFree(tr->counts);
+  tr->rec = tr->pgrad = nullptr; tr->dkeys = tr->dkeys_tmp = nullptr;
+  tr->ids = tr->ids_tmp = tr->counts_by_id = tr->counts = nullptr;
+  tr->stride = 0;
+}
+
+static void trainer_free_pairs(sc_trainer* tr) {
+  cudaFree(tr->keys); cudaFree(tr->keys_tmp); cudaFree(tr->vals); cudaFree(tr->vals_tmp);
+  tr->keys = tr->keys_tmp = tr->vals = tr->vals_tmp = nullptr;
+  tr->kcap = 0;
+}
+
+static void trainer_drop_graph(sc_trainer* tr) {
+  if (tr->exec) cudaGraphExecDestroy(tr->exec);
+  tr->exec = nullptr;
+}
+
+static sc_status ensure_scratch(sc_trainer* tr) {
+  sc_ctx* ctx = tr->ctx;
+  const uint64_t nsp = (uint64_t)tr->V * tr->stride;
+  size_t need = std::max({sck::radix_scratch_bytes(nsp, 8), sck::radix_scratch_bytes(std::max<uint64_t>(tr->kcap, 1), 4),
+                          sck::scan_scratch_bytes(nsp + 1)});
+  if (need <= tr->scratch_bytes) return SC_OK;
+  SC_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+  cudaFree(tr->scratch);
+  tr->scratch = nullptr;
+  need = need + need / 4;
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->scratch, need), "trainer scratch");
+  tr->scratch_bytes = need;
+  trainer_drop_graph(tr);
+  return SC_OK;
+}
+
+static sc_status ensure_splat_arrays(sc_trainer* tr, uint32_t cap) {
+  if (tr->stride == cap) return SC_OK;
+  sc_ctx* ctx = tr->ctx;
+  SC_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+  trainer_free_splat_arrays(tr);
+  const size_t nv = (size_t)tr->V * cap;
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->rec, nv * 48), "rec");
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->pgrad, nv * 48), "pgrad");
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->dkeys, nv * 8), "dkeys");
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->dkeys_tmp, nv * 8), "dkeys");
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->ids, nv * 4), "ids");
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->ids_tmp, nv * 4), "ids");
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->counts_by_id, nv * 4), "counts");
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->counts, (nv + 1) * 4), "counts");
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->rec, 0, nv * 48, ctx->stream), "zero");
+  tr->stride = cap;
+  trainer_drop_graph(tr);
+  return ensure_scratch(tr);
+}
+
+static sc_status ensure_pairs(sc_trainer* tr, uint64_t K) {
+  if (K <= tr->kcap && tr->kcap) return SC_OK;
+  sc_ctx* ctx = tr->ctx;
+  SC_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+  trainer_free_pairs(tr);
+  uint64_t cap = K + K / 4 + 65536;
+  if (cap > (1ull << 30) - 1) cap = (1ull << 30) - 1;
+  if (K > cap) return sc_fail(ctx, SC_ERR_CAPACITY, "more than 2^30 tile/splat pairs in one step");
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->keys, cap * 4), "keys");
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->keys_tmp, cap * 4), "keys");
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->vals, cap * 4), "vals");
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->vals_tmp, cap * 4), "vals");
+  // zero-filled so a step whose emission overflowed still reads valid ids
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->keys, 0, cap * 4, ctx->stream), "zero");
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->keys_tmp, 0, cap * 4, ctx->stream), "zero");
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->vals, 0, cap * 4, ctx->stream), "zero");
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->vals_tmp, 0, cap * 4, ctx->stream), "zero");
+  tr->kcap = cap;
+  trainer_drop_graph(tr);
+  return ensure_scratch(tr);
+}
+
+static void mark(sc_trainer* tr, int i, bool capturing) {
+  if (!tr->profiling) return;
+  if (capturing)
+    cudaEventRecordWithFlags(tr->ev[i], tr->ctx->stream, cudaEventRecordExternal);
+  else
+    cudaEventRecord(tr->ev[i], tr->ctx->stream);
+}
+
+// Enqueue one step.  sizing: stop after the scan, read the pair count and
+// (re)size the pair buffers before emitting (eager runs only).
+static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, float* acc, bool capturing, bool sizing) {
+  sc_ctx* ctx = tr->ctx;
+  const sc_camera* d_cams = reinterpret_cast<const sc_camera*>(tr->d_params);  // cams is the first member
+  const float* d_bc = reinterpret_cast<const float*>(reinterpret_cast<const char*>(tr->d_params) +
+                                                     offsetof(StepParams, bc));
+  const uint32_t V = tr->V;
+  const uint64_t nsp = (uint64_t)V * tr->stride;
+  const DSplats ds = dview(s);
+  const DMoments dm = dview(mo);
+  const uint64_t launches0 = ctx->launches;
+  SC_CUDA_TRY(ctx, cudaMemcpyAsync(tr->d_params, tr->h_params, sizeof(StepParams), cudaMemcpyHostToDevice, ctx->stream),
+              "params H2D");
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->d_loss, 0, 8 * (size_t)V, ctx->stream), "zero loss");
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->pgrad, 0, nsp * 48, ctx->stream), "zero pgrad");
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->counts + nsp, 0, 4, ctx->stream), "zero count tail");
+  mark(tr, 0, capturing);
+  SC_TRY(sck::launch_project(ctx, ds, d_cams, V, tr->stride, tr->rec, &tr->cfg.tiling, tr->dkeys, tr->ids,
+                             tr->counts_by_id, 0));
+  mark(tr, 1, capturing);
+  bool in_tmp = false;
+  SC_TRY(sck::radix_sort<uint64_t>(ctx, tr->dkeys, tr->ids, tr->dkeys_tmp, tr->ids_tmp, nsp, 32 + bits_for(V - 1),
+                                   nullptr, tr->scratch, tr->scratch_bytes, &in_tmp));
+  const uint32_t* sorted_ids = in_tmp ? tr->ids_tmp : tr->ids;
+  mark(tr, 2, capturing);
+  SC_TRY(sck::launch_presorted_counts(ctx, tr->counts_by_id, tr->stride, V, sorted_ids, tr->counts));
+  SC_TRY(sck::scan_u32(ctx, tr->counts, nsp + 1, tr->d_total, tr->scratch, tr->scratch_bytes));
+  if (sizing) {
+    uint64_t K = 0;
+    SC_CUDA_TRY(ctx, cudaMemcpyAsync(&K, tr->d_total, 8, cudaMemcpyDeviceToHost, ctx->stream), "K");
+    SC_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+    SC_TRY(ensure_pairs(tr, K));
+  }
+  mark(tr, 3, capturing);
+  SC_TRY(sck::launch_presorted_emit(ctx, tr->rec, tr->stride, V, sorted_ids, tr->counts, &tr->cfg.tiling, tr->keys,
+                                    tr->vals, tr->kcap, ctx->d_error));
+  mark(tr, 4, capturing);
+  const uint32_t all_tiles = V * tr->T;
+  SC_TRY(sck::radix_sort<uint32_t>(ctx, tr->keys, tr->vals, tr->keys_tmp, tr->vals_tmp, tr->kcap,
+                                   std::max(1u, bits_for(all_tiles - 1)), tr->d_total, tr->scratch, tr->scratch_bytes,
+                                   &in_tmp));
+  const uint32_t* skeys = in_tmp ? tr->keys_tmp : tr->keys;
+  const uint32_t* svals = in_tmp ? tr->vals_tmp : tr->vals;
+  mark(tr, 5, capturing);
+  SC_TRY(sck::launch_tile_ranges(ctx, skeys, 2, tr->d_total, tr->kcap, all_tiles, tr->ranges));
+  mark(tr, 6, capturing);
+  SC_TRY(sck::launch_composite(ctx, tr->rec, tr->stride, V, svals, tr->ranges, &tr->cfg.tiling, tr->image, tr->aux,
+                               tr->targets, 1.0f / (float)V, tr->dl_dc, tr->d_loss, ctx->d_error));
+  mark(tr, 7, capturing);
+  SC_TRY(sck::launch_composite_backward(ctx, tr->rec, tr->stride, V, svals, tr->ranges, &tr->cfg.tiling, tr->image,
+                                        tr->dl_dc, (int)tr->cfg.bwd_mode, tr->aux, tr->pgrad, ctx->d_error));
+  mark(tr, 8, capturing);
+  sck::AdamParams ap;
+  for (int k = 0; k < 6; ++k) ap.lr[k] = tr->cfg.adam.lr[k];
+  ap.beta1 = tr->cfg.adam.beta1; ap.beta2 = tr->cfg.adam.beta2; ap.eps = tr->cfg.adam.eps;
+  ap.bc1 = ap.bc2 = 1.0f;
+  ap.log_scale_min = tr->cfg.log_scale_min; ap.log_scale_max = tr->cfg.log_scale_max;
+  ap.opacity_logit_max = tr->cfg.opacity_logit_max;
+  SC_TRY(sck::launch_fused_backward_adam(ctx, ds, dm, tr->pgrad, tr->stride, d_cams, V, acc, ap, ctx->d_error, d_bc));
+  mark(tr, 9, capturing);
+  k_finalize<<<1, 1, 0, ctx->stream>>>(tr->d_loss, V, 1.0 / (3.0 * (double)tr->P), tr->d_total, ctx->d_error, tr->d_out);
+  SC_TRY(sc_check_launch(ctx, "k_finalize"));
+  SC_CUDA_TRY(ctx, cudaMemcpyAsync(tr->h_out, tr->d_out, sizeof(StepOut), cudaMemcpyDeviceToHost, ctx->stream), "out D2H");
+  tr->kernels_per_step = (uint32_t)(ctx->launches - launches0);
+  return SC_OK;
+}
+
+extern "C" {
+
+sc_status sc_trainer_create(sc_ctx* ctx, const sc_train_config* cfg, sc_trainer** out) {
+  if (!ctx || !cfg || !out) return SC_ERR_INVALID_ARG;
+  if (cfg->n_views == 0 || cfg->n_views > SC_MAX_VIEWS) return sc_fail(ctx, SC_ERR_INVALID_ARG, "n_views out of range");
+  const sc_tiling& t = cfg->tiling;
+  if (!t.width || !t.height || !t.tile_w || !t.tile_h) return SC_ERR_INVALID_ARG;
+  const uint32_t threads = t.tile_w * t.tile_h;
+  if (threads > 256 || threads % 32) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile must hold 32..256 pixels, multiple of 32");
+  if (cfg->bwd_mode != SC_BWD_REF && cfg->bwd_mode != SC_BWD_EXACT) return SC_ERR_INVALID_ARG;
+  sc_trainer* tr = new sc_trainer();
+  tr->ctx = ctx;
+  tr->cfg = *cfg;
+  tr->V = cfg->n_views;
+  tr->tiles_x = (t.width + t.tile_w - 1) / t.tile_w;
+  tr->tiles_y = (t.height + t.tile_h - 1) / t.tile_h;
+  tr->T = tr->tiles_x * tr->tiles_y;
+  tr->P = (uint64_t)t.width * t.height;
+  const size_t pix = (size_t)tr->V * tr->P;
+  cudaError_t e = cudaMallocHost(&tr->h_params, sizeof(StepParams));
+  if (e == cudaSuccess) e = cudaMallocHost(&tr->h_out, sizeof(StepOut));
+  if (e == cudaSuccess) e = cudaMalloc(&tr->d_params, sizeof(StepParams));
+  if (e == cudaSuccess) e = cudaMalloc(&tr->d_out, sizeof(StepOut));
+  if (e == cudaSuccess) e = cudaMalloc(&tr->ranges, (size_t)tr->V * tr->T * 8);
+  if (e == cudaSuccess) e = cudaMalloc(&tr->image, pix * 16);
+  if (e == cudaSuccess) e = cudaMalloc(&tr->aux, pix * 8);
+  if (e == cudaSuccess) e = cudaMalloc(&tr->dl_dc, pix * 16);
+  if (e == cudaSuccess) e = cudaMalloc(&tr->d_loss, 8 * (size_t)tr->V);
+  if (e == cudaSuccess) e = cudaMalloc(&tr->d_total, 64);
+  for (int i = 0; i <= kStages && e == cudaSuccess; ++i) e = cudaEventCreate(&tr->ev[i]);
+  if (e != cudaSuccess) {
+    sc_trainer_free(ctx, tr);
+    return sc_cuda_fail(ctx, e, "trainer alloc");
+  }
+  std::memset(tr->h_params, 0, sizeof(StepParams));
+  *out = tr;
+  return SC_OK;
+}
+
+void sc_trainer_free(sc_ctx* ctx, sc_trainer* tr) {
+  if (!tr) return;
+  if (ctx) cudaStreamSynchronize(ctx->stream);
+  trainer_drop_graph(tr);
+  trainer_free_splat_arrays(tr);
+  trainer_free_pairs(tr);
+  cudaFree(tr->ranges); cudaFree(tr->image); cudaFree(tr->aux); cudaFree(tr->dl_dc);
+  cudaFree(tr->d_loss); cudaFree(tr->d_total); cudaFree(tr->d_params); cudaFree(tr->d_out);
+  cudaFree(tr->scratch);
+  if (tr->h_params) cudaFreeHost(tr->h_params);
+  if (tr->h_out) cudaFreeHost(tr->h_out);
+  for (int i = 0; i <= kStages; ++i)
+    if (tr->ev[i]) cudaEventDestroy(tr->ev[i]);
+  delete tr;
+}
+
+sc_status sc_trainer_set_targets(sc_trainer* tr, const float* targets) {
+  if (!tr || !targets) return SC_ERR_INVALID_ARG;
+  if (tr->targets != targets) trainer_drop_graph(tr);
+  tr->targets = targets;
+  return SC_OK;
+}
+
+sc_status sc_trainer_set_profiling(sc_trainer* tr, int enabled) {
+  if (!tr) return SC_ERR_INVALID_ARG;
+  if (tr->profiling != (enabled != 0)) trainer_drop_graph(tr);
+  tr->profiling = enabled != 0;
+  for (int i = 0; i < kStages; ++i) tr->acc_ms[i] = 0.0;
+  tr->prof_steps = 0;
+  return SC_OK;
+}
+
+sc_status sc_trainer_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, float* acc, const sc_camera* cams, uint64_t t,
+                          double* loss_out) {
+  if (!tr || !s || !mo || !acc || !cams || t == 0) return SC_ERR_INVALID_ARG;
+  if (!tr->targets) return sc_fail(tr->ctx, SC_ERR_INVALID_ARG, "trainer has no targets");
+  if (mo->cap < s->n) return SC_ERR_INVALID_ARG;
+  sc_ctx* ctx = tr->ctx;
+  // step parameters into pinned memory (the graph's first node copies them)
+  std::memcpy(tr->h_params->cams, cams, sizeof(sc_camera) * tr->V);
+  tr->h_params->bc[0] = 1.0f - sc_powi_f32(tr->cfg.adam.beta1, (int)t);
+  tr->h_params->bc[1] = 1.0f - sc_powi_f32(tr->cfg.adam.beta2, (int)t);
+  SC_TRY(ensure_splat_arrays(tr, s->cap));
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    const bool sizing = tr->kcap == 0;
+    const void* key[6] = {s->slab, s->rest16, mo->m ? (const void*)mo->m : (const void*)mo->m16, acc, tr->targets,
+                          tr->scratch};
+    const bool key_ok = tr->exec && std::equal(key, key + 6, tr->g_key) && tr->g_key_n == s->n &&
+                        tr->g_key_kcap == tr->kcap;
+    if (!key_ok) trainer_drop_graph(tr);
+    if (tr->cfg.use_graph && !sizing) {
+      if (!tr->exec) {
+        cudaGraph_t g = nullptr;
+        SC_CUDA_TRY(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed), "begin capture");
+        sc_status st = enqueue_step(tr, s, mo, acc, true, false);
+        cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
+        if (st != SC_OK) { if (g) cudaGraphDestroy(g); return st; }
+        if (ce != cudaSuccess) return sc_cuda_fail(ctx, ce, "end capture");
+        ce = cudaGraphInstantiate(&tr->exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) { tr->exec = nullptr; return sc_cuda_fail(ctx, ce, "graph instantiate"); }
+        std::copy(key, key + 6, tr->g_key);
+        tr->g_key_n = s->n;
+        tr->g_key_kcap = tr->kcap;
+      }
+      SC_CUDA_TRY(ctx, cudaGraphLaunch(tr->exec, ctx->stream), "graph launch");
+      ctx->launches += tr->kernels_per_step;
+    } else {
+      SC_TRY(enqueue_step(tr, s, mo, acc, false, sizing));
+    }
+    SC_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "step sync");
+    const StepOut o = *tr->h_out;
+    tr->last_pairs = o.pairs;
+    if (o.err & SC_DEVERR_TIMEOUT) {
+      cudaMemsetAsync(ctx->d_error, 0, 4, ctx->stream);
+      return sc_fail(ctx, SC_ERR_TIMEOUT, "a bounded device wait gave up during the step");
+    }
+    if (o.err & SC_DEVERR_CAPACITY) {
+      // the blend and Adam kernels skipped this step; grow and run it again
+      SC_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_error, 0, 4, ctx->stream), "clear error");
+      SC_TRY(ensure_pairs(tr, o.pairs));
+      continue;
+    }
+    if (tr->profiling) {
+      for (int i = 0; i < kStages; ++i) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, tr->ev[i], tr->ev[i + 1]) == cudaSuccess) tr->acc_ms[i] += ms;
+      }
+      tr->prof_steps++;
+    }
+    if (loss_out) *loss_out = o.loss;
+    return SC_OK;
+  }
+  return sc_fail(ctx, SC_ERR_CAPACITY, "pair capacity kept overflowing");
+}
+
+sc_status sc_trainer_images(const sc_trainer* tr, const float** images) {
+  if (!tr || !images) return SC_ERR_INVALID_ARG;
+  *images = reinterpret_cast<const float*>(tr->image);
+  return SC_OK;
+}
+
+sc_status sc_trainer_stats(const sc_trainer* tr, uint64_t* pairs, uint32_t* n_kernels, const char** names,
+                           float* avg_ms) {
+  if (!tr) return SC_ERR_INVALID_ARG;
+  if (pairs) *pairs = tr->last_pairs;
+  if (n_kernels) *n_kernels = tr->kernels_per_step;
+  for (int i = 0; i < kStages; ++i) {
+    if (names) names[i] = kStageNames[i];
+    if (avg_ms) avg_ms[i] = tr->prof_steps ? (float)(tr->acc_ms[i] / (double)tr->prof_steps) : 0.0f;
+  }
+  return SC_OK;
+}
+
+}  // extern "C"

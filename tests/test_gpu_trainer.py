@@ -1,0 +1,158 @@
+"""The batched training step (sc_trainer): equivalence with the stage-by-stage
+reference-shaped path, parity with the oracle's whole iteration, finite
+differences through the device adjoint, graph replay, capacity growth."""
+import json
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from nanotracer_b200 import (AdamMomentBuffers, CameraUniform, GpuSplatBuffer, GradSplatBuffers, SplatBuffer,
+                             TilingParams, TrainConfig, Trainer)
+from nanotracer_b200._lib import SC_BWD_EXACT, SC_BWD_REF, SC_KEYS_NATIVE64
+from nanotracer_b200.scene import FOV_Y, orbit_views, perturbed, random_scene
+from nanotracer_b200.train import BENCH_LRS, render_targets
+
+from tests.util import GpuPipe
+
+pytestmark = pytest.mark.gpu
+KATS = json.loads((Path(__file__).parent / "golden" / "reference_kats.json").read_text())
+
+
+def _setup(ctx, n=3000, W=128, H=96, V=2, step=0, exact=True, graph=True, tile=(16, 16), bf16=False, seed=21):
+    scene = random_scene(n, seed)
+    tl = TilingParams(W, H, tile[0], 8.0, tile_h_override=tile[1])
+    cams = [CameraUniform.from_pose(*p, FOV_Y, W, H, n) for p in orbit_views(V, step)]
+    tgt = render_targets(ctx, perturbed(scene), cams, tl)
+    cfg = TrainConfig(n_views=V, width=W, height=H, tile_w=tile[0], tile_h=tile[1], depth_max=8.0,
+                      exact_backward=exact, use_graph=graph, bf16=bf16)
+    return scene, tl, cams, tgt, cfg
+
+
+def _run(ctx, scene, cams, tgt, cfg, steps=1, cap=0):
+    g = GpuSplatBuffer.upload(ctx, scene, capacity=cap, bf16_rest=cfg.bf16)
+    mo = AdamMomentBuffers(ctx, g.capacity, bf16=cfg.bf16)
+    acc = ctx.storage_buffer_zeroed("acc", 4 * g.capacity)
+    tr = Trainer(ctx, cfg)
+    tb = ctx.storage_buffer("targets", np.ascontiguousarray(tgt, np.float32))
+    tr.set_targets(tb)
+    losses = [tr.step(g, mo, acc, cams, t) for t in range(1, steps + 1)]
+    return tr, g, mo, acc, losses
+
+
+@pytest.mark.parametrize("tile", [(16, 16), (8, 8), (32, 8)])
+def test_trainer_images_equal_reference_order_binning(ctx, tile):
+    """The trainer's depth-presort + tile-key sort reproduces the 64-bit
+    (tile, depth) key order exactly: its forward images equal, bit for bit,
+    those of sc_bin(NATIVE64) + sc_composite on the same records."""
+    scene, tl, cams, tgt, cfg = _setup(ctx, V=3, tile=tile)
+    pipe = GpuPipe(ctx, scene, cams, tl, key_mode=SC_KEYS_NATIVE64)
+    pipe.project()
+    pipe.bin()
+    ref_img, _ = pipe.composite()
+    tr, *_ = _run(ctx, scene, cams, tgt, cfg)
+    assert np.array_equal(tr.images(), ref_img)
+
+
+@pytest.mark.parametrize("exact", [True, False])
+def test_trainer_step_matches_oracle_iteration(ctx, oracle, exact):
+    scene, tl, cams, tgt, cfg = _setup(ctx, n=1500, W=96, H=64, V=2, exact=exact)
+    tr, g, mo, acc, losses = _run(ctx, scene, cams, tgt, cfg)
+    os_ = oracle.OSplats.from_buffer(scene)
+    om, ov = oracle.OSplats.zeros(len(scene)), oracle.OSplats.zeros(len(scene))
+    oacc = np.zeros(len(scene), np.float32)
+    ocams = [oracle.camera_from_struct(bytes(c.c)) for c in cams]
+    oloss, oimgs = oracle.train_step(os_, om, ov, oacc, ocams, tgt, oracle.tiling(96, 64, 16, 16, 8.0),
+                                     1 if exact else 0, BENCH_LRS, 1, want_images=True)
+    assert abs(losses[0] - oloss) <= 1e-5 * oloss
+    imgs = tr.images().reshape(-1)
+    assert np.mean(np.abs(imgs - oimgs) <= 1e-4) > 0.999
+    got, want = g.readback().flat(), os_.flat()
+    d = np.abs(got - want)
+    # one Adam step moves each parameter by about lr * sign(g): parameters agree
+    # unless a gradient is within rounding of zero
+    assert np.mean(d <= 1e-6 + 1e-6 * np.abs(want)) > 0.995
+    gacc = acc.readback(np.float32, len(scene))
+    assert np.allclose(gacc, oacc, rtol=2e-3, atol=1e-9 + 1e-3 * np.abs(oacc).max())
+
+
+def test_trainer_graph_replay_equals_eager(ctx):
+    scene, tl, cams, tgt, cfg = _setup(ctx, n=2000)
+    cfg_e = TrainConfig(**{**cfg.__dict__, "use_graph": False})
+    _, g1, _, _, l1 = _run(ctx, scene, cams, tgt, cfg, steps=3)
+    _, g2, _, _, l2 = _run(ctx, scene, cams, tgt, cfg_e, steps=3)
+    # the backward's float atomics make the summation order (not the values) vary
+    assert np.allclose(g1.readback().flat(), g2.readback().flat(), rtol=1e-5, atol=1e-7)
+    assert np.allclose(l1, l2, rtol=1e-6)
+
+
+def test_trainer_pair_capacity_growth(ctx):
+    """A step that emits more pairs than the device capacity changes nothing,
+    grows the buffers and runs again; the result equals a fresh run's."""
+    small, tl, cams, tgt, cfg = _setup(ctx, n=200)
+    big = random_scene(20000, 22)
+    tgt_big = render_targets(ctx, perturbed(big), cams, tl)
+    g = GpuSplatBuffer.upload(ctx, big)
+    mo = AdamMomentBuffers(ctx, g.capacity)
+    acc = ctx.storage_buffer_zeroed("acc", 4 * g.capacity)
+    tr = Trainer(ctx, cfg)
+    tr.set_targets(ctx.storage_buffer("t0", np.ascontiguousarray(tgt, np.float32)))
+    gs = GpuSplatBuffer.upload(ctx, small)
+    ms = AdamMomentBuffers(ctx, gs.capacity)
+    accs = ctx.storage_buffer_zeroed("a", 4 * gs.capacity)
+    tr.step(gs, ms, accs, cams, 1)  # sizes the pair buffers for the small scene
+    small_pairs = tr.stats()["pairs"]
+    tr.set_targets(ctx.storage_buffer("t1", np.ascontiguousarray(tgt_big, np.float32)))
+    loss = tr.step(g, mo, acc, cams, 1)
+    assert tr.stats()["pairs"] > 4 * small_pairs
+    _, g2, _, _, l2 = _run(ctx, big, cams, tgt_big, cfg)
+    assert abs(loss - l2[0]) <= 1e-9 * l2[0]
+    assert np.allclose(g.readback().flat(), g2.readback().flat(), rtol=1e-5, atol=1e-7)
+
+
+def test_finite_diff_through_device_adjoint(ctx):
+    """backward_finite_diff.rs:173-246 on the device path (forward and analytic
+    gradient both from the CUDA kernels), with the reference's tolerances."""
+    k = KATS["finite_diff_matches_analytic"]
+    sp, cm, t = k["splat"], k["camera"], k["tiling"]
+    rest = np.zeros(45, np.float32)
+    for i, v in sp["sh_rest"].items():
+        rest[int(i)] = v
+    base = SplatBuffer([sp["pos"]], [sp["rot"]], [sp["log_scale"]], [sp["opacity_logit"]], [sp["sh_dc"]], [rest])
+    cam = CameraUniform.from_pose(cm["eye"], cm["target"], cm["up"], cm["fov_y"], cm["width"], cm["height"], 1)
+    tl = TilingParams(cm["width"], cm["height"], t["tile_size"], t["depth_max"])
+
+    def loss(s):
+        p = GpuPipe(ctx, s, cam, tl)
+        p.project()
+        p.bin()
+        img, _ = p.composite()
+        return float(img[..., :3].astype(np.float64).sum())
+
+    p = GpuPipe(ctx, base, cam, tl)
+    p.project()
+    p.bin()
+    p.composite()
+    p.backward(np.tile(np.array([1, 1, 1, 0], np.float32), (tl.width * tl.height, 1)), SC_BWD_REF)
+    grads = GradSplatBuffers(ctx, 1)
+    p.r.project_backward(p.g, p.pg, cam, grads)
+    ga = grads.readback(1).flat()[0]
+    eps = k["eps"]
+    for name, col in {"sh_dc.r": 11, "opacity": 10, "sh_rest[0]": 14, "pos.x": 0, "log_scale.x": 7}.items():
+        fp, fm = base.flat().copy(), base.flat().copy()
+        fp[0, col] += eps
+        fm[0, col] -= eps
+        num = (loss(SplatBuffer.from_flat(fp)) - loss(SplatBuffer.from_flat(fm))) / (2 * eps)
+        rel, ab = k["checks"][name]
+        a = float(ga[col])
+        assert abs(a - num) <= ab or abs(a - num) <= rel * (abs(a) + abs(num)), (name, a, num)
+
+
+def test_bf16_storage_step_close_to_fp32(ctx):
+    scene, tl, cams, tgt, cfg = _setup(ctx, n=3000)
+    cfg16 = TrainConfig(**{**cfg.__dict__, "bf16": True})
+    _, _, _, _, l32 = _run(ctx, scene, cams, tgt, cfg, steps=5)
+    _, _, _, _, l16 = _run(ctx, scene, cams, tgt, cfg16, steps=5)
+    assert abs(l16[0] - l32[0]) <= 2e-3 * l32[0]
+    assert l16[-1] < l16[0] and l32[-1] < l32[0]
