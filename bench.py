@@ -45,18 +45,22 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """nvidia-smi clock / throttle sampling (100 ms period).  Started before the
+    warm-up so samples exist for short timed regions; summary() keeps the
+    samples taken inside [t0, t1] (host wall clock), or the nearest ones."""
 
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    QUERY = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
-    def __init__(self, device_index: int):
+    def __init__(self, device_index: int, raw_copy: str | None = None):
         self.dev = device_index
         self.proc = None
+        self.raw_copy = raw_copy
         self.path = Path(tempfile.mkstemp(suffix=".csv")[1])
 
-    def __enter__(self):
+    def start(self):
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.QUERY}",
@@ -66,28 +70,44 @@ class ClockSampler:
             self.proc = None
         return self
 
-    def __exit__(self, *a):
+    def stop(self):
         if self.proc is not None:
+            time.sleep(0.25)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
             self.f.close()
+            self.proc = None
 
-    def summary(self):
+    def summary(self, t0: float, t1: float):
+        import datetime
         try:
-            rows = [l.split(",") for l in self.path.read_text().splitlines() if l.strip()]
+            text = self.path.read_text()
+            if self.raw_copy:
+                Path(self.raw_copy).parent.mkdir(exist_ok=True)
+                Path(self.raw_copy).write_text(text)
         except Exception:
-            rows = []
+            text = ""
+        rows = []
+        for line in text.splitlines():
+            r = [x.strip() for x in line.split(",")]
+            if len(r) < 10:
+                continue
+            try:
+                ts = datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rows.append((ts, float(r[2]), float(r[3]), r[6:10]))
+            except ValueError:
+                continue
         if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if len(r) > 5 + k and "Active" in r[5 + k]})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        inside = [r for r in rows if t0 - 0.05 <= r[0] <= t1 + 0.05]
+        if not inside:  # timed region shorter than the sampling period: nearest samples
+            inside = sorted(rows, key=lambda r: min(abs(r[0] - t0), abs(r[0] - t1)))[:2]
+        reasons = sorted({self.NAMES[k] for r in inside for k in range(4) if r[3][k] == "Active"})
+        return {"sm_mhz": statistics.median([r[1] for r in inside]), "sm_max_mhz": max(r[2] for r in inside),
+                "reasons": reasons, "samples": len(inside)}
 
 
 def dist_setup():
@@ -157,6 +177,7 @@ def run_ours(args):
     tbuf = ctx.storage_buffer("targets", tgt0)
     tr.set_targets(tbuf)
     cams_steps = [cams_for(s) for s in range(args.warmup + args.steps)]
+    clk = ClockSampler(local, raw_copy=os.environ.get("BENCH_CLOCKS_CSV")).start()
     t = 0
     for s in range(args.warmup):
         t += 1
@@ -171,20 +192,22 @@ def run_ours(args):
     launches0 = ctx.launch_count
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        torch.cuda.synchronize(local)
-        e0.record(stream)
-        for s in range(args.steps):
-            t += 1
-            loss = tr.step(g, mo, acc, cams_steps[args.warmup + s], t)
-        e1.record(stream)
-        torch.cuda.synchronize(local)
+    torch.cuda.synchronize(local)
+    w0 = time.time()
+    e0.record(stream)
+    for s in range(args.steps):
+        t += 1
+        loss = tr.step(g, mo, acc, cams_steps[args.warmup + s], t)
+    e1.record(stream)
+    torch.cuda.synchronize(local)
+    w1 = time.time()
+    clk.stop()
     barrier(pg)
     ms = e0.elapsed_time(e1)
     ms_max = max_over_ranks(pg, ms)
     launches = ctx.launch_count - launches0
     st = tr.stats()
-    clocks = clk.summary()
+    clocks = clk.summary(w0, w1)
 
     # ---- e2e through the public API: pinned host targets + cameras in, loss out
     e2e = None
@@ -305,8 +328,8 @@ def run_reference(args):
     O.set_threads(threads)
     n = args.splats
     scene = random_scene(n, 0x5EED5EED)
-    # bounded sample: one view per step at a quarter of the image area
-    W, H = args.width // 2, args.height // 2
+    # bounded sample: one of the iteration's views per step, full resolution
+    W, H = args.width, args.height
     otl = O.tiling(W, H, args.tile_w, args.tile_h, 8.0)
     os_ = O.OSplats.from_buffer(scene)
     om, ov = O.OSplats.zeros(n), O.OSplats.zeros(n)
@@ -319,16 +342,17 @@ def run_reference(args):
     for s in range(args.steps):
         O.train_step(os_, om, ov, acc, cam_at(args.warmup + s), tgt, otl, 1, BENCH_LRS, args.warmup + s + 1)
     dt = (time.perf_counter() - t0) / args.steps
-    # a full iteration: views x (4 x the quarter-area sample's raster work); counted conservatively as views x 4 x sample
-    per_iter = dt * args.views * 4
+    # a full iteration = n_views such samples (Adam over all parameters is
+    # counted once per sample, so the CPU iteration time is an upper estimate)
+    per_iter = dt * args.views
     v = 1.0 / per_iter
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": per_iter * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic seeded scene",
             "config": {"workload": f"{n} splats, {args.views} views x {args.width}x{args.height} per iteration"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"1 view at {W}x{H} (1/4 of the image area) fwd+bwd+Adam over all {n} splats "
-                                       f"per step, {dt:.2f} s; iteration = {args.views} views x 4 x sample"},
+                             "sample": f"1 of the {args.views} views at {W}x{H}, fwd+bwd+Adam over all {n} splats "
+                                       f"per step, {dt:.2f} s; iteration = {args.views} x sample"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -349,10 +373,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
-    args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         run_reference(args)
     else:
+        args.warmup = max(args.warmup, 3)
         run_ours(args)
 
 

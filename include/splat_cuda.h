@@ -292,6 +292,8 @@ typedef struct sc_train_config {
   uint32_t use_graph;          /* capture the iteration as a CUDA graph          */
   uint32_t blend_batch;        /* splats staged per shared-memory batch (0=auto) */
   uint32_t sort_mode;          /* 0 = auto, 1 = depth presort + tile pass, 2 = 64-bit key sort */
+  uint32_t tile_cull;          /* drop (tile, splat) pairs whose alpha stays below 1/255 over the
+                                  whole tile (images unchanged: the blend skips those pairs) */
   float log_scale_min, log_scale_max, opacity_logit_max; /* train.rs:37-39 */
 } sc_train_config;
 

@@ -58,6 +58,7 @@ class sc_adam_groups(C.Structure):
 class sc_train_config(C.Structure):
     _fields_ = [("n_views", C.c_uint32), ("tiling", sc_tiling), ("adam", sc_adam_groups), ("bwd_mode", C.c_uint32),
                 ("use_graph", C.c_uint32), ("blend_batch", C.c_uint32), ("sort_mode", C.c_uint32),
+                ("tile_cull", C.c_uint32),
                 ("log_scale_min", C.c_float), ("log_scale_max", C.c_float), ("opacity_logit_max", C.c_float)]
 
 

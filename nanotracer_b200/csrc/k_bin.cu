@@ -179,25 +179,35 @@ sc_status launch_presorted_counts(sc_ctx* ctx, const uint32_t* counts_by_id, uin
 }
 
 // One warp emits the pairs of 32 consecutive depth-ranked splats: the lanes
-// walk the concatenation of the 32 tile rectangles, so long rectangles do not
-// serialise a single thread.
+// walk the tile rectangle of one splat at a time, 32 tiles per step, so long
+// rectangles do not serialise a single thread.  With culling, lanes test their
+// tiles with tile_reachable (the function the projection counted with) and
+// compact the survivors with a ballot.  Exactly `count` pairs are written per
+// splat; should a decision ever differ from the count, surplus tiles are
+// dropped and missing slots get an out-of-range key that sorts last and that
+// the range kernel ignores.
 __global__ void __launch_bounds__(256) k_presorted_emit(const float4* __restrict__ rec, uint32_t stride,
                                                          uint32_t n_views, const uint32_t* __restrict__ sorted_ids,
-                                                         const uint32_t* __restrict__ offsets, BinArgs a,
+                                                         const uint32_t* __restrict__ offsets,
+                                                         const uint32_t* __restrict__ counts_by_id, BinArgs a,
                                                          uint32_t* __restrict__ keys, uint32_t* __restrict__ payloads,
-                                                         uint64_t cap, uint32_t* __restrict__ err) {
+                                                         uint64_t cap, uint32_t* __restrict__ err, int cull) {
   const uint64_t total = (uint64_t)n_views * stride;
   const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
   int x0 = 0, y0 = 0, x1 = -1, y1 = -1;
   uint32_t id = 0, v = 0, cnt = 0;
   uint64_t off = 0;
+  float4 ra = make_float4(0, 0, 0, 0), rb = ra, rc = ra;
   if (j < total) {
     v = (uint32_t)(j / stride);
     id = sorted_ids[j];
     const size_t o = (size_t)v * stride + id;
-    if (rect_of(rec[3 * o], rec[3 * o + 1], a, x0, y0, x1, y1)) {
-      cnt = (uint32_t)(x1 - x0 + 1) * (uint32_t)(y1 - y0 + 1);
+    cnt = counts_by_id[o];
+    if (cnt) {
+      ra = rec[3 * o]; rb = rec[3 * o + 1]; rc = rec[3 * o + 2];
+      if (!rect_of(ra, rb, a, x0, y0, x1, y1)) cnt = 0;
       off = offsets[j];
     }
   }
@@ -205,8 +215,6 @@ __global__ void __launch_bounds__(256) k_presorted_emit(const float4* __restrict
     atomicOr(err, SC_DEVERR_CAPACITY);
     cnt = 0;
   }
-  // warp-cooperative emission: process the lanes' rectangles one lane at a time,
-  // all 32 lanes writing consecutive pairs of that rectangle
   unsigned pending = __ballot_sync(0xffffffffu, cnt > 0);
   while (pending) {
     const int src = __ffs(pending) - 1;
@@ -214,25 +222,50 @@ __global__ void __launch_bounds__(256) k_presorted_emit(const float4* __restrict
     const uint32_t c = __shfl_sync(0xffffffffu, cnt, src);
     const uint64_t base = __shfl_sync(0xffffffffu, off, src);
     const int rx0 = __shfl_sync(0xffffffffu, x0, src), ry0 = __shfl_sync(0xffffffffu, y0, src);
-    const int rx1 = __shfl_sync(0xffffffffu, x1, src);
+    const int rx1 = __shfl_sync(0xffffffffu, x1, src), ry1 = __shfl_sync(0xffffffffu, y1, src);
     const uint32_t sid = __shfl_sync(0xffffffffu, id, src), sv = __shfl_sync(0xffffffffu, v, src);
+    const float mx = __shfl_sync(0xffffffffu, ra.x, src), my = __shfl_sync(0xffffffffu, ra.y, src);
+    const float ca = __shfl_sync(0xffffffffu, rb.x, src), cb = __shfl_sync(0xffffffffu, rb.y, src);
+    const float cc = __shfl_sync(0xffffffffu, rb.z, src), op = __shfl_sync(0xffffffffu, rc.w, src);
     const uint32_t wdt = (uint32_t)(rx1 - rx0 + 1);
+    const uint32_t rect = wdt * (uint32_t)(ry1 - ry0 + 1);
     const uint32_t vbase = sv * a.num_tiles;
-    for (uint32_t k = lane; k < c; k += 32) {
-      const uint32_t ry = k / wdt, rx = k - ry * wdt;
-      keys[base + k] = vbase + (uint32_t)(ry0 + (int)ry) * a.tiles_x + (uint32_t)(rx0 + (int)rx);
-      payloads[base + k] = sid;
+    uint32_t written = 0;
+    for (uint32_t k0 = 0; k0 < rect && written < c; k0 += 32) {
+      const uint32_t k = k0 + lane;
+      bool ok = k < rect;
+      uint32_t tx = 0, ty = 0;
+      if (ok) {
+        const uint32_t ry = k / wdt, rx = k - ry * wdt;
+        tx = (uint32_t)rx0 + rx;
+        ty = (uint32_t)ry0 + ry;
+        if (cull)
+          ok = tile_reachable(mx, my, ca, cb, cc, op, (float)(tx * a.tw) + 0.5f, (float)((tx + 1) * a.tw) - 0.5f,
+                              (float)(ty * a.th) + 0.5f, (float)((ty + 1) * a.th) - 0.5f);
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, ok);
+      const uint32_t pos = written + __popc(m & lt);
+      if (ok && pos < c) {
+        keys[base + pos] = vbase + ty * a.tiles_x + tx;
+        payloads[base + pos] = sid;
+      }
+      written += __popc(m);
+    }
+    for (uint32_t p = written + lane; p < c; p += 32) {  // count and emission disagreed: pad
+      keys[base + p] = 0xFFFFFFFFu;
+      payloads[base + p] = 0;
     }
   }
 }
 
 sc_status launch_presorted_emit(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
-                                const uint32_t* sorted_ids, const uint32_t* offsets, const sc_tiling* tl,
-                                uint32_t* keys, uint32_t* payloads, uint64_t cap, uint32_t* d_error) {
+                                const uint32_t* sorted_ids, const uint32_t* offsets, const uint32_t* counts_by_id,
+                                const sc_tiling* tl, uint32_t* keys, uint32_t* payloads, uint64_t cap,
+                                uint32_t* d_error, int cull) {
   const uint64_t total = (uint64_t)n_views * stride;
   if (total == 0) return SC_OK;
-  k_presorted_emit<<<(unsigned)sc_div_up(total, 256), 256, 0, ctx->stream>>>(rec, stride, n_views, sorted_ids, offsets,
-                                                                             bin_args(tl), keys, payloads, cap, d_error);
+  k_presorted_emit<<<(unsigned)sc_div_up(total, 256), 256, 0, ctx->stream>>>(
+      rec, stride, n_views, sorted_ids, offsets, counts_by_id, bin_args(tl), keys, payloads, cap, d_error, cull);
   return sc_check_launch(ctx, "k_presorted_emit");
 }
 

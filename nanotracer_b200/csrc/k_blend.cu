@@ -1,21 +1,22 @@
 // k_blend.cu — per-tile alpha blending (forward + adjoint), MSE, tonemap.
 //
-// Forward (rasterize.wgsl:48-118): one CTA per (view, tile), one thread per
-// pixel.  The tile's depth-sorted splat records are staged into shared memory
-// in batches of blockDim records with cp.async (LDGSTS, 3 x 16 B per record),
-// double-buffered so the gather of batch b+1 overlaps the blending of batch b.
-// The CTA leaves as soon as every pixel is saturated (T < 1e-4).  The MSE of
-// loss.rs:163-179 is fused into the epilogue: each pixel writes
-// dL/dC = scale * 2 (C - target) / (3 W H) and its squared error, reduced per
-// CTA in FP64 and added once per CTA.
+// Forward (rasterize.wgsl:48-118): one CTA per (view, tile); each thread owns
+// PPT vertically adjacent pixels (a warp covers a compact tile_w x (32/tile_w*PPT)
+// block).  The tile's depth-sorted records are staged into shared memory in
+// batches of blockDim records with cp.async (3 x 16 B per record), double
+// buffered so the gather of batch b+1 overlaps the blending of batch b, and
+// the CTA leaves as soon as every pixel is saturated (T < 1e-4).  The MSE of
+// loss.rs:163-179 is fused into the epilogue: dL/dC = scale * 2 (C - target)
+// / (3 W H) per pixel, squared errors reduced per CTA in FP64.
 //
 // Backward (rasterize_backward.wgsl:73-210): same grid, reverse walk.  Per
 // (pixel, splat) gradients (dmean.xy, dopacity, dconic.abc, dcolor.rgb) are
-// summed across the warp with shuffles (skipped when no lane contributes),
-// the warp sums are added into a per-batch shared-memory slot, and each
-// batch slot goes to global memory with three float4 vector atomics — one set
-// per (tile, splat) instead of the reference's nine CAS loops per
-// (pixel, splat).
+// summed over the thread's pixels, then over the warp by a 12-shuffle
+// reduce-scatter that leaves the nine totals on nine lanes, which add them to
+// a per-batch shared-memory slot with one atomic instruction; each slot goes
+// to global memory with three float4 vector atomics per (tile, splat) — the
+// reference issues nine CAS loops per (pixel, splat).  The transmittance
+// reconstruction T_i = T_{i+1} / (1 - alpha_i) uses one reciprocal per splat.
 #include "sc_internal.cuh"
 
 namespace sck {
@@ -46,10 +47,11 @@ __device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wai
 
 #define ALPHA_MIN (1.0f / 255.0f)
 #define ALPHA_MAX 0.99f
+#define FULL_MASK 0xffffffffu
 
-// Gaussian weight and alpha of one (pixel, splat); returns false when the
-// reference skips the pair (power > 0 or alpha < 1/255).  Shared by forward
-// and backward so both make identical skip decisions.
+// Gaussian weight and alpha of one (pixel, splat); false when the reference
+// skips the pair (power > 0 or alpha < 1/255).  Shared by forward and backward
+// so both make identical skip decisions.
 __device__ __forceinline__ bool eval_alpha(float dx, float dy, const float4 rb, float op, float& g, float& alpha_raw,
                                            float& alpha) {
   const float power = -0.5f * (rb.x * dx * dx + 2.0f * rb.y * dx * dy + rb.z * dy * dy);
@@ -64,7 +66,7 @@ template <typename T>
 __device__ __forceinline__ T block_sum(T x, T* sred) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(FULL_MASK, x, o);
   if (lane == 0) sred[warp] = x;
   __syncthreads();
   T r = 0;
@@ -73,7 +75,14 @@ __device__ __forceinline__ T block_sum(T x, T* sred) {
   return r;  // valid in thread 0
 }
 
+// Pixel placement: thread t owns column t % tw and rows PPT*(t / tw) + k.
+struct PixelSet {
+  uint32_t px, py0;
+  float fx, fy0;
+};
+
 // ---------------------------------------------------------------- forward
+template <int PPT>
 __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ rec, const uint32_t* __restrict__ payloads,
                                                    const uint2* __restrict__ ranges, BlendArgs a,
                                                    float4* __restrict__ image, uint2* __restrict__ aux,
@@ -87,10 +96,9 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
   const uint32_t vt = blockIdx.x;
   const uint32_t v = vt / a.num_tiles, tile = vt - v * a.num_tiles;
   const uint32_t ty = tile / a.tiles_x, tx = tile - ty * a.tiles_x;
-  const uint32_t lx = threadIdx.x % a.tw, ly = threadIdx.x / a.tw;
-  const uint32_t px = tx * a.tw + lx, py = ty * a.th + ly;
-  const bool inb = px < a.width && py < a.height;
-  const float pxf = (float)px + 0.5f, pyf = (float)py + 0.5f;
+  const uint32_t px = tx * a.tw + threadIdx.x % a.tw;
+  const uint32_t py0 = ty * a.th + PPT * (threadIdx.x / a.tw);
+  const float fx = (float)px + 0.5f;
   const uint2 r = ranges[vt];
   const uint32_t begin = r.x, end = r.y > r.x ? r.y : r.x;
   const uint32_t nb = (end - begin + B - 1) / B;
@@ -108,40 +116,61 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
     cp_async_commit();
   };
 
-  float T = 1.0f, cr = 0.f, cg = 0.f, cb = 0.f;
-  uint32_t last = 0;
-  bool done = !inb;
+  float T[PPT], cr[PPT], cg[PPT], cb[PPT], fy[PPT];
+  uint32_t last[PPT];
+  bool done[PPT];
+  bool all_done = true;
+#pragma unroll
+  for (int k = 0; k < PPT; ++k) {
+    T[k] = 1.0f; cr[k] = cg[k] = cb[k] = 0.f; last[k] = 0;
+    fy[k] = (float)(py0 + k) + 0.5f;
+    done[k] = !(px < a.width && py0 + k < a.height);
+    all_done &= done[k];
+  }
   if (nb > 0) stage(0);
   for (uint32_t b = 0; b < nb; ++b) {
     if (b + 1 < nb) { stage(b + 1); cp_async_wait_one(); } else { cp_async_wait_all(); }
     __syncthreads();
     const uint32_t cnt = min(B, end - (begin + b * B));
-    if (!done) {
+    if (!all_done) {
       const float4* sb = sbuf + (size_t)(b & 1) * 3 * B;
       for (uint32_t k = 0; k < cnt; ++k) {
-        const float4 ra = sb[3 * k], rb = sb[3 * k + 1];
-        float g, araw, alpha;
-        if (!eval_alpha(pxf - ra.x, pyf - ra.y, rb, sb[3 * k + 2].w, g, araw, alpha)) continue;
-        const float4 rc = sb[3 * k + 2];
-        const float ta = T * alpha;
-        cr += ta * rc.x; cg += ta * rc.y; cb += ta * rc.z;
-        T = T * (1.0f - alpha);
-        last = b * B + k + 1;
-        if (T < 1e-4f) { done = true; break; }
+        const float4 ra = sb[3 * k], rb = sb[3 * k + 1], rc = sb[3 * k + 2];
+        const float dx = fx - ra.x;
+        all_done = true;
+#pragma unroll
+        for (int q = 0; q < PPT; ++q) {
+          if (!done[q]) {
+            float g, araw, alpha;
+            if (eval_alpha(dx, fy[q] - ra.y, rb, rc.w, g, araw, alpha)) {
+              const float ta = T[q] * alpha;
+              cr[q] += ta * rc.x; cg[q] += ta * rc.y; cb[q] += ta * rc.z;
+              T[q] = T[q] * (1.0f - alpha);
+              last[q] = b * B + k + 1;
+              if (T[q] < 1e-4f) done[q] = true;
+            }
+          }
+          all_done &= done[q];
+        }
+        if (all_done) break;
       }
     }
-    if (__syncthreads_count(done) == (int)B) break;
+    if (__syncthreads_count(all_done) == (int)B) break;
   }
   cp_async_wait_all();
   double sq = 0.0;
-  if (inb) {
-    const size_t pix = (size_t)v * a.pixels + (size_t)py * a.width + px;
-    image[pix] = make_float4(cr, cg, cb, 1.0f - T);
-    if (aux) aux[pix] = make_uint2(__float_as_uint(T), last);
-    if (target) {
-      const float dx = cr - target[3 * pix], dy = cg - target[3 * pix + 1], dz = cb - target[3 * pix + 2];
-      dl_dc[pix] = make_float4(dx * gscale, dy * gscale, dz * gscale, 0.0f);
-      sq = (double)(dx * dx + dy * dy + dz * dz);
+#pragma unroll
+  for (int q = 0; q < PPT; ++q) {
+    const uint32_t py = py0 + q;
+    if (px < a.width && py < a.height) {
+      const size_t pix = (size_t)v * a.pixels + (size_t)py * a.width + px;
+      image[pix] = make_float4(cr[q], cg[q], cb[q], 1.0f - T[q]);
+      if (aux) aux[pix] = make_uint2(__float_as_uint(T[q]), last[q]);
+      if (target) {
+        const float dx = cr[q] - target[3 * pix], dy = cg[q] - target[3 * pix + 1], dz = cb[q] - target[3 * pix + 2];
+        dl_dc[pix] = make_float4(dx * gscale, dy * gscale, dz * gscale, 0.0f);
+        sq += (double)(dx * dx + dy * dy + dz * dz);
+      }
     }
   }
   if (target && loss) {
@@ -150,20 +179,39 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
   }
 }
 
+template <int PPT>
+static sc_status composite_ppt(sc_ctx* ctx, const BlendArgs& a, uint32_t grid, uint32_t threads, const float4* rec,
+                               const uint32_t* payloads, const uint32_t* ranges, float4* image, uint2* aux,
+                               const float* target, float gscale, float4* dl_dc, double* loss, const uint32_t* d_skip) {
+  const size_t smem = (size_t)2 * 3 * threads * sizeof(float4);
+  k_composite<PPT><<<grid, threads, smem, ctx->stream>>>(rec, payloads, reinterpret_cast<const uint2*>(ranges), a,
+                                                         image, aux, target, gscale, dl_dc, loss, d_skip);
+  return sc_check_launch(ctx, "k_composite");
+}
+
+// pixels per thread: 2 when the tile splits into >= 32 threads that way
+static int pick_ppt(const sc_tiling* tl) {
+  const uint32_t px = tl->tile_w * tl->tile_h;
+  return (tl->tile_h % 2 == 0 && (px / 2) % 32 == 0) ? 2 : 1;
+}
+
 sc_status launch_composite(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views, const uint32_t* payloads,
                            const uint32_t* ranges, const sc_tiling* tl, float4* image, uint2* aux, const float* target,
                            float mse_scale, float4* dl_dc, double* loss, const uint32_t* d_skip) {
   const BlendArgs a = blend_args(tl, stride);
-  const uint32_t threads = tl->tile_w * tl->tile_h;
-  if (threads > 256 || threads % 32 != 0) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile must hold 32..256 pixels, multiple of 32");
+  const uint32_t pixels = tl->tile_w * tl->tile_h;
+  if (pixels > 512 || pixels % 32 != 0) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile must hold 32..512 pixels, multiple of 32");
   const uint64_t grid = (uint64_t)n_views * a.num_tiles;
   if (grid == 0) return SC_OK;
   const float n_scalars = (float)tl->width * (float)tl->height * 3.0f;
   const float gscale = (2.0f / n_scalars) * mse_scale;
-  const size_t smem = (size_t)2 * 3 * threads * sizeof(float4);
-  k_composite<<<(unsigned)grid, threads, smem, ctx->stream>>>(rec, payloads, reinterpret_cast<const uint2*>(ranges), a,
-                                                              image, aux, target, gscale, dl_dc, loss, d_skip);
-  return sc_check_launch(ctx, "k_composite");
+  const int ppt = pick_ppt(tl);
+  if (ppt == 1 && pixels > 256) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile too large for one pixel per thread");
+  if (ppt == 2)
+    return composite_ppt<2>(ctx, a, (uint32_t)grid, pixels / 2, rec, payloads, ranges, image, aux, target, gscale, dl_dc,
+                            loss, d_skip);
+  return composite_ppt<1>(ctx, a, (uint32_t)grid, pixels, rec, payloads, ranges, image, aux, target, gscale, dl_dc, loss,
+                          d_skip);
 }
 
 // ---------------------------------------------------------------- MSE (standalone)
@@ -215,12 +263,52 @@ sc_status launch_mse(sc_ctx* ctx, const float4* pred, const float* target, uint6
 }
 
 // ---------------------------------------------------------------- backward
-__device__ __forceinline__ float warp_sum(float x) {
+// Sums a[0..8] over the warp with 12 shuffles (a reduce-scatter: each level
+// halves the values a lane carries).  Lane 0 ends with the total of a[0],
+// lane 2 with a[1], lanes 4, 8, 12, 16, 20, 24, 28 with a[2..8]; *idx is the
+// value index a lane owns, -1 for the others.
+__device__ __forceinline__ float warp_reduce_scatter9(const float a[9], int lane, int* idx) {
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
+  // xor 16: lanes below 16 keep values 0..4, the others 5..8
+  float x[5];
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-  return x;
+  for (int i = 0; i < 5; ++i) {
+    const float hi = i < 4 ? a[5 + i] : 0.0f;
+    const float send = b4 ? a[i] : hi;
+    const float keep = b4 ? hi : a[i];
+    x[i] = keep + __shfl_xor_sync(FULL_MASK, send, 16);
+  }
+  // xor 8: {0,1,2 | 3,4} and {5,6 | 7,8}
+  const float k0 = b3 ? (b4 ? x[2] : x[3]) : x[0];
+  const float s0 = b3 ? x[0] : (b4 ? x[2] : x[3]);
+  const float k1 = b3 ? (b4 ? x[3] : x[4]) : x[1];
+  const float s1 = b3 ? x[1] : (b4 ? x[3] : x[4]);
+  const float k2 = (!b4 && !b3) ? x[2] : 0.0f;
+  const float s2 = (!b4 && b3) ? x[2] : 0.0f;
+  const float y0 = k0 + __shfl_xor_sync(FULL_MASK, s0, 8);
+  const float y1 = k1 + __shfl_xor_sync(FULL_MASK, s1, 8);
+  const float y2 = k2 + __shfl_xor_sync(FULL_MASK, s2, 8);
+  // xor 4: {0,1 | 2}, {3 | 4}, {5 | 6}, {7 | 8}
+  const bool g00 = !b4 && !b3;
+  const float kz0 = g00 ? (b2 ? y2 : y0) : (b2 ? y1 : y0);
+  const float sz0 = g00 ? (b2 ? y0 : y2) : (b2 ? y0 : y1);
+  const float kz1 = (g00 && !b2) ? y1 : 0.0f;
+  const float sz1 = (g00 && b2) ? y1 : 0.0f;
+  const float z0 = kz0 + __shfl_xor_sync(FULL_MASK, sz0, 4);
+  const float z1 = kz1 + __shfl_xor_sync(FULL_MASK, sz1, 4);
+  // xor 2: {0 | 1}; single values collect on the b1 = 0 lane
+  const bool g000 = g00 && !b2;
+  const float kw = g000 ? (b1 ? z1 : z0) : (b1 ? 0.0f : z0);
+  const float sw = g000 ? (b1 ? z0 : z1) : z0;
+  float w = kw + __shfl_xor_sync(FULL_MASK, sw, 2);
+  // xor 1: full sum of the pair
+  w += __shfl_xor_sync(FULL_MASK, w, 1);
+  const bool owner = !(lane & 1) && (g000 || !b1);
+  *idx = owner ? (g000 ? (b1 ? 1 : 0) : 1 + ((lane >> 2) & 7)) : -1;
+  return w;
 }
 
+template <int PPT>
 __global__ void __launch_bounds__(256) k_composite_backward(const float4* __restrict__ rec,
                                                             const uint32_t* __restrict__ payloads,
                                                             const uint2* __restrict__ ranges, BlendArgs a,
@@ -238,43 +326,53 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
   const uint32_t vt = blockIdx.x;
   const uint32_t v = vt / a.num_tiles, tile = vt - v * a.num_tiles;
   const uint32_t ty = tile / a.tiles_x, tx = tile - ty * a.tiles_x;
-  const uint32_t lx = threadIdx.x % a.tw, ly = threadIdx.x / a.tw;
-  const uint32_t px = tx * a.tw + lx, py = ty * a.th + ly;
-  const bool inb = px < a.width && py < a.height;
-  const float pxf = (float)px + 0.5f, pyf = (float)py + 0.5f;
+  const uint32_t px = tx * a.tw + threadIdx.x % a.tw;
+  const uint32_t py0 = ty * a.th + PPT * (threadIdx.x / a.tw);
+  const float fx = (float)px + 0.5f;
   const uint2 r = ranges[vt];
   const uint32_t begin = r.x, end = r.y > r.x ? r.y : r.x;
   if (end <= begin) return;
   const float4* vrec = rec + (size_t)3 * v * a.stride;
   float4* vgrad = proj_grad + (size_t)3 * v * a.stride;
 
-  float T = 1.0f, gr = 0.f, gg = 0.f, gb = 0.f;
-  uint32_t stop = begin;
-  if (inb) {
-    const size_t pix = (size_t)v * a.pixels + (size_t)py * a.width + px;
-    const float4 d = dl_dc[pix];
-    gr = d.x; gg = d.y; gb = d.z;
-    if (mode == SC_BWD_REF) {
-      T = 1.0f - fwd[pix].w;
-      stop = end;
-    } else {
-      const uint2 x = aux[pix];
-      T = __uint_as_float(x.x);
-      stop = begin + min(x.y, end - begin);
+  float T[PPT], gr[PPT], gg[PPT], gb[PPT], Sr[PPT], Sg[PPT], Sb[PPT], fy[PPT];
+  uint32_t stop[PPT];
+  bool done[PPT];
+  uint32_t tstop = begin;
+  bool all_done = true;
+#pragma unroll
+  for (int q = 0; q < PPT; ++q) {
+    const uint32_t py = py0 + q;
+    fy[q] = (float)py + 0.5f;
+    T[q] = 1.0f; gr[q] = gg[q] = gb[q] = 0.f; Sr[q] = Sg[q] = Sb[q] = 0.f;
+    stop[q] = begin;
+    done[q] = !(px < a.width && py < a.height);
+    if (!done[q]) {
+      const size_t pix = (size_t)v * a.pixels + (size_t)py * a.width + px;
+      const float4 d = dl_dc[pix];
+      gr[q] = d.x; gg[q] = d.y; gb[q] = d.z;
+      if (mode == SC_BWD_REF) {
+        T[q] = 1.0f - fwd[pix].w;
+        stop[q] = end;
+      } else {
+        const uint2 x = aux[pix];
+        T[q] = __uint_as_float(x.x);
+        stop[q] = begin + min(x.y, end - begin);
+      }
+      tstop = max(tstop, stop[q]);
     }
+    all_done &= done[q];
   }
-  bool done = !inb;
   if (threadIdx.x == 0) s_max = begin;
+  sacc[3 * threadIdx.x] = make_float4(0, 0, 0, 0);
+  sacc[3 * threadIdx.x + 1] = make_float4(0, 0, 0, 0);
+  sacc[3 * threadIdx.x + 2] = make_float4(0, 0, 0, 0);
   __syncthreads();
-  if (inb) atomicMax(&s_max, stop);
-  for (uint32_t t = threadIdx.x; t < B; t += B) {
-    sacc[3 * t] = make_float4(0, 0, 0, 0); sacc[3 * t + 1] = make_float4(0, 0, 0, 0); sacc[3 * t + 2] = make_float4(0, 0, 0, 0);
-  }
+  if (tstop > begin) atomicMax(&s_max, tstop);
   __syncthreads();
   const uint32_t hi0 = s_max;
   if (hi0 <= begin) return;
   const uint32_t nb = (hi0 - begin + B - 1) / B;
-  auto lo_of = [&](uint32_t b) -> uint32_t { const uint32_t hi = hi0 - b * B; return hi - min(B, hi - begin); };
   auto stage = [&](uint32_t b) {
     const uint32_t hi = hi0 - b * B, lo = hi - min(B, hi - begin);
     const uint32_t j = lo + threadIdx.x;
@@ -290,59 +388,64 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
     cp_async_commit();
   };
 
-  float Sr = 0.f, Sg = 0.f, Sb = 0.f;
   const int lane = threadIdx.x & 31;
   stage(0);
   for (uint32_t b = 0; b < nb; ++b) {
     if (b + 1 < nb) { stage(b + 1); cp_async_wait_one(); } else { cp_async_wait_all(); }
     __syncthreads();
-    const uint32_t lo = lo_of(b);
-    const uint32_t cnt = (hi0 - b * B) - lo;
+    const uint32_t hi = hi0 - b * B;
+    const uint32_t lo = hi - min(B, hi - begin);
+    const uint32_t cnt = hi - lo;
     const float4* sb = sbuf + (size_t)(b & 1) * 3 * B;
-    if (!__all_sync(0xffffffffu, done)) {
+    if (!__all_sync(FULL_MASK, all_done)) {
       for (int k = (int)cnt - 1; k >= 0; --k) {
         const uint32_t j = lo + (uint32_t)k;
-        float c0 = 0.f, c1 = 0.f, c2 = 0.f, c4 = 0.f, c5 = 0.f, c6 = 0.f, c8 = 0.f, c9 = 0.f, c10 = 0.f;
+        float c[9];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) c[e] = 0.0f;
         bool contrib = false;
-        if (!done && j < stop) {
-          const float4 ra = sb[3 * k], rb = sb[3 * k + 1], rc = sb[3 * k + 2];
-          const float dx = pxf - ra.x, dy = pyf - ra.y;
-          float g, araw, alpha;
-          if (eval_alpha(dx, dy, rb, rc.w, g, araw, alpha)) {
-            const float oma = fmaxf(1.0f - alpha, 1e-4f);
-            T = T / oma;
-            if (mode == SC_BWD_REF && T > 1.0001f) {
-              done = true;
-            } else {
-              const float ta = T * alpha;
-              c8 = gr * ta; c9 = gg * ta; c10 = gb * ta;
-              const float da_r = T * rc.x - Sr / oma, da_g = T * rc.y - Sg / oma, da_b = T * rc.z - Sb / oma;
-              const float galpha = gr * da_r + gg * da_g + gb * da_b;
-              const float gar = araw < ALPHA_MAX ? galpha : 0.0f;
-              c2 = gar * g;
-              const float gpow = gar * rc.w * g;
-              c4 = gpow * -0.5f * (dx * dx);
-              c5 = gpow * -0.5f * (2.0f * dx * dy);
-              c6 = gpow * -0.5f * (dy * dy);
-              c0 = gpow * (rb.x * dx + rb.y * dy);
-              c1 = gpow * (rb.y * dx + rb.z * dy);
-              Sr += ta * rc.x; Sg += ta * rc.y; Sb += ta * rc.z;
-              contrib = true;
+        const float4 ra = sb[3 * k], rb = sb[3 * k + 1], rc = sb[3 * k + 2];
+        const float dx = fx - ra.x;
+        all_done = true;
+#pragma unroll
+        for (int q = 0; q < PPT; ++q) {
+          if (!done[q] && j < stop[q]) {
+            const float dy = fy[q] - ra.y;
+            float g, araw, alpha;
+            if (eval_alpha(dx, dy, rb, rc.w, g, araw, alpha)) {
+              const float oma = fmaxf(1.0f - alpha, 1e-4f);
+              const float inv = __fdividef(1.0f, oma);
+              const float Tn = T[q] * inv;  // T_i = T_{i+1} / (1 - alpha_i)
+              if (mode == SC_BWD_REF && Tn > 1.0001f) {
+                done[q] = true;
+              } else {
+                const float ta = Tn * alpha;
+                c[6] += gr[q] * ta; c[7] += gg[q] * ta; c[8] += gb[q] * ta;
+                // dC/dalpha = T_i c - S / (1 - alpha) = (T_{i+1} c - S) / (1 - alpha)
+                const float galpha = inv * (gr[q] * (T[q] * rc.x - Sr[q]) + gg[q] * (T[q] * rc.y - Sg[q]) +
+                                            gb[q] * (T[q] * rc.z - Sb[q]));
+                const float gar = araw < ALPHA_MAX ? galpha : 0.0f;
+                c[2] += gar * g;
+                const float gpow = gar * rc.w * g;
+                c[3] += gpow * -0.5f * (dx * dx);
+                c[4] += gpow * -(dx * dy);
+                c[5] += gpow * -0.5f * (dy * dy);
+                c[0] += gpow * (rb.x * dx + rb.y * dy);
+                c[1] += gpow * (rb.y * dx + rb.z * dy);
+                Sr[q] += ta * rc.x; Sg[q] += ta * rc.y; Sb[q] += ta * rc.z;
+                T[q] = Tn;
+                contrib = true;
+              }
             }
           }
+          all_done &= done[q] || j <= begin;
         }
-        if (__any_sync(0xffffffffu, contrib)) {
-          c0 = warp_sum(c0); c1 = warp_sum(c1); c2 = warp_sum(c2);
-          c4 = warp_sum(c4); c5 = warp_sum(c5); c6 = warp_sum(c6);
-          c8 = warp_sum(c8); c9 = warp_sum(c9); c10 = warp_sum(c10);
-          if (lane == 0) {
-            float* acc = reinterpret_cast<float*>(sacc + 3 * k);
-            atomicAdd(acc + 0, c0); atomicAdd(acc + 1, c1); atomicAdd(acc + 2, c2);
-            atomicAdd(acc + 4, c4); atomicAdd(acc + 5, c5); atomicAdd(acc + 6, c6);
-            atomicAdd(acc + 8, c8); atomicAdd(acc + 9, c9); atomicAdd(acc + 10, c10);
-          }
+        if (__any_sync(FULL_MASK, contrib)) {
+          int idx;
+          const float w = warp_reduce_scatter9(c, lane, &idx);
+          if (idx >= 0) atomicAdd(reinterpret_cast<float*>(sacc + 3 * k) + idx + idx / 3, w);
         }
-        if (__all_sync(0xffffffffu, done)) break;
+        if (__all_sync(FULL_MASK, all_done)) break;
       }
     }
     __syncthreads();
@@ -356,9 +459,19 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
       if (a2.x != 0.f || a2.y != 0.f || a2.z != 0.f) atomicAdd(dst + 2, a2);
       acc[0] = make_float4(0, 0, 0, 0); acc[1] = acc[0]; acc[2] = acc[0];
     }
-    if (__syncthreads_count(done) == (int)B) break;
+    if (__syncthreads_count(all_done) == (int)B) break;
   }
   cp_async_wait_all();
+}
+
+template <int PPT>
+static sc_status backward_ppt(sc_ctx* ctx, const BlendArgs& a, uint32_t grid, uint32_t threads, const float4* rec,
+                              const uint32_t* payloads, const uint32_t* ranges, const float4* fwd, const float4* dl_dc,
+                              int mode, const uint2* aux, float4* proj_grad, const uint32_t* d_skip) {
+  const size_t smem = (size_t)9 * threads * sizeof(float4) + (size_t)2 * threads * sizeof(uint32_t);
+  k_composite_backward<PPT><<<grid, threads, smem, ctx->stream>>>(
+      rec, payloads, reinterpret_cast<const uint2*>(ranges), a, fwd, dl_dc, mode, aux, proj_grad, d_skip);
+  return sc_check_launch(ctx, "k_composite_backward");
 }
 
 sc_status launch_composite_backward(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
@@ -366,15 +479,18 @@ sc_status launch_composite_backward(sc_ctx* ctx, const float4* rec, uint32_t str
                                     const float4* fwd, const float4* dl_dc, int mode, const uint2* aux,
                                     float4* proj_grad, const uint32_t* d_skip) {
   const BlendArgs a = blend_args(tl, stride);
-  const uint32_t threads = tl->tile_w * tl->tile_h;
-  if (threads > 256 || threads % 32 != 0) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile must hold 32..256 pixels, multiple of 32");
+  const uint32_t pixels = tl->tile_w * tl->tile_h;
+  if (pixels > 512 || pixels % 32 != 0) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile must hold 32..512 pixels, multiple of 32");
   if (mode == SC_BWD_EXACT && !aux) return sc_fail(ctx, SC_ERR_INVALID_ARG, "exact backward needs the forward aux buffer");
   const uint64_t grid = (uint64_t)n_views * a.num_tiles;
   if (grid == 0) return SC_OK;
-  const size_t smem = (size_t)9 * threads * sizeof(float4) + (size_t)2 * threads * sizeof(uint32_t);
-  k_composite_backward<<<(unsigned)grid, threads, smem, ctx->stream>>>(
-      rec, payloads, reinterpret_cast<const uint2*>(ranges), a, fwd, dl_dc, mode, aux, proj_grad, d_skip);
-  return sc_check_launch(ctx, "k_composite_backward");
+  const int ppt = pick_ppt(tl);
+  if (ppt == 1 && pixels > 256) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile too large for one pixel per thread");
+  if (ppt == 2)
+    return backward_ppt<2>(ctx, a, (uint32_t)grid, pixels / 2, rec, payloads, ranges, fwd, dl_dc, mode, aux, proj_grad,
+                           d_skip);
+  return backward_ppt<1>(ctx, a, (uint32_t)grid, pixels, rec, payloads, ranges, fwd, dl_dc, mode, aux, proj_grad,
+                         d_skip);
 }
 
 // ---------------------------------------------------------------- tonemap (tonemap.wgsl:27-41)

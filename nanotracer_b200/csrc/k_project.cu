@@ -157,7 +157,7 @@ __device__ __forceinline__ bool tile_rect(float mx, float my, float r, float vis
   return !(x1 < x0 || y1 < y0);
 }
 
-struct TileArgs { uint32_t tw, th, tiles_x, tiles_y; };
+struct TileArgs { uint32_t tw, th, tiles_x, tiles_y, cull; };
 
 __global__ void __launch_bounds__(128) k_project(DSplats s, const sc_camera* __restrict__ cams, uint32_t n_views,
                                                  uint32_t stride, float4* __restrict__ rec, TileArgs ta,
@@ -211,8 +211,17 @@ __global__ void __launch_bounds__(128) k_project(DSplats s, const sc_camera* __r
           if (depth_keys) {
             int x0, y0, x1, y1;
             if (tile_rect(mx, my, radius, 1.0f, ta.tw, ta.th, ta.tiles_x, ta.tiles_y, x0, y0, x1, y1)) {
-              cnt = (uint32_t)(x1 - x0 + 1) * (uint32_t)(y1 - y0 + 1);
-              key = __float_as_uint(g.tz);
+              if (ta.cull) {
+                for (int ty = y0; ty <= y1; ++ty)
+                  for (int tx = x0; tx <= x1; ++tx)
+                    cnt += tile_reachable(mx, my, g.ca, g.cb, g.cc, opacity, (float)(tx * (int)ta.tw) + 0.5f,
+                                          (float)((tx + 1) * (int)ta.tw) - 0.5f, (float)(ty * (int)ta.th) + 0.5f,
+                                          (float)((ty + 1) * (int)ta.th) - 0.5f)
+                               ? 1u : 0u;
+              } else {
+                cnt = (uint32_t)(x1 - x0 + 1) * (uint32_t)(y1 - y0 + 1);
+              }
+              if (cnt) key = __float_as_uint(g.tz);
             }
           }
         }
@@ -230,11 +239,11 @@ __global__ void __launch_bounds__(128) k_project(DSplats s, const sc_camera* __r
 
 sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams, uint32_t n_views, uint32_t stride,
                          float4* rec, const sc_tiling* tl, uint64_t* depth_keys, uint32_t* ids, uint32_t* counts,
-                         int precise) {
+                         int precise, int cull) {
   if (stride == 0 || n_views == 0) return SC_OK;
-  TileArgs ta{1, 1, 1, 1};
+  TileArgs ta{1, 1, 1, 1, 0};
   if (tl) ta = TileArgs{tl->tile_w, tl->tile_h, (tl->width + tl->tile_w - 1) / tl->tile_w,
-                        (tl->height + tl->tile_h - 1) / tl->tile_h};
+                        (tl->height + tl->tile_h - 1) / tl->tile_h, cull ? 1u : 0u};
   const uint32_t bs = 128;
   k_project<<<(unsigned)sc_div_up(stride, bs), bs, 0, ctx->stream>>>(s, d_cams, n_views, stride, rec, ta, depth_keys,
                                                                      ids, counts, precise);
@@ -380,7 +389,7 @@ __device__ __forceinline__ float adam_one(const DMoments& mo, size_t k, float p,
   return p - lr * mh / (sqrtf(vh) + ap.eps);
 }
 
-__global__ void __launch_bounds__(128) k_fused_backward_adam(DSplats s, DMoments mo, const float4* __restrict__ pg,
+__global__ void __launch_bounds__(128, 4) k_fused_backward_adam(DSplats s, DMoments mo, const float4* __restrict__ pg,
                                                              uint32_t stride, const sc_camera* __restrict__ cams,
                                                              uint32_t n_views, float* __restrict__ grad_acc,
                                                              AdamParams ap, const uint32_t* __restrict__ skip,

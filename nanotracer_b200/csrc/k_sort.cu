@@ -210,7 +210,7 @@ struct RsSmem {
 };
 
 template <typename K>
-__global__ void __launch_bounds__(RS_THREADS) k_rs_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
+__global__ void __launch_bounds__(RS_THREADS, 4) k_rs_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                         K* __restrict__ kout, uint32_t* __restrict__ vout,
                                                         uint64_t n_cap, const uint64_t* __restrict__ d_n, int shift,
                                                         const uint32_t* __restrict__ digit_base,
@@ -327,6 +327,10 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_pass(const K* __restrict__ ki
     const K kk = sm.keys[idx];
     const uint32_t dd = (uint32_t)(kk >> shift) & 0xFFu;
     const long long g = sm.out_base[dd] + (long long)idx;
+    if (g < 0 || (uint64_t)g >= n) {  // only after a look-back gave up: keep the write in bounds
+      atomicOr(err, SC_DEVERR_TIMEOUT);
+      continue;
+    }
     kout[g] = kk;
     vout[g] = sm.vals[idx];
   }

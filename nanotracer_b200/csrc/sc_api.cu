@@ -487,7 +487,7 @@ sc_status sc_project(sc_ctx* ctx, const sc_splats* s, const sc_camera* cams, uin
   sc_camera* d_cams;
   SC_TRY(stage_cams(ctx, cams, n_views, &d_cams));
   sc_status st = sck::launch_project(ctx, dview(s), d_cams, n_views, s->cap, reinterpret_cast<float4*>(projected),
-                                     nullptr, nullptr, nullptr, nullptr, 0);
+                                     nullptr, nullptr, nullptr, nullptr, 0, 0);
   cudaFreeAsync(d_cams, ctx->stream);
   return st;
 }

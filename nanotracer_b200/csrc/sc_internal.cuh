@@ -96,6 +96,43 @@ __device__ __forceinline__ void sp_set(const DSplats& s, int r, uint32_t i, floa
   s.slab[(size_t)r * s.cap + i] = v;
 }
 
+// ---------------------------------------------------------------- tile culling
+// Can any pixel centre of the tile [x0, x1] x [y0, y1] (pixel-centre bounds) reach
+// alpha >= 1/255 for a splat of mean (mx, my), conic (a, b, c), opacity op?
+// alpha = op exp(-q/2) with q the conic's quadratic form, so the pair matters
+// only when min q over the rectangle <= 2 ln(255 op).  The minimum of a
+// positive-definite quadratic over a rectangle is 0 when the mean is inside,
+// otherwise it is attained on an edge, where it is a clamped 1-D minimum.
+// The bound is widened by 1e-3 (relative) + 1e-3 so float rounding in the
+// blend can never accept a pair this test rejects.
+__device__ __forceinline__ float q_form(float a, float b, float c, float u, float w) {
+  return a * u * u + 2.0f * b * u * w + c * w * w;
+}
+__device__ __forceinline__ float edge_min_x(float a, float b, float c, float u, float w0, float w1) {
+  // u fixed, w in [w0, w1]: minimiser w* = -b u / c
+  const float w = fminf(fmaxf(-b * u / c, w0), w1);
+  return q_form(a, b, c, u, w);
+}
+__device__ __forceinline__ float edge_min_y(float a, float b, float c, float w, float u0, float u1) {
+  const float u = fminf(fmaxf(-b * w / a, u0), u1);
+  return q_form(a, b, c, u, w);
+}
+// Not inlined: the projection kernel (which counts) and the emit kernel (which
+// writes) must take the same decision for every tile, so both call one
+// compiled body rather than two separately contracted inline copies.
+static __device__ __noinline__ bool tile_reachable(float mx, float my, float a, float b, float c, float op, float x0,
+                                                   float x1, float y0, float y1) {
+  if (!(op * 255.0f > 1.0f)) return false;
+  const float qmax = 2.0f * __logf(op * 255.0f);
+  const float lim = qmax + 1e-3f * fabsf(qmax) + 1e-3f;
+  if (!(a > 0.0f && c > 0.0f)) return true;  // not positive definite: keep (the blend decides)
+  const float u0 = x0 - mx, u1 = x1 - mx, w0 = y0 - my, w1 = y1 - my;
+  if (u0 <= 0.0f && u1 >= 0.0f && w0 <= 0.0f && w1 >= 0.0f) return true;
+  float m = fminf(edge_min_x(a, b, c, u0, w0, w1), edge_min_x(a, b, c, u1, w0, w1));
+  m = fminf(m, fminf(edge_min_y(a, b, c, w0, u0, u1), edge_min_y(a, b, c, w1, u0, u1)));
+  return m <= lim;
+}
+
 // ---------------------------------------------------------------- host helpers
 sc_status sc_fail(sc_ctx* ctx, sc_status st, const std::string& msg);
 sc_status sc_cuda_fail(sc_ctx* ctx, cudaError_t e, const char* what);
@@ -129,7 +166,7 @@ namespace sck {
 // splat emits no pairs) and the tile count (for the native pipeline).
 sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams, uint32_t n_views,
                          uint32_t stride, float4* rec, const sc_tiling* tiling, uint64_t* depth_keys,
-                         uint32_t* splat_ids, uint32_t* counts, int precise_det);
+                         uint32_t* splat_ids, uint32_t* counts, int precise_det, int cull);
 
 sc_status launch_project_backward(sc_ctx* ctx, const DSplats& s, const float4* proj_grad, const sc_camera* d_cam,
                                   float* grads, uint32_t gcap, int accumulate);
@@ -164,8 +201,9 @@ sc_status launch_tile_ranges(sc_ctx* ctx, const void* keys, int key_mode, const 
 sc_status launch_presorted_counts(sc_ctx* ctx, const uint32_t* counts_by_id, uint32_t stride, uint32_t n_views,
                                   const uint32_t* sorted_ids, uint32_t* counts);
 sc_status launch_presorted_emit(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
-                                const uint32_t* sorted_ids, const uint32_t* offsets, const sc_tiling* tl,
-                                uint32_t* keys, uint32_t* payloads, uint64_t cap, uint32_t* d_error);
+                                const uint32_t* sorted_ids, const uint32_t* offsets, const uint32_t* counts_by_id,
+                                const sc_tiling* tl, uint32_t* keys, uint32_t* payloads, uint64_t cap,
+                                uint32_t* d_error, int cull);
 
 // blending
 sc_status launch_composite(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,

@@ -205,7 +205,7 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->counts + nsp, 0, 4, ctx->stream), "zero count tail");
   mark(tr, 0, capturing);
   SC_TRY(sck::launch_project(ctx, ds, d_cams, V, tr->stride, tr->rec, &tr->cfg.tiling, tr->dkeys, tr->ids,
-                             tr->counts_by_id, 0));
+                             tr->counts_by_id, 0, (int)tr->cfg.tile_cull));
   mark(tr, 1, capturing);
   bool in_tmp = false;
   SC_TRY(sck::radix_sort<uint64_t>(ctx, tr->dkeys, tr->ids, tr->dkeys_tmp, tr->ids_tmp, nsp, 32 + bits_for(V - 1),
@@ -221,12 +221,13 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
     SC_TRY(ensure_pairs(tr, K));
   }
   mark(tr, 3, capturing);
-  SC_TRY(sck::launch_presorted_emit(ctx, tr->rec, tr->stride, V, sorted_ids, tr->counts, &tr->cfg.tiling, tr->keys,
-                                    tr->vals, tr->kcap, ctx->d_error));
+  SC_TRY(sck::launch_presorted_emit(ctx, tr->rec, tr->stride, V, sorted_ids, tr->counts, tr->counts_by_id,
+                                    &tr->cfg.tiling, tr->keys, tr->vals, tr->kcap, ctx->d_error,
+                                    (int)tr->cfg.tile_cull));
   mark(tr, 4, capturing);
   const uint32_t all_tiles = V * tr->T;
   SC_TRY(sck::radix_sort<uint32_t>(ctx, tr->keys, tr->vals, tr->keys_tmp, tr->vals_tmp, tr->kcap,
-                                   std::max(1u, bits_for(all_tiles - 1)), tr->d_total, tr->scratch, tr->scratch_bytes,
+                                   bits_for(all_tiles), tr->d_total, tr->scratch, tr->scratch_bytes,
                                    &in_tmp));
   const uint32_t* skeys = in_tmp ? tr->keys_tmp : tr->keys;
   const uint32_t* svals = in_tmp ? tr->vals_tmp : tr->vals;

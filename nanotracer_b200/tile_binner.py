@@ -49,12 +49,14 @@ class TilingParams:
 
 
 class TileBinningResult:
-    """Device arrays owned by the library's bins object (valid until the next bin())."""
+    """Device arrays owned by the library's bins object (valid until the next bin()).
+    Holds its binner so the arrays outlive a temporary TileBinner(ctx).bin(...)."""
 
-    def __init__(self, ctx: CudaCtx, handle, key_mode: int):
+    def __init__(self, ctx: CudaCtx, handle, key_mode: int, owner=None):
         self.ctx = ctx
         self.handle = handle
         self.key_mode = key_mode
+        self._owner = owner
 
     def _info(self):
         total, nt = C.c_uint64(), C.c_uint32()
@@ -102,7 +104,7 @@ class TileBinner:
         t = params.struct()
         check(lib().sc_bin(self.ctx.handle, projected.cptr, int(n_splats), int(stride if stride is not None else n_splats),
                            int(n_views), C.byref(t), int(key_mode), self.handle), self.ctx.handle)
-        return TileBinningResult(self.ctx, self.handle, key_mode)
+        return TileBinningResult(self.ctx, self.handle, key_mode, owner=self)
 
     def __del__(self):
         try:

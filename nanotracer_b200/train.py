@@ -47,6 +47,7 @@ class TrainConfig:
     use_graph: bool = True
     densify: bool = True
     bf16: bool = False
+    tile_cull: bool = True
 
     def struct(self) -> sc_train_config:
         c = sc_train_config()
@@ -57,6 +58,7 @@ class TrainConfig:
         c.adam = adam_groups(self.lrs, self.beta1, self.beta2, self.eps)
         c.bwd_mode = SC_BWD_EXACT if self.exact_backward else SC_BWD_REF
         c.use_graph = 1 if self.use_graph else 0
+        c.tile_cull = 1 if self.tile_cull else 0
         c.log_scale_min, c.log_scale_max, c.opacity_logit_max = LOG_SCALE_MIN, LOG_SCALE_MAX, OPACITY_LOGIT_MAX
         return c
 

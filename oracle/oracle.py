@@ -129,6 +129,21 @@ class OSplats:
     def n(self):
         return self.h.n
 
+    @property
+    def capacity(self):
+        return len(self.arrays[3])
+
+    def reserve(self, cap):
+        """Grow the backing arrays (the reference's Vecs grow on push)."""
+        if cap <= self.capacity:
+            return
+        n = self.n
+        for k, w in enumerate((3, 4, 3, 1, 3, 45)):
+            buf = np.zeros(cap * w, np.float32)
+            buf[: n * w] = self.arrays[k][: n * w]
+            self.arrays[k] = buf
+        self.h = HostSplats(n, *[C.c_void_p(b.ctypes.data) for b in self.arrays])
+
     def get(self):
         n = self.n
         w = (3, 4, 3, 1, 3, 45)
@@ -265,7 +280,14 @@ def prune(s: OSplats, m: OSplats | None, v: OSplats | None, acc, threshold):
 
 
 def densify(s: OSplats, m, v, acc, grad_count, gthr, sthr, max_splats, it):
+    """acc must hold n + 2 * max(0, max_splats - n) entries: children are
+    appended before their parents are swap-removed (train.rs:486-546)."""
     counts = np.zeros(3, np.uint32)
+    room = s.n + 2 * max(0, int(max_splats) - s.n)
+    for b in (s, m, v):
+        if b is not None:
+            b.reserve(room)
+    assert acc is None or len(acc) >= room, "grad_acc needs room for the transient children"
     n = lib().oracle_densify(C.byref(s.h), C.byref(m.h) if m else None, C.byref(v.h) if v else None, _p(acc),
                              int(grad_count), float(gthr), float(sthr), int(max_splats), int(it), _p(counts))
     if m: m.h.n = n

@@ -184,7 +184,7 @@ def test_densify_matches_oracle_swap_remove_order(ctx, oracle, n, max_splats, it
     c = densify(ctx, g, mo, accb, 1, 2e-4, -2.3, max_splats, it)
     os_ = oracle.OSplats.from_buffer(s, cap)
     om, ov = oracle.OSplats.from_buffer(m, cap), oracle.OSplats.from_buffer(v, cap)
-    oacc = np.zeros(cap, np.float32)
+    oacc = np.zeros(n + 2 * max(0, max_splats - n), np.float32)
     oacc[:n] = acc
     oc = oracle.densify(os_, om, ov, oacc, 1, 2e-4, -2.3, max_splats, it)
     assert c == oc and g.n == os_.n

@@ -55,6 +55,17 @@ def test_trainer_images_equal_reference_order_binning(ctx, tile):
     assert np.array_equal(tr.images(), ref_img)
 
 
+def test_tile_culling_keeps_images_bit_identical_and_cuts_pairs(ctx):
+    """Pairs whose alpha cannot reach 1/255 anywhere in the tile are dropped;
+    the blend would skip them, so images are unchanged bit for bit."""
+    scene, tl, cams, tgt, cfg = _setup(ctx, n=20000, W=256, H=192, V=2)
+    cfg_off = TrainConfig(**{**cfg.__dict__, "tile_cull": False})
+    tr_on, *_ = _run(ctx, scene, cams, tgt, cfg)
+    tr_off, *_ = _run(ctx, scene, cams, tgt, cfg_off)
+    assert np.array_equal(tr_on.images(), tr_off.images())
+    assert tr_on.stats()["pairs"] < 0.95 * tr_off.stats()["pairs"]
+
+
 @pytest.mark.parametrize("exact", [True, False])
 def test_trainer_step_matches_oracle_iteration(ctx, oracle, exact):
     scene, tl, cams, tgt, cfg = _setup(ctx, n=1500, W=96, H=64, V=2, exact=exact)

@@ -197,7 +197,7 @@ def _densify_kat_buffers(oracle, k):
 def test_densify_clones_small_and_splits_large(oracle):
     k = KATS["densify_clones_small_and_splits_large"]
     s, m, v = _densify_kat_buffers(oracle, k)
-    acc = np.zeros(16, np.float32)
+    acc = np.zeros(3 + 2 * k["max_splats"], np.float32)
     acc[:3] = k["grad_acc"]
     c = oracle.densify(s, m, v, acc, k["grad_count"], k["threshold"], k["split_thr"], k["max_splats"], k["iter"])
     ex = k["expect"]
