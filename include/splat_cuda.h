@@ -222,6 +222,23 @@ sc_status sc_radix_sort_u64(sc_ctx* ctx, uint64_t* keys, uint32_t* vals, uint64_
  * total (device pointer, may be NULL) receives the sum.  PrefixScan::scan,
  * prefix_scan.rs:127-186 (limited to 2^24 elements there). */
 sc_status sc_exclusive_scan_u32(sc_ctx* ctx, uint32_t* data, uint64_t n, uint64_t* total);
+/* The same scan for callers that cannot allocate device memory: a host engine
+ * that owns every device allocation through its own pool and forbids hidden
+ * library allocations, or code on a latency-critical path where cudaMalloc's
+ * implicit device synchronisation is not acceptable.  No counterpart in the
+ * reference (its PrefixScan allocates its block sums per call,
+ * prefix_scan.rs:127-186).
+ * Its look-back scratch is a fixed file-scope device array of 128 KiB + 256 B
+ * that every GPU loading the library holds until the process exits; n above
+ * SC_NOALLOC_SCAN_MAX_N returns SC_ERR_INVALID_ARG without touching data.
+ * The first call on a device looks the array's device address up (no
+ * allocation); make that first call before any stream capture.  All calls
+ * share the array, which keeps the last call's contents (each call clears the
+ * part it uses), so calls that overlap on the GPU — on different streams or
+ * contexts of the same device — race and must be serialised by the caller.
+ * It calls no cudaMalloc, cudaFree or allocating library routine. */
+#define SC_NOALLOC_SCAN_MAX_N (1ull << 26)
+sc_status sc_exclusive_scan_u32_noalloc(sc_ctx* ctx, uint32_t* data, uint64_t n, uint64_t* total);
 
 /* rasterize.wgsl:48-118 over n_views views; image is n_views*W*H float4
  * (rgb, 1-T).  aux (nullable) receives per pixel {T_final bits, last

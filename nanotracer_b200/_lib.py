@@ -112,6 +112,7 @@ _PROTOS = {
     "sc_radix_sort_u32": (ST, [P, P, P, P, P, U64, U32]),
     "sc_radix_sort_u64": (ST, [P, P, P, P, P, U64, U32]),
     "sc_exclusive_scan_u32": (ST, [P, P, U64, P]),
+    "sc_exclusive_scan_u32_noalloc": (ST, [P, P, U64, P]),
     "sc_composite": (ST, [P, P, U32, U32, P, C.POINTER(sc_tiling), P, P]),
     "sc_mse_loss_grad": (ST, [P, P, P, U32, C.POINTER(sc_tiling), F32, P, P]),
     "sc_composite_backward": (ST, [P, P, U32, U32, P, C.POINTER(sc_tiling), P, P, I32, P, P]),

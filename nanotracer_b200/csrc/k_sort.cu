@@ -148,6 +148,67 @@ sc_status scan_u32(sc_ctx* ctx, uint32_t* data, uint64_t n, uint64_t* d_total, v
   return sc_check_launch(ctx, "k_scan");
 }
 
+// ---------------------------------------------------------------- allocation-free scan
+// Scratch of sc_exclusive_scan_u32_noalloc: a 256-byte ticket area followed by
+// one 8-byte look-back status word per 4096-element tile, for at most
+// SC_NOALLOC_SCAN_MAX_N elements (128 KiB + 256 B).  It is a file-scope device
+// array, so every GPU that loads this library holds it until the process
+// exits, and every call shares it.
+static __device__ __align__(256) unsigned char g_noalloc_scan_scratch[256 + (SC_NOALLOC_SCAN_MAX_N / SCAN_TILE) * 8];
+
+static_assert(SC_NOALLOC_SCAN_MAX_N % SCAN_TILE == 0, "maximum must be a whole number of scan tiles");
+
+}  // namespace sck
+
+#include <mutex>
+
+namespace {
+// Device address of the scratch array, per device.  Host code cannot use the
+// array's name as a device pointer: it is a host-side stand-in.
+constexpr int kMaxDevices = 64;
+void* g_noalloc_ptr[kMaxDevices] = {};
+std::mutex g_noalloc_mu;
+}  // namespace
+
+extern "C" sc_status sc_exclusive_scan_u32_noalloc(sc_ctx* ctx, uint32_t* data, uint64_t n, uint64_t* total) {
+  if (!ctx || (n && !data)) return SC_ERR_INVALID_ARG;
+  if (n > SC_NOALLOC_SCAN_MAX_N)
+    return sc_fail(ctx, SC_ERR_INVALID_ARG,
+                   "sc_exclusive_scan_u32_noalloc: n exceeds SC_NOALLOC_SCAN_MAX_N (67108864 elements)");
+  if (ctx->device < 0 || ctx->device >= kMaxDevices) return SC_ERR_INVALID_ARG;
+  void* scratch = nullptr;
+  {
+    // one-time set-up per device, with that device current: look up the
+    // array's device address (a query, not an allocation)
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    scratch = g_noalloc_ptr[ctx->device];
+    if (!scratch) {
+      int cur = -1;
+      SC_CUDA_TRY(ctx, cudaGetDevice(&cur), "get device");
+      if (cur != ctx->device) SC_CUDA_TRY(ctx, cudaSetDevice(ctx->device), "set device");
+      const cudaError_t e = cudaGetSymbolAddress(&scratch, sck::g_noalloc_scan_scratch);
+      if (cur != ctx->device) cudaSetDevice(cur);
+      if (e != cudaSuccess || !scratch) return sc_cuda_fail(ctx, e != cudaSuccess ? e : cudaErrorInvalidSymbol,
+                                                           "scratch symbol address");
+      g_noalloc_ptr[ctx->device] = scratch;
+    }
+  }
+  if (n == 0) {
+    if (total) SC_CUDA_TRY(ctx, cudaMemsetAsync(total, 0, 8, ctx->stream), "memset total");
+    return SC_OK;
+  }
+  const uint64_t tiles = sc_div_up(n, SCAN_TILE);
+  // the ticket and the look-back flags of this call's tiles must start at zero
+  // (the array keeps the previous call's contents)
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(scratch, 0, 256 + tiles * 8, ctx->stream), "clear scan scratch");
+  unsigned* ticket = reinterpret_cast<unsigned*>(scratch);
+  unsigned long long* status = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(scratch) + 256);
+  sck::k_scan<<<(unsigned)tiles, SCAN_THREADS, 0, ctx->stream>>>(data, n, status, ticket, total, ctx->d_error);
+  return sc_check_launch(ctx, "k_scan");
+}
+
+namespace sck {
+
 // ---------------------------------------------------------------- onesweep radix sort
 #define RS_THREADS 256
 #define RS_WARPS (RS_THREADS / 32)
