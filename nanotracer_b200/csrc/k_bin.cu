@@ -230,6 +230,8 @@ __global__ void __launch_bounds__(256) k_presorted_emit(const float4* __restrict
     const uint32_t wdt = (uint32_t)(rx1 - rx0 + 1);
     const uint32_t rect = wdt * (uint32_t)(ry1 - ry0 + 1);
     const uint32_t vbase = sv * a.num_tiles;
+    const CullShape cs = cull_shape(mx, my, ca, cb, cc, op);
+    const bool test = cull && !cs.keep;
     uint32_t written = 0;
     for (uint32_t k0 = 0; k0 < rect && written < c; k0 += 32) {
       const uint32_t k = k0 + lane;
@@ -239,9 +241,10 @@ __global__ void __launch_bounds__(256) k_presorted_emit(const float4* __restrict
         const uint32_t ry = k / wdt, rx = k - ry * wdt;
         tx = (uint32_t)rx0 + rx;
         ty = (uint32_t)ry0 + ry;
-        if (cull)
-          ok = tile_reachable(mx, my, ca, cb, cc, op, (float)(tx * a.tw) + 0.5f, (float)((tx + 1) * a.tw) - 0.5f,
-                              (float)(ty * a.th) + 0.5f, (float)((ty + 1) * a.th) - 0.5f);
+        if (test) {  // the row span the projection counted with
+          int lo, hi;
+          ok = cs.any && cull_row_span(cs, (int)ty, a.tw, a.th, lo, hi) && (int)tx >= lo && (int)tx <= hi;
+        }
       }
       const unsigned m = __ballot_sync(0xffffffffu, ok);
       const uint32_t pos = written + __popc(m & lt);

@@ -212,12 +212,18 @@ __global__ void __launch_bounds__(128) k_project(DSplats s, const sc_camera* __r
             int x0, y0, x1, y1;
             if (tile_rect(mx, my, radius, 1.0f, ta.tw, ta.th, ta.tiles_x, ta.tiles_y, x0, y0, x1, y1)) {
               if (ta.cull) {
-                for (int ty = y0; ty <= y1; ++ty)
-                  for (int tx = x0; tx <= x1; ++tx)
-                    cnt += tile_reachable(mx, my, g.ca, g.cb, g.cc, opacity, (float)(tx * (int)ta.tw) + 0.5f,
-                                          (float)((tx + 1) * (int)ta.tw) - 0.5f, (float)(ty * (int)ta.th) + 0.5f,
-                                          (float)((ty + 1) * (int)ta.th) - 0.5f)
-                               ? 1u : 0u;
+                const CullShape cs = cull_shape(mx, my, g.ca, g.cb, g.cc, opacity);
+                if (cs.keep) {
+                  cnt = (uint32_t)(x1 - x0 + 1) * (uint32_t)(y1 - y0 + 1);
+                } else if (cs.any) {
+                  for (int ty = y0; ty <= y1; ++ty) {
+                    int lo, hi;
+                    if (!cull_row_span(cs, ty, ta.tw, ta.th, lo, hi)) continue;
+                    lo = max(lo, x0);
+                    hi = min(hi, x1);
+                    if (hi >= lo) cnt += (uint32_t)(hi - lo + 1);
+                  }
+                }
               } else {
                 cnt = (uint32_t)(x1 - x0 + 1) * (uint32_t)(y1 - y0 + 1);
               }

@@ -97,40 +97,54 @@ __device__ __forceinline__ void sp_set(const DSplats& s, int r, uint32_t i, floa
 }
 
 // ---------------------------------------------------------------- tile culling
-// Can any pixel centre of the tile [x0, x1] x [y0, y1] (pixel-centre bounds) reach
-// alpha >= 1/255 for a splat of mean (mx, my), conic (a, b, c), opacity op?
-// alpha = op exp(-q/2) with q the conic's quadratic form, so the pair matters
-// only when min q over the rectangle <= 2 ln(255 op).  The minimum of a
-// positive-definite quadratic over a rectangle is 0 when the mean is inside,
-// otherwise it is attained on an edge, where it is a clamped 1-D minimum.
-// The bound is widened by 1e-3 (relative) + 1e-3 so float rounding in the
-// blend can never accept a pair this test rejects.
-__device__ __forceinline__ float q_form(float a, float b, float c, float u, float w) {
-  return a * u * u + 2.0f * b * u * w + c * w * w;
+// A pixel reaches alpha = op exp(-q/2) >= 1/255 only inside the ellipse
+// q(u, w) = a u^2 + 2 b u w + c w^2 <= L, L = 2 ln(255 op) (u, w: offsets from
+// the mean, (a, b, c) the conic).  For a tile row (pixel-centre band
+// w in [w0, w1]) the ellipse covers u in [u_min(w), u_max(w)] with
+// u_max(w) = (-b w + sqrt(L a - det w^2)) / a concave and u_min convex, so
+// their extremes over the band sit at the clamped extreme points of the
+// ellipse (w = -/+ b xh / c, xh the half-width).  A tile whose pixel centres
+// miss that interval holds no pixel the blend would accept, so the pair can be
+// dropped without changing any image.  L is widened by 1e-3 relative + 1e-3
+// and the interval by 1e-3 px, so float rounding in the blend can never
+// accept a pixel this test rejects.
+struct CullShape {
+  float mx, my, a, b, det, L, xh, yh, kx, inv_a;
+  bool any;   // op > 1/255 and the conic is positive definite
+  bool keep;  // not positive definite: keep the reference rectangle whole
+};
+
+__device__ __forceinline__ CullShape cull_shape(float mx, float my, float a, float b, float c, float op) {
+  CullShape s;
+  s.mx = mx; s.my = my; s.a = a; s.b = b;
+  s.det = a * c - b * b;
+  s.keep = !(a > 0.0f && c > 0.0f && s.det > 0.0f);
+  s.any = op * 255.0f > 1.0f;
+  const float q = 2.0f * __logf(fmaxf(op * 255.0f, 1.0f));
+  s.L = q + 1e-3f * q + 1e-3f;
+  s.xh = sqrtf(s.L * c / s.det);
+  s.yh = sqrtf(s.L * a / s.det);
+  s.kx = b * s.xh / c;
+  s.inv_a = 1.0f / a;
+  return s;
 }
-__device__ __forceinline__ float edge_min_x(float a, float b, float c, float u, float w0, float w1) {
-  // u fixed, w in [w0, w1]: minimiser w* = -b u / c
-  const float w = fminf(fmaxf(-b * u / c, w0), w1);
-  return q_form(a, b, c, u, w);
-}
-__device__ __forceinline__ float edge_min_y(float a, float b, float c, float w, float u0, float u1) {
-  const float u = fminf(fmaxf(-b * w / a, u0), u1);
-  return q_form(a, b, c, u, w);
-}
-// Not inlined: the projection kernel (which counts) and the emit kernel (which
-// writes) must take the same decision for every tile, so both call one
-// compiled body rather than two separately contracted inline copies.
-static __device__ __noinline__ bool tile_reachable(float mx, float my, float a, float b, float c, float op, float x0,
-                                                   float x1, float y0, float y1) {
-  if (!(op * 255.0f > 1.0f)) return false;
-  const float qmax = 2.0f * __logf(op * 255.0f);
-  const float lim = qmax + 1e-3f * fabsf(qmax) + 1e-3f;
-  if (!(a > 0.0f && c > 0.0f)) return true;  // not positive definite: keep (the blend decides)
-  const float u0 = x0 - mx, u1 = x1 - mx, w0 = y0 - my, w1 = y1 - my;
-  if (u0 <= 0.0f && u1 >= 0.0f && w0 <= 0.0f && w1 >= 0.0f) return true;
-  float m = fminf(edge_min_x(a, b, c, u0, w0, w1), edge_min_x(a, b, c, u1, w0, w1));
-  m = fminf(m, fminf(edge_min_y(a, b, c, w0, u0, u1), edge_min_y(a, b, c, w1, u0, u1)));
-  return m <= lim;
+
+// Tiles [tlo, thi] of row ty (tile width tw, height th) that the ellipse can
+// reach; false when the row misses it.  Caller clamps to the 3-sigma rectangle.
+__device__ __forceinline__ bool cull_row_span(const CullShape& s, int ty, uint32_t tw, uint32_t th, int& tlo,
+                                              int& thi) {
+  const float w0 = (float)(ty * (int)th) + 0.5f - s.my, w1 = (float)((ty + 1) * (int)th) - 0.5f - s.my;
+  if (w1 < -s.yh || w0 > s.yh) return false;
+  const float a0 = fmaxf(w0, -s.yh), a1 = fminf(w1, s.yh);
+  const float wr = fminf(fmaxf(-s.kx, a0), a1), wl = fminf(fmaxf(s.kx, a0), a1);
+  const float ur = (-s.b * wr + sqrtf(fmaxf(s.L * s.a - wr * wr * s.det, 0.0f))) * s.inv_a;
+  const float ul = (-s.b * wl - sqrtf(fmaxf(s.L * s.a - wl * wl * s.det, 0.0f))) * s.inv_a;
+  const float X0 = s.mx + ul - 1e-3f, X1 = s.mx + ur + 1e-3f;
+  // tile tx's pixel centres span [tx*tw + 0.5, (tx+1)*tw - 0.5]
+  const float ftw = (float)tw;
+  tlo = (int)ceilf((X0 + 0.5f) / ftw - 1.0f);
+  thi = (int)floorf((X1 - 0.5f) / ftw);
+  return thi >= tlo;
 }
 
 // ---------------------------------------------------------------- host helpers
