@@ -178,14 +178,12 @@ sc_status launch_presorted_counts(sc_ctx* ctx, const uint32_t* counts_by_id, uin
   return sc_check_launch(ctx, "k_presorted_counts");
 }
 
-// One warp emits the pairs of 32 consecutive depth-ranked splats: the lanes
-// walk the tile rectangle of one splat at a time, 32 tiles per step, so long
-// rectangles do not serialise a single thread.  With culling, lanes test their
-// tiles with tile_reachable (the function the projection counted with) and
-// compact the survivors with a ballot.  Exactly `count` pairs are written per
-// splat; should a decision ever differ from the count, surplus tiles are
-// dropped and missing slots get an out-of-range key that sorts last and that
-// the range kernel ignores.
+// One thread emits the pairs of one depth-ranked splat, row by row.  With
+// culling, each row keeps the span of tiles that cull_row_span returns — the
+// function the projection counted with — clamped to the 3-sigma rectangle.
+// Exactly `count` pairs are written per splat; should a row span ever differ
+// from the count, surplus tiles are dropped and missing slots get an
+// out-of-range key that sorts last and that the range kernel ignores.
 __global__ void __launch_bounds__(256) k_presorted_emit(const float4* __restrict__ rec, uint32_t stride,
                                                          uint32_t n_views, const uint32_t* __restrict__ sorted_ids,
                                                          const uint32_t* __restrict__ offsets,
@@ -194,70 +192,42 @@ __global__ void __launch_bounds__(256) k_presorted_emit(const float4* __restrict
                                                          uint64_t cap, uint32_t* __restrict__ err, int cull) {
   const uint64_t total = (uint64_t)n_views * stride;
   const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int lane = threadIdx.x & 31;
-  const unsigned lt = (1u << lane) - 1u;
-  int x0 = 0, y0 = 0, x1 = -1, y1 = -1;
-  uint32_t id = 0, v = 0, cnt = 0;
-  uint64_t off = 0;
-  float4 ra = make_float4(0, 0, 0, 0), rb = ra, rc = ra;
-  if (j < total) {
-    v = (uint32_t)(j / stride);
-    id = sorted_ids[j];
-    const size_t o = (size_t)v * stride + id;
-    cnt = counts_by_id[o];
-    if (cnt) {
-      ra = rec[3 * o]; rb = rec[3 * o + 1]; rc = rec[3 * o + 2];
-      if (!rect_of(ra, rb, a, x0, y0, x1, y1)) cnt = 0;
-      off = offsets[j];
-    }
-  }
-  if (cnt && off + cnt > cap) {
+  if (j >= total) return;
+  const uint32_t v = (uint32_t)(j / stride);
+  const uint32_t id = sorted_ids[j];
+  const size_t o = (size_t)v * stride + id;
+  const uint32_t cnt = counts_by_id[o];
+  if (!cnt) return;
+  const float4 ra = rec[3 * o], rb = rec[3 * o + 1], rc = rec[3 * o + 2];
+  int x0, y0, x1, y1;
+  if (!rect_of(ra, rb, a, x0, y0, x1, y1)) return;
+  const uint64_t off = offsets[j];
+  if (off + cnt > cap) {
     atomicOr(err, SC_DEVERR_CAPACITY);
-    cnt = 0;
+    return;
   }
-  unsigned pending = __ballot_sync(0xffffffffu, cnt > 0);
-  while (pending) {
-    const int src = __ffs(pending) - 1;
-    pending &= pending - 1;
-    const uint32_t c = __shfl_sync(0xffffffffu, cnt, src);
-    const uint64_t base = __shfl_sync(0xffffffffu, off, src);
-    const int rx0 = __shfl_sync(0xffffffffu, x0, src), ry0 = __shfl_sync(0xffffffffu, y0, src);
-    const int rx1 = __shfl_sync(0xffffffffu, x1, src), ry1 = __shfl_sync(0xffffffffu, y1, src);
-    const uint32_t sid = __shfl_sync(0xffffffffu, id, src), sv = __shfl_sync(0xffffffffu, v, src);
-    const float mx = __shfl_sync(0xffffffffu, ra.x, src), my = __shfl_sync(0xffffffffu, ra.y, src);
-    const float ca = __shfl_sync(0xffffffffu, rb.x, src), cb = __shfl_sync(0xffffffffu, rb.y, src);
-    const float cc = __shfl_sync(0xffffffffu, rb.z, src), op = __shfl_sync(0xffffffffu, rc.w, src);
-    const uint32_t wdt = (uint32_t)(rx1 - rx0 + 1);
-    const uint32_t rect = wdt * (uint32_t)(ry1 - ry0 + 1);
-    const uint32_t vbase = sv * a.num_tiles;
-    const CullShape cs = cull_shape(mx, my, ca, cb, cc, op);
-    const bool test = cull && !cs.keep;
-    uint32_t written = 0;
-    for (uint32_t k0 = 0; k0 < rect && written < c; k0 += 32) {
-      const uint32_t k = k0 + lane;
-      bool ok = k < rect;
-      uint32_t tx = 0, ty = 0;
-      if (ok) {
-        const uint32_t ry = k / wdt, rx = k - ry * wdt;
-        tx = (uint32_t)rx0 + rx;
-        ty = (uint32_t)ry0 + ry;
-        if (test) {  // the row span the projection counted with
-          int lo, hi;
-          ok = cs.any && cull_row_span(cs, (int)ty, a.tw, a.th, lo, hi) && (int)tx >= lo && (int)tx <= hi;
-        }
-      }
-      const unsigned m = __ballot_sync(0xffffffffu, ok);
-      const uint32_t pos = written + __popc(m & lt);
-      if (ok && pos < c) {
-        keys[base + pos] = vbase + ty * a.tiles_x + tx;
-        payloads[base + pos] = sid;
-      }
-      written += __popc(m);
+  uint32_t* kp = keys + off;
+  uint32_t* pp = payloads + off;
+  const uint32_t vbase = v * a.num_tiles;
+  uint32_t w = 0;
+  const CullShape cs = cull_shape(ra.x, ra.y, rb.x, rb.y, rb.z, rc.w);
+  const bool test = cull && !cs.keep;
+  for (int ty = y0; ty <= y1; ++ty) {
+    int lo = x0, hi = x1;
+    if (test) {
+      if (!cs.any || !cull_row_span(cs, ty, a.tw, a.th, lo, hi)) continue;
+      lo = max(lo, x0);
+      hi = min(hi, x1);
     }
-    for (uint32_t p = written + lane; p < c; p += 32) {  // count and emission disagreed: pad
-      keys[base + p] = 0xFFFFFFFFu;
-      payloads[base + p] = 0;
+    const uint32_t row = vbase + (uint32_t)ty * a.tiles_x;
+    for (int tx = lo; tx <= hi && w < cnt; ++tx, ++w) {
+      kp[w] = row + (uint32_t)tx;
+      pp[w] = id;
     }
+  }
+  for (; w < cnt; ++w) {  // count and emission disagreed: pad
+    kp[w] = 0xFFFFFFFFu;
+    pp[w] = 0;
   }
 }
 

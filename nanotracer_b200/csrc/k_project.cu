@@ -159,7 +159,7 @@ __device__ __forceinline__ bool tile_rect(float mx, float my, float r, float vis
 
 struct TileArgs { uint32_t tw, th, tiles_x, tiles_y, cull; };
 
-__global__ void __launch_bounds__(128) k_project(DSplats s, const sc_camera* __restrict__ cams, uint32_t n_views,
+__global__ void __launch_bounds__(128, 4) k_project(DSplats s, const sc_camera* __restrict__ cams, uint32_t n_views,
                                                  uint32_t stride, float4* __restrict__ rec, TileArgs ta,
                                                  uint64_t* __restrict__ depth_keys, uint32_t* __restrict__ ids,
                                                  uint32_t* __restrict__ counts, int precise) {

@@ -6,8 +6,8 @@
 // dispatches per sort).  Here one sort is one histogram kernel plus one kernel
 // per 8-bit digit.  Both are stable and deterministic: tiles take their
 // position from an atomic ticket, rank their items warp-by-warp in input
-// order (match.any), and obtain the running digit offsets from their
-// predecessors' published aggregates.
+// order (ballot-based peer masks), and obtain the running digit offsets from
+// their predecessors' published aggregates.
 //
 // Every look-back wait is bounded: after SC_SPIN_LIMIT polls the block sets
 // SC_DEVERR_TIMEOUT in the context's error word and proceeds with what it has
@@ -262,14 +262,33 @@ template <typename K>
 struct RsSmem {
   static constexpr int IPT = RsCfg<K>::IPT;
   static constexpr int TILE = RS_THREADS * IPT;
-  K keys[TILE];
-  uint32_t vals[TILE];
+  K keys[TILE];                       // keys in digit order (scatter staging)
+  uint32_t vals[TILE];                // payloads in input (warp-striped) order, prefetched with cp.async
+  uint16_t src[TILE];                 // digit-order slot -> input slot of its payload
   uint32_t warp_hist[RS_WARPS][RS_RADIX];
   uint32_t tile_excl[RS_RADIX];
-  long long out_base[RS_RADIX];
+  int out_base[RS_RADIX];             // global position of digit d's first slot, minus its tile offset
   uint32_t tile_id;
 };
 
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_u32(unsigned* p, unsigned v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// One onesweep pass.  Ranking: the lanes of a warp holding the same digit are
+// found with 8 ballots (one per digit bit), a fixed cost independent of how
+// many distinct digits the warp holds; lanes are ranked in input order, so the
+// pass is stable.  Look-back status words carry their own value (flag in the
+// top 2 bits, count below), so relaxed loads and stores suffice.
 template <typename K>
 __global__ void __launch_bounds__(RS_THREADS, 4) k_rs_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                         K* __restrict__ kout, uint32_t* __restrict__ vout,
@@ -289,27 +308,39 @@ __global__ void __launch_bounds__(RS_THREADS, 4) k_rs_pass(const K* __restrict__
   const uint64_t n = d_n ? min(*d_n, n_cap) : n_cap;
   const uint64_t tbase = (uint64_t)tile * TILE;
   if (tbase >= n) return;  // every later ticket is beyond n as well: nobody waits on this tile
-  // warp-striped load: item k of lane l in warp w is tbase + w*32*IPT + k*32 + l
-  const uint64_t wbase = tbase + (uint64_t)warp * 32 * IPT;
-  K key[IPT];
-  uint32_t rank[IPT];
-  uint32_t dig[IPT];
+  // warp-striped layout: item k of lane l in warp w is input slot w*32*IPT + k*32 + l
+  const uint32_t wslot = (uint32_t)warp * 32 * IPT;
+  const uint64_t wbase = tbase + wslot;
 #pragma unroll
   for (int k = 0; k < IPT; ++k) {
     const uint64_t i = wbase + (uint64_t)k * 32 + lane;
-    const bool valid = i < n;
-    key[k] = valid ? kin[i] : (K)0;
-    dig[k] = valid ? (uint32_t)(key[k] >> shift) & 0xFFu : 256u;
+    if (i < n) cp_async4(&sm.vals[wslot + k * 32 + lane], vin + i);
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  K key[IPT];
+  uint32_t rank[IPT];
+#pragma unroll
+  for (int k = 0; k < IPT; ++k) {
+    const uint64_t i = wbase + (uint64_t)k * 32 + lane;
+    key[k] = i < n ? kin[i] : (K)0;
   }
   const unsigned lt = lanemask_lt();
 #pragma unroll
   for (int k = 0; k < IPT; ++k) {
-    const unsigned peers = __match_any_sync(0xffffffffu, dig[k]);
-    const int leader = 31 - __clz(peers);
+    const bool valid = wbase + (uint64_t)k * 32 + lane < n;
+    const uint32_t d = (uint32_t)(key[k] >> shift) & 0xFFu;
+    unsigned peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const bool bit = (d >> b) & 1u;
+      const unsigned m = __ballot_sync(0xffffffffu, bit);
+      peers &= bit ? m : ~m;
+    }
+    const int leader = valid ? 31 - __clz(peers) : lane;
     uint32_t old = 0;
-    if (lane == leader && dig[k] < 256u) {
-      old = sm.warp_hist[warp][dig[k]];
-      sm.warp_hist[warp][dig[k]] = old + __popc(peers);
+    if (valid && lane == leader) {
+      old = sm.warp_hist[warp][d];
+      sm.warp_hist[warp][d] = old + __popc(peers);
     }
     old = __shfl_sync(0xffffffffu, old, leader);
     rank[k] = old + __popc(peers & lt);
@@ -327,13 +358,13 @@ __global__ void __launch_bounds__(RS_THREADS, 4) k_rs_pass(const K* __restrict__
   }
   // publish this tile's count, then look back for the running prefix
   unsigned* lb = lookback + (size_t)tile * RS_RADIX;
-  st_release_u32(&lb[d], (tile == 0 ? RS_FLAG_PRE : RS_FLAG_AGG) | cnt);
+  st_relaxed_u32(&lb[d], (tile == 0 ? RS_FLAG_PRE : RS_FLAG_AGG) | cnt);
   uint32_t excl = 0;
   if (tile > 0) {
     long long pred = (long long)tile - 1;
     unsigned spins = 0;
     while (pred >= 0) {
-      const unsigned st = ld_acquire_u32(&lookback[(size_t)pred * RS_RADIX + d]);
+      const unsigned st = ld_relaxed_u32(&lookback[(size_t)pred * RS_RADIX + d]);
       const unsigned flag = st & ~RS_VAL_MASK;
       if (flag == 0u) {
         if (++spins > SC_SPIN_LIMIT) { atomicOr(err, SC_DEVERR_TIMEOUT); break; }
@@ -344,7 +375,7 @@ __global__ void __launch_bounds__(RS_THREADS, 4) k_rs_pass(const K* __restrict__
       if (flag == RS_FLAG_PRE) break;
       --pred;
     }
-    st_release_u32(&lb[d], RS_FLAG_PRE | ((excl + cnt) & RS_VAL_MASK));
+    st_relaxed_u32(&lb[d], RS_FLAG_PRE | ((excl + cnt) & RS_VAL_MASK));
   }
   // tile-local exclusive scan of the digit counts (256 values, one per thread)
   {
@@ -369,31 +400,32 @@ __global__ void __launch_bounds__(RS_THREADS, 4) k_rs_pass(const K* __restrict__
     __syncthreads();
     const uint32_t te = x - cnt + (warp > 0 ? s_w[warp - 1] : 0u);
     sm.tile_excl[d] = te;
-    sm.out_base[d] = (long long)digit_base[d] + (long long)excl - (long long)te;
+    sm.out_base[d] = (int)(digit_base[d] + excl) - (int)te;
   }
   __syncthreads();
-  // scatter into shared memory in digit order
+  // keys to digit order in shared memory, with the input slot of each payload
 #pragma unroll
   for (int k = 0; k < IPT; ++k) {
-    if (dig[k] < 256u) {
-      const uint32_t pos = sm.tile_excl[dig[k]] + sm.warp_hist[warp][dig[k]] + rank[k];
+    if (wbase + (uint64_t)k * 32 + lane < n) {
+      const uint32_t dd = (uint32_t)(key[k] >> shift) & 0xFFu;
+      const uint32_t pos = sm.tile_excl[dd] + sm.warp_hist[warp][dd] + rank[k];
       sm.keys[pos] = key[k];
-      const uint64_t i = wbase + (uint64_t)k * 32 + lane;
-      sm.vals[pos] = vin[i];
+      sm.src[pos] = (uint16_t)(wslot + k * 32 + lane);
     }
   }
+  asm volatile("cp.async.wait_all;" ::: "memory");
   __syncthreads();
   const uint32_t valid = (uint32_t)min((uint64_t)TILE, n - tbase);
   for (uint32_t idx = threadIdx.x; idx < valid; idx += RS_THREADS) {
     const K kk = sm.keys[idx];
     const uint32_t dd = (uint32_t)(kk >> shift) & 0xFFu;
-    const long long g = sm.out_base[dd] + (long long)idx;
+    const long long g = (long long)sm.out_base[dd] + (long long)idx;
     if (g < 0 || (uint64_t)g >= n) {  // only after a look-back gave up: keep the write in bounds
       atomicOr(err, SC_DEVERR_TIMEOUT);
       continue;
     }
     kout[g] = kk;
-    vout[g] = sm.vals[idx];
+    vout[g] = sm.vals[sm.src[idx]];
   }
 }
 

@@ -141,9 +141,9 @@ __device__ __forceinline__ bool cull_row_span(const CullShape& s, int ty, uint32
   const float ul = (-s.b * wl - sqrtf(fmaxf(s.L * s.a - wl * wl * s.det, 0.0f))) * s.inv_a;
   const float X0 = s.mx + ul - 1e-3f, X1 = s.mx + ur + 1e-3f;
   // tile tx's pixel centres span [tx*tw + 0.5, (tx+1)*tw - 0.5]
-  const float ftw = (float)tw;
-  tlo = (int)ceilf((X0 + 0.5f) / ftw - 1.0f);
-  thi = (int)floorf((X1 - 0.5f) / ftw);
+  const float inv_tw = 1.0f / (float)tw;  // exact for power-of-two tiles; the 1e-3 px margin covers the rest
+  tlo = (int)ceilf((X0 + 0.5f) * inv_tw - 1.0f);
+  thi = (int)floorf((X1 - 0.5f) * inv_tw);
   return thi >= tlo;
 }
 
