@@ -336,6 +336,48 @@ sc_status sc_trainer_stats(const sc_trainer* tr, uint64_t* pairs, uint32_t* n_ke
 /* Record CUDA events between the stages of each step (also inside the graph). */
 sc_status sc_trainer_set_profiling(sc_trainer* tr, int enabled);
 
+/* ------------------------------------------------ data-parallel views
+ * No counterpart in the reference, which trains on one device (train.rs:155-250
+ * renders the iteration's views one after another).  One iteration is split
+ * across R ranks by views, ZeRO-1 style:
+ *   1. every rank: sc_trainer_step_grads over its own views -> per-splat
+ *      gradient summed over those views, written shard-major;
+ *   2. the caller reduce-scatters that buffer (R chunks) over its communicator;
+ *   3. every rank: sc_adam_step_shard on its chunk of splats [lo, lo+count);
+ *   4. sc_splats_pack_range of that chunk, all-gather, sc_splats_unpack_shards.
+ * Shard-major layout with chunks of `shard` splats: element (row r, splat i)
+ * is at ((i / shard) * 59 + r) * shard + i % shard; rows 0-58 are the
+ * parameter rows of sc_host_splats in slab order (pos 3, rot 4, log-scale 3,
+ * opacity logit 1, sh_dc 3, sh_rest 45 planar). */
+#define SC_PARAM_ROWS 59
+
+/* Steps 1: the trainer's views rendered, dL/dC scaled by loss_weight (the
+ * single-device step uses 1/n_views; a split iteration of V views in total
+ * uses 1/V on every rank), and the per-splat gradient summed over the views
+ * written to grads (n_shards * 59 * shard floats, n_shards * shard >= n;
+ * rows of padding splats are zero).  loss_out = loss_weight * sum of the
+ * views' MSE.  Parameters, moments and the densify statistic are untouched.
+ * Blocking, like sc_trainer_step. */
+sc_status sc_trainer_step_grads(sc_trainer* tr, sc_splats* s, const sc_camera* cams, float loss_weight,
+                                uint32_t n_shards, uint32_t shard, float* grads, double* loss_out);
+/* Step 3: Adam (shared t), densify statistic and constraints for splats
+ * [lo, lo+count) from the reduced chunk shard_grads[r * shard + j]. */
+sc_status sc_adam_step_shard(sc_ctx* ctx, sc_splats* s, sc_moments* mo, float* grad_acc, const float* shard_grads,
+                             uint32_t lo, uint32_t count, uint32_t shard, uint64_t t, const sc_adam_groups* groups,
+                             float log_scale_min, float log_scale_max, float opacity_logit_max);
+/* Step 4: parameters of [lo, lo+count) as f32 rows out[r * shard + j], and the
+ * inverse over n_shards gathered chunks (splats >= n are ignored; bf16 rows
+ * round to nearest even, which reproduces the owner's stored value). */
+sc_status sc_splats_pack_range(sc_ctx* ctx, const sc_splats* s, uint32_t lo, uint32_t count, uint32_t shard,
+                               float* out);
+sc_status sc_splats_unpack_shards(sc_ctx* ctx, sc_splats* s, const float* in, uint32_t n_shards, uint32_t shard);
+/* The same for the Adam moments (chunks of 2 * 59 rows: m then v), used to
+ * give every rank the full moments before a densify or prune. */
+sc_status sc_moments_pack_range(sc_ctx* ctx, const sc_moments* mo, uint32_t lo, uint32_t count, uint32_t shard,
+                                float* out);
+sc_status sc_moments_unpack_shards(sc_ctx* ctx, sc_moments* mo, uint32_t n, const float* in, uint32_t n_shards,
+                                   uint32_t shard);
+
 #ifdef __cplusplus
 }
 #endif

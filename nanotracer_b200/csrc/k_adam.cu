@@ -47,14 +47,10 @@ sc_status launch_adam_lanes(sc_ctx* ctx, float* p, const float* g, float* m, flo
   return sc_check_launch(ctx, "k_adam_lanes");
 }
 
-__device__ __forceinline__ int row_group(int r) {
-  return r < 3 ? 0 : (r < 7 ? 1 : (r < 10 ? 2 : (r < 11 ? 3 : (r < 14 ? 4 : 5))));
-}
-
 // grid.y = row (59), grid.x covers splats
 __global__ void k_adam_all(DSplats s, const float* __restrict__ g, uint32_t gcap, DMoments mo, AdamParams ap) {
   const int r = blockIdx.y;
-  const float lr = ap.lr[row_group(r)];
+  const float lr = ap.lr[adam_group(r)];
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += gridDim.x * blockDim.x) {
     const float gi = g[(size_t)r * gcap + i];
     const size_t k = (size_t)r * mo.cap + i;
@@ -110,6 +106,103 @@ sc_status launch_accumulate(sc_ctx* ctx, const float* g, uint32_t gcap, float* a
   if (n == 0) return SC_OK;
   k_accumulate<<<(unsigned)sc_div_up(n, 256), 256, 0, ctx->stream>>>(g, gcap, acc, n);
   return sc_check_launch(ctx, "k_accumulate");
+}
+
+// ---------------------------------------------------------------- data-parallel shards
+// Adam + constraints + densify statistic over splats [lo, lo+count), gradient
+// rows g[r * shard + j] (one reduce-scattered chunk).  Same arithmetic as the
+// fused single-device kernel; one thread per splat so the 59 row accesses of a
+// warp are 32 consecutive splats.
+__global__ void k_adam_shard(DSplats s, DMoments mo, float* __restrict__ acc, const float* __restrict__ g, uint32_t lo,
+                             uint32_t count, uint32_t shard, AdamParams ap) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= count) return;
+  const uint32_t i = lo + j;
+  float gg[14], np[14];
+#pragma unroll
+  for (int r = 0; r < 14; ++r) gg[r] = g[(size_t)r * shard + j];
+  if (acc) acc[i] = acc[i] + fabsf(gg[0]) + fabsf(gg[1]) + fabsf(gg[2]);
+#pragma unroll
+  for (int r = 0; r < 14; ++r)
+    np[r] = adam_scalar(mo, (size_t)r * mo.cap + i, s.slab[(size_t)r * s.cap + i], gg[r], ap.lr[adam_group(r)], ap);
+  constrain_geometry(np, ap);
+#pragma unroll
+  for (int r = 0; r < 14; ++r) s.slab[(size_t)r * s.cap + i] = np[r];
+#pragma unroll 5
+  for (int r = SC_ROW_REST; r < SC_NROWS; ++r)
+    sp_set(s, r, i, adam_scalar(mo, (size_t)r * mo.cap + i, sp_row(s, r, i), g[(size_t)r * shard + j], ap.lr[5], ap));
+}
+
+sc_status launch_adam_shard(sc_ctx* ctx, const DSplats& s, const DMoments& mo, float* acc, const float* g, uint32_t lo,
+                            uint32_t count, uint32_t shard, const AdamParams& ap) {
+  if (count == 0) return SC_OK;
+  k_adam_shard<<<(unsigned)sc_div_up(count, 256), 256, 0, ctx->stream>>>(s, mo, acc, g, lo, count, shard, ap);
+  return sc_check_launch(ctx, "k_adam_shard");
+}
+
+// grid.y = row
+__global__ void k_pack_params(DSplats s, uint32_t lo, uint32_t count, uint32_t shard, float* __restrict__ out) {
+  const int r = blockIdx.y;
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x)
+    out[(size_t)r * shard + j] = sp_row(s, r, lo + j);
+}
+
+// in = n_shards chunks of SC_NROWS rows x shard; splat i = q * shard + j
+__global__ void k_unpack_params(DSplats s, const float* __restrict__ in, uint32_t n_shards, uint32_t shard) {
+  const int r = blockIdx.y;
+  const uint64_t total = std::min<uint64_t>((uint64_t)n_shards * shard, s.n);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t q = i / shard, j = i % shard;
+    sp_set(s, r, (uint32_t)i, in[(q * SC_NROWS + r) * shard + j]);
+  }
+}
+
+__global__ void k_pack_moments(DMoments mo, uint32_t lo, uint32_t count, uint32_t shard, float* __restrict__ out) {
+  const int r = blockIdx.y >> 1, which = blockIdx.y & 1;  // m rows then v rows, interleaved by grid.y
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x) {
+    const size_t k = (size_t)r * mo.cap + lo + j;
+    const float x = which ? mo_ld(mo, mo.v, mo.v16, k) : mo_ld(mo, mo.m, mo.m16, k);
+    out[((size_t)which * SC_NROWS + r) * shard + j] = x;
+  }
+}
+
+// in = n_shards chunks of 2 * SC_NROWS rows (m then v) x shard
+__global__ void k_unpack_moments(DMoments mo, uint32_t n, const float* __restrict__ in, uint32_t n_shards,
+                                 uint32_t shard) {
+  const int r = blockIdx.y >> 1, which = blockIdx.y & 1;
+  const uint64_t total = std::min<uint64_t>((uint64_t)n_shards * shard, n);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t q = i / shard, j = i % shard;
+    const float x = in[((q * 2 + which) * SC_NROWS + r) * shard + j];
+    const size_t k = (size_t)r * mo.cap + i;
+    if (which) mo_st(mo, mo.v, mo.v16, k, x); else mo_st(mo, mo.m, mo.m16, k, x);
+  }
+}
+
+static unsigned rows_grid_x(sc_ctx* ctx, uint64_t n) {
+  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(sc_div_up(n, 256), (uint64_t)ctx->sm_count * 4));
+}
+
+sc_status launch_pack_params(sc_ctx* ctx, const DSplats& s, uint32_t lo, uint32_t count, uint32_t shard, float* out) {
+  if (count == 0) return SC_OK;
+  k_pack_params<<<dim3(rows_grid_x(ctx, count), SC_NROWS), 256, 0, ctx->stream>>>(s, lo, count, shard, out);
+  return sc_check_launch(ctx, "k_pack_params");
+}
+sc_status launch_unpack_params(sc_ctx* ctx, const DSplats& s, const float* in, uint32_t n_shards, uint32_t shard) {
+  if (s.n == 0 || n_shards == 0 || shard == 0) return SC_OK;
+  k_unpack_params<<<dim3(rows_grid_x(ctx, s.n), SC_NROWS), 256, 0, ctx->stream>>>(s, in, n_shards, shard);
+  return sc_check_launch(ctx, "k_unpack_params");
+}
+sc_status launch_pack_moments(sc_ctx* ctx, const DMoments& mo, uint32_t lo, uint32_t count, uint32_t shard, float* out) {
+  if (count == 0) return SC_OK;
+  k_pack_moments<<<dim3(rows_grid_x(ctx, count), 2 * SC_NROWS), 256, 0, ctx->stream>>>(mo, lo, count, shard, out);
+  return sc_check_launch(ctx, "k_pack_moments");
+}
+sc_status launch_unpack_moments(sc_ctx* ctx, const DMoments& mo, uint32_t n, const float* in, uint32_t n_shards,
+                                uint32_t shard) {
+  if (n == 0 || n_shards == 0 || shard == 0) return SC_OK;
+  k_unpack_moments<<<dim3(rows_grid_x(ctx, n), 2 * SC_NROWS), 256, 0, ctx->stream>>>(mo, n, in, n_shards, shard);
+  return sc_check_launch(ctx, "k_unpack_moments");
 }
 
 // ---------------------------------------------------------------- compaction helpers

@@ -373,45 +373,26 @@ sc_status launch_project_backward(sc_ctx* ctx, const DSplats& s, const float4* p
   return sc_check_launch(ctx, "k_project_backward");
 }
 
-// ---------------------------------------------------------------- fused backward + Adam
-__device__ __forceinline__ float ld_m(const DMoments& mo, const float* f, const __nv_bfloat16* h, size_t k) {
-  return mo.bf16 ? __bfloat162float(h[k]) : f[k];
-}
-__device__ __forceinline__ void st_m(const DMoments& mo, float* f, __nv_bfloat16* h, size_t k, float x) {
-  if (mo.bf16) h[k] = __float2bfloat16_rn(x); else f[k] = x;
-}
+// ---------------------------------------------------------------- multi-view gradient sum
+// Sum of splat i's parameter gradients over n_views views, in the order of the
+// views (project_backward.wgsl:79-304 per view, accumulated like the
+// reference's per-view passes into one gradient buffer).
+struct SplatGrads {
+  float gpos[3], grot[4], gsc[3], gop, gdc[3], grest[45];
+};
 
-__device__ __forceinline__ int lr_group(int r) {
-  return r < 3 ? 0 : (r < 7 ? 1 : (r < 10 ? 2 : (r < 11 ? 3 : (r < 14 ? 4 : 5))));
-}
-
-// Adam for one scalar (adam_step.wgsl:24-36)
-__device__ __forceinline__ float adam_one(const DMoments& mo, size_t k, float p, float gr, float lr, const AdamParams& ap) {
-  const float m = ap.beta1 * ld_m(mo, mo.m, mo.m16, k) + (1.0f - ap.beta1) * gr;
-  const float v = ap.beta2 * ld_m(mo, mo.v, mo.v16, k) + (1.0f - ap.beta2) * gr * gr;
-  st_m(mo, mo.m, mo.m16, k, m);
-  st_m(mo, mo.v, mo.v16, k, v);
-  const float mh = m / ap.bc1, vh = v / ap.bc2;
-  return p - lr * mh / (sqrtf(vh) + ap.eps);
-}
-
-__global__ void __launch_bounds__(128, 4) k_fused_backward_adam(DSplats s, DMoments mo, const float4* __restrict__ pg,
-                                                             uint32_t stride, const sc_camera* __restrict__ cams,
-                                                             uint32_t n_views, float* __restrict__ grad_acc,
-                                                             AdamParams ap, const uint32_t* __restrict__ skip,
-                                                             const float* __restrict__ d_bc) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= s.n) return;
-  if (skip && (*skip & SC_DEVERR_CAPACITY)) return;  // a capacity overflow earlier in the step: leave parameters untouched
-  if (d_bc) { ap.bc1 = d_bc[0]; ap.bc2 = d_bc[1]; }
+__device__ __forceinline__ void sum_view_grads(const DSplats& s, uint32_t i, const float4* __restrict__ pg,
+                                               uint32_t stride, const sc_camera* __restrict__ cams, uint32_t n_views,
+                                               SplatGrads& G) {
   const float px = sp_row(s, 0, i), py = sp_row(s, 1, i), pz = sp_row(s, 2, i);
   const float qw = sp_row(s, 3, i), qx = sp_row(s, 4, i), qy = sp_row(s, 5, i), qz = sp_row(s, 6, i);
   const float l0 = sp_row(s, 7, i), l1 = sp_row(s, 8, i), l2 = sp_row(s, 9, i);
-  const float olog = sp_row(s, 10, i);
-  const float opacity = 1.0f / (1.0f + expf(-olog));
-  float gpos[3] = {0, 0, 0}, grot[4] = {0, 0, 0, 0}, gsc[3] = {0, 0, 0}, gop = 0;
-  float gdc[3] = {0, 0, 0};
-  float grest[45];
+  const float opacity = 1.0f / (1.0f + expf(-sp_row(s, 10, i)));
+  float* gpos = G.gpos; float* grot = G.grot; float* gsc = G.gsc; float& gop = G.gop;
+  float* gdc = G.gdc; float* grest = G.grest;
+  for (int k = 0; k < 3; ++k) { gpos[k] = 0.f; gsc[k] = 0.f; gdc[k] = 0.f; }
+  for (int k = 0; k < 4; ++k) grot[k] = 0.f;
+  gop = 0.f;
 #pragma unroll
   for (int k = 0; k < 45; ++k) grest[k] = 0.f;
   for (uint32_t v = 0; v < n_views; ++v) {
@@ -432,33 +413,76 @@ __global__ void __launch_bounds__(128, 4) k_fused_backward_adam(DSplats s, DMome
       grest[k] += p2.x * basis[k]; grest[15 + k] += p2.y * basis[k]; grest[30 + k] += p2.z * basis[k];
     }
   }
+}
+
+// ---------------------------------------------------------------- fused backward + Adam
+__global__ void __launch_bounds__(128, 4) k_fused_backward_adam(DSplats s, DMoments mo, const float4* __restrict__ pg,
+                                                             uint32_t stride, const sc_camera* __restrict__ cams,
+                                                             uint32_t n_views, float* __restrict__ grad_acc,
+                                                             AdamParams ap, const uint32_t* __restrict__ skip,
+                                                             const float* __restrict__ d_bc) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n) return;
+  if (skip && (*skip & SC_DEVERR_CAPACITY)) return;  // a capacity overflow earlier in the step: leave parameters untouched
+  if (d_bc) { ap.bc1 = d_bc[0]; ap.bc2 = d_bc[1]; }
+  SplatGrads G;
+  sum_view_grads(s, i, pg, stride, cams, n_views, G);
   // densify statistic, accumulate_grad_pos.wgsl:17-23 (before the step, train.rs:228)
-  if (grad_acc) grad_acc[i] = grad_acc[i] + fabsf(gpos[0]) + fabsf(gpos[1]) + fabsf(gpos[2]);
+  if (grad_acc) grad_acc[i] = grad_acc[i] + fabsf(G.gpos[0]) + fabsf(G.gpos[1]) + fabsf(G.gpos[2]);
   const size_t cap = s.cap;
   // geometric rows
-  const float gg[14] = {gpos[0], gpos[1], gpos[2], grot[0], grot[1], grot[2], grot[3],
-                        gsc[0], gsc[1], gsc[2], gop, gdc[0], gdc[1], gdc[2]};
-  const float pp[14] = {px, py, pz, qw, qx, qy, qz, l0, l1, l2, olog, sp_row(s, 11, i), sp_row(s, 12, i),
-                        sp_row(s, 13, i)};
+  const float gg[14] = {G.gpos[0], G.gpos[1], G.gpos[2], G.grot[0], G.grot[1], G.grot[2], G.grot[3],
+                        G.gsc[0],  G.gsc[1],  G.gsc[2],  G.gop,     G.gdc[0],  G.gdc[1],  G.gdc[2]};
   float np[14];
 #pragma unroll
-  for (int r = 0; r < 14; ++r) np[r] = adam_one(mo, (size_t)r * mo.cap + i, pp[r], gg[r], ap.lr[lr_group(r)], ap);
-  // constraints, apply_constraints.wgsl:24-41
-  {
-    const float n2 = np[3] * np[3] + np[4] * np[4] + np[5] * np[5] + np[6] * np[6];
-    const float nrm = fmaxf(sqrtf(n2), 1e-8f);
-    np[3] /= nrm; np[4] /= nrm; np[5] /= nrm; np[6] /= nrm;
-    for (int k = 7; k < 10; ++k) np[k] = fminf(fmaxf(np[k], ap.log_scale_min), ap.log_scale_max);
-    np[10] = fminf(fmaxf(np[10], -ap.opacity_logit_max), ap.opacity_logit_max);
-  }
+  for (int r = 0; r < 14; ++r)
+    np[r] = adam_scalar(mo, (size_t)r * mo.cap + i, s.slab[(size_t)r * cap + i], gg[r], ap.lr[adam_group(r)], ap);
+  constrain_geometry(np, ap);
 #pragma unroll
   for (int r = 0; r < 14; ++r) s.slab[(size_t)r * cap + i] = np[r];
 #pragma unroll
   for (int k = 0; k < 45; ++k) {
     const int r = SC_ROW_REST + k;
     const float p = sp_row(s, r, i);
-    sp_set(s, r, i, adam_one(mo, (size_t)r * mo.cap + i, p, grest[k], ap.lr[5], ap));
+    sp_set(s, r, i, adam_scalar(mo, (size_t)r * mo.cap + i, p, G.grest[k], ap.lr[5], ap));
   }
+}
+
+// ---------------------------------------------------------------- data-parallel views
+__global__ void __launch_bounds__(128, 4) k_project_backward_shards(DSplats s, const float4* __restrict__ pg,
+                                                                 uint32_t stride, const sc_camera* __restrict__ cams,
+                                                                 uint32_t n_views, float* __restrict__ out,
+                                                                 uint32_t n_shards, uint32_t shard,
+                                                                 const uint32_t* __restrict__ skip) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (uint64_t)n_shards * shard) return;
+  float* dst = out + (i / shard) * SC_NROWS * (uint64_t)shard + i % shard;
+  SplatGrads G;
+  if (i < s.n && !(skip && (*skip & SC_DEVERR_CAPACITY))) {
+    sum_view_grads(s, (uint32_t)i, pg, stride, cams, n_views, G);
+  } else {  // padding splats, or a step whose emission overflowed: contribute nothing
+    for (int k = 0; k < 3; ++k) { G.gpos[k] = 0.f; G.gsc[k] = 0.f; G.gdc[k] = 0.f; }
+    for (int k = 0; k < 4; ++k) G.grot[k] = 0.f;
+    G.gop = 0.f;
+#pragma unroll
+    for (int k = 0; k < 45; ++k) G.grest[k] = 0.f;
+  }
+  const float gg[14] = {G.gpos[0], G.gpos[1], G.gpos[2], G.grot[0], G.grot[1], G.grot[2], G.grot[3],
+                        G.gsc[0],  G.gsc[1],  G.gsc[2],  G.gop,     G.gdc[0],  G.gdc[1],  G.gdc[2]};
+#pragma unroll
+  for (int r = 0; r < 14; ++r) dst[(size_t)r * shard] = gg[r];
+#pragma unroll
+  for (int k = 0; k < 45; ++k) dst[(size_t)(SC_ROW_REST + k) * shard] = G.grest[k];
+}
+
+sc_status launch_project_backward_shards(sc_ctx* ctx, const DSplats& s, const float4* pg, uint32_t stride,
+                                         const sc_camera* d_cams, uint32_t n_views, float* grads, uint32_t n_shards,
+                                         uint32_t shard, const uint32_t* d_skip) {
+  const uint64_t total = (uint64_t)n_shards * shard;
+  if (total == 0) return SC_OK;
+  k_project_backward_shards<<<(unsigned)sc_div_up(total, 128), 128, 0, ctx->stream>>>(s, pg, stride, d_cams, n_views,
+                                                                                      grads, n_shards, shard, d_skip);
+  return sc_check_launch(ctx, "k_project_backward_shards");
 }
 
 sc_status launch_fused_backward_adam(sc_ctx* ctx, const DSplats& s, const DMoments& mo, const float4* pg,

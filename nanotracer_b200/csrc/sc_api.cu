@@ -749,6 +749,53 @@ sc_status sc_adam_step_all(sc_ctx* ctx, sc_splats* s, const sc_grads* g, sc_mome
   return sck::launch_adam_all(ctx, dview(s), g->slab, g->cap, dview(mo), ap);
 }
 
+sc_status sc_adam_step_shard(sc_ctx* ctx, sc_splats* s, sc_moments* mo, float* acc, const float* g, uint32_t lo,
+                             uint32_t count, uint32_t shard, uint64_t t, const sc_adam_groups* gr, float lsmin,
+                             float lsmax, float opmax) {
+  if (!ctx || !s || !mo || !gr || t == 0 || (count && !g)) return SC_ERR_INVALID_ARG;
+  if (count > shard || (uint64_t)lo + count > s->n)
+    return sc_fail(ctx, SC_ERR_INVALID_ARG, "shard range outside the splat count or wider than the chunk");
+  if (mo->cap < s->n) return sc_fail(ctx, SC_ERR_CAPACITY, "moments smaller than the splat count");
+  sck::AdamParams ap;
+  for (int k = 0; k < 6; ++k) ap.lr[k] = gr->lr[k];
+  ap.beta1 = gr->beta1; ap.beta2 = gr->beta2; ap.eps = gr->eps;
+  ap.bc1 = 1.0f - sc_powi_f32(gr->beta1, (int)t);
+  ap.bc2 = 1.0f - sc_powi_f32(gr->beta2, (int)t);
+  ap.log_scale_min = lsmin; ap.log_scale_max = lsmax; ap.opacity_logit_max = opmax;
+  return sck::launch_adam_shard(ctx, dview(s), dview(mo), acc, g, lo, count, shard, ap);
+}
+
+sc_status sc_splats_pack_range(sc_ctx* ctx, const sc_splats* s, uint32_t lo, uint32_t count, uint32_t shard,
+                               float* out) {
+  if (!ctx || !s || (count && !out)) return SC_ERR_INVALID_ARG;
+  if (count > shard || (uint64_t)lo + count > s->n)
+    return sc_fail(ctx, SC_ERR_INVALID_ARG, "pack range outside the splat count or wider than the chunk");
+  return sck::launch_pack_params(ctx, dview(s), lo, count, shard, out);
+}
+
+sc_status sc_splats_unpack_shards(sc_ctx* ctx, sc_splats* s, const float* in, uint32_t n_shards, uint32_t shard) {
+  if (!ctx || !s || (n_shards && shard && !in)) return SC_ERR_INVALID_ARG;
+  if ((uint64_t)n_shards * shard < s->n)
+    return sc_fail(ctx, SC_ERR_INVALID_ARG, "gathered chunks cover fewer splats than the store holds");
+  return sck::launch_unpack_params(ctx, dview(s), in, n_shards, shard);
+}
+
+sc_status sc_moments_pack_range(sc_ctx* ctx, const sc_moments* mo, uint32_t lo, uint32_t count, uint32_t shard,
+                                float* out) {
+  if (!ctx || !mo || (count && !out)) return SC_ERR_INVALID_ARG;
+  if (count > shard || (uint64_t)lo + count > mo->cap)
+    return sc_fail(ctx, SC_ERR_INVALID_ARG, "pack range outside the moments or wider than the chunk");
+  return sck::launch_pack_moments(ctx, dview(mo), lo, count, shard, out);
+}
+
+sc_status sc_moments_unpack_shards(sc_ctx* ctx, sc_moments* mo, uint32_t n, const float* in, uint32_t n_shards,
+                                   uint32_t shard) {
+  if (!ctx || !mo || (n_shards && shard && !in)) return SC_ERR_INVALID_ARG;
+  if (n > mo->cap || (uint64_t)n_shards * shard < n)
+    return sc_fail(ctx, SC_ERR_INVALID_ARG, "moments unpack: n beyond capacity or not covered by the chunks");
+  return sck::launch_unpack_moments(ctx, dview(mo), n, in, n_shards, shard);
+}
+
 sc_status sc_apply_constraints(sc_ctx* ctx, sc_splats* s, float lsmin, float lsmax, float opmax) {
   if (!ctx || !s) return SC_ERR_INVALID_ARG;
   return sck::launch_constraints(ctx, dview(s), lsmin, lsmax, opmax);

@@ -195,6 +195,55 @@ sc_status launch_fused_backward_adam(sc_ctx* ctx, const DSplats& s, const DMomen
                                      uint32_t stride, const sc_camera* d_cams, uint32_t n_views, float* grad_acc,
                                      const AdamParams& ap, const uint32_t* d_skip_flag, const float* d_bc);
 
+// moments widened to / rounded from f32
+__device__ __forceinline__ float mo_ld(const DMoments& mo, const float* f, const __nv_bfloat16* h, size_t k) {
+  return mo.bf16 ? __bfloat162float(h[k]) : f[k];
+}
+__device__ __forceinline__ void mo_st(const DMoments& mo, float* f, __nv_bfloat16* h, size_t k, float x) {
+  if (mo.bf16) h[k] = __float2bfloat16_rn(x); else f[k] = x;
+}
+// learning-rate group of parameter row r: pos, rot, scale, opacity, sh_dc, sh_rest
+__device__ __forceinline__ int adam_group(int r) {
+  return r < 3 ? 0 : (r < 7 ? 1 : (r < 10 ? 2 : (r < 11 ? 3 : (r < 14 ? 4 : 5))));
+}
+// Adam on one scalar (adam_step.wgsl:24-36), moments at flat index k
+__device__ __forceinline__ float adam_scalar(const DMoments& mo, size_t k, float p, float gr, float lr,
+                                             const AdamParams& ap) {
+  const float m = ap.beta1 * mo_ld(mo, mo.m, mo.m16, k) + (1.0f - ap.beta1) * gr;
+  const float v = ap.beta2 * mo_ld(mo, mo.v, mo.v16, k) + (1.0f - ap.beta2) * gr * gr;
+  mo_st(mo, mo.m, mo.m16, k, m);
+  mo_st(mo, mo.v, mo.v16, k, v);
+  const float mh = m / ap.bc1, vh = v / ap.bc2;
+  return p - lr * mh / (sqrtf(vh) + ap.eps);
+}
+// constraints on the updated geometric rows 0..13 (apply_constraints.wgsl:24-41)
+__device__ __forceinline__ void constrain_geometry(float np[14], const AdamParams& ap) {
+  const float n2 = np[3] * np[3] + np[4] * np[4] + np[5] * np[5] + np[6] * np[6];
+  const float nrm = fmaxf(sqrtf(n2), 1e-8f);
+  np[3] /= nrm; np[4] /= nrm; np[5] /= nrm; np[6] /= nrm;
+  for (int k = 7; k < 10; ++k) np[k] = fminf(fmaxf(np[k], ap.log_scale_min), ap.log_scale_max);
+  np[10] = fminf(fmaxf(np[10], -ap.opacity_logit_max), ap.opacity_logit_max);
+}
+
+// ---- data-parallel views (one iteration split across ranks by views)
+// Shard-major gradient layout: element (row r, splat i) of a buffer cut into
+// chunks of `shard` splats sits at ((i / shard) * SC_NROWS + r) * shard + i % shard.
+// Per-splat gradient summed over this rank's views, written shard-major; rows
+// of splats in [n, n_shards*shard) are zero.
+sc_status launch_project_backward_shards(sc_ctx* ctx, const DSplats& s, const float4* proj_grad, uint32_t stride,
+                                         const sc_camera* d_cams, uint32_t n_views, float* grads, uint32_t n_shards,
+                                         uint32_t shard, const uint32_t* d_skip_flag);
+// Adam + constraints + densify statistic for splats [lo, lo+count) from one
+// reduce-scattered chunk g[r * shard + j]
+sc_status launch_adam_shard(sc_ctx* ctx, const DSplats& s, const DMoments& mo, float* grad_acc, const float* g,
+                            uint32_t lo, uint32_t count, uint32_t shard, const AdamParams& ap);
+// parameters / moments of [lo, lo+count) as f32 rows out[r * shard + j], and back
+sc_status launch_pack_params(sc_ctx* ctx, const DSplats& s, uint32_t lo, uint32_t count, uint32_t shard, float* out);
+sc_status launch_unpack_params(sc_ctx* ctx, const DSplats& s, const float* in, uint32_t n_shards, uint32_t shard);
+sc_status launch_pack_moments(sc_ctx* ctx, const DMoments& mo, uint32_t lo, uint32_t count, uint32_t shard, float* out);
+sc_status launch_unpack_moments(sc_ctx* ctx, const DMoments& mo, uint32_t n, const float* in, uint32_t n_shards,
+                                uint32_t shard);
+
 // scan / sort
 sc_status scan_u32(sc_ctx* ctx, uint32_t* data, uint64_t n, uint64_t* d_total, void* scratch, size_t scratch_bytes);
 size_t scan_scratch_bytes(uint64_t n);

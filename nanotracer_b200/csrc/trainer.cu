@@ -39,12 +39,13 @@ struct StepOut {
   uint32_t pad;
 };
 
-__global__ void k_finalize(const double* __restrict__ loss_sums, uint32_t n_views, double inv_count,
+// loss = mean over the views, or (weight > 0) weight * sum over the views
+__global__ void k_finalize(const double* __restrict__ loss_sums, uint32_t n_views, double inv_count, double weight,
                            const uint64_t* __restrict__ d_total, const uint32_t* __restrict__ err,
                            StepOut* __restrict__ out) {
   double acc = 0.0;
   for (uint32_t v = 0; v < n_views; ++v) acc += loss_sums[v] * inv_count;
-  out->loss = acc / (double)n_views;
+  out->loss = weight > 0.0 ? acc * weight : acc / (double)n_views;
   out->pairs = *d_total;
   out->err = *err;
 }
@@ -86,10 +87,18 @@ struct sc_trainer {
   double* d_loss = nullptr;
   uint64_t* d_total = nullptr;
   void* scratch = nullptr; size_t scratch_bytes = 0;
+  // gradient-only steps (data-parallel views): shard-major output
+  bool grads_mode = false;
+  float loss_weight = 0.0f;
+  float* gout = nullptr;
+  uint32_t g_shards = 0, g_shard = 0;
   // graph
   cudaGraphExec_t exec = nullptr;
-  const void* g_key[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  const void* g_key[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   uint64_t g_key_n = 0, g_key_kcap = 0;
+  bool g_key_grads = false;
+  float g_key_w = 0.0f;
+  uint32_t g_key_shards = 0, g_key_shard = 0;
   // results of the last step
   uint64_t last_pairs = 0;
   uint32_t kernels_per_step = 0;
@@ -196,7 +205,7 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   const uint32_t V = tr->V;
   const uint64_t nsp = (uint64_t)V * tr->stride;
   const DSplats ds = dview(s);
-  const DMoments dm = dview(mo);
+  const DMoments dm = mo ? dview(mo) : DMoments{};
   const uint64_t launches0 = ctx->launches;
   SC_CUDA_TRY(ctx, cudaMemcpyAsync(tr->d_params, tr->h_params, sizeof(StepParams), cudaMemcpyHostToDevice, ctx->stream),
               "params H2D");
@@ -234,8 +243,9 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   mark(tr, 5, capturing);
   SC_TRY(sck::launch_tile_ranges(ctx, skeys, 2, tr->d_total, tr->kcap, all_tiles, tr->ranges));
   mark(tr, 6, capturing);
+  const float weight = tr->grads_mode ? tr->loss_weight : 1.0f / (float)V;
   SC_TRY(sck::launch_composite(ctx, tr->rec, tr->stride, V, svals, tr->ranges, &tr->cfg.tiling, tr->image, tr->aux,
-                               tr->targets, 1.0f / (float)V, tr->dl_dc, tr->d_loss, ctx->d_error));
+                               tr->targets, weight, tr->dl_dc, tr->d_loss, ctx->d_error));
   mark(tr, 7, capturing);
   SC_TRY(sck::launch_composite_backward(ctx, tr->rec, tr->stride, V, svals, tr->ranges, &tr->cfg.tiling, tr->image,
                                         tr->dl_dc, (int)tr->cfg.bwd_mode, tr->aux, tr->pgrad, ctx->d_error));
@@ -246,9 +256,15 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   ap.bc1 = ap.bc2 = 1.0f;
   ap.log_scale_min = tr->cfg.log_scale_min; ap.log_scale_max = tr->cfg.log_scale_max;
   ap.opacity_logit_max = tr->cfg.opacity_logit_max;
-  SC_TRY(sck::launch_fused_backward_adam(ctx, ds, dm, tr->pgrad, tr->stride, d_cams, V, acc, ap, ctx->d_error, d_bc));
+  if (tr->grads_mode)
+    SC_TRY(sck::launch_project_backward_shards(ctx, ds, tr->pgrad, tr->stride, d_cams, V, tr->gout, tr->g_shards,
+                                               tr->g_shard, ctx->d_error));
+  else
+    SC_TRY(sck::launch_fused_backward_adam(ctx, ds, dm, tr->pgrad, tr->stride, d_cams, V, acc, ap, ctx->d_error, d_bc));
   mark(tr, 9, capturing);
-  k_finalize<<<1, 1, 0, ctx->stream>>>(tr->d_loss, V, 1.0 / (3.0 * (double)tr->P), tr->d_total, ctx->d_error, tr->d_out);
+  k_finalize<<<1, 1, 0, ctx->stream>>>(tr->d_loss, V, 1.0 / (3.0 * (double)tr->P),
+                                       tr->grads_mode ? (double)tr->loss_weight : 0.0, tr->d_total, ctx->d_error,
+                                       tr->d_out);
   SC_TRY(sc_check_launch(ctx, "k_finalize"));
   SC_CUDA_TRY(ctx, cudaMemcpyAsync(tr->h_out, tr->d_out, sizeof(StepOut), cudaMemcpyDeviceToHost, ctx->stream), "out D2H");
   tr->kernels_per_step = (uint32_t)(ctx->launches - launches0);
@@ -326,23 +342,21 @@ sc_status sc_trainer_set_profiling(sc_trainer* tr, int enabled) {
   return SC_OK;
 }
 
-sc_status sc_trainer_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, float* acc, const sc_camera* cams, uint64_t t,
-                          double* loss_out) {
-  if (!tr || !s || !mo || !acc || !cams || t == 0) return SC_ERR_INVALID_ARG;
-  if (!tr->targets) return sc_fail(tr->ctx, SC_ERR_INVALID_ARG, "trainer has no targets");
-  if (mo->cap < s->n) return SC_ERR_INVALID_ARG;
+}  // extern "C"
+
+// Run one step (fused or gradient-only, per tr->grads_mode) with the step
+// parameters already in pinned memory: graph capture/replay, capacity retry.
+static sc_status run_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, float* acc, double* loss_out) {
   sc_ctx* ctx = tr->ctx;
-  // step parameters into pinned memory (the graph's first node copies them)
-  std::memcpy(tr->h_params->cams, cams, sizeof(sc_camera) * tr->V);
-  tr->h_params->bc[0] = 1.0f - sc_powi_f32(tr->cfg.adam.beta1, (int)t);
-  tr->h_params->bc[1] = 1.0f - sc_powi_f32(tr->cfg.adam.beta2, (int)t);
   SC_TRY(ensure_splat_arrays(tr, s->cap));
   for (int attempt = 0; attempt < 4; ++attempt) {
     const bool sizing = tr->kcap == 0;
-    const void* key[6] = {s->slab, s->rest16, mo->m ? (const void*)mo->m : (const void*)mo->m16, acc, tr->targets,
-                          tr->scratch};
-    const bool key_ok = tr->exec && std::equal(key, key + 6, tr->g_key) && tr->g_key_n == s->n &&
-                        tr->g_key_kcap == tr->kcap;
+    const void* mkey = mo ? (mo->m ? (const void*)mo->m : (const void*)mo->m16) : nullptr;
+    const void* key[7] = {s->slab, s->rest16, mkey, acc, tr->targets, tr->scratch, tr->gout};
+    const bool key_ok = tr->exec && std::equal(key, key + 7, tr->g_key) && tr->g_key_n == s->n &&
+                        tr->g_key_kcap == tr->kcap && tr->g_key_grads == tr->grads_mode &&
+                        tr->g_key_w == tr->loss_weight && tr->g_key_shards == tr->g_shards &&
+                        tr->g_key_shard == tr->g_shard;
     if (!key_ok) trainer_drop_graph(tr);
     if (tr->cfg.use_graph && !sizing) {
       if (!tr->exec) {
@@ -355,9 +369,13 @@ sc_status sc_trainer_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, float* a
         ce = cudaGraphInstantiate(&tr->exec, g, 0);
         cudaGraphDestroy(g);
         if (ce != cudaSuccess) { tr->exec = nullptr; return sc_cuda_fail(ctx, ce, "graph instantiate"); }
-        std::copy(key, key + 6, tr->g_key);
+        std::copy(key, key + 7, tr->g_key);
         tr->g_key_n = s->n;
         tr->g_key_kcap = tr->kcap;
+        tr->g_key_grads = tr->grads_mode;
+        tr->g_key_w = tr->loss_weight;
+        tr->g_key_shards = tr->g_shards;
+        tr->g_key_shard = tr->g_shard;
       }
       SC_CUDA_TRY(ctx, cudaGraphLaunch(tr->exec, ctx->stream), "graph launch");
       ctx->launches += tr->kernels_per_step;
@@ -388,6 +406,41 @@ sc_status sc_trainer_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, float* a
     return SC_OK;
   }
   return sc_fail(ctx, SC_ERR_CAPACITY, "pair capacity kept overflowing");
+}
+
+extern "C" {
+
+sc_status sc_trainer_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, float* acc, const sc_camera* cams, uint64_t t,
+                          double* loss_out) {
+  if (!tr || !s || !mo || !acc || !cams || t == 0) return SC_ERR_INVALID_ARG;
+  if (!tr->targets) return sc_fail(tr->ctx, SC_ERR_INVALID_ARG, "trainer has no targets");
+  if (mo->cap < s->n) return SC_ERR_INVALID_ARG;
+  // step parameters into pinned memory (the graph's first node copies them)
+  std::memcpy(tr->h_params->cams, cams, sizeof(sc_camera) * tr->V);
+  tr->h_params->bc[0] = 1.0f - sc_powi_f32(tr->cfg.adam.beta1, (int)t);
+  tr->h_params->bc[1] = 1.0f - sc_powi_f32(tr->cfg.adam.beta2, (int)t);
+  tr->grads_mode = false;
+  tr->loss_weight = 0.0f;
+  tr->gout = nullptr;
+  tr->g_shards = tr->g_shard = 0;
+  return run_step(tr, s, mo, acc, loss_out);
+}
+
+sc_status sc_trainer_step_grads(sc_trainer* tr, sc_splats* s, const sc_camera* cams, float loss_weight,
+                                uint32_t n_shards, uint32_t shard, float* grads, double* loss_out) {
+  if (!tr || !s || !cams || !grads || !(loss_weight > 0.0f) || n_shards == 0 || shard == 0)
+    return SC_ERR_INVALID_ARG;
+  if (!tr->targets) return sc_fail(tr->ctx, SC_ERR_INVALID_ARG, "trainer has no targets");
+  if ((uint64_t)n_shards * shard < s->n)
+    return sc_fail(tr->ctx, SC_ERR_INVALID_ARG, "n_shards * shard must cover the splat count");
+  std::memcpy(tr->h_params->cams, cams, sizeof(sc_camera) * tr->V);
+  tr->h_params->bc[0] = tr->h_params->bc[1] = 1.0f;
+  tr->grads_mode = true;
+  tr->loss_weight = loss_weight;
+  tr->gout = grads;
+  tr->g_shards = n_shards;
+  tr->g_shard = shard;
+  return run_step(tr, s, nullptr, nullptr, loss_out);
 }
 
 sc_status sc_trainer_images(const sc_trainer* tr, const float** images) {
