@@ -155,6 +155,8 @@ def make_workload(args, rank, ctx):
 
 def run_ours(args):
     ws, rank, local, pg = dist_setup()
+    if (ws > 1 and args.parallel == "views") or args.view_path:
+        return run_views(args, ws, rank, local, pg)
     import torch
 
     import nanotracer_b200 as nt
@@ -274,17 +276,151 @@ def run_ours(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 blend/grad, bf16 SH-rest + Adam moments" if bf16 else "f32",
             "data": "synthetic seeded scene and targets (no dataset)",
-            "config": {"workload": f"{N} splats, {V} views x {args.width}x{args.height} per iteration, "
+            "config": {"workload": f"{N} splats, {V} views x {args.width}x{args.height} per iteration"
+                                   f"{' per GPU (one scene per GPU)' if ws > 1 else ''}, "
                                    f"{args.tile_w}x{args.tile_h} tiles, exact transmittance backward, CUDA graph",
                        "form": "batched-" + ("bf16" if bf16 else "fp32"), "splats": N, "views_per_iter": V,
                        "width": args.width, "height": args.height, "pairs_per_iter": K,
                        "l2": "inputs larger than L2 (params, pair lists and images >> 126 MB)",
-                       "parallelism": f"dp{ws} over views" if ws > 1 else "single GPU"},
+                       "parallelism": f"{ws} GPUs, one scene each (no exchange)" if ws > 1 else "single GPU"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clocks, "loss": loss,
         }
         print(json.dumps(line))
     del tr
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def run_views(args, ws, rank, local, pg):
+    """N ranks share one iteration of one scene: the iteration's views are split
+    across the ranks (data-parallel views, one NCCL reduce-scatter of the
+    gradients and one all-gather of the parameters per iteration).  Total work
+    per iteration is fixed, so the scaling is strong."""
+    import torch
+
+    import nanotracer_b200 as nt
+    from nanotracer_b200.multiview import CudaViewBackend, ViewParallelTrainer, split_views
+    from nanotracer_b200.train import TrainConfig
+    if pg is None:  # the split path on one GPU: a one-rank group
+        import datetime
+        import socket
+
+        import torch.distributed as dist
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", str(port))
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    ctx = nt.CudaCtx(local)
+    scene, tscene, tl, cams_for, render_targets = make_workload(args, 0, ctx)  # one scene on every rank
+    V = args.views
+    bf16 = args.form == "bf16"
+    cfg = TrainConfig(n_views=V, width=args.width, height=args.height, tile_w=args.tile_w, tile_h=args.tile_h,
+                      depth_max=8.0, exact_backward=True, use_graph=True, bf16=bf16, densify=False)
+    views = split_views(V, ws, rank)
+    cams0 = cams_for(0)
+    tgt_local = render_targets(ctx, tscene, [cams0[v] for v in views], tl)
+    tgt_all = np.zeros((V,) + tgt_local.shape[1:], np.float32)
+    tgt_all[views] = tgt_local
+    be = CudaViewBackend(ctx, scene, cfg, tgt_all, views)
+    tr = ViewParallelTrainer(be, V)
+    stream = be.ext_stream
+    cams_steps = [[cams_for(s)[v] for v in views] for s in range(args.warmup + args.steps)]
+    clk = ClockSampler(local, raw_copy=os.environ.get("BENCH_CLOCKS_CSV")).start()
+    t = 0
+    for s in range(args.warmup):
+        t += 1
+        be.set_cameras(cams_steps[s])
+        tr.step(t)
+    be.trainer.set_profiling(True)
+    for s in range(2):
+        t += 1
+        be.set_cameras(cams_steps[s])
+        tr.step(t)
+    be.trainer.set_profiling(True)
+    torch.cuda.synchronize(local)
+    barrier(pg)
+    launches0 = ctx.launch_count
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    w0 = time.time()
+    e0.record(stream)
+    for s in range(args.steps):
+        t += 1
+        be.set_cameras(cams_steps[args.warmup + s])
+        loss = tr.step(t)
+    e1.record(stream)
+    torch.cuda.synchronize(local)
+    w1 = time.time()
+    clk.stop()
+    barrier(pg)
+    ms_max = max_over_ranks(pg, e0.elapsed_time(e1))
+    launches = ctx.launch_count - launches0
+    st = be.trainer.stats()
+    clocks = clk.summary(w0, w1)
+    e2e = None
+    if not args.no_e2e:
+        pinned = torch.empty(tgt_local.size, dtype=torch.float32, pin_memory=True)
+        pinned.numpy()[:] = tgt_local.reshape(-1)
+        import ctypes as C
+        from nanotracer_b200._lib import check, lib
+        torch.cuda.synchronize(local)
+        barrier(pg)
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        p0 = time.perf_counter()
+        f0.record(stream)
+        for s in range(args.steps):
+            t += 1
+            check(lib().sc_buffer_upload(ctx.handle, be.targets.cptr, C.c_void_p(pinned.data_ptr()),
+                                         pinned.numel() * 4), ctx.handle)
+            be.set_cameras(cams_steps[args.warmup + s])
+            tr.step(t)
+        f1.record(stream)
+        torch.cuda.synchronize(local)
+        wall = time.perf_counter() - p0
+        e2e_ms = max_over_ranks(pg, max(f0.elapsed_time(f1), wall * 1e3))
+        e2e = {"value": args.steps / (e2e_ms / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": int(pinned.numel() * 4 + len(views) * 96), "d2h_bytes_per_step": 24}
+    stage = st["stage_ms"]
+    dom = max(stage, key=stage.get)
+    peaks = load_peaks()
+    N, K, P, Vl = len(scene), st["pairs"], args.width * args.height, len(views)
+    algo = {"blend_bwd": K * (4 + 48) + Vl * P * (16 + 16 + 8) + Vl * N * 48 * 2,
+            "blend_fwd": K * (4 + 48) + Vl * P * (16 + 8 + 12 + 16),
+            "tile_sort": 2 * K * 16 + K * 4, "emit": Vl * N * (4 + 16 + 4) + K * 8}
+    ab = algo.get(dom)
+    achieved = ab / (stage[dom] / 1e3) / 1e9 if ab and stage[dom] > 0 else None
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": None if achieved is None else round(achieved, 1),
+                "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": None if achieved is None else round(achieved / peaks["hbm_gbs"], 4), "traffic": None,
+                "peak_source": peaks["source"], "algorithmic_bytes": ab, "avg_ms": round(stage[dom], 4),
+                "stage_ms": {k: round(v, 4) for k, v in stage.items()}}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": args.steps / (ms_max / 1e3), "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32 blend/grad, bf16 SH-rest + Adam moments" if bf16 else "f32",
+            "data": "synthetic seeded scene and targets (no dataset)",
+            "config": {"workload": f"{N} splats, {V} views x {args.width}x{args.height} per iteration split over "
+                                   f"{ws} GPUs, {args.tile_w}x{args.tile_h} tiles, exact transmittance backward",
+                       "form": "batched-" + ("bf16" if bf16 else "fp32"), "splats": N, "views_per_iter": V,
+                       "views_per_gpu": Vl, "width": args.width, "height": args.height,
+                       "l2": "inputs larger than L2 (params, pair lists and images >> 126 MB)",
+                       "parallelism": f"dp{ws} over views (NCCL reduce-scatter + all-gather, ZeRO-1 Adam)"},
+            "roofline": roofline, "cpu_baseline": None, "e2e": e2e, "gpu_launches": int(launches),
+            "clocks": clocks, "loss": loss,
+        }
+        print(json.dumps(line))
+    tr.close()
+    del tr, be
+    torch.cuda.synchronize(local)
     if pg is not None:
         pg.destroy_process_group()
 
@@ -370,6 +506,9 @@ def main():
     ap.add_argument("--tile-w", type=int, default=16)
     ap.add_argument("--tile-h", type=int, default=16)
     ap.add_argument("--form", default="bf16", choices=["bf16", "fp32"])
+    ap.add_argument("--parallel", default="views", choices=["views", "scenes"],
+                    help="N>1: split each iteration's views over the GPUs (strong), or one scene per GPU (weak)")
+    ap.add_argument("--view-path", action="store_true", help="run the split-views path even on one GPU")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -253,6 +253,20 @@ sc_status sc_composite(sc_ctx* ctx, const sc_projected_splat* projected, uint32_
 sc_status sc_mse_loss_grad(sc_ctx* ctx, const float* pred, const float* target, uint32_t n_views,
                            const sc_tiling* tiling, float scale, float* dl_dc, double* loss_out);
 
+/* loss.rs:340-375 (ssim_loss_grad) on the device: dl_dc = scale * dL/dC of
+ * L = 1 - mean SSIM over the pixels and the three channels (11-tap Gaussian
+ * window, sigma 1.5, reflect-101 padding, C1 = 1e-4, C2 = 9e-4); loss_out
+ * (device double per view, nullable) receives L.  Images of at least 6x6. */
+sc_status sc_ssim_loss_grad(sc_ctx* ctx, const float* pred, const float* target, uint32_t n_views,
+                            const sc_tiling* tiling, float scale, float* dl_dc, double* loss_out);
+
+/* loss.rs:383-410 (combined_loss_grad): (1 - lambda) MSE + lambda (1 - SSIM),
+ * lambda clamped to [0, 1]; lambda 0 is sc_mse_loss_grad exactly.  loss_out
+ * (device double, nullable) receives per view {total, mse, ssim}. */
+sc_status sc_combined_loss_grad(sc_ctx* ctx, const float* pred, const float* target, uint32_t n_views,
+                                const sc_tiling* tiling, float lambda, float scale, float* dl_dc,
+                                double* loss_out);
+
 /* rasterize_backward.wgsl:73-210: accumulates into projected_grad, which the
  * caller zeroes first (raster.rs:647-651). */
 sc_status sc_composite_backward(sc_ctx* ctx, const sc_projected_splat* projected, uint32_t stride_splats,
@@ -312,6 +326,8 @@ typedef struct sc_train_config {
   uint32_t tile_cull;          /* drop (tile, splat) pairs whose alpha stays below 1/255 over the
                                   whole tile (images unchanged: the blend skips those pairs) */
   float log_scale_min, log_scale_max, opacity_logit_max; /* train.rs:37-39 */
+  float ssim_lambda;           /* loss = (1 - l) MSE + l (1 - SSIM), loss.rs:383-410 (TrainConfig::ssim_lambda,
+                                  train.rs:52); 0 = MSE only, fused into the blend */
 } sc_train_config;
 
 sc_status sc_trainer_create(sc_ctx* ctx, const sc_train_config* cfg, sc_trainer** out);

@@ -59,7 +59,8 @@ class sc_train_config(C.Structure):
     _fields_ = [("n_views", C.c_uint32), ("tiling", sc_tiling), ("adam", sc_adam_groups), ("bwd_mode", C.c_uint32),
                 ("use_graph", C.c_uint32), ("blend_batch", C.c_uint32), ("sort_mode", C.c_uint32),
                 ("tile_cull", C.c_uint32),
-                ("log_scale_min", C.c_float), ("log_scale_max", C.c_float), ("opacity_logit_max", C.c_float)]
+                ("log_scale_min", C.c_float), ("log_scale_max", C.c_float), ("opacity_logit_max", C.c_float),
+                ("ssim_lambda", C.c_float)]
 
 
 assert C.sizeof(sc_camera) == 96
@@ -115,6 +116,8 @@ _PROTOS = {
     "sc_exclusive_scan_u32_noalloc": (ST, [P, P, U64, P]),
     "sc_composite": (ST, [P, P, U32, U32, P, C.POINTER(sc_tiling), P, P]),
     "sc_mse_loss_grad": (ST, [P, P, P, U32, C.POINTER(sc_tiling), F32, P, P]),
+    "sc_ssim_loss_grad": (ST, [P, P, P, U32, C.POINTER(sc_tiling), F32, P, P]),
+    "sc_combined_loss_grad": (ST, [P, P, P, U32, C.POINTER(sc_tiling), F32, F32, P, P]),
     "sc_composite_backward": (ST, [P, P, U32, U32, P, C.POINTER(sc_tiling), P, P, I32, P, P]),
     "sc_project_backward": (ST, [P, P, P, P, P, I32]),
     "sc_tonemap": (ST, [P, P, U32, U32, P]),

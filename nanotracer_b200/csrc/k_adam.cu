@@ -111,26 +111,29 @@ sc_status launch_accumulate(sc_ctx* ctx, const float* g, uint32_t gcap, float* a
 // ---------------------------------------------------------------- data-parallel shards
 // Adam + constraints + densify statistic over splats [lo, lo+count), gradient
 // rows g[r * shard + j] (one reduce-scattered chunk).  Same arithmetic as the
-// fused single-device kernel; one thread per splat so the 59 row accesses of a
+// fused single-device kernel (folded bias corrections); one thread per splat so the 59 row accesses of a
 // warp are 32 consecutive splats.
 __global__ void k_adam_shard(DSplats s, DMoments mo, float* __restrict__ acc, const float* __restrict__ g, uint32_t lo,
                              uint32_t count, uint32_t shard, AdamParams ap) {
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= count) return;
   const uint32_t i = lo + j;
+  const AdamFast af = adam_fast(ap);
   float gg[14], np[14];
 #pragma unroll
   for (int r = 0; r < 14; ++r) gg[r] = g[(size_t)r * shard + j];
   if (acc) acc[i] = acc[i] + fabsf(gg[0]) + fabsf(gg[1]) + fabsf(gg[2]);
 #pragma unroll
   for (int r = 0; r < 14; ++r)
-    np[r] = adam_scalar(mo, (size_t)r * mo.cap + i, s.slab[(size_t)r * s.cap + i], gg[r], ap.lr[adam_group(r)], ap);
+    np[r] = adam_scalar_fast(mo, (size_t)r * mo.cap + i, s.slab[(size_t)r * s.cap + i], gg[r], af.a[adam_group(r)],
+                             af.s2, ap);
   constrain_geometry(np, ap);
 #pragma unroll
   for (int r = 0; r < 14; ++r) s.slab[(size_t)r * s.cap + i] = np[r];
 #pragma unroll 5
   for (int r = SC_ROW_REST; r < SC_NROWS; ++r)
-    sp_set(s, r, i, adam_scalar(mo, (size_t)r * mo.cap + i, sp_row(s, r, i), g[(size_t)r * shard + j], ap.lr[5], ap));
+    sp_set(s, r, i, adam_scalar_fast(mo, (size_t)r * mo.cap + i, sp_row(s, r, i), g[(size_t)r * shard + j], af.a[5],
+                                     af.s2, ap));
 }
 
 sc_status launch_adam_shard(sc_ctx* ctx, const DSplats& s, const DMoments& mo, float* acc, const float* g, uint32_t lo,

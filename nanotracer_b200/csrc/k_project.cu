@@ -88,22 +88,30 @@ struct Geo {
   float ca, cb, cc;         // conic
 };
 
+// Division and exp for the geometry: IEEE-rounded in the forward (its radius
+// and tile rectangle must match the reference's float arithmetic), the SFU
+// approximations (a few ulp) in the backward, whose gradients are compared by
+// tolerance.
+template <bool FAST> __device__ __forceinline__ float gdiv(float a, float b) { return FAST ? __fdividef(a, b) : a / b; }
+template <bool FAST> __device__ __forceinline__ float gexp(float a) { return FAST ? __expf(a) : expf(a); }
+
 // returns false when culled by the near plane or a non-positive determinant
+template <bool FAST>
 __device__ __forceinline__ bool geometry(const Cam& c, float px, float py, float pz, float qw, float qx, float qy,
                                          float qz, float l0, float l1, float l2, int precise, Geo& g) {
   const float vx = c.v[0] * px + c.v[4] * py + c.v[8] * pz + c.v[12];
   const float vy = c.v[1] * px + c.v[5] * py + c.v[9] * pz + c.v[13];
   const float vz = c.v[2] * px + c.v[6] * py + c.v[10] * pz + c.v[14];
   const float vw = c.v[3] * px + c.v[7] * py + c.v[11] * pz + c.v[15];
-  const float depth = -(vz / vw);
+  const float depth = -gdiv<FAST>(vz, vw);
   if (!(depth >= c.near_plane)) return false;
-  g.tx = vx / vw; g.ty = vy / vw; g.tz = depth;
+  g.tx = gdiv<FAST>(vx, vw); g.ty = gdiv<FAST>(vy, vw); g.tz = depth;
   quat_rot(qw, qx, qy, qz, g.R);
   for (int r = 0; r < 3; ++r)
     for (int k = 0; k < 3; ++k) g.W[r][k] = c.v[4 * k + r];
-  g.sig[0] = expf(l0); g.sig[1] = expf(l1); g.sig[2] = expf(l2);
+  g.sig[0] = gexp<FAST>(l0); g.sig[1] = gexp<FAST>(l1); g.sig[2] = gexp<FAST>(l2);
   const float f = c.focal;
-  const float iz = 1.0f / g.tz, iz2 = iz * iz;
+  const float iz = gdiv<FAST>(1.0f, g.tz), iz2 = iz * iz;
   g.j0[0] = f * iz; g.j0[1] = 0.0f; g.j0[2] = -f * g.tx * iz2;
   g.j1[0] = 0.0f; g.j1[1] = -f * iz; g.j1[2] = f * g.ty * iz2;
   // B = J W R S (2x3)
@@ -140,7 +148,7 @@ __device__ __forceinline__ bool geometry(const Cam& c, float px, float py, float
     return true;
   }
   if (!(g.det > 0.0f)) return false;
-  const float inv = 1.0f / g.det;
+  const float inv = gdiv<FAST>(1.0f, g.det);
   g.ca = g.s11 * inv; g.cb = -g.s01 * inv; g.cc = g.s00 * inv;
   return true;
 }
@@ -181,7 +189,7 @@ __global__ void __launch_bounds__(128, 4) k_project(DSplats s, const sc_camera* 
     if (live) {
       const Cam c = load_cam(cams + v);
       Geo g;
-      if (geometry(c, px, py, pz, qw, qx, qy, qz, l0, l1, l2, precise, g)) {
+      if (geometry<false>(c, px, py, pz, qw, qx, qy, qz, l0, l1, l2, precise, g)) {
         const float f = c.focal;
         const float mx = c.width * 0.5f + (f * g.tx) / g.tz;
         const float my = c.height * 0.5f - (f * g.ty) / g.tz;
@@ -260,21 +268,27 @@ sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams,
 // Per-view gradient of one splat (project_backward.wgsl:79-304).  Writes the
 // 11 geometric gradients into gpos/grot/gsc/gop and returns the colour
 // gradient and SH basis for the caller to form the 48 SH gradients.
+template <bool FAST>
 __device__ __forceinline__ bool splat_backward_view(const Cam& c, float px, float py, float pz, float qw, float qx,
                                                     float qy, float qz, float l0, float l1, float l2, float opacity,
                                                     const float4 pg0, const float4 pg1, const float4 pg2,
                                                     float gpos[3], float grot[4], float gsc[3], float& gop,
                                                     float basis[15]) {
   Geo g;
-  if (!geometry(c, px, py, pz, qw, qx, qy, qz, l0, l1, l2, 0, g)) return false;
+  if (!geometry<FAST>(c, px, py, pz, qw, qx, qy, qz, l0, l1, l2, 0, g)) return false;
   const float f = c.focal;
-  const float iz = 1.0f / g.tz, iz2 = iz * iz;
+  const float iz = gdiv<FAST>(1.0f, g.tz), iz2 = iz * iz;
   // opacity logit
   gop += pg0.z * opacity * (1.0f - opacity);
   // SH basis at the view direction
   float dx = c.cp[0] - px, dy = c.cp[1] - py, dz = c.cp[2] - pz;
-  const float len = sqrtf(dx * dx + dy * dy + dz * dz);
-  sh_basis15(dx / len, dy / len, dz / len, basis);
+  if (FAST) {
+    const float il = rsqrtf(dx * dx + dy * dy + dz * dz);
+    sh_basis15(dx * il, dy * il, dz * il, basis);
+  } else {
+    const float len = sqrtf(dx * dx + dy * dy + dz * dz);
+    sh_basis15(dx / len, dy / len, dz / len, basis);
+  }
   // dSigma2D = -C dConic C with the off-diagonal conic gradient halved
   const float C00 = g.ca, C01 = g.cb, C11 = g.cc;
   const float D00 = pg1.x, D01 = 0.5f * pg1.y, D11 = pg1.z;
@@ -342,7 +356,7 @@ __global__ void __launch_bounds__(128) k_project_backward(DSplats s, const float
   float gpos[3] = {0, 0, 0}, grot[4] = {0, 0, 0, 0}, gsc[3] = {0, 0, 0}, gop = 0, basis[15];
   const float4 p0 = pg[3 * (size_t)i], p1 = pg[3 * (size_t)i + 1], p2 = pg[3 * (size_t)i + 2];
   const float op = 1.0f / (1.0f + expf(-sp_row(s, 10, i)));
-  const bool ok = splat_backward_view(c, sp_row(s, 0, i), sp_row(s, 1, i), sp_row(s, 2, i), sp_row(s, 3, i),
+  const bool ok = splat_backward_view<false>(c, sp_row(s, 0, i), sp_row(s, 1, i), sp_row(s, 2, i), sp_row(s, 3, i),
                                       sp_row(s, 4, i), sp_row(s, 5, i), sp_row(s, 6, i), sp_row(s, 7, i),
                                       sp_row(s, 8, i), sp_row(s, 9, i), op, p0, p1, p2, gpos, grot, gsc, gop, basis);
   float row[SC_NROWS];
@@ -387,7 +401,7 @@ __device__ __forceinline__ void sum_view_grads(const DSplats& s, uint32_t i, con
   const float px = sp_row(s, 0, i), py = sp_row(s, 1, i), pz = sp_row(s, 2, i);
   const float qw = sp_row(s, 3, i), qx = sp_row(s, 4, i), qy = sp_row(s, 5, i), qz = sp_row(s, 6, i);
   const float l0 = sp_row(s, 7, i), l1 = sp_row(s, 8, i), l2 = sp_row(s, 9, i);
-  const float opacity = 1.0f / (1.0f + expf(-sp_row(s, 10, i)));
+  const float opacity = __fdividef(1.0f, 1.0f + __expf(-sp_row(s, 10, i)));
   float* gpos = G.gpos; float* grot = G.grot; float* gsc = G.gsc; float& gop = G.gop;
   float* gdc = G.gdc; float* grest = G.grest;
   for (int k = 0; k < 3; ++k) { gpos[k] = 0.f; gsc[k] = 0.f; gdc[k] = 0.f; }
@@ -404,8 +418,8 @@ __device__ __forceinline__ void sum_view_grads(const DSplats& s, uint32_t i, con
       continue;  // splat untouched in this view: every gradient term is zero
     const Cam c = load_cam(cams + v);
     float basis[15];
-    if (!splat_backward_view(c, px, py, pz, qw, qx, qy, qz, l0, l1, l2, opacity, p0, p1, p2, gpos, grot, gsc, gop,
-                             basis))
+    if (!splat_backward_view<true>(c, px, py, pz, qw, qx, qy, qz, l0, l1, l2, opacity, p0, p1, p2, gpos, grot, gsc,
+                                   gop, basis))
       continue;
     gdc[0] += p2.x * SH_C0; gdc[1] += p2.y * SH_C0; gdc[2] += p2.z * SH_C0;
 #pragma unroll
@@ -433,10 +447,12 @@ __global__ void __launch_bounds__(128, 4) k_fused_backward_adam(DSplats s, DMome
   // geometric rows
   const float gg[14] = {G.gpos[0], G.gpos[1], G.gpos[2], G.grot[0], G.grot[1], G.grot[2], G.grot[3],
                         G.gsc[0],  G.gsc[1],  G.gsc[2],  G.gop,     G.gdc[0],  G.gdc[1],  G.gdc[2]};
+  const AdamFast af = adam_fast(ap);
   float np[14];
 #pragma unroll
   for (int r = 0; r < 14; ++r)
-    np[r] = adam_scalar(mo, (size_t)r * mo.cap + i, s.slab[(size_t)r * cap + i], gg[r], ap.lr[adam_group(r)], ap);
+    np[r] = adam_scalar_fast(mo, (size_t)r * mo.cap + i, s.slab[(size_t)r * cap + i], gg[r], af.a[adam_group(r)],
+                             af.s2, ap);
   constrain_geometry(np, ap);
 #pragma unroll
   for (int r = 0; r < 14; ++r) s.slab[(size_t)r * cap + i] = np[r];
@@ -444,7 +460,7 @@ __global__ void __launch_bounds__(128, 4) k_fused_backward_adam(DSplats s, DMome
   for (int k = 0; k < 45; ++k) {
     const int r = SC_ROW_REST + k;
     const float p = sp_row(s, r, i);
-    sp_set(s, r, i, adam_scalar(mo, (size_t)r * mo.cap + i, p, G.grest[k], ap.lr[5], ap));
+    sp_set(s, r, i, adam_scalar_fast(mo, (size_t)r * mo.cap + i, p, G.grest[k], af.a[5], af.s2, ap));
   }
 }
 

@@ -698,6 +698,67 @@ sc_status sc_mse_loss_grad(sc_ctx* ctx, const float* pred, const float* target, 
                          reinterpret_cast<float4*>(dl_dc), loss_out);
 }
 
+// scratch for the SSIM coefficient planes plus 2 doubles per view (MSE means, SSIM sums)
+static sc_status ssim_scratch(sc_ctx* ctx, uint64_t P, uint32_t n_views, float** terms, double** sums) {
+  const size_t tb = (sck::ssim_terms_bytes(P, n_views) + 255) & ~(size_t)255;
+  void* scr = nullptr;
+  SC_TRY(sc_scratch(ctx, tb + 16 * (size_t)n_views, &scr));
+  *terms = reinterpret_cast<float*>(scr);
+  *sums = reinterpret_cast<double*>(reinterpret_cast<char*>(scr) + tb);
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(*sums, 0, 16 * (size_t)n_views, ctx->stream), "zero sums");
+  return SC_OK;
+}
+
+sc_status sc_ssim_loss_grad(sc_ctx* ctx, const float* pred, const float* target, uint32_t n_views, const sc_tiling* tl,
+                            float scale, float* dl_dc, double* loss_out) {
+  if (!ctx || !pred || !target || !dl_dc || !tiling_ok(tl)) return SC_ERR_INVALID_ARG;
+  if (n_views == 0) return SC_OK;
+  const uint64_t P = (uint64_t)tl->width * tl->height;
+  float* terms; double* sums;
+  SC_TRY(ssim_scratch(ctx, P, n_views, &terms, &sums));
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(dl_dc, 0, (size_t)n_views * P * 16, ctx->stream), "zero dl_dc");
+  SC_TRY(sck::launch_ssim(ctx, reinterpret_cast<const float4*>(pred), target, tl->width, tl->height, n_views, scale,
+                          reinterpret_cast<float4*>(dl_dc), sums + n_views, terms));
+  if (!loss_out) return SC_OK;
+  // {total, mse, ssim} triples into the scratch's MSE slot region is too small; write L directly
+  double* parts = nullptr;
+  SC_CUDA_TRY(ctx, cudaMallocAsync(&parts, 24 * (size_t)n_views, ctx->stream), "loss parts");
+  sc_status st = sck::launch_loss_parts(ctx, nullptr, sums + n_views, n_views, P, 1.0f, parts);
+  if (st == SC_OK)
+    st = cudaMemcpy2DAsync(loss_out, 8, parts, 24, 8, n_views, cudaMemcpyDeviceToDevice, ctx->stream) == cudaSuccess
+             ? SC_OK
+             : sc_fail(ctx, SC_ERR_CUDA, "loss copy");
+  cudaFreeAsync(parts, ctx->stream);
+  return st;
+}
+
+sc_status sc_combined_loss_grad(sc_ctx* ctx, const float* pred, const float* target, uint32_t n_views,
+                                const sc_tiling* tl, float lambda, float scale, float* dl_dc, double* loss_out) {
+  if (!ctx || !pred || !target || !dl_dc || !tiling_ok(tl)) return SC_ERR_INVALID_ARG;
+  if (n_views == 0) return SC_OK;
+  if (!(lambda >= 0.0f)) lambda = 0.0f;  // also maps NaN to 0
+  if (lambda > 1.0f) lambda = 1.0f;
+  const uint64_t P = (uint64_t)tl->width * tl->height;
+  float* terms = nullptr; double* sums = nullptr;
+  if (lambda > 0.0f) SC_TRY(ssim_scratch(ctx, P, n_views, &terms, &sums));
+  double* mse = nullptr;
+  if (lambda < 1.0f) {
+    SC_CUDA_TRY(ctx, cudaMallocAsync(&mse, 8 * (size_t)n_views, ctx->stream), "mse sums");
+    SC_CUDA_TRY(ctx, cudaMemsetAsync(mse, 0, 8 * (size_t)n_views, ctx->stream), "zero mse");
+    SC_TRY(sck::launch_mse(ctx, reinterpret_cast<const float4*>(pred), target, P, n_views, scale * (1.0f - lambda),
+                           reinterpret_cast<float4*>(dl_dc), mse));
+  } else {
+    SC_CUDA_TRY(ctx, cudaMemsetAsync(dl_dc, 0, (size_t)n_views * P * 16, ctx->stream), "zero dl_dc");
+  }
+  sc_status st = SC_OK;
+  if (lambda > 0.0f)
+    st = sck::launch_ssim(ctx, reinterpret_cast<const float4*>(pred), target, tl->width, tl->height, n_views,
+                          scale * lambda, reinterpret_cast<float4*>(dl_dc), sums, terms);
+  if (st == SC_OK && loss_out) st = sck::launch_loss_parts(ctx, mse, sums, n_views, P, lambda, loss_out);
+  if (mse) cudaFreeAsync(mse, ctx->stream);
+  return st;
+}
+
 sc_status sc_composite_backward(sc_ctx* ctx, const sc_projected_splat* projected, uint32_t stride, uint32_t n_views,
                                 const sc_bins* b, const sc_tiling* tl, const float* fwd, const float* dl_dc,
                                 sc_bwd_mode mode, const uint32_t* aux, sc_projected_grad* pg) {

@@ -216,6 +216,26 @@ __device__ __forceinline__ float adam_scalar(const DMoments& mo, size_t k, float
   const float mh = m / ap.bc1, vh = v / ap.bc2;
   return p - lr * mh / (sqrtf(vh) + ap.eps);
 }
+// The same update with the bias corrections folded into per-group constants,
+// a = lr / bc1 and s2 = 1 / sqrt(bc2): lr (m / bc1) / (sqrt(v / bc2) + eps)
+// = a m / (sqrt(v) s2 + eps), with SFU reciprocals (a few ulp of the update,
+// far below the parameters' own rounding).
+struct AdamFast { float a[6]; float s2; };
+__device__ __forceinline__ AdamFast adam_fast(const AdamParams& ap) {
+  AdamFast f;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) f.a[k] = __fdividef(ap.lr[k], ap.bc1);
+  f.s2 = rsqrtf(ap.bc2);
+  return f;
+}
+__device__ __forceinline__ float adam_scalar_fast(const DMoments& mo, size_t k, float p, float gr, float a, float s2,
+                                                  const AdamParams& ap) {
+  const float m = ap.beta1 * mo_ld(mo, mo.m, mo.m16, k) + (1.0f - ap.beta1) * gr;
+  const float v = ap.beta2 * mo_ld(mo, mo.v, mo.v16, k) + (1.0f - ap.beta2) * gr * gr;
+  mo_st(mo, mo.m, mo.m16, k, m);
+  mo_st(mo, mo.v, mo.v16, k, v);
+  return p - __fdividef(a * m, fmaf(sqrtf(v), s2, ap.eps));
+}
 // constraints on the updated geometric rows 0..13 (apply_constraints.wgsl:24-41)
 __device__ __forceinline__ void constrain_geometry(float np[14], const AdamParams& ap) {
   const float n2 = np[3] * np[3] + np[4] * np[4] + np[5] * np[5] + np[6] * np[6];
@@ -280,6 +300,16 @@ sc_status launch_composite_backward(sc_ctx* ctx, const float4* rec, uint32_t str
                                     const float4* fwd, const float4* dl_dc, int mode, const uint2* aux,
                                     float4* proj_grad, const uint32_t* d_skip);
 sc_status launch_tonemap(sc_ctx* ctx, const float4* img, uint32_t w, uint32_t h, uint8_t* out);
+
+// SSIM (loss.rs:22-375): scale * dL_ssim/dC added into dl_dc, per-view sum of
+// the SSIM map added into ssim_sum; terms = ssim_terms_bytes() of scratch
+void ssim_window(float g[11]);
+size_t ssim_terms_bytes(uint64_t pixels_per_view, uint32_t n_views);
+sc_status launch_ssim(sc_ctx* ctx, const float4* pred, const float* target, uint32_t w, uint32_t h, uint32_t n_views,
+                      float scale, float4* dl_dc, double* ssim_sum, float* terms);
+// per view {total, mse, ssim} from the MSE means and SSIM-map sums (loss.rs:383-410)
+sc_status launch_loss_parts(sc_ctx* ctx, const double* mse, const double* ssim_sum, uint32_t n_views, uint64_t P,
+                            float lambda, double* out);
 
 // optimiser
 sc_status launch_adam_lanes(sc_ctx* ctx, float* p, const float* g, float* m, float* v, uint64_t n, float lr,

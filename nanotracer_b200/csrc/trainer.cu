@@ -39,12 +39,18 @@ struct StepOut {
   uint32_t pad;
 };
 
-// loss = mean over the views, or (weight > 0) weight * sum over the views
-__global__ void k_finalize(const double* __restrict__ loss_sums, uint32_t n_views, double inv_count, double weight,
-                           const uint64_t* __restrict__ d_total, const uint32_t* __restrict__ err,
-                           StepOut* __restrict__ out) {
+// loss = mean over the views, or (weight > 0) weight * sum over the views, of
+// (1 - lambda) MSE + lambda (1 - SSIM) (loss.rs:383-410; MSE alone without SSIM sums)
+__global__ void k_finalize(const double* __restrict__ loss_sums, const double* __restrict__ ssim_sums, float lambda,
+                           uint32_t n_views, double inv_count, double weight, const uint64_t* __restrict__ d_total,
+                           const uint32_t* __restrict__ err, StepOut* __restrict__ out) {
   double acc = 0.0;
-  for (uint32_t v = 0; v < n_views; ++v) acc += loss_sums[v] * inv_count;
+  for (uint32_t v = 0; v < n_views; ++v) {
+    const double m = loss_sums[v] * inv_count;
+    if (!ssim_sums) { acc += m; continue; }
+    const double sv = 1.0 - ssim_sums[v] * inv_count;
+    acc += lambda == 1.0f ? sv : (1.0 - (double)lambda) * m + (double)lambda * sv;
+  }
   out->loss = weight > 0.0 ? acc * weight : acc / (double)n_views;
   out->pairs = *d_total;
   out->err = *err;
@@ -83,6 +89,8 @@ struct sc_trainer {
   // per (view, tile) / pixel
   uint32_t* ranges = nullptr;
   float4* image = nullptr; uint2* aux = nullptr; float4* dl_dc = nullptr;
+  // SSIM term of the loss (cfg.ssim_lambda > 0): coefficient planes and per-view map sums
+  float* ssim_terms = nullptr; double* d_ssim = nullptr;
   const float* targets = nullptr;
   double* d_loss = nullptr;
   uint64_t* d_total = nullptr;
@@ -244,8 +252,15 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   SC_TRY(sck::launch_tile_ranges(ctx, skeys, 2, tr->d_total, tr->kcap, all_tiles, tr->ranges));
   mark(tr, 6, capturing);
   const float weight = tr->grads_mode ? tr->loss_weight : 1.0f / (float)V;
+  const float lam = tr->cfg.ssim_lambda;
   SC_TRY(sck::launch_composite(ctx, tr->rec, tr->stride, V, svals, tr->ranges, &tr->cfg.tiling, tr->image, tr->aux,
-                               tr->targets, weight, tr->dl_dc, tr->d_loss, ctx->d_error));
+                               tr->targets, lam > 0.0f ? weight * (1.0f - lam) : weight, tr->dl_dc, tr->d_loss,
+                               ctx->d_error));
+  if (lam > 0.0f) {
+    SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->d_ssim, 0, 8 * (size_t)V, ctx->stream), "zero ssim");
+    SC_TRY(sck::launch_ssim(ctx, tr->image, tr->targets, tr->cfg.tiling.width, tr->cfg.tiling.height, V,
+                            weight * lam, tr->dl_dc, tr->d_ssim, tr->ssim_terms));
+  }
   mark(tr, 7, capturing);
   SC_TRY(sck::launch_composite_backward(ctx, tr->rec, tr->stride, V, svals, tr->ranges, &tr->cfg.tiling, tr->image,
                                         tr->dl_dc, (int)tr->cfg.bwd_mode, tr->aux, tr->pgrad, ctx->d_error));
@@ -262,9 +277,9 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   else
     SC_TRY(sck::launch_fused_backward_adam(ctx, ds, dm, tr->pgrad, tr->stride, d_cams, V, acc, ap, ctx->d_error, d_bc));
   mark(tr, 9, capturing);
-  k_finalize<<<1, 1, 0, ctx->stream>>>(tr->d_loss, V, 1.0 / (3.0 * (double)tr->P),
-                                       tr->grads_mode ? (double)tr->loss_weight : 0.0, tr->d_total, ctx->d_error,
-                                       tr->d_out);
+  k_finalize<<<1, 1, 0, ctx->stream>>>(tr->d_loss, lam > 0.0f ? tr->d_ssim : nullptr, lam, V,
+                                       1.0 / (3.0 * (double)tr->P), tr->grads_mode ? (double)tr->loss_weight : 0.0,
+                                       tr->d_total, ctx->d_error, tr->d_out);
   SC_TRY(sc_check_launch(ctx, "k_finalize"));
   SC_CUDA_TRY(ctx, cudaMemcpyAsync(tr->h_out, tr->d_out, sizeof(StepOut), cudaMemcpyDeviceToHost, ctx->stream), "out D2H");
   tr->kernels_per_step = (uint32_t)(ctx->launches - launches0);
@@ -281,6 +296,10 @@ sc_status sc_trainer_create(sc_ctx* ctx, const sc_train_config* cfg, sc_trainer*
   const uint32_t threads = t.tile_w * t.tile_h;
   if (threads > 256 || threads % 32) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile must hold 32..256 pixels, multiple of 32");
   if (cfg->bwd_mode != SC_BWD_REF && cfg->bwd_mode != SC_BWD_EXACT) return SC_ERR_INVALID_ARG;
+  if (!(cfg->ssim_lambda >= 0.0f && cfg->ssim_lambda <= 1.0f))
+    return sc_fail(ctx, SC_ERR_INVALID_ARG, "ssim_lambda must lie in [0, 1]");
+  if (cfg->ssim_lambda > 0.0f && (t.width < 6 || t.height < 6))
+    return sc_fail(ctx, SC_ERR_INVALID_ARG, "the SSIM loss needs images of at least 6x6 pixels");
   sc_trainer* tr = new sc_trainer();
   tr->ctx = ctx;
   tr->cfg = *cfg;
@@ -300,6 +319,8 @@ sc_status sc_trainer_create(sc_ctx* ctx, const sc_train_config* cfg, sc_trainer*
   if (e == cudaSuccess) e = cudaMalloc(&tr->dl_dc, pix * 16);
   if (e == cudaSuccess) e = cudaMalloc(&tr->d_loss, 8 * (size_t)tr->V);
   if (e == cudaSuccess) e = cudaMalloc(&tr->d_total, 64);
+  if (e == cudaSuccess && cfg->ssim_lambda > 0.0f) e = cudaMalloc(&tr->ssim_terms, sck::ssim_terms_bytes(tr->P, tr->V));
+  if (e == cudaSuccess && cfg->ssim_lambda > 0.0f) e = cudaMalloc(&tr->d_ssim, 8 * (size_t)tr->V);
   for (int i = 0; i <= kStages && e == cudaSuccess; ++i) e = cudaEventCreate(&tr->ev[i]);
   if (e != cudaSuccess) {
     sc_trainer_free(ctx, tr);
@@ -318,6 +339,7 @@ void sc_trainer_free(sc_ctx* ctx, sc_trainer* tr) {
   trainer_free_pairs(tr);
   cudaFree(tr->ranges); cudaFree(tr->image); cudaFree(tr->aux); cudaFree(tr->dl_dc);
   cudaFree(tr->d_loss); cudaFree(tr->d_total); cudaFree(tr->d_params); cudaFree(tr->d_out);
+  cudaFree(tr->ssim_terms); cudaFree(tr->d_ssim);
   cudaFree(tr->scratch);
   if (tr->h_params) cudaFreeHost(tr->h_params);
   if (tr->h_out) cudaFreeHost(tr->h_out);

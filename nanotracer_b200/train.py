@@ -48,6 +48,7 @@ class TrainConfig:
     densify: bool = True
     bf16: bool = False
     tile_cull: bool = True
+    ssim_lambda: float = 0.0
 
     def struct(self) -> sc_train_config:
         c = sc_train_config()
@@ -60,6 +61,7 @@ class TrainConfig:
         c.use_graph = 1 if self.use_graph else 0
         c.tile_cull = 1 if self.tile_cull else 0
         c.log_scale_min, c.log_scale_max, c.opacity_logit_max = LOG_SCALE_MIN, LOG_SCALE_MAX, OPACITY_LOGIT_MAX
+        c.ssim_lambda = self.ssim_lambda
         return c
 
 

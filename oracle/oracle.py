@@ -86,7 +86,10 @@ def lib():
                 f"oracle_project_backward_{sfx}": (None, [C.POINTER(HostSplats), P, C.POINTER(Camera), P, P, P, P, P,
                                                           P, I32]),
                 f"oracle_train_step_{sfx}": (D, [C.POINTER(HostSplats), C.POINTER(HostSplats), C.POINTER(HostSplats),
-                                                 P, U32, P, P, C.POINTER(Tiling), I32, C.POINTER(AdamGroups), U64, P]),
+                                                 P, U32, P, P, C.POINTER(Tiling), I32, C.POINTER(AdamGroups), U64, P,
+                                                 F32]),
+                f"oracle_ssim_loss_grad_{sfx}": (D, [I32, I32, P, P, P, F32]),
+                f"oracle_combined_loss_grad_{sfx}": (D, [I32, I32, P, P, P, F32, F32, P]),
             })
         for name, (res, args) in protos.items():
             f = getattr(L, name)
@@ -305,8 +308,28 @@ def read_ply(path, cap):
     return r, out
 
 
+def ssim(pred4, target3, w, h, scale=1.0, sfx="f32"):
+    """loss.rs:340-375: (1 - mean SSIM over the three channels, scale * dL/dC as rgba)."""
+    pred4 = np.ascontiguousarray(pred4, _dt(sfx)).reshape(-1)
+    t = np.ascontiguousarray(target3, np.float32).reshape(-1)
+    dl = np.zeros(w * h * 4, _dt(sfx))
+    loss = getattr(lib(), f"oracle_ssim_loss_grad_{sfx}")(int(w), int(h), _p(pred4), _p(t), _p(dl), float(scale))
+    return loss, dl
+
+
+def combined(pred4, target3, w, h, lam, scale=1.0, sfx="f32"):
+    """loss.rs:383-410: (total, mse, ssim, scale * dL/dC as rgba)."""
+    pred4 = np.ascontiguousarray(pred4, _dt(sfx)).reshape(-1)
+    t = np.ascontiguousarray(target3, np.float32).reshape(-1)
+    dl = np.zeros(w * h * 4, _dt(sfx))
+    parts = np.zeros(2, np.float64)
+    total = getattr(lib(), f"oracle_combined_loss_grad_{sfx}")(int(w), int(h), _p(pred4), _p(t), _p(dl),
+                                                               float(lam), float(scale), _p(parts))
+    return total, parts[0], parts[1], dl
+
+
 def train_step(s: OSplats, m: OSplats, v: OSplats, acc, cams: list, targets, tl: Tiling, mode: int, lrs, t: int,
-               sfx="f32", want_images=False):
+               sfx="f32", want_images=False, ssim_lambda=0.0):
     V = len(cams)
     arr = (Camera * V)(*cams)
     g = AdamGroups()
@@ -316,7 +339,8 @@ def train_step(s: OSplats, m: OSplats, v: OSplats, acc, cams: list, targets, tl:
     imgs = np.zeros(V * tl.width * tl.height * 4, np.float32) if want_images else None
     t3 = np.ascontiguousarray(targets, np.float32)
     loss = getattr(lib(), f"oracle_train_step_{sfx}")(C.byref(s.h), C.byref(m.h), C.byref(v.h), _p(acc), V, arr,
-                                                      _p(t3), C.byref(tl), int(mode), C.byref(g), int(t), _p(imgs))
+                                                      _p(t3), C.byref(tl), int(mode), C.byref(g), int(t), _p(imgs),
+                                                      float(ssim_lambda))
     return loss, imgs
 
 

@@ -16,6 +16,7 @@
 //                   from emission order, which is what radix_sort.rs:1-26 produces
 //   composite       shaders/rasterize.wgsl:48-118
 //   MSE             crates/nano-optimize/src/loss.rs:163-179
+//   SSIM, combined  crates/nano-optimize/src/loss.rs:22-152, 193-410
 //   backward        shaders/rasterize_backward.wgsl:73-210
 //   project bwd     shaders/project_backward.wgsl:79-304
 //   Adam            crates/nano-optimize/src/adam.rs:70-90, adam_gpu.rs:262-323
@@ -430,6 +431,161 @@ static double mse(uint64_t P, const T* pred4, const float* target3, T* dl_dc4, f
     dl_dc4[4 * i] = dx * inv_n; dl_dc4[4 * i + 1] = dy * inv_n; dl_dc4[4 * i + 2] = dz * inv_n; dl_dc4[4 * i + 3] = T(0);
   }
   return sum / ((double)P * 3.0);
+}
+
+// ---------------------------------------------------------------- SSIM (loss.rs:22-375)
+// Wang et al. 2004 structural similarity over an 11-tap separable Gaussian
+// window (sigma 1.5) with reflect-101 padding, C1 = 1e-4, C2 = 9e-4, and the
+// reference's analytic gradient: three quotient-rule coefficient planes
+// P = dSSIM/dmu_x, Q = dSSIM/dsigma_x^2, R = dSSIM/dsigma_xy pulled back
+// through the adjoint of the blur (loss.rs:193-335).
+static const int SSIM_WIN = 11;
+static const int SSIM_RAD = 5;
+static const float SSIM_C1 = 0.0001f;
+static const float SSIM_C2 = 0.0009f;
+
+// loss.rs:36-51, in f32 like the reference
+static void ssim_window(float g[SSIM_WIN]) {
+  const float centre = (float)(SSIM_WIN - 1) * 0.5f;
+  const float two_sigma_sq = 2.0f * 1.5f * 1.5f;
+  float sum = 0.0f;
+  for (int i = 0; i < SSIM_WIN; ++i) {
+    const float d = (float)i - centre;
+    g[i] = std::exp(-d * d / two_sigma_sq);
+    sum += g[i];
+  }
+  for (int i = 0; i < SSIM_WIN; ++i) g[i] /= sum;
+}
+
+// loss.rs:56-67: reflect-101 index into [0, n)
+static inline int reflect101(int i, int n) {
+  if (n == 1) return 0;
+  const int period = 2 * (n - 1);
+  int x = ((i % period) + period) % period;
+  if (x >= n) x = period - x;
+  return x;
+}
+
+// loss.rs:73-100: horizontal then vertical gather pass
+template <typename T>
+static void ssim_blur(const T* src, int w, int h, const float* g, T* dst) {
+  std::vector<T> tmp((size_t)w * h);
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      T acc = T(0);
+      for (int k = 0; k < SSIM_WIN; ++k) acc += src[(size_t)y * w + reflect101(x + k - SSIM_RAD, w)] * T(g[k]);
+      tmp[(size_t)y * w + x] = acc;
+    }
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      T acc = T(0);
+      for (int k = 0; k < SSIM_WIN; ++k) acc += tmp[(size_t)reflect101(y + k - SSIM_RAD, h) * w + x] * T(g[k]);
+      dst[(size_t)y * w + x] = acc;
+    }
+}
+
+// loss.rs:122-152: transpose of ssim_blur, vertical scatter then horizontal scatter
+template <typename T>
+static void ssim_blur_adjoint(const T* src, int w, int h, const float* g, T* dst) {
+  std::vector<T> tmp((size_t)w * h, T(0));
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      const T s = src[(size_t)y * w + x];
+      for (int k = 0; k < SSIM_WIN; ++k) tmp[(size_t)reflect101(y + k - SSIM_RAD, h) * w + x] += s * T(g[k]);
+    }
+  std::fill(dst, dst + (size_t)w * h, T(0));
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      const T s = tmp[(size_t)y * w + x];
+      for (int k = 0; k < SSIM_WIN; ++k) dst[(size_t)y * w + reflect101(x + k - SSIM_RAD, w)] += s * T(g[k]);
+    }
+}
+
+// loss.rs:193-335 for one channel plane: returns sum of the SSIM map (f64)
+// and writes dSSIM/dx (before the -1/N and channel-average factors).
+template <typename T>
+static double ssim_channel(const T* x, const T* y, int w, int h, const float* g, T* dssim) {
+  const size_t n = (size_t)w * h;
+  std::vector<T> xx(n), yy(n), xy(n), mx(n), my(n), gxx(n), gyy(n), gxy(n);
+  for (size_t i = 0; i < n; ++i) { xx[i] = x[i] * x[i]; yy[i] = y[i] * y[i]; xy[i] = x[i] * y[i]; }
+  ssim_blur(x, w, h, g, mx.data());
+  ssim_blur(y, w, h, g, my.data());
+  ssim_blur(xx.data(), w, h, g, gxx.data());
+  ssim_blur(yy.data(), w, h, g, gyy.data());
+  ssim_blur(xy.data(), w, h, g, gxy.data());
+  std::vector<T> p(n), q(n), r(n), mq(n), mr(n);
+  double sum = 0.0;
+  const T c1 = T(SSIM_C1), c2 = T(SSIM_C2);
+  for (size_t i = 0; i < n; ++i) {
+    const T mux = mx[i], muy = my[i];
+    const T mux2 = mux * mux, muy2 = muy * muy;
+    const T sxx = gxx[i] - mux2, syy = gyy[i] - muy2, sxy = gxy[i] - mux * muy;
+    const T a = T(2) * mux * muy + c1, b = T(2) * sxy + c2;
+    const T c = mux2 + muy2 + c1, d = sxx + syy + c2;
+    sum += (double)((a * b) / (c * d));
+    const T cd = c * d;
+    p[i] = T(2) * b * (muy * c - mux * a) / (c * cd);
+    q[i] = -a * b / (c * d * d);
+    r[i] = T(2) * a / cd;
+    mq[i] = mux * q[i];
+    mr[i] = muy * r[i];
+  }
+  std::vector<T> sp(n), sq(n), sr(n), smq(n), smr(n);
+  ssim_blur_adjoint(p.data(), w, h, g, sp.data());
+  ssim_blur_adjoint(q.data(), w, h, g, sq.data());
+  ssim_blur_adjoint(r.data(), w, h, g, sr.data());
+  ssim_blur_adjoint(mq.data(), w, h, g, smq.data());
+  ssim_blur_adjoint(mr.data(), w, h, g, smr.data());
+  for (size_t i = 0; i < n; ++i)
+    dssim[i] = sp[i] + T(2) * (x[i] * sq[i] - smq[i]) + (y[i] * sr[i] - smr[i]);
+  return sum;
+}
+
+// loss.rs:340-375 on an rgba prediction and rgb target: loss = 1 - mean of the
+// three channel SSIMs; dl_dc4 = scale * dL/dC (alpha lane zero).
+template <typename T>
+static double ssim_loss_grad(int w, int h, const T* pred4, const float* target3, T* dl_dc4, float scale) {
+  float g[SSIM_WIN];
+  ssim_window(g);
+  const size_t n = (size_t)w * h;
+  std::vector<T> xc(n), yc(n), ds(n);
+  T lc[3];
+  const T inv_n = T(1.0f / (float)n);
+  for (int ch = 0; ch < 3; ++ch) {
+    for (size_t i = 0; i < n; ++i) { xc[i] = pred4[4 * i + ch]; yc[i] = T(target3[3 * i + ch]); }
+    const double sum = ssim_channel(xc.data(), yc.data(), w, h, g, ds.data());
+    lc[ch] = T(1) - (T)(sum / (double)n);
+    for (size_t i = 0; i < n; ++i) dl_dc4[4 * i + ch] = (-inv_n * ds[i]) / T(3) * T(scale);
+  }
+  for (size_t i = 0; i < n; ++i) dl_dc4[4 * i + 3] = T(0);
+  return (double)((lc[0] + lc[1] + lc[2]) / T(3));
+}
+
+// loss.rs:383-410: (1 - lambda) MSE + lambda (1 - SSIM); lambda 0 is the pure
+// MSE path bit for bit, lambda 1 the pure SSIM path.  scale multiplies the
+// gradient (1/V for a V-view mean).  parts (nullable) = {mse, ssim}.
+template <typename T>
+static double combined_loss_grad(int w, int h, const T* pred4, const float* target3, T* dl_dc4, float lambda,
+                                 float scale, double* parts) {
+  lambda = std::min(std::max(lambda, 0.0f), 1.0f);
+  const uint64_t P = (uint64_t)w * h;
+  if (lambda == 0.0f) {
+    const double m = mse<T>(P, pred4, target3, dl_dc4, scale);
+    if (parts) { parts[0] = m; parts[1] = 0.0; }
+    return m;
+  }
+  if (lambda == 1.0f) {
+    const double sv = ssim_loss_grad<T>(w, h, pred4, target3, dl_dc4, scale);
+    if (parts) { parts[0] = 0.0; parts[1] = sv; }
+    return sv;
+  }
+  std::vector<T> gm(4 * P), gs(4 * P);
+  const double m = mse<T>(P, pred4, target3, gm.data(), 1.0f);
+  const double sv = ssim_loss_grad<T>(w, h, pred4, target3, gs.data(), 1.0f);
+  const T om = T(1.0f - lambda), l = T(lambda);
+  for (uint64_t k = 0; k < 4 * P; ++k) dl_dc4[k] = (gm[k] * om + gs[k] * l) * T(scale);
+  if (parts) { parts[0] = m; parts[1] = sv; }
+  return (double)(om * (T)m + l * (T)sv);
 }
 
 template <typename T> static inline void atomic_add(T* p, T v) {
@@ -891,7 +1047,8 @@ struct AdamGroups { float lr[6]; float beta1, beta2, eps; };
 template <typename T>
 static double train_step(HostSplats& s, HostSplats& m, HostSplats& v, float* grad_acc, uint32_t n_views,
                          const Camera* cams, const float* targets, const Tiling& tl, int mode,
-                         const AdamGroups& ag, uint64_t t, float* out_images /* nullable, V*P*4 f32 */) {
+                         const AdamGroups& ag, uint64_t t, float* out_images /* nullable, V*P*4 f32 */,
+                         float ssim_lambda) {
   const uint32_t n = s.n;
   const uint64_t P = (uint64_t)tl.width * tl.height;
   const uint32_t ntiles = tl.num_tiles();
@@ -910,7 +1067,9 @@ static double train_step(HostSplats& s, HostSplats& m, HostSplats& v, float* gra
     std::vector<uint32_t> pay(K), ranges(2 * (size_t)ntiles);
     bin64<T>(1, n, rec.data(), tl, keys.data(), pay.data(), K, ranges.data());
     composite<T>(rec.data(), pay.data(), ranges.data(), tl, img.data(), ncon.data(), tfin.data());
-    loss += mse<T>(P, img.data(), targets + 3 * P * vi, dl.data(), 1.0f / (float)n_views) / (double)n_views;
+    loss += combined_loss_grad<T>((int)tl.width, (int)tl.height, img.data(), targets + 3 * P * vi, dl.data(),
+                                  ssim_lambda, 1.0f / (float)n_views, nullptr) /
+            (double)n_views;
     if (out_images) for (uint64_t k = 0; k < 4 * P; ++k) out_images[4 * P * vi + k] = (float)img[k];
     pg.assign((size_t)12 * n, T(0));
     composite_backward<T>(rec.data(), pay.data(), ranges.data(), tl, img.data(), dl.data(), mode, ncon.data(), tfin.data(), pg.data());
@@ -986,8 +1145,15 @@ void oracle_camera_from_pose(const float* eye, const float* target, const float*
   }                                                                                                              \
   double oracle_train_step_##SFX(HostSplats* s, HostSplats* m, HostSplats* v, float* acc, uint32_t nv,          \
                                  const Camera* cams, const float* targets, const Tiling* tl, int mode,           \
-                                 const AdamGroups* ag, uint64_t t, float* out_images) {                          \
-    return train_step<T>(*s, *m, *v, acc, nv, cams, targets, *tl, mode, *ag, t, out_images);                     \
+                                 const AdamGroups* ag, uint64_t t, float* out_images, float ssim_lambda) {       \
+    return train_step<T>(*s, *m, *v, acc, nv, cams, targets, *tl, mode, *ag, t, out_images, ssim_lambda);        \
+  }                                                                                                              \
+  double oracle_ssim_loss_grad_##SFX(int w, int h, const T* pred, const float* target, T* dl, float scale) {     \
+    return ssim_loss_grad<T>(w, h, pred, target, dl, scale);                                                     \
+  }                                                                                                              \
+  double oracle_combined_loss_grad_##SFX(int w, int h, const T* pred, const float* target, T* dl, float lambda,  \
+                                         float scale, double* parts) {                                           \
+    return combined_loss_grad<T>(w, h, pred, target, dl, lambda, scale, parts);                                  \
   }
 
 ORACLE_FLOAT_API(float, f32)

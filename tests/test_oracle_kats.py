@@ -274,3 +274,101 @@ def test_mse_matches_reference_formula(oracle):
     assert np.array_equal(dl.reshape(P, 4)[:, :3], d * inv_n)
     per_pixel = (d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1] + d[:, 2] * d[:, 2]).astype(np.float64)  # f32, then f64 sum
     assert abs(loss - float(per_pixel.sum() / (P * 3))) < 1e-12
+
+
+# ---- SSIM and the combined loss: the reference's loss tests (loss.rs:412-600,
+# tests/loss_tests.rs:10-125) run on the oracle's restatement
+def _rgba(rgb):
+    rgb = np.asarray(rgb, np.float32).reshape(-1, 3)
+    return np.concatenate([rgb, np.zeros((len(rgb), 1), np.float32)], axis=1)
+
+
+def _checkerboard(w, h, scale):
+    out = []
+    for y in range(h):
+        for x in range(w):
+            v = scale if (x + y) % 2 == 0 else 0.0
+            out.append((v, v * 0.5, v * 0.25))
+    return np.array(out, np.float32)
+
+
+def _ramp(w, h, scale):
+    n = w * h
+    f = np.arange(n, dtype=np.float32) / np.float32(n)
+    return np.stack([scale * f, scale * (1 - f), scale * (0.3 + 0.4 * f)], axis=1).astype(np.float32)
+
+
+def _lcg_noise(img, seed):
+    out = img.copy()
+    s = seed
+    for i in range(len(out)):
+        s = (s * 1103515245 + 12345) & 0xFFFFFFFF
+        out[i] += np.float32(((s >> 16) / 65535.0 - 0.5) * 0.4)
+    return out
+
+
+@pytest.mark.parametrize("img", [_checkerboard(8, 8, 0.7), _ramp(8, 8, 0.7)])
+def test_ssim_is_zero_loss_for_identical_images(oracle, img):
+    loss, dl = oracle.ssim(_rgba(img), img, 8, 8)
+    assert abs(loss) < 1e-5
+    assert np.all(np.linalg.norm(dl.reshape(-1, 4)[:, :3], axis=1) < 1e-4)
+
+
+@pytest.mark.parametrize("img,seed", [(_checkerboard(8, 8, 0.7), 1), (_ramp(8, 8, 0.7), 12345)])
+def test_ssim_loss_grows_with_noise(oracle, img, seed):
+    clean, _ = oracle.ssim(_rgba(img), img, 8, 8)
+    dirty, _ = oracle.ssim(_rgba(_lcg_noise(img, seed)), img, 8, 8)
+    assert dirty > clean
+
+
+def test_ssim_gradient_matches_finite_diff(oracle):
+    n = 64
+    f = np.arange(n, dtype=np.float32) / np.float32(n)
+    pred = np.stack([0.3 + 0.4 * f, 0.5 - 0.3 * f, 0.2 + 0.6 * f], 1).astype(np.float32)
+    tgt = np.stack([0.4 + 0.3 * f, 0.6 - 0.4 * f, 0.3 + 0.5 * f], 1).astype(np.float32)
+    _, an = oracle.ssim(_rgba(pred), tgt, 8, 8)
+    an = an.reshape(-1, 4)
+    eps = np.float32(1e-3)
+    for i in range(n):
+        for ch in range(3):
+            pp, pm = pred.copy(), pred.copy()
+            pp[i, ch] += eps
+            pm[i, ch] -= eps
+            lp, _ = oracle.ssim(_rgba(pp), tgt, 8, 8)
+            lm, _ = oracle.ssim(_rgba(pm), tgt, 8, 8)
+            fd = (np.float32(lp) - np.float32(lm)) / (2 * eps)
+            assert abs(fd - an[i, ch]) < 5e-3
+
+
+def _pair(kind):
+    n = 64
+    f = np.arange(n, dtype=np.float32) / np.float32(n)
+    if kind == "a":
+        p = np.stack([f, 1 - f, np.full(n, 0.3, np.float32)], 1)
+        t = np.stack([f * 0.9, 1 - f * 1.1, np.full(n, 0.4, np.float32)], 1)
+    else:
+        p = np.stack([0.2 + f, np.full(n, 0.4, np.float32), 0.5 - f * 0.3], 1)
+        t = np.stack([0.25 + f * 0.9, np.full(n, 0.5, np.float32), 0.55 - f * 0.2], 1)
+    return p.astype(np.float32), t.astype(np.float32)
+
+
+def test_combined_lambda_zero_is_pure_mse_and_one_is_pure_ssim(oracle):
+    p, t = _pair("a")
+    mse, gm = oracle.mse(_rgba(p), t)
+    total, mc, sc, g = oracle.combined(_rgba(p), t, 8, 8, 0.0)
+    assert total == mse and mc == mse and sc == 0.0
+    assert np.max(np.abs(g - gm)) < 1e-9
+    ssim, gs = oracle.ssim(_rgba(p), t, 8, 8)
+    total, mc, sc, g = oracle.combined(_rgba(p), t, 8, 8, 1.0)
+    assert total == ssim and mc == 0.0 and sc == ssim
+    assert np.max(np.abs(g - gs)) < 1e-9
+
+
+def test_combined_gradient_is_lambda_weighted_sum(oracle):
+    p, t = _pair("b")
+    lam = np.float32(0.2)
+    _, gm = oracle.mse(_rgba(p), t)
+    _, gs = oracle.ssim(_rgba(p), t, 8, 8)
+    _, _, _, g = oracle.combined(_rgba(p), t, 8, 8, float(lam))
+    want = gm * (np.float32(1) - lam) + gs * lam
+    assert np.max(np.linalg.norm((g - want).reshape(-1, 4), axis=1)) < 1e-6
