@@ -248,7 +248,8 @@ sc_status sc_composite(sc_ctx* ctx, const sc_projected_splat* projected, uint32_
                        uint32_t* aux);                               /* Rasterizer::composite, raster.rs:468-529 */
 
 /* loss.rs:163-179 on the device: dl_dc = scale * 2 (p - t) / (3 W H) as float4,
- * loss_out (device double, nullable) receives sum (p-t)^2 / (3 W H) per view.
+ * loss_out (device double, nullable) receives per view the sum of (p-t)^2 over
+ * pixels and channels (the loss is that sum / (3 W H)).
  * target is n_views*W*H float3. */
 sc_status sc_mse_loss_grad(sc_ctx* ctx, const float* pred, const float* target, uint32_t n_views,
                            const sc_tiling* tiling, float scale, float* dl_dc, double* loss_out);

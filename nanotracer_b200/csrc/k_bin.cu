@@ -178,56 +178,108 @@ sc_status launch_presorted_counts(sc_ctx* ctx, const uint32_t* counts_by_id, uin
   return sc_check_launch(ctx, "k_presorted_counts");
 }
 
-// One thread emits the pairs of one depth-ranked splat, row by row.  With
+// One thread generates the pairs of one depth-ranked splat, row by row.  With
 // culling, each row keeps the span of tiles that cull_row_span returns — the
 // function the projection counted with — clamped to the 3-sigma rectangle.
 // Exactly `count` pairs are written per splat; should a row span ever differ
 // from the count, surplus tiles are dropped and missing slots get an
 // out-of-range key that sorts last and that the range kernel ignores.
-__global__ void __launch_bounds__(256) k_presorted_emit(const float4* __restrict__ rec, uint32_t stride,
-                                                         uint32_t n_views, const uint32_t* __restrict__ sorted_ids,
-                                                         const uint32_t* __restrict__ offsets,
-                                                         const uint32_t* __restrict__ counts_by_id, BinArgs a,
-                                                         uint32_t* __restrict__ keys, uint32_t* __restrict__ payloads,
-                                                         uint64_t cap, uint32_t* __restrict__ err, int cull) {
+//
+// A warp's 32 consecutive ranked splats own one contiguous output range
+// [offsets[j0], offsets[j0 + 32]).  The warp walks it in chunks of
+// EMIT_WCHUNK pairs: every lane writes the pairs of its splat that fall in the
+// chunk into the warp's shared-memory buffer (resuming its row walk where the
+// previous chunk stopped, one run of a row at a time), then the warp stores
+// the chunk with coalesced 4-byte stores.  Warps never wait for each other.
+constexpr int EMIT_WARPS = 8;
+constexpr int EMIT_WCHUNK = 512;
+
+__global__ void __launch_bounds__(EMIT_WARPS * 32) k_presorted_emit(
+    const float4* __restrict__ rec, uint32_t stride, uint32_t n_views, const uint32_t* __restrict__ sorted_ids,
+    const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ counts_by_id, BinArgs a,
+    uint32_t* __restrict__ keys, uint32_t* __restrict__ payloads, uint64_t cap, uint32_t* __restrict__ err, int cull) {
+  __shared__ uint32_t sk[EMIT_WARPS][EMIT_WCHUNK], sp[EMIT_WARPS][EMIT_WCHUNK];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint64_t total = (uint64_t)n_views * stride;
-  const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= total) return;
-  const uint32_t v = (uint32_t)(j / stride);
-  const uint32_t id = sorted_ids[j];
-  const size_t o = (size_t)v * stride + id;
-  const uint32_t cnt = counts_by_id[o];
-  if (!cnt) return;
-  const float4 ra = rec[3 * o], rb = rec[3 * o + 1], rc = rec[3 * o + 2];
-  int x0, y0, x1, y1;
-  if (!rect_of(ra, rb, a, x0, y0, x1, y1)) return;
-  const uint64_t off = offsets[j];
-  if (off + cnt > cap) {
-    atomicOr(err, SC_DEVERR_CAPACITY);
-    return;
-  }
-  uint32_t* kp = keys + off;
-  uint32_t* pp = payloads + off;
-  const uint32_t vbase = v * a.num_tiles;
-  uint32_t w = 0;
-  const CullShape cs = cull_shape(ra.x, ra.y, rb.x, rb.y, rb.z, rc.w);
-  const bool test = cull && !cs.keep;
-  for (int ty = y0; ty <= y1; ++ty) {
-    int lo = x0, hi = x1;
-    if (test) {
-      if (!cs.any || !cull_row_span(cs, ty, a.tw, a.th, lo, hi)) continue;
-      lo = max(lo, x0);
-      hi = min(hi, x1);
-    }
-    const uint32_t row = vbase + (uint32_t)ty * a.tiles_x;
-    for (int tx = lo; tx <= hi && w < cnt; ++tx, ++w) {
-      kp[w] = row + (uint32_t)tx;
-      pp[w] = id;
+  const uint64_t jw = (uint64_t)blockIdx.x * blockDim.x + (uint64_t)warp * 32;
+  if (jw >= total) return;
+  const uint64_t j = jw + lane;
+  const uint64_t jend = jw + 32 < total ? jw + 32 : total;
+  const uint64_t wlo = offsets[jw], whi = offsets[jend];  // offsets holds total + 1 entries
+  if (lane == 0 && whi > cap) atomicOr(err, SC_DEVERR_CAPACITY);
+  // this lane's splat and its row walk
+  uint32_t cnt = 0, id = 0, vbase = 0;
+  uint64_t off = 0;
+  int x0 = 0, y0 = 0, x1 = -1, y1 = -1;
+  CullShape cs{};
+  bool test = false;
+  if (j < total) {
+    const uint32_t v = (uint32_t)(j / stride);
+    id = sorted_ids[j];
+    const size_t o = (size_t)v * stride + id;
+    cnt = counts_by_id[o];
+    if (cnt) {
+      off = offsets[j];
+      const float4 ra = rec[3 * o], rb = rec[3 * o + 1], rc = rec[3 * o + 2];
+      if (!rect_of(ra, rb, a, x0, y0, x1, y1)) { x0 = 0; y0 = 0; x1 = -1; y1 = -1; }
+      cs = cull_shape(ra.x, ra.y, rb.x, rb.y, rb.z, rc.w);
+      test = cull && !cs.keep;
+      vbase = v * a.num_tiles;
     }
   }
-  for (; w < cnt; ++w) {  // count and emission disagreed: pad
-    kp[w] = 0xFFFFFFFFu;
-    pp[w] = 0;
+  uint32_t* wk = sk[warp];
+  uint32_t* wp = sp[warp];
+  int ty = y0 - 1, tx = 0, hi = -1;  // tx > hi: the next pair starts a new row
+  bool rows_done = cnt == 0;
+  uint32_t w = 0, rowbase = 0;
+  for (uint64_t cb = wlo; cb < whi; cb += EMIT_WCHUNK) {
+    const uint64_t ce = cb + EMIT_WCHUNK < whi ? cb + EMIT_WCHUNK : whi;
+    const int64_t room = (int64_t)ce - (int64_t)off;  // this lane's pairs with index < ce
+    const uint32_t wend = room <= (int64_t)w ? w : (uint32_t)(room < (int64_t)cnt ? room : (int64_t)cnt);
+    int slot = (int)((int64_t)off - (int64_t)cb) + (int)w;
+    while (w < wend) {
+      if (tx > hi) {  // next row whose span is not empty
+        bool found = false;
+        while (!rows_done) {
+          ++ty;
+          if (ty > y1) { rows_done = true; break; }
+          int lo = x0, h = x1;
+          if (test) {
+            if (!cs.any || !cull_row_span(cs, ty, a.tw, a.th, lo, h)) continue;
+            lo = max(lo, x0);
+            h = min(h, x1);
+            if (h < lo) continue;
+          }
+          tx = lo;
+          hi = h;
+          found = true;
+          break;
+        }
+        if (!found) {  // count and emission disagreed: pad
+          for (; w < wend; ++w, ++slot) { wk[slot] = 0xFFFFFFFFu; wp[slot] = 0; }
+          break;
+        }
+        rowbase = vbase + (uint32_t)ty * a.tiles_x;
+      }
+      const uint32_t run = min((uint32_t)(hi - tx + 1), wend - w);
+      for (uint32_t q = 0; q < run; ++q) {
+        wk[slot + q] = rowbase + (uint32_t)tx + q;
+        wp[slot + q] = id;
+      }
+      tx += (int)run;
+      w += run;
+      slot += (int)run;
+    }
+    __syncwarp();
+    const uint32_t n = (uint32_t)(ce - cb);
+    for (uint32_t t = lane; t < n; t += 32) {
+      const uint64_t g = cb + t;
+      if (g < cap) {
+        keys[g] = wk[t];
+        payloads[g] = wp[t];
+      }
+    }
+    __syncwarp();
   }
 }
 
@@ -237,7 +289,7 @@ sc_status launch_presorted_emit(sc_ctx* ctx, const float4* rec, uint32_t stride,
                                 uint32_t* d_error, int cull) {
   const uint64_t total = (uint64_t)n_views * stride;
   if (total == 0) return SC_OK;
-  k_presorted_emit<<<(unsigned)sc_div_up(total, 256), 256, 0, ctx->stream>>>(
+  k_presorted_emit<<<(unsigned)sc_div_up(total, EMIT_WARPS * 32), EMIT_WARPS * 32, 0, ctx->stream>>>(
       rec, stride, n_views, sorted_ids, offsets, counts_by_id, bin_args(tl), keys, payloads, cap, d_error, cull);
   return sc_check_launch(ctx, "k_presorted_emit");
 }

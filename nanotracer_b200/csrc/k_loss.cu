@@ -226,7 +226,7 @@ __global__ void k_loss_parts(const double* __restrict__ mse, const double* __res
                              double inv_3p, float lambda, double* __restrict__ out) {
   const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= n_views) return;
-  const double m = mse ? mse[v] : 0.0;
+  const double m = mse ? mse[v] * inv_3p : 0.0;
   const double s = ssim_sum ? 1.0 - ssim_sum[v] * inv_3p : 0.0;
   const double l = (double)lambda;
   out[3 * v] = lambda == 0.0f ? m : (lambda == 1.0f ? s : (1.0 - l) * m + l * s);

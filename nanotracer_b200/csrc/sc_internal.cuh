@@ -107,7 +107,14 @@ __device__ __forceinline__ void sp_set(const DSplats& s, int r, uint32_t i, floa
 // miss that interval holds no pixel the blend would accept, so the pair can be
 // dropped without changing any image.  L is widened by 1e-3 relative + 1e-3
 // and the interval by 1e-3 px, so float rounding in the blend can never
-// accept a pixel this test rejects.
+// accept a pixel this test rejects; the same margins cover the SFU
+// approximations used here (relative errors near 1e-7, i.e. below 1e-5 px).
+// Counting (projection) and emission call the same functions, so they agree.
+__device__ __forceinline__ float cull_sqrt(float x) {
+  float r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
 struct CullShape {
   float mx, my, a, b, det, L, xh, yh, kx, inv_a;
   bool any;   // op > 1/255 and the conic is positive definite
@@ -122,10 +129,10 @@ __device__ __forceinline__ CullShape cull_shape(float mx, float my, float a, flo
   s.any = op * 255.0f > 1.0f;
   const float q = 2.0f * __logf(fmaxf(op * 255.0f, 1.0f));
   s.L = q + 1e-3f * q + 1e-3f;
-  s.xh = sqrtf(s.L * c / s.det);
-  s.yh = sqrtf(s.L * a / s.det);
-  s.kx = b * s.xh / c;
-  s.inv_a = 1.0f / a;
+  s.xh = cull_sqrt(__fdividef(s.L * c, s.det));
+  s.yh = cull_sqrt(__fdividef(s.L * a, s.det));
+  s.kx = __fdividef(b * s.xh, c);
+  s.inv_a = __fdividef(1.0f, a);
   return s;
 }
 
@@ -137,11 +144,11 @@ __device__ __forceinline__ bool cull_row_span(const CullShape& s, int ty, uint32
   if (w1 < -s.yh || w0 > s.yh) return false;
   const float a0 = fmaxf(w0, -s.yh), a1 = fminf(w1, s.yh);
   const float wr = fminf(fmaxf(-s.kx, a0), a1), wl = fminf(fmaxf(s.kx, a0), a1);
-  const float ur = (-s.b * wr + sqrtf(fmaxf(s.L * s.a - wr * wr * s.det, 0.0f))) * s.inv_a;
-  const float ul = (-s.b * wl - sqrtf(fmaxf(s.L * s.a - wl * wl * s.det, 0.0f))) * s.inv_a;
+  const float ur = (-s.b * wr + cull_sqrt(fmaxf(s.L * s.a - wr * wr * s.det, 0.0f))) * s.inv_a;
+  const float ul = (-s.b * wl - cull_sqrt(fmaxf(s.L * s.a - wl * wl * s.det, 0.0f))) * s.inv_a;
   const float X0 = s.mx + ul - 1e-3f, X1 = s.mx + ur + 1e-3f;
   // tile tx's pixel centres span [tx*tw + 0.5, (tx+1)*tw - 0.5]
-  const float inv_tw = 1.0f / (float)tw;  // exact for power-of-two tiles; the 1e-3 px margin covers the rest
+  const float inv_tw = __fdividef(1.0f, (float)tw);  // the 1e-3 px margin covers its rounding
   tlo = (int)ceilf((X0 + 0.5f) * inv_tw - 1.0f);
   thi = (int)floorf((X1 - 0.5f) * inv_tw);
   return thi >= tlo;
@@ -307,7 +314,7 @@ void ssim_window(float g[11]);
 size_t ssim_terms_bytes(uint64_t pixels_per_view, uint32_t n_views);
 sc_status launch_ssim(sc_ctx* ctx, const float4* pred, const float* target, uint32_t w, uint32_t h, uint32_t n_views,
                       float scale, float4* dl_dc, double* ssim_sum, float* terms);
-// per view {total, mse, ssim} from the MSE means and SSIM-map sums (loss.rs:383-410)
+// per view {total, mse, ssim} from the squared-error sums and SSIM-map sums (loss.rs:383-410)
 sc_status launch_loss_parts(sc_ctx* ctx, const double* mse, const double* ssim_sum, uint32_t n_views, uint64_t P,
                             float lambda, double* out);
 
