@@ -189,12 +189,11 @@ static sc_status composite_ppt(sc_ctx* ctx, const BlendArgs& a, uint32_t grid, u
   return sc_check_launch(ctx, "k_composite");
 }
 
-// pixels per thread: as many as keep whole warps (the per-entry cost of a
-// warp -- record loads, and in the backward the gradient reduction -- is then
-// shared by more pixels)
+// pixels per thread: 2 when the tile splits into whole warps that way (4 per
+// thread measured slower in both kernels at 16x16 tiles: fewer warps per tile
+// to hide the entry loop's latency)
 static int pick_ppt(const sc_tiling* tl) {
   const uint32_t px = tl->tile_w * tl->tile_h;
-  if (tl->tile_h % 4 == 0 && (px / 4) % 32 == 0) return 4;
   return (tl->tile_h % 2 == 0 && (px / 2) % 32 == 0) ? 2 : 1;
 }
 
@@ -210,9 +209,6 @@ sc_status launch_composite(sc_ctx* ctx, const float4* rec, uint32_t stride, uint
   const float gscale = (2.0f / n_scalars) * mse_scale;
   const int ppt = pick_ppt(tl);
   if (ppt == 1 && pixels > 256) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile too large for one pixel per thread");
-  if (ppt == 4)
-    return composite_ppt<4>(ctx, a, (uint32_t)grid, pixels / 4, rec, payloads, ranges, image, aux, target, gscale, dl_dc,
-                            loss, d_skip);
   if (ppt == 2)
     return composite_ppt<2>(ctx, a, (uint32_t)grid, pixels / 2, rec, payloads, ranges, image, aux, target, gscale, dl_dc,
                             loss, d_skip);
@@ -492,9 +488,6 @@ sc_status launch_composite_backward(sc_ctx* ctx, const float4* rec, uint32_t str
   if (grid == 0) return SC_OK;
   const int ppt = pick_ppt(tl);
   if (ppt == 1 && pixels > 256) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile too large for one pixel per thread");
-  if (ppt == 4)
-    return backward_ppt<4>(ctx, a, (uint32_t)grid, pixels / 4, rec, payloads, ranges, fwd, dl_dc, mode, aux, proj_grad,
-                           d_skip);
   if (ppt == 2)
     return backward_ppt<2>(ctx, a, (uint32_t)grid, pixels / 2, rec, payloads, ranges, fwd, dl_dc, mode, aux, proj_grad,
                            d_skip);
