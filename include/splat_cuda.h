@@ -353,6 +353,13 @@ sc_status sc_trainer_stats(const sc_trainer* tr, uint64_t* pairs, uint32_t* n_ke
 /* Record CUDA events between the stages of each step (also inside the graph). */
 sc_status sc_trainer_set_profiling(sc_trainer* tr, int enabled);
 
+/* Failure-detection self-test (no counterpart in the reference): runs one
+ * radix-sort pass whose look-back waits on a tile that is never processed.
+ * The bounded wait gives up (about a second), the kernel ends, and the call
+ * returns SC_ERR_TIMEOUT; the context stays usable.  Any other status means
+ * the timeout path is broken. */
+sc_status sc_selftest_wait_timeout(sc_ctx* ctx);
+
 /* ------------------------------------------------ data-parallel views
  * No counterpart in the reference, which trains on one device (train.rs:155-250
  * renders the iteration's views one after another).  One iteration is split

@@ -337,7 +337,9 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
   const float4* vrec = rec + (size_t)3 * v * a.stride;
   float4* vgrad = proj_grad + (size_t)3 * v * a.stride;
 
-  float T[PPT], gr[PPT], gg[PPT], gb[PPT], Sr[PPT], Sg[PPT], Sb[PPT], fy[PPT];
+  // GS = dL/dC . S, the accumulated colour behind the pixel dotted with its
+  // colour gradient: dL/dalpha_i = (T_{i+1} (dL/dC . c_i) - GS) / (1 - alpha_i)
+  float T[PPT], gr[PPT], gg[PPT], gb[PPT], GS[PPT], fy[PPT];
   uint32_t stop[PPT];
   bool done[PPT];
   uint32_t tstop = begin;
@@ -346,7 +348,7 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
   for (int q = 0; q < PPT; ++q) {
     const uint32_t py = py0 + q;
     fy[q] = (float)py + 0.5f;
-    T[q] = 1.0f; gr[q] = gg[q] = gb[q] = 0.f; Sr[q] = Sg[q] = Sb[q] = 0.f;
+    T[q] = 1.0f; gr[q] = gg[q] = gb[q] = 0.f; GS[q] = 0.f;
     stop[q] = begin;
     done[q] = !(px < a.width && py < a.height);
     if (!done[q]) {
@@ -402,9 +404,11 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
     if (!__all_sync(FULL_MASK, all_done)) {
       for (int k = (int)cnt - 1; k >= 0; --k) {
         const uint32_t j = lo + (uint32_t)k;
-        float c[9];
-#pragma unroll
-        for (int e = 0; e < 9; ++e) c[e] = 0.0f;
+        // this thread's sums over its pixels: h = dL/dalpha * gauss (the opacity
+        // gradient), its first and second moments in (dx, dy), and the colour
+        // gradient; the per-splat terms are formed from them once per entry
+        float sh = 0.f, shx = 0.f, shy = 0.f, shxx = 0.f, shxy = 0.f, shyy = 0.f;
+        float scr = 0.f, scg = 0.f, scb = 0.f;
         bool contrib = false;
         const float4 ra = sb[3 * k], rb = sb[3 * k + 1], rc = sb[3 * k + 2];
         const float dx = fx - ra.x;
@@ -422,19 +426,16 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
                 done[q] = true;
               } else {
                 const float ta = Tn * alpha;
-                c[6] += gr[q] * ta; c[7] += gg[q] * ta; c[8] += gb[q] * ta;
+                scr += gr[q] * ta; scg += gg[q] * ta; scb += gb[q] * ta;
                 // dC/dalpha = T_i c - S / (1 - alpha) = (T_{i+1} c - S) / (1 - alpha)
-                const float galpha = inv * (gr[q] * (T[q] * rc.x - Sr[q]) + gg[q] * (T[q] * rc.y - Sg[q]) +
-                                            gb[q] * (T[q] * rc.z - Sb[q]));
-                const float gar = araw < ALPHA_MAX ? galpha : 0.0f;
-                c[2] += gar * g;
-                const float gpow = gar * rc.w * g;
-                c[3] += gpow * -0.5f * (dx * dx);
-                c[4] += gpow * -(dx * dy);
-                c[5] += gpow * -0.5f * (dy * dy);
-                c[0] += gpow * (rb.x * dx + rb.y * dy);
-                c[1] += gpow * (rb.y * dx + rb.z * dy);
-                Sr[q] += ta * rc.x; Sg[q] += ta * rc.y; Sb[q] += ta * rc.z;
+                const float dc = gr[q] * rc.x + gg[q] * rc.y + gb[q] * rc.z;
+                const float galpha = inv * (T[q] * dc - GS[q]);
+                const float h = araw < ALPHA_MAX ? galpha * g : 0.0f;
+                const float hx = h * dx, hy = h * dy;
+                sh += h;
+                shx += hx; shy += hy;
+                shxx += hx * dx; shxy += hx * dy; shyy += hy * dy;
+                GS[q] += ta * dc;
                 T[q] = Tn;
                 contrib = true;
               }
@@ -443,6 +444,17 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
           all_done &= done[q] || j <= begin;
         }
         if (__any_sync(FULL_MASK, contrib)) {
+          // dpower = op h; dconic = dpower (-1/2)(dx^2, 2 dx dy, dy^2);
+          // dmean = dpower (a dx + b dy, b dx + c dy)  (rasterize_backward.wgsl:174-185)
+          const float op = rc.w;
+          float c[9];
+          c[0] = op * (rb.x * shx + rb.y * shy);
+          c[1] = op * (rb.y * shx + rb.z * shy);
+          c[2] = sh;
+          c[3] = -0.5f * op * shxx;
+          c[4] = -op * shxy;
+          c[5] = -0.5f * op * shyy;
+          c[6] = scr; c[7] = scg; c[8] = scb;
           int idx;
           const float w = warp_reduce_scatter9(c, lane, &idx);
           if (idx >= 0) atomicAdd(reinterpret_cast<float*>(sacc + 3 * k) + idx + idx / 3, w);

@@ -483,6 +483,38 @@ sc_status radix_sort(sc_ctx* ctx, K* keys, uint32_t* vals, K* keys_tmp, uint32_t
 
 template sc_status radix_sort<uint32_t>(sc_ctx*, uint32_t*, uint32_t*, uint32_t*, uint32_t*, uint64_t, uint32_t,
                                         const uint64_t*, void*, size_t, bool*);
+
+// Failure-detection self-test: one onesweep pass over two tiles whose ticket
+// counter starts at 1, so the first tile to run looks back on tile 0, which no
+// block ever processes.  Its bounded wait gives up after SC_SPIN_LIMIT polls,
+// raises SC_DEVERR_TIMEOUT and skips every out-of-range write; the kernel
+// ends and the host reads the error word.
+sc_status selftest_lookback_timeout(sc_ctx* ctx) {
+  using K = uint32_t;
+  constexpr int TILE = RS_THREADS * RsCfg<K>::IPT;
+  const uint64_t n = 2 * (uint64_t)TILE;
+  const size_t data = (size_t)n * 4;
+  const size_t need = 4 * data + 8192 + 64 + (size_t)2 * RS_RADIX * 4;
+  void* buf = nullptr;
+  SC_TRY(sc_scratch(ctx, need, &buf));
+  char* p = reinterpret_cast<char*>(buf);
+  K* keys = reinterpret_cast<K*>(p);
+  uint32_t* vals = reinterpret_cast<uint32_t*>(p + data);
+  K* kout = reinterpret_cast<K*>(p + 2 * data);
+  uint32_t* vout = reinterpret_cast<uint32_t*>(p + 3 * data);
+  uint32_t* hist = reinterpret_cast<uint32_t*>(p + 4 * data);
+  unsigned* ticket = reinterpret_cast<unsigned*>(p + 4 * data + 8192);
+  unsigned* lookback = reinterpret_cast<unsigned*>(p + 4 * data + 8192 + 64);
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(p, 0, need, ctx->stream), "zero");
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(ticket, 1, 1, ctx->stream), "ticket = 1");  // tile 0 is never handed out
+  const size_t smem = sizeof(RsSmem<K>);
+  SC_CUDA_TRY(ctx, cudaFuncSetAttribute(k_rs_pass<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+              "smem attr");
+  k_rs_pass<K><<<2, RS_THREADS, smem, ctx->stream>>>(keys, vals, kout, vout, n, nullptr, 0, hist, lookback, ticket,
+                                                     ctx->d_error);
+  SC_TRY(sc_check_launch(ctx, "k_rs_pass (timeout self-test)"));
+  return sc_check_device_error(ctx);
+}
 template sc_status radix_sort<uint64_t>(sc_ctx*, uint64_t*, uint32_t*, uint64_t*, uint32_t*, uint64_t, uint32_t,
                                         const uint64_t*, void*, size_t, bool*);
 

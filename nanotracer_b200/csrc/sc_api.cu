@@ -810,6 +810,11 @@ sc_status sc_adam_step_all(sc_ctx* ctx, sc_splats* s, const sc_grads* g, sc_mome
   return sck::launch_adam_all(ctx, dview(s), g->slab, g->cap, dview(mo), ap);
 }
 
+sc_status sc_selftest_wait_timeout(sc_ctx* ctx) {
+  if (!ctx) return SC_ERR_INVALID_ARG;
+  return sck::selftest_lookback_timeout(ctx);
+}
+
 sc_status sc_adam_step_shard(sc_ctx* ctx, sc_splats* s, sc_moments* mo, float* acc, const float* g, uint32_t lo,
                              uint32_t count, uint32_t shard, uint64_t t, const sc_adam_groups* gr, float lsmin,
                              float lsmax, float opmax) {

@@ -278,6 +278,8 @@ template <typename K>
 sc_status radix_sort(sc_ctx* ctx, K* keys, uint32_t* vals, K* keys_tmp, uint32_t* vals_tmp, uint64_t n,
                      uint32_t key_bits, const uint64_t* d_n, void* scratch, size_t scratch_bytes, bool* result_in_tmp);
 size_t radix_scratch_bytes(uint64_t n, uint32_t key_bytes);
+// one look-back pass whose predecessor never publishes (bounded-wait self-test)
+sc_status selftest_lookback_timeout(sc_ctx* ctx);
 
 // binning
 sc_status launch_tile_count(sc_ctx* ctx, const float4* rec, uint32_t n, uint32_t stride, uint32_t n_views,
