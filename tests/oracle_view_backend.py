@@ -166,3 +166,27 @@ def run_rank(rank, world, port, out_dir, steps, n, V, densify_at):
                  acc=be.acc_np[: be.n], losses=np.array(losses), views=np.array(tr.views))
     finally:
         torch.distributed.destroy_process_group()
+
+
+def run_rank_leaving(rank, world, port, out_dir):
+    """Rank 1 leaves before the first collective; rank 0 must get an error, not hang."""
+    import datetime
+    import sys
+    import time
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    torch.distributed.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=5))
+    O.lib()
+    scene, cams, tl, tgt = problem(n=200, V=2)
+    be = OracleViewBackend(scene, cams, tl, tgt)
+    tr = ViewParallelTrainer(be, 2)
+    if rank == 1:
+        open(os.path.join(out_dir, "rank1.txt"), "w").write("left")
+        sys.exit(0)  # between steps, with no collective in flight
+    t0 = time.time()
+    try:
+        tr.step(1)
+        outcome = "completed"
+    except Exception as e:  # gloo reports the closed peer or the timeout
+        outcome = "error:" + type(e).__name__
+    open(os.path.join(out_dir, "rank0.txt"), "w").write(f"{outcome} {time.time() - t0:.1f}")

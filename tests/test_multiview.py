@@ -94,3 +94,21 @@ def test_two_rank_state_gather_then_densify_and_prune(oracle, tmp_path):
     assert got.shape == want.shape and s.n > n
     assert np.mean(np.abs(got - want) <= 1e-5 + 1e-5 * np.abs(want)) > 0.99
     assert np.allclose(outs[0]["losses"], losses, rtol=1e-5)
+
+
+def test_a_rank_that_leaves_makes_the_others_fail_not_hang(tmp_path):
+    from tests.oracle_view_backend import run_rank_leaving
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=run_rank_leaving, args=(r, 2, port, str(tmp_path))) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    alive = [p for p in procs if p.is_alive()]
+    for p in alive:
+        p.kill()
+    assert not alive, "a rank hung"
+    assert (tmp_path / "rank1.txt").read_text() == "left"
+    outcome, secs = (tmp_path / "rank0.txt").read_text().split()
+    assert outcome.startswith("error:") and float(secs) < 60
