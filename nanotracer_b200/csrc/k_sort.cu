@@ -284,37 +284,24 @@ __device__ __forceinline__ void st_relaxed_u32(unsigned* p, unsigned v) {
   asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// One onesweep pass.  Ranking: the lanes of a warp holding the same digit are
-// found with 8 ballots (one per digit bit), a fixed cost independent of how
-// many distinct digits the warp holds; lanes are ranked in input order, so the
-// pass is stable.  Look-back status words carry their own value (flag in the
-// top 2 bits, count below), so relaxed loads and stores suffice.
-template <typename K>
-__global__ void __launch_bounds__(RS_THREADS, 4) k_rs_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
-                                                        K* __restrict__ kout, uint32_t* __restrict__ vout,
-                                                        uint64_t n_cap, const uint64_t* __restrict__ d_n, int shift,
-                                                        const uint32_t* __restrict__ digit_base,
-                                                        unsigned* __restrict__ lookback, unsigned* __restrict__ ticket,
-                                                        uint32_t* __restrict__ err) {
+// The work of one tile once its index is known.  FULL: the tile lies wholly
+// below n, so no per-key bounds test is needed.
+template <typename K, bool FULL>
+__device__ __forceinline__ void rs_pass_tile(RsSmem<K>& sm, const K* __restrict__ kin,
+                                             const uint32_t* __restrict__ vin, K* __restrict__ kout,
+                                             uint32_t* __restrict__ vout, uint64_t n, int shift,
+                                             const uint32_t* __restrict__ digit_base, unsigned* __restrict__ lookback,
+                                             uint32_t* __restrict__ err, uint32_t tile, uint64_t tbase) {
   constexpr int IPT = RsCfg<K>::IPT;
   constexpr int TILE = RS_THREADS * IPT;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  RsSmem<K>& sm = *reinterpret_cast<RsSmem<K>*>(smem_raw);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (threadIdx.x == 0) sm.tile_id = atomicAdd(ticket, 1u);
-  for (int t = threadIdx.x; t < RS_WARPS * RS_RADIX; t += RS_THREADS) (&sm.warp_hist[0][0])[t] = 0;
-  __syncthreads();
-  const uint32_t tile = sm.tile_id;
-  const uint64_t n = d_n ? min(*d_n, n_cap) : n_cap;
-  const uint64_t tbase = (uint64_t)tile * TILE;
-  if (tbase >= n) return;  // every later ticket is beyond n as well: nobody waits on this tile
   // warp-striped layout: item k of lane l in warp w is input slot w*32*IPT + k*32 + l
   const uint32_t wslot = (uint32_t)warp * 32 * IPT;
   const uint64_t wbase = tbase + wslot;
 #pragma unroll
   for (int k = 0; k < IPT; ++k) {
     const uint64_t i = wbase + (uint64_t)k * 32 + lane;
-    if (i < n) cp_async4(&sm.vals[wslot + k * 32 + lane], vin + i);
+    if (FULL || i < n) cp_async4(&sm.vals[wslot + k * 32 + lane], vin + i);
   }
   asm volatile("cp.async.commit_group;" ::: "memory");
   K key[IPT];
@@ -322,14 +309,14 @@ __global__ void __launch_bounds__(RS_THREADS, 4) k_rs_pass(const K* __restrict__
 #pragma unroll
   for (int k = 0; k < IPT; ++k) {
     const uint64_t i = wbase + (uint64_t)k * 32 + lane;
-    key[k] = i < n ? kin[i] : (K)0;
+    key[k] = (FULL || i < n) ? kin[i] : (K)0;
   }
   const unsigned lt = lanemask_lt();
 #pragma unroll
   for (int k = 0; k < IPT; ++k) {
-    const bool valid = wbase + (uint64_t)k * 32 + lane < n;
+    const bool valid = FULL || wbase + (uint64_t)k * 32 + lane < n;
     const uint32_t d = (uint32_t)(key[k] >> shift) & 0xFFu;
-    unsigned peers = __ballot_sync(0xffffffffu, valid);
+    unsigned peers = FULL ? 0xffffffffu : __ballot_sync(0xffffffffu, valid);
 #pragma unroll
     for (int b = 0; b < 8; ++b) {
       const bool bit = (d >> b) & 1u;
@@ -406,7 +393,7 @@ __global__ void __launch_bounds__(RS_THREADS, 4) k_rs_pass(const K* __restrict__
   // keys to digit order in shared memory, with the input slot of each payload
 #pragma unroll
   for (int k = 0; k < IPT; ++k) {
-    if (wbase + (uint64_t)k * 32 + lane < n) {
+    if (FULL || wbase + (uint64_t)k * 32 + lane < n) {
       const uint32_t dd = (uint32_t)(key[k] >> shift) & 0xFFu;
       const uint32_t pos = sm.tile_excl[dd] + sm.warp_hist[warp][dd] + rank[k];
       sm.keys[pos] = key[k];
@@ -415,7 +402,7 @@ __global__ void __launch_bounds__(RS_THREADS, 4) k_rs_pass(const K* __restrict__
   }
   asm volatile("cp.async.wait_all;" ::: "memory");
   __syncthreads();
-  const uint32_t valid = (uint32_t)min((uint64_t)TILE, n - tbase);
+  const uint32_t valid = FULL ? (uint32_t)TILE : (uint32_t)min((uint64_t)TILE, n - tbase);
   for (uint32_t idx = threadIdx.x; idx < valid; idx += RS_THREADS) {
     const K kk = sm.keys[idx];
     const uint32_t dd = (uint32_t)(kk >> shift) & 0xFFu;
@@ -427,6 +414,35 @@ __global__ void __launch_bounds__(RS_THREADS, 4) k_rs_pass(const K* __restrict__
     kout[g] = kk;
     vout[g] = sm.vals[sm.src[idx]];
   }
+}
+
+// One onesweep pass.  Ranking: the lanes of a warp holding the same digit are
+// found with 8 ballots (one per digit bit), a fixed cost independent of how
+// many distinct digits the warp holds; lanes are ranked in input order, so the
+// pass is stable.  Look-back status words carry their own value (flag in the
+// top 2 bits, count below), so relaxed loads and stores suffice.
+template <typename K>
+__global__ void __launch_bounds__(RS_THREADS, 4) k_rs_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
+                                                        K* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                        uint64_t n_cap, const uint64_t* __restrict__ d_n, int shift,
+                                                        const uint32_t* __restrict__ digit_base,
+                                                        unsigned* __restrict__ lookback, unsigned* __restrict__ ticket,
+                                                        uint32_t* __restrict__ err) {
+  constexpr int IPT = RsCfg<K>::IPT;
+  constexpr int TILE = RS_THREADS * IPT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  RsSmem<K>& sm = *reinterpret_cast<RsSmem<K>*>(smem_raw);
+  if (threadIdx.x == 0) sm.tile_id = atomicAdd(ticket, 1u);
+  for (int t = threadIdx.x; t < RS_WARPS * RS_RADIX; t += RS_THREADS) (&sm.warp_hist[0][0])[t] = 0;
+  __syncthreads();
+  const uint32_t tile = sm.tile_id;
+  const uint64_t n = d_n ? min(*d_n, n_cap) : n_cap;
+  const uint64_t tbase = (uint64_t)tile * TILE;
+  if (tbase >= n) return;  // every later ticket is beyond n as well: nobody waits on this tile
+  if (tbase + TILE <= n)
+    rs_pass_tile<K, true>(sm, kin, vin, kout, vout, n, shift, digit_base, lookback, err, tile, tbase);
+  else
+    rs_pass_tile<K, false>(sm, kin, vin, kout, vout, n, shift, digit_base, lookback, err, tile, tbase);
 }
 
 size_t radix_scratch_bytes(uint64_t n, uint32_t key_bytes) {
