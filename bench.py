@@ -214,11 +214,15 @@ def run_ours(args):
     # ---- e2e through the public API: pinned host targets + cameras in, loss out
     e2e = None
     if not args.no_e2e:
+        # the step's targets come from pinned host memory: the trainer copies them
+        # on a side stream every step, overlapped with the stages before the blend
         pinned = torch.empty(tgt0.size, dtype=torch.float32, pin_memory=True)
         pinned.numpy()[:] = tgt0.reshape(-1)
-        import ctypes as C
-        from nanotracer_b200._lib import check, lib
+        tr.set_profiling(False)
+        tr.set_host_targets(pinned.data_ptr(), keepalive=pinned)
         h2d = pinned.numel() * 4 + V * 96
+        t += 1
+        tr.step(g, mo, acc, cams_steps[args.warmup], t)  # re-capture the graph with the copy node (untimed)
         torch.cuda.synchronize(local)
         barrier(pg)
         t0 = time.perf_counter()
@@ -227,8 +231,6 @@ def run_ours(args):
         f0.record(stream)
         for s in range(args.steps):
             t += 1
-            check(lib().sc_buffer_upload(ctx.handle, tbuf.cptr, C.c_void_p(pinned.data_ptr()), pinned.numel() * 4),
-                  ctx.handle)
             tr.step(g, mo, acc, cams_steps[args.warmup + s], t)
         f1.record(stream)
         torch.cuda.synchronize(local)

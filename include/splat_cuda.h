@@ -335,6 +335,12 @@ sc_status sc_trainer_create(sc_ctx* ctx, const sc_train_config* cfg, sc_trainer*
 void sc_trainer_free(sc_ctx* ctx, sc_trainer* tr);
 /* targets: device array n_views*W*H float3 (rgb). */
 sc_status sc_trainer_set_targets(sc_trainer* tr, const float* targets);
+/* Targets in page-locked host memory (n_views*W*H float3): every step copies
+ * them to a trainer-owned device buffer on a side stream, overlapped with the
+ * projection, sorting and emission, and the blend waits for the copy (the
+ * reference uploads its target before the iteration, train.rs:166-196).  The
+ * caller may rewrite the host buffer between steps. */
+sc_status sc_trainer_set_host_targets(sc_trainer* tr, const float* pinned_targets);
 /* One training step with cameras cams[n_views] (host array); t is the new Adam
  * step count.  Blocks until the step has finished; loss_out (host, nullable)
  * receives the mean loss.  A step whose pair lists overflowed the device

@@ -132,6 +132,7 @@ _PROTOS = {
     "sc_trainer_create": (ST, [P, C.POINTER(sc_train_config), C.POINTER(P)]),
     "sc_trainer_free": (None, [P, P]),
     "sc_trainer_set_targets": (ST, [P, P]),
+    "sc_trainer_set_host_targets": (ST, [P, P]),
     "sc_trainer_step": (ST, [P, P, P, P, P, U64, C.POINTER(C.c_double)]),
     "sc_trainer_images": (ST, [P, C.POINTER(P)]),
     "sc_trainer_stats": (ST, [P, C.POINTER(U64), C.POINTER(U32), P, P]),

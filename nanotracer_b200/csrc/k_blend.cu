@@ -310,12 +310,15 @@ __device__ __forceinline__ float warp_reduce_scatter9(const float a[9], int lane
   return w;
 }
 
-template <int PPT>
+// MODE is the sc_bwd_mode.  In exact mode a pixel takes part from its last
+// contributor down to the start of the tile's list and never stops early, so
+// the early-exit bookkeeping exists only in reference mode.
+template <int PPT, int MODE>
 __global__ void __launch_bounds__(256) k_composite_backward(const float4* __restrict__ rec,
                                                             const uint32_t* __restrict__ payloads,
                                                             const uint2* __restrict__ ranges, BlendArgs a,
                                                             const float4* __restrict__ fwd,
-                                                            const float4* __restrict__ dl_dc, int mode,
+                                                            const float4* __restrict__ dl_dc,
                                                             const uint2* __restrict__ aux,
                                                             float4* __restrict__ proj_grad,
                                                             const uint32_t* __restrict__ skip) {
@@ -355,7 +358,7 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
       const size_t pix = (size_t)v * a.pixels + (size_t)py * a.width + px;
       const float4 d = dl_dc[pix];
       gr[q] = d.x; gg[q] = d.y; gb[q] = d.z;
-      if (mode == SC_BWD_REF) {
+      if (MODE == SC_BWD_REF) {
         T[q] = 1.0f - fwd[pix].w;
         stop[q] = end;
       } else {
@@ -415,14 +418,14 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
         all_done = true;
 #pragma unroll
         for (int q = 0; q < PPT; ++q) {
-          if (!done[q] && j < stop[q]) {
+          if ((MODE == SC_BWD_EXACT || !done[q]) && j < stop[q]) {
             const float dy = fy[q] - ra.y;
             float g, araw, alpha;
             if (eval_alpha(dx, dy, rb, rc.w, g, araw, alpha)) {
               const float oma = fmaxf(1.0f - alpha, 1e-4f);
               const float inv = __fdividef(1.0f, oma);
               const float Tn = T[q] * inv;  // T_i = T_{i+1} / (1 - alpha_i)
-              if (mode == SC_BWD_REF && Tn > 1.0001f) {
+              if (MODE == SC_BWD_REF && Tn > 1.0001f) {
                 done[q] = true;
               } else {
                 const float ta = Tn * alpha;
@@ -441,8 +444,9 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
               }
             }
           }
-          all_done &= done[q] || j <= begin;
+          if (MODE == SC_BWD_REF) all_done &= done[q] || j <= begin;
         }
+        if (MODE == SC_BWD_EXACT) all_done = false;
         if (__any_sync(FULL_MASK, contrib)) {
           // dpower = op h; dconic = dpower (-1/2)(dx^2, 2 dx dy, dy^2);
           // dmean = dpower (a dx + b dy, b dx + c dy)  (rasterize_backward.wgsl:174-185)
@@ -483,8 +487,12 @@ static sc_status backward_ppt(sc_ctx* ctx, const BlendArgs& a, uint32_t grid, ui
                               const uint32_t* payloads, const uint32_t* ranges, const float4* fwd, const float4* dl_dc,
                               int mode, const uint2* aux, float4* proj_grad, const uint32_t* d_skip) {
   const size_t smem = (size_t)9 * threads * sizeof(float4) + (size_t)2 * threads * sizeof(uint32_t);
-  k_composite_backward<PPT><<<grid, threads, smem, ctx->stream>>>(
-      rec, payloads, reinterpret_cast<const uint2*>(ranges), a, fwd, dl_dc, mode, aux, proj_grad, d_skip);
+  if (mode == SC_BWD_EXACT)
+    k_composite_backward<PPT, SC_BWD_EXACT><<<grid, threads, smem, ctx->stream>>>(
+        rec, payloads, reinterpret_cast<const uint2*>(ranges), a, fwd, dl_dc, aux, proj_grad, d_skip);
+  else
+    k_composite_backward<PPT, SC_BWD_REF><<<grid, threads, smem, ctx->stream>>>(
+        rec, payloads, reinterpret_cast<const uint2*>(ranges), a, fwd, dl_dc, aux, proj_grad, d_skip);
   return sc_check_launch(ctx, "k_composite_backward");
 }
 

@@ -92,6 +92,12 @@ struct sc_trainer {
   // SSIM term of the loss (cfg.ssim_lambda > 0): coefficient planes and per-view map sums
   float* ssim_terms = nullptr; double* d_ssim = nullptr;
   const float* targets = nullptr;
+  // targets in pinned host memory: copied every step on a side stream, in
+  // parallel with projection, sorting and emission, into d_host_targets
+  const float* h_targets = nullptr;
+  float* d_host_targets = nullptr;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_copied = nullptr;
   double* d_loss = nullptr;
   uint64_t* d_total = nullptr;
   void* scratch = nullptr; size_t scratch_bytes = 0;
@@ -102,7 +108,7 @@ struct sc_trainer {
   uint32_t g_shards = 0, g_shard = 0;
   // graph
   cudaGraphExec_t exec = nullptr;
-  const void* g_key[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  const void* g_key[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   uint64_t g_key_n = 0, g_key_kcap = 0;
   bool g_key_grads = false;
   float g_key_w = 0.0f;
@@ -217,6 +223,13 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   const uint64_t launches0 = ctx->launches;
   SC_CUDA_TRY(ctx, cudaMemcpyAsync(tr->d_params, tr->h_params, sizeof(StepParams), cudaMemcpyHostToDevice, ctx->stream),
               "params H2D");
+  if (tr->h_targets) {  // host targets: this step's copy runs beside the stages that do not read them
+    SC_CUDA_TRY(ctx, cudaEventRecord(tr->ev_fork, ctx->stream), "fork");
+    SC_CUDA_TRY(ctx, cudaStreamWaitEvent(tr->copy_stream, tr->ev_fork, 0), "fork wait");
+    SC_CUDA_TRY(ctx, cudaMemcpyAsync(tr->d_host_targets, tr->h_targets, (size_t)V * tr->P * 3 * sizeof(float),
+                                     cudaMemcpyHostToDevice, tr->copy_stream), "targets H2D");
+    SC_CUDA_TRY(ctx, cudaEventRecord(tr->ev_copied, tr->copy_stream), "copied");
+  }
   SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->d_loss, 0, 8 * (size_t)V, ctx->stream), "zero loss");
   SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->pgrad, 0, nsp * 48, ctx->stream), "zero pgrad");
   SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->counts + nsp, 0, 4, ctx->stream), "zero count tail");
@@ -251,6 +264,7 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   mark(tr, 5, capturing);
   SC_TRY(sck::launch_tile_ranges(ctx, skeys, 2, tr->d_total, tr->kcap, all_tiles, tr->ranges));
   mark(tr, 6, capturing);
+  if (tr->h_targets) SC_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, tr->ev_copied, 0), "join");
   const float weight = tr->grads_mode ? tr->loss_weight : 1.0f / (float)V;
   const float lam = tr->cfg.ssim_lambda;
   SC_TRY(sck::launch_composite(ctx, tr->rec, tr->stride, V, svals, tr->ranges, &tr->cfg.tiling, tr->image, tr->aux,
@@ -340,6 +354,10 @@ void sc_trainer_free(sc_ctx* ctx, sc_trainer* tr) {
   cudaFree(tr->ranges); cudaFree(tr->image); cudaFree(tr->aux); cudaFree(tr->dl_dc);
   cudaFree(tr->d_loss); cudaFree(tr->d_total); cudaFree(tr->d_params); cudaFree(tr->d_out);
   cudaFree(tr->ssim_terms); cudaFree(tr->d_ssim);
+  cudaFree(tr->d_host_targets);
+  if (tr->copy_stream) cudaStreamDestroy(tr->copy_stream);
+  if (tr->ev_fork) cudaEventDestroy(tr->ev_fork);
+  if (tr->ev_copied) cudaEventDestroy(tr->ev_copied);
   cudaFree(tr->scratch);
   if (tr->h_params) cudaFreeHost(tr->h_params);
   if (tr->h_out) cudaFreeHost(tr->h_out);
@@ -350,8 +368,29 @@ void sc_trainer_free(sc_ctx* ctx, sc_trainer* tr) {
 
 sc_status sc_trainer_set_targets(sc_trainer* tr, const float* targets) {
   if (!tr || !targets) return SC_ERR_INVALID_ARG;
-  if (tr->targets != targets) trainer_drop_graph(tr);
+  if (tr->targets != targets || tr->h_targets) trainer_drop_graph(tr);
   tr->targets = targets;
+  tr->h_targets = nullptr;
+  return SC_OK;
+}
+
+sc_status sc_trainer_set_host_targets(sc_trainer* tr, const float* pinned_targets) {
+  if (!tr || !pinned_targets) return SC_ERR_INVALID_ARG;
+  sc_ctx* ctx = tr->ctx;
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, pinned_targets) != cudaSuccess || at.type != cudaMemoryTypeHost) {
+    cudaGetLastError();
+    return sc_fail(ctx, SC_ERR_INVALID_ARG, "host targets must be page-locked (cudaMallocHost / pinned) memory");
+  }
+  if (!tr->d_host_targets) {
+    SC_CUDA_TRY(ctx, cudaMalloc(&tr->d_host_targets, (size_t)tr->V * tr->P * 3 * sizeof(float)), "targets");
+    SC_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&tr->copy_stream, cudaStreamNonBlocking), "copy stream");
+    SC_CUDA_TRY(ctx, cudaEventCreateWithFlags(&tr->ev_fork, cudaEventDisableTiming), "event");
+    SC_CUDA_TRY(ctx, cudaEventCreateWithFlags(&tr->ev_copied, cudaEventDisableTiming), "event");
+  }
+  if (tr->h_targets != pinned_targets) trainer_drop_graph(tr);
+  tr->h_targets = pinned_targets;
+  tr->targets = tr->d_host_targets;
   return SC_OK;
 }
 
@@ -374,8 +413,8 @@ static sc_status run_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, float* a
   for (int attempt = 0; attempt < 4; ++attempt) {
     const bool sizing = tr->kcap == 0;
     const void* mkey = mo ? (mo->m ? (const void*)mo->m : (const void*)mo->m16) : nullptr;
-    const void* key[7] = {s->slab, s->rest16, mkey, acc, tr->targets, tr->scratch, tr->gout};
-    const bool key_ok = tr->exec && std::equal(key, key + 7, tr->g_key) && tr->g_key_n == s->n &&
+    const void* key[8] = {s->slab, s->rest16, mkey, acc, tr->targets, tr->scratch, tr->gout, tr->h_targets};
+    const bool key_ok = tr->exec && std::equal(key, key + 8, tr->g_key) && tr->g_key_n == s->n &&
                         tr->g_key_kcap == tr->kcap && tr->g_key_grads == tr->grads_mode &&
                         tr->g_key_w == tr->loss_weight && tr->g_key_shards == tr->g_shards &&
                         tr->g_key_shard == tr->g_shard;
@@ -391,7 +430,7 @@ static sc_status run_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, float* a
         ce = cudaGraphInstantiate(&tr->exec, g, 0);
         cudaGraphDestroy(g);
         if (ce != cudaSuccess) { tr->exec = nullptr; return sc_cuda_fail(ctx, ce, "graph instantiate"); }
-        std::copy(key, key + 7, tr->g_key);
+        std::copy(key, key + 8, tr->g_key);
         tr->g_key_n = s->n;
         tr->g_key_kcap = tr->kcap;
         tr->g_key_grads = tr->grads_mode;

@@ -79,6 +79,12 @@ class Trainer:
         self._targets = targets
         check(lib().sc_trainer_set_targets(self.handle, targets.cptr), self.ctx.handle)
 
+    def set_host_targets(self, pinned_ptr: int, keepalive=None) -> None:
+        """Targets in page-locked host memory at `pinned_ptr`; copied on a side
+        stream every step, overlapped with the stages before the blend."""
+        self._targets = keepalive
+        check(lib().sc_trainer_set_host_targets(self.handle, C.c_void_p(pinned_ptr)), self.ctx.handle)
+
     def set_profiling(self, on: bool) -> None:
         check(lib().sc_trainer_set_profiling(self.handle, 1 if on else 0), self.ctx.handle)
 

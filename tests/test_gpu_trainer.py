@@ -167,3 +167,24 @@ def test_bf16_storage_step_close_to_fp32(ctx):
     _, _, _, _, l16 = _run(ctx, scene, cams, tgt, cfg16, steps=5)
     assert abs(l16[0] - l32[0]) <= 2e-3 * l32[0]
     assert l16[-1] < l16[0] and l32[-1] < l32[0]
+
+
+def test_host_targets_copied_beside_the_step_match_device_targets(ctx):
+    import torch
+    scene, tl, cams, tgt, cfg = _setup(ctx, n=2000, V=2)
+    tr1, g1, _, _, l1 = _run(ctx, scene, cams, tgt, cfg, steps=2)
+    g2 = GpuSplatBuffer.upload(ctx, scene)
+    mo2 = AdamMomentBuffers(ctx, g2.capacity)
+    acc2 = ctx.storage_buffer_zeroed("acc", 4 * g2.capacity)
+    tr2 = Trainer(ctx, cfg)
+    pinned = torch.empty(tgt.size, dtype=torch.float32, pin_memory=True)
+    pinned.numpy()[:] = np.ascontiguousarray(tgt, np.float32).reshape(-1)
+    tr2.set_host_targets(pinned.data_ptr(), keepalive=pinned)
+    l2 = [tr2.step(g2, mo2, acc2, cams, t) for t in (1, 2)]
+    assert np.array_equal(tr1.images(), tr2.images())
+    assert np.allclose(l1, l2, rtol=1e-6)
+    assert np.allclose(g1.readback().flat(), g2.readback().flat(), rtol=1e-5, atol=1e-7)
+    # pageable memory is refused
+    host = np.zeros(tgt.size, np.float32)
+    with pytest.raises(Exception):
+        tr2.set_host_targets(host.ctypes.data)
