@@ -24,7 +24,6 @@ namespace sck {
 struct BlendArgs {
   uint32_t width, height, tw, th, tiles_x, tiles_y, num_tiles, stride;
   uint64_t pixels;  // per view
-  uint32_t blocked;  // warps own 8 x (4 PPT) pixel blocks (see pixel_of)
 };
 
 static BlendArgs blend_args(const sc_tiling* tl, uint32_t stride) {
@@ -35,7 +34,6 @@ static BlendArgs blend_args(const sc_tiling* tl, uint32_t stride) {
   a.num_tiles = a.tiles_x * a.tiles_y;
   a.stride = stride;
   a.pixels = (uint64_t)tl->width * tl->height;
-  a.blocked = 0;
   return a;
 }
 
@@ -77,51 +75,11 @@ __device__ __forceinline__ T block_sum(T x, T* sred) {
   return r;  // valid in thread 0
 }
 
-// Pixel placement.  Blocked (tiles whose width is a multiple of 8 and height a
-// multiple of 4 PPT): warp w owns an 8-column x 4PPT-row block of the tile,
-// lane l its column l % 8 and rows PPT (l / 8) + k, so a splat whose footprint
-// misses the block costs that warp one test instead of an evaluation per
-// pixel.  Otherwise: thread t owns column t % tw and rows PPT (t / tw) + k.
-template <int PPT>
-__device__ __forceinline__ void pixel_of(const BlendArgs& a, uint32_t tx, uint32_t ty, uint32_t& px, uint32_t& py0) {
-  const uint32_t t = threadIdx.x;
-  if (a.blocked) {
-    const uint32_t w = t >> 5, lane = t & 31, wbx = a.tw >> 3;
-    px = tx * a.tw + (w % wbx) * 8 + (lane & 7);
-    py0 = ty * a.th + (w / wbx) * (4 * PPT) + (lane >> 3) * PPT;
-  } else {
-    px = tx * a.tw + t % a.tw;
-    py0 = ty * a.th + PPT * (t / a.tw);
-  }
-}
-
-// Pixel-centre rectangle of the calling warp's pixels (all lanes call it).
-template <int PPT>
-__device__ __forceinline__ float4 warp_rect(uint32_t px, uint32_t py0) {
-  float x0 = (float)px + 0.5f, x1 = x0, y0 = (float)py0 + 0.5f, y1 = y0 + (float)(PPT - 1);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    x0 = fminf(x0, __shfl_xor_sync(FULL_MASK, x0, o));
-    x1 = fmaxf(x1, __shfl_xor_sync(FULL_MASK, x1, o));
-    y0 = fminf(y0, __shfl_xor_sync(FULL_MASK, y0, o));
-    y1 = fmaxf(y1, __shfl_xor_sync(FULL_MASK, y1, o));
-  }
-  return make_float4(x0, x1, y0, y1);
-}
-
-// Pixel-centre box outside which the splat of this record accepts no pixel:
-// the alpha >= 1/255 ellipse of the culling test with its margins (conservative
-// against eval_alpha's rounding), or everything when the conic is not positive
-// definite.
-__device__ __forceinline__ float4 footprint_box(const float4 ra, const float4 rb, const float4 rc) {
-  const CullShape cs = cull_shape(ra.x, ra.y, rb.x, rb.y, rb.z, rc.w);
-  if (cs.keep || !(cs.xh < 1e30f && cs.yh < 1e30f)) return make_float4(-INFINITY, INFINITY, -INFINITY, INFINITY);
-  return make_float4(ra.x - cs.xh - 1e-3f, ra.x + cs.xh + 1e-3f, ra.y - cs.yh - 1e-3f, ra.y + cs.yh + 1e-3f);
-}
-
-__device__ __forceinline__ bool box_misses(const float4 box, const float4 wr) {
-  return box.y < wr.x || box.x > wr.y || box.w < wr.z || box.z > wr.w;
-}
+// Pixel placement: thread t owns column t % tw and rows PPT*(t / tw) + k.
+struct PixelSet {
+  uint32_t px, py0;
+  float fx, fy0;
+};
 
 // ---------------------------------------------------------------- forward
 template <int PPT>
@@ -131,17 +89,15 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
                                                    const float* __restrict__ target, float gscale,
                                                    float4* __restrict__ dl_dc, double* __restrict__ loss,
                                                    const uint32_t* __restrict__ skip) {
-  extern __shared__ float4 sbuf[];  // records [2][B][3], footprint boxes [B]
+  extern __shared__ float4 sbuf[];  // [2][B][3]
   __shared__ double sred[8];
   if (skip && (*skip & SC_DEVERR_CAPACITY)) return;  // pair lists of this step are incomplete
   const uint32_t B = blockDim.x;
-  float4* sbox = sbuf + (size_t)6 * B;
   const uint32_t vt = blockIdx.x;
   const uint32_t v = vt / a.num_tiles, tile = vt - v * a.num_tiles;
   const uint32_t ty = tile / a.tiles_x, tx = tile - ty * a.tiles_x;
-  uint32_t px, py0;
-  pixel_of<PPT>(a, tx, ty, px, py0);
-  const float4 wr = warp_rect<PPT>(px, py0);
+  const uint32_t px = tx * a.tw + threadIdx.x % a.tw;
+  const uint32_t py0 = ty * a.th + PPT * (threadIdx.x / a.tw);
   const float fx = (float)px + 0.5f;
   const uint2 r = ranges[vt];
   const uint32_t begin = r.x, end = r.y > r.x ? r.y : r.x;
@@ -176,13 +132,9 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
     if (b + 1 < nb) { stage(b + 1); cp_async_wait_one(); } else { cp_async_wait_all(); }
     __syncthreads();
     const uint32_t cnt = min(B, end - (begin + b * B));
-    const float4* sb = sbuf + (size_t)(b & 1) * 3 * B;
-    if (threadIdx.x < cnt) sbox[threadIdx.x] = footprint_box(sb[3 * threadIdx.x], sb[3 * threadIdx.x + 1],
-                                                             sb[3 * threadIdx.x + 2]);
-    __syncthreads();
     if (!all_done) {
+      const float4* sb = sbuf + (size_t)(b & 1) * 3 * B;
       for (uint32_t k = 0; k < cnt; ++k) {
-        if (box_misses(sbox[k], wr)) continue;  // no pixel of this warp can accept the splat
         const float4 ra = sb[3 * k], rb = sb[3 * k + 1], rc = sb[3 * k + 2];
         const float dx = fx - ra.x;
         all_done = true;
@@ -231,10 +183,8 @@ template <int PPT>
 static sc_status composite_ppt(sc_ctx* ctx, const BlendArgs& a, uint32_t grid, uint32_t threads, const float4* rec,
                                const uint32_t* payloads, const uint32_t* ranges, float4* image, uint2* aux,
                                const float* target, float gscale, float4* dl_dc, double* loss, const uint32_t* d_skip) {
-  const size_t smem = (size_t)(2 * 3 + 1) * threads * sizeof(float4);
-  BlendArgs ab = a;
-  ab.blocked = (a.tw % 8 == 0 && a.th % (4 * PPT) == 0) ? 1u : 0u;
-  k_composite<PPT><<<grid, threads, smem, ctx->stream>>>(rec, payloads, reinterpret_cast<const uint2*>(ranges), ab,
+  const size_t smem = (size_t)2 * 3 * threads * sizeof(float4);
+  k_composite<PPT><<<grid, threads, smem, ctx->stream>>>(rec, payloads, reinterpret_cast<const uint2*>(ranges), a,
                                                          image, aux, target, gscale, dl_dc, loss, d_skip);
   return sc_check_launch(ctx, "k_composite");
 }
@@ -372,20 +322,17 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
                                                             const uint2* __restrict__ aux,
                                                             float4* __restrict__ proj_grad,
                                                             const uint32_t* __restrict__ skip) {
-  // records [2][B][3], acc [B][3] (float4), ids [2][B] (u32), footprint boxes [B]
-  extern __shared__ float4 sbuf[];
+  extern __shared__ float4 sbuf[];  // records [2][B][3], acc [B][3] (float4), ids [2][B]
   __shared__ uint32_t s_max;
   if (skip && (*skip & SC_DEVERR_CAPACITY)) return;
   const uint32_t B = blockDim.x;
   float4* sacc = sbuf + (size_t)6 * B;
   uint32_t* sids = reinterpret_cast<uint32_t*>(sbuf + (size_t)9 * B);
-  float4* sbox = sbuf + (size_t)9 * B + B / 2;
   const uint32_t vt = blockIdx.x;
   const uint32_t v = vt / a.num_tiles, tile = vt - v * a.num_tiles;
   const uint32_t ty = tile / a.tiles_x, tx = tile - ty * a.tiles_x;
-  uint32_t px, py0;
-  pixel_of<PPT>(a, tx, ty, px, py0);
-  const float4 wr = warp_rect<PPT>(px, py0);
+  const uint32_t px = tx * a.tw + threadIdx.x % a.tw;
+  const uint32_t py0 = ty * a.th + PPT * (threadIdx.x / a.tw);
   const float fx = (float)px + 0.5f;
   const uint2 r = ranges[vt];
   const uint32_t begin = r.x, end = r.y > r.x ? r.y : r.x;
@@ -457,12 +404,8 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
     const uint32_t lo = hi - min(B, hi - begin);
     const uint32_t cnt = hi - lo;
     const float4* sb = sbuf + (size_t)(b & 1) * 3 * B;
-    if (threadIdx.x < cnt) sbox[threadIdx.x] = footprint_box(sb[3 * threadIdx.x], sb[3 * threadIdx.x + 1],
-                                                             sb[3 * threadIdx.x + 2]);
-    __syncthreads();
     if (!__all_sync(FULL_MASK, all_done)) {
       for (int k = (int)cnt - 1; k >= 0; --k) {
-        if (box_misses(sbox[k], wr)) continue;  // no pixel of this warp can accept the splat
         const uint32_t j = lo + (uint32_t)k;
         // this thread's sums over its pixels: h = dL/dalpha * gauss (the opacity
         // gradient), its first and second moments in (dx, dy), and the colour
@@ -543,15 +486,13 @@ template <int PPT>
 static sc_status backward_ppt(sc_ctx* ctx, const BlendArgs& a, uint32_t grid, uint32_t threads, const float4* rec,
                               const uint32_t* payloads, const uint32_t* ranges, const float4* fwd, const float4* dl_dc,
                               int mode, const uint2* aux, float4* proj_grad, const uint32_t* d_skip) {
-  const size_t smem = (size_t)10 * threads * sizeof(float4) + (size_t)2 * threads * sizeof(uint32_t);
-  BlendArgs ab = a;
-  ab.blocked = (a.tw % 8 == 0 && a.th % (4 * PPT) == 0) ? 1u : 0u;
+  const size_t smem = (size_t)9 * threads * sizeof(float4) + (size_t)2 * threads * sizeof(uint32_t);
   if (mode == SC_BWD_EXACT)
     k_composite_backward<PPT, SC_BWD_EXACT><<<grid, threads, smem, ctx->stream>>>(
-        rec, payloads, reinterpret_cast<const uint2*>(ranges), ab, fwd, dl_dc, aux, proj_grad, d_skip);
+        rec, payloads, reinterpret_cast<const uint2*>(ranges), a, fwd, dl_dc, aux, proj_grad, d_skip);
   else
     k_composite_backward<PPT, SC_BWD_REF><<<grid, threads, smem, ctx->stream>>>(
-        rec, payloads, reinterpret_cast<const uint2*>(ranges), ab, fwd, dl_dc, aux, proj_grad, d_skip);
+        rec, payloads, reinterpret_cast<const uint2*>(ranges), a, fwd, dl_dc, aux, proj_grad, d_skip);
   return sc_check_launch(ctx, "k_composite_backward");
 }
 
