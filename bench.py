@@ -270,6 +270,9 @@ def run_ours(args):
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args, scene, tscene, tl, cams_for)
+    psnr = None
+    if rank == 0 and ws == 1 and not args.no_psnr:
+        psnr = psnr_check(ctx, args)
 
     if rank == 0:
         line = {
@@ -286,7 +289,7 @@ def run_ours(args):
                        "l2": "inputs larger than L2 (params, pair lists and images >> 126 MB)",
                        "parallelism": f"{ws} GPUs, one scene each (no exchange)" if ws > 1 else "single GPU"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-            "clocks": clocks, "loss": loss,
+            "clocks": clocks, "loss": loss, "psnr": psnr,
         }
         print(json.dumps(line))
     del tr
@@ -427,6 +430,40 @@ def run_views(args, ws, rank, local, pg):
         pg.destroy_process_group()
 
 
+def psnr_check(ctx, args, iters=100, n=200_000, V=4, W=480, H=272):
+    """The metric's "same PSNR" claim, measured beside the timed run (untimed):
+    the same seeded scene trained `iters` iterations in the BF16 form and in
+    the plain FP32 form on V fixed views; PSNR of the final renders against
+    the targets (values in [0, 1])."""
+    import nanotracer_b200 as nt
+    from nanotracer_b200.scene import FOV_Y, orbit_views, perturbed, random_scene
+    from nanotracer_b200.train import TrainConfig, Trainer, render_targets
+    scene = random_scene(n, 0x5EED5EED)
+    tl = nt.TilingParams(W, H, 16, 8.0)
+    cams = [nt.CameraUniform.from_pose(*p, FOV_Y, W, H, n) for p in orbit_views(V, 0)]
+    tgt = render_targets(ctx, perturbed(scene), cams, tl)
+    out = {}
+    for form in ("bf16", "fp32"):
+        bf16 = form == "bf16"
+        cfg = TrainConfig(n_views=V, width=W, height=H, tile_w=16, tile_h=16, depth_max=8.0, exact_backward=True,
+                          use_graph=True, bf16=bf16, densify=False)
+        g = nt.GpuSplatBuffer.upload(ctx, scene, bf16_rest=bf16)
+        mo = nt.AdamMomentBuffers(ctx, g.capacity, bf16=bf16)
+        acc = ctx.storage_buffer_zeroed("acc", 4 * g.capacity)
+        tr = Trainer(ctx, cfg)
+        tb = ctx.storage_buffer("targets", tgt)
+        tr.set_targets(tb)
+        for t in range(1, iters + 1):
+            tr.step(g, mo, acc, cams, t)
+        img = tr.images()[..., :3]
+        mse = float(np.mean((img.astype(np.float64) - tgt) ** 2))
+        out[form] = round(10.0 * math.log10(1.0 / max(mse, 1e-30)), 3)
+        del tr
+    out["delta_db"] = round(out["bf16"] - out["fp32"], 3)
+    out["workload"] = f"{n} splats, {V} views {W}x{H}, {iters} iterations from the same start, exact backward"
+    return out
+
+
 def cpu_baseline(args, scene, tscene, tl, cams_for):
     """The oracle (CPU restatement of the reference path) on the host cores: one
     view of the workload per sample (fwd+bwd over all splats + Adam over all
@@ -513,6 +550,7 @@ def main():
     ap.add_argument("--view-path", action="store_true", help="run the split-views path even on one GPU")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-psnr", action="store_true", help="skip the untimed BF16-vs-FP32 PSNR side run")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

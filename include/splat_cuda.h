@@ -212,7 +212,9 @@ sc_status sc_bins_info(const sc_bins* b, uint64_t* total_pairs, uint32_t* num_ti
 
 /* Stable LSD radix sort (onesweep, decoupled look-back) of n (key, value)
  * pairs in place; keys_tmp / vals_tmp are ping-pong buffers of the same size.
- * key_bits: number of low key bits that can be non-zero.  RadixSort::sort,
+ * key_bits: the pairs are ordered by the low key_bits bits of the key; any
+ * higher bits travel with the key and keep their input order within equal
+ * low bits (so key_bits = the width of the keys sorts them fully).  RadixSort::sort,
  * radix_sort.rs:144-303 (32 one-bit passes there; 8-bit digits here). */
 sc_status sc_radix_sort_u32(sc_ctx* ctx, uint32_t* keys, uint32_t* vals, uint32_t* keys_tmp, uint32_t* vals_tmp,
                             uint64_t n, uint32_t key_bits);

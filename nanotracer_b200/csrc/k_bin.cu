@@ -20,6 +20,7 @@ namespace sck {
 struct BinArgs {
   uint32_t tw, th, tiles_x, tiles_y, num_tiles;
   float depth_max;
+  uint32_t tile_bits;  // presorted pipeline: pair key = (view << tile_bits) | tile
 };
 
 static BinArgs bin_args(const sc_tiling* tl) {
@@ -29,6 +30,8 @@ static BinArgs bin_args(const sc_tiling* tl) {
   a.tiles_y = (tl->height + tl->tile_h - 1) / tl->tile_h;
   a.num_tiles = a.tiles_x * a.tiles_y;
   a.depth_max = tl->depth_max;
+  a.tile_bits = 0;
+  while ((1u << a.tile_bits) <= a.num_tiles) ++a.tile_bits;  // 2^tile_bits > num_tiles
   return a;
 }
 
@@ -115,11 +118,13 @@ sc_status launch_tile_emit(sc_ctx* ctx, const float4* rec, uint32_t n, uint32_t 
   return sc_check_launch(ctx, "k_tile_emit");
 }
 
-// tile_ranges.wgsl:22-41.  tile of a key: REF32 key >> 16, NATIVE key >> 32,
-// presorted u32 key itself (mode 2).
+// tile_ranges.wgsl:22-41.  tile of a key: REF32 key >> 16, NATIVE key >> 32;
+// presorted u32 key (mode 2) (view << tile_bits) | tile, range index
+// view * tiles_per_view + tile.  Boundaries are changes of the whole key.
 template <int MODE>
 __global__ void k_tile_ranges(const void* __restrict__ keys_v, const uint64_t* __restrict__ d_total, uint64_t cap,
-                              uint32_t num_tiles, uint32_t* __restrict__ ranges) {
+                              uint32_t num_tiles, uint32_t tiles_per_view, uint32_t tile_bits,
+                              uint32_t* __restrict__ ranges) {
   const uint64_t K = min(*d_total, cap);
   for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < K; j += (uint64_t)gridDim.x * blockDim.x) {
     uint64_t t, tp = ~0ull, tn = ~0ull;
@@ -139,23 +144,29 @@ __global__ void k_tile_ranges(const void* __restrict__ keys_v, const uint64_t* _
       if (j > 0) tp = k[j - 1];
       if (j + 1 < K) tn = k[j + 1];
     }
-    if (t >= num_tiles) continue;
-    if (tp != t) ranges[2 * t] = (uint32_t)j;
-    if (tn != t) ranges[2 * t + 1] = (uint32_t)(j + 1);
+    uint64_t idx = t;
+    if (MODE == 2) {
+      const uint32_t tile = (uint32_t)t & ((1u << tile_bits) - 1u);
+      if (tile >= tiles_per_view) continue;
+      idx = (uint64_t)(t >> tile_bits) * tiles_per_view + tile;
+    }
+    if (idx >= num_tiles) continue;
+    if (tp != t) ranges[2 * idx] = (uint32_t)j;
+    if (tn != t) ranges[2 * idx + 1] = (uint32_t)(j + 1);
   }
 }
 
 sc_status launch_tile_ranges(sc_ctx* ctx, const void* keys, int key_mode, const uint64_t* d_total, uint64_t cap,
-                             uint32_t num_tiles, uint32_t* ranges) {
+                             uint32_t num_tiles, uint32_t* ranges, uint32_t tiles_per_view, uint32_t tile_bits) {
   SC_CUDA_TRY(ctx, cudaMemsetAsync(ranges, 0, (size_t)num_tiles * 8, ctx->stream), "memset ranges");
   if (cap == 0) return SC_OK;
   const unsigned g = (unsigned)std::min<uint64_t>(sc_div_up(cap, 256), (uint64_t)ctx->sm_count * 16);
   if (key_mode == 0)
-    k_tile_ranges<0><<<g, 256, 0, ctx->stream>>>(keys, d_total, cap, num_tiles, ranges);
+    k_tile_ranges<0><<<g, 256, 0, ctx->stream>>>(keys, d_total, cap, num_tiles, 0, 0, ranges);
   else if (key_mode == 1)
-    k_tile_ranges<1><<<g, 256, 0, ctx->stream>>>(keys, d_total, cap, num_tiles, ranges);
+    k_tile_ranges<1><<<g, 256, 0, ctx->stream>>>(keys, d_total, cap, num_tiles, 0, 0, ranges);
   else
-    k_tile_ranges<2><<<g, 256, 0, ctx->stream>>>(keys, d_total, cap, num_tiles, ranges);
+    k_tile_ranges<2><<<g, 256, 0, ctx->stream>>>(keys, d_total, cap, num_tiles, tiles_per_view, tile_bits, ranges);
   return sc_check_launch(ctx, "k_tile_ranges");
 }
 
@@ -224,7 +235,7 @@ __global__ void __launch_bounds__(EMIT_WARPS * 32) k_presorted_emit(
       if (!rect_of(ra, rb, a, x0, y0, x1, y1)) { x0 = 0; y0 = 0; x1 = -1; y1 = -1; }
       cs = cull_shape(ra.x, ra.y, rb.x, rb.y, rb.z, rc.w);
       test = cull && !cs.keep;
-      vbase = v * a.num_tiles;
+      vbase = v << a.tile_bits;
     }
   }
   uint32_t* wk = sk[warp];

@@ -223,17 +223,23 @@ template <> struct RsCfg<uint32_t> { static constexpr int IPT = 16; };
 template <> struct RsCfg<uint64_t> { static constexpr int IPT = 12; };
 
 // Global digit histograms of all passes in one read of the keys.
+// digit mask of pass p when only the low key_bits bits are sorted
+__host__ __device__ __forceinline__ uint32_t rs_digit_mask(uint32_t key_bits, int p) {
+  const int rem = (int)key_bits - 8 * p;
+  return rem >= 8 ? 0xFFu : (rem <= 0 ? 0u : (1u << rem) - 1u);
+}
+
 template <typename K>
 __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const K* __restrict__ keys, uint64_t n_cap,
                                                         const uint64_t* __restrict__ d_n, int passes,
-                                                        uint32_t* __restrict__ hist /* passes x 256 */) {
+                                                        uint32_t key_bits, uint32_t* __restrict__ hist /* passes x 256 */) {
   __shared__ uint32_t sh[8][RS_RADIX];
   for (int t = threadIdx.x; t < passes * RS_RADIX; t += RS_THREADS) (&sh[0][0])[t] = 0;
   __syncthreads();
   const uint64_t n = d_n ? min(*d_n, n_cap) : n_cap;
   for (uint64_t i = (uint64_t)blockIdx.x * RS_THREADS + threadIdx.x; i < n; i += (uint64_t)gridDim.x * RS_THREADS) {
     const K k = keys[i];
-    for (int p = 0; p < passes; ++p) atomicAdd(&sh[p][(uint32_t)(k >> (8 * p)) & 0xFFu], 1u);
+    for (int p = 0; p < passes; ++p) atomicAdd(&sh[p][(uint32_t)(k >> (8 * p)) & rs_digit_mask(key_bits, p)], 1u);
   }
   __syncthreads();
   for (int t = threadIdx.x; t < passes * RS_RADIX; t += RS_THREADS) {
@@ -291,10 +297,11 @@ __device__ __forceinline__ void rs_pass_tile(RsSmem<K>& sm, const K* __restrict_
                                              const uint32_t* __restrict__ vin, K* __restrict__ kout,
                                              uint32_t* __restrict__ vout, uint64_t n, int shift,
                                              const uint32_t* __restrict__ digit_base, unsigned* __restrict__ lookback,
-                                             uint32_t* __restrict__ err, uint32_t tile, uint64_t tbase) {
+                                             uint32_t* __restrict__ err, uint32_t tile, uint64_t tbase, int dbits) {
   constexpr int IPT = RsCfg<K>::IPT;
   constexpr int TILE = RS_THREADS * IPT;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t dmask = (1u << dbits) - 1u;
   // warp-striped layout: item k of lane l in warp w is input slot w*32*IPT + k*32 + l
   const uint32_t wslot = (uint32_t)warp * 32 * IPT;
   const uint64_t wbase = tbase + wslot;
@@ -315,13 +322,15 @@ __device__ __forceinline__ void rs_pass_tile(RsSmem<K>& sm, const K* __restrict_
 #pragma unroll
   for (int k = 0; k < IPT; ++k) {
     const bool valid = FULL || wbase + (uint64_t)k * 32 + lane < n;
-    const uint32_t d = (uint32_t)(key[k] >> shift) & 0xFFu;
+    const uint32_t d = (uint32_t)(key[k] >> shift) & dmask;
     unsigned peers = FULL ? 0xffffffffu : __ballot_sync(0xffffffffu, valid);
 #pragma unroll
     for (int b = 0; b < 8; ++b) {
-      const bool bit = (d >> b) & 1u;
-      const unsigned m = __ballot_sync(0xffffffffu, bit);
-      peers &= bit ? m : ~m;
+      if (b < dbits) {  // digits narrower than 8 bits (the last pass of a short key) need fewer ballots
+        const bool bit = (d >> b) & 1u;
+        const unsigned m = __ballot_sync(0xffffffffu, bit);
+        peers &= bit ? m : ~m;
+      }
     }
     const int leader = valid ? 31 - __clz(peers) : lane;
     uint32_t old = 0;
@@ -394,7 +403,7 @@ __device__ __forceinline__ void rs_pass_tile(RsSmem<K>& sm, const K* __restrict_
 #pragma unroll
   for (int k = 0; k < IPT; ++k) {
     if (FULL || wbase + (uint64_t)k * 32 + lane < n) {
-      const uint32_t dd = (uint32_t)(key[k] >> shift) & 0xFFu;
+      const uint32_t dd = (uint32_t)(key[k] >> shift) & dmask;
       const uint32_t pos = sm.tile_excl[dd] + sm.warp_hist[warp][dd] + rank[k];
       sm.keys[pos] = key[k];
       sm.src[pos] = (uint16_t)(wslot + k * 32 + lane);
@@ -405,7 +414,7 @@ __device__ __forceinline__ void rs_pass_tile(RsSmem<K>& sm, const K* __restrict_
   const uint32_t valid = FULL ? (uint32_t)TILE : (uint32_t)min((uint64_t)TILE, n - tbase);
   for (uint32_t idx = threadIdx.x; idx < valid; idx += RS_THREADS) {
     const K kk = sm.keys[idx];
-    const uint32_t dd = (uint32_t)(kk >> shift) & 0xFFu;
+    const uint32_t dd = (uint32_t)(kk >> shift) & dmask;
     const long long g = (long long)sm.out_base[dd] + (long long)idx;
     if (g < 0 || (uint64_t)g >= n) {  // only after a look-back gave up: keep the write in bounds
       atomicOr(err, SC_DEVERR_TIMEOUT);
@@ -427,7 +436,7 @@ __global__ void __launch_bounds__(RS_THREADS, 4) k_rs_pass(const K* __restrict__
                                                         uint64_t n_cap, const uint64_t* __restrict__ d_n, int shift,
                                                         const uint32_t* __restrict__ digit_base,
                                                         unsigned* __restrict__ lookback, unsigned* __restrict__ ticket,
-                                                        uint32_t* __restrict__ err) {
+                                                        uint32_t* __restrict__ err, int dbits) {
   constexpr int IPT = RsCfg<K>::IPT;
   constexpr int TILE = RS_THREADS * IPT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -440,9 +449,9 @@ __global__ void __launch_bounds__(RS_THREADS, 4) k_rs_pass(const K* __restrict__
   const uint64_t tbase = (uint64_t)tile * TILE;
   if (tbase >= n) return;  // every later ticket is beyond n as well: nobody waits on this tile
   if (tbase + TILE <= n)
-    rs_pass_tile<K, true>(sm, kin, vin, kout, vout, n, shift, digit_base, lookback, err, tile, tbase);
+    rs_pass_tile<K, true>(sm, kin, vin, kout, vout, n, shift, digit_base, lookback, err, tile, tbase, dbits);
   else
-    rs_pass_tile<K, false>(sm, kin, vin, kout, vout, n, shift, digit_base, lookback, err, tile, tbase);
+    rs_pass_tile<K, false>(sm, kin, vin, kout, vout, n, shift, digit_base, lookback, err, tile, tbase, dbits);
 }
 
 size_t radix_scratch_bytes(uint64_t n, uint32_t key_bytes) {
@@ -472,7 +481,7 @@ sc_status radix_sort(sc_ctx* ctx, K* keys, uint32_t* vals, K* keys_tmp, uint32_t
   SC_CUDA_TRY(ctx, cudaMemsetAsync(scratch, 0, need, ctx->stream), "memset radix scratch");
   const unsigned hist_blocks = (unsigned)std::min<uint64_t>(sc_div_up(n_cap, RS_THREADS),
                                                             (uint64_t)ctx->sm_count * RS_HIST_BLOCKS_PER_SM);
-  k_rs_hist<K><<<hist_blocks, RS_THREADS, 0, ctx->stream>>>(keys, n_cap, d_n, passes, hist);
+  k_rs_hist<K><<<hist_blocks, RS_THREADS, 0, ctx->stream>>>(keys, n_cap, d_n, passes, key_bits, hist);
   SC_TRY(sc_check_launch(ctx, "k_rs_hist"));
   k_rs_hist_scan<<<passes, RS_RADIX, 0, ctx->stream>>>(hist);
   SC_TRY(sc_check_launch(ctx, "k_rs_hist_scan"));
@@ -485,10 +494,11 @@ sc_status radix_sort(sc_ctx* ctx, K* keys, uint32_t* vals, K* keys_tmp, uint32_t
   }
   K* kin = keys; uint32_t* vin = vals; K* kout = keys_tmp; uint32_t* vout = vals_tmp;
   for (int p = 0; p < passes; ++p) {
+    const int dbits = std::min(8, (int)key_bits - 8 * p);
     k_rs_pass<K><<<(unsigned)tiles, RS_THREADS, smem, ctx->stream>>>(kin, vin, kout, vout, n_cap, d_n, 8 * p,
                                                                      hist + p * RS_RADIX,
                                                                      lookback + (size_t)p * tiles * RS_RADIX,
-                                                                     tickets + p, ctx->d_error);
+                                                                     tickets + p, ctx->d_error, dbits);
     SC_TRY(sc_check_launch(ctx, "k_rs_pass"));
     std::swap(kin, kout);
     std::swap(vin, vout);
@@ -527,7 +537,7 @@ sc_status selftest_lookback_timeout(sc_ctx* ctx) {
   SC_CUDA_TRY(ctx, cudaFuncSetAttribute(k_rs_pass<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
               "smem attr");
   k_rs_pass<K><<<2, RS_THREADS, smem, ctx->stream>>>(keys, vals, kout, vout, n, nullptr, 0, hist, lookback, ticket,
-                                                     ctx->d_error);
+                                                     ctx->d_error, 8);
   SC_TRY(sc_check_launch(ctx, "k_rs_pass (timeout self-test)"));
   return sc_check_device_error(ctx);
 }

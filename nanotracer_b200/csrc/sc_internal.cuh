@@ -287,8 +287,10 @@ sc_status launch_tile_count(sc_ctx* ctx, const float4* rec, uint32_t n, uint32_t
 sc_status launch_tile_emit(sc_ctx* ctx, const float4* rec, uint32_t n, uint32_t stride, uint32_t n_views,
                            const sc_tiling* tl, const uint32_t* offsets, int key_mode, void* keys,
                            uint32_t* payloads, uint64_t cap);
+// key_mode 2: presorted keys (view << tile_bits) | tile, tiles_per_view tiles per view
 sc_status launch_tile_ranges(sc_ctx* ctx, const void* keys, int key_mode, const uint64_t* d_total, uint64_t cap,
-                             uint32_t num_tiles, uint32_t* ranges);
+                             uint32_t num_tiles, uint32_t* ranges, uint32_t tiles_per_view = 0,
+                             uint32_t tile_bits = 0);
 // depth-presorted emission for the native pipeline
 sc_status launch_presorted_counts(sc_ctx* ctx, const uint32_t* counts_by_id, uint32_t stride, uint32_t n_views,
                                   const uint32_t* sorted_ids, uint32_t* counts);

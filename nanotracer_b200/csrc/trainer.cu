@@ -255,14 +255,16 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
                                     &tr->cfg.tiling, tr->keys, tr->vals, tr->kcap, ctx->d_error,
                                     (int)tr->cfg.tile_cull));
   mark(tr, 4, capturing);
+  // keys are (view << tile_bits) | tile: the stable sort on the tile bits alone
+  // groups the pairs by tile, then view (the emission is view-major), then depth
   const uint32_t all_tiles = V * tr->T;
-  SC_TRY(sck::radix_sort<uint32_t>(ctx, tr->keys, tr->vals, tr->keys_tmp, tr->vals_tmp, tr->kcap,
-                                   bits_for(all_tiles), tr->d_total, tr->scratch, tr->scratch_bytes,
-                                   &in_tmp));
+  const uint32_t tile_bits = bits_for(tr->T);
+  SC_TRY(sck::radix_sort<uint32_t>(ctx, tr->keys, tr->vals, tr->keys_tmp, tr->vals_tmp, tr->kcap, tile_bits,
+                                   tr->d_total, tr->scratch, tr->scratch_bytes, &in_tmp));
   const uint32_t* skeys = in_tmp ? tr->keys_tmp : tr->keys;
   const uint32_t* svals = in_tmp ? tr->vals_tmp : tr->vals;
   mark(tr, 5, capturing);
-  SC_TRY(sck::launch_tile_ranges(ctx, skeys, 2, tr->d_total, tr->kcap, all_tiles, tr->ranges));
+  SC_TRY(sck::launch_tile_ranges(ctx, skeys, 2, tr->d_total, tr->kcap, all_tiles, tr->ranges, tr->T, tile_bits));
   mark(tr, 6, capturing);
   if (tr->h_targets) SC_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, tr->ev_copied, 0), "join");
   const float weight = tr->grads_mode ? tr->loss_weight : 1.0f / (float)V;
@@ -321,6 +323,10 @@ sc_status sc_trainer_create(sc_ctx* ctx, const sc_train_config* cfg, sc_trainer*
   tr->tiles_x = (t.width + t.tile_w - 1) / t.tile_w;
   tr->tiles_y = (t.height + t.tile_h - 1) / t.tile_h;
   tr->T = tr->tiles_x * tr->tiles_y;
+  if (bits_for(tr->T) + bits_for(tr->V - 1) > 32) {
+    delete tr;
+    return sc_fail(ctx, SC_ERR_INVALID_ARG, "too many tiles x views for 32-bit pair keys");
+  }
   tr->P = (uint64_t)t.width * t.height;
   const size_t pix = (size_t)tr->V * tr->P;
   cudaError_t e = cudaMallocHost(&tr->h_params, sizeof(StepParams));

@@ -412,3 +412,15 @@ def test_tonemap_headless_buffer(ctx):
     rgb = img[0, :, :3] / (1 + np.maximum(img[0, :, :3], 0))
     want = np.concatenate([np.round(np.clip(srgb(rgb), 0, 1) * 255), np.round(img[0, :, 3:] * 255)], 1)
     assert np.abs(px.astype(int) - want.astype(int)).max() <= 1
+
+
+def test_sort_on_low_key_bits_keeps_high_bits_in_input_order(ctx):
+    """key_bits below the key width: ordered by the low bits only, stable, the
+    high bits carried along (the trainer's (view << tile_bits) | tile keys)."""
+    rng = np.random.default_rng(11)
+    n = 300_001
+    keys = ((rng.integers(0, 8, n, dtype=np.uint64) << 13) | rng.integers(0, 8160, n, dtype=np.uint64)).astype(np.uint32)
+    vals = np.arange(n, dtype=np.uint32)
+    sk, sv = _sort_gpu(ctx, keys, vals, 13, 4)
+    order = np.argsort(keys & 0x1FFF, kind="stable")
+    assert np.array_equal(sv, order.astype(np.uint32)) and np.array_equal(sk, keys[order])
