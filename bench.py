@@ -248,6 +248,7 @@ def run_ours(args):
     tiles = V * tl.num_tiles()
     rest_b = 90 if bf16 else 180
     mom_b = 59 * 2 * (2 if bf16 else 4)
+    items = st.get("items") or 0
     algo = {
         "project": N * (56 + rest_b) + V * N * (48 + 8 + 4 + 4),
         "depth_sort": 5 * V * N * 24,
@@ -255,6 +256,10 @@ def run_ours(args):
         "emit": V * N * (4 + 16 + 4) + K * 8,
         "tile_sort": 2 * K * 16 + K * 4,
         "ranges": K * 4 + tiles * 8,
+        # two-level binning: items (super tile, splat)
+        "item_emit": V * N * (4 + 16 + 4) + items * 8,
+        "item_sort": 2 * items * 16 + items * 4,
+        "tile_lists": items * (4 + 48 + 2) + items * (4 + 2) + K * 4 + tiles * 16,
         "blend_fwd": K * (4 + 48) + V * P * (16 + 8 + 12 + 16),
         "blend_bwd": K * (4 + 48) + V * P * (16 + 16 + 8) + V * N * 48 * 2,
         "bwd_adam": N * (56 + rest_b + 2 * rest_b) + V * N * 48 + N * (mom_b * 2) + N * 8,

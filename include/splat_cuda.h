@@ -324,8 +324,10 @@ typedef struct sc_train_config {
   sc_adam_groups adam;         /* per-group learning rates                        */
   uint32_t bwd_mode;           /* sc_bwd_mode                                    */
   uint32_t use_graph;          /* capture the iteration as a CUDA graph          */
-  uint32_t blend_batch;        /* splats staged per shared-memory batch (0=auto) */
-  uint32_t sort_mode;          /* 0 = auto, 1 = depth presort + tile pass, 2 = 64-bit key sort */
+  uint32_t blend_batch;        /* reserved, 0 (the blend stages one splat per thread per batch) */
+  uint32_t sort_mode;          /* 0 = auto (two-level), 1 = depth presort + stable sort of the
+                                  (tile, splat) pairs, 2 = depth presort + two-level binning
+                                  (super tiles of 4x4 tiles, per-tile lists filled in depth order) */
   uint32_t tile_cull;          /* drop (tile, splat) pairs whose alpha stays below 1/255 over the
                                   whole tile (images unchanged: the blend skips those pairs) */
   float log_scale_min, log_scale_max, opacity_logit_max; /* train.rs:37-39 */
@@ -354,10 +356,11 @@ sc_status sc_trainer_images(const sc_trainer* tr, const float** images);
 /* pairs: (tile, splat) pairs of the last step (all views); n_kernels: kernel
  * launches per step; names / avg_ms (arrays of SC_TRAINER_STAGES, nullable):
  * stage names and average device time per stage in ms over the steps since
- * profiling was enabled. */
+ * profiling was enabled; items (nullable): two-level binning items of the last
+ * step (0 on the pair-sort path). */
 #define SC_TRAINER_STAGES 9
 sc_status sc_trainer_stats(const sc_trainer* tr, uint64_t* pairs, uint32_t* n_kernels, const char** names,
-                           float* avg_ms);
+                           float* avg_ms, uint64_t* items);
 /* Record CUDA events between the stages of each step (also inside the graph). */
 sc_status sc_trainer_set_profiling(sc_trainer* tr, int enabled);
 

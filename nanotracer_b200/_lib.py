@@ -135,7 +135,7 @@ _PROTOS = {
     "sc_trainer_set_host_targets": (ST, [P, P]),
     "sc_trainer_step": (ST, [P, P, P, P, P, U64, C.POINTER(C.c_double)]),
     "sc_trainer_images": (ST, [P, C.POINTER(P)]),
-    "sc_trainer_stats": (ST, [P, C.POINTER(U64), C.POINTER(U32), P, P]),
+    "sc_trainer_stats": (ST, [P, C.POINTER(U64), C.POINTER(U32), P, P, C.POINTER(U64)]),
     "sc_trainer_set_profiling": (ST, [P, I32]),
     "sc_selftest_wait_timeout": (ST, [P]),
     "sc_trainer_step_grads": (ST, [P, P, P, F32, U32, U32, P, C.POINTER(C.c_double)]),

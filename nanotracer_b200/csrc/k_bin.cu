@@ -305,4 +305,276 @@ sc_status launch_presorted_emit(sc_ctx* ctx, const float4* rec, uint32_t stride,
   return sc_check_launch(ctx, "k_presorted_emit");
 }
 
+// ---------------------------------------------------------------- two-level binning
+// Super tiles of SC_SUPER x SC_SUPER tiles.  Items (super tile, splat) are
+// emitted in depth order and grouped per super tile by a short stable sort;
+// then one CTA per super tile decides for each of its items which of the 16
+// tiles it covers (the same splat_row_span test as the pair counting) and
+// appends the splat to those tiles' lists in item order, so every tile's list
+// is the depth-ordered list of the pair pipeline without sorting the pairs.
+uint32_t super_tiles_per_view(const sc_tiling* tl) {
+  const BinArgs a = bin_args(tl);
+  return ((a.tiles_x + SC_SUPER - 1) / SC_SUPER) * ((a.tiles_y + SC_SUPER - 1) / SC_SUPER);
+}
+
+static uint32_t super_bits_for(uint32_t n) {  // 2^b > n
+  uint32_t b = 0;
+  while ((1ull << b) <= n) ++b;
+  return b;
+}
+
+// Same warp-staged emission as k_presorted_emit; a lane regenerates its few
+// items for every chunk that holds some of them.
+__global__ void __launch_bounds__(EMIT_WARPS * 32) k_super_emit(
+    const float4* __restrict__ rec, uint32_t stride, uint32_t n_views, const uint32_t* __restrict__ sorted_ids,
+    const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ counts_by_id, BinArgs a, uint32_t super_x,
+    uint32_t super_bits, uint32_t* __restrict__ keys, uint32_t* __restrict__ payloads, uint64_t cap,
+    uint32_t* __restrict__ err, int cull) {
+  __shared__ uint32_t sk[EMIT_WARPS][EMIT_WCHUNK], sp[EMIT_WARPS][EMIT_WCHUNK];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t total = (uint64_t)n_views * stride;
+  const uint64_t jw = (uint64_t)blockIdx.x * blockDim.x + (uint64_t)warp * 32;
+  if (jw >= total) return;
+  const uint64_t j = jw + lane;
+  const uint64_t jend = jw + 32 < total ? jw + 32 : total;
+  const uint64_t wlo = offsets[jw], whi = offsets[jend];
+  if (lane == 0 && whi > cap) atomicOr(err, SC_DEVERR_CAPACITY);
+  uint32_t cnt = 0, id = 0, vkey = 0;
+  uint64_t off = 0;
+  int x0 = 0, y0 = 0, x1 = -1, y1 = -1;
+  CullShape cs{};
+  bool test = false;
+  if (j < total) {
+    const uint32_t v = (uint32_t)(j / stride);
+    id = sorted_ids[j];
+    const size_t o = (size_t)v * stride + id;
+    cnt = counts_by_id[o];
+    if (cnt) {
+      off = offsets[j];
+      const float4 ra = rec[3 * o], rb = rec[3 * o + 1], rc = rec[3 * o + 2];
+      if (!rect_of(ra, rb, a, x0, y0, x1, y1)) { x0 = 0; y0 = 0; x1 = -1; y1 = -1; }
+      cs = cull_shape(ra.x, ra.y, rb.x, rb.y, rb.z, rc.w);
+      test = (cull & 1) && !cs.keep;
+      vkey = v << super_bits;
+    }
+  }
+  uint32_t* wk = sk[warp];
+  uint32_t* wp = sp[warp];
+  for (uint64_t cb = wlo; cb < whi; cb += EMIT_WCHUNK) {
+    const uint64_t ce = cb + EMIT_WCHUNK < whi ? cb + EMIT_WCHUNK : whi;
+    if (cnt && off < ce && off + cnt > cb) {
+      uint32_t w = 0;
+      for_each_super_span(cs, test, x0, y0, x1, y1, a.tw, a.th, [&](int sy, int sx0, int sx1) {
+        for (int sx = sx0; sx <= sx1; ++sx, ++w) {
+          const uint64_t g = off + w;
+          if (w < cnt && g >= cb && g < ce) {
+            wk[g - cb] = vkey | ((uint32_t)sy * super_x + (uint32_t)sx);
+            wp[g - cb] = id;
+          }
+        }
+      });
+      for (; w < cnt; ++w) {  // count and emission disagreed: pad with a key that sorts last
+        const uint64_t g = off + w;
+        if (g >= cb && g < ce) { wk[g - cb] = 0xFFFFFFFFu; wp[g - cb] = 0; }
+      }
+    }
+    __syncwarp();
+    const uint32_t n = (uint32_t)(ce - cb);
+    for (uint32_t t = lane; t < n; t += 32) {
+      const uint64_t g = cb + t;
+      if (g < cap) {
+        keys[g] = wk[t];
+        payloads[g] = wp[t];
+      }
+    }
+    __syncwarp();
+  }
+}
+
+sc_status launch_super_emit(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
+                            const uint32_t* sorted_ids, const uint32_t* offsets, const uint32_t* counts_by_id,
+                            const sc_tiling* tl, uint32_t* keys, uint32_t* payloads, uint64_t cap, uint32_t* d_error,
+                            int cull) {
+  const uint64_t total = (uint64_t)n_views * stride;
+  if (total == 0) return SC_OK;
+  const BinArgs a = bin_args(tl);
+  const uint32_t sx = (a.tiles_x + SC_SUPER - 1) / SC_SUPER;
+  const uint32_t bits = super_bits_for(super_tiles_per_view(tl));
+  k_super_emit<<<(unsigned)sc_div_up(total, EMIT_WARPS * 32), EMIT_WARPS * 32, 0, ctx->stream>>>(
+      rec, stride, n_views, sorted_ids, offsets, counts_by_id, a, sx, bits, keys, payloads, cap, d_error, cull);
+  return sc_check_launch(ctx, "k_super_emit");
+}
+
+constexpr int SUPER_THREADS = 256;
+constexpr int SUPER_TILES = SC_SUPER * SC_SUPER;  // 16 tiles, one bit each in a 16-bit mask
+
+// Member tiles of one item: bit (c * SC_SUPER + a) for tile (sx*4 + a, sy*4 + c).
+__device__ __forceinline__ uint32_t super_member_mask(const float4 ra, const float4 rb, const float4 rc,
+                                                      const BinArgs& a, int cull, int tx0, int ty0) {
+  int x0, y0, x1, y1;
+  if (!rect_of(ra, rb, a, x0, y0, x1, y1)) return 0u;
+  const CullShape cs = cull_shape(ra.x, ra.y, rb.x, rb.y, rb.z, rc.w);
+  const bool test = (cull & 1) && !cs.keep;
+  uint32_t mask = 0;
+#pragma unroll
+  for (int c = 0; c < SC_SUPER; ++c) {
+    const int ty = ty0 + c;
+    if (ty < y0 || ty > y1) continue;
+    int lo, hi;
+    if (!splat_row_span(cs, test, ty, x0, x1, a.tw, a.th, lo, hi)) continue;
+#pragma unroll
+    for (int q = 0; q < SC_SUPER; ++q) {
+      const int tx = tx0 + q;
+      if (tx >= lo && tx <= hi) mask |= 1u << (c * SC_SUPER + q);
+    }
+  }
+  return mask;
+}
+
+__global__ void __launch_bounds__(SUPER_THREADS) k_super_count(const float4* __restrict__ rec, uint32_t stride,
+                                                               const uint32_t* __restrict__ items,
+                                                               const uint2* __restrict__ item_ranges, BinArgs a,
+                                                               uint32_t super_x, uint32_t super_per_view, int cull,
+                                                               uint16_t* __restrict__ masks,
+                                                               uint32_t* __restrict__ tile_counts) {
+  __shared__ uint32_t s_cnt[SUPER_TILES];
+  const uint32_t vst = blockIdx.x;
+  const uint32_t v = vst / super_per_view, st = vst - v * super_per_view;
+  const int tx0 = (int)(st % super_x) * SC_SUPER, ty0 = (int)(st / super_x) * SC_SUPER;
+  const int lane = threadIdx.x & 31;
+  if (threadIdx.x < SUPER_TILES) s_cnt[threadIdx.x] = 0;
+  __syncthreads();
+  const uint2 r = item_ranges[vst];
+  const float4* vrec = rec + (size_t)3 * v * stride;
+  uint32_t mine = 0;  // lane t < 16: this warp's members of tile t
+  for (uint32_t base = r.x; base < r.y; base += SUPER_THREADS) {
+    const uint32_t jj = base + threadIdx.x;
+    uint32_t mask = 0;
+    if (jj < r.y) {
+      const uint32_t id = items[jj];
+      const float4* p = vrec + (size_t)3 * id;
+      mask = super_member_mask(p[0], p[1], p[2], a, cull, tx0, ty0);
+      masks[jj] = (uint16_t)mask;
+    }
+#pragma unroll
+    for (int t = 0; t < SUPER_TILES; ++t) {
+      const uint32_t b = __ballot_sync(0xffffffffu, (mask >> t) & 1u);
+      if (lane == t) mine += __popc(b);
+    }
+  }
+  if (lane < SUPER_TILES && mine) atomicAdd(&s_cnt[lane], mine);
+  __syncthreads();
+  if (threadIdx.x < SUPER_TILES) {
+    const int tx = tx0 + (int)(threadIdx.x % SC_SUPER), ty = ty0 + (int)(threadIdx.x / SC_SUPER);
+    if (tx < (int)a.tiles_x && ty < (int)a.tiles_y)
+      tile_counts[(size_t)v * a.num_tiles + (uint32_t)ty * a.tiles_x + (uint32_t)tx] = s_cnt[threadIdx.x];
+  }
+}
+
+sc_status launch_super_count(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
+                             const uint32_t* items, const uint32_t* item_ranges, const sc_tiling* tl, int cull,
+                             uint16_t* masks, uint32_t* tile_counts) {
+  const BinArgs a = bin_args(tl);
+  const uint32_t spv = super_tiles_per_view(tl);
+  const uint64_t grid = (uint64_t)n_views * spv;
+  if (grid == 0) return SC_OK;
+  k_super_count<<<(unsigned)grid, SUPER_THREADS, 0, ctx->stream>>>(
+      rec, stride, items, reinterpret_cast<const uint2*>(item_ranges), a, (a.tiles_x + SC_SUPER - 1) / SC_SUPER, spv,
+      cull, masks, tile_counts);
+  return sc_check_launch(ctx, "k_super_count");
+}
+
+__global__ void k_ranges_from_offsets(const uint32_t* __restrict__ off, uint32_t num_tiles,
+                                      uint32_t* __restrict__ ranges) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= num_tiles) return;
+  ranges[2 * (size_t)t] = off[t];
+  ranges[2 * (size_t)t + 1] = off[t + 1];
+}
+
+sc_status launch_ranges_from_offsets(sc_ctx* ctx, const uint32_t* offsets, uint32_t num_tiles, uint32_t* ranges) {
+  if (num_tiles == 0) return SC_OK;
+  k_ranges_from_offsets<<<(num_tiles + 255) / 256, 256, 0, ctx->stream>>>(offsets, num_tiles, ranges);
+  return sc_check_launch(ctx, "k_ranges_from_offsets");
+}
+
+__global__ void __launch_bounds__(SUPER_THREADS) k_super_fill(const uint32_t* __restrict__ items,
+                                                              const uint2* __restrict__ item_ranges,
+                                                              const uint16_t* __restrict__ masks,
+                                                              const uint32_t* __restrict__ tile_off, BinArgs a,
+                                                              uint32_t super_x, uint32_t super_per_view,
+                                                              uint32_t all_tiles, uint32_t* __restrict__ pairs,
+                                                              uint64_t cap, uint32_t* __restrict__ err) {
+  constexpr int WARPS = SUPER_THREADS / 32;
+  __shared__ uint32_t s_run[SUPER_TILES];            // next free slot of each tile's list
+  __shared__ uint32_t s_wcnt[WARPS][SUPER_TILES];    // members per warp in this chunk, then their prefix
+  const uint32_t vst = blockIdx.x;
+  const uint32_t v = vst / super_per_view, st = vst - v * super_per_view;
+  const int tx0 = (int)(st % super_x) * SC_SUPER, ty0 = (int)(st / super_x) * SC_SUPER;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (vst == 0 && threadIdx.x == 0 && tile_off[all_tiles] > cap) atomicOr(err, SC_DEVERR_CAPACITY);
+  if (threadIdx.x < SUPER_TILES) {
+    const int tx = tx0 + (int)(threadIdx.x % SC_SUPER), ty = ty0 + (int)(threadIdx.x / SC_SUPER);
+    s_run[threadIdx.x] = (tx < (int)a.tiles_x && ty < (int)a.tiles_y)
+                             ? tile_off[(size_t)v * a.num_tiles + (uint32_t)ty * a.tiles_x + (uint32_t)tx]
+                             : 0u;
+  }
+  const uint2 r = item_ranges[vst];
+  const unsigned lt = (1u << lane) - 1u;
+  for (uint32_t base = r.x; base < r.y; base += SUPER_THREADS) {
+    const uint32_t jj = base + threadIdx.x;
+    uint32_t mask = 0, id = 0;
+    if (jj < r.y) {
+      mask = masks[jj];
+      id = items[jj];
+    }
+#pragma unroll
+    for (int t = 0; t < SUPER_TILES; ++t) {
+      const uint32_t b = __ballot_sync(0xffffffffu, (mask >> t) & 1u);
+      if (lane == 0) s_wcnt[warp][t] = __popc(b);
+    }
+    __syncthreads();
+    if (threadIdx.x < SUPER_TILES) {  // exclusive prefix over the warps, per tile
+      uint32_t acc = 0;
+#pragma unroll
+      for (int w = 0; w < WARPS; ++w) {
+        const uint32_t c = s_wcnt[w][threadIdx.x];
+        s_wcnt[w][threadIdx.x] = acc;
+        acc += c;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int t = 0; t < SUPER_TILES; ++t) {
+      const uint32_t b = __ballot_sync(0xffffffffu, (mask >> t) & 1u);
+      if ((mask >> t) & 1u) {
+        const uint64_t pos = (uint64_t)s_run[t] + s_wcnt[warp][t] + __popc(b & lt);
+        if (pos < cap) pairs[pos] = id;
+      }
+    }
+    __syncthreads();
+    if (warp == WARPS - 1) {  // advance past this chunk: prefix before the last warp + the last warp's members
+#pragma unroll
+      for (int t = 0; t < SUPER_TILES; ++t) {
+        const uint32_t b = __ballot_sync(0xffffffffu, (mask >> t) & 1u);
+        if (lane == t) s_run[t] += s_wcnt[WARPS - 1][t] + __popc(b);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+sc_status launch_super_fill(sc_ctx* ctx, uint32_t n_views, const uint32_t* items, const uint32_t* item_ranges,
+                            const uint16_t* masks, const uint32_t* tile_offsets, const sc_tiling* tl,
+                            uint32_t* pairs, uint64_t cap, uint32_t* d_error) {
+  const BinArgs a = bin_args(tl);
+  const uint32_t spv = super_tiles_per_view(tl);
+  const uint64_t grid = (uint64_t)n_views * spv;
+  if (grid == 0) return SC_OK;
+  k_super_fill<<<(unsigned)grid, SUPER_THREADS, 0, ctx->stream>>>(
+      items, reinterpret_cast<const uint2*>(item_ranges), masks, tile_offsets, a,
+      (a.tiles_x + SC_SUPER - 1) / SC_SUPER, spv, n_views * a.num_tiles, pairs, cap, d_error);
+  return sc_check_launch(ctx, "k_super_fill");
+}
+
 }  // namespace sck

@@ -165,7 +165,9 @@ __device__ __forceinline__ bool tile_rect(float mx, float my, float r, float vis
   return !(x1 < x0 || y1 < y0);
 }
 
-struct TileArgs { uint32_t tw, th, tiles_x, tiles_y, cull; };
+// cull: exact tile culling; super: count two-level binning items (super tiles
+// reached) instead of (tile, splat) pairs
+struct TileArgs { uint32_t tw, th, tiles_x, tiles_y, cull, super; };
 
 __global__ void __launch_bounds__(128, 4) k_project(DSplats s, const sc_camera* __restrict__ cams, uint32_t n_views,
                                                  uint32_t stride, float4* __restrict__ rec, TileArgs ta,
@@ -219,21 +221,18 @@ __global__ void __launch_bounds__(128, 4) k_project(DSplats s, const sc_camera* 
           if (depth_keys) {
             int x0, y0, x1, y1;
             if (tile_rect(mx, my, radius, 1.0f, ta.tw, ta.th, ta.tiles_x, ta.tiles_y, x0, y0, x1, y1)) {
-              if (ta.cull) {
-                const CullShape cs = cull_shape(mx, my, g.ca, g.cb, g.cc, opacity);
-                if (cs.keep) {
-                  cnt = (uint32_t)(x1 - x0 + 1) * (uint32_t)(y1 - y0 + 1);
-                } else if (cs.any) {
-                  for (int ty = y0; ty <= y1; ++ty) {
-                    int lo, hi;
-                    if (!cull_row_span(cs, ty, ta.tw, ta.th, lo, hi)) continue;
-                    lo = max(lo, x0);
-                    hi = min(hi, x1);
-                    if (hi >= lo) cnt += (uint32_t)(hi - lo + 1);
-                  }
-                }
-              } else {
+              const CullShape cs = cull_shape(mx, my, g.ca, g.cb, g.cc, opacity);
+              const bool test = ta.cull && !cs.keep;
+              if (ta.super) {
+                for_each_super_span(cs, test, x0, y0, x1, y1, ta.tw, ta.th,
+                                    [&](int, int sx0, int sx1) { cnt += (uint32_t)(sx1 - sx0 + 1); });
+              } else if (!test) {
                 cnt = (uint32_t)(x1 - x0 + 1) * (uint32_t)(y1 - y0 + 1);
+              } else {
+                for (int ty = y0; ty <= y1; ++ty) {
+                  int lo, hi;
+                  if (splat_row_span(cs, test, ty, x0, x1, ta.tw, ta.th, lo, hi)) cnt += (uint32_t)(hi - lo + 1);
+                }
               }
               if (cnt) key = __float_as_uint(g.tz);
             }
@@ -255,9 +254,9 @@ sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams,
                          float4* rec, const sc_tiling* tl, uint64_t* depth_keys, uint32_t* ids, uint32_t* counts,
                          int precise, int cull) {
   if (stride == 0 || n_views == 0) return SC_OK;
-  TileArgs ta{1, 1, 1, 1, 0};
+  TileArgs ta{1, 1, 1, 1, 0, 0};
   if (tl) ta = TileArgs{tl->tile_w, tl->tile_h, (tl->width + tl->tile_w - 1) / tl->tile_w,
-                        (tl->height + tl->tile_h - 1) / tl->tile_h, cull ? 1u : 0u};
+                        (tl->height + tl->tile_h - 1) / tl->tile_h, (cull & 1) ? 1u : 0u, (cull & 2) ? 1u : 0u};
   const uint32_t bs = 128;
   k_project<<<(unsigned)sc_div_up(stride, bs), bs, 0, ctx->stream>>>(s, d_cams, n_views, stride, rec, ta, depth_keys,
                                                                      ids, counts, precise);

@@ -292,7 +292,7 @@ __device__ __forceinline__ void st_relaxed_u32(unsigned* p, unsigned v) {
 
 // The work of one tile once its index is known.  FULL: the tile lies wholly
 // below n, so no per-key bounds test is needed.
-template <typename K, bool FULL>
+template <typename K, bool FULL, bool NARROW>
 __device__ __forceinline__ void rs_pass_tile(RsSmem<K>& sm, const K* __restrict__ kin,
                                              const uint32_t* __restrict__ vin, K* __restrict__ kout,
                                              uint32_t* __restrict__ vout, uint64_t n, int shift,
@@ -301,6 +301,7 @@ __device__ __forceinline__ void rs_pass_tile(RsSmem<K>& sm, const K* __restrict_
   constexpr int IPT = RsCfg<K>::IPT;
   constexpr int TILE = RS_THREADS * IPT;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (!NARROW) dbits = 8;
   const uint32_t dmask = (1u << dbits) - 1u;
   // warp-striped layout: item k of lane l in warp w is input slot w*32*IPT + k*32 + l
   const uint32_t wslot = (uint32_t)warp * 32 * IPT;
@@ -326,7 +327,7 @@ __device__ __forceinline__ void rs_pass_tile(RsSmem<K>& sm, const K* __restrict_
     unsigned peers = FULL ? 0xffffffffu : __ballot_sync(0xffffffffu, valid);
 #pragma unroll
     for (int b = 0; b < 8; ++b) {
-      if (b < dbits) {  // digits narrower than 8 bits (the last pass of a short key) need fewer ballots
+      if (!NARROW || b < dbits) {  // a narrower digit (last pass of a short key) needs fewer ballots
         const bool bit = (d >> b) & 1u;
         const unsigned m = __ballot_sync(0xffffffffu, bit);
         peers &= bit ? m : ~m;
@@ -430,7 +431,7 @@ __device__ __forceinline__ void rs_pass_tile(RsSmem<K>& sm, const K* __restrict_
 // many distinct digits the warp holds; lanes are ranked in input order, so the
 // pass is stable.  Look-back status words carry their own value (flag in the
 // top 2 bits, count below), so relaxed loads and stores suffice.
-template <typename K>
+template <typename K, bool NARROW>
 __global__ void __launch_bounds__(RS_THREADS, 4) k_rs_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                         K* __restrict__ kout, uint32_t* __restrict__ vout,
                                                         uint64_t n_cap, const uint64_t* __restrict__ d_n, int shift,
@@ -449,9 +450,9 @@ __global__ void __launch_bounds__(RS_THREADS, 4) k_rs_pass(const K* __restrict__
   const uint64_t tbase = (uint64_t)tile * TILE;
   if (tbase >= n) return;  // every later ticket is beyond n as well: nobody waits on this tile
   if (tbase + TILE <= n)
-    rs_pass_tile<K, true>(sm, kin, vin, kout, vout, n, shift, digit_base, lookback, err, tile, tbase, dbits);
+    rs_pass_tile<K, true, NARROW>(sm, kin, vin, kout, vout, n, shift, digit_base, lookback, err, tile, tbase, dbits);
   else
-    rs_pass_tile<K, false>(sm, kin, vin, kout, vout, n, shift, digit_base, lookback, err, tile, tbase, dbits);
+    rs_pass_tile<K, false, NARROW>(sm, kin, vin, kout, vout, n, shift, digit_base, lookback, err, tile, tbase, dbits);
 }
 
 size_t radix_scratch_bytes(uint64_t n, uint32_t key_bytes) {
@@ -488,17 +489,23 @@ sc_status radix_sort(sc_ctx* ctx, K* keys, uint32_t* vals, K* keys_tmp, uint32_t
   const size_t smem = sizeof(RsSmem<K>);
   static bool attr_set = false;
   if (!attr_set) {
-    SC_CUDA_TRY(ctx, cudaFuncSetAttribute(k_rs_pass<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                "smem attr");
+    SC_CUDA_TRY(ctx, cudaFuncSetAttribute(k_rs_pass<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem), "smem attr");
+    SC_CUDA_TRY(ctx, cudaFuncSetAttribute(k_rs_pass<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem), "smem attr");
     attr_set = true;
   }
   K* kin = keys; uint32_t* vin = vals; K* kout = keys_tmp; uint32_t* vout = vals_tmp;
   for (int p = 0; p < passes; ++p) {
     const int dbits = std::min(8, (int)key_bits - 8 * p);
-    k_rs_pass<K><<<(unsigned)tiles, RS_THREADS, smem, ctx->stream>>>(kin, vin, kout, vout, n_cap, d_n, 8 * p,
-                                                                     hist + p * RS_RADIX,
-                                                                     lookback + (size_t)p * tiles * RS_RADIX,
-                                                                     tickets + p, ctx->d_error, dbits);
+    if (dbits == 8)
+      k_rs_pass<K, false><<<(unsigned)tiles, RS_THREADS, smem, ctx->stream>>>(
+          kin, vin, kout, vout, n_cap, d_n, 8 * p, hist + p * RS_RADIX, lookback + (size_t)p * tiles * RS_RADIX,
+          tickets + p, ctx->d_error, 8);
+    else
+      k_rs_pass<K, true><<<(unsigned)tiles, RS_THREADS, smem, ctx->stream>>>(
+          kin, vin, kout, vout, n_cap, d_n, 8 * p, hist + p * RS_RADIX, lookback + (size_t)p * tiles * RS_RADIX,
+          tickets + p, ctx->d_error, dbits);
     SC_TRY(sc_check_launch(ctx, "k_rs_pass"));
     std::swap(kin, kout);
     std::swap(vin, vout);
@@ -534,10 +541,10 @@ sc_status selftest_lookback_timeout(sc_ctx* ctx) {
   SC_CUDA_TRY(ctx, cudaMemsetAsync(p, 0, need, ctx->stream), "zero");
   SC_CUDA_TRY(ctx, cudaMemsetAsync(ticket, 1, 1, ctx->stream), "ticket = 1");  // tile 0 is never handed out
   const size_t smem = sizeof(RsSmem<K>);
-  SC_CUDA_TRY(ctx, cudaFuncSetAttribute(k_rs_pass<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-              "smem attr");
-  k_rs_pass<K><<<2, RS_THREADS, smem, ctx->stream>>>(keys, vals, kout, vout, n, nullptr, 0, hist, lookback, ticket,
-                                                     ctx->d_error, 8);
+  SC_CUDA_TRY(ctx, cudaFuncSetAttribute(k_rs_pass<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem), "smem attr");
+  k_rs_pass<K, false><<<2, RS_THREADS, smem, ctx->stream>>>(keys, vals, kout, vout, n, nullptr, 0, hist, lookback,
+                                                            ticket, ctx->d_error, 8);
   SC_TRY(sc_check_launch(ctx, "k_rs_pass (timeout self-test)"));
   return sc_check_device_error(ctx);
 }

@@ -154,6 +154,44 @@ __device__ __forceinline__ bool cull_row_span(const CullShape& s, int ty, uint32
   return thi >= tlo;
 }
 
+// Tiles [lo, hi] of row ty that a splat with 3-sigma tile rectangle
+// [x0, x1] x [y0, y1] emits pairs for: the whole rectangle row, or with
+// culling (test = culling on and the conic positive definite) the clamped
+// cull_row_span.  false: the row emits nothing.  Counting, emission and the
+// two-level binning all decide membership through this one function.
+__device__ __forceinline__ bool splat_row_span(const CullShape& cs, bool test, int ty, int x0, int x1, uint32_t tw,
+                                               uint32_t th, int& lo, int& hi) {
+  lo = x0;
+  hi = x1;
+  if (test) {
+    if (!cs.any || !cull_row_span(cs, ty, tw, th, lo, hi)) return false;
+    lo = max(lo, x0);
+    hi = min(hi, x1);
+  }
+  return hi >= lo;
+}
+
+// Two-level binning: super tiles of SC_SUPER x SC_SUPER tiles.  A splat emits
+// one item per super tile that the hull of its row spans reaches, super row by
+// super row (the hull of the spans of the super row's tile rows).
+#define SC_SUPER 4
+template <typename F>
+__device__ __forceinline__ void for_each_super_span(const CullShape& cs, bool test, int x0, int y0, int x1, int y1,
+                                                    uint32_t tw, uint32_t th, F&& f) {
+  for (int sy = y0 / SC_SUPER; sy <= y1 / SC_SUPER; ++sy) {
+    int slo = INT32_MAX, shi = -1;
+    const int r0 = max(y0, sy * SC_SUPER), r1 = min(y1, sy * SC_SUPER + SC_SUPER - 1);
+    for (int ty = r0; ty <= r1; ++ty) {
+      int lo, hi;
+      if (splat_row_span(cs, test, ty, x0, x1, tw, th, lo, hi)) {
+        slo = min(slo, lo);
+        shi = max(shi, hi);
+      }
+    }
+    if (shi >= slo) f(sy, slo / SC_SUPER, shi / SC_SUPER);
+  }
+}
+
 // ---------------------------------------------------------------- host helpers
 sc_status sc_fail(sc_ctx* ctx, sc_status st, const std::string& msg);
 sc_status sc_cuda_fail(sc_ctx* ctx, cudaError_t e, const char* what);
@@ -184,7 +222,9 @@ namespace sck {
 
 // projection: writes n_views*stride records; when depth_keys != nullptr also
 // writes per (view, splat) a depth sort key (float bits, 0xFFFFFFFF when the
-// splat emits no pairs) and the tile count (for the native pipeline).
+// splat emits no pairs) and a count for the native pipeline: (tile, splat)
+// pairs, or with bit 1 of `cull` two-level binning items.  Bit 0 of `cull`:
+// exact tile culling.
 sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams, uint32_t n_views,
                          uint32_t stride, float4* rec, const sc_tiling* tiling, uint64_t* depth_keys,
                          uint32_t* splat_ids, uint32_t* counts, int precise_det, int cull);
@@ -298,6 +338,25 @@ sc_status launch_presorted_emit(sc_ctx* ctx, const float4* rec, uint32_t stride,
                                 const uint32_t* sorted_ids, const uint32_t* offsets, const uint32_t* counts_by_id,
                                 const sc_tiling* tl, uint32_t* keys, uint32_t* payloads, uint64_t cap,
                                 uint32_t* d_error, int cull);
+// two-level binning (super tiles of SC_SUPER x SC_SUPER tiles):
+// items (view << super_bits | super tile, splat) in depth order
+sc_status launch_super_emit(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
+                            const uint32_t* sorted_ids, const uint32_t* offsets, const uint32_t* counts_by_id,
+                            const sc_tiling* tl, uint32_t* keys, uint32_t* payloads, uint64_t cap, uint32_t* d_error,
+                            int cull);
+uint32_t super_tiles_per_view(const sc_tiling* tl);
+// per super tile (its items grouped by a stable sort): the member tiles of each
+// item (16-bit masks) and the pair count of every tile
+sc_status launch_super_count(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
+                             const uint32_t* items, const uint32_t* item_ranges, const sc_tiling* tl, int cull,
+                             uint16_t* masks, uint32_t* tile_counts);
+// ranges[vt] = [off[vt], off[vt+1]) from the scanned tile counts
+sc_status launch_ranges_from_offsets(sc_ctx* ctx, const uint32_t* offsets, uint32_t num_tiles, uint32_t* ranges);
+// per super tile, in item order: each item's splat id appended to the lists of
+// its member tiles at their offsets (pairs in tile, then depth order)
+sc_status launch_super_fill(sc_ctx* ctx, uint32_t n_views, const uint32_t* items, const uint32_t* item_ranges,
+                            const uint16_t* masks, const uint32_t* tile_offsets, const sc_tiling* tl,
+                            uint32_t* pairs, uint64_t cap, uint32_t* d_error);
 
 // blending
 sc_status launch_composite(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,

@@ -35,6 +35,7 @@ struct StepParams {
 struct StepOut {
   double loss;
   unsigned long long pairs;
+  unsigned long long items;  // two-level binning items
   uint32_t err;
   uint32_t pad;
 };
@@ -52,10 +53,14 @@ __global__ void k_finalize(const double* __restrict__ loss_sums, const double* _
     acc += lambda == 1.0f ? sv : (1.0 - (double)lambda) * m + (double)lambda * sv;
   }
   out->loss = weight > 0.0 ? acc * weight : acc / (double)n_views;
-  out->pairs = *d_total;
+  out->pairs = d_total[0];
+  out->items = d_total[1];
   out->err = *err;
 }
 
+// stage names of the two-level binning step (the pair-sort step uses kStageNames)
+const char* kStageNames2[] = {"project", "depth_sort", "count_scan", "item_emit", "item_sort", "tile_lists",
+                              "blend_fwd", "blend_bwd", "bwd_adam"};
 const char* kStageNames[] = {"project", "depth_sort", "count_scan", "emit", "tile_sort", "ranges",
                              "blend_fwd", "blend_bwd", "bwd_adam"};
 constexpr int kStages = 9;
@@ -83,9 +88,17 @@ struct sc_trainer {
   uint64_t* dkeys = nullptr; uint64_t* dkeys_tmp = nullptr;
   uint32_t* ids = nullptr; uint32_t* ids_tmp = nullptr;
   uint32_t* counts_by_id = nullptr; uint32_t* counts = nullptr;
-  // pairs
+  // pairs (the pair-sort path uses all four; two-level binning writes vals only)
   uint64_t kcap = 0;
   uint32_t* keys = nullptr; uint32_t* keys_tmp = nullptr; uint32_t* vals = nullptr; uint32_t* vals_tmp = nullptr;
+  // two-level binning: (super tile, splat) items, their member masks, per-tile counts -> offsets
+  bool two_level = false;
+  uint32_t ST = 0, super_bits = 0;
+  uint64_t icap = 0;
+  uint32_t* ikeys = nullptr; uint32_t* ikeys_tmp = nullptr; uint32_t* ivals = nullptr; uint32_t* ivals_tmp = nullptr;
+  uint16_t* masks = nullptr;
+  uint32_t* iranges = nullptr;      // [V * ST] (begin, end) of each super tile's items
+  uint32_t* tile_counts = nullptr;  // [V * T + 1] pair counts, scanned in place into offsets
   // per (view, tile) / pixel
   uint32_t* ranges = nullptr;
   float4* image = nullptr; uint2* aux = nullptr; float4* dl_dc = nullptr;
@@ -109,12 +122,12 @@ struct sc_trainer {
   // graph
   cudaGraphExec_t exec = nullptr;
   const void* g_key[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-  uint64_t g_key_n = 0, g_key_kcap = 0;
+  uint64_t g_key_n = 0, g_key_kcap = 0, g_key_icap = 0;
   bool g_key_grads = false;
   float g_key_w = 0.0f;
   uint32_t g_key_shards = 0, g_key_shard = 0;
   // results of the last step
-  uint64_t last_pairs = 0;
+  uint64_t last_pairs = 0, last_items = 0;
   uint32_t kernels_per_step = 0;
   // profiling
   bool profiling = false;
@@ -138,6 +151,13 @@ static void trainer_free_pairs(sc_trainer* tr) {
   tr->kcap = 0;
 }
 
+static void trainer_free_items(sc_trainer* tr) {
+  cudaFree(tr->ikeys); cudaFree(tr->ikeys_tmp); cudaFree(tr->ivals); cudaFree(tr->ivals_tmp); cudaFree(tr->masks);
+  tr->ikeys = tr->ikeys_tmp = tr->ivals = tr->ivals_tmp = nullptr;
+  tr->masks = nullptr;
+  tr->icap = 0;
+}
+
 static void trainer_drop_graph(sc_trainer* tr) {
   if (tr->exec) cudaGraphExecDestroy(tr->exec);
   tr->exec = nullptr;
@@ -147,7 +167,8 @@ static sc_status ensure_scratch(sc_trainer* tr) {
   sc_ctx* ctx = tr->ctx;
   const uint64_t nsp = (uint64_t)tr->V * tr->stride;
   size_t need = std::max({sck::radix_scratch_bytes(nsp, 8), sck::radix_scratch_bytes(std::max<uint64_t>(tr->kcap, 1), 4),
-                          sck::scan_scratch_bytes(nsp + 1)});
+                          sck::radix_scratch_bytes(std::max<uint64_t>(tr->icap, 1), 4), sck::scan_scratch_bytes(nsp + 1),
+                          sck::scan_scratch_bytes((uint64_t)tr->V * tr->T + 1)});
   if (need <= tr->scratch_bytes) return SC_OK;
   SC_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "sync");
   cudaFree(tr->scratch);
@@ -179,6 +200,29 @@ static sc_status ensure_splat_arrays(sc_trainer* tr, uint32_t cap) {
   return ensure_scratch(tr);
 }
 
+static sc_status ensure_items(sc_trainer* tr, uint64_t I) {
+  if (!tr->two_level || (I <= tr->icap && tr->icap)) return SC_OK;
+  sc_ctx* ctx = tr->ctx;
+  SC_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+  trainer_free_items(tr);
+  uint64_t cap = I + I / 4 + 65536;
+  if (cap > (1ull << 30) - 1) cap = (1ull << 30) - 1;
+  if (I > cap) return sc_fail(ctx, SC_ERR_CAPACITY, "more than 2^30 binning items in one step");
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->ikeys, cap * 4), "items");
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->ikeys_tmp, cap * 4), "items");
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->ivals, cap * 4), "items");
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->ivals_tmp, cap * 4), "items");
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->masks, cap * 2), "masks");
+  // zero-filled so a step whose emission overflowed still reads valid ids
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->ivals, 0, cap * 4, ctx->stream), "zero");
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->ivals_tmp, 0, cap * 4, ctx->stream), "zero");
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->ikeys, 0, cap * 4, ctx->stream), "zero");
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->ikeys_tmp, 0, cap * 4, ctx->stream), "zero");
+  tr->icap = cap;
+  trainer_drop_graph(tr);
+  return ensure_scratch(tr);
+}
+
 static sc_status ensure_pairs(sc_trainer* tr, uint64_t K) {
   if (K <= tr->kcap && tr->kcap) return SC_OK;
   sc_ctx* ctx = tr->ctx;
@@ -187,15 +231,17 @@ static sc_status ensure_pairs(sc_trainer* tr, uint64_t K) {
   uint64_t cap = K + K / 4 + 65536;
   if (cap > (1ull << 30) - 1) cap = (1ull << 30) - 1;
   if (K > cap) return sc_fail(ctx, SC_ERR_CAPACITY, "more than 2^30 tile/splat pairs in one step");
-  SC_CUDA_TRY(ctx, cudaMalloc(&tr->keys, cap * 4), "keys");
-  SC_CUDA_TRY(ctx, cudaMalloc(&tr->keys_tmp, cap * 4), "keys");
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->vals, cap * 4), "vals");
-  SC_CUDA_TRY(ctx, cudaMalloc(&tr->vals_tmp, cap * 4), "vals");
   // zero-filled so a step whose emission overflowed still reads valid ids
-  SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->keys, 0, cap * 4, ctx->stream), "zero");
-  SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->keys_tmp, 0, cap * 4, ctx->stream), "zero");
   SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->vals, 0, cap * 4, ctx->stream), "zero");
-  SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->vals_tmp, 0, cap * 4, ctx->stream), "zero");
+  if (!tr->two_level) {  // the pair sort's keys and ping-pong buffers
+    SC_CUDA_TRY(ctx, cudaMalloc(&tr->keys, cap * 4), "keys");
+    SC_CUDA_TRY(ctx, cudaMalloc(&tr->keys_tmp, cap * 4), "keys");
+    SC_CUDA_TRY(ctx, cudaMalloc(&tr->vals_tmp, cap * 4), "vals");
+    SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->keys, 0, cap * 4, ctx->stream), "zero");
+    SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->keys_tmp, 0, cap * 4, ctx->stream), "zero");
+    SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->vals_tmp, 0, cap * 4, ctx->stream), "zero");
+  }
   tr->kcap = cap;
   trainer_drop_graph(tr);
   return ensure_scratch(tr);
@@ -235,7 +281,7 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->counts + nsp, 0, 4, ctx->stream), "zero count tail");
   mark(tr, 0, capturing);
   SC_TRY(sck::launch_project(ctx, ds, d_cams, V, tr->stride, tr->rec, &tr->cfg.tiling, tr->dkeys, tr->ids,
-                             tr->counts_by_id, 0, (int)tr->cfg.tile_cull));
+                             tr->counts_by_id, 0, (tr->cfg.tile_cull ? 1 : 0) | (tr->two_level ? 2 : 0)));
   mark(tr, 1, capturing);
   bool in_tmp = false;
   SC_TRY(sck::radix_sort<uint64_t>(ctx, tr->dkeys, tr->ids, tr->dkeys_tmp, tr->ids_tmp, nsp, 32 + bits_for(V - 1),
@@ -243,6 +289,45 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   const uint32_t* sorted_ids = in_tmp ? tr->ids_tmp : tr->ids;
   mark(tr, 2, capturing);
   SC_TRY(sck::launch_presorted_counts(ctx, tr->counts_by_id, tr->stride, V, sorted_ids, tr->counts));
+  const uint32_t all_tiles = V * tr->T;
+  const uint32_t* svals = nullptr;
+  if (tr->two_level) {
+    // items (super tile, splat) in depth order -> grouped per super tile ->
+    // per-tile counts -> offsets (the ranges) -> each tile's depth-ordered list
+    const int cull = tr->cfg.tile_cull ? 1 : 0;
+    uint64_t* d_items = tr->d_total + 1;
+    SC_TRY(sck::scan_u32(ctx, tr->counts, nsp + 1, d_items, tr->scratch, tr->scratch_bytes));
+    if (sizing) {
+      uint64_t I = 0;
+      SC_CUDA_TRY(ctx, cudaMemcpyAsync(&I, d_items, 8, cudaMemcpyDeviceToHost, ctx->stream), "items");
+      SC_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+      SC_TRY(ensure_items(tr, I));
+    }
+    mark(tr, 3, capturing);
+    SC_TRY(sck::launch_super_emit(ctx, tr->rec, tr->stride, V, sorted_ids, tr->counts, tr->counts_by_id,
+                                  &tr->cfg.tiling, tr->ikeys, tr->ivals, tr->icap, ctx->d_error, cull));
+    mark(tr, 4, capturing);
+    SC_TRY(sck::radix_sort<uint32_t>(ctx, tr->ikeys, tr->ivals, tr->ikeys_tmp, tr->ivals_tmp, tr->icap, tr->super_bits,
+                                     d_items, tr->scratch, tr->scratch_bytes, &in_tmp));
+    const uint32_t* ik = in_tmp ? tr->ikeys_tmp : tr->ikeys;
+    const uint32_t* iv = in_tmp ? tr->ivals_tmp : tr->ivals;
+    mark(tr, 5, capturing);
+    SC_TRY(sck::launch_tile_ranges(ctx, ik, 2, d_items, tr->icap, V * tr->ST, tr->iranges, tr->ST, tr->super_bits));
+    SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->tile_counts + all_tiles, 0, 4, ctx->stream), "zero tail");
+    SC_TRY(sck::launch_super_count(ctx, tr->rec, tr->stride, V, iv, tr->iranges, &tr->cfg.tiling, cull, tr->masks,
+                                   tr->tile_counts));
+    SC_TRY(sck::scan_u32(ctx, tr->tile_counts, (uint64_t)all_tiles + 1, tr->d_total, tr->scratch, tr->scratch_bytes));
+    if (sizing) {
+      uint64_t K = 0;
+      SC_CUDA_TRY(ctx, cudaMemcpyAsync(&K, tr->d_total, 8, cudaMemcpyDeviceToHost, ctx->stream), "K");
+      SC_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+      SC_TRY(ensure_pairs(tr, K));
+    }
+    SC_TRY(sck::launch_ranges_from_offsets(ctx, tr->tile_counts, all_tiles, tr->ranges));
+    SC_TRY(sck::launch_super_fill(ctx, V, iv, tr->iranges, tr->masks, tr->tile_counts, &tr->cfg.tiling, tr->vals,
+                                  tr->kcap, ctx->d_error));
+    svals = tr->vals;
+  } else {
   SC_TRY(sck::scan_u32(ctx, tr->counts, nsp + 1, tr->d_total, tr->scratch, tr->scratch_bytes));
   if (sizing) {
     uint64_t K = 0;
@@ -257,14 +342,14 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   mark(tr, 4, capturing);
   // keys are (view << tile_bits) | tile: the stable sort on the tile bits alone
   // groups the pairs by tile, then view (the emission is view-major), then depth
-  const uint32_t all_tiles = V * tr->T;
   const uint32_t tile_bits = bits_for(tr->T);
   SC_TRY(sck::radix_sort<uint32_t>(ctx, tr->keys, tr->vals, tr->keys_tmp, tr->vals_tmp, tr->kcap, tile_bits,
                                    tr->d_total, tr->scratch, tr->scratch_bytes, &in_tmp));
   const uint32_t* skeys = in_tmp ? tr->keys_tmp : tr->keys;
-  const uint32_t* svals = in_tmp ? tr->vals_tmp : tr->vals;
+  svals = in_tmp ? tr->vals_tmp : tr->vals;
   mark(tr, 5, capturing);
   SC_TRY(sck::launch_tile_ranges(ctx, skeys, 2, tr->d_total, tr->kcap, all_tiles, tr->ranges, tr->T, tile_bits));
+  }
   mark(tr, 6, capturing);
   if (tr->h_targets) SC_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, tr->ev_copied, 0), "join");
   const float weight = tr->grads_mode ? tr->loss_weight : 1.0f / (float)V;
@@ -327,6 +412,14 @@ sc_status sc_trainer_create(sc_ctx* ctx, const sc_train_config* cfg, sc_trainer*
     delete tr;
     return sc_fail(ctx, SC_ERR_INVALID_ARG, "too many tiles x views for 32-bit pair keys");
   }
+  // sort_mode 0 (auto) and 2: two-level binning; 1: depth presort + sort of the (tile, splat) pairs
+  if (cfg->sort_mode > 2) {
+    delete tr;
+    return sc_fail(ctx, SC_ERR_INVALID_ARG, "sort_mode must be 0, 1 or 2");
+  }
+  tr->ST = sck::super_tiles_per_view(&t);
+  tr->super_bits = bits_for(tr->ST);
+  tr->two_level = cfg->sort_mode != 1 && tr->super_bits + bits_for(tr->V - 1) <= 32;
   tr->P = (uint64_t)t.width * t.height;
   const size_t pix = (size_t)tr->V * tr->P;
   cudaError_t e = cudaMallocHost(&tr->h_params, sizeof(StepParams));
@@ -339,6 +432,9 @@ sc_status sc_trainer_create(sc_ctx* ctx, const sc_train_config* cfg, sc_trainer*
   if (e == cudaSuccess) e = cudaMalloc(&tr->dl_dc, pix * 16);
   if (e == cudaSuccess) e = cudaMalloc(&tr->d_loss, 8 * (size_t)tr->V);
   if (e == cudaSuccess) e = cudaMalloc(&tr->d_total, 64);
+  if (e == cudaSuccess) e = cudaMemset(tr->d_total, 0, 64);
+  if (e == cudaSuccess && tr->two_level) e = cudaMalloc(&tr->iranges, (size_t)tr->V * tr->ST * 8);
+  if (e == cudaSuccess && tr->two_level) e = cudaMalloc(&tr->tile_counts, ((size_t)tr->V * tr->T + 1) * 4);
   if (e == cudaSuccess && cfg->ssim_lambda > 0.0f) e = cudaMalloc(&tr->ssim_terms, sck::ssim_terms_bytes(tr->P, tr->V));
   if (e == cudaSuccess && cfg->ssim_lambda > 0.0f) e = cudaMalloc(&tr->d_ssim, 8 * (size_t)tr->V);
   for (int i = 0; i <= kStages && e == cudaSuccess; ++i) e = cudaEventCreate(&tr->ev[i]);
@@ -357,6 +453,8 @@ void sc_trainer_free(sc_ctx* ctx, sc_trainer* tr) {
   trainer_drop_graph(tr);
   trainer_free_splat_arrays(tr);
   trainer_free_pairs(tr);
+  trainer_free_items(tr);
+  cudaFree(tr->iranges); cudaFree(tr->tile_counts);
   cudaFree(tr->ranges); cudaFree(tr->image); cudaFree(tr->aux); cudaFree(tr->dl_dc);
   cudaFree(tr->d_loss); cudaFree(tr->d_total); cudaFree(tr->d_params); cudaFree(tr->d_out);
   cudaFree(tr->ssim_terms); cudaFree(tr->d_ssim);
@@ -417,11 +515,11 @@ static sc_status run_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, float* a
   sc_ctx* ctx = tr->ctx;
   SC_TRY(ensure_splat_arrays(tr, s->cap));
   for (int attempt = 0; attempt < 4; ++attempt) {
-    const bool sizing = tr->kcap == 0;
+    const bool sizing = tr->kcap == 0 || (tr->two_level && tr->icap == 0);
     const void* mkey = mo ? (mo->m ? (const void*)mo->m : (const void*)mo->m16) : nullptr;
     const void* key[8] = {s->slab, s->rest16, mkey, acc, tr->targets, tr->scratch, tr->gout, tr->h_targets};
     const bool key_ok = tr->exec && std::equal(key, key + 8, tr->g_key) && tr->g_key_n == s->n &&
-                        tr->g_key_kcap == tr->kcap && tr->g_key_grads == tr->grads_mode &&
+                        tr->g_key_kcap == tr->kcap && tr->g_key_icap == tr->icap && tr->g_key_grads == tr->grads_mode &&
                         tr->g_key_w == tr->loss_weight && tr->g_key_shards == tr->g_shards &&
                         tr->g_key_shard == tr->g_shard;
     if (!key_ok) trainer_drop_graph(tr);
@@ -439,6 +537,7 @@ static sc_status run_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, float* a
         std::copy(key, key + 8, tr->g_key);
         tr->g_key_n = s->n;
         tr->g_key_kcap = tr->kcap;
+        tr->g_key_icap = tr->icap;
         tr->g_key_grads = tr->grads_mode;
         tr->g_key_w = tr->loss_weight;
         tr->g_key_shards = tr->g_shards;
@@ -452,6 +551,7 @@ static sc_status run_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, float* a
     SC_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "step sync");
     const StepOut o = *tr->h_out;
     tr->last_pairs = o.pairs;
+    tr->last_items = o.items;
     if (o.err & SC_DEVERR_TIMEOUT) {
       cudaMemsetAsync(ctx->d_error, 0, 4, ctx->stream);
       return sc_fail(ctx, SC_ERR_TIMEOUT, "a bounded device wait gave up during the step");
@@ -459,6 +559,7 @@ static sc_status run_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, float* a
     if (o.err & SC_DEVERR_CAPACITY) {
       // the blend and Adam kernels skipped this step; grow and run it again
       SC_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_error, 0, 4, ctx->stream), "clear error");
+      SC_TRY(ensure_items(tr, o.items));
       SC_TRY(ensure_pairs(tr, o.pairs));
       continue;
     }
@@ -517,12 +618,13 @@ sc_status sc_trainer_images(const sc_trainer* tr, const float** images) {
 }
 
 sc_status sc_trainer_stats(const sc_trainer* tr, uint64_t* pairs, uint32_t* n_kernels, const char** names,
-                           float* avg_ms) {
+                           float* avg_ms, uint64_t* items) {
   if (!tr) return SC_ERR_INVALID_ARG;
   if (pairs) *pairs = tr->last_pairs;
+  if (items) *items = tr->last_items;
   if (n_kernels) *n_kernels = tr->kernels_per_step;
   for (int i = 0; i < kStages; ++i) {
-    if (names) names[i] = kStageNames[i];
+    if (names) names[i] = tr->two_level ? kStageNames2[i] : kStageNames[i];
     if (avg_ms) avg_ms[i] = tr->prof_steps ? (float)(tr->acc_ms[i] / (double)tr->prof_steps) : 0.0f;
   }
   return SC_OK;

@@ -49,6 +49,7 @@ class TrainConfig:
     bf16: bool = False
     tile_cull: bool = True
     ssim_lambda: float = 0.0
+    sort_mode: int = 0  # 0 auto (two-level binning), 1 sort of the (tile, splat) pairs, 2 two-level
 
     def struct(self) -> sc_train_config:
         c = sc_train_config()
@@ -62,6 +63,7 @@ class TrainConfig:
         c.tile_cull = 1 if self.tile_cull else 0
         c.log_scale_min, c.log_scale_max, c.opacity_logit_max = LOG_SCALE_MIN, LOG_SCALE_MAX, OPACITY_LOGIT_MAX
         c.ssim_lambda = self.ssim_lambda
+        c.sort_mode = self.sort_mode
         return c
 
 
@@ -109,11 +111,12 @@ class Trainer:
         return out.reshape(self.cfg.n_views, self.cfg.height, self.cfg.width, 4)
 
     def stats(self) -> dict:
-        pairs, nk = C.c_uint64(), C.c_uint32()
+        pairs, nk, items = C.c_uint64(), C.c_uint32(), C.c_uint64()
         names = (C.c_char_p * 9)()
         ms = (C.c_float * 9)()
-        check(lib().sc_trainer_stats(self.handle, C.byref(pairs), C.byref(nk), names, ms), self.ctx.handle)
-        return {"pairs": pairs.value, "kernels_per_step": nk.value,
+        check(lib().sc_trainer_stats(self.handle, C.byref(pairs), C.byref(nk), names, ms, C.byref(items)),
+              self.ctx.handle)
+        return {"pairs": pairs.value, "items": items.value, "kernels_per_step": nk.value,
                 "stage_ms": {names[i].decode(): float(ms[i]) for i in range(9)}}
 
     def __del__(self):

@@ -188,3 +188,19 @@ def test_host_targets_copied_beside_the_step_match_device_targets(ctx):
     host = np.zeros(tgt.size, np.float32)
     with pytest.raises(Exception):
         tr2.set_host_targets(host.ctypes.data)
+
+
+@pytest.mark.parametrize("tile", [(16, 16), (8, 8), (32, 8)])
+def test_two_level_binning_equals_the_pair_sort(ctx, tile):
+    """sort_mode 0/2 (super tiles, per-tile lists filled in depth order) and
+    sort_mode 1 (stable sort of the pairs) give the same per-tile lists: the
+    images and parameters after a step are identical and the pair counts equal."""
+    scene, tl, cams, tgt, cfg = _setup(ctx, n=4000, V=3, tile=tile)
+    assert cfg.sort_mode == 0
+    tr2, g2, _, _, l2 = _run(ctx, scene, cams, tgt, cfg)        # default: two-level
+    tr1, g1, _, _, l1 = _run(ctx, scene, cams, tgt, TrainConfig(**{**cfg.__dict__, "sort_mode": 1}))
+    assert np.array_equal(tr1.images(), tr2.images())
+    assert tr1.stats()["pairs"] == tr2.stats()["pairs"]
+    assert tr2.stats()["items"] > 0 and tr1.stats()["items"] == 0
+    assert np.allclose(l1, l2, rtol=1e-6)
+    assert np.allclose(g1.readback().flat(), g2.readback().flat(), rtol=1e-5, atol=1e-7)
