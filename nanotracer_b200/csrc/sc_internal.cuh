@@ -345,17 +345,23 @@ sc_status launch_super_emit(sc_ctx* ctx, const float4* rec, uint32_t stride, uin
                             const sc_tiling* tl, uint32_t* keys, uint32_t* payloads, uint64_t cap, uint32_t* d_error,
                             int cull);
 uint32_t super_tiles_per_view(const sc_tiling* tl);
-// per super tile (its items grouped by a stable sort): the member tiles of each
-// item (16-bit masks) and the pair count of every tile
+// per super tile (its items grouped by a stable sort), cut into segments of
+// 256 items: seg_base (n_super + 1 entries) = first segment of each super
+// tile; per item the member tiles (16-bit mask); per segment and tile the
+// members before it (exclusive, item order); per tile the pair count.
+// max_segments = super_max_segments(item capacity, n_super) CTAs are launched.
+uint64_t super_max_segments(uint64_t item_cap, uint32_t n_super);
 sc_status launch_super_count(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
-                             const uint32_t* items, const uint32_t* item_ranges, const sc_tiling* tl, int cull,
-                             uint16_t* masks, uint32_t* tile_counts);
+                             const uint32_t* items, const uint32_t* item_ranges, uint32_t* seg_base,
+                             uint64_t max_segments, const sc_tiling* tl, int cull, uint16_t* masks,
+                             uint32_t* seg_counts, uint32_t* tile_counts, void* scratch, size_t scratch_bytes);
 // ranges[vt] = [off[vt], off[vt+1]) from the scanned tile counts
 sc_status launch_ranges_from_offsets(sc_ctx* ctx, const uint32_t* offsets, uint32_t num_tiles, uint32_t* ranges);
-// per super tile, in item order: each item's splat id appended to the lists of
+// per segment, in item order: each item's splat id appended to the lists of
 // its member tiles at their offsets (pairs in tile, then depth order)
 sc_status launch_super_fill(sc_ctx* ctx, uint32_t n_views, const uint32_t* items, const uint32_t* item_ranges,
-                            const uint16_t* masks, const uint32_t* tile_offsets, const sc_tiling* tl,
+                            const uint32_t* seg_base, uint64_t max_segments, const uint16_t* masks,
+                            const uint32_t* seg_counts, const uint32_t* tile_offsets, const sc_tiling* tl,
                             uint32_t* pairs, uint64_t cap, uint32_t* d_error);
 
 // blending

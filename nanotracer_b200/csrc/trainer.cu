@@ -99,6 +99,9 @@ struct sc_trainer {
   uint16_t* masks = nullptr;
   uint32_t* iranges = nullptr;      // [V * ST] (begin, end) of each super tile's items
   uint32_t* tile_counts = nullptr;  // [V * T + 1] pair counts, scanned in place into offsets
+  uint32_t* seg_base = nullptr;     // [V * ST + 1] first 256-item segment of each super tile
+  uint32_t* seg_counts = nullptr;   // [max segments * 16] members before each segment, per tile
+  uint64_t max_segments = 0;
   // per (view, tile) / pixel
   uint32_t* ranges = nullptr;
   float4* image = nullptr; uint2* aux = nullptr; float4* dl_dc = nullptr;
@@ -153,9 +156,12 @@ static void trainer_free_pairs(sc_trainer* tr) {
 
 static void trainer_free_items(sc_trainer* tr) {
   cudaFree(tr->ikeys); cudaFree(tr->ikeys_tmp); cudaFree(tr->ivals); cudaFree(tr->ivals_tmp); cudaFree(tr->masks);
+  cudaFree(tr->seg_counts);
   tr->ikeys = tr->ikeys_tmp = tr->ivals = tr->ivals_tmp = nullptr;
   tr->masks = nullptr;
+  tr->seg_counts = nullptr;
   tr->icap = 0;
+  tr->max_segments = 0;
 }
 
 static void trainer_drop_graph(sc_trainer* tr) {
@@ -213,6 +219,8 @@ static sc_status ensure_items(sc_trainer* tr, uint64_t I) {
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->ivals, cap * 4), "items");
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->ivals_tmp, cap * 4), "items");
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->masks, cap * 2), "masks");
+  tr->max_segments = sck::super_max_segments(cap, tr->V * tr->ST);
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->seg_counts, tr->max_segments * 16 * 4), "segments");
   // zero-filled so a step whose emission overflowed still reads valid ids
   SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->ivals, 0, cap * 4, ctx->stream), "zero");
   SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->ivals_tmp, 0, cap * 4, ctx->stream), "zero");
@@ -314,8 +322,9 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
     mark(tr, 5, capturing);
     SC_TRY(sck::launch_tile_ranges(ctx, ik, 2, d_items, tr->icap, V * tr->ST, tr->iranges, tr->ST, tr->super_bits));
     SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->tile_counts + all_tiles, 0, 4, ctx->stream), "zero tail");
-    SC_TRY(sck::launch_super_count(ctx, tr->rec, tr->stride, V, iv, tr->iranges, &tr->cfg.tiling, cull, tr->masks,
-                                   tr->tile_counts));
+    SC_TRY(sck::launch_super_count(ctx, tr->rec, tr->stride, V, iv, tr->iranges, tr->seg_base, tr->max_segments,
+                                   &tr->cfg.tiling, cull, tr->masks, tr->seg_counts, tr->tile_counts, tr->scratch,
+                                   tr->scratch_bytes));
     SC_TRY(sck::scan_u32(ctx, tr->tile_counts, (uint64_t)all_tiles + 1, tr->d_total, tr->scratch, tr->scratch_bytes));
     if (sizing) {
       uint64_t K = 0;
@@ -324,8 +333,8 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
       SC_TRY(ensure_pairs(tr, K));
     }
     SC_TRY(sck::launch_ranges_from_offsets(ctx, tr->tile_counts, all_tiles, tr->ranges));
-    SC_TRY(sck::launch_super_fill(ctx, V, iv, tr->iranges, tr->masks, tr->tile_counts, &tr->cfg.tiling, tr->vals,
-                                  tr->kcap, ctx->d_error));
+    SC_TRY(sck::launch_super_fill(ctx, V, iv, tr->iranges, tr->seg_base, tr->max_segments, tr->masks, tr->seg_counts,
+                                  tr->tile_counts, &tr->cfg.tiling, tr->vals, tr->kcap, ctx->d_error));
     svals = tr->vals;
   } else {
   SC_TRY(sck::scan_u32(ctx, tr->counts, nsp + 1, tr->d_total, tr->scratch, tr->scratch_bytes));
@@ -435,6 +444,7 @@ sc_status sc_trainer_create(sc_ctx* ctx, const sc_train_config* cfg, sc_trainer*
   if (e == cudaSuccess) e = cudaMemset(tr->d_total, 0, 64);
   if (e == cudaSuccess && tr->two_level) e = cudaMalloc(&tr->iranges, (size_t)tr->V * tr->ST * 8);
   if (e == cudaSuccess && tr->two_level) e = cudaMalloc(&tr->tile_counts, ((size_t)tr->V * tr->T + 1) * 4);
+  if (e == cudaSuccess && tr->two_level) e = cudaMalloc(&tr->seg_base, ((size_t)tr->V * tr->ST + 1) * 4);
   if (e == cudaSuccess && cfg->ssim_lambda > 0.0f) e = cudaMalloc(&tr->ssim_terms, sck::ssim_terms_bytes(tr->P, tr->V));
   if (e == cudaSuccess && cfg->ssim_lambda > 0.0f) e = cudaMalloc(&tr->d_ssim, 8 * (size_t)tr->V);
   for (int i = 0; i <= kStages && e == cudaSuccess; ++i) e = cudaEventCreate(&tr->ev[i]);
@@ -454,7 +464,7 @@ void sc_trainer_free(sc_ctx* ctx, sc_trainer* tr) {
   trainer_free_splat_arrays(tr);
   trainer_free_pairs(tr);
   trainer_free_items(tr);
-  cudaFree(tr->iranges); cudaFree(tr->tile_counts);
+  cudaFree(tr->iranges); cudaFree(tr->tile_counts); cudaFree(tr->seg_base);
   cudaFree(tr->ranges); cudaFree(tr->image); cudaFree(tr->aux); cudaFree(tr->dl_dc);
   cudaFree(tr->d_loss); cudaFree(tr->d_total); cudaFree(tr->d_params); cudaFree(tr->d_out);
   cudaFree(tr->ssim_terms); cudaFree(tr->d_ssim);
