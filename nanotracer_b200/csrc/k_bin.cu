@@ -123,7 +123,7 @@ sc_status launch_tile_emit(sc_ctx* ctx, const float4* rec, uint32_t n, uint32_t 
 // view * tiles_per_view + tile.  Boundaries are changes of the whole key.
 template <int MODE>
 __global__ void k_tile_ranges(const void* __restrict__ keys_v, const uint64_t* __restrict__ d_total, uint64_t cap,
-                              uint32_t num_tiles, uint32_t tiles_per_view, uint32_t tile_bits,
+                              uint32_t num_tiles, uint32_t tiles_per_view, uint32_t tile_bits, uint32_t key_mask,
                               uint32_t* __restrict__ ranges) {
   const uint64_t K = min(*d_total, cap);
   for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < K; j += (uint64_t)gridDim.x * blockDim.x) {
@@ -140,9 +140,9 @@ __global__ void k_tile_ranges(const void* __restrict__ keys_v, const uint64_t* _
       if (j + 1 < K) tn = k[j + 1] >> 32;
     } else {
       const uint32_t* k = reinterpret_cast<const uint32_t*>(keys_v);
-      t = k[j];
-      if (j > 0) tp = k[j - 1];
-      if (j + 1 < K) tn = k[j + 1];
+      t = k[j] & key_mask;
+      if (j > 0) tp = k[j - 1] & key_mask;
+      if (j + 1 < K) tn = k[j + 1] & key_mask;
     }
     uint64_t idx = t;
     if (MODE == 2) {
@@ -157,16 +157,18 @@ __global__ void k_tile_ranges(const void* __restrict__ keys_v, const uint64_t* _
 }
 
 sc_status launch_tile_ranges(sc_ctx* ctx, const void* keys, int key_mode, const uint64_t* d_total, uint64_t cap,
-                             uint32_t num_tiles, uint32_t* ranges, uint32_t tiles_per_view, uint32_t tile_bits) {
+                             uint32_t num_tiles, uint32_t* ranges, uint32_t tiles_per_view, uint32_t tile_bits,
+                             uint32_t key_bits) {
   SC_CUDA_TRY(ctx, cudaMemsetAsync(ranges, 0, (size_t)num_tiles * 8, ctx->stream), "memset ranges");
   if (cap == 0) return SC_OK;
   const unsigned g = (unsigned)std::min<uint64_t>(sc_div_up(cap, 256), (uint64_t)ctx->sm_count * 16);
   if (key_mode == 0)
-    k_tile_ranges<0><<<g, 256, 0, ctx->stream>>>(keys, d_total, cap, num_tiles, 0, 0, ranges);
+    k_tile_ranges<0><<<g, 256, 0, ctx->stream>>>(keys, d_total, cap, num_tiles, 0, 0, ~0u, ranges);
   else if (key_mode == 1)
-    k_tile_ranges<1><<<g, 256, 0, ctx->stream>>>(keys, d_total, cap, num_tiles, 0, 0, ranges);
+    k_tile_ranges<1><<<g, 256, 0, ctx->stream>>>(keys, d_total, cap, num_tiles, 0, 0, ~0u, ranges);
   else
-    k_tile_ranges<2><<<g, 256, 0, ctx->stream>>>(keys, d_total, cap, num_tiles, tiles_per_view, tile_bits, ranges);
+    k_tile_ranges<2><<<g, 256, 0, ctx->stream>>>(keys, d_total, cap, num_tiles, tiles_per_view, tile_bits,
+                                                 key_bits >= 32 ? ~0u : (1u << key_bits) - 1u, ranges);
   return sc_check_launch(ctx, "k_tile_ranges");
 }
 
@@ -323,6 +325,8 @@ static uint32_t super_bits_for(uint32_t n) {  // 2^b > n
   return b;
 }
 
+constexpr int SUPER_MASK_SHIFT = 16;  // item key: member mask << 16 | view << super_bits | super tile
+
 // Same warp-staged emission as k_presorted_emit; a lane regenerates its few
 // items for every chunk that holds some of them.
 __global__ void __launch_bounds__(EMIT_WARPS * 32) k_super_emit(
@@ -364,11 +368,13 @@ __global__ void __launch_bounds__(EMIT_WARPS * 32) k_super_emit(
     const uint64_t ce = cb + EMIT_WCHUNK < whi ? cb + EMIT_WCHUNK : whi;
     if (cnt && off < ce && off + cnt > cb) {
       uint32_t w = 0;
-      for_each_super_span(cs, test, x0, y0, x1, y1, a.tw, a.th, [&](int sy, int sx0, int sx1) {
+      for_each_super_span(cs, test, x0, y0, x1, y1, a.tw, a.th,
+                          [&](int sy, int sx0, int sx1, const int* rlo, const int* rhi) {
         for (int sx = sx0; sx <= sx1; ++sx, ++w) {
           const uint64_t g = off + w;
           if (w < cnt && g >= cb && g < ce) {
-            wk[g - cb] = vkey | ((uint32_t)sy * super_x + (uint32_t)sx);
+            wk[g - cb] = (super_mask_of(sx, rlo, rhi) << SUPER_MASK_SHIFT) | vkey |
+                         ((uint32_t)sy * super_x + (uint32_t)sx);
             wp[g - cb] = id;
           }
         }
@@ -408,29 +414,6 @@ sc_status launch_super_emit(sc_ctx* ctx, const float4* rec, uint32_t stride, uin
 constexpr int SUPER_THREADS = 256;
 constexpr int SUPER_TILES = SC_SUPER * SC_SUPER;  // 16 tiles, one bit each in a 16-bit mask
 
-// Member tiles of one item: bit (c * SC_SUPER + a) for tile (sx*4 + a, sy*4 + c).
-__device__ __forceinline__ uint32_t super_member_mask(const float4 ra, const float4 rb, const float4 rc,
-                                                      const BinArgs& a, int cull, int tx0, int ty0) {
-  int x0, y0, x1, y1;
-  if (!rect_of(ra, rb, a, x0, y0, x1, y1)) return 0u;
-  const CullShape cs = cull_shape(ra.x, ra.y, rb.x, rb.y, rb.z, rc.w);
-  const bool test = (cull & 1) && !cs.keep;
-  uint32_t mask = 0;
-#pragma unroll
-  for (int c = 0; c < SC_SUPER; ++c) {
-    const int ty = ty0 + c;
-    if (ty < y0 || ty > y1) continue;
-    int lo, hi;
-    if (!splat_row_span(cs, test, ty, x0, x1, a.tw, a.th, lo, hi)) continue;
-#pragma unroll
-    for (int q = 0; q < SC_SUPER; ++q) {
-      const int tx = tx0 + q;
-      if (tx >= lo && tx <= hi) mask |= 1u << (c * SC_SUPER + q);
-    }
-  }
-  return mask;
-}
-
 // The items of a super tile are cut into segments of SUPER_THREADS items (one
 // item per thread), so a crowded super tile is spread over many CTAs.
 // seg_base[vst] = first segment of super tile vst (exclusive scan of its
@@ -458,31 +441,22 @@ __device__ __forceinline__ int tile_of_bit(int t, int tx0, int ty0, const BinArg
                                                       : -1;
 }
 
-// One segment: member masks of its items and its member count per tile.
-__global__ void __launch_bounds__(SUPER_THREADS) k_super_count(const float4* __restrict__ rec, uint32_t stride,
-                                                               const uint32_t* __restrict__ items,
+// One segment: its member count per tile (from the masks the emission put in
+// the item keys).
+__global__ void __launch_bounds__(SUPER_THREADS) k_super_count(const uint32_t* __restrict__ item_keys,
                                                                const uint2* __restrict__ item_ranges,
-                                                               const uint32_t* __restrict__ seg_base, BinArgs a,
-                                                               uint32_t super_x, uint32_t super_per_view,
-                                                               uint32_t n_super, int cull, uint16_t* __restrict__ masks,
+                                                               const uint32_t* __restrict__ seg_base, uint32_t n_super,
                                                                uint32_t* __restrict__ seg_counts) {
   __shared__ uint32_t s_cnt[SUPER_TILES];
   const uint32_t b = blockIdx.x;
   if (b >= seg_base[n_super]) return;
   const uint32_t vst = segment_owner(seg_base, n_super, b);
-  const uint32_t v = vst / super_per_view, st = vst - v * super_per_view;
-  const int tx0 = (int)(st % super_x) * SC_SUPER, ty0 = (int)(st / super_x) * SC_SUPER;
   const int lane = threadIdx.x & 31;
   if (threadIdx.x < SUPER_TILES) s_cnt[threadIdx.x] = 0;
   __syncthreads();
   const uint2 r = item_ranges[vst];
   const uint32_t jj = r.x + (b - seg_base[vst]) * SUPER_THREADS + threadIdx.x;
-  uint32_t mask = 0;
-  if (jj < r.y) {
-    const float4* p = rec + (size_t)3 * ((size_t)v * stride + items[jj]);
-    mask = super_member_mask(p[0], p[1], p[2], a, cull, tx0, ty0);
-    masks[jj] = (uint16_t)mask;
-  }
+  const uint32_t mask = jj < r.y ? item_keys[jj] >> SUPER_MASK_SHIFT : 0u;
   uint32_t mine = 0;  // lane t < 16: this warp's members of tile t
 #pragma unroll
   for (int t = 0; t < SUPER_TILES; ++t) {
@@ -495,30 +469,45 @@ __global__ void __launch_bounds__(SUPER_THREADS) k_super_count(const float4* __r
 }
 
 // Per super tile and tile: the segments' counts become exclusive prefixes in
-// item order, and the total is the tile's pair count.
-__global__ void k_super_seg_scan(const uint32_t* __restrict__ seg_base, uint32_t n_super, BinArgs a, uint32_t super_x,
-                                 uint32_t super_per_view, uint32_t* __restrict__ seg_counts,
-                                 uint32_t* __restrict__ tile_counts) {
-  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= n_super * SUPER_TILES) return;
-  const uint32_t vst = q / SUPER_TILES;
-  const int t = (int)(q % SUPER_TILES);
-  const uint32_t v = vst / super_per_view, st = vst - v * super_per_view;
-  uint32_t acc = 0;
-  for (uint32_t b = seg_base[vst]; b < seg_base[vst + 1]; ++b) {
+// item order, and the total is the tile's pair count.  One CTA per super tile:
+// thread (l, t) takes the l-th of 16 runs of consecutive segments for tile t,
+// so the dependent loads of a crowded super tile are 16 runs long, not one.
+__global__ void __launch_bounds__(256) k_super_seg_scan(const uint32_t* __restrict__ seg_base, BinArgs a,
+                                                         uint32_t super_x, uint32_t super_per_view,
+                                                         uint32_t* __restrict__ seg_counts,
+                                                         uint32_t* __restrict__ tile_counts) {
+  __shared__ uint32_t s_sum[16][SUPER_TILES];
+  const uint32_t vst = blockIdx.x;
+  const int t = (int)(threadIdx.x % SUPER_TILES), l = (int)(threadIdx.x / SUPER_TILES);
+  const uint32_t b0 = seg_base[vst], b1 = seg_base[vst + 1];
+  const uint32_t per = (b1 - b0 + 15) / 16;
+  const uint32_t r0 = min(b0 + (uint32_t)l * per, b1), r1 = min(r0 + per, b1);
+  uint32_t sum = 0;
+  for (uint32_t b = r0; b < r1; ++b) sum += seg_counts[(size_t)b * SUPER_TILES + t];
+  s_sum[l][t] = sum;
+  __syncthreads();
+  uint32_t acc = 0, total = 0;
+  for (int q = 0; q < 16; ++q) {
+    const uint32_t x = s_sum[q][t];
+    if (q < l) acc += x;
+    total += x;
+  }
+  for (uint32_t b = r0; b < r1; ++b) {
     uint32_t* c = seg_counts + (size_t)b * SUPER_TILES + t;
     const uint32_t x = *c;
     *c = acc;
     acc += x;
   }
-  const int tile = tile_of_bit(t, (int)(st % super_x) * SC_SUPER, (int)(st / super_x) * SC_SUPER, a, v);
-  if (tile >= 0) tile_counts[tile] = acc;
+  if (l == 0) {
+    const uint32_t v = vst / super_per_view, st = vst - v * super_per_view;
+    const int tile = tile_of_bit(t, (int)(st % super_x) * SC_SUPER, (int)(st / super_x) * SC_SUPER, a, v);
+    if (tile >= 0) tile_counts[tile] = total;
+  }
 }
 
-sc_status launch_super_count(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
-                             const uint32_t* items, const uint32_t* item_ranges, uint32_t* seg_base,
-                             uint64_t max_segments, const sc_tiling* tl, int cull, uint16_t* masks,
-                             uint32_t* seg_counts, uint32_t* tile_counts, void* scratch, size_t scratch_bytes) {
+sc_status launch_super_count(sc_ctx* ctx, uint32_t n_views, const uint32_t* item_keys, const uint32_t* item_ranges,
+                             uint32_t* seg_base, uint64_t max_segments, const sc_tiling* tl, uint32_t* seg_counts,
+                             uint32_t* tile_counts, void* scratch, size_t scratch_bytes) {
   const BinArgs a = bin_args(tl);
   const uint32_t spv = super_tiles_per_view(tl);
   const uint32_t n_super = n_views * spv;
@@ -531,11 +520,9 @@ sc_status launch_super_count(sc_ctx* ctx, const float4* rec, uint32_t stride, ui
   SC_TRY(scan_u32(ctx, seg_base, (uint64_t)n_super + 1, nullptr, scratch, scratch_bytes));
   if (max_segments == 0) return SC_OK;
   k_super_count<<<(unsigned)max_segments, SUPER_THREADS, 0, ctx->stream>>>(
-      rec, stride, items, reinterpret_cast<const uint2*>(item_ranges), seg_base, a, sx, spv, n_super, cull, masks,
-      seg_counts);
+      item_keys, reinterpret_cast<const uint2*>(item_ranges), seg_base, n_super, seg_counts);
   SC_TRY(sc_check_launch(ctx, "k_super_count"));
-  const uint32_t q = n_super * SUPER_TILES;
-  k_super_seg_scan<<<(q + 255) / 256, 256, 0, ctx->stream>>>(seg_base, n_super, a, sx, spv, seg_counts, tile_counts);
+  k_super_seg_scan<<<n_super, 256, 0, ctx->stream>>>(seg_base, a, sx, spv, seg_counts, tile_counts);
   return sc_check_launch(ctx, "k_super_seg_scan");
 }
 
@@ -558,7 +545,7 @@ sc_status launch_ranges_from_offsets(sc_ctx* ctx, const uint32_t* offsets, uint3
 __global__ void __launch_bounds__(SUPER_THREADS) k_super_fill(const uint32_t* __restrict__ items,
                                                               const uint2* __restrict__ item_ranges,
                                                               const uint32_t* __restrict__ seg_base,
-                                                              const uint16_t* __restrict__ masks,
+                                                              const uint32_t* __restrict__ item_keys,
                                                               const uint32_t* __restrict__ seg_counts,
                                                               const uint32_t* __restrict__ tile_off, BinArgs a,
                                                               uint32_t super_x, uint32_t super_per_view,
@@ -583,7 +570,7 @@ __global__ void __launch_bounds__(SUPER_THREADS) k_super_fill(const uint32_t* __
   const uint32_t jj = r.x + (b - seg_base[vst]) * SUPER_THREADS + threadIdx.x;
   uint32_t mask = 0, id = 0;
   if (jj < r.y) {
-    mask = masks[jj];
+    mask = item_keys[jj] >> SUPER_MASK_SHIFT;
     id = items[jj];
   }
 #pragma unroll
@@ -614,14 +601,14 @@ __global__ void __launch_bounds__(SUPER_THREADS) k_super_fill(const uint32_t* __
 }
 
 sc_status launch_super_fill(sc_ctx* ctx, uint32_t n_views, const uint32_t* items, const uint32_t* item_ranges,
-                            const uint32_t* seg_base, uint64_t max_segments, const uint16_t* masks,
+                            const uint32_t* seg_base, uint64_t max_segments, const uint32_t* item_keys,
                             const uint32_t* seg_counts, const uint32_t* tile_offsets, const sc_tiling* tl,
                             uint32_t* pairs, uint64_t cap, uint32_t* d_error) {
   const BinArgs a = bin_args(tl);
   const uint32_t spv = super_tiles_per_view(tl);
   if (n_views * spv == 0 || max_segments == 0) return SC_OK;
   k_super_fill<<<(unsigned)max_segments, SUPER_THREADS, 0, ctx->stream>>>(
-      items, reinterpret_cast<const uint2*>(item_ranges), seg_base, masks, seg_counts, tile_offsets, a,
+      items, reinterpret_cast<const uint2*>(item_ranges), seg_base, item_keys, seg_counts, tile_offsets, a,
       (a.tiles_x + SC_SUPER - 1) / SC_SUPER, spv, n_views * spv, n_views * a.num_tiles, pairs, cap, d_error);
   return sc_check_launch(ctx, "k_super_fill");
 }

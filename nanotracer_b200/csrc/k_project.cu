@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(128, 4) k_project(DSplats s, const sc_camera* 
               const bool test = ta.cull && !cs.keep;
               if (ta.super) {
                 for_each_super_span(cs, test, x0, y0, x1, y1, ta.tw, ta.th,
-                                    [&](int, int sx0, int sx1) { cnt += (uint32_t)(sx1 - sx0 + 1); });
+                                    [&](int, int sx0, int sx1, const int*, const int*) { cnt += (uint32_t)(sx1 - sx0 + 1); });
               } else if (!test) {
                 cnt = (uint32_t)(x1 - x0 + 1) * (uint32_t)(y1 - y0 + 1);
               } else {

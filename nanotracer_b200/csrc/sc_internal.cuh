@@ -173,23 +173,45 @@ __device__ __forceinline__ bool splat_row_span(const CullShape& cs, bool test, i
 
 // Two-level binning: super tiles of SC_SUPER x SC_SUPER tiles.  A splat emits
 // one item per super tile that the hull of its row spans reaches, super row by
-// super row (the hull of the spans of the super row's tile rows).
+// super row (the hull of the spans of the super row's tile rows).  f gets the
+// super row, the hull's super columns and the spans of the super row's tile
+// rows (row c of the super row: tiles [lo[c], hi[c]], empty when lo > hi).
 #define SC_SUPER 4
 template <typename F>
 __device__ __forceinline__ void for_each_super_span(const CullShape& cs, bool test, int x0, int y0, int x1, int y1,
                                                     uint32_t tw, uint32_t th, F&& f) {
   for (int sy = y0 / SC_SUPER; sy <= y1 / SC_SUPER; ++sy) {
     int slo = INT32_MAX, shi = -1;
-    const int r0 = max(y0, sy * SC_SUPER), r1 = min(y1, sy * SC_SUPER + SC_SUPER - 1);
-    for (int ty = r0; ty <= r1; ++ty) {
+    int rlo[SC_SUPER], rhi[SC_SUPER];
+#pragma unroll
+    for (int c = 0; c < SC_SUPER; ++c) {
+      rlo[c] = 1;
+      rhi[c] = 0;
+      const int ty = sy * SC_SUPER + c;
       int lo, hi;
-      if (splat_row_span(cs, test, ty, x0, x1, tw, th, lo, hi)) {
+      if (ty >= y0 && ty <= y1 && splat_row_span(cs, test, ty, x0, x1, tw, th, lo, hi)) {
+        rlo[c] = lo;
+        rhi[c] = hi;
         slo = min(slo, lo);
         shi = max(shi, hi);
       }
     }
-    if (shi >= slo) f(sy, slo / SC_SUPER, shi / SC_SUPER);
+    if (shi >= slo) f(sy, slo / SC_SUPER, shi / SC_SUPER, rlo, rhi);
   }
+}
+
+// member tiles of super column sx given the row spans: bit c * SC_SUPER + q
+// for tile (sx * SC_SUPER + q, row c)
+__device__ __forceinline__ uint32_t super_mask_of(int sx, const int* rlo, const int* rhi) {
+  uint32_t m = 0;
+#pragma unroll
+  for (int c = 0; c < SC_SUPER; ++c)
+#pragma unroll
+    for (int q = 0; q < SC_SUPER; ++q) {
+      const int tx = sx * SC_SUPER + q;
+      if (tx >= rlo[c] && tx <= rhi[c]) m |= 1u << (c * SC_SUPER + q);
+    }
+  return m;
 }
 
 // ---------------------------------------------------------------- host helpers
@@ -327,10 +349,11 @@ sc_status launch_tile_count(sc_ctx* ctx, const float4* rec, uint32_t n, uint32_t
 sc_status launch_tile_emit(sc_ctx* ctx, const float4* rec, uint32_t n, uint32_t stride, uint32_t n_views,
                            const sc_tiling* tl, const uint32_t* offsets, int key_mode, void* keys,
                            uint32_t* payloads, uint64_t cap);
-// key_mode 2: presorted keys (view << tile_bits) | tile, tiles_per_view tiles per view
+// key_mode 2: presorted keys (view << tile_bits) | tile, tiles_per_view tiles
+// per view; only the low key_bits bits of a key take part (the rest is payload)
 sc_status launch_tile_ranges(sc_ctx* ctx, const void* keys, int key_mode, const uint64_t* d_total, uint64_t cap,
                              uint32_t num_tiles, uint32_t* ranges, uint32_t tiles_per_view = 0,
-                             uint32_t tile_bits = 0);
+                             uint32_t tile_bits = 0, uint32_t key_bits = 32);
 // depth-presorted emission for the native pipeline
 sc_status launch_presorted_counts(sc_ctx* ctx, const uint32_t* counts_by_id, uint32_t stride, uint32_t n_views,
                                   const uint32_t* sorted_ids, uint32_t* counts);
@@ -339,7 +362,9 @@ sc_status launch_presorted_emit(sc_ctx* ctx, const float4* rec, uint32_t stride,
                                 const sc_tiling* tl, uint32_t* keys, uint32_t* payloads, uint64_t cap,
                                 uint32_t* d_error, int cull);
 // two-level binning (super tiles of SC_SUPER x SC_SUPER tiles):
-// items (view << super_bits | super tile, splat) in depth order
+// items (member mask << 16 | view << super_bits | super tile, splat) in depth
+// order; bit (c * SC_SUPER + q) of the mask is tile (q, c) of the super tile.
+// view << super_bits | super tile must fit in 16 bits.
 sc_status launch_super_emit(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
                             const uint32_t* sorted_ids, const uint32_t* offsets, const uint32_t* counts_by_id,
                             const sc_tiling* tl, uint32_t* keys, uint32_t* payloads, uint64_t cap, uint32_t* d_error,
@@ -347,20 +372,19 @@ sc_status launch_super_emit(sc_ctx* ctx, const float4* rec, uint32_t stride, uin
 uint32_t super_tiles_per_view(const sc_tiling* tl);
 // per super tile (its items grouped by a stable sort), cut into segments of
 // 256 items: seg_base (n_super + 1 entries) = first segment of each super
-// tile; per item the member tiles (16-bit mask); per segment and tile the
-// members before it (exclusive, item order); per tile the pair count.
+// tile; per segment and tile the members before it (exclusive, item order);
+// per tile the pair count.  The member masks come from the sorted item keys.
 // max_segments = super_max_segments(item capacity, n_super) CTAs are launched.
 uint64_t super_max_segments(uint64_t item_cap, uint32_t n_super);
-sc_status launch_super_count(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
-                             const uint32_t* items, const uint32_t* item_ranges, uint32_t* seg_base,
-                             uint64_t max_segments, const sc_tiling* tl, int cull, uint16_t* masks,
-                             uint32_t* seg_counts, uint32_t* tile_counts, void* scratch, size_t scratch_bytes);
+sc_status launch_super_count(sc_ctx* ctx, uint32_t n_views, const uint32_t* item_keys, const uint32_t* item_ranges,
+                             uint32_t* seg_base, uint64_t max_segments, const sc_tiling* tl, uint32_t* seg_counts,
+                             uint32_t* tile_counts, void* scratch, size_t scratch_bytes);
 // ranges[vt] = [off[vt], off[vt+1]) from the scanned tile counts
 sc_status launch_ranges_from_offsets(sc_ctx* ctx, const uint32_t* offsets, uint32_t num_tiles, uint32_t* ranges);
 // per segment, in item order: each item's splat id appended to the lists of
 // its member tiles at their offsets (pairs in tile, then depth order)
 sc_status launch_super_fill(sc_ctx* ctx, uint32_t n_views, const uint32_t* items, const uint32_t* item_ranges,
-                            const uint32_t* seg_base, uint64_t max_segments, const uint16_t* masks,
+                            const uint32_t* seg_base, uint64_t max_segments, const uint32_t* item_keys,
                             const uint32_t* seg_counts, const uint32_t* tile_offsets, const sc_tiling* tl,
                             uint32_t* pairs, uint64_t cap, uint32_t* d_error);
 

@@ -91,12 +91,11 @@ struct sc_trainer {
   // pairs (the pair-sort path uses all four; two-level binning writes vals only)
   uint64_t kcap = 0;
   uint32_t* keys = nullptr; uint32_t* keys_tmp = nullptr; uint32_t* vals = nullptr; uint32_t* vals_tmp = nullptr;
-  // two-level binning: (super tile, splat) items, their member masks, per-tile counts -> offsets
+  // two-level binning: (member mask | super tile, splat) items, per-tile counts -> offsets
   bool two_level = false;
   uint32_t ST = 0, super_bits = 0;
   uint64_t icap = 0;
   uint32_t* ikeys = nullptr; uint32_t* ikeys_tmp = nullptr; uint32_t* ivals = nullptr; uint32_t* ivals_tmp = nullptr;
-  uint16_t* masks = nullptr;
   uint32_t* iranges = nullptr;      // [V * ST] (begin, end) of each super tile's items
   uint32_t* tile_counts = nullptr;  // [V * T + 1] pair counts, scanned in place into offsets
   uint32_t* seg_base = nullptr;     // [V * ST + 1] first 256-item segment of each super tile
@@ -155,10 +154,9 @@ static void trainer_free_pairs(sc_trainer* tr) {
 }
 
 static void trainer_free_items(sc_trainer* tr) {
-  cudaFree(tr->ikeys); cudaFree(tr->ikeys_tmp); cudaFree(tr->ivals); cudaFree(tr->ivals_tmp); cudaFree(tr->masks);
+  cudaFree(tr->ikeys); cudaFree(tr->ikeys_tmp); cudaFree(tr->ivals); cudaFree(tr->ivals_tmp);
   cudaFree(tr->seg_counts);
   tr->ikeys = tr->ikeys_tmp = tr->ivals = tr->ivals_tmp = nullptr;
-  tr->masks = nullptr;
   tr->seg_counts = nullptr;
   tr->icap = 0;
   tr->max_segments = 0;
@@ -218,7 +216,6 @@ static sc_status ensure_items(sc_trainer* tr, uint64_t I) {
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->ikeys_tmp, cap * 4), "items");
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->ivals, cap * 4), "items");
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->ivals_tmp, cap * 4), "items");
-  SC_CUDA_TRY(ctx, cudaMalloc(&tr->masks, cap * 2), "masks");
   tr->max_segments = sck::super_max_segments(cap, tr->V * tr->ST);
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->seg_counts, tr->max_segments * 16 * 4), "segments");
   // zero-filled so a step whose emission overflowed still reads valid ids
@@ -320,11 +317,11 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
     const uint32_t* ik = in_tmp ? tr->ikeys_tmp : tr->ikeys;
     const uint32_t* iv = in_tmp ? tr->ivals_tmp : tr->ivals;
     mark(tr, 5, capturing);
-    SC_TRY(sck::launch_tile_ranges(ctx, ik, 2, d_items, tr->icap, V * tr->ST, tr->iranges, tr->ST, tr->super_bits));
+    SC_TRY(sck::launch_tile_ranges(ctx, ik, 2, d_items, tr->icap, V * tr->ST, tr->iranges, tr->ST, tr->super_bits,
+                                   tr->super_bits + bits_for(V - 1)));
     SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->tile_counts + all_tiles, 0, 4, ctx->stream), "zero tail");
-    SC_TRY(sck::launch_super_count(ctx, tr->rec, tr->stride, V, iv, tr->iranges, tr->seg_base, tr->max_segments,
-                                   &tr->cfg.tiling, cull, tr->masks, tr->seg_counts, tr->tile_counts, tr->scratch,
-                                   tr->scratch_bytes));
+    SC_TRY(sck::launch_super_count(ctx, V, ik, tr->iranges, tr->seg_base, tr->max_segments, &tr->cfg.tiling,
+                                   tr->seg_counts, tr->tile_counts, tr->scratch, tr->scratch_bytes));
     SC_TRY(sck::scan_u32(ctx, tr->tile_counts, (uint64_t)all_tiles + 1, tr->d_total, tr->scratch, tr->scratch_bytes));
     if (sizing) {
       uint64_t K = 0;
@@ -333,7 +330,7 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
       SC_TRY(ensure_pairs(tr, K));
     }
     SC_TRY(sck::launch_ranges_from_offsets(ctx, tr->tile_counts, all_tiles, tr->ranges));
-    SC_TRY(sck::launch_super_fill(ctx, V, iv, tr->iranges, tr->seg_base, tr->max_segments, tr->masks, tr->seg_counts,
+    SC_TRY(sck::launch_super_fill(ctx, V, iv, tr->iranges, tr->seg_base, tr->max_segments, ik, tr->seg_counts,
                                   tr->tile_counts, &tr->cfg.tiling, tr->vals, tr->kcap, ctx->d_error));
     svals = tr->vals;
   } else {
@@ -428,7 +425,8 @@ sc_status sc_trainer_create(sc_ctx* ctx, const sc_train_config* cfg, sc_trainer*
   }
   tr->ST = sck::super_tiles_per_view(&t);
   tr->super_bits = bits_for(tr->ST);
-  tr->two_level = cfg->sort_mode != 1 && tr->super_bits + bits_for(tr->V - 1) <= 32;
+  // the item key holds view << super_bits | super tile in 16 bits, the member mask above
+  tr->two_level = cfg->sort_mode != 1 && tr->super_bits + bits_for(tr->V - 1) <= 16;
   tr->P = (uint64_t)t.width * t.height;
   const size_t pix = (size_t)tr->V * tr->P;
   cudaError_t e = cudaMallocHost(&tr->h_params, sizeof(StepParams));
