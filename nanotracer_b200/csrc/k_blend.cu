@@ -49,17 +49,61 @@ __device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wai
 #define ALPHA_MAX 0.99f
 #define FULL_MASK 0xffffffffu
 
+// e^(-q/2) = 2^(q * NEG_HALF_LOG2E), log2 e = 1 / ln 2
+#define NEG_HALF_LOG2E (-0.72134752044448170368f)
+
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float2 f2(float x) { return make_float2(x, x); }
+
+// The conic's quadratic form at (dx, dy) is A + B dy + c dy^2 with A = a dx^2
+// and B = 2 b dx, shared by a thread's pixels in one column; per pixel it is
+// evaluated as (c dy + B) dy + A.  Every rounding step is written out (no
+// contraction left to the compiler), so the one-pixel path and the packed
+// two-pixel path (sm_100 f32x2 instructions) produce the same bits.
+struct EntryGeom {
+  float dx, A, B;
+};
+__device__ __forceinline__ EntryGeom entry_geom(float fx, const float4 ra, const float4 rb) {
+  EntryGeom e;
+  e.dx = __fadd_rn(fx, -ra.x);
+  e.A = __fmul_rn(__fmul_rn(rb.x, e.dx), e.dx);
+  e.B = __fmul_rn(2.0f * rb.y, e.dx);
+  return e;
+}
+
 // Gaussian weight and alpha of one (pixel, splat); false when the reference
-// skips the pair (power > 0 or alpha < 1/255).  Shared by forward and backward
-// so both make identical skip decisions.
-__device__ __forceinline__ bool eval_alpha(float dx, float dy, const float4 rb, float op, float& g, float& alpha_raw,
-                                           float& alpha) {
-  const float power = -0.5f * (rb.x * dx * dx + 2.0f * rb.y * dx * dy + rb.z * dy * dy);
-  if (power > 0.0f) return false;
-  g = __expf(power);
-  alpha_raw = op * g;
+// skips the pair (power = -quad/2 > 0, or alpha < 1/255).  Shared by forward
+// and backward so both make identical skip decisions.
+__device__ __forceinline__ bool eval_alpha(const EntryGeom& e, float c, float dy, float op, float& g,
+                                           float& alpha_raw, float& alpha) {
+  const float quad = __fmaf_rn(__fmaf_rn(c, dy, e.B), dy, e.A);
+  g = ex2_approx(__fmul_rn(quad, NEG_HALF_LOG2E));
+  alpha_raw = __fmul_rn(op, g);
   alpha = fminf(alpha_raw, ALPHA_MAX);
-  return alpha >= ALPHA_MIN;
+  return quad >= 0.0f && alpha >= ALPHA_MIN;
+}
+
+// The same for a thread's two pixels (rows fy.x, fy.y of one column) with
+// packed arithmetic; v0, v1 are the per-pixel results of eval_alpha.
+__device__ __forceinline__ void eval_alpha2(const EntryGeom& e, float c, float2 fy, float ry, float op, float2& dy,
+                                            float2& g, float2& alpha_raw, float2& alpha, bool& v0, bool& v1) {
+  dy = __fadd2_rn(fy, f2(-ry));
+  const float2 quad = __ffma2_rn(__ffma2_rn(f2(c), dy, f2(e.B)), dy, f2(e.A));
+  const float2 ex = __fmul2_rn(quad, f2(NEG_HALF_LOG2E));
+  g = make_float2(ex2_approx(ex.x), ex2_approx(ex.y));
+  alpha_raw = __fmul2_rn(f2(op), g);
+  alpha = make_float2(fminf(alpha_raw.x, ALPHA_MAX), fminf(alpha_raw.y, ALPHA_MAX));
+  v0 = quad.x >= 0.0f && alpha.x >= ALPHA_MIN;
+  v1 = quad.y >= 0.0f && alpha.y >= ALPHA_MIN;
 }
 
 template <typename T>
@@ -134,25 +178,60 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
     const uint32_t cnt = min(B, end - (begin + b * B));
     if (!all_done) {
       const float4* sb = sbuf + (size_t)(b & 1) * 3 * B;
-      for (uint32_t k = 0; k < cnt; ++k) {
-        const float4 ra = sb[3 * k], rb = sb[3 * k + 1], rc = sb[3 * k + 2];
-        const float dx = fx - ra.x;
-        all_done = true;
-#pragma unroll
-        for (int q = 0; q < PPT; ++q) {
-          if (!done[q]) {
-            float g, araw, alpha;
-            if (eval_alpha(dx, fy[q] - ra.y, rb, rc.w, g, araw, alpha)) {
-              const float ta = T[q] * alpha;
-              cr[q] += ta * rc.x; cg[q] += ta * rc.y; cb[q] += ta * rc.z;
-              T[q] = T[q] * (1.0f - alpha);
-              last[q] = b * B + k + 1;
-              if (T[q] < 1e-4f) done[q] = true;
-            }
+      if constexpr (PPT == 2) {
+        // both pixels in packed arithmetic; a pixel that skips the splat gets
+        // alpha 0, which leaves its colour and T bit for bit unchanged
+        float2 T2 = make_float2(T[0], T[1]), R2 = make_float2(cr[0], cr[1]);
+        float2 G2 = make_float2(cg[0], cg[1]), B2 = make_float2(cb[0], cb[1]);
+        const float2 fy2 = make_float2(fy[0], fy[1]);
+        for (uint32_t k = 0; k < cnt; ++k) {
+          const float4 ra = sb[3 * k], rb = sb[3 * k + 1], rc = sb[3 * k + 2];
+          const EntryGeom e = entry_geom(fx, ra, rb);
+          float2 dy, g, araw, al;
+          bool v0, v1;
+          eval_alpha2(e, rb.z, fy2, ra.y, rc.w, dy, g, araw, al, v0, v1);
+          v0 &= !done[0];
+          v1 &= !done[1];
+          if (v0 || v1) {
+            const float2 am = make_float2(v0 ? al.x : 0.0f, v1 ? al.y : 0.0f);
+            const float2 ta = __fmul2_rn(T2, am);
+            R2 = __ffma2_rn(ta, f2(rc.x), R2);
+            G2 = __ffma2_rn(ta, f2(rc.y), G2);
+            B2 = __ffma2_rn(ta, f2(rc.z), B2);
+            T2 = __fmul2_rn(T2, __fadd2_rn(f2(1.0f), make_float2(-am.x, -am.y)));
+            if (v0) last[0] = b * B + k + 1;
+            if (v1) last[1] = b * B + k + 1;
+            done[0] |= T2.x < 1e-4f;
+            done[1] |= T2.y < 1e-4f;
+            if (done[0] && done[1]) break;
           }
-          all_done &= done[q];
         }
-        if (all_done) break;
+        T[0] = T2.x; T[1] = T2.y; cr[0] = R2.x; cr[1] = R2.y;
+        cg[0] = G2.x; cg[1] = G2.y; cb[0] = B2.x; cb[1] = B2.y;
+        all_done = done[0] && done[1];
+      } else {
+        for (uint32_t k = 0; k < cnt; ++k) {
+          const float4 ra = sb[3 * k], rb = sb[3 * k + 1], rc = sb[3 * k + 2];
+          const EntryGeom e = entry_geom(fx, ra, rb);
+          all_done = true;
+#pragma unroll
+          for (int q = 0; q < PPT; ++q) {
+            if (!done[q]) {
+              float g, araw, alpha;
+              if (eval_alpha(e, rb.z, __fadd_rn(fy[q], -ra.y), rc.w, g, araw, alpha)) {
+                const float ta = __fmul_rn(T[q], alpha);
+                cr[q] = __fmaf_rn(ta, rc.x, cr[q]);
+                cg[q] = __fmaf_rn(ta, rc.y, cg[q]);
+                cb[q] = __fmaf_rn(ta, rc.z, cb[q]);
+                T[q] = __fmul_rn(T[q], __fadd_rn(1.0f, -alpha));
+                last[q] = b * B + k + 1;
+                if (T[q] < 1e-4f) done[q] = true;
+              }
+            }
+            all_done &= done[q];
+          }
+          if (all_done) break;
+        }
       }
     }
     if (__syncthreads_count(all_done) == (int)B) break;
@@ -405,6 +484,9 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
     const uint32_t cnt = hi - lo;
     const float4* sb = sbuf + (size_t)(b & 1) * 3 * B;
     if (!__all_sync(FULL_MASK, all_done)) {
+      float2 T2 = make_float2(T[0], T[PPT - 1]), GS2 = make_float2(GS[0], GS[PPT - 1]);
+      const float2 gr2 = make_float2(gr[0], gr[PPT - 1]), gg2 = make_float2(gg[0], gg[PPT - 1]);
+      const float2 gb2 = make_float2(gb[0], gb[PPT - 1]), fy2 = make_float2(fy[0], fy[PPT - 1]);
       for (int k = (int)cnt - 1; k >= 0; --k) {
         const uint32_t j = lo + (uint32_t)k;
         // this thread's sums over its pixels: h = dL/dalpha * gauss (the opacity
@@ -414,37 +496,77 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
         float scr = 0.f, scg = 0.f, scb = 0.f;
         bool contrib = false;
         const float4 ra = sb[3 * k], rb = sb[3 * k + 1], rc = sb[3 * k + 2];
-        const float dx = fx - ra.x;
-        all_done = true;
-#pragma unroll
-        for (int q = 0; q < PPT; ++q) {
-          if ((MODE == SC_BWD_EXACT || !done[q]) && j < stop[q]) {
-            const float dy = fy[q] - ra.y;
-            float g, araw, alpha;
-            if (eval_alpha(dx, dy, rb, rc.w, g, araw, alpha)) {
-              const float oma = fmaxf(1.0f - alpha, 1e-4f);
-              const float inv = __fdividef(1.0f, oma);
-              const float Tn = T[q] * inv;  // T_i = T_{i+1} / (1 - alpha_i)
-              if (MODE == SC_BWD_REF && Tn > 1.0001f) {
-                done[q] = true;
-              } else {
-                const float ta = Tn * alpha;
-                scr += gr[q] * ta; scg += gg[q] * ta; scb += gb[q] * ta;
-                // dC/dalpha = T_i c - S / (1 - alpha) = (T_{i+1} c - S) / (1 - alpha)
-                const float dc = gr[q] * rc.x + gg[q] * rc.y + gb[q] * rc.z;
-                const float galpha = inv * (T[q] * dc - GS[q]);
-                const float h = araw < ALPHA_MAX ? galpha * g : 0.0f;
-                const float hx = h * dx, hy = h * dy;
-                sh += h;
-                shx += hx; shy += hy;
-                shxx += hx * dx; shxy += hx * dy; shyy += hy * dy;
-                GS[q] += ta * dc;
-                T[q] = Tn;
-                contrib = true;
-              }
+        const EntryGeom e = entry_geom(fx, ra, rb);
+        if constexpr (PPT == 2) {
+          // both pixels in packed arithmetic; a pixel that skips the splat gets
+          // zero alpha and weight, so it adds nothing and keeps its T
+          float2 dy, g, araw, al;
+          bool v0, v1;
+          eval_alpha2(e, rb.z, fy2, ra.y, rc.w, dy, g, araw, al, v0, v1);
+          v0 &= (MODE == SC_BWD_EXACT || !done[0]) && j < stop[0];
+          v1 &= (MODE == SC_BWD_EXACT || !done[1]) && j < stop[1];
+          if (v0 || v1) {
+            const float2 oma = __fadd2_rn(f2(1.0f), make_float2(-al.x, -al.y));
+            const float2 inv = make_float2(rcp_approx(oma.x), rcp_approx(oma.y));
+            const float2 Tn = __fmul2_rn(T2, inv);  // T_i = T_{i+1} / (1 - alpha_i)
+            if (MODE == SC_BWD_REF) {
+              if (v0 && Tn.x > 1.0001f) { done[0] = true; v0 = false; }
+              if (v1 && Tn.y > 1.0001f) { done[1] = true; v1 = false; }
+            }
+            if (v0 || v1) {
+              const float2 am = make_float2(v0 ? al.x : 0.0f, v1 ? al.y : 0.0f);
+              const float2 gm = make_float2(v0 && araw.x < ALPHA_MAX ? g.x : 0.0f,
+                                            v1 && araw.y < ALPHA_MAX ? g.y : 0.0f);
+              const float2 ta = __fmul2_rn(Tn, am);
+              const float2 p = __fmul2_rn(ta, gr2), q = __fmul2_rn(ta, gg2), w = __fmul2_rn(ta, gb2);
+              scr = p.x + p.y; scg = q.x + q.y; scb = w.x + w.y;
+              // dC/dalpha = T_i c - S / (1 - alpha) = (T_{i+1} c - S) / (1 - alpha)
+              const float2 dc = __ffma2_rn(gb2, f2(rc.z), __ffma2_rn(gg2, f2(rc.y), __fmul2_rn(gr2, f2(rc.x))));
+              const float2 galpha = __fmul2_rn(inv, __ffma2_rn(T2, dc, make_float2(-GS2.x, -GS2.y)));
+              const float2 h = __fmul2_rn(galpha, gm);
+              const float2 hx = __fmul2_rn(h, f2(e.dx)), hy = __fmul2_rn(h, dy);
+              sh = h.x + h.y;
+              shx = hx.x + hx.y;
+              shy = hy.x + hy.y;
+              shxx = shx * e.dx;  // both pixels share dx
+              shxy = fmaf(hx.x, dy.x, hx.y * dy.y);
+              shyy = fmaf(hy.x, dy.x, hy.y * dy.y);
+              GS2 = __ffma2_rn(ta, dc, GS2);
+              T2 = make_float2(v0 ? Tn.x : T2.x, v1 ? Tn.y : T2.y);
+              contrib = true;
             }
           }
-          if (MODE == SC_BWD_REF) all_done &= done[q] || j <= begin;
+          if (MODE == SC_BWD_REF) all_done = (done[0] || j <= begin) && (done[1] || j <= begin);
+        } else {
+          all_done = true;
+#pragma unroll
+          for (int q = 0; q < PPT; ++q) {
+            if ((MODE == SC_BWD_EXACT || !done[q]) && j < stop[q]) {
+              const float dy = __fadd_rn(fy[q], -ra.y);
+              float g, araw, alpha;
+              if (eval_alpha(e, rb.z, dy, rc.w, g, araw, alpha)) {
+                const float inv = rcp_approx(__fadd_rn(1.0f, -alpha));
+                const float Tn = __fmul_rn(T[q], inv);  // T_i = T_{i+1} / (1 - alpha_i)
+                if (MODE == SC_BWD_REF && Tn > 1.0001f) {
+                  done[q] = true;
+                } else {
+                  const float ta = __fmul_rn(Tn, alpha);
+                  scr += gr[q] * ta; scg += gg[q] * ta; scb += gb[q] * ta;
+                  const float dc = gr[q] * rc.x + gg[q] * rc.y + gb[q] * rc.z;
+                  const float galpha = inv * (T[q] * dc - GS[q]);
+                  const float h = araw < ALPHA_MAX ? galpha * g : 0.0f;
+                  const float hx = h * e.dx, hy = h * dy;
+                  sh += h;
+                  shx += hx; shy += hy;
+                  shxx += hx * e.dx; shxy += hx * dy; shyy += hy * dy;
+                  GS[q] += ta * dc;
+                  T[q] = Tn;
+                  contrib = true;
+                }
+              }
+            }
+            if (MODE == SC_BWD_REF) all_done &= done[q] || j <= begin;
+          }
         }
         if (MODE == SC_BWD_EXACT) all_done = false;
         if (__any_sync(FULL_MASK, contrib)) {
@@ -464,6 +586,9 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
           if (idx >= 0) atomicAdd(reinterpret_cast<float*>(sacc + 3 * k) + idx + idx / 3, w);
         }
         if (__all_sync(FULL_MASK, all_done)) break;
+      }
+      if constexpr (PPT == 2) {
+        T[0] = T2.x; T[1] = T2.y; GS[0] = GS2.x; GS[1] = GS2.y;
       }
     }
     __syncthreads();
