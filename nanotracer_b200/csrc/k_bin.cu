@@ -124,8 +124,9 @@ sc_status launch_tile_emit(sc_ctx* ctx, const float4* rec, uint32_t n, uint32_t 
 template <int MODE>
 __global__ void k_tile_ranges(const void* __restrict__ keys_v, const uint64_t* __restrict__ d_total, uint64_t cap,
                               uint32_t num_tiles, uint32_t tiles_per_view, uint32_t tile_bits, uint32_t key_mask,
-                              uint32_t* __restrict__ ranges) {
+                              uint32_t* __restrict__ ranges, unsigned long long* __restrict__ high_popc) {
   const uint64_t K = min(*d_total, cap);
+  uint32_t pc = 0;  // set bits above key_mask (mode 2)
   for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < K; j += (uint64_t)gridDim.x * blockDim.x) {
     uint64_t t, tp = ~0ull, tn = ~0ull;
     if (MODE == 0) {
@@ -141,6 +142,7 @@ __global__ void k_tile_ranges(const void* __restrict__ keys_v, const uint64_t* _
     } else {
       const uint32_t* k = reinterpret_cast<const uint32_t*>(keys_v);
       t = k[j] & key_mask;
+      pc += __popc(k[j] & ~key_mask);
       if (j > 0) tp = k[j - 1] & key_mask;
       if (j + 1 < K) tn = k[j + 1] & key_mask;
     }
@@ -154,21 +156,34 @@ __global__ void k_tile_ranges(const void* __restrict__ keys_v, const uint64_t* _
     if (tp != t) ranges[2 * idx] = (uint32_t)j;
     if (tn != t) ranges[2 * idx + 1] = (uint32_t)(j + 1);
   }
+  if (MODE == 2 && high_popc) {
+    __shared__ uint32_t s_pc[8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) pc += __shfl_xor_sync(0xffffffffu, pc, o);
+    if ((threadIdx.x & 31) == 0) s_pc[threadIdx.x >> 5] = pc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned long long tot = 0;
+      for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) tot += s_pc[w];
+      if (tot) atomicAdd(high_popc, tot);
+    }
+  }
 }
 
 sc_status launch_tile_ranges(sc_ctx* ctx, const void* keys, int key_mode, const uint64_t* d_total, uint64_t cap,
                              uint32_t num_tiles, uint32_t* ranges, uint32_t tiles_per_view, uint32_t tile_bits,
-                             uint32_t key_bits) {
+                             uint32_t key_bits, uint64_t* high_popc) {
   SC_CUDA_TRY(ctx, cudaMemsetAsync(ranges, 0, (size_t)num_tiles * 8, ctx->stream), "memset ranges");
   if (cap == 0) return SC_OK;
   const unsigned g = (unsigned)std::min<uint64_t>(sc_div_up(cap, 256), (uint64_t)ctx->sm_count * 16);
   if (key_mode == 0)
-    k_tile_ranges<0><<<g, 256, 0, ctx->stream>>>(keys, d_total, cap, num_tiles, 0, 0, ~0u, ranges);
+    k_tile_ranges<0><<<g, 256, 0, ctx->stream>>>(keys, d_total, cap, num_tiles, 0, 0, ~0u, ranges, nullptr);
   else if (key_mode == 1)
-    k_tile_ranges<1><<<g, 256, 0, ctx->stream>>>(keys, d_total, cap, num_tiles, 0, 0, ~0u, ranges);
+    k_tile_ranges<1><<<g, 256, 0, ctx->stream>>>(keys, d_total, cap, num_tiles, 0, 0, ~0u, ranges, nullptr);
   else
     k_tile_ranges<2><<<g, 256, 0, ctx->stream>>>(keys, d_total, cap, num_tiles, tiles_per_view, tile_bits,
-                                                 key_bits >= 32 ? ~0u : (1u << key_bits) - 1u, ranges);
+                                                 key_bits >= 32 ? ~0u : (1u << key_bits) - 1u, ranges,
+                                                 reinterpret_cast<unsigned long long*>(high_popc));
   return sc_check_launch(ctx, "k_tile_ranges");
 }
 

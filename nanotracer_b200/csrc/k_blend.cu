@@ -120,44 +120,132 @@ __device__ __forceinline__ T block_sum(T x, T* sred) {
 }
 
 // Pixel placement: thread t owns column t % tw and rows PPT*(t / tw) + k.
-struct PixelSet {
-  uint32_t px, py0;
-  float fx, fy0;
+
+// Where a CTA's depth-ordered splat list comes from.  LIST_PAIRS: the tile's
+// pair list, ids[ranges[view * tiles + tile]].  LIST_ITEMS: its super tile's
+// item list, ids[ranges[view * super tiles + super tile]], of which the CTA
+// keeps the items whose member mask (bits 16..31 of keys; bit (ty % 4) * 4 +
+// tx % 4 is tile (tx, ty)) holds its tile.  Both lists are in depth order, so
+// a tile blends the same splats in the same order either way.
+enum { LIST_PAIRS = 0, LIST_ITEMS = 1 };
+struct ListArgs {
+  const uint32_t* ids;
+  const uint2* ranges;
+  const uint32_t* keys;  // LIST_ITEMS
+  uint32_t super_x, super_per_view;
 };
 
+template <int LIST>
+__device__ __forceinline__ uint2 list_range(const ListArgs& l, const BlendArgs& a, uint32_t v, uint32_t tx,
+                                            uint32_t ty, uint32_t tile, uint32_t& bit) {
+  if (LIST == LIST_PAIRS) {
+    bit = 0;
+    return l.ranges[(size_t)v * a.num_tiles + tile];
+  }
+  bit = (ty % SC_SUPER) * SC_SUPER + tx % SC_SUPER;
+  return l.ranges[(size_t)v * l.super_per_view + (ty / SC_SUPER) * l.super_x + tx / SC_SUPER];
+}
+
+// Staging a batch of list positions [p0, p1) (at most blockDim of them) as
+// entries takes two calls, so that a batch's list words are loaded one batch
+// ahead of their use: fetch_list loads this thread's position (the id and, for
+// item lists, the key); place_list then stages the entries — each one's record
+// (3 float4) into rbuf by cp.async, its id into ids_out (when given) and, for
+// item lists, its position relative to `base` into pos.  Pair lists stage
+// every position (entry k = position p0 + k); item lists keep the items of the
+// CTA's tile in list order (a ballot per warp, then a prefix over the warps'
+// counts in wcnt).  place_list returns the entry count; every thread of the
+// CTA calls it.
+struct ListWord {
+  uint32_t key, id, j;
+  bool valid;
+};
+
+template <int LIST>
+__device__ __forceinline__ ListWord fetch_list(const ListArgs& l, uint32_t p0, uint32_t p1) {
+  ListWord f;
+  f.j = p0 + threadIdx.x;
+  f.valid = f.j < p1;
+  f.key = 0;
+  f.id = 0;
+  if (f.valid) {
+    if (LIST == LIST_ITEMS) f.key = l.keys[f.j];
+    f.id = l.ids[f.j];
+  }
+  return f;
+}
+
+template <int LIST>
+__device__ __forceinline__ uint32_t place_list(const ListWord& f, uint32_t count, const float4* vrec, uint32_t bit,
+                                               uint32_t base, float4* rbuf, uint32_t* pos, uint32_t* ids_out,
+                                               uint32_t* wcnt) {
+  const uint32_t t = threadIdx.x;
+  bool keep = f.valid;
+  uint32_t slot = t, total = count;
+  if (LIST == LIST_ITEMS) {
+    keep = keep && ((f.key >> (16u + bit)) & 1u);
+    const uint32_t bal = __ballot_sync(FULL_MASK, keep);
+    const uint32_t lane = t & 31u, warp = t >> 5;
+    if (lane == 0) wcnt[warp] = __popc(bal);
+    __syncthreads();
+    uint32_t before = 0;
+    total = 0;
+    for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) {
+      const uint32_t c = wcnt[w];
+      before += w < warp ? c : 0u;
+      total += c;
+    }
+    slot = before + __popc(bal & ((1u << lane) - 1u));
+  }
+  if (keep) {
+    const float4* src = vrec + (size_t)3 * f.id;
+    float4* dst = rbuf + 3 * slot;
+    cp_async16(dst, src);
+    cp_async16(dst + 1, src + 1);
+    cp_async16(dst + 2, src + 2);
+    if (LIST == LIST_ITEMS) pos[slot] = f.j - base;
+    if (ids_out) ids_out[slot] = f.id;
+  }
+  cp_async_commit();
+  return total;
+}
+
 // ---------------------------------------------------------------- forward
-template <int PPT>
-__global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ rec, const uint32_t* __restrict__ payloads,
-                                                   const uint2* __restrict__ ranges, BlendArgs a,
+template <int PPT, int LIST>
+__global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ rec, ListArgs l, BlendArgs a,
                                                    float4* __restrict__ image, uint2* __restrict__ aux,
                                                    const float* __restrict__ target, float gscale,
                                                    float4* __restrict__ dl_dc, double* __restrict__ loss,
                                                    const uint32_t* __restrict__ skip) {
-  extern __shared__ float4 sbuf[];  // [2][B][3]
+  extern __shared__ float4 sbuf[];  // records [2][B][3], item positions [2][B] (u32)
   __shared__ double sred[8];
-  if (skip && (*skip & SC_DEVERR_CAPACITY)) return;  // pair lists of this step are incomplete
+  __shared__ uint32_t s_wcnt[2][8];
+  if (skip && (*skip & SC_DEVERR_CAPACITY)) return;  // the lists of this step are incomplete
   const uint32_t B = blockDim.x;
+  uint32_t* spos = reinterpret_cast<uint32_t*>(sbuf + (size_t)6 * B);
   const uint32_t vt = blockIdx.x;
   const uint32_t v = vt / a.num_tiles, tile = vt - v * a.num_tiles;
   const uint32_t ty = tile / a.tiles_x, tx = tile - ty * a.tiles_x;
   const uint32_t px = tx * a.tw + threadIdx.x % a.tw;
   const uint32_t py0 = ty * a.th + PPT * (threadIdx.x / a.tw);
   const float fx = (float)px + 0.5f;
-  const uint2 r = ranges[vt];
+  uint32_t bit;
+  const uint2 r = list_range<LIST>(l, a, v, tx, ty, tile, bit);
   const uint32_t begin = r.x, end = r.y > r.x ? r.y : r.x;
   const uint32_t nb = (end - begin + B - 1) / B;
   const float4* vrec = rec + (size_t)3 * v * a.stride;
 
-  auto stage = [&](uint32_t b) {
-    const uint32_t j = begin + b * B + threadIdx.x;
-    if (j < end) {
-      const float4* src = vrec + (size_t)3 * payloads[j];
-      float4* dst = sbuf + (size_t)(b & 1) * 3 * B + 3 * threadIdx.x;
-      cp_async16(dst, src);
-      cp_async16(dst + 1, src + 1);
-      cp_async16(dst + 2, src + 2);
-    }
-    cp_async_commit();
+  auto fetch = [&](uint32_t b) -> ListWord {
+    const uint32_t p0 = begin + b * B;
+    return fetch_list<LIST>(l, p0, min(end, p0 + B));
+  };
+  auto place = [&](uint32_t b, const ListWord& f) -> uint32_t {
+    return place_list<LIST>(f, min(B, end - (begin + b * B)), vrec, bit, begin, sbuf + (size_t)(b & 1) * 3 * B,
+                            spos + (b & 1) * B, nullptr, s_wcnt[b & 1]);
+  };
+  // list position (relative to begin) of entry k of batch b
+  auto position = [&](uint32_t b, uint32_t k) -> uint32_t {
+    return LIST == LIST_PAIRS ? b * B + k : spos[(b & 1) * B + k];
   };
 
   float T[PPT], cr[PPT], cg[PPT], cb[PPT], fy[PPT];
@@ -171,11 +259,19 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
     done[k] = !(px < a.width && py0 + k < a.height);
     all_done &= done[k];
   }
-  if (nb > 0) stage(0);
+  ListWord f = fetch(0);
+  uint32_t cnt_next = nb > 0 ? place(0, f) : 0u;
+  if (nb > 1) f = fetch(1);
   for (uint32_t b = 0; b < nb; ++b) {
-    if (b + 1 < nb) { stage(b + 1); cp_async_wait_one(); } else { cp_async_wait_all(); }
+    const uint32_t cnt = cnt_next;
+    if (b + 1 < nb) {
+      cnt_next = place(b + 1, f);
+      if (b + 2 < nb) f = fetch(b + 2);
+      cp_async_wait_one();
+    } else {
+      cp_async_wait_all();
+    }
     __syncthreads();
-    const uint32_t cnt = min(B, end - (begin + b * B));
     if (!all_done) {
       const float4* sb = sbuf + (size_t)(b & 1) * 3 * B;
       if constexpr (PPT == 2) {
@@ -199,8 +295,11 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
             G2 = __ffma2_rn(ta, f2(rc.y), G2);
             B2 = __ffma2_rn(ta, f2(rc.z), B2);
             T2 = __fmul2_rn(T2, __fadd2_rn(f2(1.0f), make_float2(-am.x, -am.y)));
-            if (v0) last[0] = b * B + k + 1;
-            if (v1) last[1] = b * B + k + 1;
+            if (v0 || v1) {
+              const uint32_t pk = position(b, k) + 1;
+              if (v0) last[0] = pk;
+              if (v1) last[1] = pk;
+            }
             done[0] |= T2.x < 1e-4f;
             done[1] |= T2.y < 1e-4f;
             if (done[0] && done[1]) break;
@@ -224,7 +323,7 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
                 cg[q] = __fmaf_rn(ta, rc.y, cg[q]);
                 cb[q] = __fmaf_rn(ta, rc.z, cb[q]);
                 T[q] = __fmul_rn(T[q], __fadd_rn(1.0f, -alpha));
-                last[q] = b * B + k + 1;
+                last[q] = position(b, k) + 1;
                 if (T[q] < 1e-4f) done[q] = true;
               }
             }
@@ -258,27 +357,28 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
   }
 }
 
-template <int PPT>
+template <int PPT, int LIST>
 static sc_status composite_ppt(sc_ctx* ctx, const BlendArgs& a, uint32_t grid, uint32_t threads, const float4* rec,
-                               const uint32_t* payloads, const uint32_t* ranges, float4* image, uint2* aux,
-                               const float* target, float gscale, float4* dl_dc, double* loss, const uint32_t* d_skip) {
-  const size_t smem = (size_t)2 * 3 * threads * sizeof(float4);
-  k_composite<PPT><<<grid, threads, smem, ctx->stream>>>(rec, payloads, reinterpret_cast<const uint2*>(ranges), a,
-                                                         image, aux, target, gscale, dl_dc, loss, d_skip);
+                               const ListArgs& l, float4* image, uint2* aux, const float* target, float gscale,
+                               float4* dl_dc, double* loss, const uint32_t* d_skip) {
+  const size_t smem = (size_t)2 * 3 * threads * sizeof(float4) + (size_t)2 * threads * sizeof(uint32_t);
+  k_composite<PPT, LIST><<<grid, threads, smem, ctx->stream>>>(rec, l, a, image, aux, target, gscale, dl_dc, loss,
+                                                               d_skip);
   return sc_check_launch(ctx, "k_composite");
 }
 
 // pixels per thread: 2 when the tile splits into whole warps that way (4 per
 // thread measured slower in both kernels at 16x16 tiles: fewer warps per tile
-// to hide the entry loop's latency)
+// to hide the entry loop's latency, more registers)
 static int pick_ppt(const sc_tiling* tl) {
   const uint32_t px = tl->tile_w * tl->tile_h;
   return (tl->tile_h % 2 == 0 && (px / 2) % 32 == 0) ? 2 : 1;
 }
 
-sc_status launch_composite(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views, const uint32_t* payloads,
-                           const uint32_t* ranges, const sc_tiling* tl, float4* image, uint2* aux, const float* target,
-                           float mse_scale, float4* dl_dc, double* loss, const uint32_t* d_skip) {
+template <int LIST>
+static sc_status composite_list(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views, const ListArgs& l,
+                                const sc_tiling* tl, float4* image, uint2* aux, const float* target, float mse_scale,
+                                float4* dl_dc, double* loss, const uint32_t* d_skip) {
   const BlendArgs a = blend_args(tl, stride);
   const uint32_t pixels = tl->tile_w * tl->tile_h;
   if (pixels > 512 || pixels % 32 != 0) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile must hold 32..512 pixels, multiple of 32");
@@ -289,10 +389,29 @@ sc_status launch_composite(sc_ctx* ctx, const float4* rec, uint32_t stride, uint
   const int ppt = pick_ppt(tl);
   if (ppt == 1 && pixels > 256) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile too large for one pixel per thread");
   if (ppt == 2)
-    return composite_ppt<2>(ctx, a, (uint32_t)grid, pixels / 2, rec, payloads, ranges, image, aux, target, gscale, dl_dc,
-                            loss, d_skip);
-  return composite_ppt<1>(ctx, a, (uint32_t)grid, pixels, rec, payloads, ranges, image, aux, target, gscale, dl_dc, loss,
-                          d_skip);
+    return composite_ppt<2, LIST>(ctx, a, (uint32_t)grid, pixels / 2, rec, l, image, aux, target, gscale, dl_dc, loss,
+                                  d_skip);
+  return composite_ppt<1, LIST>(ctx, a, (uint32_t)grid, pixels, rec, l, image, aux, target, gscale, dl_dc, loss,
+                                d_skip);
+}
+
+sc_status launch_composite(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views, const uint32_t* payloads,
+                           const uint32_t* ranges, const sc_tiling* tl, float4* image, uint2* aux, const float* target,
+                           float mse_scale, float4* dl_dc, double* loss, const uint32_t* d_skip) {
+  ListArgs l{payloads, reinterpret_cast<const uint2*>(ranges), nullptr, 0, 0};
+  return composite_list<LIST_PAIRS>(ctx, rec, stride, n_views, l, tl, image, aux, target, mse_scale, dl_dc, loss,
+                                    d_skip);
+}
+
+sc_status launch_composite_items(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
+                                 const uint32_t* item_keys, const uint32_t* item_ids, const uint32_t* item_ranges,
+                                 const sc_tiling* tl, float4* image, uint2* aux, const float* target, float mse_scale,
+                                 float4* dl_dc, double* loss, const uint32_t* d_skip) {
+  const BlendArgs a = blend_args(tl, stride);
+  ListArgs l{item_ids, reinterpret_cast<const uint2*>(item_ranges), item_keys, (a.tiles_x + SC_SUPER - 1) / SC_SUPER,
+             super_tiles_per_view(tl)};
+  return composite_list<LIST_ITEMS>(ctx, rec, stride, n_views, l, tl, image, aux, target, mse_scale, dl_dc, loss,
+                                    d_skip);
 }
 
 // ---------------------------------------------------------------- MSE (standalone)
@@ -392,28 +511,30 @@ __device__ __forceinline__ float warp_reduce_scatter9(const float a[9], int lane
 // MODE is the sc_bwd_mode.  In exact mode a pixel takes part from its last
 // contributor down to the start of the tile's list and never stops early, so
 // the early-exit bookkeeping exists only in reference mode.
-template <int PPT, int MODE>
-__global__ void __launch_bounds__(256) k_composite_backward(const float4* __restrict__ rec,
-                                                            const uint32_t* __restrict__ payloads,
-                                                            const uint2* __restrict__ ranges, BlendArgs a,
+template <int PPT, int MODE, int LIST>
+__global__ void __launch_bounds__(256) k_composite_backward(const float4* __restrict__ rec, ListArgs l, BlendArgs a,
                                                             const float4* __restrict__ fwd,
                                                             const float4* __restrict__ dl_dc,
                                                             const uint2* __restrict__ aux,
                                                             float4* __restrict__ proj_grad,
                                                             const uint32_t* __restrict__ skip) {
-  extern __shared__ float4 sbuf[];  // records [2][B][3], acc [B][3] (float4), ids [2][B]
+  // records [2][B][3], acc [B][3] (float4), ids [2][B], item positions [2][B] (u32)
+  extern __shared__ float4 sbuf[];
   __shared__ uint32_t s_max;
+  __shared__ uint32_t s_wcnt[2][8];
   if (skip && (*skip & SC_DEVERR_CAPACITY)) return;
   const uint32_t B = blockDim.x;
   float4* sacc = sbuf + (size_t)6 * B;
   uint32_t* sids = reinterpret_cast<uint32_t*>(sbuf + (size_t)9 * B);
+  uint32_t* spos = sids + 2 * B;
   const uint32_t vt = blockIdx.x;
   const uint32_t v = vt / a.num_tiles, tile = vt - v * a.num_tiles;
   const uint32_t ty = tile / a.tiles_x, tx = tile - ty * a.tiles_x;
   const uint32_t px = tx * a.tw + threadIdx.x % a.tw;
   const uint32_t py0 = ty * a.th + PPT * (threadIdx.x / a.tw);
   const float fx = (float)px + 0.5f;
-  const uint2 r = ranges[vt];
+  uint32_t bit;
+  const uint2 r = list_range<LIST>(l, a, v, tx, ty, tile, bit);
   const uint32_t begin = r.x, end = r.y > r.x ? r.y : r.x;
   if (end <= begin) return;
   const float4* vrec = rec + (size_t)3 * v * a.stride;
@@ -459,36 +580,41 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
   const uint32_t hi0 = s_max;
   if (hi0 <= begin) return;
   const uint32_t nb = (hi0 - begin + B - 1) / B;
-  auto stage = [&](uint32_t b) {
+  // batch b: list positions [hi - min(B, hi - begin), hi), hi = hi0 - b B
+  auto fetch = [&](uint32_t b) -> ListWord {
     const uint32_t hi = hi0 - b * B, lo = hi - min(B, hi - begin);
-    const uint32_t j = lo + threadIdx.x;
-    if (j < hi) {
-      const uint32_t id = payloads[j];
-      sids[(b & 1) * B + threadIdx.x] = id;
-      const float4* src = vrec + (size_t)3 * id;
-      float4* dst = sbuf + (size_t)(b & 1) * 3 * B + 3 * threadIdx.x;
-      cp_async16(dst, src);
-      cp_async16(dst + 1, src + 1);
-      cp_async16(dst + 2, src + 2);
-    }
-    cp_async_commit();
+    return fetch_list<LIST>(l, lo, hi);
+  };
+  auto place = [&](uint32_t b, const ListWord& f) -> uint32_t {
+    const uint32_t hi = hi0 - b * B, lo = hi - min(B, hi - begin);
+    return place_list<LIST>(f, hi - lo, vrec, bit, begin, sbuf + (size_t)(b & 1) * 3 * B, spos + (b & 1) * B,
+                            sids + (b & 1) * B, s_wcnt[b & 1]);
   };
 
   const int lane = threadIdx.x & 31;
-  stage(0);
+  ListWord f = fetch(0);
+  uint32_t cnt_next = place(0, f);
+  if (nb > 1) f = fetch(1);
   for (uint32_t b = 0; b < nb; ++b) {
-    if (b + 1 < nb) { stage(b + 1); cp_async_wait_one(); } else { cp_async_wait_all(); }
+    const uint32_t cnt = cnt_next;
+    if (b + 1 < nb) {
+      cnt_next = place(b + 1, f);
+      if (b + 2 < nb) f = fetch(b + 2);
+      cp_async_wait_one();
+    } else {
+      cp_async_wait_all();
+    }
     __syncthreads();
     const uint32_t hi = hi0 - b * B;
     const uint32_t lo = hi - min(B, hi - begin);
-    const uint32_t cnt = hi - lo;
+    const uint32_t* bpos = spos + (b & 1) * B;
     const float4* sb = sbuf + (size_t)(b & 1) * 3 * B;
     if (!__all_sync(FULL_MASK, all_done)) {
       float2 T2 = make_float2(T[0], T[PPT - 1]), GS2 = make_float2(GS[0], GS[PPT - 1]);
       const float2 gr2 = make_float2(gr[0], gr[PPT - 1]), gg2 = make_float2(gg[0], gg[PPT - 1]);
       const float2 gb2 = make_float2(gb[0], gb[PPT - 1]), fy2 = make_float2(fy[0], fy[PPT - 1]);
       for (int k = (int)cnt - 1; k >= 0; --k) {
-        const uint32_t j = lo + (uint32_t)k;
+        const uint32_t j = LIST == LIST_PAIRS ? lo + (uint32_t)k : begin + bpos[k];
         // this thread's sums over its pixels: h = dL/dalpha * gauss (the opacity
         // gradient), its first and second moments in (dx, dy), and the colour
         // gradient; the per-splat terms are formed from them once per entry
@@ -607,24 +733,24 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
   cp_async_wait_all();
 }
 
-template <int PPT>
+template <int PPT, int LIST>
 static sc_status backward_ppt(sc_ctx* ctx, const BlendArgs& a, uint32_t grid, uint32_t threads, const float4* rec,
-                              const uint32_t* payloads, const uint32_t* ranges, const float4* fwd, const float4* dl_dc,
-                              int mode, const uint2* aux, float4* proj_grad, const uint32_t* d_skip) {
-  const size_t smem = (size_t)9 * threads * sizeof(float4) + (size_t)2 * threads * sizeof(uint32_t);
+                              const ListArgs& l, const float4* fwd, const float4* dl_dc, int mode, const uint2* aux,
+                              float4* proj_grad, const uint32_t* d_skip) {
+  const size_t smem = (size_t)9 * threads * sizeof(float4) + (size_t)4 * threads * sizeof(uint32_t);
   if (mode == SC_BWD_EXACT)
-    k_composite_backward<PPT, SC_BWD_EXACT><<<grid, threads, smem, ctx->stream>>>(
-        rec, payloads, reinterpret_cast<const uint2*>(ranges), a, fwd, dl_dc, aux, proj_grad, d_skip);
+    k_composite_backward<PPT, SC_BWD_EXACT, LIST><<<grid, threads, smem, ctx->stream>>>(rec, l, a, fwd, dl_dc, aux,
+                                                                                         proj_grad, d_skip);
   else
-    k_composite_backward<PPT, SC_BWD_REF><<<grid, threads, smem, ctx->stream>>>(
-        rec, payloads, reinterpret_cast<const uint2*>(ranges), a, fwd, dl_dc, aux, proj_grad, d_skip);
+    k_composite_backward<PPT, SC_BWD_REF, LIST><<<grid, threads, smem, ctx->stream>>>(rec, l, a, fwd, dl_dc, aux,
+                                                                                       proj_grad, d_skip);
   return sc_check_launch(ctx, "k_composite_backward");
 }
 
-sc_status launch_composite_backward(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
-                                    const uint32_t* payloads, const uint32_t* ranges, const sc_tiling* tl,
-                                    const float4* fwd, const float4* dl_dc, int mode, const uint2* aux,
-                                    float4* proj_grad, const uint32_t* d_skip) {
+template <int LIST>
+static sc_status backward_list(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views, const ListArgs& l,
+                               const sc_tiling* tl, const float4* fwd, const float4* dl_dc, int mode, const uint2* aux,
+                               float4* proj_grad, const uint32_t* d_skip) {
   const BlendArgs a = blend_args(tl, stride);
   const uint32_t pixels = tl->tile_w * tl->tile_h;
   if (pixels > 512 || pixels % 32 != 0) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile must hold 32..512 pixels, multiple of 32");
@@ -634,10 +760,27 @@ sc_status launch_composite_backward(sc_ctx* ctx, const float4* rec, uint32_t str
   const int ppt = pick_ppt(tl);
   if (ppt == 1 && pixels > 256) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile too large for one pixel per thread");
   if (ppt == 2)
-    return backward_ppt<2>(ctx, a, (uint32_t)grid, pixels / 2, rec, payloads, ranges, fwd, dl_dc, mode, aux, proj_grad,
-                           d_skip);
-  return backward_ppt<1>(ctx, a, (uint32_t)grid, pixels, rec, payloads, ranges, fwd, dl_dc, mode, aux, proj_grad,
-                         d_skip);
+    return backward_ppt<2, LIST>(ctx, a, (uint32_t)grid, pixels / 2, rec, l, fwd, dl_dc, mode, aux, proj_grad, d_skip);
+  return backward_ppt<1, LIST>(ctx, a, (uint32_t)grid, pixels, rec, l, fwd, dl_dc, mode, aux, proj_grad, d_skip);
+}
+
+sc_status launch_composite_backward(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
+                                    const uint32_t* payloads, const uint32_t* ranges, const sc_tiling* tl,
+                                    const float4* fwd, const float4* dl_dc, int mode, const uint2* aux,
+                                    float4* proj_grad, const uint32_t* d_skip) {
+  ListArgs l{payloads, reinterpret_cast<const uint2*>(ranges), nullptr, 0, 0};
+  return backward_list<LIST_PAIRS>(ctx, rec, stride, n_views, l, tl, fwd, dl_dc, mode, aux, proj_grad, d_skip);
+}
+
+sc_status launch_composite_backward_items(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
+                                          const uint32_t* item_keys, const uint32_t* item_ids,
+                                          const uint32_t* item_ranges, const sc_tiling* tl, const float4* fwd,
+                                          const float4* dl_dc, int mode, const uint2* aux, float4* proj_grad,
+                                          const uint32_t* d_skip) {
+  const BlendArgs a = blend_args(tl, stride);
+  ListArgs l{item_ids, reinterpret_cast<const uint2*>(item_ranges), item_keys, (a.tiles_x + SC_SUPER - 1) / SC_SUPER,
+             super_tiles_per_view(tl)};
+  return backward_list<LIST_ITEMS>(ctx, rec, stride, n_views, l, tl, fwd, dl_dc, mode, aux, proj_grad, d_skip);
 }
 
 // ---------------------------------------------------------------- tonemap (tonemap.wgsl:27-41)

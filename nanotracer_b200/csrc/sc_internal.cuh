@@ -350,10 +350,11 @@ sc_status launch_tile_emit(sc_ctx* ctx, const float4* rec, uint32_t n, uint32_t 
                            const sc_tiling* tl, const uint32_t* offsets, int key_mode, void* keys,
                            uint32_t* payloads, uint64_t cap);
 // key_mode 2: presorted keys (view << tile_bits) | tile, tiles_per_view tiles
-// per view; only the low key_bits bits of a key take part (the rest is payload)
+// per view; only the low key_bits bits of a key take part (the rest is payload,
+// whose set bits are added to *high_popc when it is given)
 sc_status launch_tile_ranges(sc_ctx* ctx, const void* keys, int key_mode, const uint64_t* d_total, uint64_t cap,
                              uint32_t num_tiles, uint32_t* ranges, uint32_t tiles_per_view = 0,
-                             uint32_t tile_bits = 0, uint32_t key_bits = 32);
+                             uint32_t tile_bits = 0, uint32_t key_bits = 32, uint64_t* high_popc = nullptr);
 // depth-presorted emission for the native pipeline
 sc_status launch_presorted_counts(sc_ctx* ctx, const uint32_t* counts_by_id, uint32_t stride, uint32_t n_views,
                                   const uint32_t* sorted_ids, uint32_t* counts);
@@ -399,6 +400,19 @@ sc_status launch_composite_backward(sc_ctx* ctx, const float4* rec, uint32_t str
                                     const uint32_t* payloads, const uint32_t* ranges, const sc_tiling* tl,
                                     const float4* fwd, const float4* dl_dc, int mode, const uint2* aux,
                                     float4* proj_grad, const uint32_t* d_skip);
+// the same two passes over super-tile item lists (launch_super_emit's items
+// sorted by super tile, item_ranges per (view, super tile)): each tile blends
+// the items whose member mask holds it, in list order; aux then holds
+// positions within the super tile's list
+sc_status launch_composite_items(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
+                                 const uint32_t* item_keys, const uint32_t* item_ids, const uint32_t* item_ranges,
+                                 const sc_tiling* tl, float4* image, uint2* aux, const float* target, float mse_scale,
+                                 float4* dl_dc, double* loss, const uint32_t* d_skip);
+sc_status launch_composite_backward_items(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
+                                          const uint32_t* item_keys, const uint32_t* item_ids,
+                                          const uint32_t* item_ranges, const sc_tiling* tl, const float4* fwd,
+                                          const float4* dl_dc, int mode, const uint2* aux, float4* proj_grad,
+                                          const uint32_t* d_skip);
 sc_status launch_tonemap(sc_ctx* ctx, const float4* img, uint32_t w, uint32_t h, uint8_t* out);
 
 // SSIM (loss.rs:22-375): scale * dL_ssim/dC added into dl_dc, per-view sum of

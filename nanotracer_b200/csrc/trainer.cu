@@ -59,7 +59,7 @@ __global__ void k_finalize(const double* __restrict__ loss_sums, const double* _
 }
 
 // stage names of the two-level binning step (the pair-sort step uses kStageNames)
-const char* kStageNames2[] = {"project", "depth_sort", "count_scan", "item_emit", "item_sort", "tile_lists",
+const char* kStageNames2[] = {"project", "depth_sort", "count_scan", "item_emit", "item_sort", "item_ranges",
                               "blend_fwd", "blend_bwd", "bwd_adam"};
 const char* kStageNames[] = {"project", "depth_sort", "count_scan", "emit", "tile_sort", "ranges",
                              "blend_fwd", "blend_bwd", "bwd_adam"};
@@ -96,11 +96,7 @@ struct sc_trainer {
   uint32_t ST = 0, super_bits = 0;
   uint64_t icap = 0;
   uint32_t* ikeys = nullptr; uint32_t* ikeys_tmp = nullptr; uint32_t* ivals = nullptr; uint32_t* ivals_tmp = nullptr;
-  uint32_t* iranges = nullptr;      // [V * ST] (begin, end) of each super tile's items
-  uint32_t* tile_counts = nullptr;  // [V * T + 1] pair counts, scanned in place into offsets
-  uint32_t* seg_base = nullptr;     // [V * ST + 1] first 256-item segment of each super tile
-  uint32_t* seg_counts = nullptr;   // [max segments * 16] members before each segment, per tile
-  uint64_t max_segments = 0;
+  uint32_t* iranges = nullptr;  // [V * ST] (begin, end) of each super tile's items
   // per (view, tile) / pixel
   uint32_t* ranges = nullptr;
   float4* image = nullptr; uint2* aux = nullptr; float4* dl_dc = nullptr;
@@ -155,11 +151,8 @@ static void trainer_free_pairs(sc_trainer* tr) {
 
 static void trainer_free_items(sc_trainer* tr) {
   cudaFree(tr->ikeys); cudaFree(tr->ikeys_tmp); cudaFree(tr->ivals); cudaFree(tr->ivals_tmp);
-  cudaFree(tr->seg_counts);
   tr->ikeys = tr->ikeys_tmp = tr->ivals = tr->ivals_tmp = nullptr;
-  tr->seg_counts = nullptr;
   tr->icap = 0;
-  tr->max_segments = 0;
 }
 
 static void trainer_drop_graph(sc_trainer* tr) {
@@ -216,8 +209,6 @@ static sc_status ensure_items(sc_trainer* tr, uint64_t I) {
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->ikeys_tmp, cap * 4), "items");
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->ivals, cap * 4), "items");
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->ivals_tmp, cap * 4), "items");
-  tr->max_segments = sck::super_max_segments(cap, tr->V * tr->ST);
-  SC_CUDA_TRY(ctx, cudaMalloc(&tr->seg_counts, tr->max_segments * 16 * 4), "segments");
   // zero-filled so a step whose emission overflowed still reads valid ids
   SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->ivals, 0, cap * 4, ctx->stream), "zero");
   SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->ivals_tmp, 0, cap * 4, ctx->stream), "zero");
@@ -229,7 +220,7 @@ static sc_status ensure_items(sc_trainer* tr, uint64_t I) {
 }
 
 static sc_status ensure_pairs(sc_trainer* tr, uint64_t K) {
-  if (K <= tr->kcap && tr->kcap) return SC_OK;
+  if (tr->two_level || (K <= tr->kcap && tr->kcap)) return SC_OK;  // two-level blends the item lists
   sc_ctx* ctx = tr->ctx;
   SC_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "sync");
   trainer_free_pairs(tr);
@@ -237,16 +228,14 @@ static sc_status ensure_pairs(sc_trainer* tr, uint64_t K) {
   if (cap > (1ull << 30) - 1) cap = (1ull << 30) - 1;
   if (K > cap) return sc_fail(ctx, SC_ERR_CAPACITY, "more than 2^30 tile/splat pairs in one step");
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->vals, cap * 4), "vals");
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->keys, cap * 4), "keys");
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->keys_tmp, cap * 4), "keys");
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->vals_tmp, cap * 4), "vals");
   // zero-filled so a step whose emission overflowed still reads valid ids
   SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->vals, 0, cap * 4, ctx->stream), "zero");
-  if (!tr->two_level) {  // the pair sort's keys and ping-pong buffers
-    SC_CUDA_TRY(ctx, cudaMalloc(&tr->keys, cap * 4), "keys");
-    SC_CUDA_TRY(ctx, cudaMalloc(&tr->keys_tmp, cap * 4), "keys");
-    SC_CUDA_TRY(ctx, cudaMalloc(&tr->vals_tmp, cap * 4), "vals");
-    SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->keys, 0, cap * 4, ctx->stream), "zero");
-    SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->keys_tmp, 0, cap * 4, ctx->stream), "zero");
-    SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->vals_tmp, 0, cap * 4, ctx->stream), "zero");
-  }
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->keys, 0, cap * 4, ctx->stream), "zero");
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->keys_tmp, 0, cap * 4, ctx->stream), "zero");
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->vals_tmp, 0, cap * 4, ctx->stream), "zero");
   tr->kcap = cap;
   trainer_drop_graph(tr);
   return ensure_scratch(tr);
@@ -296,9 +285,12 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   SC_TRY(sck::launch_presorted_counts(ctx, tr->counts_by_id, tr->stride, V, sorted_ids, tr->counts));
   const uint32_t all_tiles = V * tr->T;
   const uint32_t* svals = nullptr;
+  const uint32_t* item_keys = nullptr;
+  const uint32_t* item_ids = nullptr;
   if (tr->two_level) {
-    // items (super tile, splat) in depth order -> grouped per super tile ->
-    // per-tile counts -> offsets (the ranges) -> each tile's depth-ordered list
+    // items (member mask | view, super tile; splat) in depth order, grouped
+    // per super tile by a stable sort; each tile then blends the items of its
+    // super tile whose mask holds it
     const int cull = tr->cfg.tile_cull ? 1 : 0;
     uint64_t* d_items = tr->d_total + 1;
     SC_TRY(sck::scan_u32(ctx, tr->counts, nsp + 1, d_items, tr->scratch, tr->scratch_bytes));
@@ -314,25 +306,13 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
     mark(tr, 4, capturing);
     SC_TRY(sck::radix_sort<uint32_t>(ctx, tr->ikeys, tr->ivals, tr->ikeys_tmp, tr->ivals_tmp, tr->icap, tr->super_bits,
                                      d_items, tr->scratch, tr->scratch_bytes, &in_tmp));
-    const uint32_t* ik = in_tmp ? tr->ikeys_tmp : tr->ikeys;
-    const uint32_t* iv = in_tmp ? tr->ivals_tmp : tr->ivals;
+    item_keys = in_tmp ? tr->ikeys_tmp : tr->ikeys;
+    item_ids = in_tmp ? tr->ivals_tmp : tr->ivals;
     mark(tr, 5, capturing);
-    SC_TRY(sck::launch_tile_ranges(ctx, ik, 2, d_items, tr->icap, V * tr->ST, tr->iranges, tr->ST, tr->super_bits,
-                                   tr->super_bits + bits_for(V - 1)));
-    SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->tile_counts + all_tiles, 0, 4, ctx->stream), "zero tail");
-    SC_TRY(sck::launch_super_count(ctx, V, ik, tr->iranges, tr->seg_base, tr->max_segments, &tr->cfg.tiling,
-                                   tr->seg_counts, tr->tile_counts, tr->scratch, tr->scratch_bytes));
-    SC_TRY(sck::scan_u32(ctx, tr->tile_counts, (uint64_t)all_tiles + 1, tr->d_total, tr->scratch, tr->scratch_bytes));
-    if (sizing) {
-      uint64_t K = 0;
-      SC_CUDA_TRY(ctx, cudaMemcpyAsync(&K, tr->d_total, 8, cudaMemcpyDeviceToHost, ctx->stream), "K");
-      SC_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "sync");
-      SC_TRY(ensure_pairs(tr, K));
-    }
-    SC_TRY(sck::launch_ranges_from_offsets(ctx, tr->tile_counts, all_tiles, tr->ranges));
-    SC_TRY(sck::launch_super_fill(ctx, V, iv, tr->iranges, tr->seg_base, tr->max_segments, ik, tr->seg_counts,
-                                  tr->tile_counts, &tr->cfg.tiling, tr->vals, tr->kcap, ctx->d_error));
-    svals = tr->vals;
+    // the super tiles' ranges; the member bits of the masks add up to the pair count
+    SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->d_total, 0, 8, ctx->stream), "zero pairs");
+    SC_TRY(sck::launch_tile_ranges(ctx, item_keys, 2, d_items, tr->icap, V * tr->ST, tr->iranges, tr->ST,
+                                   tr->super_bits, tr->super_bits + bits_for(V - 1), tr->d_total));
   } else {
   SC_TRY(sck::scan_u32(ctx, tr->counts, nsp + 1, tr->d_total, tr->scratch, tr->scratch_bytes));
   if (sizing) {
@@ -360,17 +340,26 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   if (tr->h_targets) SC_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, tr->ev_copied, 0), "join");
   const float weight = tr->grads_mode ? tr->loss_weight : 1.0f / (float)V;
   const float lam = tr->cfg.ssim_lambda;
-  SC_TRY(sck::launch_composite(ctx, tr->rec, tr->stride, V, svals, tr->ranges, &tr->cfg.tiling, tr->image, tr->aux,
-                               tr->targets, lam > 0.0f ? weight * (1.0f - lam) : weight, tr->dl_dc, tr->d_loss,
-                               ctx->d_error));
+  const float mse_w = lam > 0.0f ? weight * (1.0f - lam) : weight;
+  if (tr->two_level)
+    SC_TRY(sck::launch_composite_items(ctx, tr->rec, tr->stride, V, item_keys, item_ids, tr->iranges, &tr->cfg.tiling,
+                                       tr->image, tr->aux, tr->targets, mse_w, tr->dl_dc, tr->d_loss, ctx->d_error));
+  else
+    SC_TRY(sck::launch_composite(ctx, tr->rec, tr->stride, V, svals, tr->ranges, &tr->cfg.tiling, tr->image, tr->aux,
+                                 tr->targets, mse_w, tr->dl_dc, tr->d_loss, ctx->d_error));
   if (lam > 0.0f) {
     SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->d_ssim, 0, 8 * (size_t)V, ctx->stream), "zero ssim");
     SC_TRY(sck::launch_ssim(ctx, tr->image, tr->targets, tr->cfg.tiling.width, tr->cfg.tiling.height, V,
                             weight * lam, tr->dl_dc, tr->d_ssim, tr->ssim_terms));
   }
   mark(tr, 7, capturing);
-  SC_TRY(sck::launch_composite_backward(ctx, tr->rec, tr->stride, V, svals, tr->ranges, &tr->cfg.tiling, tr->image,
-                                        tr->dl_dc, (int)tr->cfg.bwd_mode, tr->aux, tr->pgrad, ctx->d_error));
+  if (tr->two_level)
+    SC_TRY(sck::launch_composite_backward_items(ctx, tr->rec, tr->stride, V, item_keys, item_ids, tr->iranges,
+                                                &tr->cfg.tiling, tr->image, tr->dl_dc, (int)tr->cfg.bwd_mode, tr->aux,
+                                                tr->pgrad, ctx->d_error));
+  else
+    SC_TRY(sck::launch_composite_backward(ctx, tr->rec, tr->stride, V, svals, tr->ranges, &tr->cfg.tiling, tr->image,
+                                          tr->dl_dc, (int)tr->cfg.bwd_mode, tr->aux, tr->pgrad, ctx->d_error));
   mark(tr, 8, capturing);
   sck::AdamParams ap;
   for (int k = 0; k < 6; ++k) ap.lr[k] = tr->cfg.adam.lr[k];
@@ -441,8 +430,6 @@ sc_status sc_trainer_create(sc_ctx* ctx, const sc_train_config* cfg, sc_trainer*
   if (e == cudaSuccess) e = cudaMalloc(&tr->d_total, 64);
   if (e == cudaSuccess) e = cudaMemset(tr->d_total, 0, 64);
   if (e == cudaSuccess && tr->two_level) e = cudaMalloc(&tr->iranges, (size_t)tr->V * tr->ST * 8);
-  if (e == cudaSuccess && tr->two_level) e = cudaMalloc(&tr->tile_counts, ((size_t)tr->V * tr->T + 1) * 4);
-  if (e == cudaSuccess && tr->two_level) e = cudaMalloc(&tr->seg_base, ((size_t)tr->V * tr->ST + 1) * 4);
   if (e == cudaSuccess && cfg->ssim_lambda > 0.0f) e = cudaMalloc(&tr->ssim_terms, sck::ssim_terms_bytes(tr->P, tr->V));
   if (e == cudaSuccess && cfg->ssim_lambda > 0.0f) e = cudaMalloc(&tr->d_ssim, 8 * (size_t)tr->V);
   for (int i = 0; i <= kStages && e == cudaSuccess; ++i) e = cudaEventCreate(&tr->ev[i]);
@@ -462,7 +449,7 @@ void sc_trainer_free(sc_ctx* ctx, sc_trainer* tr) {
   trainer_free_splat_arrays(tr);
   trainer_free_pairs(tr);
   trainer_free_items(tr);
-  cudaFree(tr->iranges); cudaFree(tr->tile_counts); cudaFree(tr->seg_base);
+  cudaFree(tr->iranges);
   cudaFree(tr->ranges); cudaFree(tr->image); cudaFree(tr->aux); cudaFree(tr->dl_dc);
   cudaFree(tr->d_loss); cudaFree(tr->d_total); cudaFree(tr->d_params); cudaFree(tr->d_out);
   cudaFree(tr->ssim_terms); cudaFree(tr->d_ssim);
