@@ -119,6 +119,16 @@ __device__ __forceinline__ T block_sum(T x, T* sred) {
   return r;  // valid in thread 0
 }
 
+// MSE term of one pixel (loss.rs:163-179): returns dL/dC = gscale (C - target)
+// and adds the squared error to sq.  The forward epilogue and the backward
+// prologue both use it, so either pass can own the loss.
+__device__ __forceinline__ float3 mse_pixel(float cr, float cg, float cb, const float* __restrict__ tgt, float gscale,
+                                            double& sq) {
+  const float dx = __fadd_rn(cr, -tgt[0]), dy = __fadd_rn(cg, -tgt[1]), dz = __fadd_rn(cb, -tgt[2]);
+  sq += (double)__fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
+  return make_float3(__fmul_rn(dx, gscale), __fmul_rn(dy, gscale), __fmul_rn(dz, gscale));
+}
+
 // Pixel placement: thread t owns column t % tw and rows PPT*(t / tw) + k.
 
 // Where a CTA's depth-ordered splat list comes from.  LIST_PAIRS: the tile's
@@ -345,9 +355,8 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
       image[pix] = make_float4(cr[q], cg[q], cb[q], 1.0f - T[q]);
       if (aux) aux[pix] = make_uint2(__float_as_uint(T[q]), last[q]);
       if (target) {
-        const float dx = cr[q] - target[3 * pix], dy = cg[q] - target[3 * pix + 1], dz = cb[q] - target[3 * pix + 2];
-        dl_dc[pix] = make_float4(dx * gscale, dy * gscale, dz * gscale, 0.0f);
-        sq += (double)(dx * dx + dy * dy + dz * dz);
+        const float3 d = mse_pixel(cr[q], cg[q], cb[q], target + 3 * pix, gscale, sq);
+        dl_dc[pix] = make_float4(d.x, d.y, d.z, 0.0f);
       }
     }
   }
@@ -511,16 +520,21 @@ __device__ __forceinline__ float warp_reduce_scatter9(const float a[9], int lane
 // MODE is the sc_bwd_mode.  In exact mode a pixel takes part from its last
 // contributor down to the start of the tile's list and never stops early, so
 // the early-exit bookkeeping exists only in reference mode.
+// With a target, the MSE's dL/dC (and the loss, added to loss[view]) is formed
+// here from the forward image instead of being read from dl_dc.
 template <int PPT, int MODE, int LIST>
 __global__ void __launch_bounds__(256) k_composite_backward(const float4* __restrict__ rec, ListArgs l, BlendArgs a,
                                                             const float4* __restrict__ fwd,
                                                             const float4* __restrict__ dl_dc,
+                                                            const float* __restrict__ target, float gscale,
+                                                            double* __restrict__ loss,
                                                             const uint2* __restrict__ aux,
                                                             float4* __restrict__ proj_grad,
                                                             const uint32_t* __restrict__ skip) {
   // records [2][B][3], acc [B][3] (float4), ids [2][B], item positions [2][B] (u32)
   extern __shared__ float4 sbuf[];
   __shared__ uint32_t s_max;
+  __shared__ double s_red[8];
   __shared__ uint32_t s_wcnt[2][8];
   if (skip && (*skip & SC_DEVERR_CAPACITY)) return;
   const uint32_t B = blockDim.x;
@@ -536,7 +550,6 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
   uint32_t bit;
   const uint2 r = list_range<LIST>(l, a, v, tx, ty, tile, bit);
   const uint32_t begin = r.x, end = r.y > r.x ? r.y : r.x;
-  if (end <= begin) return;
   const float4* vrec = rec + (size_t)3 * v * a.stride;
   float4* vgrad = proj_grad + (size_t)3 * v * a.stride;
 
@@ -547,6 +560,7 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
   bool done[PPT];
   uint32_t tstop = begin;
   bool all_done = true;
+  double sq = 0.0;
 #pragma unroll
   for (int q = 0; q < PPT; ++q) {
     const uint32_t py = py0 + q;
@@ -556,10 +570,17 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
     done[q] = !(px < a.width && py < a.height);
     if (!done[q]) {
       const size_t pix = (size_t)v * a.pixels + (size_t)py * a.width + px;
-      const float4 d = dl_dc[pix];
-      gr[q] = d.x; gg[q] = d.y; gb[q] = d.z;
+      float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (target || MODE == SC_BWD_REF) c = fwd[pix];
+      if (target) {
+        const float3 d = mse_pixel(c.x, c.y, c.z, target + 3 * pix, gscale, sq);
+        gr[q] = d.x; gg[q] = d.y; gb[q] = d.z;
+      } else {
+        const float4 d = dl_dc[pix];
+        gr[q] = d.x; gg[q] = d.y; gb[q] = d.z;
+      }
       if (MODE == SC_BWD_REF) {
-        T[q] = 1.0f - fwd[pix].w;
+        T[q] = 1.0f - c.w;
         stop[q] = end;
       } else {
         const uint2 x = aux[pix];
@@ -570,6 +591,11 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
     }
     all_done &= done[q];
   }
+  if (target && loss) {  // every CTA, the ones with an empty list too
+    const double sum = block_sum(sq, s_red);
+    if (threadIdx.x == 0 && sum != 0.0) atomicAdd(&loss[v], sum);
+  }
+  if (end <= begin) return;
   if (threadIdx.x == 0) s_max = begin;
   sacc[3 * threadIdx.x] = make_float4(0, 0, 0, 0);
   sacc[3 * threadIdx.x + 1] = make_float4(0, 0, 0, 0);
@@ -735,23 +761,26 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
 
 template <int PPT, int LIST>
 static sc_status backward_ppt(sc_ctx* ctx, const BlendArgs& a, uint32_t grid, uint32_t threads, const float4* rec,
-                              const ListArgs& l, const float4* fwd, const float4* dl_dc, int mode, const uint2* aux,
-                              float4* proj_grad, const uint32_t* d_skip) {
+                              const ListArgs& l, const float4* fwd, const float4* dl_dc, const float* target,
+                              float gscale, double* loss, int mode, const uint2* aux, float4* proj_grad,
+                              const uint32_t* d_skip) {
   const size_t smem = (size_t)9 * threads * sizeof(float4) + (size_t)4 * threads * sizeof(uint32_t);
   if (mode == SC_BWD_EXACT)
-    k_composite_backward<PPT, SC_BWD_EXACT, LIST><<<grid, threads, smem, ctx->stream>>>(rec, l, a, fwd, dl_dc, aux,
-                                                                                         proj_grad, d_skip);
+    k_composite_backward<PPT, SC_BWD_EXACT, LIST><<<grid, threads, smem, ctx->stream>>>(
+        rec, l, a, fwd, dl_dc, target, gscale, loss, aux, proj_grad, d_skip);
   else
-    k_composite_backward<PPT, SC_BWD_REF, LIST><<<grid, threads, smem, ctx->stream>>>(rec, l, a, fwd, dl_dc, aux,
-                                                                                       proj_grad, d_skip);
+    k_composite_backward<PPT, SC_BWD_REF, LIST><<<grid, threads, smem, ctx->stream>>>(
+        rec, l, a, fwd, dl_dc, target, gscale, loss, aux, proj_grad, d_skip);
   return sc_check_launch(ctx, "k_composite_backward");
 }
 
 template <int LIST>
 static sc_status backward_list(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views, const ListArgs& l,
-                               const sc_tiling* tl, const float4* fwd, const float4* dl_dc, int mode, const uint2* aux,
-                               float4* proj_grad, const uint32_t* d_skip) {
+                               const sc_tiling* tl, const float4* fwd, const float4* dl_dc, const float* target,
+                               float mse_scale, double* loss, int mode, const uint2* aux, float4* proj_grad,
+                               const uint32_t* d_skip) {
   const BlendArgs a = blend_args(tl, stride);
+  const float gscale = (2.0f / ((float)tl->width * (float)tl->height * 3.0f)) * mse_scale;
   const uint32_t pixels = tl->tile_w * tl->tile_h;
   if (pixels > 512 || pixels % 32 != 0) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile must hold 32..512 pixels, multiple of 32");
   if (mode == SC_BWD_EXACT && !aux) return sc_fail(ctx, SC_ERR_INVALID_ARG, "exact backward needs the forward aux buffer");
@@ -760,27 +789,33 @@ static sc_status backward_list(sc_ctx* ctx, const float4* rec, uint32_t stride, 
   const int ppt = pick_ppt(tl);
   if (ppt == 1 && pixels > 256) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile too large for one pixel per thread");
   if (ppt == 2)
-    return backward_ppt<2, LIST>(ctx, a, (uint32_t)grid, pixels / 2, rec, l, fwd, dl_dc, mode, aux, proj_grad, d_skip);
-  return backward_ppt<1, LIST>(ctx, a, (uint32_t)grid, pixels, rec, l, fwd, dl_dc, mode, aux, proj_grad, d_skip);
+    return backward_ppt<2, LIST>(ctx, a, (uint32_t)grid, pixels / 2, rec, l, fwd, dl_dc, target, gscale, loss, mode,
+                                 aux, proj_grad, d_skip);
+  return backward_ppt<1, LIST>(ctx, a, (uint32_t)grid, pixels, rec, l, fwd, dl_dc, target, gscale, loss, mode, aux,
+                               proj_grad, d_skip);
 }
 
 sc_status launch_composite_backward(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
                                     const uint32_t* payloads, const uint32_t* ranges, const sc_tiling* tl,
                                     const float4* fwd, const float4* dl_dc, int mode, const uint2* aux,
-                                    float4* proj_grad, const uint32_t* d_skip) {
+                                    float4* proj_grad, const uint32_t* d_skip, const float* target,
+                                    float mse_scale, double* loss) {
   ListArgs l{payloads, reinterpret_cast<const uint2*>(ranges), nullptr, 0, 0};
-  return backward_list<LIST_PAIRS>(ctx, rec, stride, n_views, l, tl, fwd, dl_dc, mode, aux, proj_grad, d_skip);
+  return backward_list<LIST_PAIRS>(ctx, rec, stride, n_views, l, tl, fwd, dl_dc, target, mse_scale, loss, mode, aux,
+                                   proj_grad, d_skip);
 }
 
 sc_status launch_composite_backward_items(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
                                           const uint32_t* item_keys, const uint32_t* item_ids,
                                           const uint32_t* item_ranges, const sc_tiling* tl, const float4* fwd,
                                           const float4* dl_dc, int mode, const uint2* aux, float4* proj_grad,
-                                          const uint32_t* d_skip) {
+                                          const uint32_t* d_skip, const float* target, float mse_scale,
+                                          double* loss) {
   const BlendArgs a = blend_args(tl, stride);
   ListArgs l{item_ids, reinterpret_cast<const uint2*>(item_ranges), item_keys, (a.tiles_x + SC_SUPER - 1) / SC_SUPER,
              super_tiles_per_view(tl)};
-  return backward_list<LIST_ITEMS>(ctx, rec, stride, n_views, l, tl, fwd, dl_dc, mode, aux, proj_grad, d_skip);
+  return backward_list<LIST_ITEMS>(ctx, rec, stride, n_views, l, tl, fwd, dl_dc, target, mse_scale, loss, mode, aux,
+                                   proj_grad, d_skip);
 }
 
 // ---------------------------------------------------------------- tonemap (tonemap.wgsl:27-41)

@@ -396,10 +396,13 @@ sc_status launch_composite(sc_ctx* ctx, const float4* rec, uint32_t stride, uint
                            const uint32_t* d_skip);
 sc_status launch_mse(sc_ctx* ctx, const float4* pred, const float* target, uint64_t pixels_per_view,
                      uint32_t n_views, float scale, float4* dl_dc, double* loss);
+// with a target, dL/dC of the MSE (mse_scale as in launch_composite) and its
+// loss are formed from the image fwd instead of being read from dl_dc
 sc_status launch_composite_backward(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
                                     const uint32_t* payloads, const uint32_t* ranges, const sc_tiling* tl,
                                     const float4* fwd, const float4* dl_dc, int mode, const uint2* aux,
-                                    float4* proj_grad, const uint32_t* d_skip);
+                                    float4* proj_grad, const uint32_t* d_skip, const float* target = nullptr,
+                                    float mse_scale = 0.0f, double* loss = nullptr);
 // the same two passes over super-tile item lists (launch_super_emit's items
 // sorted by super tile, item_ranges per (view, super tile)): each tile blends
 // the items whose member mask holds it, in list order; aux then holds
@@ -412,7 +415,8 @@ sc_status launch_composite_backward_items(sc_ctx* ctx, const float4* rec, uint32
                                           const uint32_t* item_keys, const uint32_t* item_ids,
                                           const uint32_t* item_ranges, const sc_tiling* tl, const float4* fwd,
                                           const float4* dl_dc, int mode, const uint2* aux, float4* proj_grad,
-                                          const uint32_t* d_skip);
+                                          const uint32_t* d_skip, const float* target = nullptr,
+                                          float mse_scale = 0.0f, double* loss = nullptr);
 sc_status launch_tonemap(sc_ctx* ctx, const float4* img, uint32_t w, uint32_t h, uint8_t* out);
 
 // SSIM (loss.rs:22-375): scale * dL_ssim/dC added into dl_dc, per-view sum of

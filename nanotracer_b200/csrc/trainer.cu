@@ -337,29 +337,36 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   SC_TRY(sck::launch_tile_ranges(ctx, skeys, 2, tr->d_total, tr->kcap, all_tiles, tr->ranges, tr->T, tile_bits));
   }
   mark(tr, 6, capturing);
-  if (tr->h_targets) SC_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, tr->ev_copied, 0), "join");
   const float weight = tr->grads_mode ? tr->loss_weight : 1.0f / (float)V;
   const float lam = tr->cfg.ssim_lambda;
   const float mse_w = lam > 0.0f ? weight * (1.0f - lam) : weight;
+  // with the MSE alone, the backward forms dL/dC from the image, so the targets
+  // are needed only from the backward on (a host upload overlaps the forward)
+  const bool mse_in_bwd = lam == 0.0f;
+  const float* fwd_target = mse_in_bwd ? nullptr : tr->targets;
+  if (tr->h_targets && !mse_in_bwd) SC_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, tr->ev_copied, 0), "join");
   if (tr->two_level)
     SC_TRY(sck::launch_composite_items(ctx, tr->rec, tr->stride, V, item_keys, item_ids, tr->iranges, &tr->cfg.tiling,
-                                       tr->image, tr->aux, tr->targets, mse_w, tr->dl_dc, tr->d_loss, ctx->d_error));
+                                       tr->image, tr->aux, fwd_target, mse_w, tr->dl_dc, tr->d_loss, ctx->d_error));
   else
     SC_TRY(sck::launch_composite(ctx, tr->rec, tr->stride, V, svals, tr->ranges, &tr->cfg.tiling, tr->image, tr->aux,
-                                 tr->targets, mse_w, tr->dl_dc, tr->d_loss, ctx->d_error));
+                                 fwd_target, mse_w, tr->dl_dc, tr->d_loss, ctx->d_error));
   if (lam > 0.0f) {
     SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->d_ssim, 0, 8 * (size_t)V, ctx->stream), "zero ssim");
     SC_TRY(sck::launch_ssim(ctx, tr->image, tr->targets, tr->cfg.tiling.width, tr->cfg.tiling.height, V,
                             weight * lam, tr->dl_dc, tr->d_ssim, tr->ssim_terms));
   }
   mark(tr, 7, capturing);
+  if (tr->h_targets && mse_in_bwd) SC_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, tr->ev_copied, 0), "join");
+  const float* bwd_target = mse_in_bwd ? tr->targets : nullptr;
   if (tr->two_level)
     SC_TRY(sck::launch_composite_backward_items(ctx, tr->rec, tr->stride, V, item_keys, item_ids, tr->iranges,
                                                 &tr->cfg.tiling, tr->image, tr->dl_dc, (int)tr->cfg.bwd_mode, tr->aux,
-                                                tr->pgrad, ctx->d_error));
+                                                tr->pgrad, ctx->d_error, bwd_target, mse_w, tr->d_loss));
   else
     SC_TRY(sck::launch_composite_backward(ctx, tr->rec, tr->stride, V, svals, tr->ranges, &tr->cfg.tiling, tr->image,
-                                          tr->dl_dc, (int)tr->cfg.bwd_mode, tr->aux, tr->pgrad, ctx->d_error));
+                                          tr->dl_dc, (int)tr->cfg.bwd_mode, tr->aux, tr->pgrad, ctx->d_error,
+                                          bwd_target, mse_w, tr->d_loss));
   mark(tr, 8, capturing);
   sck::AdamParams ap;
   for (int k = 0; k < 6; ++k) ap.lr[k] = tr->cfg.adam.lr[k];
