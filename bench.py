@@ -249,6 +249,9 @@ def run_ours(args):
     rest_b = 90 if bf16 else 180
     mom_b = 59 * 2 * (2 if bf16 else 4)
     items = st.get("items") or 0
+    bw = st.get("blend_work") or {}
+    fwd_list = bw.get("fwd_scanned", 0) * 8 + bw.get("fwd_blended", 0) * 48  # item words + blended records
+    bwd_list = bw.get("bwd_scanned", 0) * 8 + bw.get("bwd_blended", 0) * 48
     algo = {
         "project": N * (56 + rest_b) + V * N * (48 + 8 + 4 + 4),
         "depth_sort": 5 * V * N * 24,
@@ -256,12 +259,13 @@ def run_ours(args):
         "emit": V * N * (4 + 16 + 4) + K * 8,
         "tile_sort": 2 * K * 16 + K * 4,
         "ranges": K * 4 + tiles * 8,
-        # two-level binning: items (super tile, splat)
+        # two-level binning: items (member mask | super tile, splat); the blends
+        # read each tile's super-tile item list up to where its pixels saturate
         "item_emit": V * N * (4 + 16 + 4) + items * 8,
         "item_sort": 2 * items * 16 + items * 4,
-        "tile_lists": items * (4 + 48 + 2) + items * (4 + 2) + K * 4 + tiles * 16,
-        "blend_fwd": K * (4 + 48) + V * P * (16 + 8 + 12 + 16),
-        "blend_bwd": K * (4 + 48) + V * P * (16 + 16 + 8) + V * N * 48 * 2,
+        "item_ranges": items * 4,
+        "blend_fwd": fwd_list + V * P * (16 + 8),
+        "blend_bwd": bwd_list + V * P * (16 + 8 + 12) + V * N * 48,
         "bwd_adam": N * (56 + rest_b + 2 * rest_b) + V * N * 48 + N * (mom_b * 2) + N * 8,
     }
     peaks = load_peaks()
@@ -270,7 +274,7 @@ def run_ours(args):
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"],
                 "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": None,
                 "peak_source": peaks["source"], "algorithmic_bytes": int(algo[dom]), "avg_ms": round(dom_ms, 4),
-                "stage_ms": {k: round(v, 4) for k, v in stage.items()}}
+                "stage_ms": {k: round(v, 4) for k, v in stage.items()}, "blend_work": bw}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -290,8 +294,8 @@ def run_ours(args):
                                    f"{' per GPU (one scene per GPU)' if ws > 1 else ''}, "
                                    f"{args.tile_w}x{args.tile_h} tiles, exact transmittance backward, CUDA graph",
                        "form": "batched-" + ("bf16" if bf16 else "fp32"), "splats": N, "views_per_iter": V,
-                       "width": args.width, "height": args.height, "pairs_per_iter": K,
-                       "l2": "inputs larger than L2 (params, pair lists and images >> 126 MB)",
+                       "width": args.width, "height": args.height, "pairs_per_iter": K, "items_per_iter": items,
+                       "l2": "inputs larger than L2 (params, item lists and images >> 126 MB)",
                        "parallelism": f"{ws} GPUs, one scene each (no exchange)" if ws > 1 else "single GPU"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clocks, "loss": loss, "psnr": psnr,

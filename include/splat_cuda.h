@@ -363,6 +363,11 @@ sc_status sc_trainer_stats(const sc_trainer* tr, uint64_t* pairs, uint32_t* n_ke
                            float* avg_ms, uint64_t* items);
 /* Record CUDA events between the stages of each step (also inside the graph). */
 sc_status sc_trainer_set_profiling(sc_trainer* tr, int enabled);
+/* Blend work per step, averaged over the steps since profiling was enabled
+ * (two-level binning only; zeros otherwise): out[0] list positions the
+ * forward's batches covered, out[1] entries it blended, out[2], out[3] the
+ * same for the backward.  No counterpart in the reference. */
+sc_status sc_trainer_blend_work(const sc_trainer* tr, uint64_t out[4]);
 
 /* Failure-detection self-test (no counterpart in the reference): runs one
  * radix-sort pass whose look-back waits on a tile that is never processed.

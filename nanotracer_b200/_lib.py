@@ -137,6 +137,7 @@ _PROTOS = {
     "sc_trainer_images": (ST, [P, C.POINTER(P)]),
     "sc_trainer_stats": (ST, [P, C.POINTER(U64), C.POINTER(U32), P, P, C.POINTER(U64)]),
     "sc_trainer_set_profiling": (ST, [P, I32]),
+    "sc_trainer_blend_work": (ST, [P, C.POINTER(U64)]),
     "sc_selftest_wait_timeout": (ST, [P]),
     "sc_trainer_step_grads": (ST, [P, P, P, F32, U32, U32, P, C.POINTER(C.c_double)]),
     "sc_adam_step_shard": (ST, [P, P, P, P, P, U32, U32, U32, U64, C.POINTER(sc_adam_groups), F32, F32, F32]),

@@ -426,210 +426,4 @@ sc_status launch_super_emit(sc_ctx* ctx, const float4* rec, uint32_t stride, uin
   return sc_check_launch(ctx, "k_super_emit");
 }
 
-constexpr int SUPER_THREADS = 256;
-constexpr int SUPER_TILES = SC_SUPER * SC_SUPER;  // 16 tiles, one bit each in a 16-bit mask
-
-// The items of a super tile are cut into segments of SUPER_THREADS items (one
-// item per thread), so a crowded super tile is spread over many CTAs.
-// seg_base[vst] = first segment of super tile vst (exclusive scan of its
-// segment counts); a CTA finds its super tile by binary search.
-__global__ void k_super_segments(const uint2* __restrict__ item_ranges, uint32_t n_super, uint32_t* __restrict__ nseg) {
-  const uint32_t vst = blockIdx.x * blockDim.x + threadIdx.x;
-  if (vst >= n_super) return;
-  const uint2 r = item_ranges[vst];
-  nseg[vst] = r.y > r.x ? (r.y - r.x + SUPER_THREADS - 1) / SUPER_THREADS : 0u;
-}
-
-// super tile of segment b: the vst with seg_base[vst] <= b < seg_base[vst + 1]
-__device__ __forceinline__ uint32_t segment_owner(const uint32_t* __restrict__ seg_base, uint32_t n_super, uint32_t b) {
-  uint32_t lo = 0, hi = n_super;  // seg_base[lo] <= b < seg_base[hi]
-  while (hi - lo > 1) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (seg_base[mid] <= b) lo = mid; else hi = mid;
-  }
-  return lo;
-}
-
-__device__ __forceinline__ int tile_of_bit(int t, int tx0, int ty0, const BinArgs& a, uint32_t v) {
-  const int tx = tx0 + t % SC_SUPER, ty = ty0 + t / SC_SUPER;
-  return (tx < (int)a.tiles_x && ty < (int)a.tiles_y) ? (int)(v * a.num_tiles + (uint32_t)ty * a.tiles_x + (uint32_t)tx)
-                                                      : -1;
-}
-
-// One segment: its member count per tile (from the masks the emission put in
-// the item keys).
-__global__ void __launch_bounds__(SUPER_THREADS) k_super_count(const uint32_t* __restrict__ item_keys,
-                                                               const uint2* __restrict__ item_ranges,
-                                                               const uint32_t* __restrict__ seg_base, uint32_t n_super,
-                                                               uint32_t* __restrict__ seg_counts) {
-  __shared__ uint32_t s_cnt[SUPER_TILES];
-  const uint32_t b = blockIdx.x;
-  if (b >= seg_base[n_super]) return;
-  const uint32_t vst = segment_owner(seg_base, n_super, b);
-  const int lane = threadIdx.x & 31;
-  if (threadIdx.x < SUPER_TILES) s_cnt[threadIdx.x] = 0;
-  __syncthreads();
-  const uint2 r = item_ranges[vst];
-  const uint32_t jj = r.x + (b - seg_base[vst]) * SUPER_THREADS + threadIdx.x;
-  const uint32_t mask = jj < r.y ? item_keys[jj] >> SUPER_MASK_SHIFT : 0u;
-  uint32_t mine = 0;  // lane t < 16: this warp's members of tile t
-#pragma unroll
-  for (int t = 0; t < SUPER_TILES; ++t) {
-    const uint32_t bal = __ballot_sync(0xffffffffu, (mask >> t) & 1u);
-    if (lane == t) mine = __popc(bal);
-  }
-  if (lane < SUPER_TILES && mine) atomicAdd(&s_cnt[lane], mine);
-  __syncthreads();
-  if (threadIdx.x < SUPER_TILES) seg_counts[(size_t)b * SUPER_TILES + threadIdx.x] = s_cnt[threadIdx.x];
-}
-
-// Per super tile and tile: the segments' counts become exclusive prefixes in
-// item order, and the total is the tile's pair count.  One CTA per super tile:
-// thread (l, t) takes the l-th of 16 runs of consecutive segments for tile t,
-// so the dependent loads of a crowded super tile are 16 runs long, not one.
-__global__ void __launch_bounds__(256) k_super_seg_scan(const uint32_t* __restrict__ seg_base, BinArgs a,
-                                                         uint32_t super_x, uint32_t super_per_view,
-                                                         uint32_t* __restrict__ seg_counts,
-                                                         uint32_t* __restrict__ tile_counts) {
-  __shared__ uint32_t s_sum[16][SUPER_TILES];
-  const uint32_t vst = blockIdx.x;
-  const int t = (int)(threadIdx.x % SUPER_TILES), l = (int)(threadIdx.x / SUPER_TILES);
-  const uint32_t b0 = seg_base[vst], b1 = seg_base[vst + 1];
-  const uint32_t per = (b1 - b0 + 15) / 16;
-  const uint32_t r0 = min(b0 + (uint32_t)l * per, b1), r1 = min(r0 + per, b1);
-  uint32_t sum = 0;
-  for (uint32_t b = r0; b < r1; ++b) sum += seg_counts[(size_t)b * SUPER_TILES + t];
-  s_sum[l][t] = sum;
-  __syncthreads();
-  uint32_t acc = 0, total = 0;
-  for (int q = 0; q < 16; ++q) {
-    const uint32_t x = s_sum[q][t];
-    if (q < l) acc += x;
-    total += x;
-  }
-  for (uint32_t b = r0; b < r1; ++b) {
-    uint32_t* c = seg_counts + (size_t)b * SUPER_TILES + t;
-    const uint32_t x = *c;
-    *c = acc;
-    acc += x;
-  }
-  if (l == 0) {
-    const uint32_t v = vst / super_per_view, st = vst - v * super_per_view;
-    const int tile = tile_of_bit(t, (int)(st % super_x) * SC_SUPER, (int)(st / super_x) * SC_SUPER, a, v);
-    if (tile >= 0) tile_counts[tile] = total;
-  }
-}
-
-sc_status launch_super_count(sc_ctx* ctx, uint32_t n_views, const uint32_t* item_keys, const uint32_t* item_ranges,
-                             uint32_t* seg_base, uint64_t max_segments, const sc_tiling* tl, uint32_t* seg_counts,
-                             uint32_t* tile_counts, void* scratch, size_t scratch_bytes) {
-  const BinArgs a = bin_args(tl);
-  const uint32_t spv = super_tiles_per_view(tl);
-  const uint32_t n_super = n_views * spv;
-  if (n_super == 0) return SC_OK;
-  const uint32_t sx = (a.tiles_x + SC_SUPER - 1) / SC_SUPER;
-  SC_CUDA_TRY(ctx, cudaMemsetAsync(seg_base + n_super, 0, 4, ctx->stream), "zero tail");
-  k_super_segments<<<(n_super + 255) / 256, 256, 0, ctx->stream>>>(reinterpret_cast<const uint2*>(item_ranges),
-                                                                    n_super, seg_base);
-  SC_TRY(sc_check_launch(ctx, "k_super_segments"));
-  SC_TRY(scan_u32(ctx, seg_base, (uint64_t)n_super + 1, nullptr, scratch, scratch_bytes));
-  if (max_segments == 0) return SC_OK;
-  k_super_count<<<(unsigned)max_segments, SUPER_THREADS, 0, ctx->stream>>>(
-      item_keys, reinterpret_cast<const uint2*>(item_ranges), seg_base, n_super, seg_counts);
-  SC_TRY(sc_check_launch(ctx, "k_super_count"));
-  k_super_seg_scan<<<n_super, 256, 0, ctx->stream>>>(seg_base, a, sx, spv, seg_counts, tile_counts);
-  return sc_check_launch(ctx, "k_super_seg_scan");
-}
-
-__global__ void k_ranges_from_offsets(const uint32_t* __restrict__ off, uint32_t num_tiles,
-                                      uint32_t* __restrict__ ranges) {
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= num_tiles) return;
-  ranges[2 * (size_t)t] = off[t];
-  ranges[2 * (size_t)t + 1] = off[t + 1];
-}
-
-sc_status launch_ranges_from_offsets(sc_ctx* ctx, const uint32_t* offsets, uint32_t num_tiles, uint32_t* ranges) {
-  if (num_tiles == 0) return SC_OK;
-  k_ranges_from_offsets<<<(num_tiles + 255) / 256, 256, 0, ctx->stream>>>(offsets, num_tiles, ranges);
-  return sc_check_launch(ctx, "k_ranges_from_offsets");
-}
-
-// One segment: each item appended to the lists of its member tiles at
-// tile offset + the earlier segments' members + the earlier items' in this one.
-__global__ void __launch_bounds__(SUPER_THREADS) k_super_fill(const uint32_t* __restrict__ items,
-                                                              const uint2* __restrict__ item_ranges,
-                                                              const uint32_t* __restrict__ seg_base,
-                                                              const uint32_t* __restrict__ item_keys,
-                                                              const uint32_t* __restrict__ seg_counts,
-                                                              const uint32_t* __restrict__ tile_off, BinArgs a,
-                                                              uint32_t super_x, uint32_t super_per_view,
-                                                              uint32_t n_super, uint32_t all_tiles,
-                                                              uint32_t* __restrict__ pairs, uint64_t cap,
-                                                              uint32_t* __restrict__ err) {
-  constexpr int WARPS = SUPER_THREADS / 32;
-  __shared__ uint32_t s_base[SUPER_TILES];          // list position of this segment's first member, per tile
-  __shared__ uint32_t s_wcnt[WARPS][SUPER_TILES];   // members per warp, then their exclusive prefix
-  const uint32_t b = blockIdx.x;
-  if (b == 0 && threadIdx.x == 0 && tile_off[all_tiles] > cap) atomicOr(err, SC_DEVERR_CAPACITY);
-  if (b >= seg_base[n_super]) return;
-  const uint32_t vst = segment_owner(seg_base, n_super, b);
-  const uint32_t v = vst / super_per_view, st = vst - v * super_per_view;
-  const int tx0 = (int)(st % super_x) * SC_SUPER, ty0 = (int)(st / super_x) * SC_SUPER;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (threadIdx.x < SUPER_TILES) {
-    const int tile = tile_of_bit((int)threadIdx.x, tx0, ty0, a, v);
-    s_base[threadIdx.x] = tile >= 0 ? tile_off[tile] + seg_counts[(size_t)b * SUPER_TILES + threadIdx.x] : 0u;
-  }
-  const uint2 r = item_ranges[vst];
-  const uint32_t jj = r.x + (b - seg_base[vst]) * SUPER_THREADS + threadIdx.x;
-  uint32_t mask = 0, id = 0;
-  if (jj < r.y) {
-    mask = item_keys[jj] >> SUPER_MASK_SHIFT;
-    id = items[jj];
-  }
-#pragma unroll
-  for (int t = 0; t < SUPER_TILES; ++t) {
-    const uint32_t bal = __ballot_sync(0xffffffffu, (mask >> t) & 1u);
-    if (lane == 0) s_wcnt[warp][t] = __popc(bal);
-  }
-  __syncthreads();
-  if (threadIdx.x < SUPER_TILES) {  // exclusive prefix over the warps, per tile
-    uint32_t acc = 0;
-#pragma unroll
-    for (int w = 0; w < WARPS; ++w) {
-      const uint32_t c = s_wcnt[w][threadIdx.x];
-      s_wcnt[w][threadIdx.x] = acc;
-      acc += c;
-    }
-  }
-  __syncthreads();
-  const unsigned lt = (1u << lane) - 1u;
-#pragma unroll
-  for (int t = 0; t < SUPER_TILES; ++t) {
-    const uint32_t bal = __ballot_sync(0xffffffffu, (mask >> t) & 1u);
-    if ((mask >> t) & 1u) {
-      const uint64_t pos = (uint64_t)s_base[t] + s_wcnt[warp][t] + __popc(bal & lt);
-      if (pos < cap) pairs[pos] = id;
-    }
-  }
-}
-
-sc_status launch_super_fill(sc_ctx* ctx, uint32_t n_views, const uint32_t* items, const uint32_t* item_ranges,
-                            const uint32_t* seg_base, uint64_t max_segments, const uint32_t* item_keys,
-                            const uint32_t* seg_counts, const uint32_t* tile_offsets, const sc_tiling* tl,
-                            uint32_t* pairs, uint64_t cap, uint32_t* d_error) {
-  const BinArgs a = bin_args(tl);
-  const uint32_t spv = super_tiles_per_view(tl);
-  if (n_views * spv == 0 || max_segments == 0) return SC_OK;
-  k_super_fill<<<(unsigned)max_segments, SUPER_THREADS, 0, ctx->stream>>>(
-      items, reinterpret_cast<const uint2*>(item_ranges), seg_base, item_keys, seg_counts, tile_offsets, a,
-      (a.tiles_x + SC_SUPER - 1) / SC_SUPER, spv, n_views * spv, n_views * a.num_tiles, pairs, cap, d_error);
-  return sc_check_launch(ctx, "k_super_fill");
-}
-
-uint64_t super_max_segments(uint64_t item_cap, uint32_t n_super) {
-  return (item_cap + SUPER_THREADS - 1) / SUPER_THREADS + n_super;
-}
-
 }  // namespace sck

@@ -129,6 +129,17 @@ __device__ __forceinline__ float3 mse_pixel(float cr, float cg, float cb, const 
   return make_float3(__fmul_rn(dx, gscale), __fmul_rn(dy, gscale), __fmul_rn(dz, gscale));
 }
 
+// Work counters of one blend launch (when given): per CTA, the list positions
+// its batches covered and the entries it staged, added into one of
+// BLEND_WORK_SLOTS (scanned, staged) pairs so that the atomics spread.
+__device__ __forceinline__ void add_work(unsigned long long* work, uint32_t scanned, uint32_t staged) {
+  if (work && threadIdx.x == 0 && scanned) {
+    unsigned long long* w = work + 2 * (blockIdx.x % BLEND_WORK_SLOTS);
+    atomicAdd(w, (unsigned long long)scanned);
+    atomicAdd(w + 1, (unsigned long long)staged);
+  }
+}
+
 // Pixel placement: thread t owns column t % tw and rows PPT*(t / tw) + k.
 
 // Where a CTA's depth-ordered splat list comes from.  LIST_PAIRS: the tile's
@@ -226,7 +237,8 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
                                                    float4* __restrict__ image, uint2* __restrict__ aux,
                                                    const float* __restrict__ target, float gscale,
                                                    float4* __restrict__ dl_dc, double* __restrict__ loss,
-                                                   const uint32_t* __restrict__ skip) {
+                                                   const uint32_t* __restrict__ skip,
+                                                   unsigned long long* __restrict__ work) {
   extern __shared__ float4 sbuf[];  // records [2][B][3], item positions [2][B] (u32)
   __shared__ double sred[8];
   __shared__ uint32_t s_wcnt[2][8];
@@ -272,8 +284,11 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
   ListWord f = fetch(0);
   uint32_t cnt_next = nb > 0 ? place(0, f) : 0u;
   if (nb > 1) f = fetch(1);
+  uint32_t w_scan = 0, w_staged = 0;
   for (uint32_t b = 0; b < nb; ++b) {
     const uint32_t cnt = cnt_next;
+    w_scan += min(B, end - (begin + b * B));
+    w_staged += cnt;
     if (b + 1 < nb) {
       cnt_next = place(b + 1, f);
       if (b + 2 < nb) f = fetch(b + 2);
@@ -346,6 +361,7 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
     if (__syncthreads_count(all_done) == (int)B) break;
   }
   cp_async_wait_all();
+  add_work(work, w_scan, w_staged);
   double sq = 0.0;
 #pragma unroll
   for (int q = 0; q < PPT; ++q) {
@@ -369,10 +385,11 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
 template <int PPT, int LIST>
 static sc_status composite_ppt(sc_ctx* ctx, const BlendArgs& a, uint32_t grid, uint32_t threads, const float4* rec,
                                const ListArgs& l, float4* image, uint2* aux, const float* target, float gscale,
-                               float4* dl_dc, double* loss, const uint32_t* d_skip) {
+                               float4* dl_dc, double* loss, const uint32_t* d_skip, uint64_t* work) {
   const size_t smem = (size_t)2 * 3 * threads * sizeof(float4) + (size_t)2 * threads * sizeof(uint32_t);
   k_composite<PPT, LIST><<<grid, threads, smem, ctx->stream>>>(rec, l, a, image, aux, target, gscale, dl_dc, loss,
-                                                               d_skip);
+                                                               d_skip,
+                                                               reinterpret_cast<unsigned long long*>(work));
   return sc_check_launch(ctx, "k_composite");
 }
 
@@ -387,7 +404,7 @@ static int pick_ppt(const sc_tiling* tl) {
 template <int LIST>
 static sc_status composite_list(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views, const ListArgs& l,
                                 const sc_tiling* tl, float4* image, uint2* aux, const float* target, float mse_scale,
-                                float4* dl_dc, double* loss, const uint32_t* d_skip) {
+                                float4* dl_dc, double* loss, const uint32_t* d_skip, uint64_t* work) {
   const BlendArgs a = blend_args(tl, stride);
   const uint32_t pixels = tl->tile_w * tl->tile_h;
   if (pixels > 512 || pixels % 32 != 0) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile must hold 32..512 pixels, multiple of 32");
@@ -399,9 +416,9 @@ static sc_status composite_list(sc_ctx* ctx, const float4* rec, uint32_t stride,
   if (ppt == 1 && pixels > 256) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile too large for one pixel per thread");
   if (ppt == 2)
     return composite_ppt<2, LIST>(ctx, a, (uint32_t)grid, pixels / 2, rec, l, image, aux, target, gscale, dl_dc, loss,
-                                  d_skip);
+                                  d_skip, work);
   return composite_ppt<1, LIST>(ctx, a, (uint32_t)grid, pixels, rec, l, image, aux, target, gscale, dl_dc, loss,
-                                d_skip);
+                                d_skip, work);
 }
 
 sc_status launch_composite(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views, const uint32_t* payloads,
@@ -409,18 +426,18 @@ sc_status launch_composite(sc_ctx* ctx, const float4* rec, uint32_t stride, uint
                            float mse_scale, float4* dl_dc, double* loss, const uint32_t* d_skip) {
   ListArgs l{payloads, reinterpret_cast<const uint2*>(ranges), nullptr, 0, 0};
   return composite_list<LIST_PAIRS>(ctx, rec, stride, n_views, l, tl, image, aux, target, mse_scale, dl_dc, loss,
-                                    d_skip);
+                                    d_skip, nullptr);
 }
 
 sc_status launch_composite_items(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
                                  const uint32_t* item_keys, const uint32_t* item_ids, const uint32_t* item_ranges,
                                  const sc_tiling* tl, float4* image, uint2* aux, const float* target, float mse_scale,
-                                 float4* dl_dc, double* loss, const uint32_t* d_skip) {
+                                 float4* dl_dc, double* loss, const uint32_t* d_skip, uint64_t* work) {
   const BlendArgs a = blend_args(tl, stride);
   ListArgs l{item_ids, reinterpret_cast<const uint2*>(item_ranges), item_keys, (a.tiles_x + SC_SUPER - 1) / SC_SUPER,
              super_tiles_per_view(tl)};
   return composite_list<LIST_ITEMS>(ctx, rec, stride, n_views, l, tl, image, aux, target, mse_scale, dl_dc, loss,
-                                    d_skip);
+                                    d_skip, work);
 }
 
 // ---------------------------------------------------------------- MSE (standalone)
@@ -530,7 +547,8 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
                                                             double* __restrict__ loss,
                                                             const uint2* __restrict__ aux,
                                                             float4* __restrict__ proj_grad,
-                                                            const uint32_t* __restrict__ skip) {
+                                                            const uint32_t* __restrict__ skip,
+                                                            unsigned long long* __restrict__ work) {
   // records [2][B][3], acc [B][3] (float4), ids [2][B], item positions [2][B] (u32)
   extern __shared__ float4 sbuf[];
   __shared__ uint32_t s_max;
@@ -621,8 +639,10 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
   ListWord f = fetch(0);
   uint32_t cnt_next = place(0, f);
   if (nb > 1) f = fetch(1);
+  uint32_t w_staged = 0;
   for (uint32_t b = 0; b < nb; ++b) {
     const uint32_t cnt = cnt_next;
+    w_staged += cnt;
     if (b + 1 < nb) {
       cnt_next = place(b + 1, f);
       if (b + 2 < nb) f = fetch(b + 2);
@@ -757,20 +777,22 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
     if (__syncthreads_count(all_done) == (int)B) break;
   }
   cp_async_wait_all();
+  add_work(work, hi0 - begin, w_staged);
 }
 
 template <int PPT, int LIST>
 static sc_status backward_ppt(sc_ctx* ctx, const BlendArgs& a, uint32_t grid, uint32_t threads, const float4* rec,
                               const ListArgs& l, const float4* fwd, const float4* dl_dc, const float* target,
                               float gscale, double* loss, int mode, const uint2* aux, float4* proj_grad,
-                              const uint32_t* d_skip) {
+                              const uint32_t* d_skip, uint64_t* work) {
   const size_t smem = (size_t)9 * threads * sizeof(float4) + (size_t)4 * threads * sizeof(uint32_t);
+  unsigned long long* w = reinterpret_cast<unsigned long long*>(work);
   if (mode == SC_BWD_EXACT)
     k_composite_backward<PPT, SC_BWD_EXACT, LIST><<<grid, threads, smem, ctx->stream>>>(
-        rec, l, a, fwd, dl_dc, target, gscale, loss, aux, proj_grad, d_skip);
+        rec, l, a, fwd, dl_dc, target, gscale, loss, aux, proj_grad, d_skip, w);
   else
     k_composite_backward<PPT, SC_BWD_REF, LIST><<<grid, threads, smem, ctx->stream>>>(
-        rec, l, a, fwd, dl_dc, target, gscale, loss, aux, proj_grad, d_skip);
+        rec, l, a, fwd, dl_dc, target, gscale, loss, aux, proj_grad, d_skip, w);
   return sc_check_launch(ctx, "k_composite_backward");
 }
 
@@ -778,7 +800,7 @@ template <int LIST>
 static sc_status backward_list(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views, const ListArgs& l,
                                const sc_tiling* tl, const float4* fwd, const float4* dl_dc, const float* target,
                                float mse_scale, double* loss, int mode, const uint2* aux, float4* proj_grad,
-                               const uint32_t* d_skip) {
+                               const uint32_t* d_skip, uint64_t* work) {
   const BlendArgs a = blend_args(tl, stride);
   const float gscale = (2.0f / ((float)tl->width * (float)tl->height * 3.0f)) * mse_scale;
   const uint32_t pixels = tl->tile_w * tl->tile_h;
@@ -790,9 +812,9 @@ static sc_status backward_list(sc_ctx* ctx, const float4* rec, uint32_t stride, 
   if (ppt == 1 && pixels > 256) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile too large for one pixel per thread");
   if (ppt == 2)
     return backward_ppt<2, LIST>(ctx, a, (uint32_t)grid, pixels / 2, rec, l, fwd, dl_dc, target, gscale, loss, mode,
-                                 aux, proj_grad, d_skip);
+                                 aux, proj_grad, d_skip, work);
   return backward_ppt<1, LIST>(ctx, a, (uint32_t)grid, pixels, rec, l, fwd, dl_dc, target, gscale, loss, mode, aux,
-                               proj_grad, d_skip);
+                               proj_grad, d_skip, work);
 }
 
 sc_status launch_composite_backward(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
@@ -802,7 +824,7 @@ sc_status launch_composite_backward(sc_ctx* ctx, const float4* rec, uint32_t str
                                     float mse_scale, double* loss) {
   ListArgs l{payloads, reinterpret_cast<const uint2*>(ranges), nullptr, 0, 0};
   return backward_list<LIST_PAIRS>(ctx, rec, stride, n_views, l, tl, fwd, dl_dc, target, mse_scale, loss, mode, aux,
-                                   proj_grad, d_skip);
+                                   proj_grad, d_skip, nullptr);
 }
 
 sc_status launch_composite_backward_items(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
@@ -810,12 +832,12 @@ sc_status launch_composite_backward_items(sc_ctx* ctx, const float4* rec, uint32
                                           const uint32_t* item_ranges, const sc_tiling* tl, const float4* fwd,
                                           const float4* dl_dc, int mode, const uint2* aux, float4* proj_grad,
                                           const uint32_t* d_skip, const float* target, float mse_scale,
-                                          double* loss) {
+                                          double* loss, uint64_t* work) {
   const BlendArgs a = blend_args(tl, stride);
   ListArgs l{item_ids, reinterpret_cast<const uint2*>(item_ranges), item_keys, (a.tiles_x + SC_SUPER - 1) / SC_SUPER,
              super_tiles_per_view(tl)};
   return backward_list<LIST_ITEMS>(ctx, rec, stride, n_views, l, tl, fwd, dl_dc, target, mse_scale, loss, mode, aux,
-                                   proj_grad, d_skip);
+                                   proj_grad, d_skip, work);
 }
 
 // ---------------------------------------------------------------- tonemap (tonemap.wgsl:27-41)

@@ -371,23 +371,6 @@ sc_status launch_super_emit(sc_ctx* ctx, const float4* rec, uint32_t stride, uin
                             const sc_tiling* tl, uint32_t* keys, uint32_t* payloads, uint64_t cap, uint32_t* d_error,
                             int cull);
 uint32_t super_tiles_per_view(const sc_tiling* tl);
-// per super tile (its items grouped by a stable sort), cut into segments of
-// 256 items: seg_base (n_super + 1 entries) = first segment of each super
-// tile; per segment and tile the members before it (exclusive, item order);
-// per tile the pair count.  The member masks come from the sorted item keys.
-// max_segments = super_max_segments(item capacity, n_super) CTAs are launched.
-uint64_t super_max_segments(uint64_t item_cap, uint32_t n_super);
-sc_status launch_super_count(sc_ctx* ctx, uint32_t n_views, const uint32_t* item_keys, const uint32_t* item_ranges,
-                             uint32_t* seg_base, uint64_t max_segments, const sc_tiling* tl, uint32_t* seg_counts,
-                             uint32_t* tile_counts, void* scratch, size_t scratch_bytes);
-// ranges[vt] = [off[vt], off[vt+1]) from the scanned tile counts
-sc_status launch_ranges_from_offsets(sc_ctx* ctx, const uint32_t* offsets, uint32_t num_tiles, uint32_t* ranges);
-// per segment, in item order: each item's splat id appended to the lists of
-// its member tiles at their offsets (pairs in tile, then depth order)
-sc_status launch_super_fill(sc_ctx* ctx, uint32_t n_views, const uint32_t* items, const uint32_t* item_ranges,
-                            const uint32_t* seg_base, uint64_t max_segments, const uint32_t* item_keys,
-                            const uint32_t* seg_counts, const uint32_t* tile_offsets, const sc_tiling* tl,
-                            uint32_t* pairs, uint64_t cap, uint32_t* d_error);
 
 // blending
 sc_status launch_composite(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
@@ -406,17 +389,20 @@ sc_status launch_composite_backward(sc_ctx* ctx, const float4* rec, uint32_t str
 // the same two passes over super-tile item lists (launch_super_emit's items
 // sorted by super tile, item_ranges per (view, super tile)): each tile blends
 // the items whose member mask holds it, in list order; aux then holds
-// positions within the super tile's list
+// positions within the super tile's list.  work (nullable, BLEND_WORK_SLOTS
+// (scanned, staged) pairs, accumulated): the list positions the CTAs' batches
+// covered and the entries they staged.
+constexpr uint32_t BLEND_WORK_SLOTS = 64;
 sc_status launch_composite_items(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
                                  const uint32_t* item_keys, const uint32_t* item_ids, const uint32_t* item_ranges,
                                  const sc_tiling* tl, float4* image, uint2* aux, const float* target, float mse_scale,
-                                 float4* dl_dc, double* loss, const uint32_t* d_skip);
+                                 float4* dl_dc, double* loss, const uint32_t* d_skip, uint64_t* work = nullptr);
 sc_status launch_composite_backward_items(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
                                           const uint32_t* item_keys, const uint32_t* item_ids,
                                           const uint32_t* item_ranges, const sc_tiling* tl, const float4* fwd,
                                           const float4* dl_dc, int mode, const uint2* aux, float4* proj_grad,
                                           const uint32_t* d_skip, const float* target = nullptr,
-                                          float mse_scale = 0.0f, double* loss = nullptr);
+                                          float mse_scale = 0.0f, double* loss = nullptr, uint64_t* work = nullptr);
 sc_status launch_tonemap(sc_ctx* ctx, const float4* img, uint32_t w, uint32_t h, uint8_t* out);
 
 // SSIM (loss.rs:22-375): scale * dL_ssim/dC added into dl_dc, per-view sum of

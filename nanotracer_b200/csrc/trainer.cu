@@ -133,6 +133,9 @@ struct sc_trainer {
   double acc_ms[kStages] = {};
   uint64_t prof_steps = 0;
   float avg_ms_out[kStages] = {};
+  // blend work counters while profiling: forward then backward slots
+  uint64_t* d_work = nullptr;
+  uint64_t work_acc[4] = {};
 };
 
 static void trainer_free_splat_arrays(sc_trainer* tr) {
@@ -271,6 +274,10 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
     SC_CUDA_TRY(ctx, cudaEventRecord(tr->ev_copied, tr->copy_stream), "copied");
   }
   SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->d_loss, 0, 8 * (size_t)V, ctx->stream), "zero loss");
+  uint64_t* work_fwd = tr->profiling ? tr->d_work : nullptr;
+  uint64_t* work_bwd = tr->profiling ? tr->d_work + 2 * sck::BLEND_WORK_SLOTS : nullptr;
+  if (tr->profiling)
+    SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->d_work, 0, 4 * sck::BLEND_WORK_SLOTS * 8, ctx->stream), "zero work");
   SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->pgrad, 0, nsp * 48, ctx->stream), "zero pgrad");
   SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->counts + nsp, 0, 4, ctx->stream), "zero count tail");
   mark(tr, 0, capturing);
@@ -347,7 +354,8 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   if (tr->h_targets && !mse_in_bwd) SC_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, tr->ev_copied, 0), "join");
   if (tr->two_level)
     SC_TRY(sck::launch_composite_items(ctx, tr->rec, tr->stride, V, item_keys, item_ids, tr->iranges, &tr->cfg.tiling,
-                                       tr->image, tr->aux, fwd_target, mse_w, tr->dl_dc, tr->d_loss, ctx->d_error));
+                                       tr->image, tr->aux, fwd_target, mse_w, tr->dl_dc, tr->d_loss, ctx->d_error,
+                                       work_fwd));
   else
     SC_TRY(sck::launch_composite(ctx, tr->rec, tr->stride, V, svals, tr->ranges, &tr->cfg.tiling, tr->image, tr->aux,
                                  fwd_target, mse_w, tr->dl_dc, tr->d_loss, ctx->d_error));
@@ -362,7 +370,7 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   if (tr->two_level)
     SC_TRY(sck::launch_composite_backward_items(ctx, tr->rec, tr->stride, V, item_keys, item_ids, tr->iranges,
                                                 &tr->cfg.tiling, tr->image, tr->dl_dc, (int)tr->cfg.bwd_mode, tr->aux,
-                                                tr->pgrad, ctx->d_error, bwd_target, mse_w, tr->d_loss));
+                                                tr->pgrad, ctx->d_error, bwd_target, mse_w, tr->d_loss, work_bwd));
   else
     SC_TRY(sck::launch_composite_backward(ctx, tr->rec, tr->stride, V, svals, tr->ranges, &tr->cfg.tiling, tr->image,
                                           tr->dl_dc, (int)tr->cfg.bwd_mode, tr->aux, tr->pgrad, ctx->d_error,
@@ -434,6 +442,7 @@ sc_status sc_trainer_create(sc_ctx* ctx, const sc_train_config* cfg, sc_trainer*
   if (e == cudaSuccess) e = cudaMalloc(&tr->aux, pix * 8);
   if (e == cudaSuccess) e = cudaMalloc(&tr->dl_dc, pix * 16);
   if (e == cudaSuccess) e = cudaMalloc(&tr->d_loss, 8 * (size_t)tr->V);
+  if (e == cudaSuccess) e = cudaMalloc(&tr->d_work, 4 * sck::BLEND_WORK_SLOTS * 8);
   if (e == cudaSuccess) e = cudaMalloc(&tr->d_total, 64);
   if (e == cudaSuccess) e = cudaMemset(tr->d_total, 0, 64);
   if (e == cudaSuccess && tr->two_level) e = cudaMalloc(&tr->iranges, (size_t)tr->V * tr->ST * 8);
@@ -458,7 +467,7 @@ void sc_trainer_free(sc_ctx* ctx, sc_trainer* tr) {
   trainer_free_items(tr);
   cudaFree(tr->iranges);
   cudaFree(tr->ranges); cudaFree(tr->image); cudaFree(tr->aux); cudaFree(tr->dl_dc);
-  cudaFree(tr->d_loss); cudaFree(tr->d_total); cudaFree(tr->d_params); cudaFree(tr->d_out);
+  cudaFree(tr->d_loss); cudaFree(tr->d_work); cudaFree(tr->d_total); cudaFree(tr->d_params); cudaFree(tr->d_out);
   cudaFree(tr->ssim_terms); cudaFree(tr->d_ssim);
   cudaFree(tr->d_host_targets);
   if (tr->copy_stream) cudaStreamDestroy(tr->copy_stream);
@@ -505,6 +514,7 @@ sc_status sc_trainer_set_profiling(sc_trainer* tr, int enabled) {
   if (tr->profiling != (enabled != 0)) trainer_drop_graph(tr);
   tr->profiling = enabled != 0;
   for (int i = 0; i < kStages; ++i) tr->acc_ms[i] = 0.0;
+  for (int i = 0; i < 4; ++i) tr->work_acc[i] = 0;
   tr->prof_steps = 0;
   return SC_OK;
 }
@@ -570,6 +580,9 @@ static sc_status run_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, float* a
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, tr->ev[i], tr->ev[i + 1]) == cudaSuccess) tr->acc_ms[i] += ms;
       }
+      uint64_t w[4 * sck::BLEND_WORK_SLOTS];
+      SC_CUDA_TRY(ctx, cudaMemcpy(w, tr->d_work, sizeof(w), cudaMemcpyDeviceToHost), "work D2H");
+      for (uint32_t i = 0; i < 4 * sck::BLEND_WORK_SLOTS; ++i) tr->work_acc[(i / (2 * sck::BLEND_WORK_SLOTS)) * 2 + (i & 1)] += w[i];
       tr->prof_steps++;
     }
     if (loss_out) *loss_out = o.loss;
@@ -629,6 +642,12 @@ sc_status sc_trainer_stats(const sc_trainer* tr, uint64_t* pairs, uint32_t* n_ke
     if (names) names[i] = tr->two_level ? kStageNames2[i] : kStageNames[i];
     if (avg_ms) avg_ms[i] = tr->prof_steps ? (float)(tr->acc_ms[i] / (double)tr->prof_steps) : 0.0f;
   }
+  return SC_OK;
+}
+
+sc_status sc_trainer_blend_work(const sc_trainer* tr, uint64_t out[4]) {
+  if (!tr || !out) return SC_ERR_INVALID_ARG;
+  for (int i = 0; i < 4; ++i) out[i] = tr->prof_steps ? tr->work_acc[i] / tr->prof_steps : 0;
   return SC_OK;
 }
 

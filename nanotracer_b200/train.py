@@ -116,8 +116,12 @@ class Trainer:
         ms = (C.c_float * 9)()
         check(lib().sc_trainer_stats(self.handle, C.byref(pairs), C.byref(nk), names, ms, C.byref(items)),
               self.ctx.handle)
+        work = (C.c_uint64 * 4)()
+        check(lib().sc_trainer_blend_work(self.handle, work), self.ctx.handle)
         return {"pairs": pairs.value, "items": items.value, "kernels_per_step": nk.value,
-                "stage_ms": {names[i].decode(): float(ms[i]) for i in range(9)}}
+                "stage_ms": {names[i].decode(): float(ms[i]) for i in range(9)},
+                "blend_work": {"fwd_scanned": work[0], "fwd_blended": work[1], "bwd_scanned": work[2],
+                               "bwd_blended": work[3]}}
 
     def __del__(self):
         try:
