@@ -108,39 +108,199 @@ sc_status launch_accumulate(sc_ctx* ctx, const float* g, uint32_t gcap, float* a
   return sc_check_launch(ctx, "k_accumulate");
 }
 
-// ---------------------------------------------------------------- data-parallel shards
-// Adam + constraints + densify statistic over splats [lo, lo+count), gradient
-// rows g[r * shard + j] (one reduce-scattered chunk).  Same arithmetic as the
-// fused single-device kernel (folded bias corrections); one thread per splat so the 59 row accesses of a
-// warp are 32 consecutive splats.
-__global__ void k_adam_shard(DSplats s, DMoments mo, float* __restrict__ acc, const float* __restrict__ g, uint32_t lo,
-                             uint32_t count, uint32_t shard, AdamParams ap) {
-  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= count) return;
-  const uint32_t i = lo + j;
-  const AdamFast af = adam_fast(ap);
-  float gg[14], np[14];
+// ---------------------------------------------------------------- streaming Adam over gradient rows
+// Adam + constraints + densify statistic over splats [lo, lo+count) from
+// gradient rows g[r * gstride + j], j = i - lo (gstride and lo multiples of 8,
+// as are the slab and moment capacities).  grid.y picks a row group — 0
+// position rows (+ the statistic), 1 the rotation rows (normalised together),
+// 2..4 log-scale rows (clamped), 5 opacity (clamped), 6..8 sh_dc, 9.. the 45
+// sh_rest rows — and each thread updates 8 consecutive splats of it with
+// 16-byte loads and stores, so the pass streams at the memory's pace instead
+// of waiting on one splat's 59 rows at a time.  Same arithmetic as
+// adam_scalar_fast and constrain_geometry.
+constexpr int ADAM_SPT = 8;
+constexpr int ADAM_GROUPS = 9 + (SC_NROWS - SC_ROW_REST);
+
+__device__ __forceinline__ void ld8(const float* p, float* o) {
+  const float4 a = reinterpret_cast<const float4*>(p)[0], b = reinterpret_cast<const float4*>(p)[1];
+  o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w; o[4] = b.x; o[5] = b.y; o[6] = b.z; o[7] = b.w;
+}
+__device__ __forceinline__ void ld8(const __nv_bfloat16* p, float* o) {
+  const uint4 u = *reinterpret_cast<const uint4*>(p);
+  const uint32_t w[4] = {u.x, u.y, u.z, u.w};
 #pragma unroll
-  for (int r = 0; r < 14; ++r) gg[r] = g[(size_t)r * shard + j];
-  if (acc) acc[i] = acc[i] + fabsf(gg[0]) + fabsf(gg[1]) + fabsf(gg[2]);
+  for (int k = 0; k < 4; ++k) {
+    const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w[k]));
+    o[2 * k] = f.x; o[2 * k + 1] = f.y;
+  }
+}
+__device__ __forceinline__ void st8(float* p, const float* o) {
+  reinterpret_cast<float4*>(p)[0] = make_float4(o[0], o[1], o[2], o[3]);
+  reinterpret_cast<float4*>(p)[1] = make_float4(o[4], o[5], o[6], o[7]);
+}
+__device__ __forceinline__ void st8(__nv_bfloat16* p, const float* o) {
+  uint32_t w[4];
 #pragma unroll
-  for (int r = 0; r < 14; ++r)
-    np[r] = adam_scalar_fast(mo, (size_t)r * mo.cap + i, s.slab[(size_t)r * s.cap + i], gg[r], af.a[adam_group(r)],
-                             af.s2, ap);
-  constrain_geometry(np, ap);
-#pragma unroll
-  for (int r = 0; r < 14; ++r) s.slab[(size_t)r * s.cap + i] = np[r];
-#pragma unroll 5
-  for (int r = SC_ROW_REST; r < SC_NROWS; ++r)
-    sp_set(s, r, i, adam_scalar_fast(mo, (size_t)r * mo.cap + i, sp_row(s, r, i), g[(size_t)r * shard + j], af.a[5],
-                                     af.s2, ap));
+  for (int k = 0; k < 4; ++k) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(o[2 * k], o[2 * k + 1]);
+    w[k] = *reinterpret_cast<const uint32_t*>(&h);
+  }
+  *reinterpret_cast<uint4*>(p) = make_uint4(w[0], w[1], w[2], w[3]);
 }
 
+// one row of 8 splats: parameters, moments and gradients widened to f32;
+// `nv` < 8 loads (and later stores) only the first nv splats
+struct Row8 {
+  float p[8], m[8], v[8], g[8];
+};
+__device__ __forceinline__ void load_row8(const DSplats& s, const DMoments& mo, const float* __restrict__ g, int r,
+                                          uint32_t i0, uint32_t j0, uint32_t gstride, int nv, Row8& x) {
+  const size_t pk = (size_t)r * s.cap + i0, mk = (size_t)r * mo.cap + i0, gk = (size_t)r * gstride + j0;
+  const bool rest16 = r >= SC_ROW_REST && s.bf16;
+  if (nv == ADAM_SPT) {
+    ld8(g + gk, x.g);
+    if (rest16) ld8(s.rest16 + (size_t)(r - SC_ROW_REST) * s.cap + i0, x.p); else ld8(s.slab + pk, x.p);
+    if (mo.bf16) { ld8(mo.m16 + mk, x.m); ld8(mo.v16 + mk, x.v); } else { ld8(mo.m + mk, x.m); ld8(mo.v + mk, x.v); }
+    return;
+  }
+#pragma unroll
+  for (int e = 0; e < ADAM_SPT; ++e) {
+    x.g[e] = x.p[e] = x.m[e] = x.v[e] = 0.0f;
+    if (e < nv) {
+      x.g[e] = g[gk + e];
+      x.p[e] = sp_row(s, r, i0 + e);
+      x.m[e] = mo_ld(mo, mo.m, mo.m16, mk + e);
+      x.v[e] = mo_ld(mo, mo.v, mo.v16, mk + e);
+    }
+  }
+}
+__device__ __forceinline__ void store_row8(const DSplats& s, const DMoments& mo, int r, uint32_t i0, int nv,
+                                           const Row8& x) {
+  const size_t pk = (size_t)r * s.cap + i0, mk = (size_t)r * mo.cap + i0;
+  const bool rest16 = r >= SC_ROW_REST && s.bf16;
+  if (nv == ADAM_SPT) {
+    if (rest16) st8(s.rest16 + (size_t)(r - SC_ROW_REST) * s.cap + i0, x.p); else st8(s.slab + pk, x.p);
+    if (mo.bf16) { st8(mo.m16 + mk, x.m); st8(mo.v16 + mk, x.v); } else { st8(mo.m + mk, x.m); st8(mo.v + mk, x.v); }
+    return;
+  }
+#pragma unroll
+  for (int e = 0; e < ADAM_SPT; ++e) {
+    if (e < nv) {
+      sp_set(s, r, i0 + e, x.p[e]);
+      mo_st(mo, mo.m, mo.m16, mk + e, x.m[e]);
+      mo_st(mo, mo.v, mo.v16, mk + e, x.v[e]);
+    }
+  }
+}
+// adam_scalar_fast on a row of 8
+__device__ __forceinline__ void adam_row8(Row8& x, float a, float s2, const AdamParams& ap) {
+#pragma unroll
+  for (int e = 0; e < ADAM_SPT; ++e) {
+    const float gr = x.g[e];
+    const float m = ap.beta1 * x.m[e] + (1.0f - ap.beta1) * gr;
+    const float v = ap.beta2 * x.v[e] + (1.0f - ap.beta2) * gr * gr;
+    x.m[e] = m;
+    x.v[e] = v;
+    x.p[e] = x.p[e] - __fdividef(a * m, fmaf(sqrtf(v), s2, ap.eps));
+  }
+}
+
+__global__ void __launch_bounds__(256) k_adam_rows(DSplats s, DMoments mo, float* __restrict__ acc,
+                                                   const float* __restrict__ g, uint32_t lo, uint32_t count,
+                                                   uint32_t gstride, AdamParams ap, const float* __restrict__ d_bc,
+                                                   const uint32_t* __restrict__ skip) {
+  const uint32_t j0 = (blockIdx.x * blockDim.x + threadIdx.x) * ADAM_SPT;
+  if (j0 >= count) return;
+  if (skip && (*skip & SC_DEVERR_CAPACITY)) return;  // a capacity overflow earlier in the step: leave parameters untouched
+  if (d_bc) { ap.bc1 = d_bc[0]; ap.bc2 = d_bc[1]; }
+  const AdamFast af = adam_fast(ap);
+  const int nv = (int)min((uint32_t)ADAM_SPT, count - j0);
+  const uint32_t i0 = lo + j0;
+  const int y = blockIdx.y;
+  Row8 x;
+  if (y == 0) {  // position, and the densify statistic (accumulate_grad_pos.wgsl:17-23) from its gradients
+    float st[ADAM_SPT];  // ((acc + |g0|) + |g1|) + |g2|, as the per-splat kernels add
+#pragma unroll
+    for (int e = 0; e < ADAM_SPT; ++e) st[e] = (acc && e < nv) ? acc[i0 + e] : 0.0f;
+    for (int r = 0; r < 3; ++r) {
+      load_row8(s, mo, g, r, i0, j0, gstride, nv, x);
+#pragma unroll
+      for (int e = 0; e < ADAM_SPT; ++e) st[e] = st[e] + fabsf(x.g[e]);
+      adam_row8(x, af.a[0], af.s2, ap);
+      store_row8(s, mo, r, i0, nv, x);
+    }
+    if (acc) {
+#pragma unroll
+      for (int e = 0; e < ADAM_SPT; ++e)
+        if (e < nv) acc[i0 + e] = st[e];
+    }
+    return;
+  }
+  if (y == 1) {  // rotation: update the four rows, then normalise each splat's quaternion from them
+    for (int c = 0; c < 4; ++c) {
+      load_row8(s, mo, g, SC_ROW_ROT + c, i0, j0, gstride, nv, x);
+      adam_row8(x, af.a[1], af.s2, ap);
+      store_row8(s, mo, SC_ROW_ROT + c, i0, nv, x);
+    }
+    float q[4][ADAM_SPT];
+    for (int c = 0; c < 4; ++c) {
+      const float* row = s.slab + (size_t)(SC_ROW_ROT + c) * s.cap + i0;
+      if (nv == ADAM_SPT) {
+        ld8(row, q[c]);
+      } else {
+#pragma unroll
+        for (int e = 0; e < ADAM_SPT; ++e) q[c][e] = e < nv ? row[e] : 1.0f;
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < ADAM_SPT; ++e) {
+      const float n2 = q[0][e] * q[0][e] + q[1][e] * q[1][e] + q[2][e] * q[2][e] + q[3][e] * q[3][e];
+      const float nrm = fmaxf(sqrtf(n2), 1e-8f);
+      for (int c = 0; c < 4; ++c) q[c][e] /= nrm;
+    }
+    for (int c = 0; c < 4; ++c) {
+      float* row = s.slab + (size_t)(SC_ROW_ROT + c) * s.cap + i0;
+      if (nv == ADAM_SPT) {
+        st8(row, q[c]);
+      } else {
+#pragma unroll
+        for (int e = 0; e < ADAM_SPT; ++e)
+          if (e < nv) row[e] = q[c][e];
+      }
+    }
+    return;
+  }
+  // single rows: 7..9 log scale, 10 opacity, 11..13 sh_dc, 14.. sh_rest
+  const int r = y <= 8 ? y + 5 : SC_ROW_REST + (y - 9);
+  load_row8(s, mo, g, r, i0, j0, gstride, nv, x);
+  adam_row8(x, af.a[adam_group(r)], af.s2, ap);
+  if (r >= SC_ROW_SCALE && r < SC_ROW_SCALE + 3) {
+#pragma unroll
+    for (int e = 0; e < ADAM_SPT; ++e) x.p[e] = fminf(fmaxf(x.p[e], ap.log_scale_min), ap.log_scale_max);
+  } else if (r == SC_ROW_OP) {
+#pragma unroll
+    for (int e = 0; e < ADAM_SPT; ++e) x.p[e] = fminf(fmaxf(x.p[e], -ap.opacity_logit_max), ap.opacity_logit_max);
+  }
+  store_row8(s, mo, r, i0, nv, x);
+}
+
+sc_status launch_adam_rows(sc_ctx* ctx, const DSplats& s, const DMoments& mo, float* acc, const float* g, uint32_t lo,
+                           uint32_t count, uint32_t gstride, const AdamParams& ap, const float* d_bc,
+                           const uint32_t* d_skip) {
+  if (count == 0) return SC_OK;
+  if (lo % ADAM_SPT || gstride % ADAM_SPT || s.cap % ADAM_SPT || mo.cap % ADAM_SPT)
+    return sc_fail(ctx, SC_ERR_INVALID_ARG, "Adam rows: offsets and strides must be multiples of 8");
+  const dim3 grid((unsigned)sc_div_up(sc_div_up(count, ADAM_SPT), 256), ADAM_GROUPS);
+  k_adam_rows<<<grid, 256, 0, ctx->stream>>>(s, mo, acc, g, lo, count, gstride, ap, d_bc, d_skip);
+  return sc_check_launch(ctx, "k_adam_rows");
+}
+
+// ---------------------------------------------------------------- data-parallel shards
+// Adam + constraints + densify statistic on one reduce-scattered chunk
+// g[r * shard + j] for splats [lo, lo+count): the streaming row kernel.
 sc_status launch_adam_shard(sc_ctx* ctx, const DSplats& s, const DMoments& mo, float* acc, const float* g, uint32_t lo,
                             uint32_t count, uint32_t shard, const AdamParams& ap) {
-  if (count == 0) return SC_OK;
-  k_adam_shard<<<(unsigned)sc_div_up(count, 256), 256, 0, ctx->stream>>>(s, mo, acc, g, lo, count, shard, ap);
-  return sc_check_launch(ctx, "k_adam_shard");
+  return launch_adam_rows(ctx, s, mo, acc, g, lo, count, shard, ap, nullptr, nullptr);
 }
 
 // grid.y = row

@@ -2,12 +2,14 @@
 //
 // Forward (rasterize.wgsl:48-118): one CTA per (view, tile); each thread owns
 // PPT vertically adjacent pixels (a warp covers a compact tile_w x (32/tile_w*PPT)
-// block).  The tile's depth-sorted records are staged into shared memory in
-// batches of blockDim records with cp.async (3 x 16 B per record), double
-// buffered so the gather of batch b+1 overlaps the blending of batch b, and
-// the CTA leaves as soon as every pixel is saturated (T < 1e-4).  The MSE of
-// loss.rs:163-179 is fused into the epilogue: dL/dC = scale * 2 (C - target)
-// / (3 W H) per pixel, squared errors reduced per CTA in FP64.
+// block), two of them in packed f32x2 arithmetic.  The tile's depth-ordered
+// list — its own pair list, or its super tile's item list filtered by the
+// member masks — is staged into shared memory in batches of blockDim list
+// positions with cp.async (3 x 16 B per record), double buffered so the gather
+// of batch b+1 overlaps the blending of batch b, and the CTA leaves as soon as
+// every pixel is saturated (T < 1e-4).  The MSE of loss.rs:163-179 — dL/dC =
+// scale * 2 (C - target) / (3 W H) per pixel, squared errors reduced per CTA
+// in FP64 — runs in the forward's epilogue or in the backward's prologue.
 //
 // Backward (rasterize_backward.wgsl:73-210): same grid, reverse walk.  Per
 // (pixel, splat) gradients (dmean.xy, dopacity, dconic.abc, dcolor.rgb) are

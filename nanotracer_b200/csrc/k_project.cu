@@ -9,11 +9,13 @@
 //
 // Backward: project_backward.wgsl:79-304, with the same omissions as the
 // reference (no dJ/dt in the position gradient, no SH view-direction
-// gradient, no colour-clamp gate).  The fused variant sums the per-view
-// gradients in registers and applies grad accumulation (accumulate_grad_pos.wgsl),
-// Adam (adam_step.wgsl / adam.rs:70-90) and the constraints
-// (apply_constraints.wgsl) in the same thread, so the 59 gradient rows never
-// touch HBM.
+// gradient, no colour-clamp gate).  One thread per splat sums the per-view
+// gradients in registers and writes the splat's 59 gradient rows once
+// (coefficient-major, cut into shards for the data-parallel path); Adam then
+// streams over those rows (k_adam.cu).  A single kernel doing both held 59
+// gradients and the Adam state of one splat per thread at 128 registers and
+// waited on memory; the split moves 2 x 236 bytes more per splat and ran the
+// pair in 0.49 ms instead of 0.83 ms at 1M splats and 8 views.
 #include "sc_internal.cuh"
 
 namespace sck {
@@ -428,42 +430,7 @@ __device__ __forceinline__ void sum_view_grads(const DSplats& s, uint32_t i, con
   }
 }
 
-// ---------------------------------------------------------------- fused backward + Adam
-__global__ void __launch_bounds__(128, 4) k_fused_backward_adam(DSplats s, DMoments mo, const float4* __restrict__ pg,
-                                                             uint32_t stride, const sc_camera* __restrict__ cams,
-                                                             uint32_t n_views, float* __restrict__ grad_acc,
-                                                             AdamParams ap, const uint32_t* __restrict__ skip,
-                                                             const float* __restrict__ d_bc) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= s.n) return;
-  if (skip && (*skip & SC_DEVERR_CAPACITY)) return;  // a capacity overflow earlier in the step: leave parameters untouched
-  if (d_bc) { ap.bc1 = d_bc[0]; ap.bc2 = d_bc[1]; }
-  SplatGrads G;
-  sum_view_grads(s, i, pg, stride, cams, n_views, G);
-  // densify statistic, accumulate_grad_pos.wgsl:17-23 (before the step, train.rs:228)
-  if (grad_acc) grad_acc[i] = grad_acc[i] + fabsf(G.gpos[0]) + fabsf(G.gpos[1]) + fabsf(G.gpos[2]);
-  const size_t cap = s.cap;
-  // geometric rows
-  const float gg[14] = {G.gpos[0], G.gpos[1], G.gpos[2], G.grot[0], G.grot[1], G.grot[2], G.grot[3],
-                        G.gsc[0],  G.gsc[1],  G.gsc[2],  G.gop,     G.gdc[0],  G.gdc[1],  G.gdc[2]};
-  const AdamFast af = adam_fast(ap);
-  float np[14];
-#pragma unroll
-  for (int r = 0; r < 14; ++r)
-    np[r] = adam_scalar_fast(mo, (size_t)r * mo.cap + i, s.slab[(size_t)r * cap + i], gg[r], af.a[adam_group(r)],
-                             af.s2, ap);
-  constrain_geometry(np, ap);
-#pragma unroll
-  for (int r = 0; r < 14; ++r) s.slab[(size_t)r * cap + i] = np[r];
-#pragma unroll
-  for (int k = 0; k < 45; ++k) {
-    const int r = SC_ROW_REST + k;
-    const float p = sp_row(s, r, i);
-    sp_set(s, r, i, adam_scalar_fast(mo, (size_t)r * mo.cap + i, p, G.grest[k], af.a[5], af.s2, ap));
-  }
-}
-
-// ---------------------------------------------------------------- data-parallel views
+// ---------------------------------------------------------------- per-splat gradient rows
 __global__ void __launch_bounds__(128, 4) k_project_backward_shards(DSplats s, const float4* __restrict__ pg,
                                                                  uint32_t stride, const sc_camera* __restrict__ cams,
                                                                  uint32_t n_views, float* __restrict__ out,
@@ -498,15 +465,6 @@ sc_status launch_project_backward_shards(sc_ctx* ctx, const DSplats& s, const fl
   k_project_backward_shards<<<(unsigned)sc_div_up(total, 128), 128, 0, ctx->stream>>>(s, pg, stride, d_cams, n_views,
                                                                                       grads, n_shards, shard, d_skip);
   return sc_check_launch(ctx, "k_project_backward_shards");
-}
-
-sc_status launch_fused_backward_adam(sc_ctx* ctx, const DSplats& s, const DMoments& mo, const float4* pg,
-                                     uint32_t stride, const sc_camera* d_cams, uint32_t n_views, float* grad_acc,
-                                     const AdamParams& ap, const uint32_t* d_skip, const float* d_bc) {
-  if (s.n == 0) return SC_OK;
-  k_fused_backward_adam<<<(unsigned)sc_div_up(s.n, 128), 128, 0, ctx->stream>>>(s, mo, pg, stride, d_cams, n_views,
-                                                                                 grad_acc, ap, d_skip, d_bc);
-  return sc_check_launch(ctx, "k_fused_backward_adam");
 }
 
 }  // namespace sck

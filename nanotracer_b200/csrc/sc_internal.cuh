@@ -254,15 +254,12 @@ sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams,
 sc_status launch_project_backward(sc_ctx* ctx, const DSplats& s, const float4* proj_grad, const sc_camera* d_cam,
                                   float* grads, uint32_t gcap, int accumulate);
 
-// fused multi-view project backward + grad accumulation + Adam + constraints
+// Adam hyper-parameters, clamp limits and bias corrections of one step
 struct AdamParams {
   float lr[6];
   float beta1, beta2, eps, bc1, bc2;
   float log_scale_min, log_scale_max, opacity_logit_max;
 };
-sc_status launch_fused_backward_adam(sc_ctx* ctx, const DSplats& s, const DMoments& mo, const float4* proj_grad,
-                                     uint32_t stride, const sc_camera* d_cams, uint32_t n_views, float* grad_acc,
-                                     const AdamParams& ap, const uint32_t* d_skip_flag, const float* d_bc);
 
 // moments widened to / rounded from f32
 __device__ __forceinline__ float mo_ld(const DMoments& mo, const float* f, const __nv_bfloat16* h, size_t k) {
@@ -324,6 +321,12 @@ sc_status launch_project_backward_shards(sc_ctx* ctx, const DSplats& s, const fl
                                          uint32_t shard, const uint32_t* d_skip_flag);
 // Adam + constraints + densify statistic for splats [lo, lo+count) from one
 // reduce-scattered chunk g[r * shard + j]
+// Adam + constraints + densify statistic over splats [lo, lo+count) from
+// gradient rows g[r * gstride + j] (lo, gstride multiples of 8), streaming
+// 8 splats of one row group per thread; bias corrections from d_bc when given
+sc_status launch_adam_rows(sc_ctx* ctx, const DSplats& s, const DMoments& mo, float* grad_acc, const float* g,
+                           uint32_t lo, uint32_t count, uint32_t gstride, const AdamParams& ap, const float* d_bc,
+                           const uint32_t* d_skip_flag);
 sc_status launch_adam_shard(sc_ctx* ctx, const DSplats& s, const DMoments& mo, float* grad_acc, const float* g,
                             uint32_t lo, uint32_t count, uint32_t shard, const AdamParams& ap);
 // parameters / moments of [lo, lo+count) as f32 rows out[r * shard + j], and back

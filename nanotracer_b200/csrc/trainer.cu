@@ -1,20 +1,23 @@
 // trainer.cu — the batched training iteration (train.rs:155-250 for n_views
 // views per step) as one stream of kernels, replayed as a CUDA graph.
 //
-//   H2D step params (cameras, Adam bias corrections)       memcpy node
+//   H2D step params (cameras, Adam bias corrections)         memcpy node
 //   project + SH for all views, per-view depth keys, counts  k_project
 //   per-view depth sort of the splats                        onesweep u64 (view<<32 | depth bits)
-//   tile counts in depth order -> offsets                    gather + decoupled-look-back scan
-//   pair emission (view*T + tile, splat)                     warp-cooperative emit
-//   stable tile sort of the pairs                            onesweep u32 (ceil(log2(V*T)) bits)
-//   per-tile ranges                                          k_tile_ranges
-//   alpha-blend forward + fused MSE dL/dC                    k_composite
-//   alpha-blend backward (exact or reference transmittance) k_composite_backward
-//   project backward over all views + grad acc + Adam + constraints   k_fused_backward_adam
-//   loss / pair count / error word -> pinned host           finalize + memcpy node
+//   item counts in depth order -> offsets                    gather + decoupled-look-back scan
+//   items (mask | view, super tile; splat) in depth order    k_super_emit (two-level binning)
+//   stable sort of the items by super tile                   onesweep u32 (super tile bits)
+//   per-super-tile ranges (+ pair count from the masks)      k_tile_ranges
+//   alpha-blend forward over the super-tile item lists       k_composite (item lists)
+//   alpha-blend backward, MSE dL/dC in its prologue          k_composite_backward (item lists)
+//   project backward over all views -> gradient rows         k_project_backward_shards (one shard)
+//   Adam + constraints + densify statistic over the rows     k_adam_rows
+//   loss / pair count / error word -> pinned host            finalize + memcpy node
+// (sort_mode 1 keeps the pair path: emission of (view*T + tile, splat) pairs,
+// their stable tile sort, per-tile ranges and pair-list blends.)
 //
-// The pair buffers have a device-side capacity.  When a step emits more pairs
-// than fit, the emit kernel raises SC_DEVERR_CAPACITY, the blend and Adam
+// The item (or pair) buffers have a device-side capacity.  When a step emits
+// more than fit, the emit kernel raises SC_DEVERR_CAPACITY, the blend and Adam
 // kernels of that step skip their work (parameters are untouched), and the host
 // grows the buffers and runs the step again.
 #include "sc_internal.cuh"
@@ -24,6 +27,7 @@
 #include <cstring>
 #include <string>
 #include <vector>
+
 
 namespace {
 
@@ -85,6 +89,8 @@ struct sc_trainer {
   StepOut* d_out = nullptr;
   // per (view, splat)
   float4* rec = nullptr; float4* pgrad = nullptr;
+  float* grads = nullptr;  // [SC_NROWS][grad_stride] per-splat gradient rows (one GPU)
+  uint32_t grad_stride = 0;
   uint64_t* dkeys = nullptr; uint64_t* dkeys_tmp = nullptr;
   uint32_t* ids = nullptr; uint32_t* ids_tmp = nullptr;
   uint32_t* counts_by_id = nullptr; uint32_t* counts = nullptr;
@@ -139,7 +145,7 @@ struct sc_trainer {
 };
 
 static void trainer_free_splat_arrays(sc_trainer* tr) {
-  cudaFree(tr->rec); cudaFree(tr->pgrad); cudaFree(tr->dkeys); cudaFree(tr->dkeys_tmp);
+  cudaFree(tr->rec); cudaFree(tr->pgrad); cudaFree(tr->grads); cudaFree(tr->dkeys); cudaFree(tr->dkeys_tmp);
   cudaFree(tr->ids); cudaFree(tr->ids_tmp); cudaFree(tr->counts_by_id); cudaFree(tr->counts);
   tr->rec = tr->pgrad = nullptr; tr->dkeys = tr->dkeys_tmp = nullptr;
   tr->ids = tr->ids_tmp = tr->counts_by_id = tr->counts = nullptr;
@@ -188,6 +194,8 @@ static sc_status ensure_splat_arrays(sc_trainer* tr, uint32_t cap) {
   const size_t nv = (size_t)tr->V * cap;
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->rec, nv * 48), "rec");
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->pgrad, nv * 48), "pgrad");
+  tr->grad_stride = (cap + 63u) & ~63u;
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->grads, (size_t)SC_NROWS * tr->grad_stride * 4), "grads");
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->dkeys, nv * 8), "dkeys");
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->dkeys_tmp, nv * 8), "dkeys");
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->ids, nv * 4), "ids");
@@ -385,8 +393,12 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   if (tr->grads_mode)
     SC_TRY(sck::launch_project_backward_shards(ctx, ds, tr->pgrad, tr->stride, d_cams, V, tr->gout, tr->g_shards,
                                                tr->g_shard, ctx->d_error));
-  else
-    SC_TRY(sck::launch_fused_backward_adam(ctx, ds, dm, tr->pgrad, tr->stride, d_cams, V, acc, ap, ctx->d_error, d_bc));
+  else {
+    // per-splat gradient rows summed over the views, then Adam streamed over the rows
+    SC_TRY(sck::launch_project_backward_shards(ctx, ds, tr->pgrad, tr->stride, d_cams, V, tr->grads, 1,
+                                               tr->grad_stride, ctx->d_error));
+    SC_TRY(sck::launch_adam_rows(ctx, ds, dm, acc, tr->grads, 0, ds.n, tr->grad_stride, ap, d_bc, ctx->d_error));
+  }
   mark(tr, 9, capturing);
   k_finalize<<<1, 1, 0, ctx->stream>>>(tr->d_loss, lam > 0.0f ? tr->d_ssim : nullptr, lam, V,
                                        1.0 / (3.0 * (double)tr->P), tr->grads_mode ? (double)tr->loss_weight : 0.0,
@@ -521,7 +533,7 @@ sc_status sc_trainer_set_profiling(sc_trainer* tr, int enabled) {
 
 }  // extern "C"
 
-// Run one step (fused or gradient-only, per tr->grads_mode) with the step
+// Run one step (full, or gradient-only per tr->grads_mode) with the step
 // parameters already in pinned memory: graph capture/replay, capacity retry.
 static sc_status run_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, float* acc, double* loss_out) {
   sc_ctx* ctx = tr->ctx;

@@ -2,7 +2,7 @@
 (crates/nano-optimize/src/train.rs:37-401) on the batched device trainer.
 
 Trainer wraps sc_trainer: one step = n_views views (project -> bin -> blend
--> fused MSE -> backward -> project backward summed over views -> grad
+-> MSE dL/dC -> backward -> project backward summed over views -> grad
 accumulation -> Adam -> constraints) replayed as one CUDA graph.  train()
 adds the reference's schedule around it: prune every 100 iterations after 50,
 densify every 200 after 100 (train.rs:103-114, 259-362), both on the device.
