@@ -266,7 +266,9 @@ def run_ours(args):
         "item_ranges": items * 4,
         "blend_fwd": fwd_list + V * P * (16 + 8),
         "blend_bwd": bwd_list + V * P * (16 + 8 + 12) + V * N * 48,
-        "bwd_adam": N * (56 + rest_b + 2 * rest_b) + V * N * 48 + N * (mom_b * 2) + N * 8,
+        # projection backward: per-view gradient records + geometry in, 59 f32 gradient
+        # rows out; streaming Adam: rows, parameters, moments and statistic in and out
+        "bwd_adam": V * N * 48 + N * 44 + N * 236 + N * 236 + N * 2 * (56 + rest_b) + N * 2 * mom_b + N * 8,
     }
     peaks = load_peaks()
     dom_ms = stage[dom]

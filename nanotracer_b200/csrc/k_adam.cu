@@ -205,7 +205,10 @@ __device__ __forceinline__ void adam_row8(Row8& x, float a, float s2, const Adam
   }
 }
 
-__global__ void __launch_bounds__(256) k_adam_rows(DSplats s, DMoments mo, float* __restrict__ acc,
+// GEOM: the 9 geometric row groups (grid.y 0..8); otherwise the 45 sh_rest
+// rows (grid.y 0..44), a separate launch with its own, smaller register count
+template <bool GEOM>
+__global__ void __launch_bounds__(256, GEOM ? 1 : 4) k_adam_rows(DSplats s, DMoments mo, float* __restrict__ acc,
                                                    const float* __restrict__ g, uint32_t lo, uint32_t count,
                                                    uint32_t gstride, AdamParams ap, const float* __restrict__ d_bc,
                                                    const uint32_t* __restrict__ skip) {
@@ -216,9 +219,9 @@ __global__ void __launch_bounds__(256) k_adam_rows(DSplats s, DMoments mo, float
   const AdamFast af = adam_fast(ap);
   const int nv = (int)min((uint32_t)ADAM_SPT, count - j0);
   const uint32_t i0 = lo + j0;
-  const int y = blockIdx.y;
+  const int y = GEOM ? (int)blockIdx.y : 9 + (int)blockIdx.y;
   Row8 x;
-  if (y == 0) {  // position, and the densify statistic (accumulate_grad_pos.wgsl:17-23) from its gradients
+  if (GEOM && y == 0) {  // position, and the densify statistic (accumulate_grad_pos.wgsl:17-23) from its gradients
     float st[ADAM_SPT];  // ((acc + |g0|) + |g1|) + |g2|, as the per-splat kernels add
 #pragma unroll
     for (int e = 0; e < ADAM_SPT; ++e) st[e] = (acc && e < nv) ? acc[i0 + e] : 0.0f;
@@ -236,7 +239,7 @@ __global__ void __launch_bounds__(256) k_adam_rows(DSplats s, DMoments mo, float
     }
     return;
   }
-  if (y == 1) {  // rotation: update the four rows, then normalise each splat's quaternion from them
+  if (GEOM && y == 1) {  // rotation: update the four rows, then normalise each splat's quaternion from them
     for (int c = 0; c < 4; ++c) {
       load_row8(s, mo, g, SC_ROW_ROT + c, i0, j0, gstride, nv, x);
       adam_row8(x, af.a[1], af.s2, ap);
@@ -290,8 +293,11 @@ sc_status launch_adam_rows(sc_ctx* ctx, const DSplats& s, const DMoments& mo, fl
   if (count == 0) return SC_OK;
   if (lo % ADAM_SPT || gstride % ADAM_SPT || s.cap % ADAM_SPT || mo.cap % ADAM_SPT)
     return sc_fail(ctx, SC_ERR_INVALID_ARG, "Adam rows: offsets and strides must be multiples of 8");
-  const dim3 grid((unsigned)sc_div_up(sc_div_up(count, ADAM_SPT), 256), ADAM_GROUPS);
-  k_adam_rows<<<grid, 256, 0, ctx->stream>>>(s, mo, acc, g, lo, count, gstride, ap, d_bc, d_skip);
+  const unsigned gx = (unsigned)sc_div_up(sc_div_up(count, ADAM_SPT), 256);
+  k_adam_rows<true><<<dim3(gx, 9), 256, 0, ctx->stream>>>(s, mo, acc, g, lo, count, gstride, ap, d_bc, d_skip);
+  SC_TRY(sc_check_launch(ctx, "k_adam_rows"));
+  k_adam_rows<false><<<dim3(gx, ADAM_GROUPS - 9), 256, 0, ctx->stream>>>(s, mo, acc, g, lo, count, gstride, ap, d_bc,
+                                                                          d_skip);
   return sc_check_launch(ctx, "k_adam_rows");
 }
 
