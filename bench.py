@@ -36,6 +36,18 @@ UNIT = "iters/s"
 PEAKS = {"hbm_gbs": 6537.6, "bf16_tflops": 1654.7, "source": "measured"}
 
 
+def profiled_traffic(kernel: str, views: int):
+    """DRAM bytes per launch of a stage's dominant kernel from the committed ncu
+    summaries (a line `traffic: kernel=<stage> views=<v> dram_bytes=<bytes>` of
+    one capture), scaled from the captured views to `views`; None without one."""
+    import re
+    for f in sorted((ROOT / "profiles").glob("*.md")):
+        m = re.search(r"traffic: kernel=(\w+) views=(\d+) dram_bytes=(\d+)", f.read_text())
+        if m and m.group(1) == kernel:
+            return int(int(m.group(3)) * views / int(m.group(2)))
+    return None
+
+
 def load_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -274,7 +286,8 @@ def run_ours(args):
     dom_ms = stage[dom]
     achieved = algo[dom] / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"],
-                "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": None,
+                "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4),
+                "traffic": profiled_traffic(dom, V),
                 "peak_source": peaks["source"], "algorithmic_bytes": int(algo[dom]), "avg_ms": round(dom_ms, 4),
                 "stage_ms": {k: round(v, 4) for k, v in stage.items()}, "blend_work": bw}
 
