@@ -255,8 +255,11 @@ def test_sort_random_u32_with_payload(ctx):
     assert np.array_equal(sv, order)
 
 
+# 9 bits: one 9-bit pass; the others 8-bit passes, with a narrower last digit
+# for 7, 13, 17, 26, 35 and 44 bits
 @pytest.mark.parametrize("n,bits,key_bytes", [(1, 8, 4), (4097, 13, 4), (3_000_001, 16, 4), (2_500_003, 35, 8),
-                                              (1_000_000, 64, 8), (777_777, 7, 8)])
+                                              (1_000_000, 64, 8), (777_777, 7, 8), (2_000_003, 9, 4),
+                                              (1_000_001, 17, 4), (999_999, 26, 4), (500_001, 44, 8)])
 def test_sort_stable_vs_numpy(ctx, n, bits, key_bytes):
     rng = np.random.default_rng(n + bits)
     dt = np.uint32 if key_bytes == 4 else np.uint64
@@ -414,13 +417,16 @@ def test_tonemap_headless_buffer(ctx):
     assert np.abs(px.astype(int) - want.astype(int)).max() <= 1
 
 
-def test_sort_on_low_key_bits_keeps_high_bits_in_input_order(ctx):
+@pytest.mark.parametrize("bits,extent", [(13, 8160), (9, 510)])
+def test_sort_on_low_key_bits_keeps_high_bits_in_input_order(ctx, bits, extent):
     """key_bits below the key width: ordered by the low bits only, stable, the
-    high bits carried along (the trainer's (view << tile_bits) | tile keys)."""
-    rng = np.random.default_rng(11)
+    high bits carried along (the trainer's (view << tile_bits) | tile pair keys,
+    and its items: member mask and view above the 9 super-tile bits)."""
+    rng = np.random.default_rng(11 + bits)
     n = 300_001
-    keys = ((rng.integers(0, 8, n, dtype=np.uint64) << 13) | rng.integers(0, 8160, n, dtype=np.uint64)).astype(np.uint32)
+    keys = ((rng.integers(0, 1 << (32 - bits), n, dtype=np.uint64) << bits) |
+            rng.integers(0, extent, n, dtype=np.uint64)).astype(np.uint32)
     vals = np.arange(n, dtype=np.uint32)
-    sk, sv = _sort_gpu(ctx, keys, vals, 13, 4)
-    order = np.argsort(keys & 0x1FFF, kind="stable")
+    sk, sv = _sort_gpu(ctx, keys, vals, bits, 4)
+    order = np.argsort(keys & ((1 << bits) - 1), kind="stable")
     assert np.array_equal(sv, order.astype(np.uint32)) and np.array_equal(sk, keys[order])
