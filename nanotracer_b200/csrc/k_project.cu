@@ -4,8 +4,10 @@
 // Sigma2D + 0.3 I low-pass, 3-sigma radius, frustum cull, order-3 SH,
 // sigmoid opacity).  The 2D covariance is formed as B B^T with
 // B = J W R diag(sigma) (2x3), which is algebraically the reference's
-// J (W R S^2 R^T W^T) J^T with fewer operations.  One thread per splat loops
-// over all views, so the 236 bytes of parameters are read once per step.
+// J (W R S^2 R^T W^T) J^T with fewer operations.  One thread per (splat,
+// view), the view on the grid's y axis: 70 registers instead of the 128 of a
+// thread looping over the views (0.58 against 0.67 ms at 1M splats and 8
+// views); a splat's parameters are read from L2 by its views after the first.
 //
 // Backward: project_backward.wgsl:79-304, with the same omissions as the
 // reference (no dJ/dt in the position gradient, no SH view-direction
@@ -171,11 +173,16 @@ __device__ __forceinline__ bool tile_rect(float mx, float my, float r, float vis
 // reached) instead of (tile, splat) pairs
 struct TileArgs { uint32_t tw, th, tiles_x, tiles_y, cull, super; };
 
-__global__ void __launch_bounds__(128, 4) k_project(DSplats s, const sc_camera* __restrict__ cams, uint32_t n_views,
+// One thread per (splat, view), the view being blockIdx.y: every view plane of
+// the outputs is written with coalesced stores, and the views of a splat read
+// its parameters from L2 (the per-view work — rotation, scales, SH — does not
+// share between views anyway).
+__global__ void __launch_bounds__(128) k_project(DSplats s, const sc_camera* __restrict__ cams, uint32_t n_views,
                                                  uint32_t stride, float4* __restrict__ rec, TileArgs ta,
                                                  uint64_t* __restrict__ depth_keys, uint32_t* __restrict__ ids,
                                                  uint32_t* __restrict__ counts, int precise) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t v = blockIdx.y;
   if (i >= stride) return;
   const bool live = i < s.n;
   float px = 0, py = 0, pz = 0, qw = 1, qx = 0, qy = 0, qz = 0, l0 = 0, l1 = 0, l2 = 0, op = 0, d0 = 0, d1 = 0, d2 = 0;
@@ -187,7 +194,7 @@ __global__ void __launch_bounds__(128, 4) k_project(DSplats s, const sc_camera* 
     d0 = sp_row(s, 11, i); d1 = sp_row(s, 12, i); d2 = sp_row(s, 13, i);
   }
   const float opacity = 1.0f / (1.0f + expf(-op));
-  for (uint32_t v = 0; v < n_views; ++v) {
+  {
     float4 ra = make_float4(0, 0, 0, 0), rb = ra, rc = ra;
     uint32_t key = 0xFFFFFFFFu, cnt = 0;  // splats that emit no pair sort after every emitting one
     if (live) {
@@ -259,9 +266,10 @@ sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams,
   TileArgs ta{1, 1, 1, 1, 0, 0};
   if (tl) ta = TileArgs{tl->tile_w, tl->tile_h, (tl->width + tl->tile_w - 1) / tl->tile_w,
                         (tl->height + tl->tile_h - 1) / tl->tile_h, (cull & 1) ? 1u : 0u, (cull & 2) ? 1u : 0u};
-  const uint32_t bs = 128;
-  k_project<<<(unsigned)sc_div_up(stride, bs), bs, 0, ctx->stream>>>(s, d_cams, n_views, stride, rec, ta, depth_keys,
-                                                                     ids, counts, precise);
+  const uint32_t bs = 128;  // grid: (splats / bs, views)
+  if (n_views > 65535) return sc_fail(ctx, SC_ERR_INVALID_ARG, "too many views");
+  k_project<<<dim3((unsigned)sc_div_up(stride, bs), n_views), bs, 0, ctx->stream>>>(s, d_cams, n_views, stride, rec,
+                                                                                   ta, depth_keys, ids, counts, precise);
   return sc_check_launch(ctx, "k_project");
 }
 
