@@ -698,13 +698,13 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
               const float2 dc = __ffma2_rn(gb2, f2(rc.z), __ffma2_rn(gg2, f2(rc.y), __fmul2_rn(gr2, f2(rc.x))));
               const float2 galpha = __fmul2_rn(inv, __ffma2_rn(T2, dc, make_float2(-GS2.x, -GS2.y)));
               const float2 h = __fmul2_rn(galpha, gm);
-              const float2 hx = __fmul2_rn(h, f2(e.dx)), hy = __fmul2_rn(h, dy);
+              const float2 hy = __fmul2_rn(h, dy);
               sh = h.x + h.y;
-              shx = hx.x + hx.y;
               shy = hy.x + hy.y;
-              shxx = shx * e.dx;  // both pixels share dx
-              shxy = fmaf(hx.x, dy.x, hx.y * dy.y);
               shyy = fmaf(hy.x, dy.x, hy.y * dy.y);
+              shx = sh * e.dx;  // both pixels share dx
+              shxx = shx * e.dx;
+              shxy = shy * e.dx;
               GS2 = __ffma2_rn(ta, dc, GS2);
               T2 = make_float2(v0 ? Tn.x : T2.x, v1 ? Tn.y : T2.y);
               contrib = true;
@@ -744,17 +744,8 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
         }
         if (MODE == SC_BWD_EXACT) all_done = false;
         if (__any_sync(FULL_MASK, contrib)) {
-          // dpower = op h; dconic = dpower (-1/2)(dx^2, 2 dx dy, dy^2);
-          // dmean = dpower (a dx + b dy, b dx + c dy)  (rasterize_backward.wgsl:174-185)
-          const float op = rc.w;
-          float c[9];
-          c[0] = op * (rb.x * shx + rb.y * shy);
-          c[1] = op * (rb.y * shx + rb.z * shy);
-          c[2] = sh;
-          c[3] = -0.5f * op * shxx;
-          c[4] = -op * shxy;
-          c[5] = -0.5f * op * shyy;
-          c[6] = scr; c[7] = scg; c[8] = scb;
+          // the splat's raw sums; the flush turns them into its gradients
+          const float c[9] = {shx, shy, sh, shxx, shxy, shyy, scr, scg, scb};
           int idx;
           const float w = warp_reduce_scatter9(c, lane, &idx);
           if (idx >= 0) atomicAdd(reinterpret_cast<float*>(sacc + 3 * k) + idx + idx / 3, w);
@@ -767,8 +758,17 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
     }
     __syncthreads();
     if (threadIdx.x < cnt) {
+      // the entry's sums over the CTA's pixels of h = dL/dalpha * gauss and its
+      // moments in (dx, dy) become, with the splat's opacity and conic (a, b, c)
+      // (rasterize_backward.wgsl:174-185): dpower = op h, dmean = dpower (a dx +
+      // b dy, b dx + c dy), dconic = dpower (-1/2)(dx^2, 2 dx dy, dy^2); the
+      // opacity and colour gradients are the sums themselves
       float4* acc = sacc + 3 * threadIdx.x;
-      const float4 a0 = acc[0], a1 = acc[1], a2 = acc[2];
+      const float4 m0 = acc[0], m1 = acc[1], a2 = acc[2];  // (SHX, SHY, SH), (SHXX, SHXY, SHYY), colour
+      const float4 cb = sb[3 * threadIdx.x + 1];
+      const float op = sb[3 * threadIdx.x + 2].w;
+      const float4 a0 = make_float4(op * (cb.x * m0.x + cb.y * m0.y), op * (cb.y * m0.x + cb.z * m0.y), m0.z, 0.0f);
+      const float4 a1 = make_float4(-0.5f * op * m1.x, -op * m1.y, -0.5f * op * m1.z, 0.0f);
       const uint32_t id = sids[(b & 1) * B + threadIdx.x];
       float4* dst = vgrad + (size_t)3 * id;
       if (a0.x != 0.f || a0.y != 0.f || a0.z != 0.f) atomicAdd(dst, a0);
