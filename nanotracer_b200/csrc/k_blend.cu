@@ -303,9 +303,12 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
       const float4* sb = sbuf + (size_t)(b & 1) * 3 * B;
       if constexpr (PPT == 2) {
         // both pixels in packed arithmetic; a pixel that skips the splat gets
-        // alpha 0, which leaves its colour and T bit for bit unchanged
-        float2 T2 = make_float2(T[0], T[1]), R2 = make_float2(cr[0], cr[1]);
-        float2 G2 = make_float2(cg[0], cg[1]), B2 = make_float2(cb[0], cb[1]);
+        // alpha 0, which leaves its colour and T bit for bit unchanged.  A
+        // pixel is done exactly when its T < 1e-4 (a pixel outside the image,
+        // never written, runs with T = 0).
+        const bool in0 = px < a.width && py0 < a.height, in1 = px < a.width && py0 + 1 < a.height;
+        float2 T2 = make_float2(in0 ? T[0] : 0.0f, in1 ? T[1] : 0.0f);
+        float2 R2 = make_float2(cr[0], cr[1]), G2 = make_float2(cg[0], cg[1]), B2 = make_float2(cb[0], cb[1]);
         const float2 fy2 = make_float2(fy[0], fy[1]);
         for (uint32_t k = 0; k < cnt; ++k) {
           const float4 ra = sb[3 * k], rb = sb[3 * k + 1], rc = sb[3 * k + 2];
@@ -313,8 +316,8 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
           float2 dy, g, araw, al;
           bool v0, v1;
           eval_alpha2(e, rb.z, fy2, ra.y, rc.w, dy, g, araw, al, v0, v1);
-          v0 &= !done[0];
-          v1 &= !done[1];
+          v0 &= T2.x >= 1e-4f;
+          v1 &= T2.y >= 1e-4f;
           if (v0 || v1) {
             const float2 am = make_float2(v0 ? al.x : 0.0f, v1 ? al.y : 0.0f);
             const float2 ta = __fmul2_rn(T2, am);
@@ -322,16 +325,14 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
             G2 = __ffma2_rn(ta, f2(rc.y), G2);
             B2 = __ffma2_rn(ta, f2(rc.z), B2);
             T2 = __fmul2_rn(T2, __fadd2_rn(f2(1.0f), make_float2(-am.x, -am.y)));
-            if (v0 || v1) {
-              const uint32_t pk = position(b, k) + 1;
-              if (v0) last[0] = pk;
-              if (v1) last[1] = pk;
-            }
-            done[0] |= T2.x < 1e-4f;
-            done[1] |= T2.y < 1e-4f;
-            if (done[0] && done[1]) break;
+            const uint32_t pk = position(b, k) + 1;
+            if (v0) last[0] = pk;
+            if (v1) last[1] = pk;
+            if (T2.x < 1e-4f && T2.y < 1e-4f) break;
           }
         }
+        done[0] = T2.x < 1e-4f;
+        done[1] = T2.y < 1e-4f;
         T[0] = T2.x; T[1] = T2.y; cr[0] = R2.x; cr[1] = R2.y;
         cg[0] = G2.x; cg[1] = G2.y; cb[0] = B2.x; cb[1] = B2.y;
         all_done = done[0] && done[1];
