@@ -751,7 +751,7 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
           const float w = warp_reduce_scatter9(c, lane, &idx);
           if (idx >= 0) atomicAdd(reinterpret_cast<float*>(sacc + 3 * k) + idx + idx / 3, w);
         }
-        if (__all_sync(FULL_MASK, all_done)) break;
+        if (MODE == SC_BWD_REF && __all_sync(FULL_MASK, all_done)) break;
       }
       if constexpr (PPT == 2) {
         T[0] = T2.x; T[1] = T2.y; GS[0] = GS2.x; GS[1] = GS2.y;
