@@ -356,10 +356,10 @@ __global__ void __launch_bounds__(EMIT_WARPS * 32) k_super_emit(
   if (jw >= total) return;
   const uint64_t j = jw + lane;
   const uint64_t jend = jw + 32 < total ? jw + 32 : total;
-  const uint64_t wlo = offsets[jw], whi = offsets[jend];
+  // item offsets are 32-bit (the scan of the counts), so is the chunk walk
+  const uint32_t wlo = offsets[jw], whi = offsets[jend];
   if (lane == 0 && whi > cap) atomicOr(err, SC_DEVERR_CAPACITY);
-  uint32_t cnt = 0, id = 0, vkey = 0;
-  uint64_t off = 0;
+  uint32_t cnt = 0, id = 0, vkey = 0, off = 0;
   int x0 = 0, y0 = 0, x1 = -1, y1 = -1;
   CullShape cs{};
   bool test = false;
@@ -379,14 +379,14 @@ __global__ void __launch_bounds__(EMIT_WARPS * 32) k_super_emit(
   }
   uint32_t* wk = sk[warp];
   uint32_t* wp = sp[warp];
-  for (uint64_t cb = wlo; cb < whi; cb += EMIT_WCHUNK) {
-    const uint64_t ce = cb + EMIT_WCHUNK < whi ? cb + EMIT_WCHUNK : whi;
+  for (uint32_t cb = wlo; cb < whi; cb += EMIT_WCHUNK) {
+    const uint32_t ce = min(cb + EMIT_WCHUNK, whi);
     if (cnt && off < ce && off + cnt > cb) {
       uint32_t w = 0;
       for_each_super_span(cs, test, x0, y0, x1, y1, a.tw, a.th,
                           [&](int sy, int sx0, int sx1, const int* rlo, const int* rhi) {
         for (int sx = sx0; sx <= sx1; ++sx, ++w) {
-          const uint64_t g = off + w;
+          const uint32_t g = off + w;
           if (w < cnt && g >= cb && g < ce) {
             wk[g - cb] = (super_mask_of(sx, rlo, rhi) << SUPER_MASK_SHIFT) | vkey |
                          ((uint32_t)sy * super_x + (uint32_t)sx);
@@ -395,14 +395,14 @@ __global__ void __launch_bounds__(EMIT_WARPS * 32) k_super_emit(
         }
       });
       for (; w < cnt; ++w) {  // count and emission disagreed: pad with a key that sorts last
-        const uint64_t g = off + w;
+        const uint32_t g = off + w;
         if (g >= cb && g < ce) { wk[g - cb] = 0xFFFFFFFFu; wp[g - cb] = 0; }
       }
     }
     __syncwarp();
-    const uint32_t n = (uint32_t)(ce - cb);
+    const uint32_t n = ce - cb;
     for (uint32_t t = lane; t < n; t += 32) {
-      const uint64_t g = cb + t;
+      const uint32_t g = cb + t;
       if (g < cap) {
         keys[g] = wk[t];
         payloads[g] = wp[t];

@@ -203,14 +203,15 @@ __device__ __forceinline__ void for_each_super_span(const CullShape& cs, bool te
 // member tiles of super column sx given the row spans: bit c * SC_SUPER + q
 // for tile (sx * SC_SUPER + q, row c)
 __device__ __forceinline__ uint32_t super_mask_of(int sx, const int* rlo, const int* rhi) {
+  // row c's tiles [rlo, rhi] (empty when rlo > rhi) cover columns [lo, hi] of
+  // super column sx: bits lo..hi of the row's nibble
   uint32_t m = 0;
+  const int base = sx * SC_SUPER;
 #pragma unroll
-  for (int c = 0; c < SC_SUPER; ++c)
-#pragma unroll
-    for (int q = 0; q < SC_SUPER; ++q) {
-      const int tx = sx * SC_SUPER + q;
-      if (tx >= rlo[c] && tx <= rhi[c]) m |= 1u << (c * SC_SUPER + q);
-    }
+  for (int c = 0; c < SC_SUPER; ++c) {
+    const int lo = max(rlo[c] - base, 0), hi = min(rhi[c] - base, SC_SUPER - 1);
+    if (hi >= lo) m |= ((2u << hi) - (1u << lo)) << (c * SC_SUPER);
+  }
   return m;
 }
 
