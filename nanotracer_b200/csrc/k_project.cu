@@ -179,7 +179,7 @@ struct TileArgs { uint32_t tw, th, tiles_x, tiles_y, cull, super; };
 // share between views anyway).
 __global__ void __launch_bounds__(128) k_project(DSplats s, const sc_camera* __restrict__ cams, uint32_t n_views,
                                                  uint32_t stride, float4* __restrict__ rec, TileArgs ta,
-                                                 uint64_t* __restrict__ depth_keys, uint32_t* __restrict__ ids,
+                                                 uint32_t* __restrict__ depth_keys, uint32_t* __restrict__ ids,
                                                  uint32_t* __restrict__ counts, int precise) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t v = blockIdx.y;
@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(128) k_project(DSplats s, const sc_camera* __r
     const size_t o = (size_t)v * stride + i;
     rec[3 * o + 0] = ra; rec[3 * o + 1] = rb; rec[3 * o + 2] = rc;
     if (depth_keys) {
-      depth_keys[o] = ((uint64_t)v << 32) | key;
+      depth_keys[o] = key;
       ids[o] = i;
       counts[o] = cnt;
     }
@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(128) k_project(DSplats s, const sc_camera* __r
 }
 
 sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams, uint32_t n_views, uint32_t stride,
-                         float4* rec, const sc_tiling* tl, uint64_t* depth_keys, uint32_t* ids, uint32_t* counts,
+                         float4* rec, const sc_tiling* tl, uint32_t* depth_keys, uint32_t* ids, uint32_t* counts,
                          int precise, int cull) {
   if (stride == 0 || n_views == 0) return SC_OK;
   TileArgs ta{1, 1, 1, 1, 0, 0};

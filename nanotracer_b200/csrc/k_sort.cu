@@ -571,6 +571,140 @@ sc_status radix_sort(sc_ctx* ctx, K* keys, uint32_t* vals, K* keys_tmp, uint32_t
                             result_in_tmp);
 }
 
+// ---------------------------------------------------------------- segmented sort
+// n_segs independent sorts of u32 keys (with u32 payloads), segment g holding
+// elements [g seg_len, (g + 1) seg_len), seg_len a multiple of the tile
+// (RS_SEG_TILE).  Every tile lies in one segment; the passes keep one digit
+// histogram per segment (its base includes the segment's offset) and a tile's
+// look-back stops at the first tile of its segment, so one launch per pass
+// sorts every segment.  The trainer sorts each view's depth keys this way: 32
+// bits in 4 passes instead of (view << 32 | depth) keys in 5.
+#define RS_SEG_TILE (RS_THREADS * 16)
+
+template <int RB>
+__global__ void __launch_bounds__(RS_THREADS) k_rs_hist_seg(const uint32_t* __restrict__ keys, uint32_t seg_len,
+                                                            uint32_t n_segs, int passes, uint32_t key_bits,
+                                                            uint32_t* __restrict__ hist /* [passes][n_segs][RADIX] */) {
+  constexpr int RADIX = Rdx<RB>::RADIX;
+  __shared__ uint32_t sh[4 * RADIX];
+  for (int t = threadIdx.x; t < passes * RADIX; t += RS_THREADS) sh[t] = 0;
+  __syncthreads();
+  const uint32_t g = blockIdx.y;
+  const uint32_t* k0 = keys + (size_t)g * seg_len;
+  for (uint32_t i = blockIdx.x * RS_THREADS + threadIdx.x; i < seg_len; i += gridDim.x * RS_THREADS) {
+    const uint32_t k = k0[i];
+    for (int p = 0; p < passes; ++p) atomicAdd(&sh[p * RADIX + ((k >> (RB * p)) & rs_digit_mask(key_bits, p, RB))], 1u);
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < passes * RADIX; t += RS_THREADS) {
+    const uint32_t c = sh[t];
+    if (c) atomicAdd(&hist[((size_t)(t / RADIX) * n_segs + g) * RADIX + t % RADIX], c);
+  }
+}
+
+// exclusive scan of each (pass, segment) histogram plus the segment's base
+template <int RB>
+__global__ void __launch_bounds__(1 << RB) k_rs_hist_scan_seg(uint32_t* __restrict__ hist, uint32_t n_segs,
+                                                              uint32_t seg_len) {
+  constexpr int RADIX = Rdx<RB>::RADIX;
+  __shared__ uint32_t s[RADIX];
+  uint32_t* h = hist + (size_t)blockIdx.x * RADIX;
+  const uint32_t base = (blockIdx.x % n_segs) * seg_len;
+  const uint32_t v = h[threadIdx.x];
+  s[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = 1; o < RADIX; o <<= 1) {
+    uint32_t y = threadIdx.x >= (unsigned)o ? s[threadIdx.x - o] : 0u;
+    __syncthreads();
+    s[threadIdx.x] += y;
+    __syncthreads();
+  }
+  h[threadIdx.x] = base + s[threadIdx.x] - v;
+}
+
+template <bool NARROW>
+__global__ void __launch_bounds__(RS_THREADS, 4) k_rs_pass_seg(const uint32_t* __restrict__ kin,
+                                                            const uint32_t* __restrict__ vin, uint32_t* __restrict__ kout,
+                                                            uint32_t* __restrict__ vout, uint64_t n, uint32_t tiles_per_seg,
+                                                            int shift, const uint32_t* __restrict__ digit_base,
+                                                            unsigned* __restrict__ lookback,
+                                                            unsigned* __restrict__ ticket, uint32_t* __restrict__ err,
+                                                            int dbits) {
+  constexpr int RADIX = Rdx<8>::RADIX;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  RsSmem<uint32_t, 8>& sm = *reinterpret_cast<RsSmem<uint32_t, 8>*>(smem_raw);
+  if (threadIdx.x == 0) sm.tile_id = atomicAdd(ticket, 1u);
+  for (int t = threadIdx.x; t < RS_WARPS * RADIX; t += RS_THREADS) (&sm.warp_hist[0][0])[t] = 0;
+  __syncthreads();
+  const uint32_t tile = sm.tile_id;
+  const uint64_t tbase = (uint64_t)tile * RS_SEG_TILE;
+  if (tbase >= n) return;
+  const uint32_t g = tile / tiles_per_seg, local = tile - g * tiles_per_seg;
+  // tiles of segment g look back only on their own segment's tiles, which hold
+  // earlier tickets
+  rs_pass_tile<uint32_t, true, NARROW, 8>(sm, kin, vin, kout, vout, n, shift, digit_base + (size_t)g * RADIX,
+                                          lookback + (size_t)g * tiles_per_seg * RADIX, err, local, tbase, dbits);
+}
+
+size_t radix_seg_scratch_bytes(uint64_t seg_len, uint32_t n_segs) {
+  const uint64_t tiles = sc_div_up(seg_len, RS_SEG_TILE) * n_segs;
+  return (size_t)4 * n_segs * 256 * 4 + 64 + (size_t)4 * tiles * 256 * 4;
+}
+
+sc_status radix_sort_segments(sc_ctx* ctx, uint32_t* keys, uint32_t* vals, uint32_t* keys_tmp, uint32_t* vals_tmp,
+                              uint32_t seg_len, uint32_t n_segs, uint32_t key_bits, void* scratch, size_t bytes,
+                              bool* result_in_tmp) {
+  constexpr int RB = 8, RADIX = 256;
+  *result_in_tmp = false;
+  const uint64_t n = (uint64_t)seg_len * n_segs;
+  if (n == 0 || key_bits == 0) return SC_OK;
+  if (seg_len % RS_SEG_TILE) return sc_fail(ctx, SC_ERR_INVALID_ARG, "segment length must be a multiple of the sort tile");
+  if (n > RS_VAL_MASK) return sc_fail(ctx, SC_ERR_CAPACITY, "radix sort limited to 2^30 - 1 elements");
+  if (key_bits > 32) return sc_fail(ctx, SC_ERR_INVALID_ARG, "key_bits larger than the key type");
+  const int passes = (int)((key_bits + RB - 1) / RB);
+  const uint32_t tps = seg_len / RS_SEG_TILE;
+  const uint64_t tiles = (uint64_t)tps * n_segs;
+  const size_t hist_bytes = (size_t)passes * n_segs * RADIX * 4;
+  const size_t need = hist_bytes + 64 + (size_t)passes * tiles * RADIX * 4;
+  if (bytes < need) return sc_fail(ctx, SC_ERR_INVALID_ARG, "radix scratch too small");
+  uint32_t* hist = reinterpret_cast<uint32_t*>(scratch);
+  unsigned* tickets = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(scratch) + hist_bytes);
+  unsigned* lookback = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(scratch) + hist_bytes + 64);
+  SC_CUDA_TRY(ctx, cudaMemsetAsync(scratch, 0, need, ctx->stream), "memset radix scratch");
+  const unsigned bx = (unsigned)std::max<uint64_t>(
+      1, std::min<uint64_t>(sc_div_up(seg_len, RS_THREADS), (uint64_t)ctx->sm_count * RS_HIST_BLOCKS_PER_SM / n_segs));
+  k_rs_hist_seg<RB><<<dim3(bx, n_segs), RS_THREADS, 0, ctx->stream>>>(keys, seg_len, n_segs, passes, key_bits, hist);
+  SC_TRY(sc_check_launch(ctx, "k_rs_hist_seg"));
+  k_rs_hist_scan_seg<RB><<<(unsigned)(passes * n_segs), RADIX, 0, ctx->stream>>>(hist, n_segs, seg_len);
+  SC_TRY(sc_check_launch(ctx, "k_rs_hist_scan_seg"));
+  const size_t smem = sizeof(RsSmem<uint32_t, RB>);
+  static bool attr_set = false;
+  if (!attr_set) {
+    SC_CUDA_TRY(ctx, cudaFuncSetAttribute(k_rs_pass_seg<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem), "smem attr");
+    SC_CUDA_TRY(ctx, cudaFuncSetAttribute(k_rs_pass_seg<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem), "smem attr");
+    attr_set = true;
+  }
+  uint32_t* kin = keys; uint32_t* vin = vals; uint32_t* kout = keys_tmp; uint32_t* vout = vals_tmp;
+  for (int p = 0; p < passes; ++p) {
+    const int dbits = std::min(RB, (int)key_bits - RB * p);
+    const uint32_t* db = hist + (size_t)p * n_segs * RADIX;
+    unsigned* lb = lookback + (size_t)p * tiles * RADIX;
+    if (dbits == RB)
+      k_rs_pass_seg<false><<<(unsigned)tiles, RS_THREADS, smem, ctx->stream>>>(kin, vin, kout, vout, n, tps, RB * p,
+                                                                             db, lb, tickets + p, ctx->d_error, RB);
+    else
+      k_rs_pass_seg<true><<<(unsigned)tiles, RS_THREADS, smem, ctx->stream>>>(kin, vin, kout, vout, n, tps, RB * p,
+                                                                            db, lb, tickets + p, ctx->d_error, dbits);
+    SC_TRY(sc_check_launch(ctx, "k_rs_pass_seg"));
+    std::swap(kin, kout);
+    std::swap(vin, vout);
+  }
+  *result_in_tmp = (passes & 1) != 0;
+  return SC_OK;
+}
+
 template sc_status radix_sort<uint32_t>(sc_ctx*, uint32_t*, uint32_t*, uint32_t*, uint32_t*, uint64_t, uint32_t,
                                         const uint64_t*, void*, size_t, bool*);
 

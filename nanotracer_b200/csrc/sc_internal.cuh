@@ -245,11 +245,11 @@ namespace sck {
 
 // projection: writes n_views*stride records; when depth_keys != nullptr also
 // writes per (view, splat) a depth sort key (float bits, 0xFFFFFFFF when the
-// splat emits no pairs) and a count for the native pipeline: (tile, splat)
-// pairs, or with bit 1 of `cull` two-level binning items.  Bit 0 of `cull`:
-// exact tile culling.
+// splat emits no pairs; one segment of stride keys per view) and a count for
+// the native pipeline: (tile, splat) pairs, or with bit 1 of `cull` two-level
+// binning items.  Bit 0 of `cull`: exact tile culling.
 sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams, uint32_t n_views,
-                         uint32_t stride, float4* rec, const sc_tiling* tiling, uint64_t* depth_keys,
+                         uint32_t stride, float4* rec, const sc_tiling* tiling, uint32_t* depth_keys,
                          uint32_t* splat_ids, uint32_t* counts, int precise_det, int cull);
 
 sc_status launch_project_backward(sc_ctx* ctx, const DSplats& s, const float4* proj_grad, const sc_camera* d_cam,
@@ -344,6 +344,13 @@ template <typename K>
 sc_status radix_sort(sc_ctx* ctx, K* keys, uint32_t* vals, K* keys_tmp, uint32_t* vals_tmp, uint64_t n,
                      uint32_t key_bits, const uint64_t* d_n, void* scratch, size_t scratch_bytes, bool* result_in_tmp);
 size_t radix_scratch_bytes(uint64_t n, uint32_t key_bytes);
+// n_segs independent stable sorts of u32 keys, segment g = elements
+// [g seg_len, (g + 1) seg_len); seg_len a multiple of RADIX_SEG_TILE
+constexpr uint32_t RADIX_SEG_TILE = 4096;
+sc_status radix_sort_segments(sc_ctx* ctx, uint32_t* keys, uint32_t* vals, uint32_t* keys_tmp, uint32_t* vals_tmp,
+                              uint32_t seg_len, uint32_t n_segs, uint32_t key_bits, void* scratch, size_t bytes,
+                              bool* result_in_tmp);
+size_t radix_seg_scratch_bytes(uint64_t seg_len, uint32_t n_segs);
 // one look-back pass whose predecessor never publishes (bounded-wait self-test)
 sc_status selftest_lookback_timeout(sc_ctx* ctx);
 

@@ -91,7 +91,7 @@ struct sc_trainer {
   float4* rec = nullptr; float4* pgrad = nullptr;
   float* grads = nullptr;  // [SC_NROWS][grad_stride] per-splat gradient rows (one GPU)
   uint32_t grad_stride = 0;
-  uint64_t* dkeys = nullptr; uint64_t* dkeys_tmp = nullptr;
+  uint32_t* dkeys = nullptr; uint32_t* dkeys_tmp = nullptr;  // per view, a segment of stride depth keys
   uint32_t* ids = nullptr; uint32_t* ids_tmp = nullptr;
   uint32_t* counts_by_id = nullptr; uint32_t* counts = nullptr;
   // pairs (the pair-sort path uses all four; two-level binning writes vals only)
@@ -172,7 +172,8 @@ static void trainer_drop_graph(sc_trainer* tr) {
 static sc_status ensure_scratch(sc_trainer* tr) {
   sc_ctx* ctx = tr->ctx;
   const uint64_t nsp = (uint64_t)tr->V * tr->stride;
-  size_t need = std::max({sck::radix_scratch_bytes(nsp, 8), sck::radix_scratch_bytes(std::max<uint64_t>(tr->kcap, 1), 4),
+  size_t need = std::max({sck::radix_seg_scratch_bytes(tr->stride, tr->V),
+                          sck::radix_scratch_bytes(std::max<uint64_t>(tr->kcap, 1), 4),
                           sck::radix_scratch_bytes(std::max<uint64_t>(tr->icap, 1), 4), sck::scan_scratch_bytes(nsp + 1),
                           sck::scan_scratch_bytes((uint64_t)tr->V * tr->T + 1)});
   if (need <= tr->scratch_bytes) return SC_OK;
@@ -186,7 +187,10 @@ static sc_status ensure_scratch(sc_trainer* tr) {
   return SC_OK;
 }
 
+// Per-view arrays hold stride = cap rounded up to whole sort tiles, so each
+// view's depth keys are one segment of the segmented depth sort.
 static sc_status ensure_splat_arrays(sc_trainer* tr, uint32_t cap) {
+  cap = (uint32_t)sc_div_up(cap, sck::RADIX_SEG_TILE) * sck::RADIX_SEG_TILE;
   if (tr->stride == cap) return SC_OK;
   sc_ctx* ctx = tr->ctx;
   SC_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "sync");
@@ -196,8 +200,8 @@ static sc_status ensure_splat_arrays(sc_trainer* tr, uint32_t cap) {
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->pgrad, nv * 48), "pgrad");
   tr->grad_stride = (cap + 63u) & ~63u;
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->grads, (size_t)SC_NROWS * tr->grad_stride * 4), "grads");
-  SC_CUDA_TRY(ctx, cudaMalloc(&tr->dkeys, nv * 8), "dkeys");
-  SC_CUDA_TRY(ctx, cudaMalloc(&tr->dkeys_tmp, nv * 8), "dkeys");
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->dkeys, nv * 4), "dkeys");
+  SC_CUDA_TRY(ctx, cudaMalloc(&tr->dkeys_tmp, nv * 4), "dkeys");
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->ids, nv * 4), "ids");
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->ids_tmp, nv * 4), "ids");
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->counts_by_id, nv * 4), "counts");
@@ -293,8 +297,8 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
                              tr->counts_by_id, 0, (tr->cfg.tile_cull ? 1 : 0) | (tr->two_level ? 2 : 0)));
   mark(tr, 1, capturing);
   bool in_tmp = false;
-  SC_TRY(sck::radix_sort<uint64_t>(ctx, tr->dkeys, tr->ids, tr->dkeys_tmp, tr->ids_tmp, nsp, 32 + bits_for(V - 1),
-                                   nullptr, tr->scratch, tr->scratch_bytes, &in_tmp));
+  SC_TRY(sck::radix_sort_segments(ctx, tr->dkeys, tr->ids, tr->dkeys_tmp, tr->ids_tmp, tr->stride, V, 32, tr->scratch,
+                                  tr->scratch_bytes, &in_tmp));
   const uint32_t* sorted_ids = in_tmp ? tr->ids_tmp : tr->ids;
   mark(tr, 2, capturing);
   SC_TRY(sck::launch_presorted_counts(ctx, tr->counts_by_id, tr->stride, V, sorted_ids, tr->counts));
