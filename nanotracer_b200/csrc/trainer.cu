@@ -114,7 +114,10 @@ struct sc_trainer {
   const float* h_targets = nullptr;
   float* d_host_targets = nullptr;
   cudaStream_t copy_stream = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_copied = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_fwd = nullptr;
+  cudaEvent_t ev_view[SC_MAX_VIEWS] = {};  // view v's targets copied
+  cudaStream_t bwd_stream[SC_MAX_VIEWS] = {};  // view v's blend backward (host targets)
+  cudaEvent_t ev_bwd[SC_MAX_VIEWS] = {};
   double* d_loss = nullptr;
   uint64_t* d_total = nullptr;
   void* scratch = nullptr; size_t scratch_bytes = 0;
@@ -278,12 +281,15 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   const uint64_t launches0 = ctx->launches;
   SC_CUDA_TRY(ctx, cudaMemcpyAsync(tr->d_params, tr->h_params, sizeof(StepParams), cudaMemcpyHostToDevice, ctx->stream),
               "params H2D");
-  if (tr->h_targets) {  // host targets: this step's copy runs beside the stages that do not read them
+  if (tr->h_targets) {  // host targets: this step's copy runs beside the stages that do not read them, view by view
     SC_CUDA_TRY(ctx, cudaEventRecord(tr->ev_fork, ctx->stream), "fork");
     SC_CUDA_TRY(ctx, cudaStreamWaitEvent(tr->copy_stream, tr->ev_fork, 0), "fork wait");
-    SC_CUDA_TRY(ctx, cudaMemcpyAsync(tr->d_host_targets, tr->h_targets, (size_t)V * tr->P * 3 * sizeof(float),
-                                     cudaMemcpyHostToDevice, tr->copy_stream), "targets H2D");
-    SC_CUDA_TRY(ctx, cudaEventRecord(tr->ev_copied, tr->copy_stream), "copied");
+    const size_t vb = (size_t)tr->P * 3;
+    for (uint32_t v = 0; v < V; ++v) {
+      SC_CUDA_TRY(ctx, cudaMemcpyAsync(tr->d_host_targets + v * vb, tr->h_targets + v * vb, vb * sizeof(float),
+                                       cudaMemcpyHostToDevice, tr->copy_stream), "targets H2D");
+      SC_CUDA_TRY(ctx, cudaEventRecord(tr->ev_view[v], tr->copy_stream), "copied");
+    }
   }
   SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->d_loss, 0, 8 * (size_t)V, ctx->stream), "zero loss");
   uint64_t* work_fwd = tr->profiling ? tr->d_work : nullptr;
@@ -363,7 +369,8 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   // are needed only from the backward on (a host upload overlaps the forward)
   const bool mse_in_bwd = lam == 0.0f;
   const float* fwd_target = mse_in_bwd ? nullptr : tr->targets;
-  if (tr->h_targets && !mse_in_bwd) SC_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, tr->ev_copied, 0), "join");
+  if (tr->h_targets && !mse_in_bwd)  // the copies run in order: the last view's event covers all
+    SC_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, tr->ev_view[V - 1], 0), "join");
   if (tr->two_level)
     SC_TRY(sck::launch_composite_items(ctx, tr->rec, tr->stride, V, item_keys, item_ids, tr->iranges, &tr->cfg.tiling,
                                        tr->image, tr->aux, fwd_target, mse_w, tr->dl_dc, tr->d_loss, ctx->d_error,
@@ -377,16 +384,41 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
                             weight * lam, tr->dl_dc, tr->d_ssim, tr->ssim_terms));
   }
   mark(tr, 7, capturing);
-  if (tr->h_targets && mse_in_bwd) SC_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, tr->ev_copied, 0), "join");
   const float* bwd_target = mse_in_bwd ? tr->targets : nullptr;
-  if (tr->two_level)
-    SC_TRY(sck::launch_composite_backward_items(ctx, tr->rec, tr->stride, V, item_keys, item_ids, tr->iranges,
-                                                &tr->cfg.tiling, tr->image, tr->dl_dc, (int)tr->cfg.bwd_mode, tr->aux,
-                                                tr->pgrad, ctx->d_error, bwd_target, mse_w, tr->d_loss, work_bwd));
-  else
-    SC_TRY(sck::launch_composite_backward(ctx, tr->rec, tr->stride, V, svals, tr->ranges, &tr->cfg.tiling, tr->image,
-                                          tr->dl_dc, (int)tr->cfg.bwd_mode, tr->aux, tr->pgrad, ctx->d_error,
-                                          bwd_target, mse_w, tr->d_loss));
+  // with host targets and the MSE formed here, one launch per view on its own
+  // stream, each after the forward and its own view's copy: the backward of
+  // the first views overlaps the upload of the last ones, and the views' tails
+  // (tiles with long lists) overlap each other
+  const bool per_view = tr->h_targets && mse_in_bwd;
+  if (per_view) SC_CUDA_TRY(ctx, cudaEventRecord(tr->ev_fwd, ctx->stream), "forward done");
+  for (uint32_t v0 = 0; v0 < V; v0 += per_view ? 1 : V) {
+    const uint32_t nv = per_view ? 1 : V;
+    cudaStream_t main_stream = ctx->stream;
+    if (per_view) {
+      SC_CUDA_TRY(ctx, cudaStreamWaitEvent(tr->bwd_stream[v0], tr->ev_fwd, 0), "fork");
+      SC_CUDA_TRY(ctx, cudaStreamWaitEvent(tr->bwd_stream[v0], tr->ev_view[v0], 0), "copied");
+      ctx->stream = tr->bwd_stream[v0];  // the launch helpers enqueue on the context's stream
+    }
+    const size_t so = (size_t)3 * v0 * tr->stride, po = (size_t)v0 * tr->P;
+    const float* tg = bwd_target ? bwd_target + 3 * po : nullptr;
+    sc_status st;
+    if (tr->two_level)
+      st = (sck::launch_composite_backward_items(ctx, tr->rec + so, tr->stride, nv, item_keys, item_ids,
+                                                  tr->iranges + (size_t)2 * v0 * tr->ST, &tr->cfg.tiling,
+                                                  tr->image + po, tr->dl_dc ? tr->dl_dc + po : nullptr,
+                                                  (int)tr->cfg.bwd_mode, tr->aux + po,
+                                                  tr->pgrad + so, ctx->d_error, tg, mse_w, tr->d_loss + v0, work_bwd));
+    else
+      st = (sck::launch_composite_backward(ctx, tr->rec + so, tr->stride, nv, svals, tr->ranges + (size_t)2 * v0 * tr->T,
+                                            &tr->cfg.tiling, tr->image + po, tr->dl_dc ? tr->dl_dc + po : nullptr,
+                                            (int)tr->cfg.bwd_mode,
+                                            tr->aux + po, tr->pgrad + so, ctx->d_error, tg, mse_w, tr->d_loss + v0));
+    ctx->stream = main_stream;
+    SC_TRY(st);
+    if (per_view) SC_CUDA_TRY(ctx, cudaEventRecord(tr->ev_bwd[v0], tr->bwd_stream[v0]), "view done");
+  }
+  if (per_view)
+    for (uint32_t v = 0; v < V; ++v) SC_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, tr->ev_bwd[v], 0), "join");
   mark(tr, 8, capturing);
   sck::AdamParams ap;
   for (int k = 0; k < 6; ++k) ap.lr[k] = tr->cfg.adam.lr[k];
@@ -488,7 +520,12 @@ void sc_trainer_free(sc_ctx* ctx, sc_trainer* tr) {
   cudaFree(tr->d_host_targets);
   if (tr->copy_stream) cudaStreamDestroy(tr->copy_stream);
   if (tr->ev_fork) cudaEventDestroy(tr->ev_fork);
-  if (tr->ev_copied) cudaEventDestroy(tr->ev_copied);
+  if (tr->ev_fwd) cudaEventDestroy(tr->ev_fwd);
+  for (uint32_t v = 0; v < SC_MAX_VIEWS; ++v) {
+    if (tr->ev_view[v]) cudaEventDestroy(tr->ev_view[v]);
+    if (tr->ev_bwd[v]) cudaEventDestroy(tr->ev_bwd[v]);
+    if (tr->bwd_stream[v]) cudaStreamDestroy(tr->bwd_stream[v]);
+  }
   cudaFree(tr->scratch);
   if (tr->h_params) cudaFreeHost(tr->h_params);
   if (tr->h_out) cudaFreeHost(tr->h_out);
@@ -517,7 +554,12 @@ sc_status sc_trainer_set_host_targets(sc_trainer* tr, const float* pinned_target
     SC_CUDA_TRY(ctx, cudaMalloc(&tr->d_host_targets, (size_t)tr->V * tr->P * 3 * sizeof(float)), "targets");
     SC_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&tr->copy_stream, cudaStreamNonBlocking), "copy stream");
     SC_CUDA_TRY(ctx, cudaEventCreateWithFlags(&tr->ev_fork, cudaEventDisableTiming), "event");
-    SC_CUDA_TRY(ctx, cudaEventCreateWithFlags(&tr->ev_copied, cudaEventDisableTiming), "event");
+    SC_CUDA_TRY(ctx, cudaEventCreateWithFlags(&tr->ev_fwd, cudaEventDisableTiming), "event");
+    for (uint32_t v = 0; v < tr->V; ++v) {
+      SC_CUDA_TRY(ctx, cudaEventCreateWithFlags(&tr->ev_view[v], cudaEventDisableTiming), "event");
+      SC_CUDA_TRY(ctx, cudaEventCreateWithFlags(&tr->ev_bwd[v], cudaEventDisableTiming), "event");
+      SC_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&tr->bwd_stream[v], cudaStreamNonBlocking), "stream");
+    }
   }
   if (tr->h_targets != pinned_targets) trainer_drop_graph(tr);
   tr->h_targets = pinned_targets;
