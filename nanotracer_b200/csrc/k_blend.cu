@@ -492,49 +492,45 @@ sc_status launch_mse(sc_ctx* ctx, const float4* pred, const float* target, uint6
 }
 
 // ---------------------------------------------------------------- backward
-// Sums a[0..8] over the warp with 12 shuffles (a reduce-scatter: each level
-// halves the values a lane carries).  Lane 0 ends with the total of a[0],
-// lane 2 with a[1], lanes 4, 8, 12, 16, 20, 24, 28 with a[2..8]; *idx is the
-// value index a lane owns, -1 for the others.
-__device__ __forceinline__ float warp_reduce_scatter9(const float a[9], int lane, int* idx) {
-  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
-  // xor 16: lanes below 16 keep values 0..4, the others 5..8
-  float x[5];
+// Reduce-scatter of N values over the warp by recursive halving: at the level
+// of lane bit O a lane keeps one half of its slots and sends the other half to
+// lane ^ O, which keeps the opposite half (2 selects and 1 shuffle per slot
+// pair, ceil(n / 2) slots left); after the 5 levels every lane holds one
+// slot.  rs_owner<N>(lane) is the value index that slot totals (-1: a padding
+// slot).  N = 9: 12 shuffles; N = 18: 20.
+template <int N, int O>
+__device__ __forceinline__ float rs_level(const float* x, int lane) {
+  constexpr int M = (N + 1) / 2;
+  float y[M];
+  const bool bit = lane & O;
 #pragma unroll
-  for (int i = 0; i < 5; ++i) {
-    const float hi = i < 4 ? a[5 + i] : 0.0f;
-    const float send = b4 ? a[i] : hi;
-    const float keep = b4 ? hi : a[i];
-    x[i] = keep + __shfl_xor_sync(FULL_MASK, send, 16);
+  for (int i = 0; i < M; ++i) {
+    const float lo = x[i];
+    const float hi = i + M < N ? x[i + M] : 0.0f;
+    const float send = bit ? lo : hi;
+    const float keep = bit ? hi : lo;
+    y[i] = keep + __shfl_xor_sync(FULL_MASK, send, O);
   }
-  // xor 8: {0,1,2 | 3,4} and {5,6 | 7,8}
-  const float k0 = b3 ? (b4 ? x[2] : x[3]) : x[0];
-  const float s0 = b3 ? x[0] : (b4 ? x[2] : x[3]);
-  const float k1 = b3 ? (b4 ? x[3] : x[4]) : x[1];
-  const float s1 = b3 ? x[1] : (b4 ? x[3] : x[4]);
-  const float k2 = (!b4 && !b3) ? x[2] : 0.0f;
-  const float s2 = (!b4 && b3) ? x[2] : 0.0f;
-  const float y0 = k0 + __shfl_xor_sync(FULL_MASK, s0, 8);
-  const float y1 = k1 + __shfl_xor_sync(FULL_MASK, s1, 8);
-  const float y2 = k2 + __shfl_xor_sync(FULL_MASK, s2, 8);
-  // xor 4: {0,1 | 2}, {3 | 4}, {5 | 6}, {7 | 8}
-  const bool g00 = !b4 && !b3;
-  const float kz0 = g00 ? (b2 ? y2 : y0) : (b2 ? y1 : y0);
-  const float sz0 = g00 ? (b2 ? y0 : y2) : (b2 ? y0 : y1);
-  const float kz1 = (g00 && !b2) ? y1 : 0.0f;
-  const float sz1 = (g00 && b2) ? y1 : 0.0f;
-  const float z0 = kz0 + __shfl_xor_sync(FULL_MASK, sz0, 4);
-  const float z1 = kz1 + __shfl_xor_sync(FULL_MASK, sz1, 4);
-  // xor 2: {0 | 1}; single values collect on the b1 = 0 lane
-  const bool g000 = g00 && !b2;
-  const float kw = g000 ? (b1 ? z1 : z0) : (b1 ? 0.0f : z0);
-  const float sw = g000 ? (b1 ? z0 : z1) : z0;
-  float w = kw + __shfl_xor_sync(FULL_MASK, sw, 2);
-  // xor 1: full sum of the pair
-  w += __shfl_xor_sync(FULL_MASK, w, 1);
-  const bool owner = !(lane & 1) && (g000 || !b1);
-  *idx = owner ? (g000 ? (b1 ? 1 : 0) : 1 + ((lane >> 2) & 7)) : -1;
-  return w;
+  if constexpr (O == 1) {
+    static_assert(M == 1, "at most 32 values");
+    return y[0];
+  } else {
+    return rs_level<M, O / 2>(y, lane);
+  }
+}
+template <int N>
+__device__ __forceinline__ float warp_reduce_scatter(const float (&x)[N], int lane) {
+  return rs_level<N, 16>(x, lane);
+}
+template <int N>
+__device__ __forceinline__ int rs_owner(int lane) {
+  int lo = 0, len = N, n = N;
+  for (int o = 16; o >= 1; o >>= 1) {
+    const int m = (n + 1) / 2;
+    if (lane & o) { lo += m; len = max(len - m, 0); } else { len = min(len, m); }
+    n = m;
+  }
+  return len >= 1 ? lo : -1;
 }
 
 // MODE is the sc_bwd_mode.  In exact mode a pixel takes part from its last
@@ -639,6 +635,9 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
   };
 
   const int lane = threadIdx.x & 31;
+  // the slot of an entry's 3 float4 (12 floats, w unused) this lane adds after the reduce-scatter
+  const int rs_idx = rs_owner<9>(lane);
+  const int rs_off = rs_idx >= 0 ? rs_idx + rs_idx / 3 : -1;
   ListWord f = fetch(0);
   uint32_t cnt_next = place(0, f);
   if (nb > 1) f = fetch(1);
@@ -747,9 +746,8 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
         if (__any_sync(FULL_MASK, contrib)) {
           // the splat's raw sums; the flush turns them into its gradients
           const float c[9] = {shx, shy, sh, shxx, shxy, shyy, scr, scg, scb};
-          int idx;
-          const float w = warp_reduce_scatter9(c, lane, &idx);
-          if (idx >= 0) atomicAdd(reinterpret_cast<float*>(sacc + 3 * k) + idx + idx / 3, w);
+          const float w = warp_reduce_scatter<9>(c, lane);
+          if (rs_off >= 0) atomicAdd(reinterpret_cast<float*>(sacc + 3 * k) + rs_off, w);
         }
         if (MODE == SC_BWD_REF && __all_sync(FULL_MASK, all_done)) break;
       }
