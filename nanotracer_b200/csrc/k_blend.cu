@@ -635,9 +635,11 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
   };
 
   const int lane = threadIdx.x & 31;
-  // the slot of an entry's 3 float4 (12 floats, w unused) this lane adds after the reduce-scatter
-  const int rs_idx = rs_owner<9>(lane);
-  const int rs_off = rs_idx >= 0 ? rs_idx + rs_idx / 3 : -1;
+  // after the 18-value reduce-scatter of entries (k, k - 1) this lane adds one
+  // value: of entry k - rs_ent, at float rs_off of its 3 float4 slot (w unused)
+  const int rs_idx = rs_owner<18>(lane);
+  const int rs_ent = rs_idx >= 9 ? 1 : 0;
+  const int rs_off = rs_idx >= 0 ? rs_idx % 9 + (rs_idx % 9) / 3 : -1;
   ListWord f = fetch(0);
   uint32_t cnt_next = place(0, f);
   if (nb > 1) f = fetch(1);
@@ -661,93 +663,109 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
       float2 T2 = make_float2(T[0], T[PPT - 1]), GS2 = make_float2(GS[0], GS[PPT - 1]);
       const float2 gr2 = make_float2(gr[0], gr[PPT - 1]), gg2 = make_float2(gg[0], gg[PPT - 1]);
       const float2 gb2 = make_float2(gb[0], gb[PPT - 1]), fy2 = make_float2(fy[0], fy[PPT - 1]);
-      for (int k = (int)cnt - 1; k >= 0; --k) {
-        const uint32_t j = LIST == LIST_PAIRS ? lo + (uint32_t)k : begin + bpos[k];
-        // this thread's sums over its pixels: h = dL/dalpha * gauss (the opacity
-        // gradient), its first and second moments in (dx, dy), and the colour
-        // gradient; the per-splat terms are formed from them once per entry
-        float sh = 0.f, shx = 0.f, shy = 0.f, shxx = 0.f, shxy = 0.f, shyy = 0.f;
-        float scr = 0.f, scg = 0.f, scb = 0.f;
-        bool contrib = false;
-        const float4 ra = sb[3 * k], rb = sb[3 * k + 1], rc = sb[3 * k + 2];
-        const EntryGeom e = entry_geom(fx, ra, rb);
-        if constexpr (PPT == 2) {
-          // both pixels in packed arithmetic; a pixel that skips the splat gets
-          // zero alpha and weight, so it adds nothing and keeps its T
-          float2 dy, g, araw, al;
-          bool v0, v1;
-          eval_alpha2(e, rb.z, fy2, ra.y, rc.w, dy, g, araw, al, v0, v1);
-          v0 &= (MODE == SC_BWD_EXACT || !done[0]) && j < stop[0];
-          v1 &= (MODE == SC_BWD_EXACT || !done[1]) && j < stop[1];
-          if (v0 || v1) {
-            const float2 oma = __fadd2_rn(f2(1.0f), make_float2(-al.x, -al.y));
-            const float2 inv = make_float2(rcp_approx(oma.x), rcp_approx(oma.y));
-            const float2 Tn = __fmul2_rn(T2, inv);  // T_i = T_{i+1} / (1 - alpha_i)
-            if (MODE == SC_BWD_REF) {
-              if (v0 && Tn.x > 1.0001f) { done[0] = true; v0 = false; }
-              if (v1 && Tn.y > 1.0001f) { done[1] = true; v1 = false; }
-            }
+      // one entry: this thread's raw sums of it into c[0..8] (zeros when none of
+      // its pixels takes part); returns whether one does
+      auto entry = [&](int k, float* c) -> bool {
+          const uint32_t j = LIST == LIST_PAIRS ? lo + (uint32_t)k : begin + bpos[k];
+          // this thread's sums over its pixels: h = dL/dalpha * gauss (the opacity
+          // gradient), its first and second moments in (dx, dy), and the colour
+          // gradient; the per-splat terms are formed from them once per entry
+          float sh = 0.f, shx = 0.f, shy = 0.f, shxx = 0.f, shxy = 0.f, shyy = 0.f;
+          float scr = 0.f, scg = 0.f, scb = 0.f;
+          bool contrib = false;
+          const float4 ra = sb[3 * k], rb = sb[3 * k + 1], rc = sb[3 * k + 2];
+          const EntryGeom e = entry_geom(fx, ra, rb);
+          if constexpr (PPT == 2) {
+            // both pixels in packed arithmetic; a pixel that skips the splat gets
+            // zero alpha and weight, so it adds nothing and keeps its T
+            float2 dy, g, araw, al;
+            bool v0, v1;
+            eval_alpha2(e, rb.z, fy2, ra.y, rc.w, dy, g, araw, al, v0, v1);
+            v0 &= (MODE == SC_BWD_EXACT || !done[0]) && j < stop[0];
+            v1 &= (MODE == SC_BWD_EXACT || !done[1]) && j < stop[1];
             if (v0 || v1) {
-              const float2 am = make_float2(v0 ? al.x : 0.0f, v1 ? al.y : 0.0f);
-              const float2 gm = make_float2(v0 && araw.x < ALPHA_MAX ? g.x : 0.0f,
-                                            v1 && araw.y < ALPHA_MAX ? g.y : 0.0f);
-              const float2 ta = __fmul2_rn(Tn, am);
-              const float2 p = __fmul2_rn(ta, gr2), q = __fmul2_rn(ta, gg2), w = __fmul2_rn(ta, gb2);
-              scr = p.x + p.y; scg = q.x + q.y; scb = w.x + w.y;
-              // dC/dalpha = T_i c - S / (1 - alpha) = (T_{i+1} c - S) / (1 - alpha)
-              const float2 dc = __ffma2_rn(gb2, f2(rc.z), __ffma2_rn(gg2, f2(rc.y), __fmul2_rn(gr2, f2(rc.x))));
-              const float2 galpha = __fmul2_rn(inv, __ffma2_rn(T2, dc, make_float2(-GS2.x, -GS2.y)));
-              const float2 h = __fmul2_rn(galpha, gm);
-              const float2 hy = __fmul2_rn(h, dy);
-              sh = h.x + h.y;
-              shy = hy.x + hy.y;
-              shyy = fmaf(hy.x, dy.x, hy.y * dy.y);
-              shx = sh * e.dx;  // both pixels share dx
-              shxx = shx * e.dx;
-              shxy = shy * e.dx;
-              GS2 = __ffma2_rn(ta, dc, GS2);
-              T2 = make_float2(v0 ? Tn.x : T2.x, v1 ? Tn.y : T2.y);
-              contrib = true;
-            }
-          }
-          if (MODE == SC_BWD_REF) all_done = (done[0] || j <= begin) && (done[1] || j <= begin);
-        } else {
-          all_done = true;
-#pragma unroll
-          for (int q = 0; q < PPT; ++q) {
-            if ((MODE == SC_BWD_EXACT || !done[q]) && j < stop[q]) {
-              const float dy = __fadd_rn(fy[q], -ra.y);
-              float g, araw, alpha;
-              if (eval_alpha(e, rb.z, dy, rc.w, g, araw, alpha)) {
-                const float inv = rcp_approx(__fadd_rn(1.0f, -alpha));
-                const float Tn = __fmul_rn(T[q], inv);  // T_i = T_{i+1} / (1 - alpha_i)
-                if (MODE == SC_BWD_REF && Tn > 1.0001f) {
-                  done[q] = true;
-                } else {
-                  const float ta = __fmul_rn(Tn, alpha);
-                  scr += gr[q] * ta; scg += gg[q] * ta; scb += gb[q] * ta;
-                  const float dc = gr[q] * rc.x + gg[q] * rc.y + gb[q] * rc.z;
-                  const float galpha = inv * (T[q] * dc - GS[q]);
-                  const float h = araw < ALPHA_MAX ? galpha * g : 0.0f;
-                  const float hx = h * e.dx, hy = h * dy;
-                  sh += h;
-                  shx += hx; shy += hy;
-                  shxx += hx * e.dx; shxy += hx * dy; shyy += hy * dy;
-                  GS[q] += ta * dc;
-                  T[q] = Tn;
-                  contrib = true;
-                }
+              const float2 oma = __fadd2_rn(f2(1.0f), make_float2(-al.x, -al.y));
+              const float2 inv = make_float2(rcp_approx(oma.x), rcp_approx(oma.y));
+              const float2 Tn = __fmul2_rn(T2, inv);  // T_i = T_{i+1} / (1 - alpha_i)
+              if (MODE == SC_BWD_REF) {
+                if (v0 && Tn.x > 1.0001f) { done[0] = true; v0 = false; }
+                if (v1 && Tn.y > 1.0001f) { done[1] = true; v1 = false; }
+              }
+              if (v0 || v1) {
+                const float2 am = make_float2(v0 ? al.x : 0.0f, v1 ? al.y : 0.0f);
+                const float2 gm = make_float2(v0 && araw.x < ALPHA_MAX ? g.x : 0.0f,
+                                              v1 && araw.y < ALPHA_MAX ? g.y : 0.0f);
+                const float2 ta = __fmul2_rn(Tn, am);
+                const float2 p = __fmul2_rn(ta, gr2), q = __fmul2_rn(ta, gg2), w = __fmul2_rn(ta, gb2);
+                scr = p.x + p.y; scg = q.x + q.y; scb = w.x + w.y;
+                // dC/dalpha = T_i c - S / (1 - alpha) = (T_{i+1} c - S) / (1 - alpha)
+                const float2 dc = __ffma2_rn(gb2, f2(rc.z), __ffma2_rn(gg2, f2(rc.y), __fmul2_rn(gr2, f2(rc.x))));
+                const float2 galpha = __fmul2_rn(inv, __ffma2_rn(T2, dc, make_float2(-GS2.x, -GS2.y)));
+                const float2 h = __fmul2_rn(galpha, gm);
+                const float2 hy = __fmul2_rn(h, dy);
+                sh = h.x + h.y;
+                shy = hy.x + hy.y;
+                shyy = fmaf(hy.x, dy.x, hy.y * dy.y);
+                shx = sh * e.dx;  // both pixels share dx
+                shxx = shx * e.dx;
+                shxy = shy * e.dx;
+                GS2 = __ffma2_rn(ta, dc, GS2);
+                T2 = make_float2(v0 ? Tn.x : T2.x, v1 ? Tn.y : T2.y);
+                contrib = true;
               }
             }
-            if (MODE == SC_BWD_REF) all_done &= done[q] || j <= begin;
+            if (MODE == SC_BWD_REF) all_done = (done[0] || j <= begin) && (done[1] || j <= begin);
+          } else {
+            all_done = true;
+  #pragma unroll
+            for (int q = 0; q < PPT; ++q) {
+              if ((MODE == SC_BWD_EXACT || !done[q]) && j < stop[q]) {
+                const float dy = __fadd_rn(fy[q], -ra.y);
+                float g, araw, alpha;
+                if (eval_alpha(e, rb.z, dy, rc.w, g, araw, alpha)) {
+                  const float inv = rcp_approx(__fadd_rn(1.0f, -alpha));
+                  const float Tn = __fmul_rn(T[q], inv);  // T_i = T_{i+1} / (1 - alpha_i)
+                  if (MODE == SC_BWD_REF && Tn > 1.0001f) {
+                    done[q] = true;
+                  } else {
+                    const float ta = __fmul_rn(Tn, alpha);
+                    scr += gr[q] * ta; scg += gg[q] * ta; scb += gb[q] * ta;
+                    const float dc = gr[q] * rc.x + gg[q] * rc.y + gb[q] * rc.z;
+                    const float galpha = inv * (T[q] * dc - GS[q]);
+                    const float h = araw < ALPHA_MAX ? galpha * g : 0.0f;
+                    const float hx = h * e.dx, hy = h * dy;
+                    sh += h;
+                    shx += hx; shy += hy;
+                    shxx += hx * e.dx; shxy += hx * dy; shyy += hy * dy;
+                    GS[q] += ta * dc;
+                    T[q] = Tn;
+                    contrib = true;
+                  }
+                }
+              }
+              if (MODE == SC_BWD_REF) all_done &= done[q] || j <= begin;
+            }
           }
+        c[0] = shx; c[1] = shy; c[2] = sh; c[3] = shxx; c[4] = shxy; c[5] = shyy;
+        c[6] = scr; c[7] = scg; c[8] = scb;
+        return contrib;
+      };
+      // entries k and k - 1 together: one 18-value reduce-scatter (20 shuffles
+      // instead of 2 x 12)
+      for (int k = (int)cnt - 1; k >= 0; k -= 2) {
+        float c[18];
+        bool any = entry(k, c);
+        if (k >= 1) {
+          any |= entry(k - 1, c + 9);
+        } else {
+#pragma unroll
+          for (int i = 9; i < 18; ++i) c[i] = 0.0f;
         }
         if (MODE == SC_BWD_EXACT) all_done = false;
-        if (__any_sync(FULL_MASK, contrib)) {
-          // the splat's raw sums; the flush turns them into its gradients
-          const float c[9] = {shx, shy, sh, shxx, shxy, shyy, scr, scg, scb};
-          const float w = warp_reduce_scatter<9>(c, lane);
-          if (rs_off >= 0) atomicAdd(reinterpret_cast<float*>(sacc + 3 * k) + rs_off, w);
+        if (__any_sync(FULL_MASK, any)) {
+          // the splats' raw sums; the flush turns them into their gradients
+          const float w = warp_reduce_scatter<18>(c, lane);
+          if (rs_off >= 0 && k >= rs_ent) atomicAdd(reinterpret_cast<float*>(sacc + 3 * (k - rs_ent)) + rs_off, w);
         }
         if (MODE == SC_BWD_REF && __all_sync(FULL_MASK, all_done)) break;
       }
