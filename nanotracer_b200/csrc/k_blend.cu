@@ -533,6 +533,11 @@ __device__ __forceinline__ int rs_owner(int lane) {
   return len >= 1 ? lo : -1;
 }
 
+// Entries per warp reduction: 2 (an 18-value reduce-scatter, 20 shuffles for
+// two entries).  3 entries (27 values, 28 shuffles) measured slower at 80
+// registers; more than 3 do not fit the 32 lanes.
+constexpr int RS_E = 2;
+
 // MODE is the sc_bwd_mode.  In exact mode a pixel takes part from its last
 // contributor down to the start of the tile's list and never stops early, so
 // the early-exit bookkeeping exists only in reference mode.
@@ -637,8 +642,8 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
   const int lane = threadIdx.x & 31;
   // after the 18-value reduce-scatter of entries (k, k - 1) this lane adds one
   // value: of entry k - rs_ent, at float rs_off of its 3 float4 slot (w unused)
-  const int rs_idx = rs_owner<18>(lane);
-  const int rs_ent = rs_idx >= 9 ? 1 : 0;
+  const int rs_idx = rs_owner<9 * RS_E>(lane);
+  const int rs_ent = rs_idx / 9;
   const int rs_off = rs_idx >= 0 ? rs_idx % 9 + (rs_idx % 9) / 3 : -1;
   ListWord f = fetch(0);
   uint32_t cnt_next = place(0, f);
@@ -750,21 +755,23 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
         c[6] = scr; c[7] = scg; c[8] = scb;
         return contrib;
       };
-      // entries k and k - 1 together: one 18-value reduce-scatter (20 shuffles
-      // instead of 2 x 12)
-      for (int k = (int)cnt - 1; k >= 0; k -= 2) {
-        float c[18];
-        bool any = entry(k, c);
-        if (k >= 1) {
-          any |= entry(k - 1, c + 9);
-        } else {
+      // entries k .. k - RS_E + 1 together: one 9 RS_E-value reduce-scatter
+      for (int k = (int)cnt - 1; k >= 0; k -= RS_E) {
+        float c[9 * RS_E];
+        bool any = false;
 #pragma unroll
-          for (int i = 9; i < 18; ++i) c[i] = 0.0f;
+        for (int q = 0; q < RS_E; ++q) {
+          if (k - q >= 0) {
+            any |= entry(k - q, c + 9 * q);
+          } else {
+#pragma unroll
+            for (int i = 0; i < 9; ++i) c[9 * q + i] = 0.0f;
+          }
         }
         if (MODE == SC_BWD_EXACT) all_done = false;
         if (__any_sync(FULL_MASK, any)) {
           // the splats' raw sums; the flush turns them into their gradients
-          const float w = warp_reduce_scatter<18>(c, lane);
+          const float w = warp_reduce_scatter<9 * RS_E>(c, lane);
           if (rs_off >= 0 && k >= rs_ent) atomicAdd(reinterpret_cast<float*>(sacc + 3 * (k - rs_ent)) + rs_off, w);
         }
         if (MODE == SC_BWD_REF && __all_sync(FULL_MASK, all_done)) break;
