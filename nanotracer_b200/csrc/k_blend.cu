@@ -310,6 +310,8 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
         float2 T2 = make_float2(in0 ? T[0] : 0.0f, in1 ? T[1] : 0.0f);
         float2 R2 = make_float2(cr[0], cr[1]), G2 = make_float2(cg[0], cg[1]), B2 = make_float2(cb[0], cb[1]);
         const float2 fy2 = make_float2(fy[0], fy[1]);
+        int lk0 = -1, lk1 = -1;  // this batch's last contributing entries, as list positions below
+#pragma unroll 2
         for (uint32_t k = 0; k < cnt; ++k) {
           const float4 ra = sb[3 * k], rb = sb[3 * k + 1], rc = sb[3 * k + 2];
           const EntryGeom e = entry_geom(fx, ra, rb);
@@ -325,12 +327,13 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
             G2 = __ffma2_rn(ta, f2(rc.y), G2);
             B2 = __ffma2_rn(ta, f2(rc.z), B2);
             T2 = __fmul2_rn(T2, __fadd2_rn(f2(1.0f), make_float2(-am.x, -am.y)));
-            const uint32_t pk = position(b, k) + 1;
-            if (v0) last[0] = pk;
-            if (v1) last[1] = pk;
+            if (v0) lk0 = (int)k;
+            if (v1) lk1 = (int)k;
             if (T2.x < 1e-4f && T2.y < 1e-4f) break;
           }
         }
+        if (lk0 >= 0) last[0] = position(b, (uint32_t)lk0) + 1;
+        if (lk1 >= 0) last[1] = position(b, (uint32_t)lk1) + 1;
         done[0] = T2.x < 1e-4f;
         done[1] = T2.y < 1e-4f;
         T[0] = T2.x; T[1] = T2.y; cr[0] = R2.x; cr[1] = R2.y;
