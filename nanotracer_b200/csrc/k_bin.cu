@@ -189,22 +189,6 @@ sc_status launch_tile_ranges(sc_ctx* ctx, const void* keys, int key_mode, const 
 
 // ---------------------------------------------------------------- depth-presorted path
 // sorted_ids[v*stride + r] is the splat of depth rank r in view v.
-__global__ void k_presorted_counts(const uint32_t* __restrict__ counts_by_id, uint32_t stride, uint32_t n_views,
-                                   const uint32_t* __restrict__ sorted_ids, uint32_t* __restrict__ counts) {
-  const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= (uint64_t)n_views * stride) return;
-  const uint32_t v = (uint32_t)(j / stride);
-  counts[j] = counts_by_id[(size_t)v * stride + sorted_ids[j]];
-}
-
-sc_status launch_presorted_counts(sc_ctx* ctx, const uint32_t* counts_by_id, uint32_t stride, uint32_t n_views,
-                                   const uint32_t* sorted_ids, uint32_t* counts) {
-  const uint64_t total = (uint64_t)n_views * stride;
-  if (total == 0) return SC_OK;
-  k_presorted_counts<<<(unsigned)sc_div_up(total, 256), 256, 0, ctx->stream>>>(counts_by_id, stride, n_views,
-                                                                               sorted_ids, counts);
-  return sc_check_launch(ctx, "k_presorted_counts");
-}
 
 // One thread generates the pairs of one depth-ranked splat, row by row.  With
 // culling, each row keeps the span of tiles that cull_row_span returns — the

@@ -58,10 +58,20 @@ __device__ __forceinline__ unsigned long long warp_incl_scan_u64(unsigned long l
   return x;
 }
 
+// Gather of the scanned values (when src is given): element i < gn is
+// src[(i / seg) seg + idx[i]] — the value of the idx[i]-th element of its
+// segment (a view's counts by splat, read in depth order) — and 0 beyond gn.
+struct ScanGather {
+  const uint32_t* src;
+  const uint32_t* idx;
+  uint32_t seg;
+  uint64_t n;
+};
+
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan(uint32_t* __restrict__ data, uint64_t n,
                                                        unsigned long long* __restrict__ status,
                                                        unsigned* __restrict__ ticket, uint64_t* __restrict__ total,
-                                                       uint32_t* __restrict__ err) {
+                                                       uint32_t* __restrict__ err, ScanGather gather) {
   __shared__ unsigned s_tile;
   __shared__ unsigned long long s_warp[SCAN_THREADS / 32];
   __shared__ unsigned long long s_excl;
@@ -71,10 +81,21 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan(uint32_t* __restrict__ da
   const uint64_t base = (uint64_t)tile * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_IPT;
   uint32_t x[SCAN_IPT];
   unsigned long long tsum = 0;
+  if (gather.src) {
+    uint32_t g = base < gather.n ? (uint32_t)(base / gather.seg) : 0u;  // the segment of element base
 #pragma unroll
-  for (int k = 0; k < SCAN_IPT; ++k) {
-    x[k] = (base + k < n) ? data[base + k] : 0u;
-    tsum += x[k];
+    for (int k = 0; k < SCAN_IPT; ++k) {
+      const uint64_t i = base + k;
+      if (i >= (uint64_t)(g + 1) * gather.seg) ++g;  // a thread's elements cross at most one segment end
+      x[k] = i < gather.n ? gather.src[(size_t)g * gather.seg + gather.idx[i]] : 0u;
+      tsum += x[k];
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < SCAN_IPT; ++k) {
+      x[k] = (base + k < n) ? data[base + k] : 0u;
+      tsum += x[k];
+    }
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   unsigned long long incl = warp_incl_scan_u64(tsum);
@@ -134,7 +155,8 @@ size_t scan_scratch_bytes(uint64_t n) {
   return 256 + tiles * 8;
 }
 
-sc_status scan_u32(sc_ctx* ctx, uint32_t* data, uint64_t n, uint64_t* d_total, void* scratch, size_t bytes) {
+static sc_status scan_u32_impl(sc_ctx* ctx, uint32_t* data, uint64_t n, uint64_t* d_total, void* scratch,
+                               size_t bytes, ScanGather gather) {
   if (n == 0) {
     if (d_total) SC_CUDA_TRY(ctx, cudaMemsetAsync(d_total, 0, 8, ctx->stream), "memset total");
     return SC_OK;
@@ -144,8 +166,18 @@ sc_status scan_u32(sc_ctx* ctx, uint32_t* data, uint64_t n, uint64_t* d_total, v
   unsigned* ticket = reinterpret_cast<unsigned*>(scratch);
   unsigned long long* status = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(scratch) + 256);
   SC_CUDA_TRY(ctx, cudaMemsetAsync(scratch, 0, scan_scratch_bytes(n), ctx->stream), "memset scan status");
-  k_scan<<<(unsigned)tiles, SCAN_THREADS, 0, ctx->stream>>>(data, n, status, ticket, d_total, ctx->d_error);
+  k_scan<<<(unsigned)tiles, SCAN_THREADS, 0, ctx->stream>>>(data, n, status, ticket, d_total, ctx->d_error, gather);
   return sc_check_launch(ctx, "k_scan");
+}
+
+sc_status scan_u32(sc_ctx* ctx, uint32_t* data, uint64_t n, uint64_t* d_total, void* scratch, size_t bytes) {
+  return scan_u32_impl(ctx, data, n, d_total, scratch, bytes, ScanGather{nullptr, nullptr, 1, 0});
+}
+
+sc_status scan_u32_gather(sc_ctx* ctx, uint32_t* out, uint64_t n, const uint32_t* src, const uint32_t* idx,
+                          uint32_t seg, uint64_t gn, uint64_t* d_total, void* scratch, size_t bytes) {
+  if (seg == 0 || seg % SCAN_IPT) return sc_fail(ctx, SC_ERR_INVALID_ARG, "gather segment must be a multiple of 16");
+  return scan_u32_impl(ctx, out, n, d_total, scratch, bytes, ScanGather{src, idx, seg, gn});
 }
 
 // ---------------------------------------------------------------- allocation-free scan
@@ -203,7 +235,8 @@ extern "C" sc_status sc_exclusive_scan_u32_noalloc(sc_ctx* ctx, uint32_t* data, 
   SC_CUDA_TRY(ctx, cudaMemsetAsync(scratch, 0, 256 + tiles * 8, ctx->stream), "clear scan scratch");
   unsigned* ticket = reinterpret_cast<unsigned*>(scratch);
   unsigned long long* status = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(scratch) + 256);
-  sck::k_scan<<<(unsigned)tiles, SCAN_THREADS, 0, ctx->stream>>>(data, n, status, ticket, total, ctx->d_error);
+  sck::k_scan<<<(unsigned)tiles, SCAN_THREADS, 0, ctx->stream>>>(data, n, status, ticket, total, ctx->d_error,
+                                                                 sck::ScanGather{nullptr, nullptr, 1, 0});
   return sc_check_launch(ctx, "k_scan");
 }
 

@@ -339,6 +339,10 @@ sc_status launch_unpack_moments(sc_ctx* ctx, const DMoments& mo, uint32_t n, con
 
 // scan / sort
 sc_status scan_u32(sc_ctx* ctx, uint32_t* data, uint64_t n, uint64_t* d_total, void* scratch, size_t scratch_bytes);
+// the same exclusive scan of out[0..n), out[i] = src[(i / seg) seg + idx[i]]
+// for i < gn and 0 beyond (seg a multiple of 16), gathered as it is read
+sc_status scan_u32_gather(sc_ctx* ctx, uint32_t* out, uint64_t n, const uint32_t* src, const uint32_t* idx,
+                          uint32_t seg, uint64_t gn, uint64_t* d_total, void* scratch, size_t scratch_bytes);
 size_t scan_scratch_bytes(uint64_t n);
 template <typename K>
 sc_status radix_sort(sc_ctx* ctx, K* keys, uint32_t* vals, K* keys_tmp, uint32_t* vals_tmp, uint64_t n,
@@ -367,8 +371,6 @@ sc_status launch_tile_ranges(sc_ctx* ctx, const void* keys, int key_mode, const 
                              uint32_t num_tiles, uint32_t* ranges, uint32_t tiles_per_view = 0,
                              uint32_t tile_bits = 0, uint32_t key_bits = 32, uint64_t* high_popc = nullptr);
 // depth-presorted emission for the native pipeline
-sc_status launch_presorted_counts(sc_ctx* ctx, const uint32_t* counts_by_id, uint32_t stride, uint32_t n_views,
-                                  const uint32_t* sorted_ids, uint32_t* counts);
 sc_status launch_presorted_emit(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
                                 const uint32_t* sorted_ids, const uint32_t* offsets, const uint32_t* counts_by_id,
                                 const sc_tiling* tl, uint32_t* keys, uint32_t* payloads, uint64_t cap,

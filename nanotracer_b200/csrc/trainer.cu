@@ -307,7 +307,6 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
                                   tr->scratch_bytes, &in_tmp));
   const uint32_t* sorted_ids = in_tmp ? tr->ids_tmp : tr->ids;
   mark(tr, 2, capturing);
-  SC_TRY(sck::launch_presorted_counts(ctx, tr->counts_by_id, tr->stride, V, sorted_ids, tr->counts));
   const uint32_t all_tiles = V * tr->T;
   const uint32_t* svals = nullptr;
   const uint32_t* item_keys = nullptr;
@@ -318,7 +317,9 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
     // super tile whose mask holds it
     const int cull = tr->cfg.tile_cull ? 1 : 0;
     uint64_t* d_items = tr->d_total + 1;
-    SC_TRY(sck::scan_u32(ctx, tr->counts, nsp + 1, d_items, tr->scratch, tr->scratch_bytes));
+    // item counts in depth order (gathered through the sorted ids) -> offsets
+    SC_TRY(sck::scan_u32_gather(ctx, tr->counts, nsp + 1, tr->counts_by_id, sorted_ids, tr->stride, nsp, d_items,
+                                tr->scratch, tr->scratch_bytes));
     if (sizing) {
       uint64_t I = 0;
       SC_CUDA_TRY(ctx, cudaMemcpyAsync(&I, d_items, 8, cudaMemcpyDeviceToHost, ctx->stream), "items");
@@ -339,7 +340,8 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
     SC_TRY(sck::launch_tile_ranges(ctx, item_keys, 2, d_items, tr->icap, V * tr->ST, tr->iranges, tr->ST,
                                    tr->super_bits, tr->super_bits + bits_for(V - 1), tr->d_total));
   } else {
-  SC_TRY(sck::scan_u32(ctx, tr->counts, nsp + 1, tr->d_total, tr->scratch, tr->scratch_bytes));
+  SC_TRY(sck::scan_u32_gather(ctx, tr->counts, nsp + 1, tr->counts_by_id, sorted_ids, tr->stride, nsp, tr->d_total,
+                              tr->scratch, tr->scratch_bytes));
   if (sizing) {
     uint64_t K = 0;
     SC_CUDA_TRY(ctx, cudaMemcpyAsync(&K, tr->d_total, 8, cudaMemcpyDeviceToHost, ctx->stream), "K");
