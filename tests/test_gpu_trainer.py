@@ -192,9 +192,10 @@ def test_host_targets_copied_beside_the_step_match_device_targets(ctx):
 
 @pytest.mark.parametrize("tile", [(16, 16), (8, 8), (32, 8)])
 def test_two_level_binning_equals_the_pair_sort(ctx, tile):
-    """sort_mode 0/2 (super tiles, per-tile lists filled in depth order) and
-    sort_mode 1 (stable sort of the pairs) give the same per-tile lists: the
-    images and parameters after a step are identical and the pair counts equal."""
+    """sort_mode 0/2 (super-tile item lists, each tile keeping the items whose
+    member mask holds it) and sort_mode 1 (stable sort of the pairs) blend the
+    same splats in the same order: the images and parameters after a step are
+    identical, and the pair count summed from the masks equals the pair sort's."""
     scene, tl, cams, tgt, cfg = _setup(ctx, n=4000, V=3, tile=tile)
     assert cfg.sort_mode == 0
     tr2, g2, _, _, l2 = _run(ctx, scene, cams, tgt, cfg)        # default: two-level
@@ -204,3 +205,26 @@ def test_two_level_binning_equals_the_pair_sort(ctx, tile):
     assert tr2.stats()["items"] > 0 and tr1.stats()["items"] == 0
     assert np.allclose(l1, l2, rtol=1e-6)
     assert np.allclose(g1.readback().flat(), g2.readback().flat(), rtol=1e-5, atol=1e-7)
+
+
+def test_blend_work_counters_bound_each_other(ctx):
+    """sc_trainer_blend_work while profiling: the forward blends only entries of
+    the list positions it scans, the backward walks no further than the
+    forward's last contributors, and neither touches more entries than there
+    are (tile, splat) pairs."""
+    scene, tl, cams, tgt, cfg = _setup(ctx, n=6000, V=3)
+    g = GpuSplatBuffer.upload(ctx, scene)
+    mo = AdamMomentBuffers(ctx, g.capacity)
+    acc = ctx.storage_buffer_zeroed("acc", 4 * g.capacity)
+    tr = Trainer(ctx, cfg)
+    tr.set_targets(ctx.storage_buffer("targets", np.ascontiguousarray(tgt, np.float32)))
+    tr.step(g, mo, acc, cams, 1)
+    tr.set_profiling(True)
+    for t in (2, 3):
+        tr.step(g, mo, acc, cams, t)
+    st = tr.stats()
+    w = st["blend_work"]
+    assert 0 < w["fwd_blended"] <= w["fwd_scanned"] <= st["items"] * 16
+    assert 0 < w["bwd_blended"] <= w["bwd_scanned"] <= w["fwd_scanned"]
+    assert w["bwd_blended"] <= w["fwd_blended"] <= st["pairs"]
+    tr.set_profiling(False)
