@@ -180,7 +180,8 @@ struct TileArgs { uint32_t tw, th, tiles_x, tiles_y, cull, super; };
 __global__ void __launch_bounds__(128) k_project(DSplats s, const sc_camera* __restrict__ cams, uint32_t n_views,
                                                  uint32_t stride, float4* __restrict__ rec, TileArgs ta,
                                                  uint32_t* __restrict__ depth_keys, uint32_t* __restrict__ ids,
-                                                 uint32_t* __restrict__ counts, int precise) {
+                                                 uint32_t* __restrict__ counts, int precise,
+                                                 float4* __restrict__ zero_grad) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t v = blockIdx.y;
   if (i >= stride) return;
@@ -251,6 +252,10 @@ __global__ void __launch_bounds__(128) k_project(DSplats s, const sc_camera* __r
     }
     const size_t o = (size_t)v * stride + i;
     rec[3 * o + 0] = ra; rec[3 * o + 1] = rb; rec[3 * o + 2] = rc;
+    if (zero_grad) {  // the blend backward's per-(view, splat) gradient records start at zero
+      const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+      zero_grad[3 * o + 0] = z; zero_grad[3 * o + 1] = z; zero_grad[3 * o + 2] = z;
+    }
     if (depth_keys) {
       depth_keys[o] = key;
       ids[o] = i;
@@ -261,7 +266,7 @@ __global__ void __launch_bounds__(128) k_project(DSplats s, const sc_camera* __r
 
 sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams, uint32_t n_views, uint32_t stride,
                          float4* rec, const sc_tiling* tl, uint32_t* depth_keys, uint32_t* ids, uint32_t* counts,
-                         int precise, int cull) {
+                         int precise, int cull, float4* zero_grad) {
   if (stride == 0 || n_views == 0) return SC_OK;
   TileArgs ta{1, 1, 1, 1, 0, 0};
   if (tl) ta = TileArgs{tl->tile_w, tl->tile_h, (tl->width + tl->tile_w - 1) / tl->tile_w,
@@ -269,7 +274,8 @@ sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams,
   const uint32_t bs = 128;  // grid: (splats / bs, views)
   if (n_views > 65535) return sc_fail(ctx, SC_ERR_INVALID_ARG, "too many views");
   k_project<<<dim3((unsigned)sc_div_up(stride, bs), n_views), bs, 0, ctx->stream>>>(s, d_cams, n_views, stride, rec,
-                                                                                   ta, depth_keys, ids, counts, precise);
+                                                                                   ta, depth_keys, ids, counts, precise,
+                                                                                   zero_grad);
   return sc_check_launch(ctx, "k_project");
 }
 

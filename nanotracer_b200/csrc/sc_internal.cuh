@@ -247,10 +247,12 @@ namespace sck {
 // writes per (view, splat) a depth sort key (float bits, 0xFFFFFFFF when the
 // splat emits no pairs; one segment of stride keys per view) and a count for
 // the native pipeline: (tile, splat) pairs, or with bit 1 of `cull` two-level
-// binning items.  Bit 0 of `cull`: exact tile culling.
+// binning items.  Bit 0 of `cull`: exact tile culling.  zero_grad (nullable):
+// per-(view, splat) gradient records of the same layout set to zero.
 sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams, uint32_t n_views,
                          uint32_t stride, float4* rec, const sc_tiling* tiling, uint32_t* depth_keys,
-                         uint32_t* splat_ids, uint32_t* counts, int precise_det, int cull);
+                         uint32_t* splat_ids, uint32_t* counts, int precise_det, int cull,
+                         float4* zero_grad = nullptr);
 
 sc_status launch_project_backward(sc_ctx* ctx, const DSplats& s, const float4* proj_grad, const sc_camera* d_cam,
                                   float* grads, uint32_t gcap, int accumulate);

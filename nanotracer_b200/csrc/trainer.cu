@@ -296,11 +296,10 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   uint64_t* work_bwd = tr->profiling ? tr->d_work + 2 * sck::BLEND_WORK_SLOTS : nullptr;
   if (tr->profiling)
     SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->d_work, 0, 4 * sck::BLEND_WORK_SLOTS * 8, ctx->stream), "zero work");
-  SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->pgrad, 0, nsp * 48, ctx->stream), "zero pgrad");
   SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->counts + nsp, 0, 4, ctx->stream), "zero count tail");
   mark(tr, 0, capturing);
   SC_TRY(sck::launch_project(ctx, ds, d_cams, V, tr->stride, tr->rec, &tr->cfg.tiling, tr->dkeys, tr->ids,
-                             tr->counts_by_id, 0, (tr->cfg.tile_cull ? 1 : 0) | (tr->two_level ? 2 : 0)));
+                             tr->counts_by_id, 0, (tr->cfg.tile_cull ? 1 : 0) | (tr->two_level ? 2 : 0), tr->pgrad));
   mark(tr, 1, capturing);
   bool in_tmp = false;
   SC_TRY(sck::radix_sort_segments(ctx, tr->dkeys, tr->ids, tr->dkeys_tmp, tr->ids_tmp, tr->stride, V, 32, tr->scratch,
