@@ -173,17 +173,19 @@ __device__ __forceinline__ bool tile_rect(float mx, float my, float r, float vis
 // reached) instead of (tile, splat) pairs
 struct TileArgs { uint32_t tw, th, tiles_x, tiles_y, cull, super; };
 
-// One thread per (splat, view), the view being blockIdx.y: every view plane of
-// the outputs is written with coalesced stores, and the views of a splat read
-// its parameters from L2 (the per-view work — rotation, scales, SH — does not
-// share between views anyway).
-__global__ void __launch_bounds__(128) k_project(DSplats s, const sc_camera* __restrict__ cams, uint32_t n_views,
+// One thread per (splat, view).  Consecutive CTAs take the views of one chunk
+// of splats (view = block % n_views), so the views after the first read the
+// chunk's parameters from L2 while each view plane of the outputs is still
+// written with coalesced stores (the per-view work — rotation, scales, SH —
+// does not share between views anyway).
+__global__ void __launch_bounds__(128, 8) k_project(DSplats s, const sc_camera* __restrict__ cams, uint32_t n_views,
                                                  uint32_t stride, float4* __restrict__ rec, TileArgs ta,
                                                  uint32_t* __restrict__ depth_keys, uint32_t* __restrict__ ids,
                                                  uint32_t* __restrict__ counts, int precise,
                                                  float4* __restrict__ zero_grad) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t v = blockIdx.y;
+  const uint32_t chunk = blockIdx.x / n_views;
+  const uint32_t v = blockIdx.x - chunk * n_views;
+  const uint32_t i = chunk * blockDim.x + threadIdx.x;
   if (i >= stride) return;
   const bool live = i < s.n;
   float px = 0, py = 0, pz = 0, qw = 1, qx = 0, qy = 0, qz = 0, l0 = 0, l1 = 0, l2 = 0, op = 0, d0 = 0, d1 = 0, d2 = 0;
@@ -271,11 +273,11 @@ sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams,
   TileArgs ta{1, 1, 1, 1, 0, 0};
   if (tl) ta = TileArgs{tl->tile_w, tl->tile_h, (tl->width + tl->tile_w - 1) / tl->tile_w,
                         (tl->height + tl->tile_h - 1) / tl->tile_h, (cull & 1) ? 1u : 0u, (cull & 2) ? 1u : 0u};
-  const uint32_t bs = 128;  // grid: (splats / bs, views)
-  if (n_views > 65535) return sc_fail(ctx, SC_ERR_INVALID_ARG, "too many views");
-  k_project<<<dim3((unsigned)sc_div_up(stride, bs), n_views), bs, 0, ctx->stream>>>(s, d_cams, n_views, stride, rec,
-                                                                                   ta, depth_keys, ids, counts, precise,
-                                                                                   zero_grad);
+  const uint32_t bs = 128;  // grid: (splats / bs) x views CTAs, views innermost
+  const uint64_t blocks = sc_div_up(stride, bs) * (uint64_t)n_views;
+  if (blocks > 0x7FFFFFFFull) return sc_fail(ctx, SC_ERR_INVALID_ARG, "too many splat views for one launch");
+  k_project<<<(unsigned)blocks, bs, 0, ctx->stream>>>(s, d_cams, n_views, stride, rec, ta, depth_keys, ids, counts,
+                                                      precise, zero_grad);
   return sc_check_launch(ctx, "k_project");
 }
 

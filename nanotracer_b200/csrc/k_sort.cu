@@ -249,6 +249,7 @@ namespace sck {
 #define RS_FLAG_PRE (2u << 30)
 #define RS_VAL_MASK ((1u << 30) - 1)
 #define RS_HIST_BLOCKS_PER_SM 4
+#define RS_HIST_UNROLL 8  // keys each histogram thread loads before counting them
 #define RS_MAX_PASSES 8         // 64-bit keys at 8 or 9 bits per pass
 #define RS_HIST_BYTES (RS_MAX_PASSES * 512 * 4)
 
@@ -280,10 +281,24 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const K* __restrict__ ke
   for (int t = threadIdx.x; t < passes * RADIX; t += RS_THREADS) sh[t] = 0;
   __syncthreads();
   const uint64_t n = d_n ? min(*d_n, n_cap) : n_cap;
-  for (uint64_t i = (uint64_t)blockIdx.x * RS_THREADS + threadIdx.x; i < n; i += (uint64_t)gridDim.x * RS_THREADS) {
-    const K k = keys[i];
-    for (int p = 0; p < passes; ++p)
-      atomicAdd(&sh[p * RADIX + ((uint32_t)(k >> (RB * p)) & rs_digit_mask(key_bits, p, RB))], 1u);
+  // RS_HIST_UNROLL independent coalesced loads in flight per thread before
+  // their shared-memory counts: one load per iteration left the kernel bound
+  // on memory latency, not bandwidth
+  const uint64_t step = (uint64_t)gridDim.x * RS_THREADS;
+  for (uint64_t i0 = (uint64_t)blockIdx.x * RS_THREADS + threadIdx.x; i0 < n; i0 += step * RS_HIST_UNROLL) {
+    K k[RS_HIST_UNROLL];
+#pragma unroll
+    for (int u = 0; u < RS_HIST_UNROLL; ++u) {
+      const uint64_t i = i0 + u * step;
+      k[u] = i < n ? keys[i] : K(0);
+    }
+#pragma unroll
+    for (int u = 0; u < RS_HIST_UNROLL; ++u) {
+      if (i0 + u * step < n) {
+        for (int p = 0; p < passes; ++p)
+          atomicAdd(&sh[p * RADIX + ((uint32_t)(k[u] >> (RB * p)) & rs_digit_mask(key_bits, p, RB))], 1u);
+      }
+    }
   }
   __syncthreads();
   for (int t = threadIdx.x; t < passes * RADIX; t += RS_THREADS) {
@@ -624,9 +639,21 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_hist_seg(const uint32_t* __re
   __syncthreads();
   const uint32_t g = blockIdx.y;
   const uint32_t* k0 = keys + (size_t)g * seg_len;
-  for (uint32_t i = blockIdx.x * RS_THREADS + threadIdx.x; i < seg_len; i += gridDim.x * RS_THREADS) {
-    const uint32_t k = k0[i];
-    for (int p = 0; p < passes; ++p) atomicAdd(&sh[p * RADIX + ((k >> (RB * p)) & rs_digit_mask(key_bits, p, RB))], 1u);
+  const uint64_t step = (uint64_t)gridDim.x * RS_THREADS;
+  for (uint64_t i0 = (uint64_t)blockIdx.x * RS_THREADS + threadIdx.x; i0 < seg_len; i0 += step * RS_HIST_UNROLL) {
+    uint32_t k[RS_HIST_UNROLL];
+#pragma unroll
+    for (int u = 0; u < RS_HIST_UNROLL; ++u) {
+      const uint64_t i = i0 + u * step;
+      k[u] = i < seg_len ? k0[i] : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < RS_HIST_UNROLL; ++u) {
+      if (i0 + u * step < seg_len) {
+        for (int p = 0; p < passes; ++p)
+          atomicAdd(&sh[p * RADIX + ((k[u] >> (RB * p)) & rs_digit_mask(key_bits, p, RB))], 1u);
+      }
+    }
   }
   __syncthreads();
   for (int t = threadIdx.x; t < passes * RADIX; t += RS_THREADS) {
