@@ -61,6 +61,21 @@ __device__ __forceinline__ unsigned long long warp_incl_scan_u64(unsigned long l
 // Gather of the scanned values (when src is given): element i < gn is
 // src[(i / seg) seg + idx[i]] — the value of the idx[i]-th element of its
 // segment (a view's counts by splat, read in depth order) — and 0 beyond gn.
+static_assert(SCAN_IPT == 16, "the scan's vector accesses move 16 elements per thread");
+// 16 consecutive u32 through four 16-byte accesses (p 16-byte aligned)
+__device__ __forceinline__ void load_u32x16(const uint32_t* p, uint32_t v[16]) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const uint4 t = reinterpret_cast<const uint4*>(p)[q];
+    v[4 * q] = t.x; v[4 * q + 1] = t.y; v[4 * q + 2] = t.z; v[4 * q + 3] = t.w;
+  }
+}
+__device__ __forceinline__ void store_u32x16(uint32_t* p, const uint32_t v[16]) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    reinterpret_cast<uint4*>(p)[q] = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+}
+
 struct ScanGather {
   const uint32_t* src;
   const uint32_t* idx;
@@ -82,20 +97,32 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan(uint32_t* __restrict__ da
   uint32_t x[SCAN_IPT];
   unsigned long long tsum = 0;
   if (gather.src) {
+    // a thread's SCAN_IPT indices with 16-byte loads when they are all in range
+    // and the array is 16-byte aligned (base is a multiple of SCAN_IPT)
+    uint32_t ix[SCAN_IPT];
+    if (base + SCAN_IPT <= gather.n && (reinterpret_cast<uintptr_t>(gather.idx) & 15) == 0) {
+      load_u32x16(gather.idx + base, ix);
+    } else {
+#pragma unroll
+      for (int k = 0; k < SCAN_IPT; ++k) ix[k] = base + k < gather.n ? gather.idx[base + k] : 0u;
+    }
     uint32_t g = base < gather.n ? (uint32_t)(base / gather.seg) : 0u;  // the segment of element base
 #pragma unroll
     for (int k = 0; k < SCAN_IPT; ++k) {
       const uint64_t i = base + k;
       if (i >= (uint64_t)(g + 1) * gather.seg) ++g;  // a thread's elements cross at most one segment end
-      x[k] = i < gather.n ? gather.src[(size_t)g * gather.seg + gather.idx[i]] : 0u;
+      x[k] = i < gather.n ? gather.src[(size_t)g * gather.seg + ix[k]] : 0u;
       tsum += x[k];
     }
   } else {
+    if (base + SCAN_IPT <= n && (reinterpret_cast<uintptr_t>(data) & 15) == 0) {
+      load_u32x16(data + base, x);
+    } else {
 #pragma unroll
-    for (int k = 0; k < SCAN_IPT; ++k) {
-      x[k] = (base + k < n) ? data[base + k] : 0u;
-      tsum += x[k];
+      for (int k = 0; k < SCAN_IPT; ++k) x[k] = (base + k < n) ? data[base + k] : 0u;
     }
+#pragma unroll
+    for (int k = 0; k < SCAN_IPT; ++k) tsum += x[k];
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   unsigned long long incl = warp_incl_scan_u64(tsum);
@@ -141,10 +168,20 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan(uint32_t* __restrict__ da
   }
   __syncthreads();
   unsigned long long run = s_excl + (warp > 0 ? s_warp[warp - 1] : 0ull) + (incl - tsum);
+  if (base + SCAN_IPT <= n && (reinterpret_cast<uintptr_t>(data) & 15) == 0) {
+    uint32_t o[SCAN_IPT];
 #pragma unroll
-  for (int k = 0; k < SCAN_IPT; ++k) {
-    if (base + k < n) data[base + k] = (uint32_t)run;
-    run += x[k];
+    for (int k = 0; k < SCAN_IPT; ++k) {
+      o[k] = (uint32_t)run;
+      run += x[k];
+    }
+    store_u32x16(data + base, o);
+  } else {
+#pragma unroll
+    for (int k = 0; k < SCAN_IPT; ++k) {
+      if (base + k < n) data[base + k] = (uint32_t)run;
+      run += x[k];
+    }
   }
   // the thread holding the last element publishes the total
   if (total && n > 0 && base <= n - 1 && n - 1 < base + SCAN_IPT) *total = run;
