@@ -404,73 +404,90 @@ sc_status launch_project_backward(sc_ctx* ctx, const DSplats& s, const float4* p
   return sc_check_launch(ctx, "k_project_backward");
 }
 
-// ---------------------------------------------------------------- multi-view gradient sum
+// ---------------------------------------------------------------- per-splat gradient rows
 // Sum of splat i's parameter gradients over n_views views, in the order of the
 // views (project_backward.wgsl:79-304 per view, accumulated like the
-// reference's per-view passes into one gradient buffer).
-struct SplatGrads {
-  float gpos[3], grot[4], gsc[3], gop, gdc[3], grest[45];
-};
+// reference's per-view passes into one gradient buffer), written as its 59
+// gradient rows.  The views are taken in groups of 32, in two phases per group
+// so that the geometric adjoint and the 45 SH-rest sums are never live
+// together: phase 1 runs the geometric adjoint of each view (14 sums in
+// registers) and marks the views it accepts; phase 2 forms the SH-rest sums of
+// the marked views (colour gradient times the basis at the view direction,
+// the same arithmetic as the adjoint's basis) and adds them into this thread's
+// column of a shared-memory block.  Peak register use is that of the larger
+// phase, not of both.
+constexpr int PB_THREADS = 128;
+constexpr int PB_GROUP = 32;  // views per group: one validity bit each
 
-__device__ __forceinline__ void sum_view_grads(const DSplats& s, uint32_t i, const float4* __restrict__ pg,
-                                               uint32_t stride, const sc_camera* __restrict__ cams, uint32_t n_views,
-                                               SplatGrads& G) {
-  const float px = sp_row(s, 0, i), py = sp_row(s, 1, i), pz = sp_row(s, 2, i);
-  const float qw = sp_row(s, 3, i), qx = sp_row(s, 4, i), qy = sp_row(s, 5, i), qz = sp_row(s, 6, i);
-  const float l0 = sp_row(s, 7, i), l1 = sp_row(s, 8, i), l2 = sp_row(s, 9, i);
-  const float opacity = __fdividef(1.0f, 1.0f + __expf(-sp_row(s, 10, i)));
-  float* gpos = G.gpos; float* grot = G.grot; float* gsc = G.gsc; float& gop = G.gop;
-  float* gdc = G.gdc; float* grest = G.grest;
-  for (int k = 0; k < 3; ++k) { gpos[k] = 0.f; gsc[k] = 0.f; gdc[k] = 0.f; }
-  for (int k = 0; k < 4; ++k) grot[k] = 0.f;
-  gop = 0.f;
-#pragma unroll
-  for (int k = 0; k < 45; ++k) grest[k] = 0.f;
-  for (uint32_t v = 0; v < n_views; ++v) {
-    const size_t o = (size_t)v * stride + i;
-    const float4 p2 = pg[3 * o + 2];
-    const float4 p0 = pg[3 * o], p1 = pg[3 * o + 1];
-    if (p0.x == 0.f && p0.y == 0.f && p0.z == 0.f && p1.x == 0.f && p1.y == 0.f && p1.z == 0.f && p2.x == 0.f &&
-        p2.y == 0.f && p2.z == 0.f)
-      continue;  // splat untouched in this view: every gradient term is zero
-    const Cam c = load_cam(cams + v);
-    float basis[15];
-    if (!splat_backward_view<true>(c, px, py, pz, qw, qx, qy, qz, l0, l1, l2, opacity, p0, p1, p2, gpos, grot, gsc,
-                                   gop, basis))
-      continue;
-    gdc[0] += p2.x * SH_C0; gdc[1] += p2.y * SH_C0; gdc[2] += p2.z * SH_C0;
-#pragma unroll
-    for (int k = 0; k < 15; ++k) {
-      grest[k] += p2.x * basis[k]; grest[15 + k] += p2.y * basis[k]; grest[30 + k] += p2.z * basis[k];
-    }
-  }
-}
-
-// ---------------------------------------------------------------- per-splat gradient rows
-__global__ void __launch_bounds__(128, 4) k_project_backward_shards(DSplats s, const float4* __restrict__ pg,
-                                                                 uint32_t stride, const sc_camera* __restrict__ cams,
-                                                                 uint32_t n_views, float* __restrict__ out,
-                                                                 uint32_t n_shards, uint32_t shard,
-                                                                 const uint32_t* __restrict__ skip) {
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(PB_THREADS, 5) k_project_backward_shards(DSplats s, const float4* __restrict__ pg,
+                                                                     uint32_t stride,
+                                                                     const sc_camera* __restrict__ cams,
+                                                                     uint32_t n_views, float* __restrict__ out,
+                                                                     uint32_t n_shards, uint32_t shard,
+                                                                     const uint32_t* __restrict__ skip) {
+  __shared__ float s_rest[45 * PB_THREADS];
+  const uint64_t i = (uint64_t)blockIdx.x * PB_THREADS + threadIdx.x;
   if (i >= (uint64_t)n_shards * shard) return;
   float* dst = out + (i / shard) * SC_NROWS * (uint64_t)shard + i % shard;
-  SplatGrads G;
-  if (i < s.n && !(skip && (*skip & SC_DEVERR_CAPACITY))) {
-    sum_view_grads(s, (uint32_t)i, pg, stride, cams, n_views, G);
-  } else {  // padding splats, or a step whose emission overflowed: contribute nothing
-    for (int k = 0; k < 3; ++k) { G.gpos[k] = 0.f; G.gsc[k] = 0.f; G.gdc[k] = 0.f; }
-    for (int k = 0; k < 4; ++k) G.grot[k] = 0.f;
-    G.gop = 0.f;
+  float* srest = s_rest + threadIdx.x;  // this thread's column: sum k at srest[k * PB_THREADS]
 #pragma unroll
-    for (int k = 0; k < 45; ++k) G.grest[k] = 0.f;
+  for (int k = 0; k < 45; ++k) srest[k * PB_THREADS] = 0.f;
+  float gpos[3] = {0.f, 0.f, 0.f}, grot[4] = {0.f, 0.f, 0.f, 0.f}, gsc[3] = {0.f, 0.f, 0.f}, gop = 0.f;
+  float gdc[3] = {0.f, 0.f, 0.f};
+  // padding splats, or a step whose emission overflowed, contribute nothing
+  if (i < s.n && !(skip && (*skip & SC_DEVERR_CAPACITY))) {
+    const uint32_t si = (uint32_t)i;
+    const float px = sp_row(s, 0, si), py = sp_row(s, 1, si), pz = sp_row(s, 2, si);
+    const float qw = sp_row(s, 3, si), qx = sp_row(s, 4, si), qy = sp_row(s, 5, si), qz = sp_row(s, 6, si);
+    const float l0 = sp_row(s, 7, si), l1 = sp_row(s, 8, si), l2 = sp_row(s, 9, si);
+    const float opacity = __fdividef(1.0f, 1.0f + __expf(-sp_row(s, 10, si)));
+    for (uint32_t g0 = 0; g0 < n_views; g0 += PB_GROUP) {
+      const uint32_t g1 = min(n_views, g0 + (uint32_t)PB_GROUP);
+      uint32_t accepted = 0;
+      for (uint32_t v = g0; v < g1; ++v) {
+        const size_t o = (size_t)v * stride + si;
+        const float4 p2 = pg[3 * o + 2];
+        const float4 p0 = pg[3 * o], p1 = pg[3 * o + 1];
+        if (p0.x == 0.f && p0.y == 0.f && p0.z == 0.f && p1.x == 0.f && p1.y == 0.f && p1.z == 0.f && p2.x == 0.f &&
+            p2.y == 0.f && p2.z == 0.f)
+          continue;  // splat untouched in this view: every gradient term is zero
+        const Cam c = load_cam(cams + v);
+        float basis[15];  // formed again in phase 2
+        if (!splat_backward_view<true>(c, px, py, pz, qw, qx, qy, qz, l0, l1, l2, opacity, p0, p1, p2, gpos, grot,
+                                       gsc, gop, basis))
+          continue;
+        accepted |= 1u << (v - g0);
+        gdc[0] += p2.x * SH_C0; gdc[1] += p2.y * SH_C0; gdc[2] += p2.z * SH_C0;
+      }
+      if (!accepted) continue;
+      float grest[45];
+#pragma unroll
+      for (int k = 0; k < 45; ++k) grest[k] = 0.f;
+      while (accepted) {
+        const uint32_t v = g0 + (uint32_t)(__ffs(accepted) - 1);
+        accepted &= accepted - 1u;
+        const float4 p2 = pg[3 * ((size_t)v * stride + si) + 2];
+        const float4 e = __ldg(reinterpret_cast<const float4*>(cams + v) + 4);  // camera position
+        // the view direction and basis exactly as splat_backward_view<true> forms them
+        const float dx = e.x - px, dy = e.y - py, dz = e.z - pz;
+        const float il = rsqrtf(dx * dx + dy * dy + dz * dz);
+        float basis[15];
+        sh_basis15(dx * il, dy * il, dz * il, basis);
+#pragma unroll
+        for (int k = 0; k < 15; ++k) {
+          grest[k] += p2.x * basis[k]; grest[15 + k] += p2.y * basis[k]; grest[30 + k] += p2.z * basis[k];
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 45; ++k) srest[k * PB_THREADS] += grest[k];
+    }
   }
-  const float gg[14] = {G.gpos[0], G.gpos[1], G.gpos[2], G.grot[0], G.grot[1], G.grot[2], G.grot[3],
-                        G.gsc[0],  G.gsc[1],  G.gsc[2],  G.gop,     G.gdc[0],  G.gdc[1],  G.gdc[2]};
+  const float gg[14] = {gpos[0], gpos[1], gpos[2], grot[0], grot[1], grot[2], grot[3],
+                        gsc[0],  gsc[1],  gsc[2],  gop,     gdc[0],  gdc[1],  gdc[2]};
 #pragma unroll
   for (int r = 0; r < 14; ++r) dst[(size_t)r * shard] = gg[r];
 #pragma unroll
-  for (int k = 0; k < 45; ++k) dst[(size_t)(SC_ROW_REST + k) * shard] = G.grest[k];
+  for (int k = 0; k < 45; ++k) dst[(size_t)(SC_ROW_REST + k) * shard] = srest[k * PB_THREADS];
 }
 
 sc_status launch_project_backward_shards(sc_ctx* ctx, const DSplats& s, const float4* pg, uint32_t stride,
@@ -478,8 +495,8 @@ sc_status launch_project_backward_shards(sc_ctx* ctx, const DSplats& s, const fl
                                          uint32_t shard, const uint32_t* d_skip) {
   const uint64_t total = (uint64_t)n_shards * shard;
   if (total == 0) return SC_OK;
-  k_project_backward_shards<<<(unsigned)sc_div_up(total, 128), 128, 0, ctx->stream>>>(s, pg, stride, d_cams, n_views,
-                                                                                      grads, n_shards, shard, d_skip);
+  k_project_backward_shards<<<(unsigned)sc_div_up(total, PB_THREADS), PB_THREADS, 0, ctx->stream>>>(
+      s, pg, stride, d_cams, n_views, grads, n_shards, shard, d_skip);
   return sc_check_launch(ctx, "k_project_backward_shards");
 }
 
