@@ -265,7 +265,8 @@ def run_ours(args):
     fwd_list = bw.get("fwd_scanned", 0) * 8 + bw.get("fwd_blended", 0) * 48  # item words + blended records
     bwd_list = bw.get("bwd_scanned", 0) * 8 + bw.get("bwd_blended", 0) * 48
     algo = {
-        "project": N * (56 + rest_b) + V * N * (48 + 8 + 4 + 4),
+        # records, zeroed gradient records, depth key, id, item count
+        "project": N * (56 + rest_b) + V * N * (48 + 48 + 4 + 4 + 4),
         "depth_sort": 5 * V * N * 24,
         "count_scan": V * N * (4 + 4 + 4) + V * N * 8,
         "emit": V * N * (4 + 16 + 4) + K * 8,
