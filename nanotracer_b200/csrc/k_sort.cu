@@ -464,28 +464,62 @@ __device__ __forceinline__ void rs_pass_tile(RsSmem<K, RB>& sm, const K* __restr
 #pragma unroll
   for (int j = 0; j < DPT; ++j)
     st_relaxed_u32(&lb[threadIdx.x * DPT + j], (tile == 0 ? RS_FLAG_PRE : RS_FLAG_AGG) | cnt[j]);
+  // with several digits per thread the digits walk back in lockstep, so their
+  // status loads are in flight together instead of one chain after another
   uint32_t excl[DPT];
 #pragma unroll
-  for (int j = 0; j < DPT; ++j) {
-    const int d = threadIdx.x * DPT + j;
-    excl[j] = 0;
-    if (tile > 0) {
-      long long pred = (long long)tile - 1;
-      unsigned spins = 0;
-      while (pred >= 0) {
-        const unsigned st = ld_relaxed_u32(&lookback[(size_t)pred * RADIX + d]);
-        const unsigned flag = st & ~RS_VAL_MASK;
-        if (flag == 0u) {
-          if (++spins > SC_SPIN_LIMIT) { atomicOr(err, SC_DEVERR_TIMEOUT); break; }
-          __nanosleep(20);
+  for (int j = 0; j < DPT; ++j) excl[j] = 0;
+  if (DPT == 1 && tile > 0) {
+    const int d = threadIdx.x;
+    long long pred = (long long)tile - 1;
+    unsigned spins = 0;
+    while (pred >= 0) {
+      const unsigned st = ld_relaxed_u32(&lookback[(size_t)pred * RADIX + d]);
+      const unsigned flag = st & ~RS_VAL_MASK;
+      if (flag == 0u) {
+        if (++spins > SC_SPIN_LIMIT) { atomicOr(err, SC_DEVERR_TIMEOUT); break; }
+        __nanosleep(20);
+        continue;
+      }
+      excl[0] += st & RS_VAL_MASK;
+      if (flag == RS_FLAG_PRE) break;
+      --pred;
+    }
+    st_relaxed_u32(&lb[d], RS_FLAG_PRE | ((excl[0] + cnt[0]) & RS_VAL_MASK));
+  } else if (DPT > 1 && tile > 0) {
+    long long pred[DPT];
+    bool open[DPT];
+#pragma unroll
+    for (int j = 0; j < DPT; ++j) { pred[j] = (long long)tile - 1; open[j] = true; }
+    unsigned spins = 0;
+    for (;;) {
+      unsigned st[DPT];
+#pragma unroll
+      for (int j = 0; j < DPT; ++j)
+        st[j] = open[j] ? ld_relaxed_u32(&lookback[(size_t)pred[j] * RADIX + threadIdx.x * DPT + j]) : 0u;
+      bool waiting = false, any_open = false;
+#pragma unroll
+      for (int j = 0; j < DPT; ++j) {
+        if (!open[j]) continue;
+        const unsigned flag = st[j] & ~RS_VAL_MASK;
+        if (flag == 0u) {  // predecessor not published yet: poll it again
+          waiting = true;
+          any_open = true;
           continue;
         }
-        excl[j] += st & RS_VAL_MASK;
-        if (flag == RS_FLAG_PRE) break;
-        --pred;
+        excl[j] += st[j] & RS_VAL_MASK;
+        if (flag == RS_FLAG_PRE || --pred[j] < 0) open[j] = false;
+        else any_open = true;
       }
-      st_relaxed_u32(&lb[d], RS_FLAG_PRE | ((excl[j] + cnt[j]) & RS_VAL_MASK));
+      if (!any_open) break;
+      if (waiting) {
+        if (++spins > SC_SPIN_LIMIT) { atomicOr(err, SC_DEVERR_TIMEOUT); break; }
+        __nanosleep(20);
+      }
     }
+#pragma unroll
+    for (int j = 0; j < DPT; ++j)
+      st_relaxed_u32(&lb[threadIdx.x * DPT + j], RS_FLAG_PRE | ((excl[j] + cnt[j]) & RS_VAL_MASK));
   }
   // tile-local exclusive scan of the digit counts (DPT consecutive digits per thread)
   {
