@@ -206,9 +206,11 @@ __device__ __forceinline__ void adam_row8(Row8& x, float a, float s2, const Adam
 }
 
 // GEOM: the 9 geometric row groups (grid.y 0..8); otherwise the 45 sh_rest
-// rows (grid.y 0..44), a separate launch with its own, smaller register count
+// rows (grid.y 0..44), a separate launch with its own, smaller register count.
+// The geometric launch is held to 3 CTAs per SM (80 registers, a few bytes
+// spilled in the rotation group): more rows in flight beat the spill.
 template <bool GEOM>
-__global__ void __launch_bounds__(256, GEOM ? 1 : 4) k_adam_rows(DSplats s, DMoments mo, float* __restrict__ acc,
+__global__ void __launch_bounds__(256, GEOM ? 3 : 4) k_adam_rows(DSplats s, DMoments mo, float* __restrict__ acc,
                                                    const float* __restrict__ g, uint32_t lo, uint32_t count,
                                                    uint32_t gstride, AdamParams ap, const float* __restrict__ d_bc,
                                                    const uint32_t* __restrict__ skip) {
