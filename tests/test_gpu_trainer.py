@@ -207,6 +207,39 @@ def test_two_level_binning_equals_the_pair_sort(ctx, tile):
     assert np.allclose(g1.readback().flat(), g2.readback().flat(), rtol=1e-5, atol=1e-7)
 
 
+def test_full_size_binning_paths_agree(ctx):
+    """The bench workload's sizes (1M splats, 8 views of 1920x1080, 16x16
+    tiles), where the CPU oracle does not finish in seconds, checked through
+    properties that hold at any size: the two-level binning and the stable
+    pair sort blend the same splats in the same order (images bit for bit, the
+    same pair count and loss), both equal the 64-bit (tile, depth)
+    reference-order binning's images, and the blend work counters stay within
+    each other and the pair count."""
+    scene, tl, cams, tgt, cfg = _setup(ctx, n=1_000_000, W=1920, H=1080, V=8, seed=5)
+    tr2, g2, mo2, acc2, l2 = _run(ctx, scene, cams, tgt, cfg)
+    img2 = tr2.images()
+    pairs2 = tr2.stats()["pairs"]
+    tr1, _, _, _, l1 = _run(ctx, scene, cams, tgt, TrainConfig(**{**cfg.__dict__, "sort_mode": 1}))
+    assert np.array_equal(tr1.images(), img2)
+    assert tr1.stats()["pairs"] == pairs2 > 100_000_000
+    assert np.allclose(l1, l2, rtol=1e-9)
+    del tr1
+    pipe = GpuPipe(ctx, scene, cams, tl, key_mode=SC_KEYS_NATIVE64)
+    pipe.project()
+    pipe.bin()
+    ref_img, _ = pipe.composite()
+    assert np.array_equal(ref_img, img2)
+    del pipe
+    tr2.set_profiling(True)
+    tr2.step(g2, mo2, acc2, cams, 2)
+    st = tr2.stats()
+    w = st["blend_work"]
+    assert 0 < w["fwd_blended"] <= w["fwd_scanned"] <= st["items"] * 16
+    assert 0 < w["bwd_blended"] <= w["bwd_scanned"] <= w["fwd_scanned"]
+    assert w["bwd_blended"] <= w["fwd_blended"] <= st["pairs"]
+    tr2.set_profiling(False)
+
+
 def test_blend_work_counters_bound_each_other(ctx):
     """sc_trainer_blend_work while profiling: the forward blends only entries of
     the list positions it scans, the backward walks no further than the
