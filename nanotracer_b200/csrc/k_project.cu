@@ -5,14 +5,17 @@
 // sigmoid opacity).  The 2D covariance is formed as B B^T with
 // B = J W R diag(sigma) (2x3), which is algebraically the reference's
 // J (W R S^2 R^T W^T) J^T with fewer operations.  One thread per (splat,
-// view), the view on the grid's y axis: 70 registers instead of the 128 of a
-// thread looping over the views (0.58 against 0.67 ms at 1M splats and 8
-// views); a splat's parameters are read from L2 by its views after the first.
+// view), consecutive CTAs taking the views of one 128-splat chunk: 64
+// registers instead of the 128 of a thread looping over the views, and a
+// splat's parameters are read from L2 by its views after the first (0.56 ms
+// at 1M splats and 8 views; 0.62 ms with the views on the grid's slow axis,
+// each view streaming the parameters from DRAM).
 //
 // Backward: project_backward.wgsl:79-304, with the same omissions as the
 // reference (no dJ/dt in the position gradient, no SH view-direction
 // gradient, no colour-clamp gate).  One thread per splat sums the per-view
-// gradients in registers and writes the splat's 59 gradient rows once
+// gradients (geometric sums in registers, the 45 SH-rest sums in a
+// shared-memory column) and writes the splat's 59 gradient rows once
 // (coefficient-major, cut into shards for the data-parallel path); Adam then
 // streams over those rows (k_adam.cu).  A single kernel doing both held 59
 // gradients and the Adam state of one splat per thread at 128 registers and
