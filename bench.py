@@ -184,11 +184,19 @@ def run_ours(args):
     # orbit advances each step; targets are re-rendered per distinct step in e2e)
     cams0 = cams_for(0)
     tgt0 = render_targets(ctx, tscene, cams0, tl)
+    tbuf = ctx.storage_buffer("targets", tgt0)
+    tune = None
+    if args.autotune:  # untimed: scratch copies of the scene, before the timed trainer exists
+        from nanotracer_b200.autotune import autotune
+        cfg, trials = autotune(ctx, scene, cams0, tbuf, cfg)
+        tune = {"choice": f"{cfg.tile_w}x{cfg.tile_h} tiles, sort_mode {cfg.sort_mode}",
+                "trial_ms": {f"{t.tile_w}x{t.tile_h}/sort_mode {t.sort_mode}":
+                             (round(t.ms, 3) if t.ms is not None else t.error) for t in trials}}
+        tl = nt.TilingParams(args.width, args.height, cfg.tile_w, 8.0, tile_h_override=cfg.tile_h)
     g = nt.GpuSplatBuffer.upload(ctx, scene, bf16_rest=bf16)
     mo = nt.AdamMomentBuffers(ctx, g.capacity, bf16=bf16)
     acc = ctx.storage_buffer_zeroed("grad_acc", 4 * g.capacity)
     tr = Trainer(ctx, cfg)
-    tbuf = ctx.storage_buffer("targets", tgt0)
     tr.set_targets(tbuf)
     cams_steps = [cams_for(s) for s in range(args.warmup + args.steps)]
     clk = ClockSampler(local, raw_copy=os.environ.get("BENCH_CLOCKS_CSV")).start()
@@ -308,7 +316,7 @@ def run_ours(args):
             "data": "synthetic seeded scene and targets (no dataset)",
             "config": {"workload": f"{N} splats, {V} views x {args.width}x{args.height} per iteration"
                                    f"{' per GPU (one scene per GPU)' if ws > 1 else ''}, "
-                                   f"{args.tile_w}x{args.tile_h} tiles, exact transmittance backward, CUDA graph",
+                                   f"{cfg.tile_w}x{cfg.tile_h} tiles, exact transmittance backward, CUDA graph",
                        "form": "batched-" + ("bf16" if bf16 else "fp32"), "splats": N, "views_per_iter": V,
                        "width": args.width, "height": args.height, "pairs_per_iter": K, "items_per_iter": items,
                        "l2": "inputs larger than L2 (params, item lists and images >> 126 MB)",
@@ -316,6 +324,8 @@ def run_ours(args):
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clocks, "loss": loss, "psnr": psnr,
         }
+        if tune is not None:
+            line["config"]["autotune"] = tune
         print(json.dumps(line))
     del tr
     if pg is not None:
@@ -573,6 +583,8 @@ def main():
     ap.add_argument("--parallel", default="views", choices=["views", "scenes"],
                     help="N>1: split each iteration's views over the GPUs (strong), or one scene per GPU (weak)")
     ap.add_argument("--view-path", action="store_true", help="run the split-views path even on one GPU")
+    ap.add_argument("--autotune", action="store_true",
+                    help="time every tile shape x binning path first (untimed) and run the fastest")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-psnr", action="store_true", help="skip the untimed BF16-vs-FP32 PSNR side run")
