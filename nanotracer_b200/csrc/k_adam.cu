@@ -5,7 +5,9 @@
 // Adam runs over the coefficient-major slab: one elementwise pass over the 59
 // rows with the row's learning-rate group; bias corrections bc1/bc2 come from
 // the host in f32 (adam_gpu.rs:275-276).  With bf16 storage the moments (and
-// SH-rest parameters) are widened to f32 for the update and rounded back.
+// SH-rest parameters) are widened to f32 for the update and rounded back: the
+// moments to nearest, the parameters stochastically (bf16_stochastic), since
+// an update below half a BF16 ulp would otherwise be lost every step.
 //
 // Prune and densify reproduce the reference's swap_remove order exactly.
 // Removing a set R of m indices from n by swap_remove in descending index
@@ -62,7 +64,7 @@ __global__ void k_adam_all(DSplats s, const float* __restrict__ g, uint32_t gcap
     else { mo.m[k] = mn; mo.v[k] = vn; }
     const float mh = mn / ap.bc1, vh = vn / ap.bc2;
     const float p = sp_row(s, r, i);
-    sp_set(s, r, i, p - lr * mh / (sqrtf(vh) + ap.eps));
+    sp_set_sr(s, r, i, p - lr * mh / (sqrtf(vh) + ap.eps), ap.seed);
   }
 }
 
@@ -148,6 +150,18 @@ __device__ __forceinline__ void st8(__nv_bfloat16* p, const float* o) {
   *reinterpret_cast<uint4*>(p) = make_uint4(w[0], w[1], w[2], w[3]);
 }
 
+// BF16 parameters of splats i0 .. i0+7 of row r, stochastically rounded
+__device__ __forceinline__ void st8_sr(__nv_bfloat16* p, const float* o, uint32_t seed, int r, uint32_t i0) {
+  uint32_t w[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const __nv_bfloat16 lo = bf16_stochastic(o[2 * k], sr_bits(seed, r, i0 + 2 * k));
+    const __nv_bfloat16 hi = bf16_stochastic(o[2 * k + 1], sr_bits(seed, r, i0 + 2 * k + 1));
+    w[k] = (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+  }
+  *reinterpret_cast<uint4*>(p) = make_uint4(w[0], w[1], w[2], w[3]);
+}
+
 // one row of 8 splats: parameters, moments and gradients widened to f32;
 // `nv` < 8 loads (and later stores) only the first nv splats
 struct Row8 {
@@ -175,18 +189,19 @@ __device__ __forceinline__ void load_row8(const DSplats& s, const DMoments& mo, 
   }
 }
 __device__ __forceinline__ void store_row8(const DSplats& s, const DMoments& mo, int r, uint32_t i0, int nv,
-                                           const Row8& x) {
+                                           const Row8& x, uint32_t seed) {
   const size_t pk = (size_t)r * s.cap + i0, mk = (size_t)r * mo.cap + i0;
   const bool rest16 = r >= SC_ROW_REST && s.bf16;
   if (nv == ADAM_SPT) {
-    if (rest16) st8(s.rest16 + (size_t)(r - SC_ROW_REST) * s.cap + i0, x.p); else st8(s.slab + pk, x.p);
+    if (rest16) st8_sr(s.rest16 + (size_t)(r - SC_ROW_REST) * s.cap + i0, x.p, seed, r, i0);
+    else st8(s.slab + pk, x.p);
     if (mo.bf16) { st8(mo.m16 + mk, x.m); st8(mo.v16 + mk, x.v); } else { st8(mo.m + mk, x.m); st8(mo.v + mk, x.v); }
     return;
   }
 #pragma unroll
   for (int e = 0; e < ADAM_SPT; ++e) {
     if (e < nv) {
-      sp_set(s, r, i0 + e, x.p[e]);
+      sp_set_sr(s, r, i0 + e, x.p[e], seed);
       mo_st(mo, mo.m, mo.m16, mk + e, x.m[e]);
       mo_st(mo, mo.v, mo.v16, mk + e, x.v[e]);
     }
@@ -217,7 +232,7 @@ __global__ void __launch_bounds__(256, GEOM ? 3 : 4) k_adam_rows(DSplats s, DMom
   const uint32_t j0 = (blockIdx.x * blockDim.x + threadIdx.x) * ADAM_SPT;
   if (j0 >= count) return;
   if (skip && (*skip & SC_DEVERR_CAPACITY)) return;  // a capacity overflow earlier in the step: leave parameters untouched
-  if (d_bc) { ap.bc1 = d_bc[0]; ap.bc2 = d_bc[1]; }
+  if (d_bc) { ap.bc1 = d_bc[0]; ap.bc2 = d_bc[1]; ap.seed = __float_as_uint(d_bc[2]); }  // [2]: the step's bits
   const AdamFast af = adam_fast(ap);
   const int nv = (int)min((uint32_t)ADAM_SPT, count - j0);
   const uint32_t i0 = lo + j0;
@@ -232,7 +247,7 @@ __global__ void __launch_bounds__(256, GEOM ? 3 : 4) k_adam_rows(DSplats s, DMom
 #pragma unroll
       for (int e = 0; e < ADAM_SPT; ++e) st[e] = st[e] + fabsf(x.g[e]);
       adam_row8(x, af.a[0], af.s2, ap);
-      store_row8(s, mo, r, i0, nv, x);
+      store_row8(s, mo, r, i0, nv, x, ap.seed);
     }
     if (acc) {
 #pragma unroll
@@ -245,7 +260,7 @@ __global__ void __launch_bounds__(256, GEOM ? 3 : 4) k_adam_rows(DSplats s, DMom
     for (int c = 0; c < 4; ++c) {
       load_row8(s, mo, g, SC_ROW_ROT + c, i0, j0, gstride, nv, x);
       adam_row8(x, af.a[1], af.s2, ap);
-      store_row8(s, mo, SC_ROW_ROT + c, i0, nv, x);
+      store_row8(s, mo, SC_ROW_ROT + c, i0, nv, x, ap.seed);
     }
     float q[4][ADAM_SPT];
     for (int c = 0; c < 4; ++c) {
@@ -286,7 +301,7 @@ __global__ void __launch_bounds__(256, GEOM ? 3 : 4) k_adam_rows(DSplats s, DMom
 #pragma unroll
     for (int e = 0; e < ADAM_SPT; ++e) x.p[e] = fminf(fmaxf(x.p[e], -ap.opacity_logit_max), ap.opacity_logit_max);
   }
-  store_row8(s, mo, r, i0, nv, x);
+  store_row8(s, mo, r, i0, nv, x, ap.seed);
 }
 
 sc_status launch_adam_rows(sc_ctx* ctx, const DSplats& s, const DMoments& mo, float* acc, const float* g, uint32_t lo,

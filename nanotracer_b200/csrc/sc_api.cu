@@ -807,6 +807,7 @@ sc_status sc_adam_step_all(sc_ctx* ctx, sc_splats* s, const sc_grads* g, sc_mome
   ap.bc1 = 1.0f - sc_powi_f32(gr->beta1, (int)t);
   ap.bc2 = 1.0f - sc_powi_f32(gr->beta2, (int)t);
   ap.log_scale_min = ap.log_scale_max = ap.opacity_logit_max = 0.0f;
+  ap.seed = (uint32_t)t;
   return sck::launch_adam_all(ctx, dview(s), g->slab, g->cap, dview(mo), ap);
 }
 
@@ -828,6 +829,7 @@ sc_status sc_adam_step_shard(sc_ctx* ctx, sc_splats* s, sc_moments* mo, float* a
   ap.bc1 = 1.0f - sc_powi_f32(gr->beta1, (int)t);
   ap.bc2 = 1.0f - sc_powi_f32(gr->beta2, (int)t);
   ap.log_scale_min = lsmin; ap.log_scale_max = lsmax; ap.opacity_logit_max = opmax;
+  ap.seed = (uint32_t)t;
   return sck::launch_adam_shard(ctx, dview(s), dview(mo), acc, g, lo, count, shard, ap);
 }
 

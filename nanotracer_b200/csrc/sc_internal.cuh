@@ -262,7 +262,43 @@ struct AdamParams {
   float lr[6];
   float beta1, beta2, eps, bc1, bc2;
   float log_scale_min, log_scale_max, opacity_logit_max;
+  uint32_t seed = 0;  // the step number: seeds the stochastic rounding of BF16 parameters
 };
+
+// BF16 parameters are written back with stochastic rounding.  An Adam step is
+// about lr (1.25e-4 for the SH-rest group) while a BF16 ulp at the SH-rest
+// coefficients' scale (~0.05) is 2.4e-4, so round-to-nearest would discard
+// most updates; adding uniform bits below the BF16 mantissa before truncating
+// rounds up or down with probabilities proportional to the distance, so the
+// stored value equals the f32 update in expectation.  The bits come from a
+// hash of (step, row, splat index): deterministic, and the same on every rank
+// of the data-parallel path, which updates a splat with its global index.
+__device__ __forceinline__ uint32_t sr_hash(uint32_t x) {
+  // integer finaliser of Wellons' "lowbias32" (two xorshift-multiply rounds)
+  x ^= x >> 16; x *= 0x7feb352du;
+  x ^= x >> 15; x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+__device__ __forceinline__ uint32_t sr_bits(uint32_t seed, int row, uint32_t i) {
+  return sr_hash(i * 0x9E3779B1u ^ sr_hash(seed * 0x85EBCA77u + (uint32_t)row));
+}
+__device__ __forceinline__ __nv_bfloat16 bf16_stochastic(float x, uint32_t rnd) {
+  uint32_t b = __float_as_uint(x);
+  // finite values: add 16 random bits to the magnitude below the kept 16 (the
+  // sign bit is untouched, so negative values round symmetrically); Inf and NaN
+  // pass through by truncation
+  if ((b & 0x7F800000u) != 0x7F800000u) b += rnd & 0xFFFFu;
+  return __ushort_as_bfloat16((unsigned short)(b >> 16));
+}
+// sp_set with stochastic rounding of BF16 rows
+__device__ __forceinline__ void sp_set_sr(const DSplats& s, int r, uint32_t i, float v, uint32_t seed) {
+  if (r >= SC_ROW_REST && s.bf16) {
+    s.rest16[(size_t)(r - SC_ROW_REST) * s.cap + i] = bf16_stochastic(v, sr_bits(seed, r, i));
+    return;
+  }
+  s.slab[(size_t)r * s.cap + i] = v;
+}
 
 // moments widened to / rounded from f32
 __device__ __forceinline__ float mo_ld(const DMoments& mo, const float* f, const __nv_bfloat16* h, size_t k) {

@@ -33,7 +33,7 @@ namespace {
 
 struct StepParams {
   sc_camera cams[SC_MAX_VIEWS];
-  float bc[4];  // bc1, bc2
+  float bc[4];  // bc1, bc2, the step number's bits (stochastic-rounding seed)
 };
 
 struct StepOut {
@@ -661,6 +661,8 @@ sc_status sc_trainer_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, float* a
   std::memcpy(tr->h_params->cams, cams, sizeof(sc_camera) * tr->V);
   tr->h_params->bc[0] = 1.0f - sc_powi_f32(tr->cfg.adam.beta1, (int)t);
   tr->h_params->bc[1] = 1.0f - sc_powi_f32(tr->cfg.adam.beta2, (int)t);
+  const uint32_t seed = (uint32_t)t;  // the stochastic rounding's seed, read by the Adam kernel as bits
+  std::memcpy(&tr->h_params->bc[2], &seed, sizeof(seed));
   tr->grads_mode = false;
   tr->loss_weight = 0.0f;
   tr->gout = nullptr;

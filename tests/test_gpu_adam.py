@@ -195,3 +195,27 @@ def test_densify_matches_oracle_swap_remove_order(ctx, oracle, n, max_splats, it
     gm, gv = mo.download(g.n)
     assert np.array_equal(gm.flat(), om.flat()) and np.array_equal(gv.flat(), ov.flat())
     assert np.array_equal(accb.readback(np.float32, g.n), oacc[: g.n])
+
+
+def test_bf16_parameters_round_stochastically_so_small_updates_survive(ctx):
+    """With BF16 SH-rest storage, an Adam step smaller than half a BF16 ulp
+    would vanish under round-to-nearest.  The parameters are written back with
+    stochastic rounding instead: each coefficient moves by one ulp or not at
+    all, and over many coefficients the mean change equals the f32 update."""
+    n, lr = 4096, 1e-5
+    flat = np.zeros((n, 59), np.float32)
+    flat[:, 3] = 1.0                  # unit quaternions
+    flat[:, 14:] = 0.05               # SH rest: BF16 spacing 2^-12 = 2.4e-4 here
+    g = GpuSplatBuffer.upload(ctx, SplatBuffer.from_flat(flat), bf16_rest=True)
+    before = g.readback().flat()[:, 14:].astype(np.float64)
+    gflat = np.zeros((n, 59), np.float32)
+    gflat[:, 14:] = 1.0               # first Adam step: every SH-rest value moves by -lr in f32
+    grads = GradSplatBuffers(ctx, n)
+    grads.upload(SplatBuffer.from_flat(gflat))
+    mo = AdamMomentBuffers(ctx, n)
+    AdamGpu(ctx).step_all(g, grads, mo, 1, AdamConfig(lr=lr))
+    d = g.readback().flat()[:, 14:].astype(np.float64) - before
+    ulp = 2.0 ** -12
+    assert np.all((d == 0.0) | (d == -ulp))
+    # mean of 184,320 draws with p = lr / ulp: standard error 1.1e-7, bound 5e-7
+    assert abs(d.mean() + lr) < 0.05 * lr
