@@ -290,8 +290,12 @@ sc_status sc_tonemap(sc_ctx* ctx, const float* image, uint32_t width, uint32_t h
  * replaces AdamGpu (crates/nano-optimize/src/adam_gpu.rs:31-547) */
 sc_status sc_adam_step(sc_ctx* ctx, float* params, const float* grads, float* m, float* v, uint64_t n,
                        float lr, uint64_t t, const sc_adam_config* cfg);   /* AdamGpu::step, :224-323 */
+/* AdamGpu::step_all, :334-427.  With SC_SPLATS_BF16_REST storage the SH-rest
+ * parameters are written back with stochastic rounding seeded by t (this call,
+ * sc_adam_step_shard and sc_trainer_step alike), so updates smaller than half
+ * a BF16 ulp survive in expectation; the same t gives the same bits. */
 sc_status sc_adam_step_all(sc_ctx* ctx, sc_splats* s, const sc_grads* g, sc_moments* mo, uint64_t t,
-                           const sc_adam_groups* groups);                  /* AdamGpu::step_all, :334-427 */
+                           const sc_adam_groups* groups);
 sc_status sc_apply_constraints(sc_ctx* ctx, sc_splats* s, float log_scale_min, float log_scale_max,
                                float opacity_logit_max);                   /* :431-489 */
 sc_status sc_accumulate_grad(sc_ctx* ctx, const sc_grads* g, float* grad_acc, uint32_t n); /* :492-541 */
