@@ -88,6 +88,37 @@ def test_trainer_step_matches_oracle_iteration(ctx, oracle, exact):
     assert np.allclose(gacc, oacc, rtol=2e-3, atol=1e-9 + 1e-3 * np.abs(oacc).max())
 
 
+def test_bf16_and_fp32_forms_within_0p05_db_of_the_fp64_oracle(ctx, oracle):
+    """The precision target at a size the CPU finishes in seconds (2000
+    splats, 2 views of 64x64): after 30 iterations from the same start, the
+    PSNR of the BF16-storage form's images against the targets is within
+    0.05 dB of the PSNR of the oracle's own run in f64 arithmetic, and so is
+    the FP32 form's.  Images are each run's forward at the last iteration."""
+    K, W, H = 30, 64, 64
+    scene, tl, cams, tgt, cfg = _setup(ctx, n=2000, W=W, H=H, V=2, seed=9)
+    t3 = np.asarray(tgt, np.float64).reshape(-1, 3)
+
+    def psnr(img4):
+        x = np.asarray(img4, np.float64).reshape(-1, 4)[:, :3]
+        return 10.0 * math.log10(1.0 / np.mean((x - t3) ** 2))
+
+    p = {}
+    for name, bf16 in (("fp32", False), ("bf16", True)):
+        tr, *_ = _run(ctx, scene, cams, tgt, TrainConfig(**{**cfg.__dict__, "bf16": bf16}), steps=K)
+        p[name] = psnr(tr.images())
+    os_ = oracle.OSplats.from_buffer(scene)
+    om, ov = oracle.OSplats.zeros(len(scene)), oracle.OSplats.zeros(len(scene))
+    oacc = np.zeros(len(scene), np.float32)
+    ocams = [oracle.camera_from_struct(bytes(c.c)) for c in cams]
+    otl = oracle.tiling(W, H, 16, 16, 8.0)
+    for t in range(1, K + 1):
+        _, oimgs = oracle.train_step(os_, om, ov, oacc, ocams, tgt, otl, 1, BENCH_LRS, t, sfx="f64",
+                                     want_images=(t == K))
+    p["fp64"] = psnr(oimgs)
+    assert abs(p["bf16"] - p["fp64"]) <= 0.05, p
+    assert abs(p["fp32"] - p["fp64"]) <= 0.05, p
+
+
 def test_trainer_graph_replay_equals_eager(ctx):
     scene, tl, cams, tgt, cfg = _setup(ctx, n=2000)
     cfg_e = TrainConfig(**{**cfg.__dict__, "use_graph": False})
