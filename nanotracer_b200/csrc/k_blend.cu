@@ -447,24 +447,6 @@ sc_status launch_composite_items(sc_ctx* ctx, const float4* rec, uint32_t stride
 }
 
 // ---------------------------------------------------------------- MSE (standalone)
-__global__ void k_mse(const float4* __restrict__ pred, const float* __restrict__ target, uint64_t P, uint32_t n_views,
-                      float gscale, float4* __restrict__ dl_dc, double* __restrict__ loss) {
-  __shared__ double sred[8];
-  const uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t v = (uint32_t)(((uint64_t)blockIdx.x * blockDim.x) / P);  // blocks never straddle views
-  double sq = 0.0;
-  if (q < P * n_views) {
-    const float4 p = pred[q];
-    const float dx = p.x - target[3 * q], dy = p.y - target[3 * q + 1], dz = p.z - target[3 * q + 2];
-    dl_dc[q] = make_float4(dx * gscale, dy * gscale, dz * gscale, 0.0f);
-    sq = (double)(dx * dx + dy * dy + dz * dz);
-  }
-  if (loss) {
-    const double s = block_sum(sq, sred);
-    if (threadIdx.x == 0 && s != 0.0) atomicAdd(&loss[v], s);
-  }
-}
-
 __global__ void k_mse_views(const float4* __restrict__ pred, const float* __restrict__ target, uint64_t P,
                             float gscale, float4* __restrict__ dl_dc, double* __restrict__ loss) {
   __shared__ double sred[8];
@@ -491,7 +473,7 @@ sc_status launch_mse(sc_ctx* ctx, const float4* pred, const float* target, uint6
   const float gscale = (2.0f / n_scalars) * scale;
   dim3 grid((unsigned)sc_div_up(P, 256), n_views);
   k_mse_views<<<grid, 256, 0, ctx->stream>>>(pred, target, P, gscale, dl_dc, loss);
-  return sc_check_launch(ctx, "k_mse");
+  return sc_check_launch(ctx, "k_mse_views");
 }
 
 // ---------------------------------------------------------------- backward
