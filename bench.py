@@ -33,7 +33,6 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "fwd+bwd+Adam iters/s @1M splats 1080p: batched-BF16 vs plain FP32, same PSNR"
 UNIT = "iters/s"
-PEAKS = {"hbm_gbs": 6537.6, "bf16_tflops": 1654.7, "source": "measured"}
 
 
 def profiled_traffic(kernel: str, views: int):
