@@ -190,7 +190,10 @@ void sc_camera_from_pose(const float eye[3], const float target[3], const float 
                          sc_camera* out);                            /* CameraUniform::from_pose, raster.rs:79-99 */
 
 /* project_gaussians.wgsl:156-259 for n_views cameras: projected holds
- * n_views * sc_splats_capacity() records, view-major. */
+ * n_views * sc_splats_capacity() records, view-major.  The reference forms
+ * det = s00 s11 - s01^2 in f32 and culls det <= 0 (:226-234); with
+ * sc_ctx_set_fp64_det a near-degenerate splat (det < 2^-10 s00 s11 in f32)
+ * gets its determinant and conic in FP64 instead. */
 sc_status sc_project(sc_ctx* ctx, const sc_splats* s, const sc_camera* cams, uint32_t n_views,
                      sc_projected_splat* projected);                 /* Rasterizer::project, raster.rs:731-794 */
 
@@ -283,6 +286,16 @@ sc_status sc_project_backward(sc_ctx* ctx, const sc_splats* s, const sc_projecte
                               const sc_camera* cam, sc_grads* grads,
                               int accumulate);                       /* Rasterizer::project_backward, raster.rs:559-645 */
 
+/* Precision option of sc_project and sc_project_backward (off by default,
+ * which is the reference's f32 arithmetic): when enabled, a splat whose f32
+ * 2x2 projected-covariance determinant keeps less than 2^-10 of s00 s11
+ * (a needle-like splat, where cancellation has eaten the f32 determinant)
+ * gets the determinant from Lagrange's identity det = |B0 x B1|^2 +
+ * 0.3 (|B0|^2 + |B1|^2) + 0.09 (Sigma2D = B B^T + 0.3 I) and the inverse in
+ * FP64; the adjoint recomputes the same FP64 conic.  No counterpart in the
+ * reference (project_gaussians.wgsl:226-234, project_backward.wgsl:127-139). */
+sc_status sc_ctx_set_fp64_det(sc_ctx* ctx, int enabled);
+
 /* tonemap.wgsl:27-41 into a headless RGBA8 buffer (viewer path). */
 sc_status sc_tonemap(sc_ctx* ctx, const float* image, uint32_t width, uint32_t height, uint8_t* rgba8);
 
@@ -337,6 +350,8 @@ typedef struct sc_train_config {
   float log_scale_min, log_scale_max, opacity_logit_max; /* train.rs:37-39 */
   float ssim_lambda;           /* loss = (1 - l) MSE + l (1 - SSIM), loss.rs:383-410 (TrainConfig::ssim_lambda,
                                   train.rs:52); 0 = MSE only, fused into the blend */
+  uint32_t fp64_det;           /* FP64 determinant and inverse of near-degenerate splats in the projection
+                                  and its adjoint (as sc_ctx_set_fp64_det) */
 } sc_train_config;
 
 sc_status sc_trainer_create(sc_ctx* ctx, const sc_train_config* cfg, sc_trainer** out);

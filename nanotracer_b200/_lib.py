@@ -60,7 +60,7 @@ class sc_train_config(C.Structure):
                 ("use_graph", C.c_uint32), ("blend_batch", C.c_uint32), ("sort_mode", C.c_uint32),
                 ("tile_cull", C.c_uint32),
                 ("log_scale_min", C.c_float), ("log_scale_max", C.c_float), ("opacity_logit_max", C.c_float),
-                ("ssim_lambda", C.c_float)]
+                ("ssim_lambda", C.c_float), ("fp64_det", C.c_uint32)]
 
 
 assert C.sizeof(sc_camera) == 96
@@ -84,6 +84,7 @@ _PROTOS = {
     "sc_ctx_set_stream": (ST, [P, P]),
     "sc_ctx_device_info": (ST, [P, C.POINTER(I32), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     "sc_ctx_launch_count": (U64, [P]),
+    "sc_ctx_set_fp64_det": (ST, [P, I32]),
     "sc_buffer_alloc": (ST, [P, C.c_size_t, C.POINTER(P)]),
     "sc_buffer_free": (ST, [P, P]),
     "sc_buffer_upload": (ST, [P, P, P, C.c_size_t]),

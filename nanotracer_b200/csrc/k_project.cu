@@ -13,9 +13,11 @@
 //
 // Backward: project_backward.wgsl:79-304, with the same omissions as the
 // reference (no dJ/dt in the position gradient, no SH view-direction
-// gradient, no colour-clamp gate).  One thread per splat sums the per-view
-// gradients (geometric sums in registers, the 45 SH-rest sums in a
-// shared-memory column) and writes the splat's 59 gradient rows once
+// gradient, no colour-clamp gate).  With the FP64 determinant option the
+// adjoint recomputes the same FP64 conic as the forward, so dSigma2D =
+// -C dConic C differentiates the conic the blend used.  One thread per splat
+// sums the per-view gradients (geometric sums in registers, the 45 SH-rest
+// sums in a shared-memory column) and writes the splat's 59 gradient rows once
 // (coefficient-major, cut into shards for the data-parallel path); Adam then
 // streams over those rows (k_adam.cu).  A single kernel doing both held 59
 // gradients and the Adam state of one splat per thread at 128 registers and
@@ -293,9 +295,9 @@ __device__ __forceinline__ bool splat_backward_view(const Cam& c, float px, floa
                                                     float qy, float qz, float l0, float l1, float l2, float opacity,
                                                     const float4 pg0, const float4 pg1, const float4 pg2,
                                                     float gpos[3], float grot[4], float gsc[3], float& gop,
-                                                    float basis[15]) {
+                                                    float basis[15], int precise) {
   Geo g;
-  if (!geometry<FAST>(c, px, py, pz, qw, qx, qy, qz, l0, l1, l2, 0, g)) return false;
+  if (!geometry<FAST>(c, px, py, pz, qw, qx, qy, qz, l0, l1, l2, precise, g)) return false;
   const float f = c.focal;
   const float iz = gdiv<FAST>(1.0f, g.tz), iz2 = iz * iz;
   // opacity logit
@@ -369,7 +371,7 @@ __device__ __forceinline__ bool splat_backward_view(const Cam& c, float px, floa
 
 __global__ void __launch_bounds__(128) k_project_backward(DSplats s, const float4* __restrict__ pg,
                                                           const sc_camera* __restrict__ cam, float* __restrict__ out,
-                                                          uint32_t gcap, int accumulate) {
+                                                          uint32_t gcap, int accumulate, int precise) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= s.n) return;
   const Cam c = load_cam(cam);
@@ -378,7 +380,8 @@ __global__ void __launch_bounds__(128) k_project_backward(DSplats s, const float
   const float op = 1.0f / (1.0f + expf(-sp_row(s, 10, i)));
   const bool ok = splat_backward_view<false>(c, sp_row(s, 0, i), sp_row(s, 1, i), sp_row(s, 2, i), sp_row(s, 3, i),
                                       sp_row(s, 4, i), sp_row(s, 5, i), sp_row(s, 6, i), sp_row(s, 7, i),
-                                      sp_row(s, 8, i), sp_row(s, 9, i), op, p0, p1, p2, gpos, grot, gsc, gop, basis);
+                                      sp_row(s, 8, i), sp_row(s, 9, i), op, p0, p1, p2, gpos, grot, gsc, gop, basis,
+                                      precise);
   float row[SC_NROWS];
 #pragma unroll
   for (int r = 0; r < SC_NROWS; ++r) row[r] = 0.f;
@@ -401,9 +404,10 @@ __global__ void __launch_bounds__(128) k_project_backward(DSplats s, const float
 }
 
 sc_status launch_project_backward(sc_ctx* ctx, const DSplats& s, const float4* pg, const sc_camera* d_cam,
-                                  float* grads, uint32_t gcap, int accumulate) {
+                                  float* grads, uint32_t gcap, int accumulate, int precise_det) {
   if (s.n == 0) return SC_OK;
-  k_project_backward<<<(unsigned)sc_div_up(s.n, 128), 128, 0, ctx->stream>>>(s, pg, d_cam, grads, gcap, accumulate);
+  k_project_backward<<<(unsigned)sc_div_up(s.n, 128), 128, 0, ctx->stream>>>(s, pg, d_cam, grads, gcap, accumulate,
+                                                                             precise_det);
   return sc_check_launch(ctx, "k_project_backward");
 }
 
@@ -427,7 +431,7 @@ __global__ void __launch_bounds__(PB_THREADS, 5) k_project_backward_shards(DSpla
                                                                      const sc_camera* __restrict__ cams,
                                                                      uint32_t n_views, float* __restrict__ out,
                                                                      uint32_t n_shards, uint32_t shard,
-                                                                     const uint32_t* __restrict__ skip) {
+                                                                     const uint32_t* __restrict__ skip, int precise) {
   __shared__ float s_rest[45 * PB_THREADS];
   const uint64_t i = (uint64_t)blockIdx.x * PB_THREADS + threadIdx.x;
   if (i >= (uint64_t)n_shards * shard) return;
@@ -457,7 +461,7 @@ __global__ void __launch_bounds__(PB_THREADS, 5) k_project_backward_shards(DSpla
         const Cam c = load_cam(cams + v);
         float basis[15];  // formed again in phase 2
         if (!splat_backward_view<true>(c, px, py, pz, qw, qx, qy, qz, l0, l1, l2, opacity, p0, p1, p2, gpos, grot,
-                                       gsc, gop, basis))
+                                       gsc, gop, basis, precise))
           continue;
         accepted |= 1u << (v - g0);
         gdc[0] += p2.x * SH_C0; gdc[1] += p2.y * SH_C0; gdc[2] += p2.z * SH_C0;
@@ -495,11 +499,11 @@ __global__ void __launch_bounds__(PB_THREADS, 5) k_project_backward_shards(DSpla
 
 sc_status launch_project_backward_shards(sc_ctx* ctx, const DSplats& s, const float4* pg, uint32_t stride,
                                          const sc_camera* d_cams, uint32_t n_views, float* grads, uint32_t n_shards,
-                                         uint32_t shard, const uint32_t* d_skip) {
+                                         uint32_t shard, const uint32_t* d_skip, int precise_det) {
   const uint64_t total = (uint64_t)n_shards * shard;
   if (total == 0) return SC_OK;
   k_project_backward_shards<<<(unsigned)sc_div_up(total, PB_THREADS), PB_THREADS, 0, ctx->stream>>>(
-      s, pg, stride, d_cams, n_views, grads, n_shards, shard, d_skip);
+      s, pg, stride, d_cams, n_views, grads, n_shards, shard, d_skip, precise_det);
   return sc_check_launch(ctx, "k_project_backward_shards");
 }
 

@@ -147,6 +147,12 @@ sc_status sc_ctx_device_info(sc_ctx* ctx, int* sm_count, size_t* free_b, size_t*
 
 uint64_t sc_ctx_launch_count(const sc_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+sc_status sc_ctx_set_fp64_det(sc_ctx* ctx, int enabled) {
+  if (!ctx) return SC_ERR_INVALID_ARG;
+  ctx->fp64_det = enabled ? 1 : 0;
+  return SC_OK;
+}
+
 sc_status sc_buffer_alloc(sc_ctx* ctx, size_t bytes, void** dptr) {
   if (!ctx || !dptr) return SC_ERR_INVALID_ARG;
   *dptr = nullptr;
@@ -487,7 +493,7 @@ sc_status sc_project(sc_ctx* ctx, const sc_splats* s, const sc_camera* cams, uin
   sc_camera* d_cams;
   SC_TRY(stage_cams(ctx, cams, n_views, &d_cams));
   sc_status st = sck::launch_project(ctx, dview(s), d_cams, n_views, s->cap, reinterpret_cast<float4*>(projected),
-                                     nullptr, nullptr, nullptr, nullptr, 0, 0);
+                                     nullptr, nullptr, nullptr, nullptr, ctx->fp64_det, 0);
   cudaFreeAsync(d_cams, ctx->stream);
   return st;
 }
@@ -778,7 +784,7 @@ sc_status sc_project_backward(sc_ctx* ctx, const sc_splats* s, const sc_projecte
   sc_camera* d_cam;
   SC_TRY(stage_cams(ctx, cam, 1, &d_cam));
   sc_status st = sck::launch_project_backward(ctx, dview(s), reinterpret_cast<const float4*>(pg), d_cam, g->slab,
-                                              g->cap, accumulate);
+                                              g->cap, accumulate, ctx->fp64_det);
   cudaFreeAsync(d_cam, ctx->stream);
   return st;
 }

@@ -45,6 +45,9 @@ struct sc_ctx {
   uint64_t* d_counters = nullptr; // scratch counters (tile ids, totals)
   uint32_t* h_error = nullptr;    // pinned mirror
   uint64_t launches = 0;
+  // sc_ctx_set_fp64_det: near-degenerate splats get an FP64 determinant and
+  // inverse in sc_project and sc_project_backward
+  int fp64_det = 0;
   // grow-only scratch arena for temporaries of the reference-shaped calls
   void* scratch = nullptr;
   size_t scratch_bytes = 0;
@@ -125,7 +128,11 @@ __device__ __forceinline__ CullShape cull_shape(float mx, float my, float a, flo
   CullShape s;
   s.mx = mx; s.my = my; s.a = a; s.b = b;
   s.det = a * c - b * b;
-  s.keep = !(a > 0.0f && c > 0.0f && s.det > 0.0f);
+  // An ill-conditioned conic (a needle-like splat: the determinant keeps less
+  // than 2^-10 of a c) has lost too many bits to cancellation here for the
+  // margins below, and the blend's own evaluation of the quadratic form is
+  // noisy along the needle: such a splat keeps its whole rectangle.
+  s.keep = !(a > 0.0f && c > 0.0f && s.det > 9.765625e-4f * a * c);
   s.any = op * 255.0f > 1.0f;
   const float q = 2.0f * __logf(fmaxf(op * 255.0f, 1.0f));
   s.L = q + 1e-3f * q + 1e-3f;
@@ -255,7 +262,7 @@ sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams,
                          float4* zero_grad = nullptr);
 
 sc_status launch_project_backward(sc_ctx* ctx, const DSplats& s, const float4* proj_grad, const sc_camera* d_cam,
-                                  float* grads, uint32_t gcap, int accumulate);
+                                  float* grads, uint32_t gcap, int accumulate, int precise_det);
 
 // Adam hyper-parameters, clamp limits and bias corrections of one step
 struct AdamParams {
@@ -357,7 +364,7 @@ __device__ __forceinline__ void constrain_geometry(float np[14], const AdamParam
 // of splats in [n, n_shards*shard) are zero.
 sc_status launch_project_backward_shards(sc_ctx* ctx, const DSplats& s, const float4* proj_grad, uint32_t stride,
                                          const sc_camera* d_cams, uint32_t n_views, float* grads, uint32_t n_shards,
-                                         uint32_t shard, const uint32_t* d_skip_flag);
+                                         uint32_t shard, const uint32_t* d_skip_flag, int precise_det);
 // Adam + constraints + densify statistic for splats [lo, lo+count) from one
 // reduce-scattered chunk g[r * shard + j]
 // Adam + constraints + densify statistic over splats [lo, lo+count) from

@@ -299,7 +299,8 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->counts + nsp, 0, 4, ctx->stream), "zero count tail");
   mark(tr, 0, capturing);
   SC_TRY(sck::launch_project(ctx, ds, d_cams, V, tr->stride, tr->rec, &tr->cfg.tiling, tr->dkeys, tr->ids,
-                             tr->counts_by_id, 0, (tr->cfg.tile_cull ? 1 : 0) | (tr->two_level ? 2 : 0), tr->pgrad));
+                             tr->counts_by_id, tr->cfg.fp64_det ? 1 : 0,
+                             (tr->cfg.tile_cull ? 1 : 0) | (tr->two_level ? 2 : 0), tr->pgrad));
   mark(tr, 1, capturing);
   bool in_tmp = false;
   SC_TRY(sck::radix_sort_segments(ctx, tr->dkeys, tr->ids, tr->dkeys_tmp, tr->ids_tmp, tr->stride, V, 32, tr->scratch,
@@ -429,11 +430,11 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   ap.opacity_logit_max = tr->cfg.opacity_logit_max;
   if (tr->grads_mode)
     SC_TRY(sck::launch_project_backward_shards(ctx, ds, tr->pgrad, tr->stride, d_cams, V, tr->gout, tr->g_shards,
-                                               tr->g_shard, ctx->d_error));
+                                               tr->g_shard, ctx->d_error, tr->cfg.fp64_det ? 1 : 0));
   else {
     // per-splat gradient rows summed over the views, then Adam streamed over the rows
     SC_TRY(sck::launch_project_backward_shards(ctx, ds, tr->pgrad, tr->stride, d_cams, V, tr->grads, 1,
-                                               tr->grad_stride, ctx->d_error));
+                                               tr->grad_stride, ctx->d_error, tr->cfg.fp64_det ? 1 : 0));
     SC_TRY(sck::launch_adam_rows(ctx, ds, dm, acc, tr->grads, 0, ds.n, tr->grad_stride, ap, d_bc, ctx->d_error));
   }
   mark(tr, 9, capturing);

@@ -96,6 +96,12 @@ class CudaCtx:
     def launch_count(self) -> int:
         return int(lib().sc_ctx_launch_count(self.handle))
 
+    def set_fp64_det(self, enabled: bool) -> None:
+        """FP64 determinant and inverse of near-degenerate splats in
+        project / project_backward (the reference computes them in f32,
+        project_gaussians.wgsl:226-234)."""
+        check(lib().sc_ctx_set_fp64_det(self.handle, 1 if enabled else 0), self.handle)
+
     def device_info(self) -> tuple[int, int, int]:
         sm, free, total = C.c_int(), C.c_size_t(), C.c_size_t()
         check(lib().sc_ctx_device_info(self.handle, C.byref(sm), C.byref(free), C.byref(total)), self.handle)

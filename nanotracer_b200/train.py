@@ -50,6 +50,7 @@ class TrainConfig:
     tile_cull: bool = True
     ssim_lambda: float = 0.0
     sort_mode: int = 0  # 0 auto (two-level binning), 1 sort of the (tile, splat) pairs, 2 two-level
+    fp64_det: bool = False  # FP64 determinant / inverse of near-degenerate splats (projection and adjoint)
 
     def struct(self) -> sc_train_config:
         c = sc_train_config()
@@ -64,6 +65,7 @@ class TrainConfig:
         c.log_scale_min, c.log_scale_max, c.opacity_logit_max = LOG_SCALE_MIN, LOG_SCALE_MAX, OPACITY_LOGIT_MAX
         c.ssim_lambda = self.ssim_lambda
         c.sort_mode = self.sort_mode
+        c.fp64_det = 1 if self.fp64_det else 0
         return c
 
 

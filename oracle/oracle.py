@@ -82,12 +82,13 @@ def lib():
                 f"oracle_bin64_{sfx}": (C.c_int64, [U32, U32, P, C.POINTER(Tiling), P, P, U64, P]),
                 f"oracle_composite_{sfx}": (None, [P, P, P, C.POINTER(Tiling), P, P, P]),
                 f"oracle_mse_{sfx}": (D, [U64, P, P, P, F32]),
-                f"oracle_composite_backward_{sfx}": (None, [P, P, P, C.POINTER(Tiling), P, P, I32, P, P, P]),
+                f"oracle_composite_backward_{sfx}": (None, [P, P, P, C.POINTER(Tiling), P, P, I32, P, P, P, P]),
+                f"oracle_composite_margins_{sfx}": (None, [P, P, P, C.POINTER(Tiling), I32, D, D, P, P]),
                 f"oracle_project_backward_{sfx}": (None, [C.POINTER(HostSplats), P, C.POINTER(Camera), P, P, P, P, P,
                                                           P, I32]),
                 f"oracle_train_step_{sfx}": (D, [C.POINTER(HostSplats), C.POINTER(HostSplats), C.POINTER(HostSplats),
                                                  P, U32, P, P, C.POINTER(Tiling), I32, C.POINTER(AdamGroups), U64, P,
-                                                 F32]),
+                                                 F32, P]),
                 f"oracle_ssim_loss_grad_{sfx}": (D, [I32, I32, P, P, P, F32]),
                 f"oracle_combined_loss_grad_{sfx}": (D, [I32, I32, P, P, P, F32, F32, P]),
             })
@@ -232,18 +233,41 @@ def mse(pred4, target3, scale=1.0, sfx="f32"):
     return loss, dl
 
 
-def composite_backward(rec, payloads, ranges, tl: Tiling, fwd, dl_dc, mode=0, ncon=None, tfin=None, sfx="f32"):
+def composite_backward(rec, payloads, ranges, tl: Tiling, fwd, dl_dc, mode=0, ncon=None, tfin=None, sfx="f32",
+                       want_abs=False):
+    """Projected gradients (n, 12); with want_abs also the per-component sums
+    of the pixels' absolute terms (the scale of the sum's rounding error)."""
     rec = np.ascontiguousarray(rec, _dt(sfx))
     n = rec.shape[0]
     pg = np.zeros(n * 12, _dt(sfx))
+    ab = np.zeros(n * 12, _dt(sfx)) if want_abs else None
     fwd = np.ascontiguousarray(fwd, _dt(sfx))
     dl = np.ascontiguousarray(dl_dc, _dt(sfx))
     nc = None if ncon is None else np.ascontiguousarray(ncon, np.uint32)
     tf = None if tfin is None else np.ascontiguousarray(tfin, _dt(sfx))
     getattr(lib(), f"oracle_composite_backward_{sfx}")(_p(rec), _p(np.ascontiguousarray(payloads, np.uint32)),
                                                        _p(np.ascontiguousarray(ranges, np.uint32)), C.byref(tl),
-                                                       _p(fwd), _p(dl), int(mode), _p(nc), _p(tf), _p(pg))
-    return pg.reshape(n, 12)
+                                                       _p(fwd), _p(dl), int(mode), _p(nc), _p(tf), _p(pg), _p(ab))
+    return (pg.reshape(n, 12), ab.reshape(n, 12)) if want_abs else pg.reshape(n, 12)
+
+
+def composite_margins(rec, payloads, ranges, tl: Tiling, mode=1, thr_a=1e-5, thr_t=1e-4, sfx="f32"):
+    """Near-threshold diagnostics of one view (test infrastructure; see
+    composite_margins in splat_oracle.cpp).  Returns (margin (H, W): the
+    forward walk's smallest distance to a blend threshold in units of the
+    test's tolerance, below 1 = the pixel may render differently; bwd (n,)
+    bool: splats whose gradient may differ when both sides differentiate the
+    same forward; fwd (n,) bool: splats whose gradient may differ when each
+    side differentiates its own forward)."""
+    rec = np.ascontiguousarray(rec, _dt(sfx))
+    n = rec.shape[0]
+    margin = np.zeros(tl.width * tl.height, np.float32)
+    flags = np.zeros(max(n, 1), np.uint8)
+    getattr(lib(), f"oracle_composite_margins_{sfx}")(_p(rec), _p(np.ascontiguousarray(payloads, np.uint32)),
+                                                      _p(np.ascontiguousarray(ranges, np.uint32)), C.byref(tl),
+                                                      int(mode), float(thr_a), float(thr_t), _p(margin), _p(flags))
+    f = flags[:n]
+    return margin.reshape(tl.height, tl.width), (f & 1).astype(bool), (f & 2).astype(bool)
 
 
 def project_backward(s: OSplats, pg, cam: Camera, sfx="f32"):
@@ -329,7 +353,10 @@ def combined(pred4, target3, w, h, lam, scale=1.0, sfx="f32"):
 
 
 def train_step(s: OSplats, m: OSplats, v: OSplats, acc, cams: list, targets, tl: Tiling, mode: int, lrs, t: int,
-               sfx="f32", want_images=False, ssim_lambda=0.0):
+               sfx="f32", want_images=False, ssim_lambda=0.0, grads_out=None):
+    """One iteration in place; grads_out (float32 array of 59 * n, nullable)
+    receives the iteration's gradient rows (pos 3n, rot 4n, scale 3n, opacity
+    n, sh_dc 3n, sh_rest 45n)."""
     V = len(cams)
     arr = (Camera * V)(*cams)
     g = AdamGroups()
@@ -340,7 +367,7 @@ def train_step(s: OSplats, m: OSplats, v: OSplats, acc, cams: list, targets, tl:
     t3 = np.ascontiguousarray(targets, np.float32)
     loss = getattr(lib(), f"oracle_train_step_{sfx}")(C.byref(s.h), C.byref(m.h), C.byref(v.h), _p(acc), V, arr,
                                                       _p(t3), C.byref(tl), int(mode), C.byref(g), int(t), _p(imgs),
-                                                      float(ssim_lambda))
+                                                      float(ssim_lambda), _p(grads_out))
     return loss, imgs
 
 

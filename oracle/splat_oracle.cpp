@@ -33,6 +33,10 @@
 //     "ref" mode that reverse-walks the whole tile list;
 //   * 64-bit (view, tile, depth-bits) keys next to the reference's
 //     32-bit (tile << 16 | depth16) keys, and multi-view pipelines.
+// And test diagnostics with no reference counterpart: near-threshold
+// margins of the blend's discontinuous tests (composite_margins), the
+// absolute-value sums that bound a gradient sum's rounding error, and the
+// iteration's gradient rows as an output of train_step.
 
 #include <algorithm>
 #include <cmath>
@@ -595,10 +599,14 @@ template <typename T> static inline void atomic_add(T* p, T v) {
 
 // rasterize_backward.wgsl:73-210 ("ref" mode, mode == 0) and the exact extension (mode == 1:
 // start at the forward's last contributor with the recorded final transmittance, no T bail).
+// abs_grad (nullable, test diagnostics): receives per component the sum over pixels of the
+// magnitude of each pixel's term taken before any cancellation (every product and sum that
+// forms the term replaced by its absolute value), the scale that bounds the rounding error
+// of the gradient sum, including the cancellation in T c - S / (1 - alpha).
 template <typename T>
 static void composite_backward(const T* rec, const uint32_t* payloads, const uint32_t* ranges,
                                const Tiling& tl, const T* fwd_out, const T* dl_dc, int mode,
-                               const uint32_t* n_contrib, const T* t_final, T* proj_grad) {
+                               const uint32_t* n_contrib, const T* t_final, T* proj_grad, T* abs_grad = nullptr) {
   const uint32_t tx_n = tl.tiles_x(), ty_n = tl.tiles_y();
 #pragma omp parallel for schedule(dynamic, 1) collapse(2)
   for (int64_t ty = 0; ty < (int64_t)ty_n; ++ty)
@@ -655,8 +663,138 @@ static void composite_backward(const T* rec, const uint32_t* payloads, const uin
             atomic_add(&o[G_MX], gmx); atomic_add(&o[G_MY], gmy); atomic_add(&o[G_OP], gsig);
             atomic_add(&o[G_CA], ga); atomic_add(&o[G_CB], gbb); atomic_add(&o[G_CC], gc);
             atomic_add(&o[G_R], dCr); atomic_add(&o[G_G], dCg); atomic_add(&o[G_B], dCb);
+            if (abs_grad) {
+              const T gabs = sat * (std::abs(gr) * (std::abs(Tr * p[R_R]) + std::abs(Sr / oma)) +
+                                    std::abs(gg) * (std::abs(Tr * p[R_G]) + std::abs(Sg / oma)) +
+                                    std::abs(gb) * (std::abs(Tr * p[R_B]) + std::abs(Sb / oma)));
+              const T pabs = gabs * sigma * g;
+              T* q = abs_grad + 12 * (size_t)sidx;
+              atomic_add(&q[G_MX], pabs * (std::abs(p[R_CA] * dx) + std::abs(p[R_CB] * dy)));
+              atomic_add(&q[G_MY], pabs * (std::abs(p[R_CB] * dx) + std::abs(p[R_CC] * dy)));
+              atomic_add(&q[G_OP], gabs * g);
+              atomic_add(&q[G_CA], pabs * T(0.5) * (dx * dx));
+              atomic_add(&q[G_CB], pabs * std::abs(dx * dy));
+              atomic_add(&q[G_CC], pabs * T(0.5) * (dy * dy));
+              atomic_add(&q[G_R], std::abs(dCr)); atomic_add(&q[G_G], std::abs(dCg));
+              atomic_add(&q[G_B], std::abs(dCb));
+            }
             Sr = Sr + cr; Sg = Sg + cg; Sb = Sb + cb;
           }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- near-threshold diagnostics
+// Test infrastructure with no counterpart in the reference.  The blend makes
+// discontinuous decisions: skip a pair when the quadratic form is negative
+// (power > 0) or alpha < 1/255, gate the opacity gradient at alpha_raw < 0.99,
+// stop a pixel when T < 1e-4 after a blend (forward) or when the recomputed T
+// exceeds 1.0001 (the reference backward, mode 0).  Arithmetic that differs
+// from this oracle's only by rounding (another exp, another operation order)
+// can take the other branch of such a test only where the compared quantity
+// lies within its rounding error of the threshold: thr_a (relative) for the
+// per-pair tests, thr_t for the transmittance tests, whose errors accumulate
+// along a walk.
+//
+// margin[pixel]: the smallest distance of the pixel's forward walk to a
+// threshold, in units of that test's thr (below 1: the pixel may render
+// differently).  flags[splat] bit 0: the splat is in a pixel's walk at or
+// before a near-threshold pair test (or, mode 0, a near-threshold backward
+// stop), so its gradient from that pixel may differ even when the backward
+// gets the same forward image and aux; bit 1: the splat is in the walk of a
+// pixel whose forward may differ (any near test, a near stop extended to the
+// next pair the pixel would blend), so its gradient may differ when each side
+// differentiates its own forward.
+template <typename T>
+static void composite_margins(const T* rec, const uint32_t* payloads, const uint32_t* ranges, const Tiling& tl,
+                              int mode, double thr_a, double thr_t, float* margin, uint8_t* flags) {
+  const uint32_t tx_n = tl.tiles_x(), ty_n = tl.tiles_y();
+  const double amin = (double)ALPHA_MIN, amax = (double)ALPHA_MAX;
+#pragma omp parallel for schedule(dynamic, 1) collapse(2)
+  for (int64_t ty = 0; ty < (int64_t)ty_n; ++ty)
+    for (int64_t tx = 0; tx < (int64_t)tx_n; ++tx) {
+      const uint32_t tile = (uint32_t)ty * tx_n + (uint32_t)tx;
+      const uint32_t begin = ranges[2 * tile], end = std::max(ranges[2 * tile + 1], begin);
+      for (uint32_t ly = 0; ly < tl.tile_h; ++ly)
+        for (uint32_t lx = 0; lx < tl.tile_w; ++lx) {
+          const uint32_t px = (uint32_t)tx * tl.tile_w + lx, py = (uint32_t)ty * tl.tile_h + ly;
+          if (px >= tl.width || py >= tl.height) continue;
+          const T pix_x = T((float)px + 0.5f), pix_y = T((float)py + 0.5f);
+          // the alpha of position j (-1 when the sign test skips it) and the
+          // pair tests' distances in units of thr_a: da (skip tests), dg (0.99 gate)
+          auto pair_at = [&](uint32_t j, double& da, double& dg) -> T {
+            const T* p = rec + 12 * (size_t)payloads[j];
+            const T dx = pix_x - p[R_MX], dy = pix_y - p[R_MY];
+            const T quad = p[R_CA] * dx * dx + T(2) * p[R_CB] * dx * dy + p[R_CC] * dy * dy;
+            const double qabs = std::abs((double)p[R_CA] * dx * dx) + std::abs(2.0 * (double)p[R_CB] * dx * dy) +
+                                std::abs((double)p[R_CC] * dy * dy);
+            da = qabs > 0.0 ? std::abs((double)quad) / qabs / thr_a : 1e30;
+            dg = 1e30;
+            const T power = T(-0.5) * quad;
+            if (power > T(0)) return T(-1);
+            const T araw = p[R_OP] * std::exp(power);
+            const T alpha = std::min(araw, T(ALPHA_MAX));
+            da = std::min(da, std::abs((double)alpha - amin) / amin / thr_a);
+            if (alpha >= T(ALPHA_MIN)) dg = std::abs((double)araw - amax) / amax / thr_a;
+            return alpha;
+          };
+          double m = 1e30;         // forward walk, any test
+          int64_t k_pair = -1;     // last position with a near pair test (the gate: itself only)
+          std::vector<uint32_t> gate_near;
+          T Tr = 1;
+          bool t_near = false;
+          uint32_t j = begin;
+          for (; j < end; ++j) {
+            double da, dg;
+            const T alpha = pair_at(j, da, dg);
+            m = std::min(m, std::min(da, dg));
+            if (da < 1.0) k_pair = j;
+            if (dg < 1.0) gate_near.push_back(j);
+            if (alpha < T(ALPHA_MIN)) continue;
+            Tr = Tr * (T(1) - alpha);
+            const double dt = std::abs((double)Tr - 1e-4) / 1e-4 / thr_t;
+            m = std::min(m, dt);
+            if (Tr < T(1e-4f)) {
+              t_near = dt < 1.0;
+              break;
+            }
+          }
+          uint32_t walk_end = j < end ? j + 1 : end;  // one past the forward's last position
+          if (t_near)  // the stop may move to the next pair this pixel would blend
+            for (uint32_t k = walk_end; k < end; ++k) {
+              double da, dg;
+              walk_end = k + 1;
+              if (pair_at(k, da, dg) >= T(ALPHA_MIN)) break;
+            }
+          if (mode == 0) {  // the reference backward walks every entry from the end of the list
+            T Tb = T(1) - (T(1) - Tr);
+            for (uint32_t jj = end; jj > begin; --jj) {
+              double da, dg;
+              const T alpha = pair_at(jj - 1, da, dg);
+              if (da < 1.0) k_pair = std::max<int64_t>(k_pair, (int64_t)jj - 1);
+              if (dg < 1.0) gate_near.push_back(jj - 1);
+              if (alpha < T(ALPHA_MIN)) continue;
+              Tb = Tb / std::max(T(1) - alpha, T(1e-4f));
+              const double db = std::abs((double)Tb - 1.0001) / 1.0001 / thr_t;
+              if (db < 1.0) k_pair = std::max<int64_t>(k_pair, (int64_t)jj - 1);
+              if (Tb > T(1.0001f)) break;
+            }
+          }
+          margin[(size_t)py * tl.width + px] = (float)std::min(m, 1e30);
+          if (!flags) continue;
+          for (int64_t k = begin; k <= k_pair; ++k) {
+#pragma omp atomic update
+            flags[payloads[k]] |= (uint8_t)1;
+          }
+          for (uint32_t k : gate_near) {
+#pragma omp atomic update
+            flags[payloads[k]] |= (uint8_t)1;
+          }
+          if (m < 1.0)
+            for (uint32_t k = begin; k < walk_end; ++k) {
+#pragma omp atomic update
+              flags[payloads[k]] |= (uint8_t)2;
+            }
         }
     }
 }
@@ -1048,7 +1186,7 @@ template <typename T>
 static double train_step(HostSplats& s, HostSplats& m, HostSplats& v, float* grad_acc, uint32_t n_views,
                          const Camera* cams, const float* targets, const Tiling& tl, int mode,
                          const AdamGroups& ag, uint64_t t, float* out_images /* nullable, V*P*4 f32 */,
-                         float ssim_lambda) {
+                         float ssim_lambda, float* grads_out = nullptr /* nullable, 59*n f32 slab */) {
   const uint32_t n = s.n;
   const uint64_t P = (uint64_t)tl.width * tl.height;
   const uint32_t ntiles = tl.num_tiles();
@@ -1077,6 +1215,7 @@ static double train_step(HostSplats& s, HostSplats& m, HostSplats& v, float* gra
   }
   std::vector<float> gf((size_t)59 * n);
   for (size_t k = 0; k < gf.size(); ++k) gf[k] = (float)gbuf[k];
+  if (grads_out) std::copy(gf.begin(), gf.end(), grads_out);
   accumulate_grad(n, gf.data(), grad_acc);
   float* gp = gf.data();
   const size_t off[7] = {0, 3 * (size_t)n, 7 * (size_t)n, 10 * (size_t)n, 11 * (size_t)n, 14 * (size_t)n, 59 * (size_t)n};
@@ -1135,8 +1274,13 @@ void oracle_camera_from_pose(const float* eye, const float* target, const float*
   }                                                                                                              \
   void oracle_composite_backward_##SFX(const T* rec, const uint32_t* pay, const uint32_t* ranges,                \
                                        const Tiling* tl, const T* fwd, const T* dl, int mode,                    \
-                                       const uint32_t* ncon, const T* tfin, T* pg) {                             \
-    composite_backward<T>(rec, pay, ranges, *tl, fwd, dl, mode, ncon, tfin, pg);                                 \
+                                       const uint32_t* ncon, const T* tfin, T* pg, T* abs_pg) {                  \
+    composite_backward<T>(rec, pay, ranges, *tl, fwd, dl, mode, ncon, tfin, pg, abs_pg);                         \
+  }                                                                                                              \
+  void oracle_composite_margins_##SFX(const T* rec, const uint32_t* pay, const uint32_t* ranges,                 \
+                                      const Tiling* tl, int mode, double thr_a, double thr_t, float* margin,     \
+                                      uint8_t* flags) {                                                          \
+    composite_margins<T>(rec, pay, ranges, *tl, mode, thr_a, thr_t, margin, flags);                              \
   }                                                                                                              \
   void oracle_project_backward_##SFX(const HostSplats* s, const T* pg, const Camera* cam, T* gpos, T* grot,      \
                                      T* gsc, T* gop, T* gdc, T* grest, int accumulate) {                         \
@@ -1145,8 +1289,10 @@ void oracle_camera_from_pose(const float* eye, const float* target, const float*
   }                                                                                                              \
   double oracle_train_step_##SFX(HostSplats* s, HostSplats* m, HostSplats* v, float* acc, uint32_t nv,          \
                                  const Camera* cams, const float* targets, const Tiling* tl, int mode,           \
-                                 const AdamGroups* ag, uint64_t t, float* out_images, float ssim_lambda) {       \
-    return train_step<T>(*s, *m, *v, acc, nv, cams, targets, *tl, mode, *ag, t, out_images, ssim_lambda);        \
+                                 const AdamGroups* ag, uint64_t t, float* out_images, float ssim_lambda,         \
+                                 float* grads_out) {                                                             \
+    return train_step<T>(*s, *m, *v, acc, nv, cams, targets, *tl, mode, *ag, t, out_images, ssim_lambda,         \
+                         grads_out);                                                                             \
   }                                                                                                              \
   double oracle_ssim_loss_grad_##SFX(int w, int h, const T* pred, const float* target, T* dl, float scale) {     \
     return ssim_loss_grad<T>(w, h, pred, target, dl, scale);                                                     \

@@ -3,11 +3,13 @@
 Stages are compared on shared inputs: the oracle bins the GPU's projected
 records, blends the GPU's bins, and differentiates the GPU's images, so
 integer results (bins, sort order, ranges) must match bit for bit and float
-results within the stated tolerances:
-  images  <= 1e-4 absolute on every pixel except those where an alpha lands
-          within rounding of the 1/255 cut or the 1e-4 saturation stop
-          (at most 0.05% of pixels, each still <= 1e-2)
-  grads   <= 1e-3 relative (per component, relative to the component's scale)
+results within the tolerances of tests/util.py:
+  images  <= 1e-4 absolute on every pixel except those whose walk passes
+          within a stated relative margin of a blend threshold (alpha vs
+          1/255 or 0.99, T vs 1e-4, the reference backward's T vs 1.0001),
+          counted and at most 0.1 % of the pixels
+  grads   <= 1e-3 relative per component plus 1e-4 of the sum of the terms'
+          magnitudes, except splats in the walk of such a pixel
 """
 import json
 import math
@@ -20,15 +22,10 @@ from nanotracer_b200 import CameraUniform, GpuSplatBuffer, PrefixScan, RadixSort
 from nanotracer_b200._lib import SC_BWD_EXACT, SC_BWD_REF, SC_KEYS_NATIVE64, SC_KEYS_REF32
 from nanotracer_b200.scene import FOV_Y, orbit_pose, orbit_views, random_scene
 
-from tests.util import GpuPipe, config1, frac_close
+from tests.util import GpuPipe, check_image_explained, check_param_grads, check_pg_explained, config1, margins
 
 pytestmark = pytest.mark.gpu
 KATS = json.loads((Path(__file__).parent / "golden" / "reference_kats.json").read_text())
-
-IMG_ATOL = 1e-4
-IMG_FLIP_FRAC = 5e-4
-IMG_FLIP_MAX = 1e-2
-GRAD_RTOL = 1e-3
 
 
 def _osplats(oracle, scene):
@@ -41,29 +38,6 @@ def _ocam(oracle, cam: CameraUniform):
 
 def _otl(oracle, tl: TilingParams):
     return oracle.tiling(tl.width, tl.height, tl.tile_w, tl.tile_h, tl.depth_max)
-
-
-def check_image(gpu, ora):
-    d = np.abs(gpu.astype(np.float64) - ora.astype(np.float64))
-    per_pixel = d.reshape(-1, d.shape[-1]).max(axis=1)
-    bad = per_pixel > IMG_ATOL
-    assert bad.mean() <= IMG_FLIP_FRAC, f"{bad.sum()} pixels beyond {IMG_ATOL} (max {per_pixel.max():.3g})"
-    assert per_pixel.max() <= IMG_FLIP_MAX, per_pixel.max()
-
-
-def check_grad(gpu, ora, rtol=GRAD_RTOL, allow_frac=1e-3):
-    gpu, ora = np.asarray(gpu, np.float64), np.asarray(ora, np.float64)
-    assert gpu.shape == ora.shape
-    for c in range(ora.shape[1]):
-        scale = np.abs(ora[:, c]).max()
-        if scale == 0:
-            assert np.abs(gpu[:, c]).max() <= 1e-12, c
-            continue
-        err = np.abs(gpu[:, c] - ora[:, c])
-        ok = err <= rtol * scale
-        assert ok.mean() >= 1.0 - allow_frac, (c, err.max() / scale, (~ok).sum())
-        rel = np.linalg.norm(gpu[:, c] - ora[:, c]) / np.linalg.norm(ora[:, c])
-        assert rel <= rtol, (c, rel)
 
 
 # ------------------------------------------------------------------ projection
@@ -111,8 +85,9 @@ def test_projection_parity_config1(ctx, oracle, n_views):
         assert np.all(g[g[:, 7] == 0] == 0)
 
 
-def test_projection_against_fp64_oracle_precise(ctx, oracle):
-    """The f32 GPU projection against the FP64 oracle (error statement for the precision form)."""
+def test_projection_against_fp64_oracle(ctx, oracle):
+    """The f32 GPU projection of ordinary (config-1) splats against the FP64
+    oracle: the error statement of the default f32 arithmetic."""
     scene, cam, tl = config1(2000)
     pipe = GpuPipe(ctx, scene, cam, tl)
     g = pipe.project()[0]
@@ -343,9 +318,13 @@ def test_composite_parity_config1(ctx, oracle, tile):
     _, pay, ranges = pipe.bin()
     img, aux = pipe.composite()
     oimg, oncon, otf = oracle.composite(rec, pay, ranges.reshape(-1), _otl(oracle, tl))
-    check_image(img[0], oimg)
-    assert (aux[0, ..., 1] == oncon).mean() >= 0.999
-    assert np.abs(aux[0, ..., 0].view(np.float32) - otf).max() < 1e-5
+    margin, _, _ = margins(oracle, rec, pay, ranges, _otl(oracle, tl), 1)
+    print(check_image_explained(img[0], oimg, margin))
+    near = margin < 1.0
+    # last contributor and final T: equal except where a pixel's walk is near a threshold
+    assert np.all((aux[0, ..., 1] == oncon) | near)
+    tf = aux[0, ..., 0].view(np.float32)
+    assert np.all((np.abs(tf - otf) <= 1e-5 * np.maximum(np.abs(otf), 1e-4)) | near)
 
 
 def test_mse_loss_grad_vs_oracle(ctx, oracle):
@@ -375,10 +354,11 @@ def test_composite_backward_parity_config1(ctx, oracle, mode):
     dl = (rng.normal(size=(tl.height * tl.width, 4)) * 1e-3).astype(np.float32)
     dl[:, 3] = 0
     gpu = pipe.backward(dl, mode)[0]
-    ora = oracle.composite_backward(rec, pay, ranges.reshape(-1), _otl(oracle, tl), img[0].reshape(-1, 4), dl, mode,
-                                    aux[0, ..., 1].reshape(-1), aux[0, ..., 0].view(np.float32).reshape(-1))
-    cols = [0, 1, 2, 4, 5, 6, 8, 9, 10]
-    check_grad(gpu[:, cols], ora[:, cols])
+    ora, absum = oracle.composite_backward(rec, pay, ranges.reshape(-1), _otl(oracle, tl), img[0].reshape(-1, 4), dl,
+                                           mode, aux[0, ..., 1].reshape(-1),
+                                           aux[0, ..., 0].view(np.float32).reshape(-1), want_abs=True)
+    _, flags, _ = margins(oracle, rec, pay, ranges, _otl(oracle, tl), mode)
+    print(check_pg_explained(gpu, ora, absum, flags, label=f"config1 mode {mode}"))
     assert np.all(gpu[:, [3, 7, 11]] == 0)
 
 
@@ -396,7 +376,7 @@ def test_project_backward_parity_config1(ctx, oracle):
     pipe.r.project_backward(pipe.g, pipe.pg, cam, grads)
     gpu = grads.readback(len(scene)).flat()
     ora = oracle.project_backward(_osplats(oracle, scene), pg, _ocam(oracle, cam))
-    check_grad(gpu, ora, rtol=1e-4, allow_frac=1e-3)
+    print(check_param_grads(gpu, ora, rtol=1e-4))
     # accumulate=1 adds a second view's gradient
     pipe.r.project_backward(pipe.g, pipe.pg, cam, grads, accumulate=True)
     assert np.allclose(grads.readback(len(scene)).flat(), 2 * gpu, rtol=1e-6, atol=1e-12)

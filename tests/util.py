@@ -71,3 +71,141 @@ class GpuPipe:
 def frac_close(a, b, atol, rtol=0.0):
     d = np.abs(np.asarray(a, np.float64) - np.asarray(b, np.float64))
     return float(np.mean(d <= atol + rtol * np.abs(np.asarray(b, np.float64))))
+
+
+# ------------------------------------------------------------------ tolerances with stated causes
+# Images: every pixel within IMG_ATOL of the oracle, except pixels whose
+# forward walk passes near one of the blend's discontinuous tests: a pair test
+# (alpha vs 1/255, alpha_raw vs 0.99, the quadratic form's sign) within THR_A
+# (relative) of its threshold, or the transmittance stop (T vs 1e-4; in the
+# reference backward also T vs 1.0001) within THR_T[mode].  There the GPU's
+# ex2/rcp approximations (~1e-6 relative per pair, accumulated into T along a
+# walk) may take the other branch.  Such exceptions are counted and bounded.
+IMG_ATOL = 1e-4
+THR_A = 1e-5
+THR_T = {0: 3e-5, 1: 1e-4}    # by backward mode (0 = reference walk, 1 = exact)
+
+
+def margins(oracle, rec, payloads, ranges, otl, mode):
+    """(margin (H, W) in units of the tests' tolerances, bwd flags, fwd flags)."""
+    return oracle.composite_margins(rec, payloads, np.asarray(ranges).reshape(-1), otl, mode, THR_A, THR_T[mode])
+
+
+MAX_FLIP_FRAC = 1e-3          # at most this fraction of pixels may take the other branch
+# Projected gradients: per component |gpu - oracle| <= GRAD_RTOL |oracle| +
+# GRAD_ABS_REL A, A the oracle's sum over pixels of each term's magnitude
+# before cancellation (oracle.composite_backward(want_abs=True)): the relative
+# bar plus the rounding-error scale of a cancelling sum.  Splats in the walk
+# of a near-threshold pixel are the stated exception.
+GRAD_RTOL = 1e-3
+GRAD_ABS_REL = 1e-4
+
+
+def check_image_explained(gpu, ora, margin, atol=IMG_ATOL, max_frac=MAX_FLIP_FRAC, label=""):
+    """gpu, ora (H, W, 4); margin (H, W) from margins().  Returns a summary
+    dict (printed by the caller)."""
+    d = np.abs(np.asarray(gpu, np.float64) - np.asarray(ora, np.float64)).reshape(-1, 4).max(axis=1)
+    m = np.asarray(margin).reshape(-1)
+    bad = d > atol
+    unexplained = bad & (m >= 1.0)
+    s = {"pixels": int(d.size), "beyond_atol": int(bad.sum()), "unexplained": int(unexplained.sum()),
+         "near_threshold": int((m < 1.0).sum()), "max_err": float(d.max()),
+         "max_err_explained_px": float(d[~bad].max()) if (~bad).any() else 0.0}
+    if unexplained.any():
+        i = int(np.flatnonzero(unexplained)[np.argmax(d[unexplained])])
+        s["worst_unexplained"] = (i, float(d[i]), float(m[i]))
+    assert not unexplained.any(), f"{label} pixels beyond {atol} with no near-threshold cause: {s}"
+    assert bad.mean() <= max_frac, f"{label} too many near-threshold pixels: {s}"
+    return s
+
+
+PG_COLS = [0, 1, 2, 4, 5, 6, 8, 9, 10]  # dmean.xy, dopacity, dconic.abc, dcolor.rgb
+
+
+def check_pg_explained(gpu, ora, absum, flags, rtol=GRAD_RTOL, arel=GRAD_ABS_REL, max_frac=MAX_FLIP_FRAC,
+                       label=""):
+    """Projected gradients (n, 12): per component within rtol |ora| + arel
+    absum, except splats flagged by oracle.composite_margins."""
+    g = np.asarray(gpu, np.float64)[:, PG_COLS]
+    o = np.asarray(ora, np.float64)[:, PG_COLS]
+    a = np.asarray(absum, np.float64)[:, PG_COLS]
+    err = np.abs(g - o)
+    ok_c = err <= rtol * np.abs(o) + arel * a
+    bad = ~ok_c.all(axis=1)
+    live = (np.abs(o) > 0).any(axis=1) | (np.abs(g) > 0).any(axis=1)
+    unexplained = bad & ~np.asarray(flags, bool)
+    pure = err <= rtol * np.abs(o)
+    s = {"splats_with_grad": int(live.sum()), "beyond_bound": int(bad.sum()), "unexplained": int(unexplained.sum()),
+         "flagged": int(np.asarray(flags, bool).sum()),
+         "components_within_pure_rtol": float(pure[live].mean()) if live.any() else 1.0}
+    if unexplained.any():
+        i = int(np.flatnonzero(unexplained)[0])
+        s["first_unexplained"] = (i, g[i].tolist(), o[i].tolist(), a[i].tolist())
+    assert not unexplained.any(), f"{label} gradients beyond the bound with no near-threshold cause: {s}"
+    assert bad.sum() <= max(1, max_frac * live.sum()), f"{label} too many flagged splats off the bound: {s}"
+    return s
+
+
+GROUPS = [(0, 3), (3, 7), (7, 10), (10, 11), (11, 14), (14, 59)]  # pos, rot, log-scale, logit, dc, rest
+
+
+def check_param_grads(gpu, ora, rtol=GRAD_RTOL, label=""):
+    """Per-splat parameter gradients (n, 59) from the same projected gradients:
+    per parameter group |gpu - ora|_2 <= rtol |ora|_2 + 1e-6 |ora_splat|_2."""
+    g, o = np.asarray(gpu, np.float64), np.asarray(ora, np.float64)
+    tot = np.linalg.norm(o, axis=1)
+    worst = 0.0
+    for lo, hi in GROUPS:
+        e = np.linalg.norm(g[:, lo:hi] - o[:, lo:hi], axis=1)
+        r = np.linalg.norm(o[:, lo:hi], axis=1)
+        bound = rtol * r + 1e-6 * tot
+        bad = e > bound
+        assert not bad.any(), f"{label} group {lo}:{hi}: {int(bad.sum())} splats, worst " \
+                              f"{(e[bad] / np.maximum(r[bad], 1e-30)).max():.3g} relative"
+        m = r > 0
+        if m.any():
+            worst = max(worst, float((e[m] / r[m]).max()))
+    return {"worst_group_rel": worst}
+
+
+def adam_first_step(theta, grads, lrs, b1=0.9, b2=0.999, eps=1e-15):
+    """The oracle's Adam (t = 1, zero moments) over the six parameter groups,
+    then the constraints: what the trainer's step does to the parameters."""
+    from oracle import oracle as O
+    th = np.array(theta, np.float32, copy=True)
+    g = np.asarray(grads, np.float32)
+    z = np.zeros_like(th[:, 0])
+    for k, (lo, hi) in enumerate(GROUPS):
+        p = np.ascontiguousarray(th[:, lo:hi])
+        gg = np.ascontiguousarray(g[:, lo:hi])
+        pn, _, _ = O.adam_step(p, gg, np.zeros_like(p), np.zeros_like(p), lrs[k], 1, b1, b2, eps)
+        th[:, lo:hi] = pn.reshape(p.shape)
+    rot, sc, op = O.apply_constraints(th[:, 3:7], th[:, 7:10], th[:, 10])
+    th[:, 3:7], th[:, 7:10], th[:, 10] = rot.reshape(-1, 4), sc.reshape(-1, 3), op
+    del z
+    return th
+
+
+def check_post_adam(gpu_theta, ora_theta, ora_grads, flags, label=""):
+    """After one Adam step from zero moments a parameter moves by -lr sign(g):
+    the trainer's parameters equal the oracle's except where a gradient's sign
+    is not determined by the tolerance, i.e. in a (splat, group) whose oracle
+    gradient has a component within GRAD_RTOL of the group's norm of zero (or
+    below 1e-18, where FTZ differs), or a splat flagged near a threshold."""
+    g, o, go = (np.asarray(x, np.float64) for x in (gpu_theta, ora_theta, ora_grads))
+    close = np.abs(g - o) <= 1e-6 * np.abs(o) + 1e-7
+    flags = np.asarray(flags, bool)
+    n_bad, n_unexp = 0, 0
+    for lo, hi in GROUPS:
+        bad = ~close[:, lo:hi].all(axis=1)
+        norm = np.linalg.norm(go[:, lo:hi], axis=1)
+        near0 = (np.abs(go[:, lo:hi]) <= np.maximum(GRAD_RTOL * norm, 1e-18)[:, None]).any(axis=1)
+        unexp = bad & ~near0 & ~flags
+        n_bad += int(bad.sum())
+        n_unexp += int(unexp.sum())
+        assert not unexp.any(), f"{label} group {lo}:{hi}: {int(unexp.sum())} splats off with a determined sign " \
+                                f"(first {int(np.flatnonzero(unexp)[0])})"
+    s = {"groups_off": n_bad, "unexplained": n_unexp, "params": int(g.size),
+         "params_equal_frac": float(close.mean())}
+    assert n_bad <= max(1, 1e-3 * g.shape[0]), f"{label} too many groups off: {s}"
+    return s
