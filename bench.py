@@ -164,6 +164,142 @@ def make_workload(args, rank, ctx):
     return scene, target_scene, tl, cams_for, render_targets
 
 
+def render_views(ctx, g, cams, tl):
+    """Float4 renders (V, H, W, 4) of a device splat store from cams through the
+    stage API (64-bit reference-order binning); untimed, for the PSNR side data."""
+    import nanotracer_b200 as nt
+    from nanotracer_b200._lib import SC_KEYS_NATIVE64
+    r, b = nt.Rasterizer(ctx), nt.TileBinner(ctx)
+    V = len(cams)
+    proj = r.alloc_projected(g, V)
+    r.project(g, cams, proj)
+    bins = b.bin(proj, g.n, tl, stride=g.capacity, n_views=V, key_mode=SC_KEYS_NATIVE64)
+    img = r.alloc_image(tl.width, tl.height, V)
+    r.composite(proj, bins, img, tl, stride=g.capacity, n_views=V)
+    return img.readback(np.float32).reshape(V, tl.height, tl.width, 4)
+
+
+def psnr_db(img4, tgt3) -> float:
+    x = np.asarray(img4, np.float64)[..., :3]
+    mse = float(np.mean((x - np.asarray(tgt3, np.float64)) ** 2))
+    return round(10.0 * math.log10(1.0 / max(mse, 1e-30)), 4)
+
+
+CROP = (928, 512, 64)  # x0, y0 and side of the 64x64 crop of view 0 (tile-aligned, image centre)
+
+
+def crop_fp64(host_splats, cam, W, H):
+    """The 64x64 crop of view 0 rendered by the oracle's FP64 instantiation:
+    projection of every splat in FP64, means shifted into the crop, 64-bit
+    (tile, depth) binning and blend of the crop's tiles.  A pixel's colour
+    depends only on its offset from each mean, so this is the crop of the
+    full FP64 render."""
+    from oracle import oracle as O
+    x0, y0, side = CROP
+    n = len(host_splats)
+    os_ = O.OSplats.from_buffer(host_splats)
+    rec = O.project(os_, O.camera_from_struct(bytes(cam.c)), "f64")
+    rec[:, 0] -= x0
+    rec[:, 1] -= y0
+    otl = O.tiling(side, side, 16, 16, 8.0)
+    _, pay, ranges = O.bin64(rec, 1, otl, "f64")
+    img, _, _ = O.composite(rec, pay, ranges.reshape(-1), otl, "f64")
+    del n
+    return img
+
+
+def quality(ctx, g, cams, tl, tgt, fp64=True):
+    """PSNR of a form's final parameters over the iteration's views, and on the
+    64x64 crop of view 0 for the GPU render and the FP64 oracle's render of the
+    same parameters (the "PSNR within 0.05 dB of the FP64 oracle" statement)."""
+    img = render_views(ctx, g, cams, tl)
+    out = {"psnr_views": psnr_db(img, tgt)}
+    if fp64:
+        x0, y0, side = CROP
+        tc = tgt[0, y0:y0 + side, x0:x0 + side]
+        gc = img[0, y0:y0 + side, x0:x0 + side]
+        oc = crop_fp64(g.readback(), cams[0], tl.width, tl.height)
+        out["crop_gpu"] = psnr_db(gc, tc)
+        out["crop_fp64"] = psnr_db(oc, tc)
+        out["crop_delta_db"] = round(out["crop_gpu"] - out["crop_fp64"], 4)
+        out["crop_max_abs_err"] = float(np.abs(gc.astype(np.float64) - oc).max())
+    return out
+
+
+def timed_run(ctx, torch, stream, tr, g, mo, acc, cams_seq, t):
+    """Steps over cams_seq between CUDA events on the library stream; returns (ms, t, loss)."""
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    loss = None
+    for cams in cams_seq:
+        t += 1
+        loss = tr.step(g, mo, acc, cams, t)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1), t, loss
+
+
+def side_forms(ctx, torch, stream, args, scene, tbuf, tgt0, cams0, tl, n_steps, main_form):
+    """The metric's other forms on the same box, from the same start, untimed
+    except for their own K steps: the batched form in the other precision, and
+    the plain FP32 form (one view per iteration, the reference's train() loop,
+    train.rs:155-250), whose iterations cycle through the same views with the
+    view's target copied into place every iteration (inside its timed region).
+    Every form's final parameters go through quality()."""
+    import nanotracer_b200 as nt
+    from nanotracer_b200.train import TrainConfig, Trainer
+    V, K, W = args.views, args.steps, args.warmup
+    out = {}
+    other = "fp32" if main_form == "bf16" else "bf16"
+    bf16 = other == "bf16"
+    cfg = TrainConfig(n_views=V, width=args.width, height=args.height, tile_w=tl.tile_w, tile_h=tl.tile_h,
+                      depth_max=8.0, exact_backward=True, use_graph=True, bf16=bf16, densify=False)
+    g = nt.GpuSplatBuffer.upload(ctx, scene, bf16_rest=bf16)
+    mo = nt.AdamMomentBuffers(ctx, g.capacity, bf16=bf16)
+    acc = ctx.storage_buffer_zeroed("grad_acc", 4 * g.capacity)
+    tr = Trainer(ctx, cfg)
+    tr.set_targets(tbuf)
+    t = 0
+    _, t, _ = timed_run(ctx, torch, stream, tr, g, mo, acc, [cams0] * (n_steps - K), t)
+    ms, t, _ = timed_run(ctx, torch, stream, tr, g, mo, acc, [cams0] * K, t)
+    out["batched_" + other] = {"iters_s": round(K / (ms / 1e3), 3), "ms_per_iter": round(ms / K, 4),
+                               "views_per_iter": V, "iters": t, **quality(ctx, g, cams0, tl, tgt0)}
+    del tr
+    # plain FP32: one view per iteration, V times as many iterations (the same views seen as often)
+    P3 = args.width * args.height * 3 * 4
+    cfg1 = TrainConfig(n_views=1, width=args.width, height=args.height, tile_w=tl.tile_w, tile_h=tl.tile_h,
+                       depth_max=8.0, exact_backward=True, use_graph=True, bf16=False, densify=False)
+    g1 = nt.GpuSplatBuffer.upload(ctx, scene)
+    mo1 = nt.AdamMomentBuffers(ctx, g1.capacity)
+    acc1 = ctx.storage_buffer_zeroed("grad_acc", 4 * g1.capacity)
+    one = ctx.storage_buffer_zeroed("target_view", P3)
+    tr1 = Trainer(ctx, cfg1)
+    tr1.set_targets(one)
+
+    def plain(iters, t):
+        for j in range(iters):
+            v = j % V
+            one.copy_from(tbuf, P3, src_offset=v * P3)
+            t += 1
+            tr1.step(g1, mo1, acc1, [cams0[v]], t)
+        return t
+
+    t1 = plain(V * (n_steps - K), 0)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    t1 = plain(V * K, t1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms1 = e0.elapsed_time(e1)
+    out["plain_fp32"] = {"iters_s": round(V * K / (ms1 / 1e3), 3), "ms_per_iter": round(ms1 / (V * K), 4),
+                         "views_per_iter": 1, "iters": t1, **quality(ctx, g1, cams0, tl, tgt0)}
+    del tr1
+    return out
+
+
 def run_ours(args):
     ws, rank, local, pg = dist_setup()
     if (ws > 1 and args.parallel == "views") or args.view_path:
@@ -179,8 +315,8 @@ def run_ours(args):
     bf16 = args.form == "bf16"
     cfg = TrainConfig(n_views=V, width=args.width, height=args.height, tile_w=args.tile_w, tile_h=args.tile_h,
                       depth_max=8.0, exact_backward=True, use_graph=True, bf16=bf16, densify=False)
-    # targets for the fixed set of views used by the timed steps (the camera
-    # orbit advances each step; targets are re-rendered per distinct step in e2e)
+    # the iteration's V views (radius-4 orbit, elevation jitter) and their targets;
+    # every step trains on them, so the loss and PSNR are meaningful
     cams0 = cams_for(0)
     tgt0 = render_targets(ctx, tscene, cams0, tl)
     tbuf = ctx.storage_buffer("targets", tgt0)
@@ -188,25 +324,25 @@ def run_ours(args):
     if args.autotune:  # untimed: scratch copies of the scene, before the timed trainer exists
         from nanotracer_b200.autotune import autotune
         cfg, trials = autotune(ctx, scene, cams0, tbuf, cfg)
-        tune = {"choice": f"{cfg.tile_w}x{cfg.tile_h} tiles, sort_mode {cfg.sort_mode}",
-                "trial_ms": {f"{t.tile_w}x{t.tile_h}/sort_mode {t.sort_mode}":
-                             (round(t.ms, 3) if t.ms is not None else t.error) for t in trials}}
+        tune = {"choice": f"{cfg.tile_w}x{cfg.tile_h} tiles, sort_mode {cfg.sort_mode}, blend batch "
+                          f"{cfg.blend_batch or 'all threads'}, sort digits {cfg.sort_digit_bits or 'auto'}",
+                "trial_ms": {t.label: (round(t.ms, 3) if t.ms is not None else t.error) for t in trials},
+                "identical_images": len({t.digest for t in trials if t.digest}) == 1}
         tl = nt.TilingParams(args.width, args.height, cfg.tile_w, 8.0, tile_h_override=cfg.tile_h)
     g = nt.GpuSplatBuffer.upload(ctx, scene, bf16_rest=bf16)
     mo = nt.AdamMomentBuffers(ctx, g.capacity, bf16=bf16)
     acc = ctx.storage_buffer_zeroed("grad_acc", 4 * g.capacity)
     tr = Trainer(ctx, cfg)
     tr.set_targets(tbuf)
-    cams_steps = [cams_for(s) for s in range(args.warmup + args.steps)]
     clk = ClockSampler(local, raw_copy=os.environ.get("BENCH_CLOCKS_CSV")).start()
     t = 0
     for s in range(args.warmup):
         t += 1
-        tr.step(g, mo, acc, cams_steps[s], t)
+        tr.step(g, mo, acc, cams0, t)
     tr.set_profiling(True)
     for s in range(2):  # graph rebuild with profiling events
         t += 1
-        tr.step(g, mo, acc, cams_steps[s], t)
+        tr.step(g, mo, acc, cams0, t)
     tr.set_profiling(True)  # reset the per-stage accumulators
     torch.cuda.synchronize(local)
     barrier(pg)
@@ -218,7 +354,7 @@ def run_ours(args):
     e0.record(stream)
     for s in range(args.steps):
         t += 1
-        loss = tr.step(g, mo, acc, cams_steps[args.warmup + s], t)
+        loss = tr.step(g, mo, acc, cams0, t)
     e1.record(stream)
     torch.cuda.synchronize(local)
     w1 = time.time()
@@ -229,6 +365,12 @@ def run_ours(args):
     launches = ctx.launch_count - launches0
     st = tr.stats()
     clocks = clk.summary(w0, w1)
+    n_steps = t
+    forms = None
+    if rank == 0 and ws == 1 and not args.no_forms:
+        forms = {"batched_" + args.form: {"iters_s": round(args.steps / (ms / 1e3), 3),
+                                          "ms_per_iter": round(ms / args.steps, 4), "views_per_iter": V,
+                                          "iters": n_steps, **quality(ctx, g, cams0, tl, tgt0)}}
 
     # ---- e2e through the public API: pinned host targets + cameras in, loss out
     e2e = None
@@ -241,7 +383,7 @@ def run_ours(args):
         tr.set_host_targets(pinned.data_ptr(), keepalive=pinned)
         h2d = pinned.numel() * 4 + V * 96
         t += 1
-        tr.step(g, mo, acc, cams_steps[args.warmup], t)  # re-capture the graph with the copy node (untimed)
+        tr.step(g, mo, acc, cams0, t)  # re-capture the graph with the copy node (untimed)
         torch.cuda.synchronize(local)
         barrier(pg)
         t0 = time.perf_counter()
@@ -250,13 +392,14 @@ def run_ours(args):
         f0.record(stream)
         for s in range(args.steps):
             t += 1
-            tr.step(g, mo, acc, cams_steps[args.warmup + s], t)
+            tr.step(g, mo, acc, cams0, t)
         f1.record(stream)
         torch.cuda.synchronize(local)
         wall = time.perf_counter() - t0
         e2e_ms = max_over_ranks(pg, max(f0.elapsed_time(f1), wall * 1e3))
         e2e = {"value": ws * args.steps / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": 24}
+    del tr
 
     # ---- roofline of the dominant stage
     stage = st["stage_ms"]
@@ -271,18 +414,21 @@ def run_ours(args):
     bw = st.get("blend_work") or {}
     fwd_list = bw.get("fwd_scanned", 0) * 8 + bw.get("fwd_blended", 0) * 48  # item words + blended records
     bwd_list = bw.get("bwd_scanned", 0) * 8 + bw.get("bwd_blended", 0) * 48
+    tile_passes = max(1, math.ceil(max(1, (V * tl.num_tiles() - 1).bit_length()) / 8))
     algo = {
         # records, zeroed gradient records, depth key, id, item count
         "project": N * (56 + rest_b) + V * N * (48 + 48 + 4 + 4 + 4),
-        "depth_sort": 5 * V * N * 24,
+        # segmented onesweep over u32 depth keys: a histogram read, then 4 passes of 8-bit
+        # digits each reading and writing key + id
+        "depth_sort": V * N * 4 + 4 * V * N * 16,
         "count_scan": V * N * (4 + 4 + 4) + V * N * 8,
         "emit": V * N * (4 + 16 + 4) + K * 8,
-        "tile_sort": 2 * K * 16 + K * 4,
+        "tile_sort": K * 4 + tile_passes * K * 16,
         "ranges": K * 4 + tiles * 8,
         # two-level binning: items (member mask | super tile, splat); the blends
         # read each tile's super-tile item list up to where its pixels saturate
         "item_emit": V * N * (4 + 16 + 4) + items * 8,
-        "item_sort": 2 * items * 16 + items * 4,
+        "item_sort": items * 4 + items * 16,   # histogram read + one 9-bit pass
         "item_ranges": items * 4,
         "blend_fwd": fwd_list + V * P * (16 + 8),
         "blend_bwd": bwd_list + V * P * (16 + 8 + 12) + V * N * 48,
@@ -297,14 +443,23 @@ def run_ours(args):
                 "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4),
                 "traffic": profiled_traffic(dom, V),
                 "peak_source": peaks["source"], "algorithmic_bytes": int(algo[dom]), "avg_ms": round(dom_ms, 4),
-                "stage_ms": {k: round(v, 4) for k, v in stage.items()}, "blend_work": bw}
+                "stage_ms": {k: round(v, 4) for k, v in stage.items()}, "blend_work": bw,
+                "stage_frac_of_peak": {k: round(algo[k] / (v / 1e3) / 1e9 / peaks["hbm_gbs"], 4)
+                                       for k, v in stage.items() if k in algo and v > 0}}
+
+    if forms is not None:
+        forms.update(side_forms(ctx, torch, stream, args, scene, tbuf, tgt0, cams0, tl, n_steps, args.form))
+        b, f, p = forms.get("batched_bf16"), forms.get("batched_fp32"), forms.get("plain_fp32")
+        forms["bf16_over_fp32_batched"] = round(b["iters_s"] / f["iters_s"], 4) if b and f else None
+        forms["bf16_batched_over_fp32_plain_iters"] = round(b["iters_s"] / p["iters_s"], 4) if b and p else None
+        forms["bf16_batched_over_fp32_plain_views"] = \
+            round(b["iters_s"] * V / p["iters_s"], 4) if b and p else None
+        forms["psnr_delta_db_bf16_vs_fp32_batched"] = round(b["psnr_views"] - f["psnr_views"], 4) if b and f else None
+        forms["crop"] = f"64x64 at ({CROP[0]}, {CROP[1]}) of view 0; FP64 = the oracle's double instantiation"
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args, scene, tscene, tl, cams_for)
-    psnr = None
-    if rank == 0 and ws == 1 and not args.no_psnr:
-        psnr = psnr_check(ctx, args)
+        cpu = cpu_baseline(args, scene, tl, cams0)
 
     if rank == 0:
         line = {
@@ -321,14 +476,108 @@ def run_ours(args):
                        "l2": "inputs larger than L2 (params, item lists and images >> 126 MB)",
                        "parallelism": f"{ws} GPUs, one scene each (no exchange)" if ws > 1 else "single GPU"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-            "clocks": clocks, "loss": loss, "psnr": psnr,
+            "clocks": clocks, "loss": loss, "forms": forms,
         }
         if tune is not None:
             line["config"]["autotune"] = tune
         print(json.dumps(line))
-    del tr
     if pg is not None:
         pg.destroy_process_group()
+
+
+def run_precision(args):
+    """BASELINE config 4 (the precision form), a side line beside the headline:
+    3M splats, 4 views of 1920x1080 per iteration, SH-rest and Adam moments in
+    BF16, blending and gradient sums in FP32, with and without the compensated
+    cross-tile gradient sums.  Reports each variant's iterations/s, the
+    per-image PSNR against the targets over the full views and, on the 64x64
+    crop of each view, the GPU render's and the FP64 oracle's (same
+    parameters), and the projected-gradient error on the crop against the
+    FP64 oracle's adjoint (same records, bins, image and dL/dC; the crop's
+    dL/dC only, so the oracle runs in seconds), plain and compensated."""
+    import torch
+
+    import nanotracer_b200 as nt
+    from nanotracer_b200._lib import SC_BWD_EXACT, SC_KEYS_NATIVE64
+    from nanotracer_b200.train import TrainConfig, Trainer
+    from oracle import oracle as O
+    O.set_threads(O.max_threads())
+    ctx = nt.CudaCtx(0)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
+    scene, tscene, tl, cams_for, render_targets = make_workload(args, 0, ctx)
+    V, W, H = args.views, args.width, args.height
+    cams0 = cams_for(0)
+    tgt0 = render_targets(ctx, tscene, cams0, tl)
+    tbuf = ctx.storage_buffer("targets", tgt0)
+    out = {"metric": "config 4 precision form: iters/s and error against the FP64 oracle", "unit": UNIT,
+           "config": {"workload": f"{len(scene)} splats, {V} views x {W}x{H} per iteration, BF16 SH-rest + Adam "
+                                  f"moments, FP32 blend and gradient sums", "crop": f"64x64 at ({CROP[0]}, "
+                                  f"{CROP[1]}) of every view"}}
+    for comp in (False, True):
+        cfg = TrainConfig(n_views=V, width=W, height=H, tile_w=args.tile_w, tile_h=args.tile_h, depth_max=8.0,
+                          exact_backward=True, use_graph=True, bf16=True, densify=False, compensated_sums=comp)
+        g = nt.GpuSplatBuffer.upload(ctx, scene, bf16_rest=True)
+        mo = nt.AdamMomentBuffers(ctx, g.capacity, bf16=True)
+        acc = ctx.storage_buffer_zeroed("grad_acc", 4 * g.capacity)
+        tr = Trainer(ctx, cfg)
+        tr.set_targets(tbuf)
+        _, t, _ = timed_run(ctx, torch, stream, tr, g, mo, acc, [cams0] * max(3, args.warmup), 0)
+        ms, t, _ = timed_run(ctx, torch, stream, tr, g, mo, acc, [cams0] * args.steps, t)
+        del tr
+        img = render_views(ctx, g, cams0, tl)
+        x0, y0, side = CROP
+        host = g.readback()
+        per_view = []
+        for v in range(V):
+            tc = tgt0[v, y0:y0 + side, x0:x0 + side]
+            oc = crop_fp64(host, cams0[v], W, H)
+            gc = img[v, y0:y0 + side, x0:x0 + side]
+            per_view.append({"psnr_full": psnr_db(img[v], tgt0[v]), "crop_gpu": psnr_db(gc, tc),
+                             "crop_fp64": psnr_db(oc, tc), "crop_delta_db": round(psnr_db(gc, tc) - psnr_db(oc, tc), 4),
+                             "crop_max_abs_err": float(np.abs(gc.astype(np.float64) - oc).max())})
+        out["compensated" if comp else "plain"] = {"iters_s": round(args.steps / (ms / 1e3), 3),
+                                                   "ms_per_iter": round(ms / args.steps, 4), "iters": t,
+                                                   "views": per_view}
+        del g, mo, acc
+    # projected-gradient error on the crop of view 0: the records shifted into the crop, binned for it
+    x0, y0, side = CROP
+    pipe_g = nt.GpuSplatBuffer.upload(ctx, scene, bf16_rest=True)
+    r = nt.Rasterizer(ctx)
+    proj = r.alloc_projected(pipe_g, 1)
+    r.project(pipe_g, [cams0[0]], proj)
+    rec = proj.readback(np.float32).reshape(-1, 12)[:len(scene)].copy()
+    rec[:, 0] -= x0
+    rec[:, 1] -= y0
+    ctl = nt.TilingParams(side, side, 16, 8.0)
+    cproj = ctx.storage_buffer("crop_records", rec)
+    bins = nt.TileBinner(ctx).bin(cproj, len(scene), ctl, key_mode=SC_KEYS_NATIVE64)
+    cimg, caux = r.alloc_image(side, side), r.alloc_aux(side, side)
+    r.composite(cproj, bins, cimg, ctl, stride=len(scene), aux=caux)
+    gimg = cimg.readback(np.float32).reshape(side, side, 4)
+    aux = caux.readback(np.uint32).reshape(side, side, 2)
+    _, dl = O.mse(gimg, tgt0[0, y0:y0 + side, x0:x0 + side])
+    dlb = ctx.storage_buffer("dl", dl.reshape(-1, 4).astype(np.float32))
+    grads = {}
+    for comp in (False, True):
+        pg = ctx.storage_buffer_zeroed("pg", len(scene) * 48)
+        r.composite_backward(cproj, bins, cimg, dlb, pg, ctl, stride=len(scene), mode=SC_BWD_EXACT, aux=caux,
+                             compensated=comp)
+        grads[comp] = pg.readback(np.float32).reshape(-1, 12)
+    otl = O.tiling(side, side, 16, 16, 8.0)
+    _, pay, ranges = O.bin64(rec, 1, otl)
+    ref = O.composite_backward(rec.astype(np.float64), pay, ranges.reshape(-1), otl,
+                               gimg.reshape(-1, 4).astype(np.float64), dl.astype(np.float64), SC_BWD_EXACT,
+                               aux[..., 1].reshape(-1), aux[..., 0].view(np.float32).reshape(-1).astype(np.float64),
+                               "f64")
+    cols = [0, 1, 2, 4, 5, 6, 8, 9, 10]
+    live = np.abs(ref[:, cols]).max(1) > 0
+    for comp in (False, True):
+        e = np.linalg.norm(grads[comp][live][:, cols] - ref[live][:, cols], axis=1) / \
+            np.linalg.norm(ref[live][:, cols], axis=1)
+        out["compensated" if comp else "plain"]["crop_grad_rel_err"] = {
+            "splats": int(live.sum()), "median": float(np.median(e)), "p99": float(np.percentile(e, 99)),
+            "max": float(e.max())}
+    print(json.dumps(out))
 
 
 def run_views(args, ws, rank, local, pg):
@@ -464,64 +713,33 @@ def run_views(args, ws, rank, local, pg):
         pg.destroy_process_group()
 
 
-def psnr_check(ctx, args, iters=100, n=200_000, V=4, W=480, H=272):
-    """The metric's "same PSNR" claim, measured beside the timed run (untimed):
-    the same seeded scene trained `iters` iterations in the BF16 form and in
-    the plain FP32 form on V fixed views; PSNR of the final renders against
-    the targets (values in [0, 1])."""
-    import nanotracer_b200 as nt
-    from nanotracer_b200.scene import FOV_Y, orbit_views, perturbed, random_scene
-    from nanotracer_b200.train import TrainConfig, Trainer, render_targets
-    scene = random_scene(n, 0x5EED5EED)
-    tl = nt.TilingParams(W, H, 16, 8.0)
-    cams = [nt.CameraUniform.from_pose(*p, FOV_Y, W, H, n) for p in orbit_views(V, 0)]
-    tgt = render_targets(ctx, perturbed(scene), cams, tl)
-    out = {}
-    for form in ("bf16", "fp32"):
-        bf16 = form == "bf16"
-        cfg = TrainConfig(n_views=V, width=W, height=H, tile_w=16, tile_h=16, depth_max=8.0, exact_backward=True,
-                          use_graph=True, bf16=bf16, densify=False)
-        g = nt.GpuSplatBuffer.upload(ctx, scene, bf16_rest=bf16)
-        mo = nt.AdamMomentBuffers(ctx, g.capacity, bf16=bf16)
-        acc = ctx.storage_buffer_zeroed("acc", 4 * g.capacity)
-        tr = Trainer(ctx, cfg)
-        tb = ctx.storage_buffer("targets", tgt)
-        tr.set_targets(tb)
-        for t in range(1, iters + 1):
-            tr.step(g, mo, acc, cams, t)
-        img = tr.images()[..., :3]
-        mse = float(np.mean((img.astype(np.float64) - tgt) ** 2))
-        out[form] = round(10.0 * math.log10(1.0 / max(mse, 1e-30)), 3)
-        del tr
-    out["delta_db"] = round(out["bf16"] - out["fp32"], 3)
-    out["workload"] = f"{n} splats, {V} views {W}x{H}, {iters} iterations from the same start, exact backward"
-    return out
-
-
-def cpu_baseline(args, scene, tscene, tl, cams_for):
-    """The oracle (CPU restatement of the reference path) on the host cores: one
-    view of the workload per sample (fwd+bwd over all splats + Adam over all
-    parameters); an iteration of n_views views is counted as n_views samples."""
+def cpu_baseline(args, scene, tl, cams):
+    """The oracle (the CPU restatement of the reference path) on all host
+    cores: one whole iteration of the workload (the V views' forward and
+    backward over all splats, one Adam step) on the iteration's views."""
     from oracle import oracle as O
+    from nanotracer_b200.train import BENCH_LRS
     threads = O.max_threads()
     O.set_threads(threads)
-    cams = cams_for(0)[:1]
     n = len(scene)
     os_ = O.OSplats.from_buffer(scene)
     om, ov = O.OSplats.zeros(n), O.OSplats.zeros(n)
     acc = np.zeros(n, np.float32)
     ocams = [O.camera_from_struct(bytes(c.c)) for c in cams]
-    # target of that view from the oracle itself (the CPU path renders its own ground truth)
-    tgt = np.zeros((tl.height, tl.width, 3), np.float32)
+    tgt = np.zeros((len(cams), tl.height, tl.width, 3), np.float32)
     otl = O.tiling(tl.width, tl.height, tl.tile_w, tl.tile_h, tl.depth_max)
-    from nanotracer_b200.train import BENCH_LRS
     t0 = time.perf_counter()
     O.train_step(os_, om, ov, acc, ocams, tgt, otl, 1, BENCH_LRS, 1)
     dt = time.perf_counter() - t0
-    per_iter = dt * args.views
-    return {"value": 1.0 / per_iter, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"1 of {args.views} views ({n} splats, {tl.width}x{tl.height}) fwd+bwd+Adam in {dt:.2f} s; "
-                      f"iteration time = {args.views} x sample"}
+    return {"value": 1.0 / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"one whole iteration ({len(cams)} views of {tl.width}x{tl.height}, {n} splats, "
+                      f"fwd+bwd+Adam) in {dt:.2f} s"}
+
+
+# The reference arm's bounded run: a few whole iterations (each one takes tens
+# of seconds on the host cores), after fewer warm-up iterations than asked.
+REF_MAX_STEPS = 3
+REF_MAX_WARMUP = 1
 
 
 def run_reference(args):
@@ -529,39 +747,52 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from nanotracer_b200.scene import FOV_Y, orbit_views, perturbed, random_scene
-    import nanotracer_b200 as nt
+    from nanotracer_b200.scene import FOV_Y, orbit_views, random_scene
     from oracle import oracle as O
     from nanotracer_b200.train import BENCH_LRS
     threads = O.max_threads()
-    O.set_threads(threads)
-    n = args.splats
+    n, V, W, H = args.splats, args.views, args.width, args.height
     scene = random_scene(n, 0x5EED5EED)
-    # bounded sample: one of the iteration's views per step, full resolution
-    W, H = args.width, args.height
     otl = O.tiling(W, H, args.tile_w, args.tile_h, 8.0)
-    os_ = O.OSplats.from_buffer(scene)
-    om, ov = O.OSplats.zeros(n), O.OSplats.zeros(n)
-    acc = np.zeros(n, np.float32)
-    tgt = np.zeros((H, W, 3), np.float32)
-    cam_at = lambda s: [O.camera(*orbit_views(1, s)[0], FOV_Y, W, H, n)]
-    for s in range(args.warmup):
-        O.train_step(os_, om, ov, acc, cam_at(s), tgt, otl, 1, BENCH_LRS, s + 1)
+    cams = [O.camera(*p, FOV_Y, W, H, n) for p in orbit_views(V, 0)]
+    tgt = np.zeros((V, H, W, 3), np.float32)
+
+    def fresh():
+        return O.OSplats.from_buffer(scene), O.OSplats.zeros(n), O.OSplats.zeros(n), np.zeros(n, np.float32)
+
+    # all host threads: whole V-view iterations
+    O.set_threads(threads)
+    os_, om, ov, acc = fresh()
+    warm = min(args.warmup, REF_MAX_WARMUP)
+    steps = max(1, min(args.steps, REF_MAX_STEPS))
+    t = 0
+    for _ in range(warm):
+        t += 1
+        O.train_step(os_, om, ov, acc, cams, tgt, otl, 1, BENCH_LRS, t)
     t0 = time.perf_counter()
-    for s in range(args.steps):
-        O.train_step(os_, om, ov, acc, cam_at(args.warmup + s), tgt, otl, 1, BENCH_LRS, args.warmup + s + 1)
-    dt = (time.perf_counter() - t0) / args.steps
-    # a full iteration = n_views such samples (Adam over all parameters is
-    # counted once per sample, so the CPU iteration time is an upper estimate)
-    per_iter = dt * args.views
+    for _ in range(steps):
+        t += 1
+        O.train_step(os_, om, ov, acc, cams, tgt, otl, 1, BENCH_LRS, t)
+    per_iter = (time.perf_counter() - t0) / steps
     v = 1.0 / per_iter
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": per_iter * 1e3, "higher_is_better": True, "scaling": "weak",
+    # one thread: one view of the iteration (fwd+bwd over all splats, Adam over all parameters)
+    O.set_threads(1)
+    os1, om1, ov1, acc1 = fresh()
+    s0 = time.perf_counter()
+    O.train_step(os1, om1, ov1, acc1, cams[:1], tgt[:1], otl, 1, BENCH_LRS, 1)
+    one_view = time.perf_counter() - s0
+    O.set_threads(threads)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": steps,
+            "warmup": warm, "ms_per_step": per_iter * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic seeded scene",
-            "config": {"workload": f"{n} splats, {args.views} views x {args.width}x{args.height} per iteration"},
+            "config": {"workload": f"{n} splats, {V} views x {W}x{H} per iteration"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"1 of the {args.views} views at {W}x{H}, fwd+bwd+Adam over all {n} splats "
-                                       f"per step, {dt:.2f} s; iteration = {args.views} x sample"},
+                             "sample": f"{steps} whole iterations ({V} views, fwd+bwd over all {n} splats, one Adam "
+                                       f"step each) after {warm} warm-up; asked for {args.steps} / {args.warmup}, "
+                                       f"capped at {REF_MAX_STEPS} / {REF_MAX_WARMUP} to stay within minutes"},
+            "cpu_1thread": {"seconds_per_view": round(one_view, 2), "cores": 1,
+                            "iters_s_estimate": 1.0 / (one_view * V),
+                            "sample": f"1 of the {V} views on one thread; iteration estimate = {V} x sample"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -586,8 +817,18 @@ def main():
                     help="time every tile shape x binning path first (untimed) and run the fastest")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-psnr", action="store_true", help="skip the untimed BF16-vs-FP32 PSNR side run")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the other forms' side runs (batched other precision, plain FP32) and their PSNR")
+    ap.add_argument("--no-psnr", action="store_true", help=argparse.SUPPRESS)  # older name of --no-forms
+    ap.add_argument("--workload", default="batched", choices=["batched", "precision"],
+                    help="precision: the config-4 side line (3M splats, 4 views, BF16, FP64-oracle errors)")
     args = ap.parse_args()
+    args.no_forms = args.no_forms or args.no_psnr
+    if args.workload == "precision":
+        if args.splats == 1_000_000 and args.views == 8:  # config 4's sizes unless given
+            args.splats, args.views = 3_000_000, 4
+        run_precision(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -159,6 +159,9 @@ sc_status sc_buffer_free(sc_ctx* ctx, void* dptr);
 sc_status sc_buffer_upload(sc_ctx* ctx, void* dst, const void* src, size_t bytes);   /* queue.write_buffer */
 sc_status sc_buffer_readback(sc_ctx* ctx, void* dst, const void* src, size_t bytes); /* readback, gpu.rs:119-152 */
 sc_status sc_buffer_zero(sc_ctx* ctx, void* dptr, size_t bytes);
+/* device-to-device copy, asynchronous on the context's stream
+ * (encoder.copy_buffer_to_buffer, as used by gpu.rs:119-152) */
+sc_status sc_buffer_copy(sc_ctx* ctx, void* dst, const void* src, size_t bytes);
 
 /* ------------------------------------------------------------- parameters
  * replaces GpuSplatBuffer / GradSplatBuffers / AdamMomentBuffers
@@ -280,6 +283,24 @@ sc_status sc_composite_backward(sc_ctx* ctx, const sc_projected_splat* projected
                                 const float* forward_out, const float* dl_dc, sc_bwd_mode mode,
                                 const uint32_t* aux, sc_projected_grad* projected_grad); /* raster.rs:653-724 */
 
+/* sc_composite_backward with options (flags):
+ * SC_BWD_FLAG_COMPENSATED: the per-(view, splat) gradient totals across
+ *   tiles are compensated sums.  The reference adds each (pixel, splat) term
+ *   with a CAS float atomic in arrival order (rasterize_backward.wgsl:62-71,
+ *   188-200), and plain float atomics here add one term per (tile, splat);
+ *   with the flag every tile's term is added by an atomic that returns the
+ *   old total, the exact rounding error of that addition (Knuth's TwoSum) is
+ *   accumulated in a compensation record, and the two are added once at the
+ *   end: the total is then within about one rounding of the exact sum of the
+ *   tiles' terms, whatever their number and order.  Costs a second 48-byte
+ *   record per (view, splat) (library scratch here) and 18 scalar atomics per
+ *   (tile, splat) instead of 3 vector ones. */
+#define SC_BWD_FLAG_COMPENSATED 1u
+sc_status sc_composite_backward_ex(sc_ctx* ctx, const sc_projected_splat* projected, uint32_t stride_splats,
+                                   uint32_t n_views, const sc_bins* bins, const sc_tiling* tiling,
+                                   const float* forward_out, const float* dl_dc, sc_bwd_mode mode,
+                                   const uint32_t* aux, sc_projected_grad* projected_grad, uint32_t flags);
+
 /* project_backward.wgsl:79-304 for one view; overwrites grads (accumulate = 0)
  * or adds into them (accumulate = 1, multi-view sums). */
 sc_status sc_project_backward(sc_ctx* ctx, const sc_splats* s, const sc_projected_grad* projected_grad,
@@ -341,7 +362,9 @@ typedef struct sc_train_config {
   sc_adam_groups adam;         /* per-group learning rates                        */
   uint32_t bwd_mode;           /* sc_bwd_mode                                    */
   uint32_t use_graph;          /* capture the iteration as a CUDA graph          */
-  uint32_t blend_batch;        /* reserved, 0 (the blend stages one splat per thread per batch) */
+  uint32_t blend_batch;        /* blend batch depth: list positions the blend kernels stage per batch
+                                  (a multiple of 32, capped at the tile's thread count); 0 = one per
+                                  thread (tile pixels / 2 with two pixels per thread) */
   uint32_t sort_mode;          /* 0 = auto (two-level), 1 = depth presort + stable sort of the
                                   (tile, splat) pairs, 2 = depth presort + two-level binning
                                   (super tiles of 4x4 tiles, per-tile lists filled in depth order) */
@@ -352,6 +375,10 @@ typedef struct sc_train_config {
                                   train.rs:52); 0 = MSE only, fused into the blend */
   uint32_t fp64_det;           /* FP64 determinant and inverse of near-degenerate splats in the projection
                                   and its adjoint (as sc_ctx_set_fp64_det) */
+  uint32_t compensated_sums;   /* per-(view, splat) gradient totals across tiles as TwoSum-compensated
+                                  atomic sums (as SC_BWD_FLAG_COMPENSATED) */
+  uint32_t sort_digit_bits;    /* radix digit width of the binning sort (items or pairs): 8 or 9 bits per
+                                  onesweep pass, 0 = fewer passes wins (radix_sort.rs:1-26 uses 1 bit) */
 } sc_train_config;
 
 sc_status sc_trainer_create(sc_ctx* ctx, const sc_train_config* cfg, sc_trainer** out);

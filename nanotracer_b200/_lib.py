@@ -24,6 +24,7 @@ SC_BWD_REF = 0
 SC_BWD_EXACT = 1
 SC_KEYS_REF32 = 0
 SC_KEYS_NATIVE64 = 1
+SC_BWD_FLAG_COMPENSATED = 1
 
 
 class SplatCudaError(RuntimeError):
@@ -60,7 +61,8 @@ class sc_train_config(C.Structure):
                 ("use_graph", C.c_uint32), ("blend_batch", C.c_uint32), ("sort_mode", C.c_uint32),
                 ("tile_cull", C.c_uint32),
                 ("log_scale_min", C.c_float), ("log_scale_max", C.c_float), ("opacity_logit_max", C.c_float),
-                ("ssim_lambda", C.c_float), ("fp64_det", C.c_uint32)]
+                ("ssim_lambda", C.c_float), ("fp64_det", C.c_uint32), ("compensated_sums", C.c_uint32),
+                ("sort_digit_bits", C.c_uint32)]
 
 
 assert C.sizeof(sc_camera) == 96
@@ -90,6 +92,7 @@ _PROTOS = {
     "sc_buffer_upload": (ST, [P, P, P, C.c_size_t]),
     "sc_buffer_readback": (ST, [P, P, P, C.c_size_t]),
     "sc_buffer_zero": (ST, [P, P, C.c_size_t]),
+    "sc_buffer_copy": (ST, [P, P, P, C.c_size_t]),
     "sc_splats_upload": (ST, [P, C.POINTER(sc_host_splats), U32, U32, C.POINTER(P)]),
     "sc_splats_sync_from": (ST, [P, P, C.POINTER(sc_host_splats)]),
     "sc_splats_readback": (ST, [P, P, C.POINTER(sc_host_splats)]),
@@ -120,6 +123,7 @@ _PROTOS = {
     "sc_ssim_loss_grad": (ST, [P, P, P, U32, C.POINTER(sc_tiling), F32, P, P]),
     "sc_combined_loss_grad": (ST, [P, P, P, U32, C.POINTER(sc_tiling), F32, F32, P, P]),
     "sc_composite_backward": (ST, [P, P, U32, U32, P, C.POINTER(sc_tiling), P, P, I32, P, P]),
+    "sc_composite_backward_ex": (ST, [P, P, U32, U32, P, C.POINTER(sc_tiling), P, P, I32, P, P, U32]),
     "sc_project_backward": (ST, [P, P, P, P, P, I32]),
     "sc_tonemap": (ST, [P, P, U32, U32, P]),
     "sc_adam_step": (ST, [P, P, P, P, P, U64, F32, U64, C.POINTER(sc_adam_config)]),

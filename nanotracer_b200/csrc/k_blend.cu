@@ -4,8 +4,9 @@
 // PPT vertically adjacent pixels (a warp covers a compact tile_w x (32/tile_w*PPT)
 // block), two of them in packed f32x2 arithmetic.  The tile's depth-ordered
 // list — its own pair list, or its super tile's item list filtered by the
-// member masks — is staged into shared memory in batches of blockDim list
-// positions with cp.async (3 x 16 B per record), double buffered so the gather
+// member masks — is staged into shared memory in batches of B list positions
+// (the blend batch depth: one per thread by default, fewer when configured)
+// with cp.async (3 x 16 B per record), double buffered so the gather
 // of batch b+1 overlaps the blending of batch b, and the CTA leaves as soon as
 // every pixel is saturated (T < 1e-4).  The MSE of loss.rs:163-179 — dL/dC =
 // scale * 2 (C - target) / (3 W H) per pixel, squared errors reduced per CTA
@@ -26,6 +27,7 @@ namespace sck {
 struct BlendArgs {
   uint32_t width, height, tw, th, tiles_x, tiles_y, num_tiles, stride;
   uint64_t pixels;  // per view
+  uint32_t batch;   // list positions staged per batch, at most the block's threads
 };
 
 static BlendArgs blend_args(const sc_tiling* tl, uint32_t stride) {
@@ -36,7 +38,15 @@ static BlendArgs blend_args(const sc_tiling* tl, uint32_t stride) {
   a.num_tiles = a.tiles_x * a.tiles_y;
   a.stride = stride;
   a.pixels = (uint64_t)tl->width * tl->height;
+  a.batch = 0;
   return a;
+}
+
+// the batch depth for a launch of `threads` threads: `batch` rounded down to
+// whole warps and capped at the threads (each stages one position), 0 = threads
+static uint32_t batch_depth(uint32_t batch, uint32_t threads) {
+  batch &= ~31u;
+  return (batch == 0 || batch > threads) ? threads : batch;
 }
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -169,7 +179,7 @@ __device__ __forceinline__ uint2 list_range(const ListArgs& l, const BlendArgs& 
   return l.ranges[(size_t)v * l.super_per_view + (ty / SC_SUPER) * l.super_x + tx / SC_SUPER];
 }
 
-// Staging a batch of list positions [p0, p1) (at most blockDim of them) as
+// Staging a batch of list positions [p0, p1) (at most B <= blockDim of them) as
 // entries takes two calls, so that a batch's list words are loaded one batch
 // ahead of their use: fetch_list loads this thread's position (the id and, for
 // item lists, the key); place_list then stages the entries — each one's record
@@ -245,7 +255,7 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
   __shared__ double sred[8];
   __shared__ uint32_t s_wcnt[2][8];
   if (skip && (*skip & SC_DEVERR_CAPACITY)) return;  // the lists of this step are incomplete
-  const uint32_t B = blockDim.x;
+  const uint32_t B = a.batch;
   uint32_t* spos = reinterpret_cast<uint32_t*>(sbuf + (size_t)6 * B);
   const uint32_t vt = blockIdx.x;
   const uint32_t v = vt / a.num_tiles, tile = vt - v * a.num_tiles;
@@ -364,7 +374,7 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
         }
       }
     }
-    if (__syncthreads_count(all_done) == (int)B) break;
+    if (__syncthreads_count(all_done) == (int)blockDim.x) break;
   }
   cp_async_wait_all();
   add_work(work, w_scan, w_staged);
@@ -393,7 +403,9 @@ static sc_status composite_ppt(sc_ctx* ctx, const BlendArgs& a, uint32_t grid, u
                                const ListArgs& l, float4* image, uint2* aux, const float* target, float gscale,
                                float4* dl_dc, double* loss, const uint32_t* d_skip, uint64_t* work) {
   const size_t smem = (size_t)2 * 3 * threads * sizeof(float4) + (size_t)2 * threads * sizeof(uint32_t);
-  k_composite<PPT, LIST><<<grid, threads, smem, ctx->stream>>>(rec, l, a, image, aux, target, gscale, dl_dc, loss,
+  BlendArgs ab = a;
+  ab.batch = batch_depth(a.batch, threads);
+  k_composite<PPT, LIST><<<grid, threads, smem, ctx->stream>>>(rec, l, ab, image, aux, target, gscale, dl_dc, loss,
                                                                d_skip,
                                                                reinterpret_cast<unsigned long long*>(work));
   return sc_check_launch(ctx, "k_composite");
@@ -410,8 +422,10 @@ static int pick_ppt(const sc_tiling* tl) {
 template <int LIST>
 static sc_status composite_list(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views, const ListArgs& l,
                                 const sc_tiling* tl, float4* image, uint2* aux, const float* target, float mse_scale,
-                                float4* dl_dc, double* loss, const uint32_t* d_skip, uint64_t* work) {
-  const BlendArgs a = blend_args(tl, stride);
+                                float4* dl_dc, double* loss, const uint32_t* d_skip, uint64_t* work,
+                                uint32_t batch) {
+  BlendArgs a = blend_args(tl, stride);
+  a.batch = batch;
   const uint32_t pixels = tl->tile_w * tl->tile_h;
   if (pixels > 512 || pixels % 32 != 0) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile must hold 32..512 pixels, multiple of 32");
   const uint64_t grid = (uint64_t)n_views * a.num_tiles;
@@ -432,18 +446,19 @@ sc_status launch_composite(sc_ctx* ctx, const float4* rec, uint32_t stride, uint
                            float mse_scale, float4* dl_dc, double* loss, const uint32_t* d_skip) {
   ListArgs l{payloads, reinterpret_cast<const uint2*>(ranges), nullptr, 0, 0};
   return composite_list<LIST_PAIRS>(ctx, rec, stride, n_views, l, tl, image, aux, target, mse_scale, dl_dc, loss,
-                                    d_skip, nullptr);
+                                    d_skip, nullptr, 0);
 }
 
 sc_status launch_composite_items(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
                                  const uint32_t* item_keys, const uint32_t* item_ids, const uint32_t* item_ranges,
                                  const sc_tiling* tl, float4* image, uint2* aux, const float* target, float mse_scale,
-                                 float4* dl_dc, double* loss, const uint32_t* d_skip, uint64_t* work) {
+                                 float4* dl_dc, double* loss, const uint32_t* d_skip, uint64_t* work,
+                                 uint32_t batch) {
   const BlendArgs a = blend_args(tl, stride);
   ListArgs l{item_ids, reinterpret_cast<const uint2*>(item_ranges), item_keys, (a.tiles_x + SC_SUPER - 1) / SC_SUPER,
              super_tiles_per_view(tl)};
   return composite_list<LIST_ITEMS>(ctx, rec, stride, n_views, l, tl, image, aux, target, mse_scale, dl_dc, loss,
-                                    d_skip, work);
+                                    d_skip, work, batch);
 }
 
 // ---------------------------------------------------------------- MSE (standalone)
@@ -523,12 +538,37 @@ __device__ __forceinline__ int rs_owner(int lane) {
 // registers; more than 3 do not fit the 32 lanes.
 constexpr int RS_E = 2;
 
+// Compensated accumulation of x into the sum *s, the rounding error of the
+// addition going to *c: the atomic returns the old sum, the device forms the
+// same rounded sum again (an atomic float add rounds to nearest) and Knuth's
+// TwoSum gives the exact error of that addition.  *s + *c then carries the
+// total to within about one rounding of the final value, whatever the number
+// and the order of the tiles that add to it (plain float atomics: an error
+// growing with the number of additions and their magnitudes).
+__device__ __forceinline__ void twosum_atomic_add(float* s, float* c, float x) {
+  if (x == 0.0f) return;
+  const float old = atomicAdd(s, x);
+  const float sum = __fadd_rn(old, x);
+  const float bp = __fsub_rn(sum, old);
+  const float err = __fadd_rn(__fsub_rn(old, __fsub_rn(sum, bp)), __fsub_rn(x, bp));
+  if (err != 0.0f) atomicAdd(c, err);
+}
+__device__ __forceinline__ void twosum_atomic_add4(float4* s, float4* c, float4 x) {
+  float* sp = reinterpret_cast<float*>(s);
+  float* cp = reinterpret_cast<float*>(c);
+  twosum_atomic_add(sp, cp, x.x);
+  twosum_atomic_add(sp + 1, cp + 1, x.y);
+  twosum_atomic_add(sp + 2, cp + 2, x.z);
+}
+
 // MODE is the sc_bwd_mode.  In exact mode a pixel takes part from its last
 // contributor down to the start of the tile's list and never stops early, so
 // the early-exit bookkeeping exists only in reference mode.
 // With a target, the MSE's dL/dC (and the loss, added to loss[view]) is formed
 // here from the forward image instead of being read from dl_dc.
-template <int PPT, int MODE, int LIST>
+// COMP: the per-(view, splat) totals across tiles are accumulated with
+// twosum_atomic_add into proj_grad and the compensation records proj_comp.
+template <int PPT, int MODE, int LIST, bool COMP>
 __global__ void __launch_bounds__(256) k_composite_backward(const float4* __restrict__ rec, ListArgs l, BlendArgs a,
                                                             const float4* __restrict__ fwd,
                                                             const float4* __restrict__ dl_dc,
@@ -537,14 +577,15 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
                                                             const uint2* __restrict__ aux,
                                                             float4* __restrict__ proj_grad,
                                                             const uint32_t* __restrict__ skip,
-                                                            unsigned long long* __restrict__ work) {
+                                                            unsigned long long* __restrict__ work,
+                                                            float4* __restrict__ proj_comp) {
   // records [2][B][3], acc [B][3] (float4), ids [2][B], item positions [2][B] (u32)
   extern __shared__ float4 sbuf[];
   __shared__ uint32_t s_max;
   __shared__ double s_red[8];
   __shared__ uint32_t s_wcnt[2][8];
   if (skip && (*skip & SC_DEVERR_CAPACITY)) return;
-  const uint32_t B = blockDim.x;
+  const uint32_t B = a.batch;
   float4* sacc = sbuf + (size_t)6 * B;
   uint32_t* sids = reinterpret_cast<uint32_t*>(sbuf + (size_t)9 * B);
   uint32_t* spos = sids + 2 * B;
@@ -604,9 +645,11 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
   }
   if (end <= begin) return;
   if (threadIdx.x == 0) s_max = begin;
-  sacc[3 * threadIdx.x] = make_float4(0, 0, 0, 0);
-  sacc[3 * threadIdx.x + 1] = make_float4(0, 0, 0, 0);
-  sacc[3 * threadIdx.x + 2] = make_float4(0, 0, 0, 0);
+  if (threadIdx.x < B) {
+    sacc[3 * threadIdx.x] = make_float4(0, 0, 0, 0);
+    sacc[3 * threadIdx.x + 1] = make_float4(0, 0, 0, 0);
+    sacc[3 * threadIdx.x + 2] = make_float4(0, 0, 0, 0);
+  }
   __syncthreads();
   if (tstop > begin) atomicMax(&s_max, tstop);
   __syncthreads();
@@ -780,30 +823,52 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
       const float4 a1 = make_float4(-0.5f * op * m1.x, -op * m1.y, -0.5f * op * m1.z, 0.0f);
       const uint32_t id = sids[(b & 1) * B + threadIdx.x];
       float4* dst = vgrad + (size_t)3 * id;
-      if (a0.x != 0.f || a0.y != 0.f || a0.z != 0.f) atomicAdd(dst, a0);
-      if (a1.x != 0.f || a1.y != 0.f || a1.z != 0.f) atomicAdd(dst + 1, a1);
-      if (a2.x != 0.f || a2.y != 0.f || a2.z != 0.f) atomicAdd(dst + 2, a2);
+      if constexpr (COMP) {
+        float4* cdst = proj_comp + (size_t)3 * v * a.stride + (size_t)3 * id;
+        twosum_atomic_add4(dst, cdst, a0);
+        twosum_atomic_add4(dst + 1, cdst + 1, a1);
+        twosum_atomic_add4(dst + 2, cdst + 2, a2);
+      } else {
+        if (a0.x != 0.f || a0.y != 0.f || a0.z != 0.f) atomicAdd(dst, a0);
+        if (a1.x != 0.f || a1.y != 0.f || a1.z != 0.f) atomicAdd(dst + 1, a1);
+        if (a2.x != 0.f || a2.y != 0.f || a2.z != 0.f) atomicAdd(dst + 2, a2);
+      }
       acc[0] = make_float4(0, 0, 0, 0); acc[1] = acc[0]; acc[2] = acc[0];
     }
-    if (__syncthreads_count(all_done) == (int)B) break;
+    if (__syncthreads_count(all_done) == (int)blockDim.x) break;
   }
   cp_async_wait_all();
   add_work(work, hi0 - begin, w_staged);
+}
+
+template <int PPT, int LIST, int MODE>
+static void backward_launch(const BlendArgs& a, uint32_t grid, uint32_t threads, size_t smem, cudaStream_t st,
+                            const float4* rec, const ListArgs& l, const float4* fwd, const float4* dl_dc,
+                            const float* target, float gscale, double* loss, const uint2* aux, float4* proj_grad,
+                            const uint32_t* d_skip, unsigned long long* w, float4* proj_comp) {
+  if (proj_comp)
+    k_composite_backward<PPT, MODE, LIST, true><<<grid, threads, smem, st>>>(
+        rec, l, a, fwd, dl_dc, target, gscale, loss, aux, proj_grad, d_skip, w, proj_comp);
+  else
+    k_composite_backward<PPT, MODE, LIST, false><<<grid, threads, smem, st>>>(
+        rec, l, a, fwd, dl_dc, target, gscale, loss, aux, proj_grad, d_skip, w, nullptr);
 }
 
 template <int PPT, int LIST>
 static sc_status backward_ppt(sc_ctx* ctx, const BlendArgs& a, uint32_t grid, uint32_t threads, const float4* rec,
                               const ListArgs& l, const float4* fwd, const float4* dl_dc, const float* target,
                               float gscale, double* loss, int mode, const uint2* aux, float4* proj_grad,
-                              const uint32_t* d_skip, uint64_t* work) {
+                              const uint32_t* d_skip, uint64_t* work, float4* proj_comp) {
   const size_t smem = (size_t)9 * threads * sizeof(float4) + (size_t)4 * threads * sizeof(uint32_t);
   unsigned long long* w = reinterpret_cast<unsigned long long*>(work);
+  BlendArgs ab = a;
+  ab.batch = batch_depth(a.batch, threads);
   if (mode == SC_BWD_EXACT)
-    k_composite_backward<PPT, SC_BWD_EXACT, LIST><<<grid, threads, smem, ctx->stream>>>(
-        rec, l, a, fwd, dl_dc, target, gscale, loss, aux, proj_grad, d_skip, w);
+    backward_launch<PPT, LIST, SC_BWD_EXACT>(ab, grid, threads, smem, ctx->stream, rec, l, fwd, dl_dc, target, gscale,
+                                             loss, aux, proj_grad, d_skip, w, proj_comp);
   else
-    k_composite_backward<PPT, SC_BWD_REF, LIST><<<grid, threads, smem, ctx->stream>>>(
-        rec, l, a, fwd, dl_dc, target, gscale, loss, aux, proj_grad, d_skip, w);
+    backward_launch<PPT, LIST, SC_BWD_REF>(ab, grid, threads, smem, ctx->stream, rec, l, fwd, dl_dc, target, gscale,
+                                           loss, aux, proj_grad, d_skip, w, proj_comp);
   return sc_check_launch(ctx, "k_composite_backward");
 }
 
@@ -811,8 +876,9 @@ template <int LIST>
 static sc_status backward_list(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views, const ListArgs& l,
                                const sc_tiling* tl, const float4* fwd, const float4* dl_dc, const float* target,
                                float mse_scale, double* loss, int mode, const uint2* aux, float4* proj_grad,
-                               const uint32_t* d_skip, uint64_t* work) {
-  const BlendArgs a = blend_args(tl, stride);
+                               const uint32_t* d_skip, uint64_t* work, float4* proj_comp, uint32_t batch) {
+  BlendArgs a = blend_args(tl, stride);
+  a.batch = batch;
   const float gscale = (2.0f / ((float)tl->width * (float)tl->height * 3.0f)) * mse_scale;
   const uint32_t pixels = tl->tile_w * tl->tile_h;
   if (pixels > 512 || pixels % 32 != 0) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile must hold 32..512 pixels, multiple of 32");
@@ -823,19 +889,19 @@ static sc_status backward_list(sc_ctx* ctx, const float4* rec, uint32_t stride, 
   if (ppt == 1 && pixels > 256) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile too large for one pixel per thread");
   if (ppt == 2)
     return backward_ppt<2, LIST>(ctx, a, (uint32_t)grid, pixels / 2, rec, l, fwd, dl_dc, target, gscale, loss, mode,
-                                 aux, proj_grad, d_skip, work);
+                                 aux, proj_grad, d_skip, work, proj_comp);
   return backward_ppt<1, LIST>(ctx, a, (uint32_t)grid, pixels, rec, l, fwd, dl_dc, target, gscale, loss, mode, aux,
-                               proj_grad, d_skip, work);
+                               proj_grad, d_skip, work, proj_comp);
 }
 
 sc_status launch_composite_backward(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
                                     const uint32_t* payloads, const uint32_t* ranges, const sc_tiling* tl,
                                     const float4* fwd, const float4* dl_dc, int mode, const uint2* aux,
                                     float4* proj_grad, const uint32_t* d_skip, const float* target,
-                                    float mse_scale, double* loss) {
+                                    float mse_scale, double* loss, float4* proj_comp) {
   ListArgs l{payloads, reinterpret_cast<const uint2*>(ranges), nullptr, 0, 0};
   return backward_list<LIST_PAIRS>(ctx, rec, stride, n_views, l, tl, fwd, dl_dc, target, mse_scale, loss, mode, aux,
-                                   proj_grad, d_skip, nullptr);
+                                   proj_grad, d_skip, nullptr, proj_comp, 0);
 }
 
 sc_status launch_composite_backward_items(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
@@ -843,12 +909,26 @@ sc_status launch_composite_backward_items(sc_ctx* ctx, const float4* rec, uint32
                                           const uint32_t* item_ranges, const sc_tiling* tl, const float4* fwd,
                                           const float4* dl_dc, int mode, const uint2* aux, float4* proj_grad,
                                           const uint32_t* d_skip, const float* target, float mse_scale,
-                                          double* loss, uint64_t* work) {
+                                          double* loss, uint64_t* work, float4* proj_comp, uint32_t batch) {
   const BlendArgs a = blend_args(tl, stride);
   ListArgs l{item_ids, reinterpret_cast<const uint2*>(item_ranges), item_keys, (a.tiles_x + SC_SUPER - 1) / SC_SUPER,
              super_tiles_per_view(tl)};
   return backward_list<LIST_ITEMS>(ctx, rec, stride, n_views, l, tl, fwd, dl_dc, target, mse_scale, loss, mode, aux,
-                                   proj_grad, d_skip, work);
+                                   proj_grad, d_skip, work, proj_comp, batch);
+}
+
+// proj_grad += proj_comp over n float4 (the compensated totals rounded once)
+__global__ void k_fold_comp(float4* __restrict__ g, const float4* __restrict__ c, uint64_t n) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 x = g[i], y = c[i];
+  g[i] = make_float4(x.x + y.x, x.y + y.y, x.z + y.z, x.w + y.w);
+}
+
+sc_status launch_fold_comp(sc_ctx* ctx, float4* proj_grad, const float4* proj_comp, uint64_t n_float4) {
+  if (n_float4 == 0) return SC_OK;
+  k_fold_comp<<<(unsigned)sc_div_up(n_float4, 256), 256, 0, ctx->stream>>>(proj_grad, proj_comp, n_float4);
+  return sc_check_launch(ctx, "k_fold_comp");
 }
 
 // ---------------------------------------------------------------- tonemap (tonemap.wgsl:27-41)

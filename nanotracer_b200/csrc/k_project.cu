@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(128, 8) k_project(DSplats s, const sc_camera* 
                                                  uint32_t stride, float4* __restrict__ rec, TileArgs ta,
                                                  uint32_t* __restrict__ depth_keys, uint32_t* __restrict__ ids,
                                                  uint32_t* __restrict__ counts, int precise,
-                                                 float4* __restrict__ zero_grad) {
+                                                 float4* __restrict__ zero_grad, float4* __restrict__ zero_comp) {
   const uint32_t chunk = blockIdx.x / n_views;
   const uint32_t v = blockIdx.x - chunk * n_views;
   const uint32_t i = chunk * blockDim.x + threadIdx.x;
@@ -263,6 +263,10 @@ __global__ void __launch_bounds__(128, 8) k_project(DSplats s, const sc_camera* 
       const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
       zero_grad[3 * o + 0] = z; zero_grad[3 * o + 1] = z; zero_grad[3 * o + 2] = z;
     }
+    if (zero_comp) {  // and their compensation records (compensated sums)
+      const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+      zero_comp[3 * o + 0] = z; zero_comp[3 * o + 1] = z; zero_comp[3 * o + 2] = z;
+    }
     if (depth_keys) {
       depth_keys[o] = key;
       ids[o] = i;
@@ -273,7 +277,7 @@ __global__ void __launch_bounds__(128, 8) k_project(DSplats s, const sc_camera* 
 
 sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams, uint32_t n_views, uint32_t stride,
                          float4* rec, const sc_tiling* tl, uint32_t* depth_keys, uint32_t* ids, uint32_t* counts,
-                         int precise, int cull, float4* zero_grad) {
+                         int precise, int cull, float4* zero_grad, float4* zero_comp) {
   if (stride == 0 || n_views == 0) return SC_OK;
   TileArgs ta{1, 1, 1, 1, 0, 0};
   if (tl) ta = TileArgs{tl->tile_w, tl->tile_h, (tl->width + tl->tile_w - 1) / tl->tile_w,
@@ -282,7 +286,7 @@ sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams,
   const uint64_t blocks = sc_div_up(stride, bs) * (uint64_t)n_views;
   if (blocks > 0x7FFFFFFFull) return sc_fail(ctx, SC_ERR_INVALID_ARG, "too many splat views for one launch");
   k_project<<<(unsigned)blocks, bs, 0, ctx->stream>>>(s, d_cams, n_views, stride, rec, ta, depth_keys, ids, counts,
-                                                      precise, zero_grad);
+                                                      precise, zero_grad, zero_comp);
   return sc_check_launch(ctx, "k_project");
 }
 
@@ -423,6 +427,10 @@ sc_status launch_project_backward(sc_ctx* ctx, const DSplats& s, const float4* p
 // the same arithmetic as the adjoint's basis) and adds them into this thread's
 // column of a shared-memory block.  Peak register use is that of the larger
 // phase, not of both.
+__device__ __forceinline__ float4 f4add(float4 a, float4 b) {
+  return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+}
+
 constexpr int PB_THREADS = 128;
 constexpr int PB_GROUP = 32;  // views per group: one validity bit each
 
@@ -431,7 +439,8 @@ __global__ void __launch_bounds__(PB_THREADS, 5) k_project_backward_shards(DSpla
                                                                      const sc_camera* __restrict__ cams,
                                                                      uint32_t n_views, float* __restrict__ out,
                                                                      uint32_t n_shards, uint32_t shard,
-                                                                     const uint32_t* __restrict__ skip, int precise) {
+                                                                     const uint32_t* __restrict__ skip, int precise,
+                                                                     const float4* __restrict__ pc) {
   __shared__ float s_rest[45 * PB_THREADS];
   const uint64_t i = (uint64_t)blockIdx.x * PB_THREADS + threadIdx.x;
   if (i >= (uint64_t)n_shards * shard) return;
@@ -453,8 +462,11 @@ __global__ void __launch_bounds__(PB_THREADS, 5) k_project_backward_shards(DSpla
       uint32_t accepted = 0;
       for (uint32_t v = g0; v < g1; ++v) {
         const size_t o = (size_t)v * stride + si;
-        const float4 p2 = pg[3 * o + 2];
-        const float4 p0 = pg[3 * o], p1 = pg[3 * o + 1];
+        float4 p2 = pg[3 * o + 2];
+        float4 p0 = pg[3 * o], p1 = pg[3 * o + 1];
+        if (pc) {  // compensated sums: the total is the sum plus its accumulated rounding errors
+          p0 = f4add(p0, pc[3 * o]); p1 = f4add(p1, pc[3 * o + 1]); p2 = f4add(p2, pc[3 * o + 2]);
+        }
         if (p0.x == 0.f && p0.y == 0.f && p0.z == 0.f && p1.x == 0.f && p1.y == 0.f && p1.z == 0.f && p2.x == 0.f &&
             p2.y == 0.f && p2.z == 0.f)
           continue;  // splat untouched in this view: every gradient term is zero
@@ -473,7 +485,8 @@ __global__ void __launch_bounds__(PB_THREADS, 5) k_project_backward_shards(DSpla
       while (accepted) {
         const uint32_t v = g0 + (uint32_t)(__ffs(accepted) - 1);
         accepted &= accepted - 1u;
-        const float4 p2 = pg[3 * ((size_t)v * stride + si) + 2];
+        float4 p2 = pg[3 * ((size_t)v * stride + si) + 2];
+        if (pc) p2 = f4add(p2, pc[3 * ((size_t)v * stride + si) + 2]);
         const float4 e = __ldg(reinterpret_cast<const float4*>(cams + v) + 4);  // camera position
         // the view direction and basis exactly as splat_backward_view<true> forms them
         const float dx = e.x - px, dy = e.y - py, dz = e.z - pz;
@@ -499,11 +512,12 @@ __global__ void __launch_bounds__(PB_THREADS, 5) k_project_backward_shards(DSpla
 
 sc_status launch_project_backward_shards(sc_ctx* ctx, const DSplats& s, const float4* pg, uint32_t stride,
                                          const sc_camera* d_cams, uint32_t n_views, float* grads, uint32_t n_shards,
-                                         uint32_t shard, const uint32_t* d_skip, int precise_det) {
+                                         uint32_t shard, const uint32_t* d_skip, int precise_det,
+                                         const float4* pc) {
   const uint64_t total = (uint64_t)n_shards * shard;
   if (total == 0) return SC_OK;
   k_project_backward_shards<<<(unsigned)sc_div_up(total, PB_THREADS), PB_THREADS, 0, ctx->stream>>>(
-      s, pg, stride, d_cams, n_views, grads, n_shards, shard, d_skip, precise_det);
+      s, pg, stride, d_cams, n_views, grads, n_shards, shard, d_skip, precise_det, pc);
   return sc_check_launch(ctx, "k_project_backward_shards");
 }
 

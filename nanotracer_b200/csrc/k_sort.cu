@@ -675,15 +675,19 @@ static sc_status radix_passes(sc_ctx* ctx, K* keys, uint32_t* vals, K* keys_tmp,
 // are taken only when they save a third of the passes — in practice a 9-bit
 // key, one pass instead of an 8-bit and a 1-bit pass (2.8e7 items: 0.44 ms
 // instead of 0.57 ms, with the histogram).
+// digit_bits 8 or 9 forces the digit width (the autotuner's radix-width axis).
 template <typename K>
 sc_status radix_sort(sc_ctx* ctx, K* keys, uint32_t* vals, K* keys_tmp, uint32_t* vals_tmp, uint64_t n_cap,
-                     uint32_t key_bits, const uint64_t* d_n, void* scratch, size_t bytes, bool* result_in_tmp) {
+                     uint32_t key_bits, const uint64_t* d_n, void* scratch, size_t bytes, bool* result_in_tmp,
+                     int digit_bits) {
   *result_in_tmp = false;
   if (n_cap == 0) return SC_OK;
   if (n_cap > RS_VAL_MASK) return sc_fail(ctx, SC_ERR_CAPACITY, "radix sort limited to 2^30 - 1 elements");
   if (key_bits > sizeof(K) * 8) return sc_fail(ctx, SC_ERR_INVALID_ARG, "key_bits larger than the key type");
+  if (digit_bits != 0 && digit_bits != 8 && digit_bits != 9)
+    return sc_fail(ctx, SC_ERR_INVALID_ARG, "radix digits are 8 or 9 bits (0 = chosen by pass count)");
   if (key_bits == 0) return SC_OK;
-  if (3 * ((key_bits + 8) / 9) < 2 * ((key_bits + 7) / 8))
+  if (digit_bits == 9 || (digit_bits == 0 && 3 * ((key_bits + 8) / 9) < 2 * ((key_bits + 7) / 8)))
     return radix_passes<K, 9>(ctx, keys, vals, keys_tmp, vals_tmp, n_cap, key_bits, d_n, scratch, bytes,
                               result_in_tmp);
   return radix_passes<K, 8>(ctx, keys, vals, keys_tmp, vals_tmp, n_cap, key_bits, d_n, scratch, bytes,
@@ -837,7 +841,7 @@ sc_status radix_sort_segments(sc_ctx* ctx, uint32_t* keys, uint32_t* vals, uint3
 }
 
 template sc_status radix_sort<uint32_t>(sc_ctx*, uint32_t*, uint32_t*, uint32_t*, uint32_t*, uint64_t, uint32_t,
-                                        const uint64_t*, void*, size_t, bool*);
+                                        const uint64_t*, void*, size_t, bool*, int);
 
 // Failure-detection self-test: one onesweep pass over two tiles whose ticket
 // counter starts at 1, so the first tile to run looks back on tile 0, which no
@@ -871,6 +875,6 @@ sc_status selftest_lookback_timeout(sc_ctx* ctx) {
   return sc_check_device_error(ctx);
 }
 template sc_status radix_sort<uint64_t>(sc_ctx*, uint64_t*, uint32_t*, uint64_t*, uint32_t*, uint64_t, uint32_t,
-                                        const uint64_t*, void*, size_t, bool*);
+                                        const uint64_t*, void*, size_t, bool*, int);
 
 }  // namespace sck

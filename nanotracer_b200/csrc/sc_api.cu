@@ -186,6 +186,13 @@ sc_status sc_buffer_readback(sc_ctx* ctx, void* dst, const void* src, size_t byt
   return sc_check_device_error(ctx);
 }
 
+sc_status sc_buffer_copy(sc_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  if (!ctx || (bytes && (!dst || !src))) return SC_ERR_INVALID_ARG;
+  if (!bytes) return SC_OK;
+  SC_CUDA_TRY(ctx, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+  return SC_OK;
+}
+
 sc_status sc_buffer_zero(sc_ctx* ctx, void* dptr, size_t bytes) {
   if (!ctx || (bytes && !dptr)) return SC_ERR_INVALID_ARG;
   if (!bytes) return SC_OK;
@@ -775,6 +782,33 @@ sc_status sc_composite_backward(sc_ctx* ctx, const sc_projected_splat* projected
                                         b->ranges, tl, reinterpret_cast<const float4*>(fwd),
                                         reinterpret_cast<const float4*>(dl_dc), (int)mode,
                                         reinterpret_cast<const uint2*>(aux), reinterpret_cast<float4*>(pg), nullptr);
+}
+
+sc_status sc_composite_backward_ex(sc_ctx* ctx, const sc_projected_splat* projected, uint32_t stride,
+                                   uint32_t n_views, const sc_bins* b, const sc_tiling* tl, const float* fwd,
+                                   const float* dl_dc, sc_bwd_mode mode, const uint32_t* aux, sc_projected_grad* pg,
+                                   uint32_t flags) {
+  if (!(flags & SC_BWD_FLAG_COMPENSATED))
+    return sc_composite_backward(ctx, projected, stride, n_views, b, tl, fwd, dl_dc, mode, aux, pg);
+  if (flags & ~SC_BWD_FLAG_COMPENSATED) return sc_fail(ctx, SC_ERR_INVALID_ARG, "unknown backward flag");
+  if (!ctx || !b || !tiling_ok(tl) || !fwd || !dl_dc || !pg) return SC_ERR_INVALID_ARG;
+  if (mode != SC_BWD_REF && mode != SC_BWD_EXACT) return SC_ERR_INVALID_ARG;
+  if (b->total > 0 && (!b->vals || !projected)) return SC_ERR_INVALID_ARG;
+  const uint64_t n4 = (uint64_t)n_views * stride * 3;  // float4 records of the gradient buffer
+  void* comp = nullptr;
+  SC_CUDA_TRY(ctx, cudaMallocAsync(&comp, std::max<uint64_t>(n4, 1) * 16, ctx->stream), "compensation records");
+  sc_status st = SC_OK;
+  if (cudaMemsetAsync(comp, 0, n4 * 16, ctx->stream) != cudaSuccess) st = sc_fail(ctx, SC_ERR_CUDA, "zero");
+  if (st == SC_OK)
+    st = sck::launch_composite_backward(ctx, reinterpret_cast<const float4*>(projected), stride, n_views, b->vals,
+                                        b->ranges, tl, reinterpret_cast<const float4*>(fwd),
+                                        reinterpret_cast<const float4*>(dl_dc), (int)mode,
+                                        reinterpret_cast<const uint2*>(aux), reinterpret_cast<float4*>(pg), nullptr,
+                                        nullptr, 0.0f, nullptr, reinterpret_cast<float4*>(comp));
+  if (st == SC_OK)
+    st = sck::launch_fold_comp(ctx, reinterpret_cast<float4*>(pg), reinterpret_cast<const float4*>(comp), n4);
+  cudaFreeAsync(comp, ctx->stream);
+  return st;
 }
 
 sc_status sc_project_backward(sc_ctx* ctx, const sc_splats* s, const sc_projected_grad* pg, const sc_camera* cam,

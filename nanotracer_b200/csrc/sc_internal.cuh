@@ -259,7 +259,7 @@ namespace sck {
 sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams, uint32_t n_views,
                          uint32_t stride, float4* rec, const sc_tiling* tiling, uint32_t* depth_keys,
                          uint32_t* splat_ids, uint32_t* counts, int precise_det, int cull,
-                         float4* zero_grad = nullptr);
+                         float4* zero_grad = nullptr, float4* zero_comp = nullptr);
 
 sc_status launch_project_backward(sc_ctx* ctx, const DSplats& s, const float4* proj_grad, const sc_camera* d_cam,
                                   float* grads, uint32_t gcap, int accumulate, int precise_det);
@@ -364,7 +364,8 @@ __device__ __forceinline__ void constrain_geometry(float np[14], const AdamParam
 // of splats in [n, n_shards*shard) are zero.
 sc_status launch_project_backward_shards(sc_ctx* ctx, const DSplats& s, const float4* proj_grad, uint32_t stride,
                                          const sc_camera* d_cams, uint32_t n_views, float* grads, uint32_t n_shards,
-                                         uint32_t shard, const uint32_t* d_skip_flag, int precise_det);
+                                         uint32_t shard, const uint32_t* d_skip_flag, int precise_det,
+                                         const float4* proj_comp = nullptr);
 // Adam + constraints + densify statistic for splats [lo, lo+count) from one
 // reduce-scattered chunk g[r * shard + j]
 // Adam + constraints + densify statistic over splats [lo, lo+count) from
@@ -391,7 +392,8 @@ sc_status scan_u32_gather(sc_ctx* ctx, uint32_t* out, uint64_t n, const uint32_t
 size_t scan_scratch_bytes(uint64_t n);
 template <typename K>
 sc_status radix_sort(sc_ctx* ctx, K* keys, uint32_t* vals, K* keys_tmp, uint32_t* vals_tmp, uint64_t n,
-                     uint32_t key_bits, const uint64_t* d_n, void* scratch, size_t scratch_bytes, bool* result_in_tmp);
+                     uint32_t key_bits, const uint64_t* d_n, void* scratch, size_t scratch_bytes, bool* result_in_tmp,
+                     int digit_bits = 0);
 size_t radix_scratch_bytes(uint64_t n, uint32_t key_bytes);
 // n_segs independent stable sorts of u32 keys, segment g = elements
 // [g seg_len, (g + 1) seg_len); seg_len a multiple of RADIX_SEG_TILE
@@ -443,24 +445,31 @@ sc_status launch_composite_backward(sc_ctx* ctx, const float4* rec, uint32_t str
                                     const uint32_t* payloads, const uint32_t* ranges, const sc_tiling* tl,
                                     const float4* fwd, const float4* dl_dc, int mode, const uint2* aux,
                                     float4* proj_grad, const uint32_t* d_skip, const float* target = nullptr,
-                                    float mse_scale = 0.0f, double* loss = nullptr);
+                                    float mse_scale = 0.0f, double* loss = nullptr, float4* proj_comp = nullptr);
+// proj_comp (nullable, same layout as proj_grad, zeroed by the caller): the
+// per-(view, splat) totals across tiles are then TwoSum-compensated atomic sums,
+// their rounding errors accumulated in proj_comp (the total is grad + comp)
+sc_status launch_fold_comp(sc_ctx* ctx, float4* proj_grad, const float4* proj_comp, uint64_t n_float4);
 // the same two passes over super-tile item lists (launch_super_emit's items
 // sorted by super tile, item_ranges per (view, super tile)): each tile blends
 // the items whose member mask holds it, in list order; aux then holds
-// positions within the super tile's list.  work (nullable, BLEND_WORK_SLOTS
+// positions within the super tile's list.  batch: list positions staged per
+// batch (0 = one per thread).  work (nullable, BLEND_WORK_SLOTS
 // (scanned, staged) pairs, accumulated): the list positions the CTAs' batches
 // covered and the entries they staged.
 constexpr uint32_t BLEND_WORK_SLOTS = 64;
 sc_status launch_composite_items(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
                                  const uint32_t* item_keys, const uint32_t* item_ids, const uint32_t* item_ranges,
                                  const sc_tiling* tl, float4* image, uint2* aux, const float* target, float mse_scale,
-                                 float4* dl_dc, double* loss, const uint32_t* d_skip, uint64_t* work = nullptr);
+                                 float4* dl_dc, double* loss, const uint32_t* d_skip, uint64_t* work = nullptr,
+                                 uint32_t batch = 0);
 sc_status launch_composite_backward_items(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
                                           const uint32_t* item_keys, const uint32_t* item_ids,
                                           const uint32_t* item_ranges, const sc_tiling* tl, const float4* fwd,
                                           const float4* dl_dc, int mode, const uint2* aux, float4* proj_grad,
                                           const uint32_t* d_skip, const float* target = nullptr,
-                                          float mse_scale = 0.0f, double* loss = nullptr, uint64_t* work = nullptr);
+                                          float mse_scale = 0.0f, double* loss = nullptr, uint64_t* work = nullptr,
+                                          float4* proj_comp = nullptr, uint32_t batch = 0);
 sc_status launch_tonemap(sc_ctx* ctx, const float4* img, uint32_t w, uint32_t h, uint8_t* out);
 
 // SSIM (loss.rs:22-375): scale * dL_ssim/dC added into dl_dc, per-view sum of

@@ -89,6 +89,7 @@ struct sc_trainer {
   StepOut* d_out = nullptr;
   // per (view, splat)
   float4* rec = nullptr; float4* pgrad = nullptr;
+  float4* pcomp = nullptr;  // compensation records of pgrad (cfg.compensated_sums)
   float* grads = nullptr;  // [SC_NROWS][grad_stride] per-splat gradient rows (one GPU)
   uint32_t grad_stride = 0;
   uint32_t* dkeys = nullptr; uint32_t* dkeys_tmp = nullptr;  // per view, a segment of stride depth keys
@@ -148,7 +149,9 @@ struct sc_trainer {
 };
 
 static void trainer_free_splat_arrays(sc_trainer* tr) {
-  cudaFree(tr->rec); cudaFree(tr->pgrad); cudaFree(tr->grads); cudaFree(tr->dkeys); cudaFree(tr->dkeys_tmp);
+  cudaFree(tr->rec); cudaFree(tr->pgrad); cudaFree(tr->pcomp); cudaFree(tr->grads); cudaFree(tr->dkeys);
+  cudaFree(tr->dkeys_tmp);
+  tr->pcomp = nullptr;
   cudaFree(tr->ids); cudaFree(tr->ids_tmp); cudaFree(tr->counts_by_id); cudaFree(tr->counts);
   tr->rec = tr->pgrad = nullptr; tr->dkeys = tr->dkeys_tmp = nullptr;
   tr->ids = tr->ids_tmp = tr->counts_by_id = tr->counts = nullptr;
@@ -201,6 +204,7 @@ static sc_status ensure_splat_arrays(sc_trainer* tr, uint32_t cap) {
   const size_t nv = (size_t)tr->V * cap;
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->rec, nv * 48), "rec");
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->pgrad, nv * 48), "pgrad");
+  if (tr->cfg.compensated_sums) SC_CUDA_TRY(ctx, cudaMalloc(&tr->pcomp, nv * 48), "pcomp");
   tr->grad_stride = (cap + 63u) & ~63u;
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->grads, (size_t)SC_NROWS * tr->grad_stride * 4), "grads");
   SC_CUDA_TRY(ctx, cudaMalloc(&tr->dkeys, nv * 4), "dkeys");
@@ -300,7 +304,7 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   mark(tr, 0, capturing);
   SC_TRY(sck::launch_project(ctx, ds, d_cams, V, tr->stride, tr->rec, &tr->cfg.tiling, tr->dkeys, tr->ids,
                              tr->counts_by_id, tr->cfg.fp64_det ? 1 : 0,
-                             (tr->cfg.tile_cull ? 1 : 0) | (tr->two_level ? 2 : 0), tr->pgrad));
+                             (tr->cfg.tile_cull ? 1 : 0) | (tr->two_level ? 2 : 0), tr->pgrad, tr->pcomp));
   mark(tr, 1, capturing);
   bool in_tmp = false;
   SC_TRY(sck::radix_sort_segments(ctx, tr->dkeys, tr->ids, tr->dkeys_tmp, tr->ids_tmp, tr->stride, V, 32, tr->scratch,
@@ -331,7 +335,7 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
                                   &tr->cfg.tiling, tr->ikeys, tr->ivals, tr->icap, ctx->d_error, cull));
     mark(tr, 4, capturing);
     SC_TRY(sck::radix_sort<uint32_t>(ctx, tr->ikeys, tr->ivals, tr->ikeys_tmp, tr->ivals_tmp, tr->icap, tr->super_bits,
-                                     d_items, tr->scratch, tr->scratch_bytes, &in_tmp));
+                                     d_items, tr->scratch, tr->scratch_bytes, &in_tmp, (int)tr->cfg.sort_digit_bits));
     item_keys = in_tmp ? tr->ikeys_tmp : tr->ikeys;
     item_ids = in_tmp ? tr->ivals_tmp : tr->ivals;
     mark(tr, 5, capturing);
@@ -357,7 +361,7 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   // groups the pairs by tile, then view (the emission is view-major), then depth
   const uint32_t tile_bits = bits_for(tr->T);
   SC_TRY(sck::radix_sort<uint32_t>(ctx, tr->keys, tr->vals, tr->keys_tmp, tr->vals_tmp, tr->kcap, tile_bits,
-                                   tr->d_total, tr->scratch, tr->scratch_bytes, &in_tmp));
+                                   tr->d_total, tr->scratch, tr->scratch_bytes, &in_tmp, (int)tr->cfg.sort_digit_bits));
   const uint32_t* skeys = in_tmp ? tr->keys_tmp : tr->keys;
   svals = in_tmp ? tr->vals_tmp : tr->vals;
   mark(tr, 5, capturing);
@@ -376,7 +380,7 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   if (tr->two_level)
     SC_TRY(sck::launch_composite_items(ctx, tr->rec, tr->stride, V, item_keys, item_ids, tr->iranges, &tr->cfg.tiling,
                                        tr->image, tr->aux, fwd_target, mse_w, tr->dl_dc, tr->d_loss, ctx->d_error,
-                                       work_fwd));
+                                       work_fwd, tr->cfg.blend_batch));
   else
     SC_TRY(sck::launch_composite(ctx, tr->rec, tr->stride, V, svals, tr->ranges, &tr->cfg.tiling, tr->image, tr->aux,
                                  fwd_target, mse_w, tr->dl_dc, tr->d_loss, ctx->d_error));
@@ -409,12 +413,14 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
                                                   tr->iranges + (size_t)2 * v0 * tr->ST, &tr->cfg.tiling,
                                                   tr->image + po, tr->dl_dc ? tr->dl_dc + po : nullptr,
                                                   (int)tr->cfg.bwd_mode, tr->aux + po,
-                                                  tr->pgrad + so, ctx->d_error, tg, mse_w, tr->d_loss + v0, work_bwd));
+                                                  tr->pgrad + so, ctx->d_error, tg, mse_w, tr->d_loss + v0, work_bwd,
+                                                  tr->pcomp ? tr->pcomp + so : nullptr, tr->cfg.blend_batch));
     else
       st = (sck::launch_composite_backward(ctx, tr->rec + so, tr->stride, nv, svals, tr->ranges + (size_t)2 * v0 * tr->T,
                                             &tr->cfg.tiling, tr->image + po, tr->dl_dc ? tr->dl_dc + po : nullptr,
                                             (int)tr->cfg.bwd_mode,
-                                            tr->aux + po, tr->pgrad + so, ctx->d_error, tg, mse_w, tr->d_loss + v0));
+                                            tr->aux + po, tr->pgrad + so, ctx->d_error, tg, mse_w, tr->d_loss + v0,
+                                            tr->pcomp ? tr->pcomp + so : nullptr));
     ctx->stream = main_stream;
     SC_TRY(st);
     if (per_view) SC_CUDA_TRY(ctx, cudaEventRecord(tr->ev_bwd[v0], tr->bwd_stream[v0]), "view done");
@@ -430,11 +436,11 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   ap.opacity_logit_max = tr->cfg.opacity_logit_max;
   if (tr->grads_mode)
     SC_TRY(sck::launch_project_backward_shards(ctx, ds, tr->pgrad, tr->stride, d_cams, V, tr->gout, tr->g_shards,
-                                               tr->g_shard, ctx->d_error, tr->cfg.fp64_det ? 1 : 0));
+                                               tr->g_shard, ctx->d_error, tr->cfg.fp64_det ? 1 : 0, tr->pcomp));
   else {
     // per-splat gradient rows summed over the views, then Adam streamed over the rows
     SC_TRY(sck::launch_project_backward_shards(ctx, ds, tr->pgrad, tr->stride, d_cams, V, tr->grads, 1,
-                                               tr->grad_stride, ctx->d_error, tr->cfg.fp64_det ? 1 : 0));
+                                               tr->grad_stride, ctx->d_error, tr->cfg.fp64_det ? 1 : 0, tr->pcomp));
     SC_TRY(sck::launch_adam_rows(ctx, ds, dm, acc, tr->grads, 0, ds.n, tr->grad_stride, ap, d_bc, ctx->d_error));
   }
   mark(tr, 9, capturing);
@@ -476,6 +482,14 @@ sc_status sc_trainer_create(sc_ctx* ctx, const sc_train_config* cfg, sc_trainer*
   if (cfg->sort_mode > 2) {
     delete tr;
     return sc_fail(ctx, SC_ERR_INVALID_ARG, "sort_mode must be 0, 1 or 2");
+  }
+  if (cfg->sort_digit_bits != 0 && cfg->sort_digit_bits != 8 && cfg->sort_digit_bits != 9) {
+    delete tr;
+    return sc_fail(ctx, SC_ERR_INVALID_ARG, "sort_digit_bits must be 0, 8 or 9");
+  }
+  if (cfg->blend_batch != 0 && (cfg->blend_batch % 32 || cfg->blend_batch < 32)) {
+    delete tr;
+    return sc_fail(ctx, SC_ERR_INVALID_ARG, "blend_batch must be 0 or a multiple of 32");
   }
   tr->ST = sck::super_tiles_per_view(&t);
   tr->super_bits = bits_for(tr->ST);

@@ -40,6 +40,12 @@ class DeviceBuffer:
               self.ctx.handle)
         return out
 
+    def copy_from(self, src: "DeviceBuffer", nbytes: int, dst_offset: int = 0, src_offset: int = 0) -> None:
+        """Device-to-device copy on the context's stream (asynchronous)."""
+        assert dst_offset + nbytes <= self.nbytes and src_offset + nbytes <= src.nbytes
+        check(lib().sc_buffer_copy(self.ctx.handle, C.c_void_p(self.ptr + dst_offset), C.c_void_p(src.ptr + src_offset),
+                                   nbytes), self.ctx.handle)
+
     def zero(self) -> None:
         check(lib().sc_buffer_zero(self.ctx.handle, self.cptr, self.nbytes), self.ctx.handle)
 

@@ -99,11 +99,15 @@ class Rasterizer:
 
     def composite_backward(self, projected: DeviceBuffer, bins: TileBinningResult, forward_out: DeviceBuffer,
                            dl_dc: DeviceBuffer, projected_grad: DeviceBuffer, params: TilingParams, stride: int,
-                           n_views: int = 1, mode: int = SC_BWD_REF, aux: DeviceBuffer | None = None) -> None:
+                           n_views: int = 1, mode: int = SC_BWD_REF, aux: DeviceBuffer | None = None,
+                           compensated: bool = False) -> None:
+        """compensated: TwoSum-compensated per-(view, splat) totals across tiles
+        (sc_composite_backward_ex with SC_BWD_FLAG_COMPENSATED)."""
         t = tiling_struct(params)
-        check(lib().sc_composite_backward(self.ctx.handle, projected.cptr, stride, n_views, bins.handle, C.byref(t),
-                                          forward_out.cptr, dl_dc.cptr, int(mode),
-                                          aux.cptr if aux is not None else None, projected_grad.cptr), self.ctx.handle)
+        check(lib().sc_composite_backward_ex(self.ctx.handle, projected.cptr, stride, n_views, bins.handle,
+                                             C.byref(t), forward_out.cptr, dl_dc.cptr, int(mode),
+                                             aux.cptr if aux is not None else None, projected_grad.cptr,
+                                             1 if compensated else 0), self.ctx.handle)
 
     def project_backward(self, splats: GpuSplatBuffer, projected_grad: DeviceBuffer, camera: CameraUniform,
                          grads: GradSplatBuffers, accumulate: bool = False, view_offset: int = 0) -> None:

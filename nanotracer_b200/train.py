@@ -51,6 +51,9 @@ class TrainConfig:
     ssim_lambda: float = 0.0
     sort_mode: int = 0  # 0 auto (two-level binning), 1 sort of the (tile, splat) pairs, 2 two-level
     fp64_det: bool = False  # FP64 determinant / inverse of near-degenerate splats (projection and adjoint)
+    compensated_sums: bool = False  # TwoSum-compensated per-(view, splat) gradient totals across tiles
+    blend_batch: int = 0  # list positions staged per blend batch (multiple of 32); 0 = one per thread
+    sort_digit_bits: int = 0  # radix digit width of the binning sort: 8, 9, or 0 = fewer passes wins
 
     def struct(self) -> sc_train_config:
         c = sc_train_config()
@@ -66,6 +69,9 @@ class TrainConfig:
         c.ssim_lambda = self.ssim_lambda
         c.sort_mode = self.sort_mode
         c.fp64_det = 1 if self.fp64_det else 0
+        c.compensated_sums = 1 if self.compensated_sums else 0
+        c.blend_batch = self.blend_batch
+        c.sort_digit_bits = self.sort_digit_bits
         return c
 
 

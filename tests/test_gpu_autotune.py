@@ -1,6 +1,8 @@
-"""The autotuner on the device: every candidate (tile shape x binning path)
-runs and is timed, the returned configuration is the fastest one, and a
-trainer built from it steps the scene."""
+"""The autotuner on the device: every candidate of its coordinate search
+(tile shape x binning path, blend batch depth, sort digit width) runs and is
+timed, the candidates' first-step images are bit-identical (the axes change
+speed, not results), the returned configuration is each stage's fastest, and
+a trainer built from it steps the scene."""
 import math
 
 import numpy as np
@@ -23,10 +25,16 @@ def test_autotune_times_every_candidate_and_returns_the_fastest(ctx):
                                                                np.float32))
     base = TrainConfig(n_views=V, width=W, height=H, depth_max=8.0, exact_backward=True, use_graph=True)
     best, trials = autotune(ctx, scene, cams, tbuf, base, warmup=1, steps=2)
-    assert len(trials) == len(TILE_SHAPES) * len(SORT_MODES)
-    assert all(t.error is None and t.ms > 0 for t in trials)
-    fastest = min(trials, key=lambda t: t.ms)
-    assert (best.tile_w, best.tile_h, best.sort_mode) == (fastest.tile_w, fastest.tile_h, fastest.sort_mode)
+    assert len(trials) >= len(TILE_SHAPES) * len(SORT_MODES) + 2
+    assert all(t.error is None and t.ms > 0 for t in trials), [t.label for t in trials if t.error]
+    assert len({t.digest for t in trials}) == 1, [(t.label, t.digest[:8]) for t in trials]
+    stage1 = trials[:len(TILE_SHAPES) * len(SORT_MODES)]
+    f1 = min(stage1, key=lambda t: t.ms)
+    assert (best.tile_w, best.tile_h, best.sort_mode) == (f1.tile_w, f1.tile_h, f1.sort_mode)
+    chosen = [t for t in trials if (t.tile_w, t.tile_h, t.sort_mode, t.blend_batch, t.sort_digit_bits) ==
+              (best.tile_w, best.tile_h, best.sort_mode, best.blend_batch, best.sort_digit_bits)]
+    assert chosen
+    print({t.label: round(t.ms, 3) for t in trials})
     # the chosen configuration trains the caller's own copy of the scene
     g = GpuSplatBuffer.upload(ctx, scene)
     mo = AdamMomentBuffers(ctx, g.capacity)
@@ -35,3 +43,29 @@ def test_autotune_times_every_candidate_and_returns_the_fastest(ctx):
     tr.set_targets(tbuf)
     losses = [tr.step(g, mo, acc, cams, t) for t in (1, 2)]
     assert all(math.isfinite(x) and x > 0 for x in losses)
+
+
+@pytest.mark.parametrize("batch", [32, 64])
+@pytest.mark.parametrize("digits", [8, 9])
+def test_blend_batch_and_digit_width_leave_the_step_unchanged(ctx, batch, digits):
+    """A non-default blend batch depth and sort digit width give the default
+    configuration's images bit for bit, and its parameters within the float
+    atomics' ordering noise."""
+    n, W, H, V = 6000, 256, 192, 2
+    scene = random_scene(n, 44)
+    tl = TilingParams(W, H, 16, 8.0)
+    cams = [CameraUniform.from_pose(*p, FOV_Y, W, H, n) for p in orbit_views(V, 0)]
+    tgt = render_targets(ctx, perturbed(scene), cams, tl)
+    out = []
+    for cfg in (TrainConfig(n_views=V, width=W, height=H, depth_max=8.0),
+                TrainConfig(n_views=V, width=W, height=H, depth_max=8.0, blend_batch=batch, sort_digit_bits=digits)):
+        g = GpuSplatBuffer.upload(ctx, scene)
+        mo = AdamMomentBuffers(ctx, g.capacity)
+        acc = ctx.storage_buffer_zeroed("acc", 4 * g.capacity)
+        tr = Trainer(ctx, cfg)
+        tr.set_targets(ctx.storage_buffer("t", np.ascontiguousarray(tgt, np.float32)))
+        ls = [tr.step(g, mo, acc, cams, t) for t in (1, 2)]
+        out.append((tr.images(), ls, g.readback().flat()))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.allclose(out[0][1], out[1][1], rtol=1e-6)
+    assert np.allclose(out[0][2], out[1][2], rtol=1e-5, atol=1e-6)

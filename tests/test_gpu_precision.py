@@ -141,3 +141,86 @@ def test_trainer_fp64_det_renders_what_the_fp64_projection_renders(ctx):
     assert np.isfinite(loss)
     assert np.array_equal(tr.images(), ref_img)
     assert np.all(np.isfinite(g.readback().flat()))
+
+
+def _scene_with_backdrop(n, n_big, seed):
+    """config-1-like splats plus n_big large splats behind them whose
+    footprints cover most of a 1080p view: their gradient totals add one term
+    per tile over thousands of tiles."""
+    from nanotracer_b200.scene import random_scene
+    base = random_scene(n, seed).flat()
+    rng = np.random.default_rng(seed + 1)
+    big = base[:n_big].copy()
+    big[:, 0:3] = rng.uniform(-0.3, 0.3, (n_big, 3))
+    big[:, 7:10] = np.log(0.6) + rng.normal(0.0, 0.1, (n_big, 3))
+    big[:, 10] = -2.0  # low opacity: the pixels behind stay unsaturated
+    return SplatBuffer.from_flat(np.concatenate([base, big]).astype(np.float32))
+
+
+def test_compensated_cross_tile_sums_against_the_fp64_oracle(ctx, oracle):
+    """sc_composite_backward_ex(SC_BWD_FLAG_COMPENSATED) against the plain
+    float atomics, both against the oracle's FP64 backward of the same records,
+    bins, image and dL/dC: for splats whose totals add thousands of tile terms
+    the compensated totals are closer to FP64, and everywhere they stay within
+    the parity bound."""
+    from nanotracer_b200._lib import SC_BWD_EXACT, SC_KEYS_NATIVE64
+    from tests.util import check_pg_explained, margins
+    W, H, n, n_big = 1920, 1080, 20000, 16
+    s = _scene_with_backdrop(n, n_big, 17)
+    cam = CameraUniform.from_pose(*orbit_pose(10.0), FOV_Y, W, H, n + n_big)
+    tl = TilingParams(W, H, 16, 8.0)
+    pipe = GpuPipe(ctx, s, cam, tl, key_mode=SC_KEYS_NATIVE64)
+    rec = pipe.project()[0]
+    _, pay, ranges = pipe.bin()
+    img, aux = pipe.composite()
+    rng = np.random.default_rng(4)
+    dl = (rng.normal(size=(W * H, 4)) * 1e-6).astype(np.float32)
+    dl[:, 3] = 0.0
+    plain = pipe.backward(dl, SC_BWD_EXACT)[0].astype(np.float64)
+    comp = pipe.backward(dl, SC_BWD_EXACT, compensated=True)[0].astype(np.float64)
+    otl = oracle.tiling(W, H, 16, 16, 8.0)
+    nc, tf = aux[0, ..., 1].reshape(-1), aux[0, ..., 0].view(np.float32).reshape(-1)
+    ref = oracle.composite_backward(rec.astype(np.float64), pay, ranges.reshape(-1), otl,
+                                    img[0].reshape(-1, 4).astype(np.float64), dl.astype(np.float64), SC_BWD_EXACT,
+                                    nc, tf.astype(np.float64), "f64")
+    _, absum = oracle.composite_backward(rec, pay, ranges.reshape(-1), otl, img[0].reshape(-1, 4), dl, SC_BWD_EXACT,
+                                         nc, tf, want_abs=True)
+    _, flags, _ = margins(oracle, rec, pay, ranges, otl, 1)
+    cols = [0, 1, 2, 4, 5, 6, 8, 9, 10]
+    big = np.arange(n, n + n_big)
+    tiles = np.array([((rec[i, 3] * 2 / 16 + 1) ** 2) for i in big])
+    rel = lambda g: np.abs(g[big][:, cols] - ref[big][:, cols]).max(1) / np.abs(ref[big][:, cols]).max(1)
+    e_plain, e_comp = rel(plain), rel(comp)
+    print({"tiles_per_big_splat_min": float(tiles.min()), "plain_rel_median": float(np.median(e_plain)),
+           "comp_rel_median": float(np.median(e_comp)), "plain_rel_max": float(e_plain.max()),
+           "comp_rel_max": float(e_comp.max())})
+    assert tiles.min() > 1000
+    assert np.median(e_comp) <= np.median(e_plain)
+    assert e_comp.max() <= 1e-4
+    check_pg_explained(comp.astype(np.float32), ref, absum, flags, label="compensated")
+    check_pg_explained(plain.astype(np.float32), ref, absum, flags, label="plain")
+
+
+def test_trainer_compensated_sums_step(ctx):
+    """TrainConfig.compensated_sums: the same images and, within float
+    rounding of the sums, the same step as the plain atomics."""
+    from nanotracer_b200.scene import orbit_views, perturbed, random_scene
+    from nanotracer_b200.train import render_targets
+    n, W, H, V = 20000, 256, 192, 2
+    s = random_scene(n, 12)
+    tl = TilingParams(W, H, 16, 8.0)
+    cams = [CameraUniform.from_pose(*p, FOV_Y, W, H, n) for p in orbit_views(V, 0)]
+    tgt = render_targets(ctx, perturbed(s), cams, tl)
+    out = []
+    for comp in (False, True):
+        g = GpuSplatBuffer.upload(ctx, s)
+        mo = AdamMomentBuffers(ctx, g.capacity)
+        acc = ctx.storage_buffer_zeroed("acc", 4 * g.capacity)
+        tr = Trainer(ctx, TrainConfig(n_views=V, width=W, height=H, depth_max=8.0, compensated_sums=comp))
+        tr.set_targets(ctx.storage_buffer("targets", np.ascontiguousarray(tgt, np.float32)))
+        losses = [tr.step(g, mo, acc, cams, t) for t in (1, 2)]
+        out.append((tr.images(), losses, g.readback().flat()))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.allclose(out[0][1], out[1][1], rtol=1e-6)
+    d = np.abs(out[0][2] - out[1][2])
+    assert np.mean(d <= 1e-6 + 1e-6 * np.abs(out[0][2])) > 0.999

@@ -372,3 +372,15 @@ def test_combined_gradient_is_lambda_weighted_sum(oracle):
     _, _, _, g = oracle.combined(_rgba(p), t, 8, 8, float(lam))
     want = gm * (np.float32(1) - lam) + gs * lam
     assert np.max(np.linalg.norm((g - want).reshape(-1, 4), axis=1)) < 1e-6
+
+
+def test_fp64_adjoint_matches_central_differences_on_64_random_parameters(oracle):
+    """BASELINE config 5's adjoint check on the oracle's FP64 instantiation:
+    central differences (h = 1e-3, FP64 loss) on 64 random parameters of a
+    1000-splat 64x64 scene, rotations included (tests/fd64.py states the
+    bounds and the counted exceptions)."""
+    from tests.fd64 import Scene64, compare
+    s = Scene64(oracle)
+    adj, rec = s.adjoint_f64()
+    _, summary = compare(s, adj, s.draw(adj), rec)
+    print(summary)

@@ -60,11 +60,11 @@ class GpuPipe:
         aux = self.aux.readback(np.uint32).reshape(self.V, self.tl.height, self.tl.width, 2)
         return img, aux
 
-    def backward(self, dl_dc: np.ndarray, mode: int):
+    def backward(self, dl_dc: np.ndarray, mode: int, compensated: bool = False):
         self.dl = self.ctx.storage_buffer("dl_dc", np.ascontiguousarray(dl_dc, np.float32))
         self.pg = self.r.alloc_projected_grad(self.g, self.V)
         self.r.composite_backward(self.proj, self.bins, self.img, self.dl, self.pg, self.tl, self.stride, self.V,
-                                  mode=mode, aux=self.aux)
+                                  mode=mode, aux=self.aux, compensated=compensated)
         return self.pg.readback(np.float32).reshape(self.V, self.stride, 12)[:, : len(self.scene)]
 
 
