@@ -240,7 +240,9 @@ sc_status sc_exclusive_scan_u32(sc_ctx* ctx, uint32_t* data, uint64_t n, uint64_
  * that every GPU loading the library holds until the process exits; n above
  * SC_NOALLOC_SCAN_MAX_N returns SC_ERR_INVALID_ARG without touching data.
  * The first call on a device looks the array's device address up (no
- * allocation); make that first call before any stream capture.  All calls
+ * allocation) and keeps it until the process exits; make that first call
+ * before any stream capture, and do not use the library on a device after a
+ * cudaDeviceReset of it (the kept address would be stale).  All calls
  * share the array, which keeps the last call's contents (each call clears the
  * part it uses), so calls that overlap on the GPU — on different streams or
  * contexts of the same device — race and must be serialised by the caller.
