@@ -195,7 +195,7 @@ void sc_camera_from_pose(const float eye[3], const float target[3], const float 
 /* project_gaussians.wgsl:156-259 for n_views cameras: projected holds
  * n_views * sc_splats_capacity() records, view-major.  The reference forms
  * det = s00 s11 - s01^2 in f32 and culls det <= 0 (:226-234); with
- * sc_ctx_set_fp64_det a near-degenerate splat (det < 2^-10 s00 s11 in f32)
+ * sc_ctx_set_fp64_det a near-degenerate splat (det < 2^-6 s00 s11 in f32)
  * gets its determinant and conic in FP64 instead. */
 sc_status sc_project(sc_ctx* ctx, const sc_splats* s, const sc_camera* cams, uint32_t n_views,
                      sc_projected_splat* projected);                 /* Rasterizer::project, raster.rs:731-794 */
@@ -311,7 +311,7 @@ sc_status sc_project_backward(sc_ctx* ctx, const sc_splats* s, const sc_projecte
 
 /* Precision option of sc_project and sc_project_backward (off by default,
  * which is the reference's f32 arithmetic): when enabled, a splat whose f32
- * 2x2 projected-covariance determinant keeps less than 2^-10 of s00 s11
+ * 2x2 projected-covariance determinant keeps less than 2^-6 of s00 s11
  * (a needle-like splat, where cancellation has eaten the f32 determinant)
  * gets the determinant from Lagrange's identity det = |B0 x B1|^2 +
  * 0.3 (|B0|^2 + |B1|^2) + 0.09 (Sigma2D = B B^T + 0.3 I) and the inverse in

@@ -139,9 +139,9 @@ __device__ __forceinline__ bool geometry(const Cam& c, float px, float py, float
   const float d = B1[0] * B1[0] + B1[1] * B1[1] + B1[2] * B1[2];
   g.s00 = a + 0.3f; g.s01 = b; g.s11 = d + 0.3f;
   g.det = g.s00 * g.s11 - g.s01 * g.s01;
-  if (precise && g.det < 9.765625e-4f * g.s00 * g.s11) {
+  if (precise && g.det < 0.015625f * g.s00 * g.s11) {
     // near-degenerate (needle-like) splat: the f32 determinant has lost more
-    // than 10 bits to cancellation.  Re-form it in FP64 through Lagrange's
+    // than 6 bits to cancellation.  Re-form it in FP64 through Lagrange's
     // identity |B0|^2 |B1|^2 - (B0.B1)^2 = |B0 x B1|^2, which has no
     // cancellation, and invert in FP64.
     const double c0 = (double)B0[1] * B1[2] - (double)B0[2] * B1[1];

@@ -29,8 +29,8 @@ from nanotracer_b200._lib import SC_KEYS_NATIVE64
 from nanotracer_b200.scene import perturbed
 from nanotracer_b200.train import BENCH_LRS, render_targets
 
-from tests.util import (GpuPipe, adam_first_step, check_image_explained, check_param_grads, check_pg_explained,
-                        check_post_adam, margins)
+from tests.util import (GRAD_ABS_REL, GpuPipe, adam_first_step, check_image_explained, check_param_grads,
+                        check_pg_explained, check_post_adam, margins)
 
 
 def projection_report(g, o):
@@ -93,16 +93,25 @@ def iteration_parity(ctx, oracle, scene, cams, tl: TilingParams, mode: int, labe
         per_view.append(s)
     gpg = pipe.backward(dl.reshape(-1, 4), mode)  # (V, n, 12)
     grads = GradSplatBuffers(ctx, n)
+    alt = np.zeros((n, 59), np.float64)  # the oracle's adjoint of the GPU's projected gradients
+    # the absolute term of the projected-gradient bound carried to the opacity
+    # logit (dsigma * s (1 - s)) and the SH coefficients (dcolor * basis, |basis| <= 1.1)
+    unc = np.zeros((n, 59), np.float64)
+    sig = 1.0 / (1.0 + np.exp(-scene.flat()[:, 10].astype(np.float64)))
     for v in range(V):
         rv = ranges[v * T:(v + 1) * T].reshape(-1)
         opg, absum = oracle.composite_backward(rec[v], pay, rv, otl, img[v].reshape(-1, 4), dl[v], mode,
                                                aux[v, ..., 1].reshape(-1),
                                                aux[v, ..., 0].view(np.float32).reshape(-1), want_abs=True)
         per_view[v]["proj_grads"] = check_pg_explained(gpg[v], opg, absum, flags_bwd, label=f"{label} view {v}")
+        ab = GRAD_ABS_REL * np.asarray(absum, np.float64)
+        unc[:, 10] += ab[:, 2] * sig * (1.0 - sig)
+        unc[:, 11:14] += ab[:, 8:11] * 0.2820948
+        unc[:, 14:59] += np.repeat(ab[:, 8:11], 15, axis=1) * 1.1
         pipe.r.project_backward(pipe.g, pipe.pg, cams[v], grads, view_offset=v * pipe.stride * 48)
-        per_view[v]["param_grads"] = check_param_grads(grads.readback(n).flat(),
-                                                       oracle.project_backward(os_, gpg[v], ocams[v]),
-                                                       label=f"{label} view {v}")
+        ogv = oracle.project_backward(os_, gpg[v], ocams[v])
+        alt += ogv
+        per_view[v]["param_grads"] = check_param_grads(grads.readback(n).flat(), ogv, label=f"{label} view {v}")
     report["views"] = per_view
     if trainer:
         cfg = TrainConfig(n_views=V, width=W, height=H, tile_w=tl.tile_w, tile_h=tl.tile_h, depth_max=tl.depth_max,
@@ -125,6 +134,7 @@ def iteration_parity(ctx, oracle, scene, cams, tl: TilingParams, mode: int, labe
                                              oncon.reshape(-1), otf.reshape(-1))
             ograds += oracle.project_backward(os_, opg2, ocams[v])
         want = adam_first_step(scene.flat(), ograds.astype(np.float32), BENCH_LRS)
-        report["post_adam"] = check_post_adam(g.readback().flat(), want, ograds, flags_bwd | flags_fwd, label=label)
+        report["post_adam"] = check_post_adam(g.readback().flat(), want, ograds, flags_bwd | flags_fwd, alt, unc,
+                                              BENCH_LRS, label=label)
     report["seconds"] = round(time.time() - t0, 1)
     return report
