@@ -580,6 +580,100 @@ def run_precision(args):
     print(json.dumps(out))
 
 
+def run_scenes(args):
+    """BASELINE config 5 (uneven batch), a side line beside the headline: 16
+    independent scenes with splat counts log-uniform in [10k, 500k] and image
+    sizes drawn from {512x512, 1024x768, 1920x1080}, one view each per
+    iteration, stepped by one many-scene trainer (every stage one launch over
+    all scenes, one CUDA graph), against the same scenes stepped by one
+    single-scene trainer each, one after another.  Then the reference's
+    densify / prune schedule per scene under a 6M total cap (densify by
+    gradient threshold 2e-4, prune at opacity < 0.005) over a short run."""
+    import torch
+
+    import nanotracer_b200 as nt
+    from nanotracer_b200.scene import FOV_Y, orbit_views, perturbed, random_scene
+    from nanotracer_b200.scenes import Scene, ScenesTrainer, densify_prune_scenes
+    from nanotracer_b200.train import TrainConfig, Trainer, render_targets
+    ctx = nt.CudaCtx(0)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
+    rng = np.random.default_rng(0x5CE7E5)
+    sizes = [(512, 512), (1024, 768), (1920, 1080)]
+    n_sc = 16
+    counts = [int(x) for x in np.exp(rng.uniform(np.log(1e4), np.log(5e5), n_sc))]
+    dims = [sizes[int(k)] for k in rng.integers(0, 3, n_sc)]
+    maxW, maxH = max(d[0] for d in dims), max(d[1] for d in dims)
+    scenes, cams, tgts = [], [], []
+    for i, (n, (W, H)) in enumerate(zip(counts, dims)):
+        s = random_scene(n, 0x5EED0000 + i)
+        cam = nt.CameraUniform.from_pose(*orbit_views(8, 0)[i % 8], FOV_Y, W, H, n)
+        tgts.append(render_targets(ctx, perturbed(s), [cam], nt.TilingParams(W, H, 16, 8.0))[0])
+        scenes.append(s)
+        cams.append(cam)
+    # one trainer for all scenes
+    st = ScenesTrainer(ctx, n_sc, maxW, maxH)
+    for i in range(n_sc):
+        st.set_scene(i, Scene.upload(ctx, scenes[i], tgts[i], capacity=2 * counts[i]))
+    t = 0
+    for _ in range(max(3, args.warmup)):
+        t += 1
+        st.step(cams, t)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        t += 1
+        losses = st.step(cams, t)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_one = e0.elapsed_time(e1) / args.steps
+    stats = st.stats()
+    # the same scenes, one single-scene trainer each, stepped one after another
+    singles = []
+    for i in range(n_sc):
+        W, H = dims[i]
+        g = nt.GpuSplatBuffer.upload(ctx, scenes[i])
+        mo = nt.AdamMomentBuffers(ctx, g.capacity)
+        acc = ctx.storage_buffer_zeroed("acc", 4 * g.capacity)
+        tr = Trainer(ctx, TrainConfig(n_views=1, width=W, height=H, depth_max=8.0))
+        tr.set_targets(ctx.storage_buffer("t", np.ascontiguousarray(tgts[i], np.float32)))
+        singles.append((tr, g, mo, acc))
+    for k in range(max(3, args.warmup)):
+        for i, (tr, g, mo, acc) in enumerate(singles):
+            tr.step(g, mo, acc, [cams[i]], k + 1)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for k in range(args.steps):
+        for i, (tr, g, mo, acc) in enumerate(singles):
+            tr.step(g, mo, acc, [cams[i]], k + 10)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_sep = e0.elapsed_time(e1) / args.steps
+    del singles
+    # the densify / prune schedule (train.rs:259-362) per scene, 6M total cap
+    sched = []
+    w0 = time.perf_counter()
+    for it in range(1, 201):
+        t += 1
+        st.step(cams, t)
+        ev = densify_prune_scenes(st, it, grad_count=100, max_total=6_000_000, prune_every=100, prune_warmup=50,
+                                  densify_every=100, densify_warmup=100)
+        if any(ev.values()):
+            sched.append({"iter": it, **ev, "total": sum(s.splats.n for s in st.scenes)})
+    sched_s = time.perf_counter() - w0
+    line = {"metric": "config 5 uneven batch: 16 scenes per iteration, one launch per stage", "unit": UNIT,
+            "value": 1e3 / ms_one, "ms_per_iter": round(ms_one, 4), "steps": args.steps,
+            "separate_trainers_ms_per_iter": round(ms_sep, 4),
+            "speedup_over_separate_trainers": round(ms_sep / ms_one, 3),
+            "config": {"scenes": n_sc, "splats": counts, "images": [f"{w}x{h}" for w, h in dims],
+                       "total_splats": sum(counts), "tile_grid": f"{maxW}x{maxH}, 16x16 tiles"},
+            "items_per_iter": stats["items"], "kernels_per_step": stats["kernels_per_step"],
+            "loss_mean": float(np.mean(losses)),
+            "densify_prune": {"iterations": 200, "wall_s": round(sched_s, 2), "events": sched,
+                              "final_total": sum(s.splats.n for s in st.scenes)}}
+    print(json.dumps(line))
+
+
 def run_views(args, ws, rank, local, pg):
     """N ranks share one iteration of one scene: the iteration's views are split
     across the ranks (data-parallel views, one NCCL reduce-scatter of the
@@ -820,10 +914,14 @@ def main():
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the other forms' side runs (batched other precision, plain FP32) and their PSNR")
     ap.add_argument("--no-psnr", action="store_true", help=argparse.SUPPRESS)  # older name of --no-forms
-    ap.add_argument("--workload", default="batched", choices=["batched", "precision"],
-                    help="precision: the config-4 side line (3M splats, 4 views, BF16, FP64-oracle errors)")
+    ap.add_argument("--workload", default="batched", choices=["batched", "precision", "scenes"],
+                    help="precision: the config-4 side line (3M splats, 4 views, BF16, FP64-oracle errors); "
+                         "scenes: the config-5 side line (16 uneven scenes in one launch per stage)")
     args = ap.parse_args()
     args.no_forms = args.no_forms or args.no_psnr
+    if args.workload == "scenes":
+        run_scenes(args)
+        return
     if args.workload == "precision":
         if args.splats == 1_000_000 and args.views == 8:  # config 4's sizes unless given
             args.splats, args.views = 3_000_000, 4

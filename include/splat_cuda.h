@@ -417,6 +417,44 @@ sc_status sc_trainer_set_profiling(sc_trainer* tr, int enabled);
  * same for the backward.  No counterpart in the reference. */
 sc_status sc_trainer_blend_work(const sc_trainer* tr, uint64_t out[4]);
 
+/* ------------------------------------------------ many scenes in one launch per stage
+ * No counterpart in the reference, which trains one scene per train() call
+ * (train.rs:65-401).  n_scenes independent scenes, each with its own store,
+ * Adam moments, densify statistic, camera, image size and target, step
+ * together: every stage is one launch over all scenes (projection, depth sort,
+ * two-level binning, blend forward and backward over one (scene, tile) grid,
+ * projection backward, Adam), the whole step one CUDA graph.  Images of
+ * different sizes share the tiling's tile grid (tiling.width x
+ * tiling.height, the largest); a scene's pixels are those inside its own
+ * width x height, and its loss is its own MSE (loss.rs:163-179).  Densify
+ * and prune run per scene on its own store between steps (sc_densify,
+ * sc_prune_low_opacity); a store whose capacity changes is set again. */
+typedef struct sc_scenes_config {
+  uint32_t n_scenes;           /* at most 64 */
+  sc_tiling tiling;            /* the largest image and the tile shape */
+  sc_adam_groups adam;
+  uint32_t use_graph;
+  uint32_t tile_cull;
+  float log_scale_min, log_scale_max, opacity_logit_max;
+  uint32_t fp64_det, compensated_sums;
+} sc_scenes_config;
+typedef struct sc_scenes_trainer sc_scenes_trainer;
+sc_status sc_scenes_trainer_create(sc_ctx* ctx, const sc_scenes_config* cfg, sc_scenes_trainer** out);
+void sc_scenes_trainer_free(sc_ctx* ctx, sc_scenes_trainer* st);
+/* Scene i: its store, moments (capacity >= the store's), densify statistic
+ * (device, one float per splat of capacity), image size (within the tiling)
+ * and target (device, width * height float3, copied in by this call). */
+sc_status sc_scenes_trainer_set_scene(sc_scenes_trainer* st, uint32_t i, sc_splats* s, sc_moments* mo,
+                                      float* grad_acc, uint32_t width, uint32_t height, const float* target);
+/* One step of every scene: cams[i] (host, its width/height = scene i's), the
+ * shared Adam step count t; losses (host, nullable) receives each scene's
+ * MSE.  Blocking, like sc_trainer_step. */
+sc_status sc_scenes_trainer_step(sc_scenes_trainer* st, const sc_camera* cams, uint64_t t, double* losses);
+/* device images of the last step: n_scenes x tiling.height x tiling.width float4 */
+sc_status sc_scenes_trainer_images(const sc_scenes_trainer* st, const float** images);
+sc_status sc_scenes_trainer_stats(const sc_scenes_trainer* st, uint64_t* pairs, uint32_t* n_kernels,
+                                  uint64_t* items);
+
 /* Failure-detection self-test (no counterpart in the reference): runs one
  * radix-sort pass whose look-back waits on a tile that is never processed.
  * The bounded wait gives up (about a second), the kernel ends, and the call

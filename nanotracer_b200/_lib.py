@@ -65,6 +65,12 @@ class sc_train_config(C.Structure):
                 ("sort_digit_bits", C.c_uint32)]
 
 
+class sc_scenes_config(C.Structure):
+    _fields_ = [("n_scenes", C.c_uint32), ("tiling", sc_tiling), ("adam", sc_adam_groups), ("use_graph", C.c_uint32),
+                ("tile_cull", C.c_uint32), ("log_scale_min", C.c_float), ("log_scale_max", C.c_float),
+                ("opacity_logit_max", C.c_float), ("fp64_det", C.c_uint32), ("compensated_sums", C.c_uint32)]
+
+
 assert C.sizeof(sc_camera) == 96
 
 P = C.c_void_p
@@ -144,6 +150,12 @@ _PROTOS = {
     "sc_trainer_set_profiling": (ST, [P, I32]),
     "sc_trainer_blend_work": (ST, [P, C.POINTER(U64)]),
     "sc_selftest_wait_timeout": (ST, [P]),
+    "sc_scenes_trainer_create": (ST, [P, C.POINTER(sc_scenes_config), C.POINTER(P)]),
+    "sc_scenes_trainer_free": (None, [P, P]),
+    "sc_scenes_trainer_set_scene": (ST, [P, U32, P, P, P, U32, U32, P]),
+    "sc_scenes_trainer_step": (ST, [P, P, U64, C.POINTER(C.c_double)]),
+    "sc_scenes_trainer_images": (ST, [P, C.POINTER(P)]),
+    "sc_scenes_trainer_stats": (ST, [P, C.POINTER(U64), C.POINTER(U32), C.POINTER(U64)]),
     "sc_trainer_step_grads": (ST, [P, P, P, F32, U32, U32, P, C.POINTER(C.c_double)]),
     "sc_adam_step_shard": (ST, [P, P, P, P, P, U32, U32, U32, U64, C.POINTER(sc_adam_groups), F32, F32, F32]),
     "sc_splats_pack_range": (ST, [P, P, U32, U32, U32, P]),

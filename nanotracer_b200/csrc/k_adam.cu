@@ -225,10 +225,10 @@ __device__ __forceinline__ void adam_row8(Row8& x, float a, float s2, const Adam
 // The geometric launch is held to 3 CTAs per SM (80 registers, a few bytes
 // spilled in the rotation group): more rows in flight beat the spill.
 template <bool GEOM>
-__global__ void __launch_bounds__(256, GEOM ? 3 : 4) k_adam_rows(DSplats s, DMoments mo, float* __restrict__ acc,
-                                                   const float* __restrict__ g, uint32_t lo, uint32_t count,
-                                                   uint32_t gstride, AdamParams ap, const float* __restrict__ d_bc,
-                                                   const uint32_t* __restrict__ skip) {
+__device__ __forceinline__ void adam_rows(const DSplats& s, const DMoments& mo, float* __restrict__ acc,
+                                          const float* __restrict__ g, uint32_t lo, uint32_t count, uint32_t gstride,
+                                          AdamParams ap, const float* __restrict__ d_bc,
+                                          const uint32_t* __restrict__ skip) {
   const uint32_t j0 = (blockIdx.x * blockDim.x + threadIdx.x) * ADAM_SPT;
   if (j0 >= count) return;
   if (skip && (*skip & SC_DEVERR_CAPACITY)) return;  // a capacity overflow earlier in the step: leave parameters untouched
@@ -302,6 +302,34 @@ __global__ void __launch_bounds__(256, GEOM ? 3 : 4) k_adam_rows(DSplats s, DMom
     for (int e = 0; e < ADAM_SPT; ++e) x.p[e] = fminf(fmaxf(x.p[e], -ap.opacity_logit_max), ap.opacity_logit_max);
   }
   store_row8(s, mo, r, i0, nv, x, ap.seed);
+}
+
+template <bool GEOM>
+__global__ void __launch_bounds__(256, GEOM ? 3 : 4) k_adam_rows(DSplats s, DMoments mo, float* __restrict__ acc,
+                                                   const float* __restrict__ g, uint32_t lo, uint32_t count,
+                                                   uint32_t gstride, AdamParams ap, const float* __restrict__ d_bc,
+                                                   const uint32_t* __restrict__ skip) {
+  adam_rows<GEOM>(s, mo, acc, g, lo, count, gstride, ap, d_bc, skip);
+}
+
+// Many scenes: grid.z = scene, each with its own store, moments, statistic
+// and gradient rows (all of its splats, the shared step t).
+template <bool GEOM>
+__global__ void __launch_bounds__(256, GEOM ? 3 : 4) k_adam_rows_scenes(const SceneDev* __restrict__ scenes,
+                                                          AdamParams ap, const float* __restrict__ d_bc,
+                                                          const uint32_t* __restrict__ skip) {
+  const SceneDev sd = scenes[blockIdx.z];
+  adam_rows<GEOM>(sd.s, sd.mo, sd.acc, sd.grads, 0, sd.s.n, sd.gstride, ap, d_bc, skip);
+}
+
+sc_status launch_adam_rows_scenes(sc_ctx* ctx, const SceneDev* d_scenes, uint32_t n_scenes, uint32_t max_count,
+                                  const AdamParams& ap, const float* d_bc, const uint32_t* d_skip) {
+  if (n_scenes == 0 || max_count == 0) return SC_OK;
+  const unsigned gx = (unsigned)sc_div_up(sc_div_up(max_count, ADAM_SPT), 256);
+  k_adam_rows_scenes<true><<<dim3(gx, 9, n_scenes), 256, 0, ctx->stream>>>(d_scenes, ap, d_bc, d_skip);
+  SC_TRY(sc_check_launch(ctx, "k_adam_rows_scenes"));
+  k_adam_rows_scenes<false><<<dim3(gx, ADAM_GROUPS - 9, n_scenes), 256, 0, ctx->stream>>>(d_scenes, ap, d_bc, d_skip);
+  return sc_check_launch(ctx, "k_adam_rows_scenes");
 }
 
 sc_status launch_adam_rows(sc_ctx* ctx, const DSplats& s, const DMoments& mo, float* acc, const float* g, uint32_t lo,

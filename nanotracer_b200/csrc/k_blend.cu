@@ -28,6 +28,7 @@ struct BlendArgs {
   uint32_t width, height, tw, th, tiles_x, tiles_y, num_tiles, stride;
   uint64_t pixels;  // per view
   uint32_t batch;   // list positions staged per batch, at most the block's threads
+  const SceneDev* scenes;  // per-view image sizes and MSE scales (many-scene steps), or null
 };
 
 static BlendArgs blend_args(const sc_tiling* tl, uint32_t stride) {
@@ -39,7 +40,18 @@ static BlendArgs blend_args(const sc_tiling* tl, uint32_t stride) {
   a.stride = stride;
   a.pixels = (uint64_t)tl->width * tl->height;
   a.batch = 0;
+  a.scenes = nullptr;
   return a;
+}
+
+// a view's image size and MSE scale: the scene's in a many-scene step
+__device__ __forceinline__ void view_dims(const BlendArgs& a, uint32_t v, float gscale, uint32_t& W, uint32_t& H,
+                                          float& gs) {
+  W = a.width; H = a.height; gs = gscale;
+  if (a.scenes) {
+    const SceneDev& sd = a.scenes[v];
+    W = sd.width; H = sd.height; gs = sd.gscale;
+  }
 }
 
 // the batch depth for a launch of `threads` threads: `batch` rounded down to
@@ -263,6 +275,9 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
   const uint32_t px = tx * a.tw + threadIdx.x % a.tw;
   const uint32_t py0 = ty * a.th + PPT * (threadIdx.x / a.tw);
   const float fx = (float)px + 0.5f;
+  uint32_t W, H;
+  float gs;
+  view_dims(a, v, gscale, W, H, gs);
   uint32_t bit;
   const uint2 r = list_range<LIST>(l, a, v, tx, ty, tile, bit);
   const uint32_t begin = r.x, end = r.y > r.x ? r.y : r.x;
@@ -290,7 +305,7 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
   for (int k = 0; k < PPT; ++k) {
     T[k] = 1.0f; cr[k] = cg[k] = cb[k] = 0.f; last[k] = 0;
     fy[k] = (float)(py0 + k) + 0.5f;
-    done[k] = !(px < a.width && py0 + k < a.height);
+    done[k] = !(px < W && py0 + k < H);
     all_done &= done[k];
   }
   ListWord f = fetch(0);
@@ -316,7 +331,7 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
         // alpha 0, which leaves its colour and T bit for bit unchanged.  A
         // pixel is done exactly when its T < 1e-4 (a pixel outside the image,
         // never written, runs with T = 0).
-        const bool in0 = px < a.width && py0 < a.height, in1 = px < a.width && py0 + 1 < a.height;
+        const bool in0 = px < W && py0 < H, in1 = px < W && py0 + 1 < H;
         float2 T2 = make_float2(in0 ? T[0] : 0.0f, in1 ? T[1] : 0.0f);
         float2 R2 = make_float2(cr[0], cr[1]), G2 = make_float2(cg[0], cg[1]), B2 = make_float2(cb[0], cb[1]);
         const float2 fy2 = make_float2(fy[0], fy[1]);
@@ -382,12 +397,12 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
 #pragma unroll
   for (int q = 0; q < PPT; ++q) {
     const uint32_t py = py0 + q;
-    if (px < a.width && py < a.height) {
+    if (px < W && py < H) {
       const size_t pix = (size_t)v * a.pixels + (size_t)py * a.width + px;
       image[pix] = make_float4(cr[q], cg[q], cb[q], 1.0f - T[q]);
       if (aux) aux[pix] = make_uint2(__float_as_uint(T[q]), last[q]);
       if (target) {
-        const float3 d = mse_pixel(cr[q], cg[q], cb[q], target + 3 * pix, gscale, sq);
+        const float3 d = mse_pixel(cr[q], cg[q], cb[q], target + 3 * pix, gs, sq);
         dl_dc[pix] = make_float4(d.x, d.y, d.z, 0.0f);
       }
     }
@@ -423,9 +438,10 @@ template <int LIST>
 static sc_status composite_list(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views, const ListArgs& l,
                                 const sc_tiling* tl, float4* image, uint2* aux, const float* target, float mse_scale,
                                 float4* dl_dc, double* loss, const uint32_t* d_skip, uint64_t* work,
-                                uint32_t batch) {
+                                uint32_t batch, const SceneDev* scenes) {
   BlendArgs a = blend_args(tl, stride);
   a.batch = batch;
+  a.scenes = scenes;
   const uint32_t pixels = tl->tile_w * tl->tile_h;
   if (pixels > 512 || pixels % 32 != 0) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile must hold 32..512 pixels, multiple of 32");
   const uint64_t grid = (uint64_t)n_views * a.num_tiles;
@@ -446,19 +462,19 @@ sc_status launch_composite(sc_ctx* ctx, const float4* rec, uint32_t stride, uint
                            float mse_scale, float4* dl_dc, double* loss, const uint32_t* d_skip) {
   ListArgs l{payloads, reinterpret_cast<const uint2*>(ranges), nullptr, 0, 0};
   return composite_list<LIST_PAIRS>(ctx, rec, stride, n_views, l, tl, image, aux, target, mse_scale, dl_dc, loss,
-                                    d_skip, nullptr, 0);
+                                    d_skip, nullptr, 0, nullptr);
 }
 
 sc_status launch_composite_items(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
                                  const uint32_t* item_keys, const uint32_t* item_ids, const uint32_t* item_ranges,
                                  const sc_tiling* tl, float4* image, uint2* aux, const float* target, float mse_scale,
                                  float4* dl_dc, double* loss, const uint32_t* d_skip, uint64_t* work,
-                                 uint32_t batch) {
+                                 uint32_t batch, const SceneDev* scenes) {
   const BlendArgs a = blend_args(tl, stride);
   ListArgs l{item_ids, reinterpret_cast<const uint2*>(item_ranges), item_keys, (a.tiles_x + SC_SUPER - 1) / SC_SUPER,
              super_tiles_per_view(tl)};
   return composite_list<LIST_ITEMS>(ctx, rec, stride, n_views, l, tl, image, aux, target, mse_scale, dl_dc, loss,
-                                    d_skip, work, batch);
+                                    d_skip, work, batch, scenes);
 }
 
 // ---------------------------------------------------------------- MSE (standalone)
@@ -595,6 +611,9 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
   const uint32_t px = tx * a.tw + threadIdx.x % a.tw;
   const uint32_t py0 = ty * a.th + PPT * (threadIdx.x / a.tw);
   const float fx = (float)px + 0.5f;
+  uint32_t W, H;
+  float gs;
+  view_dims(a, v, gscale, W, H, gs);
   uint32_t bit;
   const uint2 r = list_range<LIST>(l, a, v, tx, ty, tile, bit);
   const uint32_t begin = r.x, end = r.y > r.x ? r.y : r.x;
@@ -615,13 +634,13 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
     fy[q] = (float)py + 0.5f;
     T[q] = 1.0f; gr[q] = gg[q] = gb[q] = 0.f; GS[q] = 0.f;
     stop[q] = begin;
-    done[q] = !(px < a.width && py < a.height);
+    done[q] = !(px < W && py < H);
     if (!done[q]) {
       const size_t pix = (size_t)v * a.pixels + (size_t)py * a.width + px;
       float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
       if (target || MODE == SC_BWD_REF) c = fwd[pix];
       if (target) {
-        const float3 d = mse_pixel(c.x, c.y, c.z, target + 3 * pix, gscale, sq);
+        const float3 d = mse_pixel(c.x, c.y, c.z, target + 3 * pix, gs, sq);
         gr[q] = d.x; gg[q] = d.y; gb[q] = d.z;
       } else {
         const float4 d = dl_dc[pix];
@@ -876,9 +895,11 @@ template <int LIST>
 static sc_status backward_list(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views, const ListArgs& l,
                                const sc_tiling* tl, const float4* fwd, const float4* dl_dc, const float* target,
                                float mse_scale, double* loss, int mode, const uint2* aux, float4* proj_grad,
-                               const uint32_t* d_skip, uint64_t* work, float4* proj_comp, uint32_t batch) {
+                               const uint32_t* d_skip, uint64_t* work, float4* proj_comp, uint32_t batch,
+                               const SceneDev* scenes) {
   BlendArgs a = blend_args(tl, stride);
   a.batch = batch;
+  a.scenes = scenes;
   const float gscale = (2.0f / ((float)tl->width * (float)tl->height * 3.0f)) * mse_scale;
   const uint32_t pixels = tl->tile_w * tl->tile_h;
   if (pixels > 512 || pixels % 32 != 0) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile must hold 32..512 pixels, multiple of 32");
@@ -901,7 +922,7 @@ sc_status launch_composite_backward(sc_ctx* ctx, const float4* rec, uint32_t str
                                     float mse_scale, double* loss, float4* proj_comp) {
   ListArgs l{payloads, reinterpret_cast<const uint2*>(ranges), nullptr, 0, 0};
   return backward_list<LIST_PAIRS>(ctx, rec, stride, n_views, l, tl, fwd, dl_dc, target, mse_scale, loss, mode, aux,
-                                   proj_grad, d_skip, nullptr, proj_comp, 0);
+                                   proj_grad, d_skip, nullptr, proj_comp, 0, nullptr);
 }
 
 sc_status launch_composite_backward_items(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
@@ -909,12 +930,13 @@ sc_status launch_composite_backward_items(sc_ctx* ctx, const float4* rec, uint32
                                           const uint32_t* item_ranges, const sc_tiling* tl, const float4* fwd,
                                           const float4* dl_dc, int mode, const uint2* aux, float4* proj_grad,
                                           const uint32_t* d_skip, const float* target, float mse_scale,
-                                          double* loss, uint64_t* work, float4* proj_comp, uint32_t batch) {
+                                          double* loss, uint64_t* work, float4* proj_comp, uint32_t batch,
+                                          const SceneDev* scenes) {
   const BlendArgs a = blend_args(tl, stride);
   ListArgs l{item_ids, reinterpret_cast<const uint2*>(item_ranges), item_keys, (a.tiles_x + SC_SUPER - 1) / SC_SUPER,
              super_tiles_per_view(tl)};
   return backward_list<LIST_ITEMS>(ctx, rec, stride, n_views, l, tl, fwd, dl_dc, target, mse_scale, loss, mode, aux,
-                                   proj_grad, d_skip, work, proj_comp, batch);
+                                   proj_grad, d_skip, work, proj_comp, batch, scenes);
 }
 
 // proj_grad += proj_comp over n float4 (the compensated totals rounded once)

@@ -183,15 +183,18 @@ struct TileArgs { uint32_t tw, th, tiles_x, tiles_y, cull, super; };
 // chunk's parameters from L2 while each view plane of the outputs is still
 // written with coalesced stores (the per-view work — rotation, scales, SH —
 // does not share between views anyway).
-__global__ void __launch_bounds__(128, 8) k_project(DSplats s, const sc_camera* __restrict__ cams, uint32_t n_views,
+// scenes (nullable): view v projects scene v's own store.
+__global__ void __launch_bounds__(128, 8) k_project(DSplats s_all, const sc_camera* __restrict__ cams, uint32_t n_views,
                                                  uint32_t stride, float4* __restrict__ rec, TileArgs ta,
                                                  uint32_t* __restrict__ depth_keys, uint32_t* __restrict__ ids,
                                                  uint32_t* __restrict__ counts, int precise,
-                                                 float4* __restrict__ zero_grad, float4* __restrict__ zero_comp) {
+                                                 float4* __restrict__ zero_grad, float4* __restrict__ zero_comp,
+                                                 const SceneDev* __restrict__ scenes) {
   const uint32_t chunk = blockIdx.x / n_views;
   const uint32_t v = blockIdx.x - chunk * n_views;
   const uint32_t i = chunk * blockDim.x + threadIdx.x;
   if (i >= stride) return;
+  const DSplats s = scenes ? scenes[v].s : s_all;
   const bool live = i < s.n;
   float px = 0, py = 0, pz = 0, qw = 1, qx = 0, qy = 0, qz = 0, l0 = 0, l1 = 0, l2 = 0, op = 0, d0 = 0, d1 = 0, d2 = 0;
   if (live) {
@@ -277,7 +280,7 @@ __global__ void __launch_bounds__(128, 8) k_project(DSplats s, const sc_camera* 
 
 sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams, uint32_t n_views, uint32_t stride,
                          float4* rec, const sc_tiling* tl, uint32_t* depth_keys, uint32_t* ids, uint32_t* counts,
-                         int precise, int cull, float4* zero_grad, float4* zero_comp) {
+                         int precise, int cull, float4* zero_grad, float4* zero_comp, const SceneDev* scenes) {
   if (stride == 0 || n_views == 0) return SC_OK;
   TileArgs ta{1, 1, 1, 1, 0, 0};
   if (tl) ta = TileArgs{tl->tile_w, tl->tile_h, (tl->width + tl->tile_w - 1) / tl->tile_w,
@@ -286,7 +289,7 @@ sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams,
   const uint64_t blocks = sc_div_up(stride, bs) * (uint64_t)n_views;
   if (blocks > 0x7FFFFFFFull) return sc_fail(ctx, SC_ERR_INVALID_ARG, "too many splat views for one launch");
   k_project<<<(unsigned)blocks, bs, 0, ctx->stream>>>(s, d_cams, n_views, stride, rec, ta, depth_keys, ids, counts,
-                                                      precise, zero_grad, zero_comp);
+                                                      precise, zero_grad, zero_comp, scenes);
   return sc_check_launch(ctx, "k_project");
 }
 
@@ -434,13 +437,11 @@ __device__ __forceinline__ float4 f4add(float4 a, float4 b) {
 constexpr int PB_THREADS = 128;
 constexpr int PB_GROUP = 32;  // views per group: one validity bit each
 
-__global__ void __launch_bounds__(PB_THREADS, 5) k_project_backward_shards(DSplats s, const float4* __restrict__ pg,
-                                                                     uint32_t stride,
-                                                                     const sc_camera* __restrict__ cams,
-                                                                     uint32_t n_views, float* __restrict__ out,
-                                                                     uint32_t n_shards, uint32_t shard,
-                                                                     const uint32_t* __restrict__ skip, int precise,
-                                                                     const float4* __restrict__ pc) {
+__device__ __forceinline__ void project_backward_rows(const DSplats& s, const float4* __restrict__ pg,
+                                                      uint32_t stride, const sc_camera* __restrict__ cams,
+                                                      uint32_t n_views, float* __restrict__ out, uint32_t n_shards,
+                                                      uint32_t shard, const uint32_t* __restrict__ skip, int precise,
+                                                      const float4* __restrict__ pc) {
   __shared__ float s_rest[45 * PB_THREADS];
   const uint64_t i = (uint64_t)blockIdx.x * PB_THREADS + threadIdx.x;
   if (i >= (uint64_t)n_shards * shard) return;
@@ -508,6 +509,41 @@ __global__ void __launch_bounds__(PB_THREADS, 5) k_project_backward_shards(DSpla
   for (int r = 0; r < 14; ++r) dst[(size_t)r * shard] = gg[r];
 #pragma unroll
   for (int k = 0; k < 45; ++k) dst[(size_t)(SC_ROW_REST + k) * shard] = srest[k * PB_THREADS];
+}
+
+__global__ void __launch_bounds__(PB_THREADS, 5) k_project_backward_shards(DSplats s, const float4* __restrict__ pg,
+                                                                     uint32_t stride,
+                                                                     const sc_camera* __restrict__ cams,
+                                                                     uint32_t n_views, float* __restrict__ out,
+                                                                     uint32_t n_shards, uint32_t shard,
+                                                                     const uint32_t* __restrict__ skip, int precise,
+                                                                     const float4* __restrict__ pc) {
+  project_backward_rows(s, pg, stride, cams, n_views, out, n_shards, shard, skip, precise, pc);
+}
+
+// Many scenes, one view each: grid.y = scene; scene v's gradient rows from
+// its view's records (pg + 3 v stride) into its own rows (grads, gstride).
+__global__ void __launch_bounds__(PB_THREADS, 5) k_project_backward_scenes(const SceneDev* __restrict__ scenes,
+                                                                     const float4* __restrict__ pg, uint32_t stride,
+                                                                     const sc_camera* __restrict__ cams,
+                                                                     const uint32_t* __restrict__ skip, int precise,
+                                                                     const float4* __restrict__ pc) {
+  const uint32_t v = blockIdx.y;
+  const SceneDev sd = scenes[v];
+  const size_t off = (size_t)3 * v * stride;
+  project_backward_rows(sd.s, pg + off, stride, cams + v, 1, sd.grads, 1, sd.gstride, skip, precise,
+                        pc ? pc + off : nullptr);
+}
+
+sc_status launch_project_backward_scenes(sc_ctx* ctx, const SceneDev* d_scenes, uint32_t n_scenes,
+                                         uint32_t max_gstride, const float4* pg, uint32_t stride,
+                                         const sc_camera* d_cams, const uint32_t* d_skip, int precise_det,
+                                         const float4* pc) {
+  if (n_scenes == 0 || max_gstride == 0) return SC_OK;
+  const dim3 grid((unsigned)sc_div_up(max_gstride, PB_THREADS), n_scenes);
+  k_project_backward_scenes<<<grid, PB_THREADS, 0, ctx->stream>>>(d_scenes, pg, stride, d_cams, d_skip, precise_det,
+                                                                  pc);
+  return sc_check_launch(ctx, "k_project_backward_scenes");
 }
 
 sc_status launch_project_backward_shards(sc_ctx* ctx, const DSplats& s, const float4* pg, uint32_t stride,

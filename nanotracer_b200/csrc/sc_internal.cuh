@@ -83,6 +83,19 @@ struct DMoments {
   uint32_t cap, bf16;
 };
 
+// One scene of a many-scene step (one view per scene): its parameter store,
+// Adam state, densify statistic and gradient rows, its image size inside the
+// step's common tile grid, and its MSE gradient scale 2 / (3 W H).
+struct SceneDev {
+  DSplats s;
+  DMoments mo;
+  float* acc;
+  float* grads;  // SC_NROWS rows x gstride
+  uint32_t gstride;
+  uint32_t width, height;
+  float gscale;
+};
+
 static inline DSplats dview(const sc_splats* s) {
   return DSplats{s->slab, s->rest16, s->n, s->cap, (s->flags & SC_SPLATS_BF16_REST) ? 1u : 0u};
 }
@@ -256,10 +269,13 @@ namespace sck {
 // the native pipeline: (tile, splat) pairs, or with bit 1 of `cull` two-level
 // binning items.  Bit 0 of `cull`: exact tile culling.  zero_grad (nullable):
 // per-(view, splat) gradient records of the same layout set to zero.
+// scenes (nullable, n_views entries): view v projects scene v's own store
+// (its first scene.s.n splats; the rest of the view's stride is culled).
 sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams, uint32_t n_views,
                          uint32_t stride, float4* rec, const sc_tiling* tiling, uint32_t* depth_keys,
                          uint32_t* splat_ids, uint32_t* counts, int precise_det, int cull,
-                         float4* zero_grad = nullptr, float4* zero_comp = nullptr);
+                         float4* zero_grad = nullptr, float4* zero_comp = nullptr,
+                         const SceneDev* scenes = nullptr);
 
 sc_status launch_project_backward(sc_ctx* ctx, const DSplats& s, const float4* proj_grad, const sc_camera* d_cam,
                                   float* grads, uint32_t gcap, int accumulate, int precise_det);
@@ -356,6 +372,17 @@ __device__ __forceinline__ void constrain_geometry(float np[14], const AdamParam
   for (int k = 7; k < 10; ++k) np[k] = fminf(fmaxf(np[k], ap.log_scale_min), ap.log_scale_max);
   np[10] = fminf(fmaxf(np[10], -ap.opacity_logit_max), ap.opacity_logit_max);
 }
+
+// ---- many scenes in one step (one view per scene), each with its own store
+// gradient rows of every scene from its view's records (grid.y = scene)
+sc_status launch_project_backward_scenes(sc_ctx* ctx, const SceneDev* d_scenes, uint32_t n_scenes,
+                                         uint32_t max_gstride, const float4* proj_grad, uint32_t stride,
+                                         const sc_camera* d_cams, const uint32_t* d_skip, int precise_det,
+                                         const float4* proj_comp);
+// Adam + constraints + densify statistic of every scene's splats (grid.z = scene;
+// gstride and the stores' capacities multiples of 8)
+sc_status launch_adam_rows_scenes(sc_ctx* ctx, const SceneDev* d_scenes, uint32_t n_scenes, uint32_t max_count,
+                                  const AdamParams& ap, const float* d_bc, const uint32_t* d_skip);
 
 // ---- data-parallel views (one iteration split across ranks by views)
 // Shard-major gradient layout: element (row r, splat i) of a buffer cut into
@@ -454,7 +481,9 @@ sc_status launch_fold_comp(sc_ctx* ctx, float4* proj_grad, const float4* proj_co
 // sorted by super tile, item_ranges per (view, super tile)): each tile blends
 // the items whose member mask holds it, in list order; aux then holds
 // positions within the super tile's list.  batch: list positions staged per
-// batch (0 = one per thread).  work (nullable, BLEND_WORK_SLOTS
+// batch (0 = one per thread).  scenes (nullable): view v's pixels are those
+// inside scene v's width x height (the images keep the tiling's row pitch) and
+// its MSE scale is the scene's.  work (nullable, BLEND_WORK_SLOTS
 // (scanned, staged) pairs, accumulated): the list positions the CTAs' batches
 // covered and the entries they staged.
 constexpr uint32_t BLEND_WORK_SLOTS = 64;
@@ -462,14 +491,15 @@ sc_status launch_composite_items(sc_ctx* ctx, const float4* rec, uint32_t stride
                                  const uint32_t* item_keys, const uint32_t* item_ids, const uint32_t* item_ranges,
                                  const sc_tiling* tl, float4* image, uint2* aux, const float* target, float mse_scale,
                                  float4* dl_dc, double* loss, const uint32_t* d_skip, uint64_t* work = nullptr,
-                                 uint32_t batch = 0);
+                                 uint32_t batch = 0, const SceneDev* scenes = nullptr);
 sc_status launch_composite_backward_items(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
                                           const uint32_t* item_keys, const uint32_t* item_ids,
                                           const uint32_t* item_ranges, const sc_tiling* tl, const float4* fwd,
                                           const float4* dl_dc, int mode, const uint2* aux, float4* proj_grad,
                                           const uint32_t* d_skip, const float* target = nullptr,
                                           float mse_scale = 0.0f, double* loss = nullptr, uint64_t* work = nullptr,
-                                          float4* proj_comp = nullptr, uint32_t batch = 0);
+                                          float4* proj_comp = nullptr, uint32_t batch = 0,
+                                          const SceneDev* scenes = nullptr);
 sc_status launch_tonemap(sc_ctx* ctx, const float4* img, uint32_t w, uint32_t h, uint8_t* out);
 
 // SSIM (loss.rs:22-375): scale * dL_ssim/dC added into dl_dc, per-view sum of

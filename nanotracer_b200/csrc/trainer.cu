@@ -127,6 +127,19 @@ struct sc_trainer {
   float loss_weight = 0.0f;
   float* gout = nullptr;
   uint32_t g_shards = 0, g_shard = 0;
+  // many scenes (sc_scenes_trainer): view v is scene v, with its own store,
+  // moments, statistic, gradient rows and image size; the table is copied to
+  // the device by the step's first node
+  bool scenes_mode = false;
+  struct SceneHost {
+    sc_splats* s = nullptr; sc_moments* mo = nullptr; float* acc = nullptr;
+    uint32_t width = 0, height = 0;
+    float* grads = nullptr; uint32_t gstride = 0;
+  } scene[SC_MAX_VIEWS];
+  SceneDev* h_scenes = nullptr;  // pinned
+  SceneDev* d_scenes = nullptr;
+  double* h_losses = nullptr;    // pinned: per-view squared-error sums of the last step
+  uint32_t scene_max_cap = 0, scene_max_gstride = 0;
   // graph
   cudaGraphExec_t exec = nullptr;
   const void* g_key[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -280,11 +293,15 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
                                                      offsetof(StepParams, bc));
   const uint32_t V = tr->V;
   const uint64_t nsp = (uint64_t)V * tr->stride;
-  const DSplats ds = dview(s);
+  const DSplats ds = s ? dview(s) : DSplats{};
   const DMoments dm = mo ? dview(mo) : DMoments{};
   const uint64_t launches0 = ctx->launches;
   SC_CUDA_TRY(ctx, cudaMemcpyAsync(tr->d_params, tr->h_params, sizeof(StepParams), cudaMemcpyHostToDevice, ctx->stream),
               "params H2D");
+  if (tr->scenes_mode)
+    SC_CUDA_TRY(ctx, cudaMemcpyAsync(tr->d_scenes, tr->h_scenes, sizeof(SceneDev) * V, cudaMemcpyHostToDevice,
+                                     ctx->stream), "scene table H2D");
+  const SceneDev* scenes = tr->scenes_mode ? tr->d_scenes : nullptr;
   if (tr->h_targets) {  // host targets: this step's copy runs beside the stages that do not read them, view by view
     SC_CUDA_TRY(ctx, cudaEventRecord(tr->ev_fork, ctx->stream), "fork");
     SC_CUDA_TRY(ctx, cudaStreamWaitEvent(tr->copy_stream, tr->ev_fork, 0), "fork wait");
@@ -304,7 +321,8 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   mark(tr, 0, capturing);
   SC_TRY(sck::launch_project(ctx, ds, d_cams, V, tr->stride, tr->rec, &tr->cfg.tiling, tr->dkeys, tr->ids,
                              tr->counts_by_id, tr->cfg.fp64_det ? 1 : 0,
-                             (tr->cfg.tile_cull ? 1 : 0) | (tr->two_level ? 2 : 0), tr->pgrad, tr->pcomp));
+                             (tr->cfg.tile_cull ? 1 : 0) | (tr->two_level ? 2 : 0), tr->pgrad, tr->pcomp,
+                             tr->scenes_mode ? tr->d_scenes : nullptr));
   mark(tr, 1, capturing);
   bool in_tmp = false;
   SC_TRY(sck::radix_sort_segments(ctx, tr->dkeys, tr->ids, tr->dkeys_tmp, tr->ids_tmp, tr->stride, V, 32, tr->scratch,
@@ -380,7 +398,7 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   if (tr->two_level)
     SC_TRY(sck::launch_composite_items(ctx, tr->rec, tr->stride, V, item_keys, item_ids, tr->iranges, &tr->cfg.tiling,
                                        tr->image, tr->aux, fwd_target, mse_w, tr->dl_dc, tr->d_loss, ctx->d_error,
-                                       work_fwd, tr->cfg.blend_batch));
+                                       work_fwd, tr->cfg.blend_batch, scenes));
   else
     SC_TRY(sck::launch_composite(ctx, tr->rec, tr->stride, V, svals, tr->ranges, &tr->cfg.tiling, tr->image, tr->aux,
                                  fwd_target, mse_w, tr->dl_dc, tr->d_loss, ctx->d_error));
@@ -414,7 +432,8 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
                                                   tr->image + po, tr->dl_dc ? tr->dl_dc + po : nullptr,
                                                   (int)tr->cfg.bwd_mode, tr->aux + po,
                                                   tr->pgrad + so, ctx->d_error, tg, mse_w, tr->d_loss + v0, work_bwd,
-                                                  tr->pcomp ? tr->pcomp + so : nullptr, tr->cfg.blend_batch));
+                                                  tr->pcomp ? tr->pcomp + so : nullptr, tr->cfg.blend_batch,
+                                                  scenes ? scenes + v0 : nullptr));
     else
       st = (sck::launch_composite_backward(ctx, tr->rec + so, tr->stride, nv, svals, tr->ranges + (size_t)2 * v0 * tr->T,
                                             &tr->cfg.tiling, tr->image + po, tr->dl_dc ? tr->dl_dc + po : nullptr,
@@ -434,7 +453,12 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   ap.bc1 = ap.bc2 = 1.0f;
   ap.log_scale_min = tr->cfg.log_scale_min; ap.log_scale_max = tr->cfg.log_scale_max;
   ap.opacity_logit_max = tr->cfg.opacity_logit_max;
-  if (tr->grads_mode)
+  if (tr->scenes_mode) {
+    // every scene's gradient rows from its own view, then every scene's Adam step
+    SC_TRY(sck::launch_project_backward_scenes(ctx, tr->d_scenes, V, tr->scene_max_gstride, tr->pgrad, tr->stride,
+                                               d_cams, ctx->d_error, tr->cfg.fp64_det ? 1 : 0, tr->pcomp));
+    SC_TRY(sck::launch_adam_rows_scenes(ctx, tr->d_scenes, V, tr->scene_max_cap, ap, d_bc, ctx->d_error));
+  } else if (tr->grads_mode)
     SC_TRY(sck::launch_project_backward_shards(ctx, ds, tr->pgrad, tr->stride, d_cams, V, tr->gout, tr->g_shards,
                                                tr->g_shard, ctx->d_error, tr->cfg.fp64_det ? 1 : 0, tr->pcomp));
   else {
@@ -449,6 +473,9 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
                                        tr->d_total, ctx->d_error, tr->d_out);
   SC_TRY(sc_check_launch(ctx, "k_finalize"));
   SC_CUDA_TRY(ctx, cudaMemcpyAsync(tr->h_out, tr->d_out, sizeof(StepOut), cudaMemcpyDeviceToHost, ctx->stream), "out D2H");
+  if (tr->scenes_mode)
+    SC_CUDA_TRY(ctx, cudaMemcpyAsync(tr->h_losses, tr->d_loss, 8 * (size_t)V, cudaMemcpyDeviceToHost, ctx->stream),
+                "losses D2H");
   tr->kernels_per_step = (uint32_t)(ctx->launches - launches0);
   return SC_OK;
 }
@@ -543,6 +570,10 @@ void sc_trainer_free(sc_ctx* ctx, sc_trainer* tr) {
     if (tr->bwd_stream[v]) cudaStreamDestroy(tr->bwd_stream[v]);
   }
   cudaFree(tr->scratch);
+  for (uint32_t v = 0; v < SC_MAX_VIEWS; ++v) cudaFree(tr->scene[v].grads);
+  cudaFree(tr->d_scenes);
+  if (tr->h_scenes) cudaFreeHost(tr->h_scenes);
+  if (tr->h_losses) cudaFreeHost(tr->h_losses);
   if (tr->h_params) cudaFreeHost(tr->h_params);
   if (tr->h_out) cudaFreeHost(tr->h_out);
   for (int i = 0; i <= kStages; ++i)
@@ -599,12 +630,16 @@ sc_status sc_trainer_set_profiling(sc_trainer* tr, int enabled) {
 // parameters already in pinned memory: graph capture/replay, capacity retry.
 static sc_status run_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, float* acc, double* loss_out) {
   sc_ctx* ctx = tr->ctx;
-  SC_TRY(ensure_splat_arrays(tr, s->cap));
+  // many scenes: the table (stores, counts, rows) is copied by the step's first
+  // node, so the graph depends only on the capacities that size its grids
+  SC_TRY(ensure_splat_arrays(tr, tr->scenes_mode ? tr->scene_max_cap : s->cap));
   for (int attempt = 0; attempt < 4; ++attempt) {
     const bool sizing = tr->kcap == 0 || (tr->two_level && tr->icap == 0);
     const void* mkey = mo ? (mo->m ? (const void*)mo->m : (const void*)mo->m16) : nullptr;
-    const void* key[8] = {s->slab, s->rest16, mkey, acc, tr->targets, tr->scratch, tr->gout, tr->h_targets};
-    const bool key_ok = tr->exec && std::equal(key, key + 8, tr->g_key) && tr->g_key_n == s->n &&
+    const void* key[8] = {s ? s->slab : nullptr, s ? s->rest16 : nullptr, mkey, acc, tr->targets, tr->scratch,
+                          tr->gout, tr->h_targets};
+    const uint64_t key_n = s ? s->n : ((uint64_t)tr->scene_max_cap << 32 | tr->scene_max_gstride);
+    const bool key_ok = tr->exec && std::equal(key, key + 8, tr->g_key) && tr->g_key_n == key_n &&
                         tr->g_key_kcap == tr->kcap && tr->g_key_icap == tr->icap && tr->g_key_grads == tr->grads_mode &&
                         tr->g_key_w == tr->loss_weight && tr->g_key_shards == tr->g_shards &&
                         tr->g_key_shard == tr->g_shard;
@@ -621,7 +656,7 @@ static sc_status run_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, float* a
         cudaGraphDestroy(g);
         if (ce != cudaSuccess) { tr->exec = nullptr; return sc_cuda_fail(ctx, ce, "graph instantiate"); }
         std::copy(key, key + 8, tr->g_key);
-        tr->g_key_n = s->n;
+        tr->g_key_n = key_n;
         tr->g_key_kcap = tr->kcap;
         tr->g_key_icap = tr->icap;
         tr->g_key_grads = tr->grads_mode;
@@ -725,6 +760,144 @@ sc_status sc_trainer_blend_work(const sc_trainer* tr, uint64_t out[4]) {
   if (!tr || !out) return SC_ERR_INVALID_ARG;
   for (int i = 0; i < 4; ++i) out[i] = tr->prof_steps ? tr->work_acc[i] / tr->prof_steps : 0;
   return SC_OK;
+}
+
+}  // extern "C"
+
+// ================================================================ many scenes
+struct sc_scenes_trainer {
+  sc_trainer* tr = nullptr;
+  uint32_t n = 0;
+  bool set[SC_MAX_VIEWS] = {};
+};
+
+extern "C" {
+
+sc_status sc_scenes_trainer_create(sc_ctx* ctx, const sc_scenes_config* cfg, sc_scenes_trainer** out) {
+  if (!ctx || !cfg || !out) return SC_ERR_INVALID_ARG;
+  if (cfg->n_scenes == 0 || cfg->n_scenes > SC_MAX_VIEWS) return sc_fail(ctx, SC_ERR_INVALID_ARG, "n_scenes out of range");
+  sc_train_config tc{};
+  tc.n_views = cfg->n_scenes;
+  tc.tiling = cfg->tiling;
+  tc.adam = cfg->adam;
+  tc.bwd_mode = SC_BWD_EXACT;
+  tc.use_graph = cfg->use_graph;
+  tc.sort_mode = 2;
+  tc.tile_cull = cfg->tile_cull;
+  tc.log_scale_min = cfg->log_scale_min; tc.log_scale_max = cfg->log_scale_max;
+  tc.opacity_logit_max = cfg->opacity_logit_max;
+  tc.fp64_det = cfg->fp64_det;
+  tc.compensated_sums = cfg->compensated_sums;
+  sc_trainer* tr = nullptr;
+  SC_TRY(sc_trainer_create(ctx, &tc, &tr));
+  if (!tr->two_level) {
+    sc_trainer_free(ctx, tr);
+    return sc_fail(ctx, SC_ERR_INVALID_ARG, "too many scenes x super tiles for the 16-bit item keys");
+  }
+  tr->scenes_mode = true;
+  cudaError_t e = cudaMallocHost(&tr->h_scenes, sizeof(SceneDev) * cfg->n_scenes);
+  if (e == cudaSuccess) e = cudaMallocHost(&tr->h_losses, 8 * (size_t)cfg->n_scenes);
+  if (e == cudaSuccess) e = cudaMalloc(&tr->d_scenes, sizeof(SceneDev) * cfg->n_scenes);
+  if (e == cudaSuccess) e = cudaMalloc(&tr->d_host_targets, (size_t)tr->V * tr->P * 3 * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemset(tr->d_host_targets, 0, (size_t)tr->V * tr->P * 3 * sizeof(float));
+  if (e != cudaSuccess) {
+    sc_trainer_free(ctx, tr);
+    return sc_cuda_fail(ctx, e, "scenes trainer alloc");
+  }
+  std::memset(tr->h_scenes, 0, sizeof(SceneDev) * cfg->n_scenes);
+  tr->targets = tr->d_host_targets;  // the scenes' targets, copied in at the tiling's row pitch
+  sc_scenes_trainer* st = new sc_scenes_trainer();
+  st->tr = tr;
+  st->n = cfg->n_scenes;
+  *out = st;
+  return SC_OK;
+}
+
+void sc_scenes_trainer_free(sc_ctx* ctx, sc_scenes_trainer* st) {
+  if (!st) return;
+  sc_trainer_free(ctx, st->tr);
+  delete st;
+}
+
+sc_status sc_scenes_trainer_set_scene(sc_scenes_trainer* st, uint32_t i, sc_splats* s, sc_moments* mo, float* grad_acc,
+                                      uint32_t width, uint32_t height, const float* target) {
+  if (!st || i >= st->n || !s || !mo || !grad_acc || !target) return SC_ERR_INVALID_ARG;
+  sc_trainer* tr = st->tr;
+  sc_ctx* ctx = tr->ctx;
+  if (width == 0 || height == 0 || width > tr->cfg.tiling.width || height > tr->cfg.tiling.height)
+    return sc_fail(ctx, SC_ERR_INVALID_ARG, "a scene's image must fit the trainer's tiling");
+  if (mo->cap < s->cap) return sc_fail(ctx, SC_ERR_INVALID_ARG, "moments smaller than the scene's store");
+  if (s->cap % 8 || mo->cap % 8) return sc_fail(ctx, SC_ERR_INVALID_ARG, "store capacities must be multiples of 8");
+  auto& h = tr->scene[i];
+  const uint32_t gstride = (s->cap + 63u) & ~63u;
+  if (h.gstride != gstride) {
+    SC_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+    cudaFree(h.grads);
+    h.grads = nullptr;
+    SC_CUDA_TRY(ctx, cudaMalloc(&h.grads, (size_t)SC_NROWS * gstride * 4), "scene gradient rows");
+    h.gstride = gstride;
+  }
+  h.s = s; h.mo = mo; h.acc = grad_acc; h.width = width; h.height = height;
+  // the target at the tiling's row pitch (pixels outside the scene's image stay zero and unused)
+  const size_t pitch = (size_t)tr->cfg.tiling.width * 3 * sizeof(float);
+  SC_CUDA_TRY(ctx, cudaMemcpy2DAsync(tr->d_host_targets + (size_t)i * tr->P * 3, pitch, target,
+                                     (size_t)width * 3 * sizeof(float), (size_t)width * 3 * sizeof(float), height,
+                                     cudaMemcpyDeviceToDevice, ctx->stream), "scene target");
+  st->set[i] = true;
+  uint32_t mc = 0, mg = 0;
+  for (uint32_t k = 0; k < st->n; ++k)
+    if (st->set[k]) { mc = std::max(mc, tr->scene[k].s->cap); mg = std::max(mg, tr->scene[k].gstride); }
+  if (mc != tr->scene_max_cap || mg != tr->scene_max_gstride) trainer_drop_graph(tr);
+  tr->scene_max_cap = mc;
+  tr->scene_max_gstride = mg;
+  return SC_OK;
+}
+
+sc_status sc_scenes_trainer_step(sc_scenes_trainer* st, const sc_camera* cams, uint64_t t, double* losses) {
+  if (!st || !cams || t == 0) return SC_ERR_INVALID_ARG;
+  sc_trainer* tr = st->tr;
+  for (uint32_t i = 0; i < st->n; ++i)
+    if (!st->set[i]) return sc_fail(tr->ctx, SC_ERR_INVALID_ARG, "every scene needs sc_scenes_trainer_set_scene first");
+  for (uint32_t i = 0; i < st->n; ++i) {
+    const auto& h = tr->scene[i];
+    if (h.s->cap > tr->scene_max_cap || h.gstride != ((h.s->cap + 63u) & ~63u))
+      return sc_fail(tr->ctx, SC_ERR_INVALID_ARG, "a scene's store changed capacity: set the scene again");
+    if ((uint32_t)cams[i].width != h.width || (uint32_t)cams[i].height != h.height)
+      return sc_fail(tr->ctx, SC_ERR_INVALID_ARG, "a camera's image size differs from its scene's");
+    SceneDev& d = tr->h_scenes[i];
+    d.s = dview(h.s);
+    d.mo = dview(h.mo);
+    d.acc = h.acc;
+    d.grads = h.grads;
+    d.gstride = h.gstride;
+    d.width = h.width;
+    d.height = h.height;
+    d.gscale = 2.0f / ((float)h.width * (float)h.height * 3.0f);  // loss.rs:163-179, one scene's own MSE
+  }
+  std::memcpy(tr->h_params->cams, cams, sizeof(sc_camera) * tr->V);
+  tr->h_params->bc[0] = 1.0f - sc_powi_f32(tr->cfg.adam.beta1, (int)t);
+  tr->h_params->bc[1] = 1.0f - sc_powi_f32(tr->cfg.adam.beta2, (int)t);
+  const uint32_t seed = (uint32_t)t;
+  std::memcpy(&tr->h_params->bc[2], &seed, sizeof(seed));
+  tr->grads_mode = false;
+  tr->loss_weight = 0.0f;
+  tr->gout = nullptr;
+  tr->g_shards = tr->g_shard = 0;
+  SC_TRY(run_step(tr, nullptr, nullptr, nullptr, nullptr));
+  if (losses)
+    for (uint32_t i = 0; i < st->n; ++i)
+      losses[i] = tr->h_losses[i] / (3.0 * (double)tr->scene[i].width * (double)tr->scene[i].height);
+  return SC_OK;
+}
+
+sc_status sc_scenes_trainer_images(const sc_scenes_trainer* st, const float** images) {
+  if (!st) return SC_ERR_INVALID_ARG;
+  return sc_trainer_images(st->tr, images);
+}
+
+sc_status sc_scenes_trainer_stats(const sc_scenes_trainer* st, uint64_t* pairs, uint32_t* n_kernels, uint64_t* items) {
+  if (!st) return SC_ERR_INVALID_ARG;
+  return sc_trainer_stats(st->tr, pairs, n_kernels, nullptr, nullptr, items);
 }
 
 }  // extern "C"
