@@ -682,23 +682,17 @@ def run_views(args, ws, rank, local, pg):
     import torch
 
     import nanotracer_b200 as nt
-    from nanotracer_b200.multiview import CudaViewBackend, ViewParallelTrainer, split_views
+    from nanotracer_b200.multiview import CudaCollectives, CudaViewBackend, ViewParallelTrainer, split_views
+    from nanotracer_b200.nccl import NcclComm
     from nanotracer_b200.train import TrainConfig
-    if pg is None:  # the split path on one GPU: a one-rank group
-        import datetime
-        import socket
-
-        import torch.distributed as dist
-        with socket.socket() as sk:
-            sk.bind(("127.0.0.1", 0))
-            port = sk.getsockname()[1]
-        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        os.environ.setdefault("MASTER_PORT", str(port))
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-        pg = dist
     ctx = nt.CudaCtx(local)
+    # the data plane: NCCL through its C API on the library stream; its unique id
+    # travels over TCP on the port after the launcher's (MASTER_PORT + 1)
+    if ws > 1:
+        comm = NcclComm(rank, ws, ctx.stream, os.environ.get("MASTER_ADDR", "127.0.0.1"),
+                        int(os.environ.get("MASTER_PORT", "29500")) + 1)
+    else:
+        comm = NcclComm(0, 1, ctx.stream)
     scene, tscene, tl, cams_for, render_targets = make_workload(args, 0, ctx)  # one scene on every rank
     V = args.views
     bf16 = args.form == "bf16"
@@ -710,8 +704,8 @@ def run_views(args, ws, rank, local, pg):
     tgt_all = np.zeros((V,) + tgt_local.shape[1:], np.float32)
     tgt_all[views] = tgt_local
     be = CudaViewBackend(ctx, scene, cfg, tgt_all, views)
-    tr = ViewParallelTrainer(be, V)
-    stream = be.ext_stream
+    tr = ViewParallelTrainer(be, V, CudaCollectives(ctx, comm))
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
     cams_steps = [[cams_for(s)[v] for v in views] for s in range(args.warmup + args.steps)]
     clk = ClockSampler(local, raw_copy=os.environ.get("BENCH_CLOCKS_CSV")).start()
     t = 0
@@ -795,7 +789,8 @@ def run_views(args, ws, rank, local, pg):
                        "form": "batched-" + ("bf16" if bf16 else "fp32"), "splats": N, "views_per_iter": V,
                        "views_per_gpu": Vl, "width": args.width, "height": args.height,
                        "l2": "inputs larger than L2 (params, pair lists and images >> 126 MB)",
-                       "parallelism": f"dp{ws} over views (NCCL reduce-scatter + all-gather, ZeRO-1 Adam)"},
+                       "parallelism": f"dp{ws} over views (NCCL reduce-scatter + all-gather through NCCL's C API "
+                                      f"on the library stream, ZeRO-1 Adam)"},
             "roofline": roofline, "cpu_baseline": None, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clocks, "loss": loss,
         }
@@ -803,6 +798,7 @@ def run_views(args, ws, rank, local, pg):
     tr.close()
     del tr, be
     torch.cuda.synchronize(local)
+    comm.close()
     if pg is not None:
         pg.destroy_process_group()
 

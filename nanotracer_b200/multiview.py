@@ -2,8 +2,8 @@
 
 The reference trains on one device: train.rs:155-250 renders an iteration's
 views one after another and steps Adam once.  Here each of R ranks (one
-process per GPU, torch.distributed over NCCL) takes a block of the views and
-the iteration runs ZeRO-1 style, with one exchange in each direction:
+process per GPU) takes a block of the views and the iteration runs ZeRO-1
+style, with one exchange in each direction:
 
   1. every rank renders and back-propagates its views and sums the per-splat
      gradient over them, written shard-major (chunks of `shard` splats, each
@@ -25,9 +25,11 @@ The loss is the mean over all views of the iteration: each rank scales dL/dC
 and its loss by 1/V_total and the losses are summed across ranks.
 
 ViewParallelTrainer holds the sharding arithmetic and the collective sequence;
-the per-rank compute is a backend object.  CudaViewBackend is the product
-backend (the C ABI on this rank's GPU); tests drive the same trainer with a
-CPU backend over gloo.
+the per-rank compute is a backend object and the exchange a collectives
+object over the backend's buffers.  The product pair is CudaViewBackend with
+CudaCollectives: library device buffers, NCCL through its C API (nccl.py) on
+the library context's stream, no other runtime.  Tests drive the same trainer
+with an oracle backend and CPU collectives over gloo.
 """
 from __future__ import annotations
 
@@ -61,8 +63,8 @@ def split_views(total: int, world: int, rank: int) -> list[int]:
 
 
 class ViewBackend(Protocol):
-    """Per-rank compute that ViewParallelTrainer drives (buffers are torch tensors
-    on the backend's device)."""
+    """Per-rank compute that ViewParallelTrainer drives; its buffers are the
+    collectives object's."""
 
     n: int
 
@@ -74,34 +76,45 @@ class ViewBackend(Protocol):
     def unpack_moments(self, gathered, n_shards: int, shard: int) -> None: ...
     def grad_acc(self): ...
     def densify_prune(self, it: int, grad_count: int, do_prune: bool, do_densify: bool) -> None: ...
-    def stream_context(self): ...
+
+
+class Collectives(Protocol):
+    """The exchange of one split iteration over float32 buffers of the
+    backend's kind (all sums); world and rank of this process."""
+
+    world: int
+    rank: int
+
+    def alloc(self, numel: int): ...                      # zero-filled
+    def view(self, buf, offset: int, numel: int): ...     # a window into buf
+    def zero(self, buf) -> None: ...
+    def copy(self, dst, src) -> None: ...                  # same numel
+    def reduce_scatter(self, out, inp) -> None: ...        # inp = world chunks of out.numel
+    def all_gather(self, out, inp) -> None: ...            # out = world chunks of inp.numel
+    def all_reduce_scalar(self, x: float) -> float: ...
 
 
 class ViewParallelTrainer:
-    """The split iteration over a process group (torch.distributed)."""
+    """The split iteration over a collectives object."""
 
-    def __init__(self, backend: ViewBackend, total_views: int, group=None):
-        import torch.distributed as dist
-        self.dist = dist
+    def __init__(self, backend: ViewBackend, total_views: int, coll: Collectives):
         self.be = backend
-        self.group = group
-        self.world = dist.get_world_size(group)
-        self.rank = dist.get_rank(group)
+        self.coll = coll
+        self.world = coll.world
+        self.rank = coll.rank
         self.total_views = total_views
         self.views = split_views(total_views, self.world, self.rank)
         if not self.views:
             raise ValueError(f"rank {self.rank} has no views: {total_views} views over {self.world} ranks")
-        self._bufs: dict[str, object] = {}
+        self._bufs: dict[str, tuple[object, int]] = {}
 
     # -- buffers (reused while the splat count fits)
     def _buf(self, name: str, numel: int):
-        import torch
         b = self._bufs.get(name)
-        if b is None or b.numel() < numel:
-            with self.be.stream_context():  # filled on the stream that uses it
-                b = torch.zeros(numel, dtype=torch.float32, device=self.be.device)
+        if b is None or b[1] < numel:
+            b = (self.coll.alloc(numel), numel)
             self._bufs[name] = b
-        return b[:numel]
+        return self.coll.view(b[0], 0, numel)
 
     def plan(self) -> tuple[int, int, int]:
         """(shard, lo, count) for the current splat count."""
@@ -111,8 +124,7 @@ class ViewParallelTrainer:
 
     def step(self, t: int) -> float:
         """One iteration (Adam step t, 1-based); returns the loss over all views."""
-        import torch
-        dist, R = self.dist, self.world
+        R, coll = self.world, self.coll
         shard, lo, count = self.plan()
         rows = PARAM_ROWS * shard
         grads = self._buf("grads", R * rows)
@@ -120,33 +132,31 @@ class ViewParallelTrainer:
         send = self._buf("send", rows)
         gathered = self._buf("gathered", R * rows)
         loss_local = self.be.step_grads(self.views, 1.0 / self.total_views, R, shard, grads)
-        with self.be.stream_context():
-            dist.reduce_scatter_tensor(chunk, grads, op=dist.ReduceOp.SUM, group=self.group)
-            self.be.adam_shard(chunk, lo, count, shard, t)
-            self.be.pack_params(lo, count, shard, send)
-            dist.all_gather_into_tensor(gathered, send, group=self.group)
-            self.be.unpack_params(gathered, R, shard)
-            loss = torch.tensor([loss_local], dtype=torch.float64, device=self.be.device)
-            dist.all_reduce(loss, op=dist.ReduceOp.SUM, group=self.group)
-        return float(loss.item())
+        coll.reduce_scatter(chunk, grads)
+        self.be.adam_shard(chunk, lo, count, shard, t)
+        self.be.pack_params(lo, count, shard, send)
+        coll.all_gather(gathered, send)
+        self.be.unpack_params(gathered, R, shard)
+        return coll.all_reduce_scalar(loss_local)
 
     def gather_state(self) -> None:
         """Give every rank the full moments and densify statistic (before a densify/prune)."""
-        dist, R = self.dist, self.world
+        R, coll = self.world, self.coll
         shard, lo, count = self.plan()
         send = self._buf("msend", 2 * PARAM_ROWS * shard)
         gathered = self._buf("mgathered", R * 2 * PARAM_ROWS * shard)
         acc = self.be.grad_acc()
         acc_send = self._buf("asend", shard)
         acc_all = self._buf("aall", R * shard)
-        with self.be.stream_context():
-            self.be.pack_moments(lo, count, shard, send)
-            dist.all_gather_into_tensor(gathered, send, group=self.group)
-            self.be.unpack_moments(gathered, R, shard)
-            acc_send.zero_()
-            acc_send[:count].copy_(acc[lo:lo + count])
-            dist.all_gather_into_tensor(acc_all, acc_send, group=self.group)
-            acc[: self.be.n].copy_(acc_all[: self.be.n])
+        self.be.pack_moments(lo, count, shard, send)
+        coll.all_gather(gathered, send)
+        self.be.unpack_moments(gathered, R, shard)
+        coll.zero(acc_send)
+        if count:
+            coll.copy(coll.view(acc_send, 0, count), coll.view(acc, lo, count))
+        coll.all_gather(acc_all, acc_send)
+        if self.be.n:
+            coll.copy(coll.view(acc, 0, self.be.n), coll.view(acc_all, 0, self.be.n))
 
     def maybe_densify(self, it: int, grad_count: int, prune_warmup: int, prune_every: int, densify_warmup: int,
                       densify_every: int) -> bool:
@@ -164,27 +174,82 @@ class ViewParallelTrainer:
 
 
 # ---------------------------------------------------------------- CUDA backend
+class DevBuf:
+    """A float32 window of library device memory (an owner buffer keeps it alive)."""
+
+    def __init__(self, ptr: int, numel: int, owner=None):
+        self.ptr, self.numel, self.owner = int(ptr), int(numel), owner
+
+    @property
+    def cptr(self) -> C.c_void_p:
+        return C.c_void_p(self.ptr)
+
+    @property
+    def nbytes(self) -> int:
+        return 4 * self.numel
+
+
+class CudaCollectives:
+    """Collectives over library device buffers: NCCL (nccl.NcclComm) on the
+    library context's stream, device copies and fills through the C ABI on the
+    same stream, so the exchange is ordered with the kernels."""
+
+    def __init__(self, ctx, comm):
+        self.ctx, self.comm = ctx, comm
+        self.world, self.rank = comm.world, comm.rank
+        self._scalar = self.alloc(2)
+
+    def alloc(self, numel: int) -> DevBuf:
+        from .gpu import DeviceBuffer
+        b = DeviceBuffer(self.ctx, 4 * max(int(numel), 1), "collective")
+        return DevBuf(b.ptr, numel, b)
+
+    def view(self, buf: DevBuf, offset: int, numel: int) -> DevBuf:
+        assert offset + numel <= buf.numel
+        return DevBuf(buf.ptr + 4 * offset, numel, buf)
+
+    def zero(self, buf: DevBuf) -> None:
+        from ._lib import check, lib
+        check(lib().sc_buffer_zero(self.ctx.handle, buf.cptr, buf.nbytes), self.ctx.handle)
+
+    def copy(self, dst: DevBuf, src: DevBuf) -> None:
+        from ._lib import check, lib
+        assert dst.numel == src.numel
+        check(lib().sc_buffer_copy(self.ctx.handle, dst.cptr, src.cptr, dst.nbytes), self.ctx.handle)
+
+    def reduce_scatter(self, out: DevBuf, inp: DevBuf) -> None:
+        assert inp.numel == self.world * out.numel
+        self.comm.reduce_scatter_f32(out.ptr, inp.ptr, out.numel)
+
+    def all_gather(self, out: DevBuf, inp: DevBuf) -> None:
+        assert out.numel == self.world * inp.numel
+        self.comm.all_gather_f32(out.ptr, inp.ptr, inp.numel)
+
+    def all_reduce_scalar(self, x: float) -> float:
+        from ._lib import check, lib
+        v = np.array([x], np.float64)
+        check(lib().sc_buffer_upload(self.ctx.handle, self._scalar.cptr, v.ctypes.data_as(C.c_void_p), 8),
+              self.ctx.handle)
+        self.comm.all_reduce_sum_f64(self._scalar.ptr, 1)
+        check(lib().sc_buffer_readback(self.ctx.handle, v.ctypes.data_as(C.c_void_p), self._scalar.cptr, 8),
+              self.ctx.handle)
+        return float(v[0])
+
+
 class CudaViewBackend:
     """This rank's GPU through the C ABI: a batched sc_trainer for its views, the
-    splat store, moments and densify statistic.  Buffers exchanged with NCCL are
-    torch tensors whose device pointers go to the library; the collectives run
-    on the library context's stream (wrapped as a torch ExternalStream), so they
-    are ordered with the kernels without extra synchronisation."""
+    splat store, moments and densify statistic, all in library memory."""
 
     def __init__(self, ctx, splats, cfg, targets_all: np.ndarray, views: Sequence[int], max_splats: int | None = None):
-        import torch
         from .splat_gpu import AdamMomentBuffers, GpuSplatBuffer
         from .train import Trainer, TrainConfig
-        self.torch = torch
         self.ctx = ctx
-        self.device = torch.device("cuda", ctx.device)
-        torch.cuda.set_device(self.device)
-        self.ext_stream = torch.cuda.ExternalStream(ctx.stream, device=self.device)
         self.cfg = cfg
         cap = max(max_splats or len(splats), len(splats))
         self.g = GpuSplatBuffer.upload(ctx, splats, capacity=cap, bf16_rest=cfg.bf16)
         self.mo = AdamMomentBuffers(ctx, self.g.capacity, bf16=cfg.bf16)
-        self.acc = torch.zeros(self.g.capacity, dtype=torch.float32, device=self.device)
+        self._acc = ctx.storage_buffer_zeroed("grad_acc", 4 * self.g.capacity)
+        self.acc = DevBuf(self._acc.ptr, self.g.capacity, self._acc)
         local = TrainConfig(**{**cfg.__dict__, "n_views": len(views)})
         self.trainer = Trainer(ctx, local)
         tg = np.ascontiguousarray(np.asarray(targets_all, np.float32)[list(views)])
@@ -200,9 +265,6 @@ class CudaViewBackend:
         """This rank's cameras for the next step (its views only)."""
         self._cams = cams
 
-    def stream_context(self):
-        return self.torch.cuda.stream(self.ext_stream)
-
     def _lib(self):
         from ._lib import lib
         return lib()
@@ -211,80 +273,53 @@ class CudaViewBackend:
         from ._lib import check
         check(st, self.ctx.handle)
 
-    @staticmethod
-    def _ptr(t) -> C.c_void_p:
-        return C.c_void_p(t.data_ptr())
-
-    def step_grads(self, views, loss_weight, n_shards, shard, grads) -> float:
+    def step_grads(self, views, loss_weight, n_shards, shard, grads: DevBuf) -> float:
         from .raster import cameras_array
         if self._cams is None or len(self._cams) != len(views):
             raise ValueError("set_cameras() with one camera per local view before step()")
         loss = C.c_double()
-        # the library stream must not run ahead of torch work that produced `grads`' storage
-        self.ext_stream.wait_stream(self.torch.cuda.current_stream(self.device))
         self._check(self._lib().sc_trainer_step_grads(self.trainer.handle, self.g.handle, cameras_array(self._cams),
-                                                      C.c_float(loss_weight), n_shards, shard, self._ptr(grads),
+                                                      C.c_float(loss_weight), n_shards, shard, grads.cptr,
                                                       C.byref(loss)))
         return loss.value
 
-    def adam_shard(self, chunk, lo, count, shard, t) -> None:
+    def adam_shard(self, chunk: DevBuf, lo, count, shard, t) -> None:
         from .adam_gpu import LOG_SCALE_MAX, LOG_SCALE_MIN, OPACITY_LOGIT_MAX, adam_groups
         c = self.cfg
         gr = adam_groups(c.lrs, c.beta1, c.beta2, c.eps)
-        self._check(self._lib().sc_adam_step_shard(self.ctx.handle, self.g.handle, self.mo.handle,
-                                                   self._ptr(self.acc), self._ptr(chunk), lo, count, shard, int(t),
-                                                   C.byref(gr), LOG_SCALE_MIN, LOG_SCALE_MAX, OPACITY_LOGIT_MAX))
+        self._check(self._lib().sc_adam_step_shard(self.ctx.handle, self.g.handle, self.mo.handle, self.acc.cptr,
+                                                   chunk.cptr, lo, count, shard, int(t), C.byref(gr), LOG_SCALE_MIN,
+                                                   LOG_SCALE_MAX, OPACITY_LOGIT_MAX))
 
-    def pack_params(self, lo, count, shard, out) -> None:
-        self._check(self._lib().sc_splats_pack_range(self.ctx.handle, self.g.handle, lo, count, shard, self._ptr(out)))
+    def pack_params(self, lo, count, shard, out: DevBuf) -> None:
+        self._check(self._lib().sc_splats_pack_range(self.ctx.handle, self.g.handle, lo, count, shard, out.cptr))
 
-    def unpack_params(self, gathered, n_shards, shard) -> None:
-        self._check(self._lib().sc_splats_unpack_shards(self.ctx.handle, self.g.handle, self._ptr(gathered),
-                                                        n_shards, shard))
+    def unpack_params(self, gathered: DevBuf, n_shards, shard) -> None:
+        self._check(self._lib().sc_splats_unpack_shards(self.ctx.handle, self.g.handle, gathered.cptr, n_shards,
+                                                        shard))
 
-    def pack_moments(self, lo, count, shard, out) -> None:
-        self._check(self._lib().sc_moments_pack_range(self.ctx.handle, self.mo.handle, lo, count, shard,
-                                                      self._ptr(out)))
+    def pack_moments(self, lo, count, shard, out: DevBuf) -> None:
+        self._check(self._lib().sc_moments_pack_range(self.ctx.handle, self.mo.handle, lo, count, shard, out.cptr))
 
-    def unpack_moments(self, gathered, n_shards, shard) -> None:
-        self._check(self._lib().sc_moments_unpack_shards(self.ctx.handle, self.mo.handle, self.g.n,
-                                                         self._ptr(gathered), n_shards, shard))
+    def unpack_moments(self, gathered: DevBuf, n_shards, shard) -> None:
+        self._check(self._lib().sc_moments_unpack_shards(self.ctx.handle, self.mo.handle, self.g.n, gathered.cptr,
+                                                         n_shards, shard))
 
-    def grad_acc(self):
+    def grad_acc(self) -> DevBuf:
         return self.acc
 
     def densify_prune(self, it, grad_count, do_prune, do_densify) -> None:
         from .adam_gpu import (DENSIFY_GRAD_THRESHOLD, PRUNE_OPACITY_LOGIT, SPLIT_SCALE_THRESHOLD, densify,
                                prune_low_opacity)
-        acc = _TensorBuffer(self.acc)
         if do_prune:
-            prune_low_opacity(self.ctx, self.g, self.mo, acc, PRUNE_OPACITY_LOGIT)
+            prune_low_opacity(self.ctx, self.g, self.mo, self._acc, PRUNE_OPACITY_LOGIT)
         if do_densify:
-            densify(self.ctx, self.g, self.mo, acc, grad_count, DENSIFY_GRAD_THRESHOLD, SPLIT_SCALE_THRESHOLD,
+            densify(self.ctx, self.g, self.mo, self._acc, grad_count, DENSIFY_GRAD_THRESHOLD, SPLIT_SCALE_THRESHOLD,
                     min(self.cfg.max_splats, self.g.capacity), it)
-            with self.stream_context():
-                self.acc.zero_()
+            self._acc.zero()
 
     def images(self) -> np.ndarray:
         return self.trainer.images()
-
-
-class _TensorBuffer:
-    """A torch CUDA tensor seen as a library buffer (the .cptr the wrappers pass)."""
-
-    def __init__(self, t):
-        self.t = t
-
-    @property
-    def cptr(self) -> C.c_void_p:
-        return C.c_void_p(self.t.data_ptr())
-
-    @property
-    def nbytes(self) -> int:
-        return self.t.numel() * self.t.element_size()
-
-    def zero(self) -> None:
-        self.t.zero_()
 
 
 def expected_shards(n: int, world: int) -> list[tuple[int, int]]:

@@ -15,6 +15,7 @@ from oracle import oracle as O
 from nanotracer_b200.adam_gpu import DENSIFY_GRAD_THRESHOLD, PRUNE_OPACITY_LOGIT, SPLIT_SCALE_THRESHOLD
 from nanotracer_b200.multiview import PARAM_ROWS, ViewParallelTrainer
 from nanotracer_b200.scene import FOV_Y, orbit_views, perturbed, random_scene
+from tests.torch_collectives import TorchCollectives
 
 LRS = (1.6e-4, 1e-3, 5e-3, 0.05, 2.5e-3, 1.25e-4)
 WIDTHS = (3, 4, 3, 1, 3, 45)  # parameter groups in row order
@@ -153,7 +154,7 @@ def run_rank(rank, world, port, out_dir, steps, n, V, densify_at):
         O.set_threads(1)
         scene, cams, tl, tgt = problem(n=n, V=V)
         be = OracleViewBackend(scene, cams, tl, tgt, capacity=4 * n)
-        tr = ViewParallelTrainer(be, V)
+        tr = ViewParallelTrainer(be, V, TorchCollectives())
         losses = []
         grad_count = 0
         for t in range(1, steps + 1):
@@ -179,7 +180,7 @@ def run_rank_leaving(rank, world, port, out_dir):
     O.lib()
     scene, cams, tl, tgt = problem(n=200, V=2)
     be = OracleViewBackend(scene, cams, tl, tgt)
-    tr = ViewParallelTrainer(be, 2)
+    tr = ViewParallelTrainer(be, 2, TorchCollectives())
     if rank == 1:
         open(os.path.join(out_dir, "rank1.txt"), "w").write("left")
         sys.exit(0)  # between steps, with no collective in flight

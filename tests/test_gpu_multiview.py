@@ -3,8 +3,8 @@ parameter pack/unpack, checked against the fused single-device step.
 
 Two ranks are emulated on one GPU by running their steps one after the other
 (no kernel waits on another rank); the reduce-scatter is the sum of the two
-shard-major buffers.  The torch.distributed path itself runs as a one-rank
-NCCL group."""
+shard-major buffers.  The product exchange (NCCL through its C API on the
+library stream, multiview.CudaCollectives) runs as a one-rank communicator."""
 import ctypes as C
 import os
 import socket
@@ -120,17 +120,14 @@ def _free_port() -> int:
 
 
 def test_view_parallel_trainer_one_rank_nccl_matches_fused(ctx):
-    import torch.distributed as dist
+    from nanotracer_b200.multiview import CudaCollectives
+    from nanotracer_b200.nccl import NcclComm
     scene, cams, tgt, cfg = _problem(ctx, n=2000)
     want, _, _, want_loss = _fused(ctx, scene, cams, tgt, cfg, steps=2)
-    os.environ["MASTER_ADDR"] = "127.0.0.1"
-    os.environ["MASTER_PORT"] = str(_free_port())
-    import datetime
-    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60),
-                            device_id=torch.device("cuda", 0))
+    comm = NcclComm(0, 1, ctx.stream, "127.0.0.1", _free_port())
     try:
         be = CudaViewBackend(ctx, scene, cfg, tgt, views=list(range(len(cams))))
-        tr = ViewParallelTrainer(be, len(cams))
+        tr = ViewParallelTrainer(be, len(cams), CudaCollectives(ctx, comm))
         be.set_cameras([cams[v] for v in tr.views])
         losses = [tr.step(t) for t in (1, 2)]
         got = be.g.readback().flat()
@@ -138,6 +135,6 @@ def test_view_parallel_trainer_one_rank_nccl_matches_fused(ctx):
         assert np.array_equal(be.g.readback().flat(), got)
         tr.close()
     finally:
-        dist.destroy_process_group()
+        comm.close()
     assert np.allclose(losses, want_loss, rtol=1e-6)
     assert np.mean(np.abs(got - want) <= 1e-6 + 1e-6 * np.abs(want)) > 0.995

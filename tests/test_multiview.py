@@ -112,3 +112,46 @@ def test_a_rank_that_leaves_makes_the_others_fail_not_hang(tmp_path):
     assert (tmp_path / "rank1.txt").read_text() == "left"
     outcome, secs = (tmp_path / "rank0.txt").read_text().split()
     assert outcome.startswith("error:") and float(secs) < 60
+
+
+def test_multiview_data_plane_imports_no_torch():
+    """The product exchange (multiview + nccl) is the C ABI and NCCL's C API
+    only: importing it loads no torch."""
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    code = ("import sys; sys.path.insert(0, %r); import nanotracer_b200.multiview, nanotracer_b200.nccl; "
+            "print('torch' in sys.modules)" % str(root))
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, check=True)
+    assert out.stdout.strip() == "False"
+
+
+def _rendezvous_rank(rank, world, port, q):
+    from nanotracer_b200.nccl import rendezvous_bytes
+    payload = bytes(range(128)) if rank == 0 else None
+    q.put((rank, rendezvous_bytes(payload, rank, world, "127.0.0.1", port, timeout=20.0)))
+
+
+def test_unique_id_rendezvous_reaches_every_rank():
+    """The NCCL unique id's TCP rendezvous: rank 0's 128 bytes reach every rank."""
+    import multiprocessing as pmp
+    ctx = pmp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_rendezvous_rank, args=(r, 3, port, q)) for r in range(3)]
+    for p in ps:
+        p.start()
+    got = dict(q.get(timeout=60) for _ in ps)
+    for p in ps:
+        p.join(timeout=30)
+    assert all(got[r] == bytes(range(128)) for r in range(3))
+
+
+def test_rendezvous_without_rank0_errors_instead_of_hanging():
+    from nanotracer_b200.nccl import NcclError, rendezvous_bytes
+    import time
+    t0 = time.time()
+    with pytest.raises(NcclError):
+        rendezvous_bytes(None, 1, 2, "127.0.0.1", _free_port(), timeout=1.0)
+    assert time.time() - t0 < 10

@@ -59,3 +59,16 @@ def test_noalloc_scan_rejects_sizes_beyond_its_scratch(ctx):
     assert st == 1  # SC_ERR_INVALID_ARG
     assert b"SC_NOALLOC_SCAN_MAX_N" in lib().sc_last_error(ctx.handle)
     assert np.array_equal(buf.readback(np.uint32), x)  # data untouched
+
+
+def test_noalloc_scan_after_a_timed_out_wait(ctx):
+    """A look-back wait that gave up (the failure self-test) leaves the
+    context usable; the next allocation-free scan clears the scratch it uses
+    and matches the allocating scan."""
+    from nanotracer_b200._lib import lib
+    _bind()
+    assert lib().sc_selftest_wait_timeout(ctx.handle) == 5  # SC_ERR_TIMEOUT
+    x = np.random.default_rng(7).integers(0, 1000, 3_000_017).astype(np.uint32)
+    want, want_total = _scan(ctx, "sc_exclusive_scan_u32", x)
+    got, got_total = _scan(ctx, "sc_exclusive_scan_u32_noalloc", x)
+    assert np.array_equal(got, want) and got_total == want_total
