@@ -486,7 +486,7 @@ def run_ours(args):
 
 
 def run_precision(args):
-    """BASELINE config 4 (the precision form), a side line beside the headline:
+    """The precision form, a side line beside the headline:
     3M splats, 4 views of 1920x1080 per iteration, SH-rest and Adam moments in
     BF16, blending and gradient sums in FP32, with and without the compensated
     cross-tile gradient sums.  Reports each variant's iterations/s, the
@@ -509,7 +509,7 @@ def run_precision(args):
     cams0 = cams_for(0)
     tgt0 = render_targets(ctx, tscene, cams0, tl)
     tbuf = ctx.storage_buffer("targets", tgt0)
-    out = {"metric": "config 4 precision form: iters/s and error against the FP64 oracle", "unit": UNIT,
+    out = {"metric": "precision form, 3M splats x 4 views of 1080p: iters/s and error against the FP64 oracle", "unit": UNIT,
            "config": {"workload": f"{len(scene)} splats, {V} views x {W}x{H} per iteration, BF16 SH-rest + Adam "
                                   f"moments, FP32 blend and gradient sums", "crop": f"64x64 at ({CROP[0]}, "
                                   f"{CROP[1]}) of every view"}}
@@ -581,7 +581,7 @@ def run_precision(args):
 
 
 def run_scenes(args):
-    """BASELINE config 5 (uneven batch), a side line beside the headline: 16
+    """An uneven batch of scenes, a side line beside the headline: 16
     independent scenes with splat counts log-uniform in [10k, 500k] and image
     sizes drawn from {512x512, 1024x768, 1920x1080}, one view each per
     iteration, stepped by one many-scene trainer (every stage one launch over
@@ -661,7 +661,7 @@ def run_scenes(args):
         if any(ev.values()):
             sched.append({"iter": it, **ev, "total": sum(s.splats.n for s in st.scenes)})
     sched_s = time.perf_counter() - w0
-    line = {"metric": "config 5 uneven batch: 16 scenes per iteration, one launch per stage", "unit": UNIT,
+    line = {"metric": "uneven batch: 16 scenes per iteration, one launch per stage", "unit": UNIT,
             "value": 1e3 / ms_one, "ms_per_iter": round(ms_one, 4), "steps": args.steps,
             "separate_trainers_ms_per_iter": round(ms_sep, 4),
             "speedup_over_separate_trainers": round(ms_sep / ms_one, 3),
@@ -911,15 +911,15 @@ def main():
                     help="skip the other forms' side runs (batched other precision, plain FP32) and their PSNR")
     ap.add_argument("--no-psnr", action="store_true", help=argparse.SUPPRESS)  # older name of --no-forms
     ap.add_argument("--workload", default="batched", choices=["batched", "precision", "scenes"],
-                    help="precision: the config-4 side line (3M splats, 4 views, BF16, FP64-oracle errors); "
-                         "scenes: the config-5 side line (16 uneven scenes in one launch per stage)")
+                    help="precision: the precision-form side line (3M splats, 4 views, BF16, FP64-oracle errors); "
+                         "scenes: the uneven-batch side line (16 uneven scenes in one launch per stage)")
     args = ap.parse_args()
     args.no_forms = args.no_forms or args.no_psnr
     if args.workload == "scenes":
         run_scenes(args)
         return
     if args.workload == "precision":
-        if args.splats == 1_000_000 and args.views == 8:  # config 4's sizes unless given
+        if args.splats == 1_000_000 and args.views == 8:  # 3M splats x 4 views unless given
             args.splats, args.views = 3_000_000, 4
         run_precision(args)
         return

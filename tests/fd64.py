@@ -1,5 +1,5 @@
 """Central finite differences in FP64 against the hand-written adjoint
-(BASELINE config 5's check): 64 random parameters of a 1000-splat scene at
+(the uneven-batch workload's adjoint check): 64 random parameters of a 1000-splat scene at
 64x64, h = 1e-3, MSE loss against a target rendered from a perturbed copy.
 
 The loss is the oracle's FP64 instantiation end to end (projection, 64-bit

@@ -1,5 +1,5 @@
-"""The device adjoint against FP64 central differences (BASELINE config 5's
-check): 64 random parameters of a 1000-splat 64x64 scene, h = 1e-3, the
+"""The device adjoint against FP64 central differences (the uneven-batch
+workload's adjoint check): 64 random parameters of a 1000-splat 64x64 scene, h = 1e-3, the
 gradient from the CUDA kernels (exact backward), the difference quotients
 from the oracle's FP64 loss (tests/fd64.py states the bounds and the counted
 exceptions)."""

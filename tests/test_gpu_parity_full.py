@@ -1,10 +1,10 @@
 """Parity with the oracle at the benchmark configurations' full sizes
 (tests/parity.py states the checks and their tolerances).
 
-  config 3 view: BASELINE config 3's scene (1M splats, 1920x1080, 16x16
+  1M at 1080p: the benchmark's scene (1M splats, 1920x1080, 16x16
     tiles) seen from the first of its 8 orbit views (about 1.8e7 (tile, splat)
     pairs), one iteration stage by stage and through the captured step;
-  config 2: 200k splats at 1024x1024, the same for its first iteration, then
+  200k at 1024x1024: 200k splats at 1024x1024, the same for its first iteration, then
     3 iterations of its orbit (3 degrees per iteration) against the oracle's.
 
 The oracle runs on all host cores (its float atomics then vary the gradient
@@ -24,8 +24,8 @@ pytestmark = pytest.mark.gpu
 
 CONFIGS = {
     # name: (splats, width, height, orbit views, seed)
-    "config3_view0": (1_000_000, 1920, 1080, 8, 5),
-    "config2_step0": (200_000, 1024, 1024, 1, 2),
+    "1M_1080p_view0": (1_000_000, 1920, 1080, 8, 5),
+    "200k_1024_step0": (200_000, 1024, 1024, 1, 2),
 }
 
 
@@ -45,8 +45,8 @@ def test_full_size_iteration_parity(ctx, all_cores, name):
     print(report)
 
 
-def test_config2_orbit_iterations_track_the_oracle(ctx, all_cores):
-    """Config 2's run (200k splats, 1024x1024, the camera advancing 3 degrees
+def test_200k_orbit_iterations_track_the_oracle(ctx, all_cores):
+    """The 200k-splat run (200k splats, 1024x1024, the camera advancing 3 degrees
     per iteration), 3 iterations from the same start: each iteration's loss
     within 1e-4 relative of the oracle's f32 iteration, and the trained
     parameters rendered by both within 1e-4 on all but near-threshold pixels
@@ -81,5 +81,5 @@ def test_config2_orbit_iterations_track_the_oracle(ctx, all_cores):
     gimg, _ = pipe.composite()
     oimg, _, _ = oracle.composite(grec, gpay, granges.reshape(-1), otl)
     margin, _, _ = margins(oracle, grec, gpay, granges, otl, 1)
-    s = check_image_explained(gimg[0], oimg, margin, label="config2 after 3 iterations")
+    s = check_image_explained(gimg[0], oimg, margin, label="200k after 3 iterations")
     print({"losses": losses, "image": s})

@@ -160,7 +160,7 @@ def test_trainer_fp64_det_renders_what_the_fp64_projection_renders(ctx):
 
 
 def _scene_with_backdrop(n, n_big, seed):
-    """config-1-like splats plus n_big large splats behind them whose
+    """small-scene-like splats plus n_big large splats behind them whose
     footprints cover most of a 1080p view: their gradient totals add one term
     per tile over thousands of tiles."""
     from nanotracer_b200.scene import random_scene

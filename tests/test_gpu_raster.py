@@ -22,7 +22,7 @@ from nanotracer_b200 import CameraUniform, GpuSplatBuffer, PrefixScan, RadixSort
 from nanotracer_b200._lib import SC_BWD_EXACT, SC_BWD_REF, SC_KEYS_NATIVE64, SC_KEYS_REF32
 from nanotracer_b200.scene import FOV_Y, orbit_pose, orbit_views, random_scene
 
-from tests.util import GpuPipe, check_image_explained, check_param_grads, check_pg_explained, config1, margins
+from tests.util import GpuPipe, check_image_explained, check_param_grads, check_pg_explained, margins, small_scene
 
 pytestmark = pytest.mark.gpu
 KATS = json.loads((Path(__file__).parent / "golden" / "reference_kats.json").read_text())
@@ -62,8 +62,8 @@ def test_wgsl_matches_cpu_oracle_unit_splat(ctx, oracle):
 
 
 @pytest.mark.parametrize("n_views", [1, 3])
-def test_projection_parity_config1(ctx, oracle, n_views):
-    scene, _, tl = config1()
+def test_projection_parity_small_scene(ctx, oracle, n_views):
+    scene, _, tl = small_scene()
     cams = [CameraUniform.from_pose(*p, FOV_Y, tl.width, tl.height, len(scene)) for p in orbit_views(n_views, 5)]
     pipe = GpuPipe(ctx, scene, cams, tl)
     gpu = pipe.project()
@@ -86,9 +86,9 @@ def test_projection_parity_config1(ctx, oracle, n_views):
 
 
 def test_projection_against_fp64_oracle(ctx, oracle):
-    """The f32 GPU projection of ordinary (config-1) splats against the FP64
+    """The f32 GPU projection of ordinary (small-scene) splats against the FP64
     oracle: the error statement of the default f32 arithmetic."""
-    scene, cam, tl = config1(2000)
+    scene, cam, tl = small_scene(2000)
     pipe = GpuPipe(ctx, scene, cam, tl)
     g = pipe.project()[0]
     o = oracle.project(_osplats(oracle, scene), _ocam(oracle, cam), "f64")
@@ -170,7 +170,7 @@ def test_empty_scene_bins_and_composite(ctx):
 @pytest.mark.parametrize("key_mode", [SC_KEYS_REF32, SC_KEYS_NATIVE64])
 @pytest.mark.parametrize("tile", [(16, 16), (8, 8), (32, 8)])
 def test_bins_bit_exact_vs_oracle(ctx, oracle, key_mode, tile):
-    scene, cam, tl0 = config1()
+    scene, cam, tl0 = small_scene()
     tl = TilingParams(tl0.width, tl0.height, tile[0], tl0.depth_max, tile_h_override=tile[1])
     pipe = GpuPipe(ctx, scene, cam, tl, key_mode=key_mode)
     rec = pipe.project()[0]
@@ -187,7 +187,7 @@ def test_bins_bit_exact_vs_oracle(ctx, oracle, key_mode, tile):
 
 
 def test_bins_multiview_native64_vs_oracle(ctx, oracle):
-    scene, _, tl = config1(3000)
+    scene, _, tl = small_scene(3000)
     cams = [CameraUniform.from_pose(*p, FOV_Y, tl.width, tl.height, len(scene)) for p in orbit_views(4, 2)]
     pipe = GpuPipe(ctx, scene, cams, tl, key_mode=SC_KEYS_NATIVE64)
     rec = pipe.project()  # (V, n, 12)
@@ -310,8 +310,8 @@ def test_backward_accumulates_per_splat_gradients(ctx, mode):
 
 
 @pytest.mark.parametrize("tile", [(16, 16), (8, 8), (32, 8)])
-def test_composite_parity_config1(ctx, oracle, tile):
-    scene, cam, tl0 = config1()
+def test_composite_parity_small_scene(ctx, oracle, tile):
+    scene, cam, tl0 = small_scene()
     tl = TilingParams(tl0.width, tl0.height, tile[0], tl0.depth_max, tile_h_override=tile[1])
     pipe = GpuPipe(ctx, scene, cam, tl)
     rec = pipe.project()[0]
@@ -344,8 +344,8 @@ def test_mse_loss_grad_vs_oracle(ctx, oracle):
 
 
 @pytest.mark.parametrize("mode", [SC_BWD_REF, SC_BWD_EXACT])
-def test_composite_backward_parity_config1(ctx, oracle, mode):
-    scene, cam, tl = config1()
+def test_composite_backward_parity_small_scene(ctx, oracle, mode):
+    scene, cam, tl = small_scene()
     pipe = GpuPipe(ctx, scene, cam, tl)
     rec = pipe.project()[0]
     _, pay, ranges = pipe.bin()
@@ -358,13 +358,13 @@ def test_composite_backward_parity_config1(ctx, oracle, mode):
                                            mode, aux[0, ..., 1].reshape(-1),
                                            aux[0, ..., 0].view(np.float32).reshape(-1), want_abs=True)
     _, flags, _ = margins(oracle, rec, pay, ranges, _otl(oracle, tl), mode)
-    print(check_pg_explained(gpu, ora, absum, flags, label=f"config1 mode {mode}"))
+    print(check_pg_explained(gpu, ora, absum, flags, label=f"small scene mode {mode}"))
     assert np.all(gpu[:, [3, 7, 11]] == 0)
 
 
-def test_project_backward_parity_config1(ctx, oracle):
+def test_project_backward_parity_small_scene(ctx, oracle):
     from nanotracer_b200 import GradSplatBuffers
-    scene, cam, tl = config1()
+    scene, cam, tl = small_scene()
     pipe = GpuPipe(ctx, scene, cam, tl)
     pipe.project()
     pipe.bin()

@@ -375,7 +375,7 @@ def test_combined_gradient_is_lambda_weighted_sum(oracle):
 
 
 def test_fp64_adjoint_matches_central_differences_on_64_random_parameters(oracle):
-    """BASELINE config 5's adjoint check on the oracle's FP64 instantiation:
+    """The adjoint check on the oracle's FP64 instantiation:
     central differences (h = 1e-3, FP64 loss) on 64 random parameters of a
     1000-splat 64x64 scene, rotations included (tests/fd64.py states the
     bounds and the counted exceptions)."""

@@ -19,7 +19,7 @@ def records_to_array(raw: np.ndarray) -> np.ndarray:
     return np.ascontiguousarray(raw.view(np.float32).reshape(-1, 12))
 
 
-def config1(n=5000, width=256, height=256, seed=0x5EED5EED):
+def small_scene(n=5000, width=256, height=256, seed=0x5EED5EED):
     scene = random_scene(n, seed)
     eye, tgt, up = orbit_pose(0.0)
     cam = CameraUniform.from_pose(eye, tgt, up, FOV_Y, width, height, n)
