@@ -225,12 +225,25 @@ __global__ void __launch_bounds__(128, 8) k_project(DSplats s_all, const sc_came
           dx /= len; dy /= len; dz /= len;
           float b[15];
           sh_basis15(dx, dy, dz, b);
+          // the storage form decided once for the 45 loads (sp_row tests it per load)
           float ar = 0.f, ag = 0.f, ab = 0.f;
+          const size_t pitch = s.cap;
+          if (s.bf16) {
+            const __nv_bfloat16* p = s.rest16 + i;
 #pragma unroll
-          for (int k = 0; k < 15; ++k) {
-            ar += sp_row(s, SC_ROW_REST + k, i) * b[k];
-            ag += sp_row(s, SC_ROW_REST + 15 + k, i) * b[k];
-            ab += sp_row(s, SC_ROW_REST + 30 + k, i) * b[k];
+            for (int k = 0; k < 15; ++k) {
+              ar += __bfloat162float(p[(size_t)k * pitch]) * b[k];
+              ag += __bfloat162float(p[(size_t)(15 + k) * pitch]) * b[k];
+              ab += __bfloat162float(p[(size_t)(30 + k) * pitch]) * b[k];
+            }
+          } else {
+            const float* p = s.slab + (size_t)SC_ROW_REST * pitch + i;
+#pragma unroll
+            for (int k = 0; k < 15; ++k) {
+              ar += p[(size_t)k * pitch] * b[k];
+              ag += p[(size_t)(15 + k) * pitch] * b[k];
+              ab += p[(size_t)(30 + k) * pitch] * b[k];
+            }
           }
           const float cr = fmaxf(SH_C0 * d0 + ar + 0.5f, 0.0f);
           const float cg = fmaxf(SH_C0 * d1 + ag + 0.5f, 0.0f);
@@ -244,8 +257,11 @@ __global__ void __launch_bounds__(128, 8) k_project(DSplats s_all, const sc_came
               const CullShape cs = cull_shape(mx, my, g.ca, g.cb, g.cc, opacity);
               const bool test = ta.cull && !cs.keep;
               if (ta.super) {
-                for_each_super_span(cs, test, x0, y0, x1, y1, ta.tw, ta.th,
-                                    [&](int, int sx0, int sx1, const int*, const int*) { cnt += (uint32_t)(sx1 - sx0 + 1); });
+                for (int sy = y0 / SC_SUPER; sy <= y1 / SC_SUPER; ++sy) {
+                  int sx0, sx1;
+                  if (super_row_hull(cs, test, sy, x0, y0, x1, y1, ta.tw, ta.th, sx0, sx1))
+                    cnt += (uint32_t)(sx1 - sx0 + 1);
+                }
               } else if (!test) {
                 cnt = (uint32_t)(x1 - x0 + 1) * (uint32_t)(y1 - y0 + 1);
               } else {

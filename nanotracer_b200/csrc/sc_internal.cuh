@@ -191,17 +191,55 @@ __device__ __forceinline__ bool splat_row_span(const CullShape& cs, bool test, i
   return hi >= lo;
 }
 
-// Two-level binning: super tiles of SC_SUPER x SC_SUPER tiles.  A splat emits
-// one item per super tile that the hull of its row spans reaches, super row by
-// super row (the hull of the spans of the super row's tile rows).  f gets the
-// super row, the hull's super columns and the spans of the super row's tile
-// rows (row c of the super row: tiles [lo[c], hi[c]], empty when lo > hi).
+// Two-level binning: super tiles of SC_SUPER x SC_SUPER tiles.
 #define SC_SUPER 4
+
+// The super columns [sx0, sx1] a splat emits items for in super row sy: the
+// tiles that the ellipse can reach anywhere in the pixel-centre band from the
+// first to the last of the super row's tile rows inside the splat's 3-sigma
+// rectangle [x0, x1] x [y0, y1] (with culling; the rectangle's columns
+// without).  One band instead of SC_SUPER tile rows: u_min is convex and u_max
+// concave in w, so over the band their extremes sit at the clamped extreme
+// points, two square roots per super row.  The band holds every tile row's
+// band and the interval is widened by 1e-2 px (the tile rows' test uses
+// 1e-3), so the hull holds every tile-row span that cull_row_span gives for
+// the same rows, whatever the rounding: the member masks, taken from the tile
+// rows, never reach outside it.  Counting (projection) and emission both call
+// this, so they agree on the item count.
+__device__ __forceinline__ bool super_row_hull(const CullShape& s, bool test, int sy, int x0, int y0, int x1, int y1,
+                                               uint32_t tw, uint32_t th, int& sx0, int& sx1) {
+  const int ty0 = max(sy * SC_SUPER, y0), ty1 = min(sy * SC_SUPER + SC_SUPER - 1, y1);
+  if (ty1 < ty0) return false;
+  int lo = x0, hi = x1;
+  if (test) {
+    if (!s.any) return false;
+    const float w0 = (float)(ty0 * (int)th) + 0.5f - s.my, w1 = (float)((ty1 + 1) * (int)th) - 0.5f - s.my;
+    if (w1 < -s.yh || w0 > s.yh) return false;
+    const float a0 = fmaxf(w0, -s.yh), a1 = fminf(w1, s.yh);
+    const float wr = fminf(fmaxf(-s.kx, a0), a1), wl = fminf(fmaxf(s.kx, a0), a1);
+    const float ur = (-s.b * wr + cull_sqrt(fmaxf(s.L * s.a - wr * wr * s.det, 0.0f))) * s.inv_a;
+    const float ul = (-s.b * wl - cull_sqrt(fmaxf(s.L * s.a - wl * wl * s.det, 0.0f))) * s.inv_a;
+    const float X0 = s.mx + ul - 1e-2f, X1 = s.mx + ur + 1e-2f;
+    const float inv_tw = __fdividef(1.0f, (float)tw);
+    lo = max(lo, (int)ceilf((X0 + 0.5f) * inv_tw - 1.0f));
+    hi = min(hi, (int)floorf((X1 - 0.5f) * inv_tw));
+    if (hi < lo) return false;
+  }
+  sx0 = lo / SC_SUPER;
+  sx1 = hi / SC_SUPER;
+  return true;
+}
+
+// A splat's items, super row by super row: f gets the super row, the hull's
+// super columns (super_row_hull) and the spans of the super row's tile rows
+// (row c of the super row: tiles [lo[c], hi[c]], empty when lo > hi), from
+// which each item's member mask is formed.
 template <typename F>
 __device__ __forceinline__ void for_each_super_span(const CullShape& cs, bool test, int x0, int y0, int x1, int y1,
                                                     uint32_t tw, uint32_t th, F&& f) {
   for (int sy = y0 / SC_SUPER; sy <= y1 / SC_SUPER; ++sy) {
-    int slo = INT32_MAX, shi = -1;
+    int sx0, sx1;
+    if (!super_row_hull(cs, test, sy, x0, y0, x1, y1, tw, th, sx0, sx1)) continue;
     int rlo[SC_SUPER], rhi[SC_SUPER];
 #pragma unroll
     for (int c = 0; c < SC_SUPER; ++c) {
@@ -212,11 +250,9 @@ __device__ __forceinline__ void for_each_super_span(const CullShape& cs, bool te
       if (ty >= y0 && ty <= y1 && splat_row_span(cs, test, ty, x0, x1, tw, th, lo, hi)) {
         rlo[c] = lo;
         rhi[c] = hi;
-        slo = min(slo, lo);
-        shi = max(shi, hi);
       }
     }
-    if (shi >= slo) f(sy, slo / SC_SUPER, shi / SC_SUPER, rlo, rhi);
+    f(sy, sx0, sx1, rlo, rhi);
   }
 }
 
