@@ -418,9 +418,9 @@ def run_ours(args):
     algo = {
         # records, zeroed gradient records, depth key, id, item count
         "project": N * (56 + rest_b) + V * N * (48 + 48 + 4 + 4 + 4),
-        # segmented onesweep over u32 depth keys: a histogram read, then 4 passes of 8-bit
-        # digits each reading and writing key + id
-        "depth_sort": V * N * 4 + 4 * V * N * 16,
+        # segmented onesweep over the 16-bit depth keys: a histogram read, then 2 passes
+        # of 8-bit digits each reading and writing key + id
+        "depth_sort": V * N * 4 + 2 * V * N * 16,
         "count_scan": V * N * (4 + 4 + 4) + V * N * 8,
         "emit": V * N * (4 + 16 + 4) + K * 8,
         "tile_sort": K * 4 + tile_passes * K * 16,

@@ -175,8 +175,9 @@ __device__ __forceinline__ bool tile_rect(float mx, float my, float r, float vis
 }
 
 // cull: exact tile culling; super: count two-level binning items (super tiles
-// reached) instead of (tile, splat) pairs
-struct TileArgs { uint32_t tw, th, tiles_x, tiles_y, cull, super; };
+// reached) instead of (tile, splat) pairs; depth_max: the depth quantisation
+// of the reference's 32-bit pair keys
+struct TileArgs { uint32_t tw, th, tiles_x, tiles_y, cull, super; float depth_max; };
 
 // One thread per (splat, view).  Consecutive CTAs take the views of one chunk
 // of splats (view = block % n_views), so the views after the first read the
@@ -207,7 +208,9 @@ __global__ void __launch_bounds__(128, 8) k_project(DSplats s_all, const sc_came
   const float opacity = 1.0f / (1.0f + expf(-op));
   {
     float4 ra = make_float4(0, 0, 0, 0), rb = ra, rc = ra;
-    uint32_t key = 0xFFFFFFFFu, cnt = 0;  // splats that emit no pair sort after every emitting one
+    // a splat that emits no pair sorts last (the sort reads the low 16 bits: it
+    // ties only with splats at or beyond depth_max, and emits nothing)
+    uint32_t key = 0xFFFFFFFFu, cnt = 0;
     if (live) {
       const Cam c = load_cam(cams + v);
       Geo g;
@@ -270,7 +273,14 @@ __global__ void __launch_bounds__(128, 8) k_project(DSplats s_all, const sc_came
                   if (splat_row_span(cs, test, ty, x0, x1, ta.tw, ta.th, lo, hi)) cnt += (uint32_t)(hi - lo + 1);
                 }
               }
-              if (cnt) key = __float_as_uint(g.tz);
+              // the depth presort's key: the reference's 16-bit depth
+              // (tile_emit.wgsl:54-55, the same float operations as the REF32
+              // pair keys), so that a stable sort of the splats in index order
+              // gives each tile the reference's (depth, splat index) order
+              if (cnt) {
+                const float dn = fminf(fmaxf(__fdiv_rn(g.tz, ta.depth_max), 0.0f), 1.0f);
+                key = (uint32_t)(dn * 65535.0f);
+              }
             }
           }
         }
@@ -298,9 +308,10 @@ sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams,
                          float4* rec, const sc_tiling* tl, uint32_t* depth_keys, uint32_t* ids, uint32_t* counts,
                          int precise, int cull, float4* zero_grad, float4* zero_comp, const SceneDev* scenes) {
   if (stride == 0 || n_views == 0) return SC_OK;
-  TileArgs ta{1, 1, 1, 1, 0, 0};
+  TileArgs ta{1, 1, 1, 1, 0, 0, 1.0f};
   if (tl) ta = TileArgs{tl->tile_w, tl->tile_h, (tl->width + tl->tile_w - 1) / tl->tile_w,
-                        (tl->height + tl->tile_h - 1) / tl->tile_h, (cull & 1) ? 1u : 0u, (cull & 2) ? 1u : 0u};
+                        (tl->height + tl->tile_h - 1) / tl->tile_h, (cull & 1) ? 1u : 0u, (cull & 2) ? 1u : 0u,
+                        tl->depth_max};
   const uint32_t bs = 128;  // grid: (splats / bs) x views CTAs, views innermost
   const uint64_t blocks = sc_div_up(stride, bs) * (uint64_t)n_views;
   if (blocks > 0x7FFFFFFFull) return sc_fail(ctx, SC_ERR_INVALID_ARG, "too many splat views for one launch");

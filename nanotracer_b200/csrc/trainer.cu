@@ -3,7 +3,9 @@
 //
 //   H2D step params (cameras, Adam bias corrections)         memcpy node
 //   project + SH for all views, per-view depth keys, counts  k_project
-//   per-view depth sort of the splats                        onesweep u64 (view<<32 | depth bits)
+//   per-view depth sort of the splats                        segmented onesweep u32, 16-bit depth
+//     (the reference's quantised depth: a stable sort in splat order gives each tile the
+//     (depth16, splat index) order of the reference's 32-bit pair keys)
 //   item counts in depth order -> offsets                    gather + decoupled-look-back scan
 //   items (mask | view, super tile; splat) in depth order    k_super_emit (two-level binning)
 //   stable sort of the items by super tile                   onesweep u32 (super tile bits)
@@ -325,7 +327,7 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
                              tr->scenes_mode ? tr->d_scenes : nullptr));
   mark(tr, 1, capturing);
   bool in_tmp = false;
-  SC_TRY(sck::radix_sort_segments(ctx, tr->dkeys, tr->ids, tr->dkeys_tmp, tr->ids_tmp, tr->stride, V, 32, tr->scratch,
+  SC_TRY(sck::radix_sort_segments(ctx, tr->dkeys, tr->ids, tr->dkeys_tmp, tr->ids_tmp, tr->stride, V, 16, tr->scratch,
                                   tr->scratch_bytes, &in_tmp));
   const uint32_t* sorted_ids = in_tmp ? tr->ids_tmp : tr->ids;
   mark(tr, 2, capturing);

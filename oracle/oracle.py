@@ -197,6 +197,28 @@ def bin_ref(rec: np.ndarray, tl: Tiling, sfx="f32"):
     return keys[:K], pay[:K], ranges.reshape(nt, 2)
 
 
+def bin_ref_views(rec: np.ndarray, n_views: int, tl: Tiling, sfx="f32"):
+    """bin_ref for each of n_views views (rec: the views' records one after
+    another), laid out as sc_bin lays out the 32-bit keys of several views:
+    key ((view * tiles + tile) << 16) | depth16, payloads view after view,
+    ranges indexed by view * tiles + tile at positions in the whole array
+    ((0, 0) for an empty tile)."""
+    rec = np.asarray(rec).reshape(n_views, -1, 12)
+    ks, ps, rs, base = [], [], [], 0
+    for v in range(n_views):
+        k, p, r = bin_ref(rec[v], tl, sfx)
+        nt = r.shape[0]
+        assert n_views * nt <= 1 << 16, "view * tiles + tile must fit 16 bits"
+        ks.append(k.astype(np.uint32) + np.uint32((v * nt) << 16))
+        ps.append(p)
+        r = r.astype(np.uint64)
+        full = r[:, 1] > r[:, 0]
+        r[full] += base
+        rs.append(r.astype(np.uint32))
+        base += len(k)
+    return np.concatenate(ks), np.concatenate(ps), np.concatenate(rs)
+
+
 def bin64(rec: np.ndarray, n_views: int, tl: Tiling, sfx="f32"):
     rec = np.ascontiguousarray(rec, _dt(sfx))
     n = rec.shape[0] // n_views

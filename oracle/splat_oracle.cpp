@@ -1178,8 +1178,9 @@ static int64_t read_ply(const char* path, HostSplats* out, uint32_t cap) {
 
 // ---------------------------------------------------------------- whole iteration
 // One training iteration over n_views views (extension of train.rs:155-250 to several views
-// per step with a mean loss): project -> bin64 -> composite -> MSE -> backward -> project
-// backward (summed over views) -> accumulate -> Adam (6 lr groups) -> constraints.
+// per step with a mean loss): project -> bin_ref (the reference's 32-bit keys and order) ->
+// composite -> MSE -> backward -> project backward (summed over views) -> accumulate ->
+// Adam (6 lr groups) -> constraints.
 struct AdamGroups { float lr[6]; float beta1, beta2, eps; };
 
 template <typename T>
@@ -1201,9 +1202,8 @@ static double train_step(HostSplats& s, HostSplats& m, HostSplats& v, float* gra
     // count pairs first to size the key buffers
     uint64_t K = 0;
     for (uint32_t i = 0; i < n; ++i) { TileRect r = tile_rect(rec.data() + 12 * (size_t)i, tl); if (!r.empty) K += (uint64_t)(r.x1 - r.x0 + 1) * (r.y1 - r.y0 + 1); }
-    std::vector<uint64_t> keys(K);
-    std::vector<uint32_t> pay(K), ranges(2 * (size_t)ntiles);
-    bin64<T>(1, n, rec.data(), tl, keys.data(), pay.data(), K, ranges.data());
+    std::vector<uint32_t> keys(K), pay(K), ranges(2 * (size_t)ntiles);
+    bin_ref<T>(n, rec.data(), tl, keys.data(), pay.data(), K, ranges.data());
     composite<T>(rec.data(), pay.data(), ranges.data(), tl, img.data(), ncon.data(), tfin.data());
     loss += combined_loss_grad<T>((int)tl.width, (int)tl.height, img.data(), targets + 3 * P * vi, dl.data(),
                                   ssim_lambda, 1.0f / (float)n_views, nullptr) /

@@ -30,7 +30,7 @@ def problem(n=400, W=64, H=48, V=4, seed=7):
     tg = []
     for c in cams:
         rec = O.project(tgt_scene, c)
-        _, pay, ranges = O.bin64(rec, 1, tl)
+        _, pay, ranges = O.bin_ref(rec, tl)
         img, _, _ = O.composite(rec, pay, ranges, tl)
         tg.append(img[..., :3])
     return scene, cams, tl, np.ascontiguousarray(np.stack(tg), np.float32)
@@ -75,7 +75,7 @@ class OracleViewBackend:
         loss = 0.0
         for vi in views:
             rec = O.project(self.s, self.cams[vi])
-            _, pay, ranges = O.bin64(rec, 1, self.tl)
+            _, pay, ranges = O.bin_ref(rec, self.tl)
             img, ncon, tfin = O.composite(rec, pay, ranges, self.tl)
             lv, dl = O.mse(img, self.targets[vi], scale=loss_weight)
             loss += lv * loss_weight

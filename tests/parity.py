@@ -4,8 +4,9 @@ shared inputs, and through the captured training step (sc_trainer).
   projection   the oracle's f32 projection of the same parameters: same
                visibility, radius within 1 (the ceil of a rounded sqrt), the
                other fields within stated tolerances;
-  bins         keys, splat order and tile ranges from the GPU's records,
-               bit-exact against the oracle's stable (view, tile, depth) sort;
+  bins         32-bit keys (tile << 16 | depth16), splat order and tile
+               ranges from the GPU's records, bit-exact against the oracle's
+               restatement of the reference's binning (stable key sort);
   image        within 1e-4 per pixel of the oracle's blend of the same
                records, every exception a pixel whose walk passes within a
                stated relative margin of a blend threshold (at most 0.1 %);
@@ -25,7 +26,7 @@ import time
 import numpy as np
 
 from nanotracer_b200 import AdamMomentBuffers, GpuSplatBuffer, GradSplatBuffers, TilingParams, TrainConfig, Trainer
-from nanotracer_b200._lib import SC_KEYS_NATIVE64
+from nanotracer_b200._lib import SC_KEYS_REF32
 from nanotracer_b200.scene import perturbed
 from nanotracer_b200.train import BENCH_LRS, render_targets
 
@@ -62,12 +63,12 @@ def iteration_parity(ctx, oracle, scene, cams, tl: TilingParams, mode: int, labe
     os_ = oracle.OSplats.from_buffer(scene)
     report = {"config": label, "mode": mode}
 
-    pipe = GpuPipe(ctx, scene, cams, tl, key_mode=SC_KEYS_NATIVE64)
+    pipe = GpuPipe(ctx, scene, cams, tl, key_mode=SC_KEYS_REF32)
     rec = pipe.project()  # (V, n, 12)
     report["projection"] = [projection_report(rec[v], oracle.project(os_, ocams[v])) for v in range(V)]
 
     keys, pay, ranges = pipe.bin()
-    ok, op, orr = oracle.bin64(rec.reshape(-1, 12), V, otl)
+    ok, op, orr = oracle.bin_ref_views(rec.reshape(-1, 12), V, otl)
     report["pairs"] = int(len(ok))
     assert len(keys) == len(ok) and np.array_equal(keys, ok) and np.array_equal(pay, op)
     assert np.array_equal(ranges, orr)

@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from nanotracer_b200 import AdamMomentBuffers, CameraUniform, GpuSplatBuffer, TilingParams, TrainConfig, Trainer
-from nanotracer_b200._lib import SC_BWD_EXACT, SC_KEYS_NATIVE64
+from nanotracer_b200._lib import SC_BWD_EXACT, SC_KEYS_REF32
 from nanotracer_b200.scene import FOV_Y, orbit_views, perturbed, random_scene
 from nanotracer_b200.train import BENCH_LRS, render_targets
 
@@ -75,7 +75,7 @@ def test_200k_orbit_iterations_track_the_oracle(ctx, all_cores):
         losses.append((gl, ol))
         assert abs(gl - ol) <= 1e-4 * ol, (t, gl, ol)
     # the trained parameters rendered by both, on the GPU's records and bins
-    pipe = GpuPipe(ctx, g.readback(), cam, tl, key_mode=SC_KEYS_NATIVE64)
+    pipe = GpuPipe(ctx, g.readback(), cam, tl, key_mode=SC_KEYS_REF32)
     grec = pipe.project()[0]
     _, gpay, granges = pipe.bin()
     gimg, _ = pipe.composite()

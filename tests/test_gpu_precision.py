@@ -131,7 +131,7 @@ def test_trainer_fp64_det_renders_what_the_fp64_projection_renders(ctx):
     """TrainConfig.fp64_det runs the same FP64 projection inside the captured
     step: its images equal, bit for bit, the stage path's with the context
     option on, and a step with needles moves every parameter to a finite value."""
-    from nanotracer_b200._lib import SC_KEYS_NATIVE64
+    from nanotracer_b200._lib import SC_KEYS_REF32
     from nanotracer_b200.train import render_targets
     from nanotracer_b200.scene import perturbed, orbit_views
     n, W, H, V = 2000, 256, 256, 2
@@ -140,7 +140,7 @@ def test_trainer_fp64_det_renders_what_the_fp64_projection_renders(ctx):
     cams = [CameraUniform.from_pose(*p, FOV_Y, W, H, n) for p in orbit_views(V, 0)]
     ctx.set_fp64_det(True)
     try:
-        pipe = GpuPipe(ctx, s, cams, tl, key_mode=SC_KEYS_NATIVE64)
+        pipe = GpuPipe(ctx, s, cams, tl, key_mode=SC_KEYS_REF32)
         pipe.project()
         pipe.bin()
         ref_img, _ = pipe.composite()

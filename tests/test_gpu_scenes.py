@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from nanotracer_b200 import AdamMomentBuffers, CameraUniform, GpuSplatBuffer, TilingParams, TrainConfig, Trainer
-from nanotracer_b200._lib import SC_KEYS_NATIVE64
+from nanotracer_b200._lib import SC_KEYS_REF32
 from nanotracer_b200.scene import FOV_Y, orbit_views, perturbed, random_scene
 from nanotracer_b200.scenes import Scene, ScenesTrainer, densify_prune_scenes
 from nanotracer_b200.train import BENCH_LRS, render_targets
@@ -70,7 +70,7 @@ def test_scenes_match_the_oracle_scene_by_scene(ctx, oracle):
         ol, _ = oracle.train_step(os_, om, ov, np.zeros(n, np.float32), [oracle.camera_from_struct(bytes(cam.c))],
                                   tgt, otl, 1, BENCH_LRS, 1)
         assert abs(losses[i] - ol) <= 1e-5 * ol, (i, losses[i], ol)
-        pipe = GpuPipe(ctx, s, cam, TilingParams(W, H, 16, 8.0), key_mode=SC_KEYS_NATIVE64)
+        pipe = GpuPipe(ctx, s, cam, TilingParams(W, H, 16, 8.0), key_mode=SC_KEYS_REF32)
         rec = pipe.project()[0]
         _, pay, ranges = pipe.bin()
         oimg, _, _ = oracle.composite(rec, pay, ranges.reshape(-1), otl)

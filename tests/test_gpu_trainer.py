@@ -10,7 +10,7 @@ import pytest
 
 from nanotracer_b200 import (AdamMomentBuffers, CameraUniform, GpuSplatBuffer, GradSplatBuffers, SplatBuffer,
                              TilingParams, TrainConfig, Trainer)
-from nanotracer_b200._lib import SC_BWD_EXACT, SC_BWD_REF, SC_KEYS_NATIVE64
+from nanotracer_b200._lib import SC_BWD_EXACT, SC_BWD_REF, SC_KEYS_REF32
 from nanotracer_b200.scene import FOV_Y, orbit_views, perturbed, random_scene
 from nanotracer_b200.train import BENCH_LRS, render_targets
 
@@ -43,11 +43,12 @@ def _run(ctx, scene, cams, tgt, cfg, steps=1, cap=0):
 
 @pytest.mark.parametrize("tile", [(16, 16), (8, 8), (32, 8)])
 def test_trainer_images_equal_reference_order_binning(ctx, tile):
-    """The trainer's depth-presort + tile-key sort reproduces the 64-bit
-    (tile, depth) key order exactly: its forward images equal, bit for bit,
-    those of sc_bin(NATIVE64) + sc_composite on the same records."""
+    """The trainer's 16-bit depth presort + stable tile sort reproduces the
+    reference's 32-bit (tile << 16 | depth16) key order exactly, ties in the
+    quantised depth going by splat index: its forward images equal, bit for
+    bit, those of sc_bin(REF32) + sc_composite on the same records."""
     scene, tl, cams, tgt, cfg = _setup(ctx, V=3, tile=tile)
-    pipe = GpuPipe(ctx, scene, cams, tl, key_mode=SC_KEYS_NATIVE64)
+    pipe = GpuPipe(ctx, scene, cams, tl, key_mode=SC_KEYS_REF32)
     pipe.project()
     pipe.bin()
     ref_img, _ = pipe.composite()
@@ -230,9 +231,10 @@ def test_full_size_binning_paths_agree(ctx):
     tiles), where the CPU oracle does not finish in seconds, checked through
     properties that hold at any size: the two-level binning and the stable
     pair sort blend the same splats in the same order (images bit for bit, the
-    same pair count and loss), both equal the 64-bit (tile, depth)
-    reference-order binning's images, and the blend work counters stay within
-    each other and the pair count."""
+    same pair count and loss), both equal the images of the reference's own
+    binning (32-bit tile << 16 | depth16 keys, stable sort; 8 views x 8160
+    tiles fit the 16 tile bits), and the blend work counters stay within each
+    other and the pair count."""
     scene, tl, cams, tgt, cfg = _setup(ctx, n=1_000_000, W=1920, H=1080, V=8, seed=5)
     tr2, g2, mo2, acc2, l2 = _run(ctx, scene, cams, tgt, cfg)
     img2 = tr2.images()
@@ -242,7 +244,7 @@ def test_full_size_binning_paths_agree(ctx):
     assert tr1.stats()["pairs"] == pairs2 > 100_000_000
     assert np.allclose(l1, l2, rtol=1e-9)
     del tr1
-    pipe = GpuPipe(ctx, scene, cams, tl, key_mode=SC_KEYS_NATIVE64)
+    pipe = GpuPipe(ctx, scene, cams, tl, key_mode=SC_KEYS_REF32)
     pipe.project()
     pipe.bin()
     ref_img, _ = pipe.composite()
