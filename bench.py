@@ -47,6 +47,47 @@ def profiled_traffic(kernel: str, views: int):
     return None
 
 
+# Arithmetic of one contributing (pixel, entry) pair, counted from the kernels'
+# formulas (scalar FP operations, SFU included): the forward evaluates the
+# Gaussian (offset, quadratic form, exp2, opacity clamp, the two cut tests: 11)
+# and blends (T alpha, three colour FMAs, T update: 6); the backward evaluates
+# the same 11, rebuilds T (1 - alpha, reciprocal, product: 3), forms T alpha,
+# the colour gradient (3), dL/dC . c (3), dL/dalpha (2), the opacity term (1),
+# its moments in y (3) and the running dot GS (1).  With two pixels per packed
+# instruction and 32 lanes, a warp instruction does at most 64 of them.
+PAIR_OPS = {"blend_fwd": 17, "blend_bwd": 29}
+
+
+def profiled_instructions(kernel: str):
+    """Warp instructions per contributing (pixel, entry) pair of a blend kernel
+    from a committed ncu summary (a line `instructions: kernel=<stage> views=<v>
+    warp_inst=<n> pixel_pairs=<p>`: one launch's smsp__inst_executed.sum and the
+    pair counter of the same step), or None."""
+    import re
+    for f in sorted((ROOT / "profiles").glob("*.md")):
+        for m in re.finditer(r"instructions: kernel=(\w+) views=(\d+) warp_inst=(\d+) pixel_pairs=(\d+)",
+                             f.read_text()):
+            if m.group(1) == kernel and int(m.group(4)) > 0:
+                return int(m.group(3)) / int(m.group(4)), f.name
+    return None
+
+
+def issue_roofline(bw: dict) -> dict:
+    """Instruction roofline of the two issue-bound blends: warp instructions
+    per contributing (pixel, entry) pair (profiled) against PAIR_OPS / 64, the
+    pair arithmetic alone at full lanes and full packing."""
+    out = {}
+    for kernel, key in (("blend_fwd", "fwd_pixel_pairs"), ("blend_bwd", "bwd_pixel_pairs")):
+        prof = profiled_instructions(kernel)
+        floor = PAIR_OPS[kernel] / 64.0
+        e = {"pixel_pairs_per_step": bw.get(key), "min_warp_inst_per_pair": round(floor, 4)}
+        if prof:
+            e.update({"warp_inst_per_pair": round(prof[0], 4), "frac": round(floor / prof[0], 4),
+                      "profile": prof[1]})
+        out[kernel] = e
+    return out
+
+
 def load_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -339,11 +380,6 @@ def run_ours(args):
     for s in range(args.warmup):
         t += 1
         tr.step(g, mo, acc, cams0, t)
-    tr.set_profiling(True)
-    for s in range(2):  # graph rebuild with profiling events
-        t += 1
-        tr.step(g, mo, acc, cams0, t)
-    tr.set_profiling(True)  # reset the per-stage accumulators
     torch.cuda.synchronize(local)
     barrier(pg)
     launches0 = ctx.launch_count
@@ -363,8 +399,29 @@ def run_ours(args):
     ms = e0.elapsed_time(e1)
     ms_max = max_over_ranks(pg, ms)
     launches = ctx.launch_count - launches0
-    st = tr.stats()
     clocks = clk.summary(w0, w1)
+    # stage times and blend work counters from further steps with the stage
+    # events and counters on (outside the timed region, which runs without them)
+    tr.set_profiling(True)
+    for s in range(2):  # graph rebuild with profiling events
+        t += 1
+        tr.step(g, mo, acc, cams0, t)
+    tr.set_profiling(True)  # reset the per-stage accumulators
+    for s in range(min(args.steps, 10)):
+        t += 1
+        tr.step(g, mo, acc, cams0, t)
+    st = tr.stats()
+    # the blends' contributing (pixel, entry) pairs: two more steps with the pair counters on
+    tr.set_profiling(2)
+    for s in range(2):
+        t += 1
+        tr.step(g, mo, acc, cams0, t)
+    tr.set_profiling(2)
+    t += 1
+    tr.step(g, mo, acc, cams0, t)
+    for k in ("fwd_pixel_pairs", "bwd_pixel_pairs"):
+        st["blend_work"][k] = tr.stats()["blend_work"][k]
+    tr.set_profiling(True)
     n_steps = t
     forms = None
     if rank == 0 and ws == 1 and not args.no_forms:
@@ -445,7 +502,8 @@ def run_ours(args):
                 "peak_source": peaks["source"], "algorithmic_bytes": int(algo[dom]), "avg_ms": round(dom_ms, 4),
                 "stage_ms": {k: round(v, 4) for k, v in stage.items()}, "blend_work": bw,
                 "stage_frac_of_peak": {k: round(algo[k] / (v / 1e3) / 1e9 / peaks["hbm_gbs"], 4)
-                                       for k, v in stage.items() if k in algo and v > 0}}
+                                       for k, v in stage.items() if k in algo and v > 0},
+                "issue": issue_roofline(bw)}
 
     if forms is not None:
         forms.update(side_forms(ctx, torch, stream, args, scene, tbuf, tgt0, cams0, tl, n_steps, args.form))
@@ -713,12 +771,6 @@ def run_views(args, ws, rank, local, pg):
         t += 1
         be.set_cameras(cams_steps[s])
         tr.step(t)
-    be.trainer.set_profiling(True)
-    for s in range(2):
-        t += 1
-        be.set_cameras(cams_steps[s])
-        tr.step(t)
-    be.trainer.set_profiling(True)
     torch.cuda.synchronize(local)
     barrier(pg)
     launches0 = ctx.launch_count
@@ -737,8 +789,20 @@ def run_views(args, ws, rank, local, pg):
     barrier(pg)
     ms_max = max_over_ranks(pg, e0.elapsed_time(e1))
     launches = ctx.launch_count - launches0
-    st = be.trainer.stats()
     clocks = clk.summary(w0, w1)
+    # stage times from further steps with the stage events on (every rank takes them)
+    be.trainer.set_profiling(True)
+    for s in range(2):  # graph rebuild with profiling events
+        t += 1
+        be.set_cameras(cams_steps[s])
+        tr.step(t)
+    be.trainer.set_profiling(True)  # reset the per-stage accumulators
+    for s in range(min(args.steps, 10)):
+        t += 1
+        be.set_cameras(cams_steps[args.warmup + s])
+        tr.step(t)
+    st = be.trainer.stats()
+    be.trainer.set_profiling(False)
     e2e = None
     if not args.no_e2e:
         pinned = torch.empty(tgt_local.size, dtype=torch.float32, pin_memory=True)

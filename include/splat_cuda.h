@@ -409,13 +409,23 @@ sc_status sc_trainer_images(const sc_trainer* tr, const float** images);
 #define SC_TRAINER_STAGES 9
 sc_status sc_trainer_stats(const sc_trainer* tr, uint64_t* pairs, uint32_t* n_kernels, const char** names,
                            float* avg_ms, uint64_t* items);
-/* Record CUDA events between the stages of each step (also inside the graph). */
+/* Record CUDA events between the stages of each step (also inside the graph)
+ * and count the blends' work (sc_trainer_blend_work) when enabled is 1; 2
+ * also counts contributing (pixel, entry) pairs (sc_trainer_blend_pairs),
+ * which adds a few instructions per entry to the blends; 0 turns it off.
+ * Each call resets the accumulated stage times and counters. */
 sc_status sc_trainer_set_profiling(sc_trainer* tr, int enabled);
 /* Blend work per step, averaged over the steps since profiling was enabled
  * (two-level binning only; zeros otherwise): out[0] list positions the
  * forward's batches covered, out[1] entries it blended, out[2], out[3] the
  * same for the backward.  No counterpart in the reference. */
 sc_status sc_trainer_blend_work(const sc_trainer* tr, uint64_t out[4]);
+/* Contributing (pixel, entry) pairs per step with profiling level 2, averaged
+ * like sc_trainer_blend_work: out[0] pixels that took an entry's alpha in the
+ * forward, out[1] the pixel-entry adjoints the backward formed.  With the
+ * blends' warp instruction counts (from a profiler) they give the
+ * instructions per pair.  No counterpart in the reference. */
+sc_status sc_trainer_blend_pairs(const sc_trainer* tr, uint64_t out[2]);
 
 /* ------------------------------------------------ many scenes in one launch per stage
  * No counterpart in the reference, which trains one scene per train() call

@@ -149,6 +149,7 @@ _PROTOS = {
     "sc_trainer_stats": (ST, [P, C.POINTER(U64), C.POINTER(U32), P, P, C.POINTER(U64)]),
     "sc_trainer_set_profiling": (ST, [P, I32]),
     "sc_trainer_blend_work": (ST, [P, C.POINTER(U64)]),
+    "sc_trainer_blend_pairs": (ST, [P, C.POINTER(U64)]),
     "sc_selftest_wait_timeout": (ST, [P]),
     "sc_scenes_trainer_create": (ST, [P, C.POINTER(sc_scenes_config), C.POINTER(P)]),
     "sc_scenes_trainer_free": (None, [P, P]),

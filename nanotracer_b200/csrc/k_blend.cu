@@ -29,6 +29,7 @@ struct BlendArgs {
   uint64_t pixels;  // per view
   uint32_t batch;   // list positions staged per batch, at most the block's threads
   const SceneDev* scenes;  // per-view image sizes and MSE scales (many-scene steps), or null
+  bool count_pairs;        // with work counters: also count contributing (pixel, entry) pairs
 };
 
 static BlendArgs blend_args(const sc_tiling* tl, uint32_t stride) {
@@ -41,6 +42,7 @@ static BlendArgs blend_args(const sc_tiling* tl, uint32_t stride) {
   a.pixels = (uint64_t)tl->width * tl->height;
   a.batch = 0;
   a.scenes = nullptr;
+  a.count_pairs = false;
   return a;
 }
 
@@ -164,6 +166,17 @@ __device__ __forceinline__ void add_work(unsigned long long* work, uint32_t scan
   }
 }
 
+// With COUNT, a blend launch also counts its contributing (pixel, entry)
+// pairs (a pixel that takes an entry's alpha): the CTA's sum goes to the slot
+// after the BLEND_WORK_SLOTS (scanned, staged) pairs.  Every thread of the CTA
+// calls it; it ends with a barrier, so sred can be reused right after.
+__device__ __forceinline__ void add_pixel_pairs(unsigned long long* work, uint32_t n, double* sred) {
+  const double tot = block_sum((double)n, sred);
+  if (threadIdx.x == 0 && tot > 0.0)
+    atomicAdd(work + 2 * BLEND_WORK_SLOTS + blockIdx.x % BLEND_WORK_SLOTS, (unsigned long long)tot);
+  __syncthreads();
+}
+
 // Pixel placement: thread t owns column t % tw and rows PPT*(t / tw) + k.
 
 // Where a CTA's depth-ordered splat list comes from.  LIST_PAIRS: the tile's
@@ -256,7 +269,7 @@ __device__ __forceinline__ uint32_t place_list(const ListWord& f, uint32_t count
 }
 
 // ---------------------------------------------------------------- forward
-template <int PPT, int LIST>
+template <int PPT, int LIST, bool COUNT>
 __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ rec, ListArgs l, BlendArgs a,
                                                    float4* __restrict__ image, uint2* __restrict__ aux,
                                                    const float* __restrict__ target, float gscale,
@@ -311,7 +324,7 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
   ListWord f = fetch(0);
   uint32_t cnt_next = nb > 0 ? place(0, f) : 0u;
   if (nb > 1) f = fetch(1);
-  uint32_t w_scan = 0, w_staged = 0;
+  uint32_t w_scan = 0, w_staged = 0, w_pix = 0;
   for (uint32_t b = 0; b < nb; ++b) {
     const uint32_t cnt = cnt_next;
     w_scan += min(B, end - (begin + b * B));
@@ -352,6 +365,7 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
             G2 = __ffma2_rn(ta, f2(rc.y), G2);
             B2 = __ffma2_rn(ta, f2(rc.z), B2);
             T2 = __fmul2_rn(T2, __fadd2_rn(f2(1.0f), make_float2(-am.x, -am.y)));
+            if constexpr (COUNT) w_pix += (uint32_t)v0 + (uint32_t)v1;
             if (v0) lk0 = (int)k;
             if (v1) lk1 = (int)k;
             if (T2.x < 1e-4f && T2.y < 1e-4f) break;
@@ -379,6 +393,7 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
                 cg[q] = __fmaf_rn(ta, rc.y, cg[q]);
                 cb[q] = __fmaf_rn(ta, rc.z, cb[q]);
                 T[q] = __fmul_rn(T[q], __fadd_rn(1.0f, -alpha));
+                if constexpr (COUNT) ++w_pix;
                 last[q] = position(b, k) + 1;
                 if (T[q] < 1e-4f) done[q] = true;
               }
@@ -393,6 +408,7 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
   }
   cp_async_wait_all();
   add_work(work, w_scan, w_staged);
+  if constexpr (COUNT) add_pixel_pairs(work, w_pix, sred);
   double sq = 0.0;
 #pragma unroll
   for (int q = 0; q < PPT; ++q) {
@@ -420,9 +436,13 @@ static sc_status composite_ppt(sc_ctx* ctx, const BlendArgs& a, uint32_t grid, u
   const size_t smem = (size_t)2 * 3 * threads * sizeof(float4) + (size_t)2 * threads * sizeof(uint32_t);
   BlendArgs ab = a;
   ab.batch = batch_depth(a.batch, threads);
-  k_composite<PPT, LIST><<<grid, threads, smem, ctx->stream>>>(rec, l, ab, image, aux, target, gscale, dl_dc, loss,
-                                                               d_skip,
-                                                               reinterpret_cast<unsigned long long*>(work));
+  unsigned long long* w = reinterpret_cast<unsigned long long*>(work);
+  if (work && a.count_pairs)
+    k_composite<PPT, LIST, true><<<grid, threads, smem, ctx->stream>>>(rec, l, ab, image, aux, target, gscale, dl_dc,
+                                                                       loss, d_skip, w);
+  else
+    k_composite<PPT, LIST, false><<<grid, threads, smem, ctx->stream>>>(rec, l, ab, image, aux, target, gscale, dl_dc,
+                                                                        loss, d_skip, w);
   return sc_check_launch(ctx, "k_composite");
 }
 
@@ -438,10 +458,11 @@ template <int LIST>
 static sc_status composite_list(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views, const ListArgs& l,
                                 const sc_tiling* tl, float4* image, uint2* aux, const float* target, float mse_scale,
                                 float4* dl_dc, double* loss, const uint32_t* d_skip, uint64_t* work,
-                                uint32_t batch, const SceneDev* scenes) {
+                                uint32_t batch, const SceneDev* scenes, bool count_pairs) {
   BlendArgs a = blend_args(tl, stride);
   a.batch = batch;
   a.scenes = scenes;
+  a.count_pairs = count_pairs;
   const uint32_t pixels = tl->tile_w * tl->tile_h;
   if (pixels > 512 || pixels % 32 != 0) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile must hold 32..512 pixels, multiple of 32");
   const uint64_t grid = (uint64_t)n_views * a.num_tiles;
@@ -462,19 +483,19 @@ sc_status launch_composite(sc_ctx* ctx, const float4* rec, uint32_t stride, uint
                            float mse_scale, float4* dl_dc, double* loss, const uint32_t* d_skip) {
   ListArgs l{payloads, reinterpret_cast<const uint2*>(ranges), nullptr, 0, 0};
   return composite_list<LIST_PAIRS>(ctx, rec, stride, n_views, l, tl, image, aux, target, mse_scale, dl_dc, loss,
-                                    d_skip, nullptr, 0, nullptr);
+                                    d_skip, nullptr, 0, nullptr, false);
 }
 
 sc_status launch_composite_items(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
                                  const uint32_t* item_keys, const uint32_t* item_ids, const uint32_t* item_ranges,
                                  const sc_tiling* tl, float4* image, uint2* aux, const float* target, float mse_scale,
                                  float4* dl_dc, double* loss, const uint32_t* d_skip, uint64_t* work,
-                                 uint32_t batch, const SceneDev* scenes) {
+                                 uint32_t batch, const SceneDev* scenes, bool count_pairs) {
   const BlendArgs a = blend_args(tl, stride);
   ListArgs l{item_ids, reinterpret_cast<const uint2*>(item_ranges), item_keys, (a.tiles_x + SC_SUPER - 1) / SC_SUPER,
              super_tiles_per_view(tl)};
   return composite_list<LIST_ITEMS>(ctx, rec, stride, n_views, l, tl, image, aux, target, mse_scale, dl_dc, loss,
-                                    d_skip, work, batch, scenes);
+                                    d_skip, work, batch, scenes, count_pairs);
 }
 
 // ---------------------------------------------------------------- MSE (standalone)
@@ -584,7 +605,7 @@ __device__ __forceinline__ void twosum_atomic_add4(float4* s, float4* c, float4 
 // here from the forward image instead of being read from dl_dc.
 // COMP: the per-(view, splat) totals across tiles are accumulated with
 // twosum_atomic_add into proj_grad and the compensation records proj_comp.
-template <int PPT, int MODE, int LIST, bool COMP>
+template <int PPT, int MODE, int LIST, bool COMP, bool COUNT>
 __global__ void __launch_bounds__(256) k_composite_backward(const float4* __restrict__ rec, ListArgs l, BlendArgs a,
                                                             const float4* __restrict__ fwd,
                                                             const float4* __restrict__ dl_dc,
@@ -695,7 +716,7 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
   ListWord f = fetch(0);
   uint32_t cnt_next = place(0, f);
   if (nb > 1) f = fetch(1);
-  uint32_t w_staged = 0;
+  uint32_t w_staged = 0, w_pix = 0;
   for (uint32_t b = 0; b < nb; ++b) {
     const uint32_t cnt = cnt_next;
     w_staged += cnt;
@@ -763,6 +784,7 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
                 shxy = shy * e.dx;
                 GS2 = __ffma2_rn(ta, dc, GS2);
                 T2 = make_float2(v0 ? Tn.x : T2.x, v1 ? Tn.y : T2.y);
+                if constexpr (COUNT) w_pix += (uint32_t)v0 + (uint32_t)v1;
                 contrib = true;
               }
             }
@@ -791,6 +813,7 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
                     shxx += hx * e.dx; shxy += hx * dy; shyy += hy * dy;
                     GS[q] += ta * dc;
                     T[q] = Tn;
+                    if constexpr (COUNT) ++w_pix;
                     contrib = true;
                   }
                 }
@@ -858,6 +881,7 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
   }
   cp_async_wait_all();
   add_work(work, hi0 - begin, w_staged);
+  if constexpr (COUNT) add_pixel_pairs(work, w_pix, s_red);
 }
 
 template <int PPT, int LIST, int MODE>
@@ -865,11 +889,18 @@ static void backward_launch(const BlendArgs& a, uint32_t grid, uint32_t threads,
                             const float4* rec, const ListArgs& l, const float4* fwd, const float4* dl_dc,
                             const float* target, float gscale, double* loss, const uint2* aux, float4* proj_grad,
                             const uint32_t* d_skip, unsigned long long* w, float4* proj_comp) {
-  if (proj_comp)
-    k_composite_backward<PPT, MODE, LIST, true><<<grid, threads, smem, st>>>(
+  const bool count = w && a.count_pairs;
+  if (proj_comp && count)
+    k_composite_backward<PPT, MODE, LIST, true, true><<<grid, threads, smem, st>>>(
         rec, l, a, fwd, dl_dc, target, gscale, loss, aux, proj_grad, d_skip, w, proj_comp);
+  else if (proj_comp)
+    k_composite_backward<PPT, MODE, LIST, true, false><<<grid, threads, smem, st>>>(
+        rec, l, a, fwd, dl_dc, target, gscale, loss, aux, proj_grad, d_skip, w, proj_comp);
+  else if (count)
+    k_composite_backward<PPT, MODE, LIST, false, true><<<grid, threads, smem, st>>>(
+        rec, l, a, fwd, dl_dc, target, gscale, loss, aux, proj_grad, d_skip, w, nullptr);
   else
-    k_composite_backward<PPT, MODE, LIST, false><<<grid, threads, smem, st>>>(
+    k_composite_backward<PPT, MODE, LIST, false, false><<<grid, threads, smem, st>>>(
         rec, l, a, fwd, dl_dc, target, gscale, loss, aux, proj_grad, d_skip, w, nullptr);
 }
 
@@ -896,10 +927,11 @@ static sc_status backward_list(sc_ctx* ctx, const float4* rec, uint32_t stride, 
                                const sc_tiling* tl, const float4* fwd, const float4* dl_dc, const float* target,
                                float mse_scale, double* loss, int mode, const uint2* aux, float4* proj_grad,
                                const uint32_t* d_skip, uint64_t* work, float4* proj_comp, uint32_t batch,
-                               const SceneDev* scenes) {
+                               const SceneDev* scenes, bool count_pairs) {
   BlendArgs a = blend_args(tl, stride);
   a.batch = batch;
   a.scenes = scenes;
+  a.count_pairs = count_pairs;
   const float gscale = (2.0f / ((float)tl->width * (float)tl->height * 3.0f)) * mse_scale;
   const uint32_t pixels = tl->tile_w * tl->tile_h;
   if (pixels > 512 || pixels % 32 != 0) return sc_fail(ctx, SC_ERR_INVALID_ARG, "tile must hold 32..512 pixels, multiple of 32");
@@ -922,7 +954,7 @@ sc_status launch_composite_backward(sc_ctx* ctx, const float4* rec, uint32_t str
                                     float mse_scale, double* loss, float4* proj_comp) {
   ListArgs l{payloads, reinterpret_cast<const uint2*>(ranges), nullptr, 0, 0};
   return backward_list<LIST_PAIRS>(ctx, rec, stride, n_views, l, tl, fwd, dl_dc, target, mse_scale, loss, mode, aux,
-                                   proj_grad, d_skip, nullptr, proj_comp, 0, nullptr);
+                                   proj_grad, d_skip, nullptr, proj_comp, 0, nullptr, false);
 }
 
 sc_status launch_composite_backward_items(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
@@ -931,12 +963,12 @@ sc_status launch_composite_backward_items(sc_ctx* ctx, const float4* rec, uint32
                                           const float4* dl_dc, int mode, const uint2* aux, float4* proj_grad,
                                           const uint32_t* d_skip, const float* target, float mse_scale,
                                           double* loss, uint64_t* work, float4* proj_comp, uint32_t batch,
-                                          const SceneDev* scenes) {
+                                          const SceneDev* scenes, bool count_pairs) {
   const BlendArgs a = blend_args(tl, stride);
   ListArgs l{item_ids, reinterpret_cast<const uint2*>(item_ranges), item_keys, (a.tiles_x + SC_SUPER - 1) / SC_SUPER,
              super_tiles_per_view(tl)};
   return backward_list<LIST_ITEMS>(ctx, rec, stride, n_views, l, tl, fwd, dl_dc, target, mse_scale, loss, mode, aux,
-                                   proj_grad, d_skip, work, proj_comp, batch, scenes);
+                                   proj_grad, d_skip, work, proj_comp, batch, scenes, count_pairs);
 }
 
 // proj_grad += proj_comp over n float4 (the compensated totals rounded once)

@@ -519,15 +519,16 @@ sc_status launch_fold_comp(sc_ctx* ctx, float4* proj_grad, const float4* proj_co
 // positions within the super tile's list.  batch: list positions staged per
 // batch (0 = one per thread).  scenes (nullable): view v's pixels are those
 // inside scene v's width x height (the images keep the tiling's row pitch) and
-// its MSE scale is the scene's.  work (nullable, BLEND_WORK_SLOTS
-// (scanned, staged) pairs, accumulated): the list positions the CTAs' batches
-// covered and the entries they staged.
+// its MSE scale is the scene's.  work (nullable, 3 BLEND_WORK_SLOTS u64,
+// accumulated): BLEND_WORK_SLOTS (scanned, staged) pairs — the list positions
+// the CTAs' batches covered and the entries they staged — then, with
+// count_pairs, as many counts of contributing (pixel, entry) pairs.
 constexpr uint32_t BLEND_WORK_SLOTS = 64;
 sc_status launch_composite_items(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
                                  const uint32_t* item_keys, const uint32_t* item_ids, const uint32_t* item_ranges,
                                  const sc_tiling* tl, float4* image, uint2* aux, const float* target, float mse_scale,
                                  float4* dl_dc, double* loss, const uint32_t* d_skip, uint64_t* work = nullptr,
-                                 uint32_t batch = 0, const SceneDev* scenes = nullptr);
+                                 uint32_t batch = 0, const SceneDev* scenes = nullptr, bool count_pairs = false);
 sc_status launch_composite_backward_items(sc_ctx* ctx, const float4* rec, uint32_t stride, uint32_t n_views,
                                           const uint32_t* item_keys, const uint32_t* item_ids,
                                           const uint32_t* item_ranges, const sc_tiling* tl, const float4* fwd,
@@ -535,7 +536,7 @@ sc_status launch_composite_backward_items(sc_ctx* ctx, const float4* rec, uint32
                                           const uint32_t* d_skip, const float* target = nullptr,
                                           float mse_scale = 0.0f, double* loss = nullptr, uint64_t* work = nullptr,
                                           float4* proj_comp = nullptr, uint32_t batch = 0,
-                                          const SceneDev* scenes = nullptr);
+                                          const SceneDev* scenes = nullptr, bool count_pairs = false);
 sc_status launch_tonemap(sc_ctx* ctx, const float4* img, uint32_t w, uint32_t h, uint8_t* out);
 
 // SSIM (loss.rs:22-375): scale * dL_ssim/dC added into dl_dc, per-view sum of

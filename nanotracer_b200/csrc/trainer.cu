@@ -152,15 +152,15 @@ struct sc_trainer {
   // results of the last step
   uint64_t last_pairs = 0, last_items = 0;
   uint32_t kernels_per_step = 0;
-  // profiling
-  bool profiling = false;
+  // profiling: 0 off, 1 stage events + blend work counters, 2 also (pixel, entry) pair counts
+  int profiling = 0;
   cudaEvent_t ev[kStages + 1] = {};
   double acc_ms[kStages] = {};
   uint64_t prof_steps = 0;
   float avg_ms_out[kStages] = {};
   // blend work counters while profiling: forward then backward slots
   uint64_t* d_work = nullptr;
-  uint64_t work_acc[4] = {};
+  uint64_t work_acc[6] = {};  // fwd scanned, staged; bwd scanned, staged; fwd, bwd (pixel, entry) pairs
 };
 
 static void trainer_free_splat_arrays(sc_trainer* tr) {
@@ -316,9 +316,9 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   }
   SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->d_loss, 0, 8 * (size_t)V, ctx->stream), "zero loss");
   uint64_t* work_fwd = tr->profiling ? tr->d_work : nullptr;
-  uint64_t* work_bwd = tr->profiling ? tr->d_work + 2 * sck::BLEND_WORK_SLOTS : nullptr;
+  uint64_t* work_bwd = tr->profiling ? tr->d_work + 3 * sck::BLEND_WORK_SLOTS : nullptr;
   if (tr->profiling)
-    SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->d_work, 0, 4 * sck::BLEND_WORK_SLOTS * 8, ctx->stream), "zero work");
+    SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->d_work, 0, 6 * sck::BLEND_WORK_SLOTS * 8, ctx->stream), "zero work");
   SC_CUDA_TRY(ctx, cudaMemsetAsync(tr->counts + nsp, 0, 4, ctx->stream), "zero count tail");
   mark(tr, 0, capturing);
   SC_TRY(sck::launch_project(ctx, ds, d_cams, V, tr->stride, tr->rec, &tr->cfg.tiling, tr->dkeys, tr->ids,
@@ -400,7 +400,7 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
   if (tr->two_level)
     SC_TRY(sck::launch_composite_items(ctx, tr->rec, tr->stride, V, item_keys, item_ids, tr->iranges, &tr->cfg.tiling,
                                        tr->image, tr->aux, fwd_target, mse_w, tr->dl_dc, tr->d_loss, ctx->d_error,
-                                       work_fwd, tr->cfg.blend_batch, scenes));
+                                       work_fwd, tr->cfg.blend_batch, scenes, tr->profiling >= 2));
   else
     SC_TRY(sck::launch_composite(ctx, tr->rec, tr->stride, V, svals, tr->ranges, &tr->cfg.tiling, tr->image, tr->aux,
                                  fwd_target, mse_w, tr->dl_dc, tr->d_loss, ctx->d_error));
@@ -435,7 +435,7 @@ static sc_status enqueue_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, floa
                                                   (int)tr->cfg.bwd_mode, tr->aux + po,
                                                   tr->pgrad + so, ctx->d_error, tg, mse_w, tr->d_loss + v0, work_bwd,
                                                   tr->pcomp ? tr->pcomp + so : nullptr, tr->cfg.blend_batch,
-                                                  scenes ? scenes + v0 : nullptr));
+                                                  scenes ? scenes + v0 : nullptr, tr->profiling >= 2));
     else
       st = (sck::launch_composite_backward(ctx, tr->rec + so, tr->stride, nv, svals, tr->ranges + (size_t)2 * v0 * tr->T,
                                             &tr->cfg.tiling, tr->image + po, tr->dl_dc ? tr->dl_dc + po : nullptr,
@@ -535,7 +535,7 @@ sc_status sc_trainer_create(sc_ctx* ctx, const sc_train_config* cfg, sc_trainer*
   if (e == cudaSuccess) e = cudaMalloc(&tr->aux, pix * 8);
   if (e == cudaSuccess) e = cudaMalloc(&tr->dl_dc, pix * 16);
   if (e == cudaSuccess) e = cudaMalloc(&tr->d_loss, 8 * (size_t)tr->V);
-  if (e == cudaSuccess) e = cudaMalloc(&tr->d_work, 4 * sck::BLEND_WORK_SLOTS * 8);
+  if (e == cudaSuccess) e = cudaMalloc(&tr->d_work, 6 * sck::BLEND_WORK_SLOTS * 8);
   if (e == cudaSuccess) e = cudaMalloc(&tr->d_total, 64);
   if (e == cudaSuccess) e = cudaMemset(tr->d_total, 0, 64);
   if (e == cudaSuccess && tr->two_level) e = cudaMalloc(&tr->iranges, (size_t)tr->V * tr->ST * 8);
@@ -618,10 +618,11 @@ sc_status sc_trainer_set_host_targets(sc_trainer* tr, const float* pinned_target
 
 sc_status sc_trainer_set_profiling(sc_trainer* tr, int enabled) {
   if (!tr) return SC_ERR_INVALID_ARG;
-  if (tr->profiling != (enabled != 0)) trainer_drop_graph(tr);
-  tr->profiling = enabled != 0;
+  const int level = enabled <= 0 ? 0 : (enabled >= 2 ? 2 : 1);
+  if (tr->profiling != level) trainer_drop_graph(tr);
+  tr->profiling = level;
   for (int i = 0; i < kStages; ++i) tr->acc_ms[i] = 0.0;
-  for (int i = 0; i < 4; ++i) tr->work_acc[i] = 0;
+  for (int i = 0; i < 6; ++i) tr->work_acc[i] = 0;
   tr->prof_steps = 0;
   return SC_OK;
 }
@@ -691,9 +692,16 @@ static sc_status run_step(sc_trainer* tr, sc_splats* s, sc_moments* mo, float* a
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, tr->ev[i], tr->ev[i + 1]) == cudaSuccess) tr->acc_ms[i] += ms;
       }
-      uint64_t w[4 * sck::BLEND_WORK_SLOTS];
+      // per pass (forward, backward): BLEND_WORK_SLOTS (scanned, staged) pairs, then as many pixel-pair counts
+      constexpr uint32_t S = sck::BLEND_WORK_SLOTS;
+      uint64_t w[6 * S];
       SC_CUDA_TRY(ctx, cudaMemcpy(w, tr->d_work, sizeof(w), cudaMemcpyDeviceToHost), "work D2H");
-      for (uint32_t i = 0; i < 4 * sck::BLEND_WORK_SLOTS; ++i) tr->work_acc[(i / (2 * sck::BLEND_WORK_SLOTS)) * 2 + (i & 1)] += w[i];
+      for (uint32_t k = 0; k < 2; ++k)
+        for (uint32_t i = 0; i < S; ++i) {
+          tr->work_acc[2 * k] += w[3 * S * k + 2 * i];
+          tr->work_acc[2 * k + 1] += w[3 * S * k + 2 * i + 1];
+          tr->work_acc[4 + k] += w[3 * S * k + 2 * S + i];
+        }
       tr->prof_steps++;
     }
     if (loss_out) *loss_out = o.loss;
@@ -761,6 +769,12 @@ sc_status sc_trainer_stats(const sc_trainer* tr, uint64_t* pairs, uint32_t* n_ke
 sc_status sc_trainer_blend_work(const sc_trainer* tr, uint64_t out[4]) {
   if (!tr || !out) return SC_ERR_INVALID_ARG;
   for (int i = 0; i < 4; ++i) out[i] = tr->prof_steps ? tr->work_acc[i] / tr->prof_steps : 0;
+  return SC_OK;
+}
+
+sc_status sc_trainer_blend_pairs(const sc_trainer* tr, uint64_t out[2]) {
+  if (!tr || !out) return SC_ERR_INVALID_ARG;
+  for (int i = 0; i < 2; ++i) out[i] = tr->prof_steps ? tr->work_acc[4 + i] / tr->prof_steps : 0;
   return SC_OK;
 }
 

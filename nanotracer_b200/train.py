@@ -95,8 +95,11 @@ class Trainer:
         self._targets = keepalive
         check(lib().sc_trainer_set_host_targets(self.handle, C.c_void_p(pinned_ptr)), self.ctx.handle)
 
-    def set_profiling(self, on: bool) -> None:
-        check(lib().sc_trainer_set_profiling(self.handle, 1 if on else 0), self.ctx.handle)
+    def set_profiling(self, on: bool | int) -> None:
+        """False/0 off; True/1 stage times and blend work; 2 also the blends'
+        (pixel, entry) pair counts.  Each call resets the accumulators."""
+        level = int(on) if not isinstance(on, bool) else (1 if on else 0)
+        check(lib().sc_trainer_set_profiling(self.handle, level), self.ctx.handle)
 
     def step(self, splats: GpuSplatBuffer, moments: AdamMomentBuffers, grad_acc: DeviceBuffer,
              cams: list[CameraUniform], t: int) -> float:
@@ -126,10 +129,12 @@ class Trainer:
               self.ctx.handle)
         work = (C.c_uint64 * 4)()
         check(lib().sc_trainer_blend_work(self.handle, work), self.ctx.handle)
+        px = (C.c_uint64 * 2)()
+        check(lib().sc_trainer_blend_pairs(self.handle, px), self.ctx.handle)
         return {"pairs": pairs.value, "items": items.value, "kernels_per_step": nk.value,
                 "stage_ms": {names[i].decode(): float(ms[i]) for i in range(9)},
                 "blend_work": {"fwd_scanned": work[0], "fwd_blended": work[1], "bwd_scanned": work[2],
-                               "bwd_blended": work[3]}}
+                               "bwd_blended": work[3], "fwd_pixel_pairs": px[0], "bwd_pixel_pairs": px[1]}}
 
     def __del__(self):
         try:

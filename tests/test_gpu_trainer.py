@@ -281,3 +281,29 @@ def test_blend_work_counters_bound_each_other(ctx):
     assert 0 < w["bwd_blended"] <= w["bwd_scanned"] <= w["fwd_scanned"]
     assert w["bwd_blended"] <= w["fwd_blended"] <= st["pairs"]
     tr.set_profiling(False)
+
+
+def test_pixel_pair_counters(ctx):
+    """Profiling level 2 counts the blends' contributing (pixel, entry) pairs:
+    with the exact backward the backward forms an adjoint for exactly the
+    pairs the forward blended, the counts stay within the blended entries
+    times the tile's pixels, level 1 leaves them at zero, and counting changes
+    no image."""
+    scene, tl, cams, tgt, cfg = _setup(ctx, n=6000, V=3)
+    tr = Trainer(ctx, cfg)
+    tr.set_targets(ctx.storage_buffer("targets", np.ascontiguousarray(tgt, np.float32)))
+    out = []
+    for level in (1, 2):
+        g = GpuSplatBuffer.upload(ctx, scene)
+        mo = AdamMomentBuffers(ctx, g.capacity)
+        acc = ctx.storage_buffer_zeroed("acc", 4 * g.capacity)
+        tr.set_profiling(level)
+        tr.step(g, mo, acc, cams, 1)
+        out.append((tr.stats()["blend_work"], tr.images()))
+    (w1, img1), (w2, img2) = out
+    assert w1["fwd_pixel_pairs"] == 0 and w1["bwd_pixel_pairs"] == 0
+    assert np.array_equal(img1, img2)
+    assert w2["fwd_blended"] == w1["fwd_blended"]
+    assert 0 < w2["fwd_pixel_pairs"] == w2["bwd_pixel_pairs"]
+    assert w2["fwd_pixel_pairs"] <= w2["fwd_blended"] * cfg.tile_w * cfg.tile_h
+    tr.set_profiling(False)
