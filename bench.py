@@ -368,7 +368,9 @@ def run_ours(args):
         tune = {"choice": f"{cfg.tile_w}x{cfg.tile_h} tiles, sort_mode {cfg.sort_mode}, blend batch "
                           f"{cfg.blend_batch or 'all threads'}, sort digits {cfg.sort_digit_bits or 'auto'}",
                 "trial_ms": {t.label: (round(t.ms, 3) if t.ms is not None else t.error) for t in trials},
-                "identical_images": len({t.digest for t in trials if t.digest}) == 1}
+                "identical_images_per_tile_shape": all(
+                    len({t.digest for t in trials if t.digest and (t.tile_w, t.tile_h) == s}) <= 1
+                    for s in {(t.tile_w, t.tile_h) for t in trials})}
         tl = nt.TilingParams(args.width, args.height, cfg.tile_w, 8.0, tile_h_override=cfg.tile_h)
     g = nt.GpuSplatBuffer.upload(ctx, scene, bf16_rest=bf16)
     mo = nt.AdamMomentBuffers(ctx, g.capacity, bf16=bf16)

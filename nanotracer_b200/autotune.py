@@ -19,9 +19,16 @@ The search is coordinate-wise: tile shape x binning path first (with the
 default batch and digits), then the batch depth on the best of those, then
 the digit width on the best batch; 11 trials at most instead of 36.
 
-None of the axes changes the images: every pixel blends the same splats in
-the same order whatever the tiles, the list path, the batch or the digits.
-The device test checks that the candidates' first-step images are bit-identical.
+The binning path, the batch depth and the digit width never change the
+images: every pixel blends the same splats in the same order.  The tile shape
+can, as in the reference: a splat is listed in the tiles of its 3-sigma
+rectangle rounded out to whole tiles, and the blend evaluates every pixel of a
+listed tile, so a pixel just beyond 3 sigma (where alpha still passes 1/255
+for opacities near 1) takes the splat in some tilings and not in others (on
+1M splats at 1080p about 1 % of the pixels, by at most 0.015).  Tuning the
+tile shape is choosing the reference's tile_size, a training parameter there;
+pass tiles=[(tile_w, tile_h)] to keep the caller's.  The device test checks
+that candidates with the same tile shape render bit-identical first steps.
 
 The scratch copies mean that tuning leaves the caller's splats, moments and
 trainer untouched; it costs one upload and one trainer per candidate.
