@@ -80,10 +80,28 @@ __device__ __forceinline__ void sh_basis15(float x, float y, float z, float b[15
 }
 
 // rotation matrix (row r, column c) of quaternion (w, x, y, z), project_gaussians.wgsl:68-80
+// In the IEEE geometry (X = true: the forward and sc_project_backward) every
+// rounding step of the rotation and of geometry() below is written out
+// (__fmaf_rn / __fmul_rn / __fadd_rn), so the compiler has no contraction left
+// to choose and the two form bit-identical covariances: they agree on which
+// needle-like splats the f32 determinant test culls.  The trainer's adjoint
+// (X = false) leaves the contraction to the compiler.
+template <bool X> __device__ __forceinline__ float mul_(float a, float b) { return X ? __fmul_rn(a, b) : a * b; }
+template <bool X> __device__ __forceinline__ float fma_(float a, float b, float c) {
+  return X ? __fmaf_rn(a, b, c) : a * b + c;
+}
+template <bool X> __device__ __forceinline__ float sum_sq2(float a, float b) { return fma_<X>(a, a, mul_<X>(b, b)); }
+template <bool X> __device__ __forceinline__ float dot2(float a, float b, float c, float d) {
+  return fma_<X>(a, b, mul_<X>(c, d));
+}
+template <bool X>
 __device__ __forceinline__ void quat_rot(float w, float x, float y, float z, float R[3][3]) {
-  R[0][0] = 1.0f - 2.0f * (y * y + z * z); R[1][0] = 2.0f * (x * y + w * z); R[2][0] = 2.0f * (x * z - w * y);
-  R[0][1] = 2.0f * (x * y - w * z); R[1][1] = 1.0f - 2.0f * (x * x + z * z); R[2][1] = 2.0f * (y * z + w * x);
-  R[0][2] = 2.0f * (x * z + w * y); R[1][2] = 2.0f * (y * z - w * x); R[2][2] = 1.0f - 2.0f * (x * x + y * y);
+  R[0][0] = fma_<X>(-2.0f, sum_sq2<X>(y, z), 1.0f); R[1][0] = mul_<X>(2.0f, dot2<X>(x, y, w, z));
+  R[2][0] = mul_<X>(2.0f, dot2<X>(x, z, -w, y));
+  R[0][1] = mul_<X>(2.0f, dot2<X>(x, y, -w, z)); R[1][1] = fma_<X>(-2.0f, sum_sq2<X>(x, z), 1.0f);
+  R[2][1] = mul_<X>(2.0f, dot2<X>(y, z, w, x));
+  R[0][2] = mul_<X>(2.0f, dot2<X>(x, z, w, y)); R[1][2] = mul_<X>(2.0f, dot2<X>(y, z, -w, x));
+  R[2][2] = fma_<X>(-2.0f, sum_sq2<X>(x, y), 1.0f);
 }
 
 // Geometry shared by forward and backward for one (splat, view).
@@ -98,9 +116,9 @@ struct Geo {
 };
 
 // Division and exp for the geometry: IEEE-rounded in the forward (its radius
-// and tile rectangle must match the reference's float arithmetic), the SFU
-// approximations (a few ulp) in the backward, whose gradients are compared by
-// tolerance.
+// and tile rectangle must match the reference's float arithmetic) and in
+// sc_project_backward, the SFU approximations (a few ulp) in the trainer's
+// adjoint, whose gradients are compared by tolerance.
 template <bool FAST> __device__ __forceinline__ float gdiv(float a, float b) { return FAST ? __fdividef(a, b) : a / b; }
 template <bool FAST> __device__ __forceinline__ float gexp(float a) { return FAST ? __expf(a) : expf(a); }
 
@@ -108,38 +126,38 @@ template <bool FAST> __device__ __forceinline__ float gexp(float a) { return FAS
 template <bool FAST>
 __device__ __forceinline__ bool geometry(const Cam& c, float px, float py, float pz, float qw, float qx, float qy,
                                          float qz, float l0, float l1, float l2, int precise, Geo& g) {
-  const float vx = c.v[0] * px + c.v[4] * py + c.v[8] * pz + c.v[12];
-  const float vy = c.v[1] * px + c.v[5] * py + c.v[9] * pz + c.v[13];
-  const float vz = c.v[2] * px + c.v[6] * py + c.v[10] * pz + c.v[14];
-  const float vw = c.v[3] * px + c.v[7] * py + c.v[11] * pz + c.v[15];
+  const float vx = fma_<!FAST>(c.v[8], pz, fma_<!FAST>(c.v[4], py, fma_<!FAST>(c.v[0], px, c.v[12])));
+  const float vy = fma_<!FAST>(c.v[9], pz, fma_<!FAST>(c.v[5], py, fma_<!FAST>(c.v[1], px, c.v[13])));
+  const float vz = fma_<!FAST>(c.v[10], pz, fma_<!FAST>(c.v[6], py, fma_<!FAST>(c.v[2], px, c.v[14])));
+  const float vw = fma_<!FAST>(c.v[11], pz, fma_<!FAST>(c.v[7], py, fma_<!FAST>(c.v[3], px, c.v[15])));
   const float depth = -gdiv<FAST>(vz, vw);
   if (!(depth >= c.near_plane)) return false;
   g.tx = gdiv<FAST>(vx, vw); g.ty = gdiv<FAST>(vy, vw); g.tz = depth;
-  quat_rot(qw, qx, qy, qz, g.R);
+  quat_rot<!FAST>(qw, qx, qy, qz, g.R);
   for (int r = 0; r < 3; ++r)
     for (int k = 0; k < 3; ++k) g.W[r][k] = c.v[4 * k + r];
   g.sig[0] = gexp<FAST>(l0); g.sig[1] = gexp<FAST>(l1); g.sig[2] = gexp<FAST>(l2);
   const float f = c.focal;
-  const float iz = gdiv<FAST>(1.0f, g.tz), iz2 = iz * iz;
-  g.j0[0] = f * iz; g.j0[1] = 0.0f; g.j0[2] = -f * g.tx * iz2;
-  g.j1[0] = 0.0f; g.j1[1] = -f * iz; g.j1[2] = f * g.ty * iz2;
+  const float iz = gdiv<FAST>(1.0f, g.tz), iz2 = mul_<!FAST>(iz, iz);
+  g.j0[0] = mul_<!FAST>(f, iz); g.j0[1] = 0.0f; g.j0[2] = mul_<!FAST>(mul_<!FAST>(-f, g.tx), iz2);
+  g.j1[0] = 0.0f; g.j1[1] = mul_<!FAST>(-f, iz); g.j1[2] = mul_<!FAST>(mul_<!FAST>(f, g.ty), iz2);
   // B = J W R S (2x3)
   float JW0[3], JW1[3];
   for (int k = 0; k < 3; ++k) {
-    JW0[k] = g.j0[0] * g.W[0][k] + g.j0[2] * g.W[2][k];
-    JW1[k] = g.j1[1] * g.W[1][k] + g.j1[2] * g.W[2][k];
+    JW0[k] = dot2<!FAST>(g.j0[2], g.W[2][k], g.j0[0], g.W[0][k]);
+    JW1[k] = dot2<!FAST>(g.j1[2], g.W[2][k], g.j1[1], g.W[1][k]);
   }
   float B0[3], B1[3];
   for (int k = 0; k < 3; ++k) {
-    B0[k] = (JW0[0] * g.R[0][k] + JW0[1] * g.R[1][k] + JW0[2] * g.R[2][k]) * g.sig[k];
-    B1[k] = (JW1[0] * g.R[0][k] + JW1[1] * g.R[1][k] + JW1[2] * g.R[2][k]) * g.sig[k];
+    B0[k] = mul_<!FAST>(fma_<!FAST>(JW0[2], g.R[2][k], dot2<!FAST>(JW0[1], g.R[1][k], JW0[0], g.R[0][k])), g.sig[k]);
+    B1[k] = mul_<!FAST>(fma_<!FAST>(JW1[2], g.R[2][k], dot2<!FAST>(JW1[1], g.R[1][k], JW1[0], g.R[0][k])), g.sig[k]);
   }
-  const float a = B0[0] * B0[0] + B0[1] * B0[1] + B0[2] * B0[2];
-  const float b = B0[0] * B1[0] + B0[1] * B1[1] + B0[2] * B1[2];
-  const float d = B1[0] * B1[0] + B1[1] * B1[1] + B1[2] * B1[2];
-  g.s00 = a + 0.3f; g.s01 = b; g.s11 = d + 0.3f;
-  g.det = g.s00 * g.s11 - g.s01 * g.s01;
-  if (precise && g.det < 0.015625f * g.s00 * g.s11) {
+  const float a = fma_<!FAST>(B0[2], B0[2], dot2<!FAST>(B0[1], B0[1], B0[0], B0[0]));
+  const float b = fma_<!FAST>(B0[2], B1[2], dot2<!FAST>(B0[1], B1[1], B0[0], B1[0]));
+  const float d = fma_<!FAST>(B1[2], B1[2], dot2<!FAST>(B1[1], B1[1], B1[0], B1[0]));
+  g.s00 = (FAST ? a + 0.3f : __fadd_rn(a, 0.3f)); g.s01 = b; g.s11 = (FAST ? d + 0.3f : __fadd_rn(d, 0.3f));
+  g.det = (FAST ? g.s00 * g.s11 - g.s01 * g.s01 : __fsub_rn(__fmul_rn(g.s00, g.s11), __fmul_rn(g.s01, g.s01)));
+  if (precise && g.det < mul_<!FAST>(mul_<!FAST>(0.015625f, g.s00), g.s11)) {
     // near-degenerate (needle-like) splat: the f32 determinant has lost more
     // than 6 bits to cancellation.  Re-form it in FP64 through Lagrange's
     // identity |B0|^2 |B1|^2 - (B0.B1)^2 = |B0 x B1|^2, which has no
@@ -158,7 +176,7 @@ __device__ __forceinline__ bool geometry(const Cam& c, float px, float py, float
   }
   if (!(g.det > 0.0f)) return false;
   const float inv = gdiv<FAST>(1.0f, g.det);
-  g.ca = g.s11 * inv; g.cb = -g.s01 * inv; g.cc = g.s00 * inv;
+  g.ca = mul_<!FAST>(g.s11, inv); g.cb = mul_<!FAST>(-g.s01, inv); g.cc = mul_<!FAST>(g.s00, inv);
   return true;
 }
 
@@ -185,25 +203,56 @@ struct TileArgs { uint32_t tw, th, tiles_x, tiles_y, cull, super; float depth_ma
 // written with coalesced stores (the per-view work — rotation, scales, SH —
 // does not share between views anyway).
 // scenes (nullable): view v projects scene v's own store.
-__global__ void __launch_bounds__(128, 8) k_project(DSplats s_all, const sc_camera* __restrict__ cams, uint32_t n_views,
+constexpr uint32_t PROJ_THREADS = 128;
+__device__ __forceinline__ void proj_cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+__global__ void __launch_bounds__(PROJ_THREADS, 8) k_project(DSplats s_all, const sc_camera* __restrict__ cams, uint32_t n_views,
                                                  uint32_t stride, float4* __restrict__ rec, TileArgs ta,
                                                  uint32_t* __restrict__ depth_keys, uint32_t* __restrict__ ids,
                                                  uint32_t* __restrict__ counts, int precise,
                                                  float4* __restrict__ zero_grad, float4* __restrict__ zero_comp,
                                                  const SceneDev* __restrict__ scenes) {
+  // the chunk's 14 geometric / opacity / DC rows (and, in the BF16 form, its 45
+  // SH-rest rows) are staged in shared memory by 16-byte cp.async copies issued
+  // together at the start, so their latency is paid once, not once per
+  // dependent load batch
+  __shared__ __align__(16) float s_par[14 * PROJ_THREADS];
+  __shared__ __align__(16) __nv_bfloat16 s_rest[45 * PROJ_THREADS];
   const uint32_t chunk = blockIdx.x / n_views;
   const uint32_t v = blockIdx.x - chunk * n_views;
-  const uint32_t i = chunk * blockDim.x + threadIdx.x;
-  if (i >= stride) return;
+  const uint32_t i0 = chunk * PROJ_THREADS;
+  const uint32_t i = i0 + threadIdx.x;
   const DSplats s = scenes ? scenes[v].s : s_all;
+  // a chunk lies wholly inside the store's capacity or wholly outside (cap is a
+  // multiple of 256, chunks are 128 splats): only whole chunks are copied
+  const bool staged = i0 < s.cap && i0 < s.n;
+  if (staged) {
+    for (uint32_t c = threadIdx.x; c < 14 * (PROJ_THREADS / 4); c += PROJ_THREADS) {
+      const uint32_t r = c / (PROJ_THREADS / 4), q = c % (PROJ_THREADS / 4);
+      proj_cp_async16(s_par + r * PROJ_THREADS + q * 4, s.slab + (size_t)r * s.cap + i0 + q * 4);
+    }
+    if (s.bf16) {
+      for (uint32_t c = threadIdx.x; c < 45 * (PROJ_THREADS / 8); c += PROJ_THREADS) {
+        const uint32_t r = c / (PROJ_THREADS / 8), q = c % (PROJ_THREADS / 8);
+        proj_cp_async16(s_rest + r * PROJ_THREADS + q * 8, s.rest16 + (size_t)r * s.cap + i0 + q * 8);
+      }
+    }
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_all;" ::: "memory");
+  }
+  __syncthreads();
+  if (i >= stride) return;
   const bool live = i < s.n;
   float px = 0, py = 0, pz = 0, qw = 1, qx = 0, qy = 0, qz = 0, l0 = 0, l1 = 0, l2 = 0, op = 0, d0 = 0, d1 = 0, d2 = 0;
   if (live) {
-    px = sp_row(s, 0, i); py = sp_row(s, 1, i); pz = sp_row(s, 2, i);
-    qw = sp_row(s, 3, i); qx = sp_row(s, 4, i); qy = sp_row(s, 5, i); qz = sp_row(s, 6, i);
-    l0 = sp_row(s, 7, i); l1 = sp_row(s, 8, i); l2 = sp_row(s, 9, i);
-    op = sp_row(s, 10, i);
-    d0 = sp_row(s, 11, i); d1 = sp_row(s, 12, i); d2 = sp_row(s, 13, i);
+    const float* pr = s_par + threadIdx.x;
+    px = pr[0 * PROJ_THREADS]; py = pr[1 * PROJ_THREADS]; pz = pr[2 * PROJ_THREADS];
+    qw = pr[3 * PROJ_THREADS]; qx = pr[4 * PROJ_THREADS]; qy = pr[5 * PROJ_THREADS]; qz = pr[6 * PROJ_THREADS];
+    l0 = pr[7 * PROJ_THREADS]; l1 = pr[8 * PROJ_THREADS]; l2 = pr[9 * PROJ_THREADS];
+    op = pr[10 * PROJ_THREADS];
+    d0 = pr[11 * PROJ_THREADS]; d1 = pr[12 * PROJ_THREADS]; d2 = pr[13 * PROJ_THREADS];
   }
   const float opacity = 1.0f / (1.0f + expf(-op));
   {
@@ -232,12 +281,12 @@ __global__ void __launch_bounds__(128, 8) k_project(DSplats s_all, const sc_came
           float ar = 0.f, ag = 0.f, ab = 0.f;
           const size_t pitch = s.cap;
           if (s.bf16) {
-            const __nv_bfloat16* p = s.rest16 + i;
+            const __nv_bfloat16* p = s_rest + threadIdx.x;
 #pragma unroll
             for (int k = 0; k < 15; ++k) {
-              ar += __bfloat162float(p[(size_t)k * pitch]) * b[k];
-              ag += __bfloat162float(p[(size_t)(15 + k) * pitch]) * b[k];
-              ab += __bfloat162float(p[(size_t)(30 + k) * pitch]) * b[k];
+              ar += __bfloat162float(p[k * PROJ_THREADS]) * b[k];
+              ag += __bfloat162float(p[(15 + k) * PROJ_THREADS]) * b[k];
+              ab += __bfloat162float(p[(30 + k) * PROJ_THREADS]) * b[k];
             }
           } else {
             const float* p = s.slab + (size_t)SC_ROW_REST * pitch + i;
@@ -312,7 +361,7 @@ sc_status launch_project(sc_ctx* ctx, const DSplats& s, const sc_camera* d_cams,
   if (tl) ta = TileArgs{tl->tile_w, tl->tile_h, (tl->width + tl->tile_w - 1) / tl->tile_w,
                         (tl->height + tl->tile_h - 1) / tl->tile_h, (cull & 1) ? 1u : 0u, (cull & 2) ? 1u : 0u,
                         tl->depth_max};
-  const uint32_t bs = 128;  // grid: (splats / bs) x views CTAs, views innermost
+  const uint32_t bs = PROJ_THREADS;  // grid: (splats / bs) x views CTAs, views innermost
   const uint64_t blocks = sc_div_up(stride, bs) * (uint64_t)n_views;
   if (blocks > 0x7FFFFFFFull) return sc_fail(ctx, SC_ERR_INVALID_ARG, "too many splat views for one launch");
   k_project<<<(unsigned)blocks, bs, 0, ctx->stream>>>(s, d_cams, n_views, stride, rec, ta, depth_keys, ids, counts,
@@ -330,6 +379,11 @@ __device__ __forceinline__ bool splat_backward_view(const Cam& c, float px, floa
                                                     const float4 pg0, const float4 pg1, const float4 pg2,
                                                     float gpos[3], float grot[4], float gsc[3], float& gop,
                                                     float basis[15], int precise) {
+  // FAST = false (sc_project_backward) forms the geometry exactly as the
+  // forward does, so it keeps exactly the splats the forward kept; the
+  // trainer's FAST adjoint can differ from the forward only for a needle whose
+  // f32 determinant is within rounding of zero (the FP64 option decides those
+  // robustly)
   Geo g;
   if (!geometry<FAST>(c, px, py, pz, qw, qx, qy, qz, l0, l1, l2, precise, g)) return false;
   const float f = c.focal;
