@@ -326,23 +326,63 @@ static uint32_t super_bits_for(uint32_t n) {  // 2^b > n
 
 constexpr int SUPER_MASK_SHIFT = 16;  // item key: member mask << 16 | view << super_bits | super tile
 
-// Same warp-staged emission as k_presorted_emit; a lane regenerates its few
-// items for every chunk that holds some of them.
-__global__ void __launch_bounds__(EMIT_WARPS * 32) k_super_emit(
+// One CTA per 256 consecutive depth-ranked (view, splat) entries, whose items
+// form one contiguous output range.  A lane walks one splat's super rows, so a
+// warp takes as long as its largest splat: the CTA first sorts its splats into
+// classes by item count (a shared-memory counting sort, order within a class
+// arbitrary) and hands them to the lanes in class order, so that a warp's
+// lanes carry splats of about the same size.  The items are staged in shared
+// memory in chunks of SE_CHUNK positions and stored coalesced; a lane
+// regenerates its items for every chunk that holds some of them.  The output
+// does not depend on which lane takes which splat (each item's position is
+// its splat's offset plus its rank among the splat's items).
+constexpr int SE_THREADS = 256;
+constexpr int SE_CHUNK = 2048;
+constexpr int SE_CLASSES = 32;  // item counts 0..30, and 31 or more
+
+__global__ void __launch_bounds__(SE_THREADS) k_super_emit(
     const float4* __restrict__ rec, uint32_t stride, uint32_t n_views, const uint32_t* __restrict__ sorted_ids,
     const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ counts_by_id, BinArgs a, uint32_t super_x,
     uint32_t super_bits, uint32_t* __restrict__ keys, uint32_t* __restrict__ payloads, uint64_t cap,
     uint32_t* __restrict__ err, int cull) {
-  __shared__ uint32_t sk[EMIT_WARPS][EMIT_WCHUNK], sp[EMIT_WARPS][EMIT_WCHUNK];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __shared__ uint32_t sk[SE_CHUNK], sp[SE_CHUNK];
+  __shared__ uint32_t s_class[SE_CLASSES];
+  __shared__ uint16_t s_perm[SE_THREADS];
   const uint64_t total = (uint64_t)n_views * stride;
-  const uint64_t jw = (uint64_t)blockIdx.x * blockDim.x + (uint64_t)warp * 32;
-  if (jw >= total) return;
-  const uint64_t j = jw + lane;
-  const uint64_t jend = jw + 32 < total ? jw + 32 : total;
+  const uint64_t j0 = (uint64_t)blockIdx.x * SE_THREADS;
+  const uint64_t jend = j0 + SE_THREADS < total ? j0 + SE_THREADS : total;
   // item offsets are 32-bit (the scan of the counts), so is the chunk walk
-  const uint32_t wlo = offsets[jw], whi = offsets[jend];
-  if (lane == 0 && whi > cap) atomicOr(err, SC_DEVERR_CAPACITY);
+  const uint32_t clo = offsets[j0], chi = offsets[jend];
+  if (threadIdx.x == 0 && chi > cap) atomicOr(err, SC_DEVERR_CAPACITY);
+  // this thread's entry's item count decides its class
+  uint32_t own = 0;
+  {
+    const uint64_t jt = j0 + threadIdx.x;
+    if (jt < total) {
+      const uint32_t v = (uint32_t)(jt / stride);
+      own = counts_by_id[(size_t)v * stride + sorted_ids[jt]];
+    }
+  }
+  const uint32_t cls = own < SE_CLASSES - 1 ? own : SE_CLASSES - 1;
+  if (threadIdx.x < SE_CLASSES) s_class[threadIdx.x] = 0;
+  __syncthreads();
+  const uint32_t rank = atomicAdd(&s_class[cls], 1u);
+  __syncthreads();
+  if (threadIdx.x < 32) {  // exclusive scan of the class sizes
+    const uint32_t c = s_class[threadIdx.x];
+    uint32_t x = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if ((int)threadIdx.x >= o) x += y;
+    }
+    s_class[threadIdx.x] = x - c;
+  }
+  __syncthreads();
+  s_perm[s_class[cls] + rank] = (uint16_t)threadIdx.x;
+  __syncthreads();
+  // the splat this lane walks
+  const uint64_t j = j0 + s_perm[threadIdx.x];
   uint32_t cnt = 0, id = 0, vkey = 0, off = 0;
   int x0 = 0, y0 = 0, x1 = -1, y1 = -1;
   CullShape cs{};
@@ -361,10 +401,8 @@ __global__ void __launch_bounds__(EMIT_WARPS * 32) k_super_emit(
       vkey = v << super_bits;
     }
   }
-  uint32_t* wk = sk[warp];
-  uint32_t* wp = sp[warp];
-  for (uint32_t cb = wlo; cb < whi; cb += EMIT_WCHUNK) {
-    const uint32_t ce = min(cb + EMIT_WCHUNK, whi);
+  for (uint32_t cb = clo; cb < chi; cb += SE_CHUNK) {
+    const uint32_t ce = min(cb + (uint32_t)SE_CHUNK, chi);
     if (cnt && off < ce && off + cnt > cb) {
       uint32_t w = 0;
       for_each_super_span(cs, test, x0, y0, x1, y1, a.tw, a.th,
@@ -372,27 +410,27 @@ __global__ void __launch_bounds__(EMIT_WARPS * 32) k_super_emit(
         for (int sx = sx0; sx <= sx1; ++sx, ++w) {
           const uint32_t g = off + w;
           if (w < cnt && g >= cb && g < ce) {
-            wk[g - cb] = (super_mask_of(sx, rlo, rhi) << SUPER_MASK_SHIFT) | vkey |
+            sk[g - cb] = (super_mask_of(sx, rlo, rhi) << SUPER_MASK_SHIFT) | vkey |
                          ((uint32_t)sy * super_x + (uint32_t)sx);
-            wp[g - cb] = id;
+            sp[g - cb] = id;
           }
         }
       });
       for (; w < cnt; ++w) {  // count and emission disagreed: pad with a key that sorts last
         const uint32_t g = off + w;
-        if (g >= cb && g < ce) { wk[g - cb] = 0xFFFFFFFFu; wp[g - cb] = 0; }
+        if (g >= cb && g < ce) { sk[g - cb] = 0xFFFFFFFFu; sp[g - cb] = 0; }
       }
     }
-    __syncwarp();
+    __syncthreads();
     const uint32_t n = ce - cb;
-    for (uint32_t t = lane; t < n; t += 32) {
+    for (uint32_t t = threadIdx.x; t < n; t += SE_THREADS) {
       const uint32_t g = cb + t;
       if (g < cap) {
-        keys[g] = wk[t];
-        payloads[g] = wp[t];
+        keys[g] = sk[t];
+        payloads[g] = sp[t];
       }
     }
-    __syncwarp();
+    __syncthreads();
   }
 }
 
@@ -405,7 +443,7 @@ sc_status launch_super_emit(sc_ctx* ctx, const float4* rec, uint32_t stride, uin
   const BinArgs a = bin_args(tl);
   const uint32_t sx = (a.tiles_x + SC_SUPER - 1) / SC_SUPER;
   const uint32_t bits = super_bits_for(super_tiles_per_view(tl));
-  k_super_emit<<<(unsigned)sc_div_up(total, EMIT_WARPS * 32), EMIT_WARPS * 32, 0, ctx->stream>>>(
+  k_super_emit<<<(unsigned)sc_div_up(total, SE_THREADS), SE_THREADS, 0, ctx->stream>>>(
       rec, stride, n_views, sorted_ids, offsets, counts_by_id, a, sx, bits, keys, payloads, cap, d_error, cull);
   return sc_check_launch(ctx, "k_super_emit");
 }
