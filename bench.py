@@ -341,6 +341,41 @@ def side_forms(ctx, torch, stream, args, scene, tbuf, tgt0, cams0, tl, n_steps, 
     return out
 
 
+def stage_bytes(N: int, V: int, P: int, K: int, items: int, bw: dict, bf16: bool, tiles: int,
+                adam: bool = True) -> dict:
+    """Algorithmic bytes per step of each stage: N splats, V views of P pixels,
+    K (tile, splat) pairs, `items` two-level items, the blends' work counters
+    `bw`; `adam` false for the split-views step, whose last stage writes the
+    gradient rows only (Adam runs after the reduce-scatter)."""
+    rest_b = 90 if bf16 else 180
+    mom_b = 59 * 2 * (2 if bf16 else 4)
+    fwd_list = bw.get("fwd_scanned", 0) * 8 + bw.get("fwd_blended", 0) * 48  # item words + blended records
+    bwd_list = bw.get("bwd_scanned", 0) * 8 + bw.get("bwd_blended", 0) * 48
+    tile_passes = max(1, math.ceil(max(1, (tiles - 1).bit_length()) / 8))
+    return {
+        # records, zeroed gradient records, depth key, id, item count
+        "project": N * (56 + rest_b) + V * N * (48 + 48 + 4 + 4 + 4),
+        # segmented onesweep over the 16-bit depth keys: a histogram read, then 2 passes
+        # of 8-bit digits each reading and writing key + id
+        "depth_sort": V * N * 4 + 2 * V * N * 16,
+        "count_scan": V * N * (4 + 4 + 4) + V * N * 8,
+        "emit": V * N * (4 + 16 + 4) + K * 8,
+        "tile_sort": K * 4 + tile_passes * K * 16,
+        "ranges": K * 4 + tiles * 8,
+        # two-level binning: items (member mask | super tile, splat); the blends
+        # read each tile's super-tile item list up to where its pixels saturate
+        "item_emit": V * N * (4 + 16 + 4) + items * 8,
+        "item_sort": items * 4 + items * 16,   # histogram read + one 9-bit pass
+        "item_ranges": items * 4,
+        "blend_fwd": fwd_list + V * P * (16 + 8),
+        "blend_bwd": bwd_list + V * P * (16 + 8 + 12) + V * N * 48,
+        # projection backward: per-view gradient records + geometry in, 59 f32 gradient
+        # rows out; streaming Adam: rows, parameters, moments and statistic in and out
+        "bwd_adam": (V * N * 48 + N * 44 + N * 236 +
+                     ((N * 236 + N * 2 * (56 + rest_b) + N * 2 * mom_b + N * 8) if adam else 0)),
+    }
+
+
 def run_ours(args):
     ws, rank, local, pg = dist_setup()
     if (ws > 1 and args.parallel == "views") or args.view_path:
@@ -463,38 +498,10 @@ def run_ours(args):
     # ---- roofline of the dominant stage
     stage = st["stage_ms"]
     dom = max(stage, key=stage.get)
-    P = args.width * args.height
     N = len(scene)
-    K = st["pairs"]
-    tiles = V * tl.num_tiles()
-    rest_b = 90 if bf16 else 180
-    mom_b = 59 * 2 * (2 if bf16 else 4)
-    items = st.get("items") or 0
     bw = st.get("blend_work") or {}
-    fwd_list = bw.get("fwd_scanned", 0) * 8 + bw.get("fwd_blended", 0) * 48  # item words + blended records
-    bwd_list = bw.get("bwd_scanned", 0) * 8 + bw.get("bwd_blended", 0) * 48
-    tile_passes = max(1, math.ceil(max(1, (V * tl.num_tiles() - 1).bit_length()) / 8))
-    algo = {
-        # records, zeroed gradient records, depth key, id, item count
-        "project": N * (56 + rest_b) + V * N * (48 + 48 + 4 + 4 + 4),
-        # segmented onesweep over the 16-bit depth keys: a histogram read, then 2 passes
-        # of 8-bit digits each reading and writing key + id
-        "depth_sort": V * N * 4 + 2 * V * N * 16,
-        "count_scan": V * N * (4 + 4 + 4) + V * N * 8,
-        "emit": V * N * (4 + 16 + 4) + K * 8,
-        "tile_sort": K * 4 + tile_passes * K * 16,
-        "ranges": K * 4 + tiles * 8,
-        # two-level binning: items (member mask | super tile, splat); the blends
-        # read each tile's super-tile item list up to where its pixels saturate
-        "item_emit": V * N * (4 + 16 + 4) + items * 8,
-        "item_sort": items * 4 + items * 16,   # histogram read + one 9-bit pass
-        "item_ranges": items * 4,
-        "blend_fwd": fwd_list + V * P * (16 + 8),
-        "blend_bwd": bwd_list + V * P * (16 + 8 + 12) + V * N * 48,
-        # projection backward: per-view gradient records + geometry in, 59 f32 gradient
-        # rows out; streaming Adam: rows, parameters, moments and statistic in and out
-        "bwd_adam": V * N * 48 + N * 44 + N * 236 + N * 236 + N * 2 * (56 + rest_b) + N * 2 * mom_b + N * 8,
-    }
+    algo = stage_bytes(N, V, args.width * args.height, st["pairs"], st.get("items") or 0, bw, bf16,
+                       V * tl.num_tiles())
     peaks = load_peaks()
     dom_ms = stage[dom]
     achieved = algo[dom] / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
@@ -532,7 +539,7 @@ def run_ours(args):
                                    f"{' per GPU (one scene per GPU)' if ws > 1 else ''}, "
                                    f"{cfg.tile_w}x{cfg.tile_h} tiles, exact transmittance backward, CUDA graph",
                        "form": "batched-" + ("bf16" if bf16 else "fp32"), "splats": N, "views_per_iter": V,
-                       "width": args.width, "height": args.height, "pairs_per_iter": K, "items_per_iter": items,
+                       "width": args.width, "height": args.height, "pairs_per_iter": st["pairs"], "items_per_iter": st.get("items") or 0,
                        "l2": "inputs larger than L2 (params, item lists and images >> 126 MB)",
                        "parallelism": f"{ws} GPUs, one scene each (no exchange)" if ws > 1 else "single GPU"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
@@ -833,9 +840,8 @@ def run_views(args, ws, rank, local, pg):
     dom = max(stage, key=stage.get)
     peaks = load_peaks()
     N, K, P, Vl = len(scene), st["pairs"], args.width * args.height, len(views)
-    algo = {"blend_bwd": K * (4 + 48) + Vl * P * (16 + 16 + 8) + Vl * N * 48 * 2,
-            "blend_fwd": K * (4 + 48) + Vl * P * (16 + 8 + 12 + 16),
-            "tile_sort": 2 * K * 16 + K * 4, "emit": Vl * N * (4 + 16 + 4) + K * 8}
+    algo = stage_bytes(N, Vl, P, K, st.get("items") or 0, st.get("blend_work") or {}, bf16, Vl * tl.num_tiles(),
+                       adam=False)
     ab = algo.get(dom)
     achieved = ab / (stage[dom] / 1e3) / 1e9 if ab and stage[dom] > 0 else None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": None if achieved is None else round(achieved, 1),
