@@ -307,3 +307,75 @@ def test_pixel_pair_counters(ctx):
     assert 0 < w2["fwd_pixel_pairs"] == w2["bwd_pixel_pairs"]
     assert w2["fwd_pixel_pairs"] <= w2["fwd_blended"] * cfg.tile_w * cfg.tile_h
     tr.set_profiling(False)
+
+
+def test_trainer_ragged_image_matches_oracle_iteration(ctx, oracle):
+    """An image that is not a whole number of tiles (100x70 with 16x16 tiles:
+    the last tile column and row hold 4 and 6 pixels): the iteration stage by
+    stage and through the captured step against the oracle."""
+    from tests.parity import iteration_parity
+    scene, tl, cams, _, _ = _setup(ctx, n=1500, W=100, H=70, V=2)
+    print(iteration_parity(ctx, oracle, scene, cams, tl, 1, "ragged 100x70"))
+
+
+def test_trainer_step_with_every_splat_culled(ctx, oracle):
+    """Every splat behind the camera: no items, empty lists, black images; the
+    loss is the targets' mean square as in the oracle's iteration, and Adam's
+    zero gradients leave every parameter where it was (the constraints
+    renormalise the quaternions, a few ulp)."""
+    n, W, H, V = 500, 64, 48, 2
+    base = random_scene(n, 31).flat().copy()
+    base[:, 0:3] = base[:, 0:3] * 0.1 + np.array([0.0, 0.0, 50.0], np.float32)  # far behind the orbit cameras
+    scene = SplatBuffer.from_flat(base)
+    tl = TilingParams(W, H, 16, 8.0)
+    cams = [CameraUniform.from_pose((0.0, 0.0, -4.0), (0.0, 0.0, -10.0), (0.0, 1.0, 0.0), FOV_Y, W, H, n)] * V
+    rng = np.random.default_rng(3)
+    tgt = rng.uniform(0.0, 1.0, (V, H, W, 3)).astype(np.float32)
+    cfg = TrainConfig(n_views=V, width=W, height=H, depth_max=8.0)
+    tr, g, mo, acc, losses = _run(ctx, scene, cams, tgt, cfg)
+    assert tr.stats()["items"] == 0 and tr.stats()["pairs"] == 0
+    img = tr.images()
+    assert np.all(img == 0.0)
+    want = float(np.mean(tgt.astype(np.float64) ** 2))
+    assert abs(losses[0] - want) <= 1e-6 * want, (losses[0], want)
+    os_ = oracle.OSplats.from_buffer(scene)
+    om, ov = oracle.OSplats.zeros(n), oracle.OSplats.zeros(n)
+    ol, _ = oracle.train_step(os_, om, ov, np.zeros(n, np.float32), [oracle.camera_from_struct(bytes(c.c)) for c in cams],
+                              tgt, oracle.tiling(W, H, 16, 16, 8.0), 1, BENCH_LRS, 1)
+    assert abs(losses[0] - ol) <= 1e-6 * ol, (losses[0], ol)
+    after, before = g.readback().flat(), scene.flat()
+    rest = np.r_[0:3, 7:59]
+    assert np.array_equal(after[:, rest], before[:, rest])
+    assert np.allclose(after[:, 3:7], before[:, 3:7], rtol=0.0, atol=1e-6)
+
+
+def test_trainer_culls_a_nonfinite_splat(ctx):
+    """A splat whose position is NaN is culled (the projection's depth test
+    rejects non-finite depths): the step renders what the same scene renders
+    with that splat made transparent (an opacity logit of -30, below the 1/255
+    cut everywhere, so it emits no item), bit for bit, and every other
+    parameter stays finite."""
+    scene, tl, cams, tgt, cfg = _setup(ctx, n=3000, V=2)
+    f = scene.flat().copy()
+    bad, away = f.copy(), f.copy()
+    bad[17, 0] = np.nan
+    away[17, 10] = -30.0
+    tr_bad, g_bad, *_ = _run(ctx, SplatBuffer.from_flat(bad), cams, tgt, cfg)
+    tr_away, *_ = _run(ctx, SplatBuffer.from_flat(away), cams, tgt, cfg)
+    assert np.array_equal(tr_bad.images(), tr_away.images())
+    out = g_bad.readback().flat()
+    assert np.all(np.isfinite(np.delete(out, 17, axis=0)))
+
+
+def test_trainer_step_with_no_splats(ctx):
+    """An empty store (every splat pruned): the step runs, renders black and
+    reports the targets' mean square as its loss."""
+    W, H, V = 64, 48, 2
+    scene = SplatBuffer.from_flat(np.zeros((0, 59), np.float32))
+    cams = [CameraUniform.from_pose(*p, FOV_Y, W, H, 0) for p in orbit_views(V, 0)]
+    tgt = np.random.default_rng(5).uniform(0.0, 1.0, (V, H, W, 3)).astype(np.float32)
+    cfg = TrainConfig(n_views=V, width=W, height=H, depth_max=8.0)
+    tr, g, mo, acc, losses = _run(ctx, scene, cams, tgt, cfg, cap=256)
+    assert np.all(tr.images() == 0.0)
+    want = float(np.mean(tgt.astype(np.float64) ** 2))
+    assert abs(losses[0] - want) <= 1e-6 * want, (losses[0], want)
