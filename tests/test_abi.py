@@ -166,3 +166,15 @@ def test_compute_calls_fail_loudly_without_a_device():
     from nanotracer_b200 import CudaCtx, SplatCudaError
     with pytest.raises(SplatCudaError):
         CudaCtx(0)
+
+
+def test_integration_ffi_block_binds_every_declared_function():
+    """The Rust extern block a maintainer would add names every
+    function include/splat_cuda.h declares."""
+    import re
+    root = Path(__file__).resolve().parent.parent
+    header = (root / "include" / "splat_cuda.h").read_text()
+    ffi = (root / "INTEGRATION.md").read_text()
+    declared = sorted(set(re.findall(r"\b(sc_[a-z0-9_]+)\s*\(", header)))
+    assert declared
+    assert [f for f in declared if f"fn {f}(" not in ffi] == []
