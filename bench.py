@@ -192,6 +192,89 @@ def max_over_ranks(pg, x: float) -> float:
     return float(t.item())
 
 
+class _Cuda:
+    """The few CUDA runtime calls the harness needs around the library, through
+    cuda-python (cuda.bindings.runtime): events recorded on the library's
+    stream, a device-wide synchronize, page-locked host buffers."""
+
+    def __init__(self):
+        self._rt = None
+
+    @property
+    def rt(self):
+        if self._rt is None:
+            from cuda.bindings import runtime
+            self._rt = runtime
+        return self._rt
+
+    def check(self, err, what: str):
+        if int(err) != 0:
+            raise RuntimeError(f"{what}: CUDA error {int(err)}")
+
+    def set_device(self, device: int):
+        self.check(self.rt.cudaSetDevice(int(device))[0], "cudaSetDevice")
+
+    def synchronize(self):
+        self.check(self.rt.cudaDeviceSynchronize()[0], "cudaDeviceSynchronize")
+
+    def Event(self):
+        return _CudaEvent(self)
+
+    def pinned_f32(self, n: int):
+        return _Pinned(self, n)
+
+
+class _CudaEvent:
+    def __init__(self, cu: _Cuda):
+        self.cu = cu
+        err, self.ev = cu.rt.cudaEventCreate()
+        cu.check(err, "cudaEventCreate")
+
+    def record(self, stream: int):
+        self.cu.check(self.cu.rt.cudaEventRecord(self.ev, self.cu.rt.cudaStream_t(int(stream)))[0], "cudaEventRecord")
+
+    def elapsed_time(self, later: "_CudaEvent") -> float:
+        err, ms = self.cu.rt.cudaEventElapsedTime(self.ev, later.ev)
+        self.cu.check(err, "cudaEventElapsedTime")
+        return float(ms)
+
+    def __del__(self):
+        try:
+            self.cu.rt.cudaEventDestroy(self.ev)
+        except Exception:
+            pass
+
+
+class _Pinned:
+    """n float32 in page-locked host memory (cudaHostAlloc), viewed as numpy."""
+
+    def __init__(self, cu: _Cuda, n: int):
+        import ctypes
+        self.cu, self.n = cu, int(n)
+        err, self.ptr = cu.rt.cudaHostAlloc(4 * self.n, cu.rt.cudaHostAllocDefault)
+        cu.check(err, "cudaHostAlloc")
+        self.arr = np.ctypeslib.as_array((ctypes.c_float * self.n).from_address(int(self.ptr)))
+
+    def numpy(self):
+        return self.arr
+
+    def data_ptr(self) -> int:
+        return int(self.ptr)
+
+    def numel(self) -> int:
+        return self.n
+
+    def __del__(self):
+        try:
+            self.arr = None
+            self.cu.rt.cudaFreeHost(self.ptr)
+        except Exception:
+            pass
+
+
+cu = _Cuda()
+
+
 # ------------------------------------------------------------------ workload
 def make_workload(args, rank, ctx):
     import nanotracer_b200 as nt
@@ -267,22 +350,22 @@ def quality(ctx, g, cams, tl, tgt, fp64=True):
     return out
 
 
-def timed_run(ctx, torch, stream, tr, g, mo, acc, cams_seq, t):
+def timed_run(ctx, stream, tr, g, mo, acc, cams_seq, t):
     """Steps over cams_seq between CUDA events on the library stream; returns (ms, t, loss)."""
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
+    e0 = cu.Event()
+    e1 = cu.Event()
+    cu.synchronize()
     e0.record(stream)
     loss = None
     for cams in cams_seq:
         t += 1
         loss = tr.step(g, mo, acc, cams, t)
     e1.record(stream)
-    torch.cuda.synchronize()
+    cu.synchronize()
     return e0.elapsed_time(e1), t, loss
 
 
-def side_forms(ctx, torch, stream, args, scene, tbuf, tgt0, cams0, tl, n_steps, main_form):
+def side_forms(ctx, stream, args, scene, tbuf, tgt0, cams0, tl, n_steps, main_form):
     """The metric's other forms on the same box, from the same start, untimed
     except for their own K steps: the batched form in the other precision, and
     the plain FP32 form (one view per iteration, the reference's train() loop,
@@ -303,8 +386,8 @@ def side_forms(ctx, torch, stream, args, scene, tbuf, tgt0, cams0, tl, n_steps, 
     tr = Trainer(ctx, cfg)
     tr.set_targets(tbuf)
     t = 0
-    _, t, _ = timed_run(ctx, torch, stream, tr, g, mo, acc, [cams0] * (n_steps - K), t)
-    ms, t, _ = timed_run(ctx, torch, stream, tr, g, mo, acc, [cams0] * K, t)
+    _, t, _ = timed_run(ctx, stream, tr, g, mo, acc, [cams0] * (n_steps - K), t)
+    ms, t, _ = timed_run(ctx, stream, tr, g, mo, acc, [cams0] * K, t)
     out["batched_" + other] = {"iters_s": round(K / (ms / 1e3), 3), "ms_per_iter": round(ms / K, 4),
                                "views_per_iter": V, "iters": t, **quality(ctx, g, cams0, tl, tgt0)}
     del tr
@@ -328,12 +411,12 @@ def side_forms(ctx, torch, stream, args, scene, tbuf, tgt0, cams0, tl, n_steps, 
         return t
 
     t1 = plain(V * (n_steps - K), 0)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    cu.synchronize()
+    e0, e1 = cu.Event(), cu.Event()
     e0.record(stream)
     t1 = plain(V * K, t1)
     e1.record(stream)
-    torch.cuda.synchronize()
+    cu.synchronize()
     ms1 = e0.elapsed_time(e1)
     out["plain_fp32"] = {"iters_s": round(V * K / (ms1 / 1e3), 3), "ms_per_iter": round(ms1 / (V * K), 4),
                          "views_per_iter": 1, "iters": t1, **quality(ctx, g1, cams0, tl, tgt0)}
@@ -380,12 +463,12 @@ def run_ours(args):
     ws, rank, local, pg = dist_setup()
     if (ws > 1 and args.parallel == "views") or args.view_path:
         return run_views(args, ws, rank, local, pg)
-    import torch
 
     import nanotracer_b200 as nt
     from nanotracer_b200.train import TrainConfig, Trainer
     ctx = nt.CudaCtx(local)
-    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+    cu.set_device(local)  # this process's events and host buffers on the library's device
+    stream = ctx.stream
     scene, tscene, tl, cams_for, render_targets = make_workload(args, rank, ctx)
     V = args.views
     bf16 = args.form == "bf16"
@@ -417,19 +500,19 @@ def run_ours(args):
     for s in range(args.warmup):
         t += 1
         tr.step(g, mo, acc, cams0, t)
-    torch.cuda.synchronize(local)
+    cu.synchronize()
     barrier(pg)
     launches0 = ctx.launch_count
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize(local)
+    e0 = cu.Event()
+    e1 = cu.Event()
+    cu.synchronize()
     w0 = time.time()
     e0.record(stream)
     for s in range(args.steps):
         t += 1
         loss = tr.step(g, mo, acc, cams0, t)
     e1.record(stream)
-    torch.cuda.synchronize(local)
+    cu.synchronize()
     w1 = time.time()
     clk.stop()
     barrier(pg)
@@ -471,24 +554,24 @@ def run_ours(args):
     if not args.no_e2e:
         # the step's targets come from pinned host memory: the trainer copies them
         # on a side stream every step, overlapped with the stages before the blend
-        pinned = torch.empty(tgt0.size, dtype=torch.float32, pin_memory=True)
+        pinned = cu.pinned_f32(tgt0.size)
         pinned.numpy()[:] = tgt0.reshape(-1)
         tr.set_profiling(False)
         tr.set_host_targets(pinned.data_ptr(), keepalive=pinned)
         h2d = pinned.numel() * 4 + V * 96
         t += 1
         tr.step(g, mo, acc, cams0, t)  # re-capture the graph with the copy node (untimed)
-        torch.cuda.synchronize(local)
+        cu.synchronize()
         barrier(pg)
         t0 = time.perf_counter()
-        f0 = torch.cuda.Event(enable_timing=True)
-        f1 = torch.cuda.Event(enable_timing=True)
+        f0 = cu.Event()
+        f1 = cu.Event()
         f0.record(stream)
         for s in range(args.steps):
             t += 1
             tr.step(g, mo, acc, cams0, t)
         f1.record(stream)
-        torch.cuda.synchronize(local)
+        cu.synchronize()
         wall = time.perf_counter() - t0
         e2e_ms = max_over_ranks(pg, max(f0.elapsed_time(f1), wall * 1e3))
         e2e = {"value": ws * args.steps / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
@@ -515,7 +598,7 @@ def run_ours(args):
                 "issue": issue_roofline(bw)}
 
     if forms is not None:
-        forms.update(side_forms(ctx, torch, stream, args, scene, tbuf, tgt0, cams0, tl, n_steps, args.form))
+        forms.update(side_forms(ctx, stream, args, scene, tbuf, tgt0, cams0, tl, n_steps, args.form))
         b, f, p = forms.get("batched_bf16"), forms.get("batched_fp32"), forms.get("plain_fp32")
         forms["bf16_over_fp32_batched"] = round(b["iters_s"] / f["iters_s"], 4) if b and f else None
         forms["bf16_batched_over_fp32_plain_iters"] = round(b["iters_s"] / p["iters_s"], 4) if b and p else None
@@ -562,7 +645,6 @@ def run_precision(args):
     parameters), and the projected-gradient error on the crop against the
     FP64 oracle's adjoint (same records, bins, image and dL/dC; the crop's
     dL/dC only, so the oracle runs in seconds), plain and compensated."""
-    import torch
 
     import nanotracer_b200 as nt
     from nanotracer_b200._lib import SC_BWD_EXACT, SC_KEYS_NATIVE64
@@ -570,7 +652,8 @@ def run_precision(args):
     from oracle import oracle as O
     O.set_threads(O.max_threads())
     ctx = nt.CudaCtx(0)
-    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
+    cu.set_device(0)  # this process's events and host buffers on the library's device
+    stream = ctx.stream
     scene, tscene, tl, cams_for, render_targets = make_workload(args, 0, ctx)
     V, W, H = args.views, args.width, args.height
     cams0 = cams_for(0)
@@ -588,8 +671,8 @@ def run_precision(args):
         acc = ctx.storage_buffer_zeroed("grad_acc", 4 * g.capacity)
         tr = Trainer(ctx, cfg)
         tr.set_targets(tbuf)
-        _, t, _ = timed_run(ctx, torch, stream, tr, g, mo, acc, [cams0] * max(3, args.warmup), 0)
-        ms, t, _ = timed_run(ctx, torch, stream, tr, g, mo, acc, [cams0] * args.steps, t)
+        _, t, _ = timed_run(ctx, stream, tr, g, mo, acc, [cams0] * max(3, args.warmup), 0)
+        ms, t, _ = timed_run(ctx, stream, tr, g, mo, acc, [cams0] * args.steps, t)
         del tr
         img = render_views(ctx, g, cams0, tl)
         x0, y0, side = CROP
@@ -656,14 +739,14 @@ def run_scenes(args):
     single-scene trainer each, one after another.  Then the reference's
     densify / prune schedule per scene under a 6M total cap (densify by
     gradient threshold 2e-4, prune at opacity < 0.005) over a short run."""
-    import torch
 
     import nanotracer_b200 as nt
     from nanotracer_b200.scene import FOV_Y, orbit_views, perturbed, random_scene
     from nanotracer_b200.scenes import Scene, ScenesTrainer, densify_prune_scenes
     from nanotracer_b200.train import TrainConfig, Trainer, render_targets
     ctx = nt.CudaCtx(0)
-    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
+    cu.set_device(0)  # this process's events and host buffers on the library's device
+    stream = ctx.stream
     rng = np.random.default_rng(0x5CE7E5)
     sizes = [(512, 512), (1024, 768), (1920, 1080)]
     n_sc = 16
@@ -685,14 +768,14 @@ def run_scenes(args):
     for _ in range(max(3, args.warmup)):
         t += 1
         st.step(cams, t)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    cu.synchronize()
+    e0, e1 = cu.Event(), cu.Event()
     e0.record(stream)
     for _ in range(args.steps):
         t += 1
         losses = st.step(cams, t)
     e1.record(stream)
-    torch.cuda.synchronize()
+    cu.synchronize()
     ms_one = e0.elapsed_time(e1) / args.steps
     stats = st.stats()
     # the same scenes, one single-scene trainer each, stepped one after another
@@ -708,13 +791,13 @@ def run_scenes(args):
     for k in range(max(3, args.warmup)):
         for i, (tr, g, mo, acc) in enumerate(singles):
             tr.step(g, mo, acc, [cams[i]], k + 1)
-    torch.cuda.synchronize()
+    cu.synchronize()
     e0.record(stream)
     for k in range(args.steps):
         for i, (tr, g, mo, acc) in enumerate(singles):
             tr.step(g, mo, acc, [cams[i]], k + 10)
     e1.record(stream)
-    torch.cuda.synchronize()
+    cu.synchronize()
     ms_sep = e0.elapsed_time(e1) / args.steps
     del singles
     # the densify / prune schedule (train.rs:259-362) per scene, 6M total cap
@@ -746,13 +829,13 @@ def run_views(args, ws, rank, local, pg):
     across the ranks (data-parallel views, one NCCL reduce-scatter of the
     gradients and one all-gather of the parameters per iteration).  Total work
     per iteration is fixed, so the scaling is strong."""
-    import torch
 
     import nanotracer_b200 as nt
     from nanotracer_b200.multiview import CudaCollectives, CudaViewBackend, ViewParallelTrainer, split_views
     from nanotracer_b200.nccl import NcclComm
     from nanotracer_b200.train import TrainConfig
     ctx = nt.CudaCtx(local)
+    cu.set_device(local)  # this process's events and host buffers on the library's device
     # the data plane: NCCL through its C API on the library stream; its unique id
     # travels over TCP on the port after the launcher's (MASTER_PORT + 1)
     if ws > 1:
@@ -772,7 +855,7 @@ def run_views(args, ws, rank, local, pg):
     tgt_all[views] = tgt_local
     be = CudaViewBackend(ctx, scene, cfg, tgt_all, views)
     tr = ViewParallelTrainer(be, V, CudaCollectives(ctx, comm))
-    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+    stream = ctx.stream
     cams_steps = [[cams_for(s)[v] for v in views] for s in range(args.warmup + args.steps)]
     clk = ClockSampler(local, raw_copy=os.environ.get("BENCH_CLOCKS_CSV")).start()
     t = 0
@@ -780,11 +863,11 @@ def run_views(args, ws, rank, local, pg):
         t += 1
         be.set_cameras(cams_steps[s])
         tr.step(t)
-    torch.cuda.synchronize(local)
+    cu.synchronize()
     barrier(pg)
     launches0 = ctx.launch_count
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
+    e0 = cu.Event()
+    e1 = cu.Event()
     w0 = time.time()
     e0.record(stream)
     for s in range(args.steps):
@@ -792,7 +875,7 @@ def run_views(args, ws, rank, local, pg):
         be.set_cameras(cams_steps[args.warmup + s])
         loss = tr.step(t)
     e1.record(stream)
-    torch.cuda.synchronize(local)
+    cu.synchronize()
     w1 = time.time()
     clk.stop()
     barrier(pg)
@@ -814,14 +897,14 @@ def run_views(args, ws, rank, local, pg):
     be.trainer.set_profiling(False)
     e2e = None
     if not args.no_e2e:
-        pinned = torch.empty(tgt_local.size, dtype=torch.float32, pin_memory=True)
+        pinned = cu.pinned_f32(tgt_local.size)
         pinned.numpy()[:] = tgt_local.reshape(-1)
         import ctypes as C
         from nanotracer_b200._lib import check, lib
-        torch.cuda.synchronize(local)
+        cu.synchronize()
         barrier(pg)
-        f0 = torch.cuda.Event(enable_timing=True)
-        f1 = torch.cuda.Event(enable_timing=True)
+        f0 = cu.Event()
+        f1 = cu.Event()
         p0 = time.perf_counter()
         f0.record(stream)
         for s in range(args.steps):
@@ -831,7 +914,7 @@ def run_views(args, ws, rank, local, pg):
             be.set_cameras(cams_steps[args.warmup + s])
             tr.step(t)
         f1.record(stream)
-        torch.cuda.synchronize(local)
+        cu.synchronize()
         wall = time.perf_counter() - p0
         e2e_ms = max_over_ranks(pg, max(f0.elapsed_time(f1), wall * 1e3))
         e2e = {"value": args.steps / (e2e_ms / 1e3), "unit": UNIT,
@@ -869,7 +952,7 @@ def run_views(args, ws, rank, local, pg):
         print(json.dumps(line))
     tr.close()
     del tr, be
-    torch.cuda.synchronize(local)
+    cu.synchronize()
     comm.close()
     if pg is not None:
         pg.destroy_process_group()
