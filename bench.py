@@ -897,10 +897,14 @@ def run_views(args, ws, rank, local, pg):
     be.trainer.set_profiling(False)
     e2e = None
     if not args.no_e2e:
+        # this rank's targets from page-locked host memory, copied by the trainer
+        # every step on a side stream, view by view, beside the stages before the blend
         pinned = cu.pinned_f32(tgt_local.size)
         pinned.numpy()[:] = tgt_local.reshape(-1)
-        import ctypes as C
-        from nanotracer_b200._lib import check, lib
+        be.trainer.set_host_targets(pinned.data_ptr(), keepalive=pinned)
+        t += 1
+        be.set_cameras(cams_steps[args.warmup])
+        tr.step(t)  # re-capture the graph with the copy nodes (untimed; every rank takes it)
         cu.synchronize()
         barrier(pg)
         f0 = cu.Event()
@@ -909,8 +913,6 @@ def run_views(args, ws, rank, local, pg):
         f0.record(stream)
         for s in range(args.steps):
             t += 1
-            check(lib().sc_buffer_upload(ctx.handle, be.targets.cptr, C.c_void_p(pinned.data_ptr()),
-                                         pinned.numel() * 4), ctx.handle)
             be.set_cameras(cams_steps[args.warmup + s])
             tr.step(t)
         f1.record(stream)
