@@ -8,11 +8,16 @@
 // Emission order is (view, splat, ty, tx), so a stable key sort reproduces
 // the reference's order exactly (ties resolve to ascending splat index).
 //
-// Native pipeline path (trainer): splats are first sorted by depth within
-// each view (u64 key (view << 32) | depth bits), then pairs are emitted in
-// that order with a u32 key view*num_tiles + tile, so a stable sort on the
-// tile key alone (2 passes of 8 bits instead of 6) gives the same per-tile
-// front-to-back order as the 64-bit key.
+// Trainer path: the splats of each view are first sorted, stably in index
+// order, on the reference's 16-bit quantised depth (one segmented sort over
+// the views), so every later stable sort keeps each tile's (depth16, splat
+// index) order, the order of the REF32 keys.  Then either (sort_mode 1) pairs
+// are emitted in that order with a u32 key (view << tile_bits) | tile and
+// sorted on the tile bits alone, or (the default, two-level binning) one item
+// per (view, super tile of 4 x 4 tiles, splat) is emitted with the tiles it
+// reaches as a 16-bit member mask in the key, sorted on the super-tile bits in
+// one pass, and each tile's blend keeps its super tile's items whose mask
+// holds it.
 #include "sc_internal.cuh"
 
 namespace sck {

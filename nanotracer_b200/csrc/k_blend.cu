@@ -12,14 +12,19 @@
 // scale * 2 (C - target) / (3 W H) per pixel, squared errors reduced per CTA
 // in FP64 — runs in the forward's epilogue or in the backward's prologue.
 //
-// Backward (rasterize_backward.wgsl:73-210): same grid, reverse walk.  Per
-// (pixel, splat) gradients (dmean.xy, dopacity, dconic.abc, dcolor.rgb) are
-// summed over the thread's pixels, then over the warp by a 12-shuffle
-// reduce-scatter that leaves the nine totals on nine lanes, which add them to
-// a per-batch shared-memory slot with one atomic instruction; each slot goes
-// to global memory with three float4 vector atomics per (tile, splat) — the
-// reference issues nine CAS loops per (pixel, splat).  The transmittance
-// reconstruction T_i = T_{i+1} / (1 - alpha_i) uses one reciprocal per splat.
+// Backward (rasterize_backward.wgsl:73-210): same grid, reverse walk from each
+// pixel's last contributor (exact mode) or from the list's end (the
+// reference's mode).  Per (pixel, splat) a thread forms the raw sums of the
+// opacity gradient h and its moments (h, h dx, h dy, h dx^2, h dx dy, h dy^2)
+// and the colour gradient over its pixels; two entries' 18 sums are reduced
+// over the warp together by a recursive-halving reduce-scatter (20 shuffles)
+// that leaves each total on one lane, which adds it to the entry's
+// shared-memory slot; after each batch the slots become the splats' gradients
+// (dmean.xy, dopacity, dconic.abc, dcolor.rgb, with the conic and opacity
+// applied once per entry) and go to global memory with three float4 vector
+// atomics per (tile, splat) — the reference issues nine CAS loops per (pixel,
+// splat).  The transmittance reconstruction T_i = T_{i+1} / (1 - alpha_i) uses
+// one approximate reciprocal per (pixel, splat).
 #include "sc_internal.cuh"
 
 namespace sck {
