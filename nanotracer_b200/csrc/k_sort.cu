@@ -4,7 +4,7 @@
 // Replaces the reference's 3-level Hillis-Steele scan (prefix_scan.rs:127-186,
 // n <= 2^24) and its 32 one-bit split passes (radix_sort.rs:144-303, ~160
 // dispatches per sort).  Here one sort is one histogram kernel plus one kernel
-// per 8-bit digit.  Both are stable and deterministic: tiles take their
+// per 8- or 9-bit digit.  Both are stable and deterministic: tiles take their
 // position from an atomic ticket, rank their items warp-by-warp in input
 // order (ballot-based peer masks), and obtain the running digit offsets from
 // their predecessors' published aggregates.
