@@ -363,7 +363,7 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
           eval_alpha2(e, rb.z, fy2, ra.y, rc.w, dy, g, araw, al, v0, v1);
           v0 &= T2.x >= 1e-4f;
           v1 &= T2.y >= 1e-4f;
-          if (v0 || v1) {
+          {  // without a branch: a pixel that skips gets alpha 0, which changes no bit
             const float2 am = make_float2(v0 ? al.x : 0.0f, v1 ? al.y : 0.0f);
             const float2 ta = __fmul2_rn(T2, am);
             R2 = __ffma2_rn(ta, f2(rc.x), R2);
@@ -371,9 +371,9 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
             B2 = __ffma2_rn(ta, f2(rc.z), B2);
             T2 = __fmul2_rn(T2, __fadd2_rn(f2(1.0f), make_float2(-am.x, -am.y)));
             if constexpr (COUNT) w_pix += (uint32_t)v0 + (uint32_t)v1;
-            if (v0) lk0 = (int)k;
-            if (v1) lk1 = (int)k;
-            if (T2.x < 1e-4f && T2.y < 1e-4f) break;
+            lk0 = v0 ? (int)k : lk0;
+            lk1 = v1 ? (int)k : lk1;
+            if ((v0 || v1) && T2.x < 1e-4f && T2.y < 1e-4f) break;
           }
         }
         if (lk0 >= 0) last[0] = position(b, (uint32_t)lk0) + 1;
