@@ -761,7 +761,9 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
             eval_alpha2(e, rb.z, fy2, ra.y, rc.w, dy, g, araw, al, v0, v1);
             v0 &= (MODE == SC_BWD_EXACT || !done[0]) && j < stop[0];
             v1 &= (MODE == SC_BWD_EXACT || !done[1]) && j < stop[1];
-            if (v0 || v1) {
+            // the exact mode takes no branch here: with both pixels skipping, every
+            // sum below is zero and T and GS keep their values
+            if (MODE == SC_BWD_REF ? (v0 || v1) : true) {
               const float2 oma = __fadd2_rn(f2(1.0f), make_float2(-al.x, -al.y));
               const float2 inv = make_float2(rcp_approx(oma.x), rcp_approx(oma.y));
               const float2 Tn = __fmul2_rn(T2, inv);  // T_i = T_{i+1} / (1 - alpha_i)
@@ -769,7 +771,7 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
                 if (v0 && Tn.x > 1.0001f) { done[0] = true; v0 = false; }
                 if (v1 && Tn.y > 1.0001f) { done[1] = true; v1 = false; }
               }
-              if (v0 || v1) {
+              if (MODE == SC_BWD_REF ? (v0 || v1) : true) {
                 const float2 am = make_float2(v0 ? al.x : 0.0f, v1 ? al.y : 0.0f);
                 const float2 gm = make_float2(v0 && araw.x < ALPHA_MAX ? g.x : 0.0f,
                                               v1 && araw.y < ALPHA_MAX ? g.y : 0.0f);
@@ -790,7 +792,7 @@ __global__ void __launch_bounds__(256) k_composite_backward(const float4* __rest
                 GS2 = __ffma2_rn(ta, dc, GS2);
                 T2 = make_float2(v0 ? Tn.x : T2.x, v1 ? Tn.y : T2.y);
                 if constexpr (COUNT) w_pix += (uint32_t)v0 + (uint32_t)v1;
-                contrib = true;
+                contrib = v0 || v1;
               }
             }
             if (MODE == SC_BWD_REF) all_done = (done[0] || j <= begin) && (done[1] || j <= begin);
