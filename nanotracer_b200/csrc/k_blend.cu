@@ -555,22 +555,29 @@ sc_status launch_mse(sc_ctx* ctx, const float4* pred, const float* target, uint6
 // Reduce-scatter of N values over the warp by recursive halving: at the level
 // of lane bit O a lane keeps one half of its slots and sends the other half to
 // lane ^ O, which keeps the opposite half (2 selects and 1 shuffle per slot
-// pair, ceil(n / 2) slots left); after the 5 levels every lane holds one
-// slot.  rs_owner<N>(lane) is the value index that slot totals (-1: a padding
+// pair, ceil(n / 2) slots left; the adds go two at a time as packed f32x2
+// adds, the same roundings); after the 5 levels every lane holds one slot.
+// rs_owner<N>(lane) is the value index that slot totals (-1: a padding
 // slot).  N = 9: 12 shuffles; N = 18: 20.
 template <int N, int O>
 __device__ __forceinline__ float rs_level(const float* x, int lane) {
   constexpr int M = (N + 1) / 2;
-  float y[M];
+  float y[M], kp[M], rv[M];
   const bool bit = lane & O;
 #pragma unroll
   for (int i = 0; i < M; ++i) {
     const float lo = x[i];
     const float hi = i + M < N ? x[i + M] : 0.0f;
     const float send = bit ? lo : hi;
-    const float keep = bit ? hi : lo;
-    y[i] = keep + __shfl_xor_sync(FULL_MASK, send, O);
+    kp[i] = bit ? hi : lo;
+    rv[i] = __shfl_xor_sync(FULL_MASK, send, O);
   }
+#pragma unroll
+  for (int i = 0; i + 1 < M; i += 2) {
+    const float2 t = __fadd2_rn(make_float2(kp[i], kp[i + 1]), make_float2(rv[i], rv[i + 1]));
+    y[i] = t.x; y[i + 1] = t.y;
+  }
+  if constexpr (M & 1) y[M - 1] = kp[M - 1] + rv[M - 1];
   if constexpr (O == 1) {
     static_assert(M == 1, "at most 32 values");
     return y[0];
