@@ -175,6 +175,73 @@ __global__ void k_tile_ranges(const void* __restrict__ keys_v, const uint64_t* _
   }
 }
 
+// The same for presorted u32 keys (mode 2) read four at a time: a thread
+// loads keys [4q, 4q + 4) with one 16-byte access and takes the key before and
+// after its four from the neighbouring lanes (lanes 0 and 31 load theirs), so
+// every key is read once instead of three times.  The warp walks the quads
+// together (the loop condition is the warp's first quad), which the shuffles
+// need.
+__global__ void __launch_bounds__(256) k_tile_ranges_u32x4(const uint32_t* __restrict__ k,
+                                                           const uint64_t* __restrict__ d_total, uint64_t cap,
+                                                           uint32_t num_tiles, uint32_t tiles_per_view,
+                                                           uint32_t tile_bits, uint32_t key_mask,
+                                                           uint32_t* __restrict__ ranges,
+                                                           unsigned long long* __restrict__ high_popc) {
+  const uint64_t K = min(*d_total, cap);
+  const uint64_t nq = (K + 3) >> 2;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
+  constexpr uint64_t NONE = ~0ull;  // no neighbour: differs from every masked key
+  uint32_t pc = 0;
+  for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q - lane < nq; q += step) {
+    const uint64_t j0 = q << 2;
+    uint32_t x[4] = {0u, 0u, 0u, 0u};
+    if (j0 + 3 < K) {
+      const uint4 v = *reinterpret_cast<const uint4*>(k + j0);
+      x[0] = v.x; x[1] = v.y; x[2] = v.z; x[3] = v.w;
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if (j0 + i < K) x[i] = k[j0 + i];
+    }
+    // the keys either side of this thread's four
+    uint32_t before = __shfl_up_sync(0xffffffffu, x[3], 1);
+    uint32_t after = __shfl_down_sync(0xffffffffu, x[0], 1);
+    if (lane == 0 && j0 > 0 && j0 - 1 < K) before = k[j0 - 1];
+    if (lane == 31 && j0 + 4 < K) after = k[j0 + 4];
+    uint64_t m[6];
+    m[0] = j0 > 0 ? (uint64_t)(before & key_mask) : NONE;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) m[i + 1] = j0 + i < K ? (uint64_t)(x[i] & key_mask) : NONE;
+    m[5] = j0 + 4 < K ? (uint64_t)(after & key_mask) : NONE;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const uint64_t j = j0 + i;
+      if (j >= K) break;
+      pc += __popc(x[i] & ~key_mask);
+      const uint64_t t = m[i + 1];
+      const uint32_t tile = (uint32_t)t & ((1u << tile_bits) - 1u);
+      if (tile >= tiles_per_view) continue;
+      const uint64_t idx = (t >> tile_bits) * tiles_per_view + tile;
+      if (idx >= num_tiles) continue;
+      if (m[i] != t) ranges[2 * idx] = (uint32_t)j;
+      if (m[i + 2] != t) ranges[2 * idx + 1] = (uint32_t)(j + 1);
+    }
+  }
+  if (high_popc) {
+    __shared__ uint32_t s_pc[8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) pc += __shfl_xor_sync(0xffffffffu, pc, o);
+    if (lane == 0) s_pc[threadIdx.x >> 5] = pc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned long long tot = 0;
+      for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) tot += s_pc[w];
+      if (tot) atomicAdd(high_popc, tot);
+    }
+  }
+}
+
 sc_status launch_tile_ranges(sc_ctx* ctx, const void* keys, int key_mode, const uint64_t* d_total, uint64_t cap,
                              uint32_t num_tiles, uint32_t* ranges, uint32_t tiles_per_view, uint32_t tile_bits,
                              uint32_t key_bits, uint64_t* high_popc) {
@@ -185,8 +252,14 @@ sc_status launch_tile_ranges(sc_ctx* ctx, const void* keys, int key_mode, const 
     k_tile_ranges<0><<<g, 256, 0, ctx->stream>>>(keys, d_total, cap, num_tiles, 0, 0, ~0u, ranges, nullptr);
   else if (key_mode == 1)
     k_tile_ranges<1><<<g, 256, 0, ctx->stream>>>(keys, d_total, cap, num_tiles, 0, 0, ~0u, ranges, nullptr);
-  else
+  else if (reinterpret_cast<uintptr_t>(keys) % 16 != 0)  // the 16-byte loads need an aligned array
     k_tile_ranges<2><<<g, 256, 0, ctx->stream>>>(keys, d_total, cap, num_tiles, tiles_per_view, tile_bits,
+                                                 key_bits >= 32 ? ~0u : (1u << key_bits) - 1u, ranges,
+                                                 reinterpret_cast<unsigned long long*>(high_popc));
+  else
+    k_tile_ranges_u32x4<<<(unsigned)std::min<uint64_t>(sc_div_up(sc_div_up(cap, 4), 256), (uint64_t)ctx->sm_count * 8),
+                          256, 0, ctx->stream>>>(static_cast<const uint32_t*>(keys), d_total, cap, num_tiles,
+                                                 tiles_per_view, tile_bits,
                                                  key_bits >= 32 ? ~0u : (1u << key_bits) - 1u, ranges,
                                                  reinterpret_cast<unsigned long long*>(high_popc));
   return sc_check_launch(ctx, "k_tile_ranges");

@@ -9,7 +9,7 @@
 //   item counts in depth order -> offsets                    gather + decoupled-look-back scan
 //   items (mask | view, super tile; splat) in depth order    k_super_emit (two-level binning)
 //   stable sort of the items by super tile                   onesweep u32 (super tile bits)
-//   per-super-tile ranges (+ pair count from the masks)      k_tile_ranges
+//   per-super-tile ranges (+ pair count from the masks)      k_tile_ranges_u32x4
 //   alpha-blend forward over the super-tile item lists       k_composite (item lists)
 //   alpha-blend backward, MSE dL/dC in its prologue          k_composite_backward (item lists)
 //   project backward over all views -> gradient rows         k_project_backward_shards (one shard)
