@@ -372,8 +372,7 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
         float2 R2 = make_float2(cr[0], cr[1]), G2 = make_float2(cg[0], cg[1]), B2 = make_float2(cb[0], cb[1]);
         const float2 fy2 = make_float2(fy[0], fy[1]);
         int lk0 = -1, lk1 = -1;  // this batch's last contributing entries, as list positions below
-#pragma unroll 2
-        for (uint32_t k = 0; k < cnt; ++k) {
+        auto blend1 = [&](uint32_t k) {
           const float4 ra = sb[3 * k], rb = sb[3 * k + 1], rc = sb[3 * k + 2];
           const EntryGeom e = entry_geom(fx, ra, rb);
           float2 dy, g, araw, al;
@@ -381,19 +380,31 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
           eval_alpha2(e, rb.z, fy2, ra.y, rc.w, dy, g, araw, al, v0, v1);
           v0 &= T2.x >= 1e-4f;
           v1 &= T2.y >= 1e-4f;
-          {  // without a branch: a pixel that skips gets alpha 0, which changes no bit
-            const float2 am = make_float2(v0 ? al.x : 0.0f, v1 ? al.y : 0.0f);
-            const float2 ta = __fmul2_rn(T2, am);
-            R2 = __ffma2_rn(ta, f2(rc.x), R2);
-            G2 = __ffma2_rn(ta, f2(rc.y), G2);
-            B2 = __ffma2_rn(ta, f2(rc.z), B2);
-            T2 = __fmul2_rn(T2, __fadd2_rn(f2(1.0f), make_float2(-am.x, -am.y)));
-            if constexpr (COUNT) w_pix += (uint32_t)v0 + (uint32_t)v1;
-            lk0 = v0 ? (int)k : lk0;
-            lk1 = v1 ? (int)k : lk1;
-            if ((v0 || v1) && T2.x < 1e-4f && T2.y < 1e-4f) break;
-          }
+          // without a branch: a pixel that skips gets alpha 0, which changes no bit
+          const float2 am = make_float2(v0 ? al.x : 0.0f, v1 ? al.y : 0.0f);
+          const float2 ta = __fmul2_rn(T2, am);
+          R2 = __ffma2_rn(ta, f2(rc.x), R2);
+          G2 = __ffma2_rn(ta, f2(rc.y), G2);
+          B2 = __ffma2_rn(ta, f2(rc.z), B2);
+          T2 = __fmul2_rn(T2, __fadd2_rn(f2(1.0f), make_float2(-am.x, -am.y)));
+          if constexpr (COUNT) w_pix += (uint32_t)v0 + (uint32_t)v1;
+          lk0 = v0 ? (int)k : lk0;
+          lk1 = v1 ? (int)k : lk1;
+        };
+        // one saturation test per four entries (1M splats, 8 views of 1920x1080:
+        // 0.986 ms with a test per entry, 0.928 per two, 0.893 per four): an
+        // entry past a pixel's saturation gives it alpha 0 and changes nothing
+        uint32_t k = 0;
+        bool sat = false;
+        for (; k + 3 < cnt; k += 4) {
+          blend1(k);
+          blend1(k + 1);
+          blend1(k + 2);
+          blend1(k + 3);
+          if (T2.x < 1e-4f && T2.y < 1e-4f) { sat = true; break; }
         }
+        if (!sat)
+          for (; k < cnt; ++k) blend1(k);
         if (lk0 >= 0) last[0] = position(b, (uint32_t)lk0) + 1;
         if (lk1 >= 0) last[1] = position(b, (uint32_t)lk1) + 1;
         done[0] = T2.x < 1e-4f;
