@@ -392,8 +392,9 @@ __global__ void __launch_bounds__(256) k_composite(const float4* __restrict__ re
           lk1 = v1 ? (int)k : lk1;
         };
         // one saturation test per four entries (1M splats, 8 views of 1920x1080:
-        // 0.986 ms with a test per entry, 0.928 per two, 0.893 per four): an
-        // entry past a pixel's saturation gives it alpha 0 and changes nothing
+        // 0.986 ms with a test per entry, 0.928 per two, 0.893 per four, no
+        // gain per eight at 69 registers): an entry past a pixel's saturation
+        // gives it alpha 0 and changes nothing
         uint32_t k = 0;
         bool sat = false;
         for (; k + 3 < cnt; k += 4) {
